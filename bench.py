@@ -1,0 +1,365 @@
+"""Coupled-step throughput of the B200 path (and the CPU reference arm).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2] [--impl b200|reference]
+
+One step is one coupled FSI step of the graded 128 x 128 x 256 workload
+(predict -> MG-PCG projection to relative residual 1e-8 -> marker tractions ->
+force spreading -> neo-Hookean MPM substep -> surface feedback) on synthetic
+seeded inputs already resident in HBM.  The JSON line carries:
+
+* value: coupled steps/s over all ranks (independent replicas per GPU);
+* e2e: the same through the public API with the fluid and particle state
+  uploaded from pinned host memory before and downloaded after every step;
+* roofline: the dominant kernel family's algorithmic bytes / CUDA-event time
+  against the measured HBM copy bandwidth;
+* cpu_baseline: the CPU oracle (restatement of the reference path) on the
+  host cores, one coupled step of the same workload;
+* clocks: SM clocks and throttle reasons sampled during the timed region.
+
+``--impl reference`` times only the CPU oracle (the reference algorithm on the
+host cores): the reference itself is Taichi-only and GPU-only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "steps/s; pressure solve ms to rel-res 1e-8, learned+mixed vs plain CG, 1×B200"
+WORKING_SET_NOTE = "working set per step > L2 (fluid vectors 13 x 34 MB + MPM grid), no extra flush"
+
+
+def _measured_peaks() -> dict:
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return json.loads(path.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+def _hbm_peak() -> tuple[float, str]:
+    peaks = _measured_peaks()
+    if "hbm_gbs" in peaks:
+        return float(peaks["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self) -> None:
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL,
+            )
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(smax)) if smax else None,
+            "samples": len(sm),
+            "reasons": sorted(reasons),
+        }
+
+
+def cpu_reference(cfg, steps: int, warmup: int, initial_velocity=None) -> dict:
+    """Time the CPU oracle's coupled step (all host threads)."""
+    from oracle import oracle as orc
+
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    scene = orc.OracleScene(cfg, variant="mirror", initial_velocity=initial_velocity, project_initial=initial_velocity is None)
+    for _ in range(warmup):
+        scene.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        scene.step()
+    dt = time.perf_counter() - t0
+    return {
+        "value": steps / dt,
+        "unit": "steps/s",
+        "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
+        "kind": "port",
+        "sample": f"{steps} coupled step(s) of {cfg.name} after {warmup} warm-up, CPU oracle (C++/OpenMP restatement of the reference)",
+        "seconds": dt,
+        "cg_iterations": int(scene.last_stats.iterations) if scene.last_stats is not None else None,
+    }
+
+
+def run_reference_arm(args, cfg) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    res = cpu_reference(cfg, args.steps, args.warmup)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": res["value"],
+        "unit": "steps/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 / res["value"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": cfg.name, "grid": list(cfg.grid_nodes), "mpm_nodes": list(cfg.mpm_nodes)},
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": res["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Taichi-only (GPU-only); this arm times its CPU restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    from easyfsi_b200 import scenarios
+
+    cfg = scenarios.CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference_arm(args, cfg)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from easyfsi_b200 import _native
+    from easyfsi_b200.scenarios import CoupledScene
+
+    scene = CoupledScene(cfg)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        scene.step()
+    torch.cuda.synchronize()
+    families = ["spmv_dir", "sweep_l0", "cg_update", "restrict_l0", "cg_dots", "p2g", "predict"]
+    for fam in families:
+        _native.kernel_timing_enable(fam, True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = _native.kernel_launches()
+    iters = []
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        scene.step()
+        iters.append(scene.last_cg_iterations)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = _native.kernel_launches() - launches0
+    clocks = sampler.stop()
+    elapsed_ms = start.elapsed_time(stop)
+    fam_stats = {}
+    for fam in families:
+        n, ms, by = _native.kernel_timing_read(fam)
+        _native.kernel_timing_enable(fam, False)
+        fam_stats[fam] = {"launches": n, "ms": ms, "bytes": by}
+    t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps / (max_ms / 1000.0)
+
+    # --- e2e through the public API with host-resident state ---
+    e2e = None
+    if not args.no_e2e:
+        fl, so, mk = scene.fluid, scene.solid, scene.markers
+        n = so.particle_count
+        host_in = {
+            "velocity": fl.velocity.tensor.cpu().pin_memory(),
+            "x": so.x.tensor[:n].cpu().pin_memory(),
+            "v": so.v.tensor[:n].cpu().pin_memory(),
+            "C": so.C.tensor[:n].cpu().pin_memory(),
+            "F": so.F.tensor[:n].cpu().pin_memory(),
+            "markers": mk.x_gamma_m.tensor.cpu().pin_memory(),
+        }
+        host_out = {
+            "velocity": torch.empty_like(fl.velocity.tensor, device="cpu").pin_memory(),
+            "pressure": torch.empty_like(fl.pressure.tensor, device="cpu").pin_memory(),
+            "x": torch.empty_like(so.x.tensor[:n], device="cpu").pin_memory(),
+        }
+        h2d = sum(t_.numel() * t_.element_size() for t_ in host_in.values())
+        d2h = sum(t_.numel() * t_.element_size() for t_ in host_out.values())
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fl.velocity.tensor.copy_(host_in["velocity"], non_blocking=True)
+            so.x.tensor[:n].copy_(host_in["x"], non_blocking=True)
+            so.v.tensor[:n].copy_(host_in["v"], non_blocking=True)
+            so.C.tensor[:n].copy_(host_in["C"], non_blocking=True)
+            so.F.tensor[:n].copy_(host_in["F"], non_blocking=True)
+            mk.x_gamma_m.tensor.copy_(host_in["markers"], non_blocking=True)
+            scene.step()
+            host_out["velocity"].copy_(fl.velocity.tensor, non_blocking=True)
+            host_out["pressure"].copy_(fl.pressure.tensor, non_blocking=True)
+            host_out["x"].copy_(so.x.tensor[:n], non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        te = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {
+            "value": world * args.steps / (float(te.item()) / 1000.0),
+            "unit": "steps/s",
+            "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h),
+        }
+
+    peak, peak_kind = _hbm_peak()
+    dom = max(fam_stats, key=lambda f: fam_stats[f]["ms"])
+    st = fam_stats[dom]
+    achieved = (st["bytes"] / max(st["ms"], 1e-12)) * 1e3 / 1e9 if st["launches"] else 0.0
+    traffic = None
+    traffic_path = REPO / "profiles" / "dram_traffic.json"
+    if traffic_path.exists():
+        try:
+            per_unit = json.loads(traffic_path.read_text()).get(dom, {}).get("bytes_per_cell")
+            if per_unit is not None and st["launches"]:
+                traffic = per_unit * scene.fluid.nx * scene.fluid.ny * scene.fluid.nz
+        except Exception:
+            traffic = None
+    roofline = {
+        "bound": "hbm",
+        "kernel": dom,
+        "achieved": achieved,
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+        "traffic": traffic,
+        "avg_launch_us": 1000.0 * st["ms"] / max(st["launches"], 1),
+        "algorithmic_bytes_per_launch": st["bytes"] / max(st["launches"], 1),
+    }
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference(cfg, args.cpu_steps, 0, initial_velocity=scene.fluid.velocity.to_numpy())
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {exc}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {
+                "workload": cfg.name,
+                "grid": list(cfg.grid_nodes),
+                "mpm_nodes": list(cfg.mpm_nodes),
+                "particles": int(scene.solid.particle_count),
+                "markers": int(scene.markers.marker_count),
+                "dt_s": cfg.dt_s,
+                "cg": "flexible MG-PCG (fv_multigrid 2/24/2), rel-res 1e-8",
+                "parallelism": f"replicas x{world}",
+                "l2": WORKING_SET_NOTE,
+            },
+            "pressure_solve": {
+                "cg_iterations_mean": float(np.mean(iters)) if iters else None,
+                "cg_iterations": iters,
+            },
+            "kernel_families": fam_stats,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

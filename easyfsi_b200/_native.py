@@ -1,0 +1,216 @@
+"""ctypes binding of the easyfsi_b200 C ABI (include/easyfsi_b200.h).
+
+This is the Python side of the drop-in boundary: the solver classes call the
+CUDA library only through the functions bound here.  There is no fallback: if
+the library cannot be loaded the import of a solver fails loudly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int32, c_void_p
+from pathlib import Path
+
+_LIB_NAME = "libeasyfsi_b200.so"
+_PACKAGE_DIR = Path(__file__).resolve().parent
+
+
+class LevelDesc(Structure):
+    _fields_ = [
+        ("nx", c_int32),
+        ("ny", c_int32),
+        ("nz", c_int32),
+        ("wx", c_void_p),
+        ("wy", c_void_p),
+        ("wz", c_void_p),
+        ("cdx", c_void_p),
+        ("cdy", c_void_p),
+        ("cdz", c_void_p),
+    ]
+
+
+class PcgParams(Structure):
+    _fields_ = [
+        ("max_iters", c_int32),
+        ("precond", c_int32),
+        ("remove_mean", c_int32),
+        ("outlet", c_int32),
+        ("iface_active", c_int32),
+        ("use_graphs", c_int32),
+        ("tolerance", c_double),
+    ]
+
+
+class CgStats(Structure):
+    _fields_ = [
+        ("iterations", c_int32),
+        ("converged", c_int32),
+        ("breakdown_code", c_int32),
+        ("breakdown_reason", c_int32),
+        ("host_residual_checks", c_int32),
+        ("restart_count", c_int32),
+        ("mean_projection_count", c_int32),
+        ("used_mg", c_int32),
+        ("initial_relative_residual", c_double),
+        ("relative_residual", c_double),
+        ("breakdown_dAd", c_double),
+        ("b_norm", c_double),
+    ]
+
+
+class GridAxes(Structure):
+    _fields_ = [("fx", c_void_p), ("fy", c_void_p), ("fz", c_void_p), ("cx", c_void_p), ("cy", c_void_p), ("cz", c_void_p)]
+
+
+class MpmState(Structure):
+    _fields_ = [
+        ("particle_count", c_int32),
+        ("nx", c_int32),
+        ("ny", c_int32),
+        ("nz", c_int32),
+        ("bmin", c_float * 3),
+        ("dx", c_float * 3),
+        ("x", c_void_p),
+        ("v", c_void_p),
+        ("C", c_void_p),
+        ("F", c_void_p),
+        ("mass", c_void_p),
+        ("volume", c_void_p),
+        ("fext", c_void_p),
+        ("fixed", c_void_p),
+        ("region", c_void_p),
+        ("rest_x", c_void_p),
+        ("normal", c_void_p),
+        ("area", c_void_p),
+        ("rest_normal", c_void_p),
+        ("rest_area", c_void_p),
+        ("grid_mass", c_void_p),
+        ("grid_velocity", c_void_p),
+        ("grid_force", c_void_p),
+    ]
+
+
+P = c_void_p
+I = c_int32
+F = c_float
+D = c_double
+
+# name -> argtypes (all return int status except the two string getters)
+_PROTOTYPES: dict[str, list] = {
+    "efsi_kernel_timing_enable": [I, I],
+    "efsi_kernel_timing_read": [I, POINTER(ctypes.c_int64), POINTER(c_double), POINTER(c_double)],
+    "efsi_fv_plan_create": [POINTER(LevelDesc), I, I, POINTER(c_void_p)],
+    "efsi_fv_plan_destroy": [P],
+    "efsi_fv_set_masks": [P, P, P, P, P, P],
+    "efsi_compute_divergence": [P, P, I, P, P],
+    "efsi_mg_prepare_level0": [P, P, P, P, F, P, P],
+    "efsi_fv_apply": [P, P, P, I, P],
+    "efsi_fv_diagonal": [P, P, I, P],
+    "efsi_apply_jacobi_preconditioner": [P, P, P, P, P],
+    "efsi_weighted_dot": [P, P, P, POINTER(c_double), P],
+    "efsi_fv_jacobi_sweep": [P, I, P, P, P, I, D, P],
+    "efsi_fv_residual": [P, I, P, P, P, I, P],
+    "efsi_mg_restrict": [P, I, P, P, P, P, P, P, P],
+    "efsi_legacy_jacobi_solve": [P, P, P, F, F, F, F, I, I, P, P, P],
+    "efsi_mg_prolong": [P, I, P, P, D, P],
+    "efsi_mg_vcycle": [P, P, P, I, I, I, I, P],
+    "efsi_fv_pcg_solve": [P, P, P, POINTER(PcgParams), POINTER(CgStats), P],
+    "efsi_fv_multigrid_solve": [P, P, P, I, I, I, P],
+    "efsi_fv_jacobi_solve": [P, P, P, I, I, P],
+    "efsi_subtract_pressure_gradient": [P, P, P, P, P, F, I, P, P],
+    "efsi_apply_closed_boundary": [P, I, P, P],
+    "efsi_apply_zmin_no_backflow": [P, P, P],
+    "efsi_apply_velocity_dirichlet_rows": [P, P, P, F, P, P, P],
+    "efsi_predict": [P, POINTER(GridAxes), P, F, F, I, P, P],
+    "efsi_divergence_stats": [P, P, P, P, I, I, POINTER(c_double), P],
+    "efsi_spread_surface_forces": [P, POINTER(GridAxes), P, P, I, F, F, F, F, P, P, P],
+    "efsi_apply_body_force": [P, P, F, F, P, P, P],
+    "efsi_mpm_plan_create": [I, I, I, I, POINTER(c_void_p)],
+    "efsi_mpm_plan_destroy": [P],
+    "efsi_mpm_step": [P, POINTER(MpmState), F, F, F, F, I, I, P, P],
+    "efsi_sample_pressure_tractions": [I, I, I, POINTER(GridAxes), P, P, P, P, P, I, P, P, P, I, I, F, P, P, P, P],
+    "efsi_compute_marker_forces": [I, P, P, P, P],
+    "efsi_clear_external_forces": [I, P, P, P],
+    "efsi_bin_plan_create": [I, POINTER(c_float), POINTER(c_float), F, POINTER(c_void_p)],
+    "efsi_bin_plan_destroy": [P],
+    "efsi_bin_particles": [P, P, I, P],
+    "efsi_scatter_marker_forces": [P, I, P, P, P, P, P, P],
+    "efsi_surface_feedback": [P, I, P, P, P, P, P, P, P, P, F, P, P],
+}
+
+_lib = None
+
+
+def library_path() -> Path:
+    override = os.environ.get("EASYFSI_B200_LIB")
+    return Path(override) if override else _PACKAGE_DIR / _LIB_NAME
+
+
+def load():
+    """Load (once) and return the CUDA library with typed prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not path.exists():
+        raise RuntimeError(
+            f"easyfsi_b200 CUDA library not found at {path}; build it with `python -m easyfsi_b200.build`"
+        )
+    lib = ctypes.CDLL(str(path))
+    lib.efsi_last_error.restype = c_char_p
+    lib.efsi_last_error.argtypes = []
+    lib.efsi_version.restype = c_char_p
+    lib.efsi_version.argtypes = []
+    lib.efsi_kernel_launch_count.restype = ctypes.c_uint64
+    lib.efsi_kernel_launch_count.argtypes = []
+    for name, args in _PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = c_int32
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_names() -> list[str]:
+    return ["efsi_last_error", "efsi_version", "efsi_kernel_launch_count", *_PROTOTYPES.keys()]
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+def check(status: int, what: str = "") -> None:
+    if status != 0:
+        msg = load().efsi_last_error().decode(errors="replace")
+        raise NativeError(f"{what or 'easyfsi_b200'} failed (status {status}): {msg}")
+
+
+def kernel_launches() -> int:
+    return int(load().efsi_kernel_launch_count())
+
+
+KERNEL_FAMILIES = {
+    "spmv_dir": 0,
+    "sweep_l0": 1,
+    "cg_update": 2,
+    "restrict_l0": 3,
+    "cg_dots": 4,
+    "p2g": 5,
+    "predict": 6,
+}
+
+
+def kernel_timing_enable(family: str, enable: bool = True) -> None:
+    call("efsi_kernel_timing_enable", KERNEL_FAMILIES[family], 1 if enable else 0)
+
+
+def kernel_timing_read(family: str) -> tuple[int, float, float]:
+    """(launches, total ms, total algorithmic bytes) of a timed kernel family."""
+    n, ms, by = ctypes.c_int64(0), c_double(0.0), c_double(0.0)
+    call("efsi_kernel_timing_read", KERNEL_FAMILIES[family], ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by))
+    return int(n.value), float(ms.value), float(by.value)
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args), name)

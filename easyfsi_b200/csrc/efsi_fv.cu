@@ -1,0 +1,1512 @@
+// Finite-volume pressure projection on a graded Cartesian grid, B200 path.
+//
+// Replaces the Taichi kernels of simulation_core/fluid.py that sit on the
+// pressure-projection hot path: the variable-spacing 7-point operator
+// (fluid.py:4080-4456), its damped-Jacobi smoother (fluid.py:4224-4273), the
+// multigrid residual / restriction / prolongation (fluid.py:5262-5406), the
+// weighted CG inner products and updates (fluid.py:4459-4726) and the flexible
+// PCG driver (fluid.py:6535-6811).
+//
+// Layout in HBM: every cell field is C order (nx, ny, nz), k fastest; level 0
+// keeps the reference's f64 pressure / CG vectors, coarse levels are f32.  The
+// obstacle / Dirichlet / outlet structure of a level is folded once per
+// projection into one byte per cell (six "face open" bits, fluid bit, solid
+// bit), and the f32 axis metrics into per-axis f64 face-coefficient tables, so
+// a stencil evaluation reads 1 byte of structure per cell instead of seven
+// 4-byte obstacle values.
+//
+// Fusions relative to the reference's kernel sequence (each keeps the
+// reference's per-element arithmetic):
+//   * SpMV + <d, Ad>_V + alpha, and the direction update d = z + beta d is
+//     evaluated inside the SpMV (d ping-pongs between two buffers);
+//   * the CG update also forms delta = r_new - r_old for the flexible beta;
+//   * z's zero-mean projection is applied on the fly by its consumers;
+//   * the V-cycle's level residual is formed inside the restriction, the
+//     prolongation inside the first post-smoothing sweep, and the first
+//     pre-smoothing sweep uses the zero initial guess;
+//   * every scalar reduction is a deterministic two-stage block reduction whose
+//     last block also evaluates alpha / beta / means (no extra launches).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "efsi_fv_internal.cuh"
+
+namespace efsi {
+
+#define EFSI_CELL_PROLOGUE(L)                                 \
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;       \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;       \
+  const int i = blockIdx.z * blockDim.z + threadIdx.z;       \
+  const bool active = (i < (L).nx && j < (L).ny && k < (L).nz); \
+  const int64_t c = active ? cidx(i, j, k, (L).ny, (L).nz) : 0;
+
+// ---------------------------------------------------------------------------
+// Setup kernels
+// ---------------------------------------------------------------------------
+
+// f64 face coefficient tables: c-[i] = 1/(w[i] cd[i]), c+[i] = 1/(w[i] cd[i+1]).
+__global__ void k_axis_coef(const float* w, const float* cd, int n, double* cm, double* cp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  cm[i] = i > 0 ? 1.0 / ((double)w[i] * (double)cd[i]) : 0.0;
+  cp[i] = i < n - 1 ? 1.0 / ((double)w[i] * (double)cd[i + 1]) : 0.0;
+}
+
+__global__ void k_mask_from_obstacle(int nx, int ny, int nz, const int32_t* obs, const int32_t* va,
+                                     const float* vw, uint8_t* mask, float* fw) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= nx || j >= ny || k >= nz) return;
+  const int64_t c = cidx(i, j, k, ny, nz);
+  const int64_t sx = (int64_t)ny * nz, sy = nz;
+  unsigned m = 0;
+  if (i > 0 && obs[c - sx] == 0) m |= M_XM;
+  if (i < nx - 1 && obs[c + sx] == 0) m |= M_XP;
+  if (j > 0 && obs[c - sy] == 0) m |= M_YM;
+  if (j < ny - 1 && obs[c + sy] == 0) m |= M_YP;
+  if (k > 0 && obs[c - 1] == 0) m |= M_ZM;
+  if (k < nz - 1 && obs[c + 1] == 0) m |= M_ZP;
+  if (obs[c] == 0) m |= M_FLUID;
+  if (obs[c] == 1) m |= M_SOLID;
+  mask[c] = (uint8_t)m;
+  if (fw != nullptr) {
+    float w = 1.0f;
+    if (va != nullptr && va[c] != 0) w = fminf(fmaxf(vw[c], 0.0f), 1.0f);
+    fw[c] = w;
+  }
+}
+
+// Coarse obstacle / Dirichlet flag and weight / interface diagonal of level
+// l+1 from level l (fluid.py:5331-5382).  The f32 locals of the reference
+// round every accumulation to f32; a product of an f64 fine value with the f32
+// cell volume is formed in f64 first.
+template <typename TF>
+__global__ void k_coarsen_structure(int fnx, int fny, int fnz, const int32_t* fobs, const int32_t* fva,
+                                    const float* fvw, const TF* fiface, const float* fwx, const float* fwy,
+                                    const float* fwz, int cnx, int cny, int cnz, int32_t* cobs, int32_t* cva,
+                                    float* cvw, float* ciface) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= cnx || j >= cny || k >= cnz) return;
+  float wdiag = 0.0f, free_vol = 0.0f, vdw = 0.0f;
+  int ocount = 0, vcount = 0;
+  for (int oi = 0; oi < 2; ++oi)
+    for (int oj = 0; oj < 2; ++oj)
+      for (int ok = 0; ok < 2; ++ok) {
+        int fi = 2 * i + oi, fj = 2 * j + oj, fk = 2 * k + ok;
+        if (fi < fnx && fj < fny && fk < fnz) {
+          int64_t f = cidx(fi, fj, fk, fny, fnz);
+          if (fva != nullptr && fva[f] != 0) {
+            vcount += 1;
+            vdw = fmaxf(vdw, fvw[f]);
+          }
+          if (fobs[f] == 1) {
+            ocount += 1;
+          } else {
+            float vol = __fmul_rn(__fmul_rn(fwx[fi], fwy[fj]), fwz[fk]);
+            if (fiface != nullptr) {
+              if (sizeof(TF) == 8)
+                wdiag = (float)__dadd_rn((double)wdiag, __dmul_rn((double)fiface[f], (double)vol));
+              else
+                wdiag = __fadd_rn(wdiag, __fmul_rn((float)fiface[f], vol));
+            }
+            free_vol = __fadd_rn(free_vol, vol);
+          }
+        }
+      }
+  int64_t cc = cidx(i, j, k, cny, cnz);
+  cobs[cc] = ocount > 0 ? 1 : 0;
+  if (ciface != nullptr) ciface[cc] = ocount > 0 ? 0.0f : __fdiv_rn(wdiag, fmaxf(free_vol, 1.0e-30f));
+  if (cva != nullptr) {
+    cva[cc] = vcount > 0 ? 1 : 0;
+    cvw[cc] = vcount > 0 ? vdw : 0.0f;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Level kernels (smoother, residual, restriction, prolongation)
+// ---------------------------------------------------------------------------
+
+// Right-hand side of a level row: the level's rhs array, or -r at level 0 of
+// the PCG's V-cycle (legacy_rhs = -positive_rhs, fluid.py:4485-4500).
+template <typename TP, bool kNegR>
+__device__ __forceinline__ double rhs_at(const void* rhs, int64_t c, unsigned m) {
+  if (kNegR) {
+    if (m & M_SOLID) return 0.0;
+    return -__ldg(reinterpret_cast<const double*>(rhs) + c);
+  }
+  return (double)__ldg(reinterpret_cast<const TP*>(rhs) + c);
+}
+
+struct ProlongSrc {
+  const float* pc;  // coarse iterate, null when no prolongation is fused
+  int cnx, cny, cnz;
+  float scale;
+};
+
+template <typename TP>
+__device__ __forceinline__ double fused_iterate(const TP* __restrict__ p, const ProlongSrc& pr, int64_t cell, int ii,
+                                                int jj, int kk, bool fluid) {
+  if (pr.pc == nullptr) return (double)__ldg(p + cell);
+  TP v = __ldg(p + cell);
+  if (fluid) {
+    int ci = min(ii / 2, pr.cnx - 1), cj = min(jj / 2, pr.cny - 1), ck = min(kk / 2, pr.cnz - 1);
+    float corr = __fmul_rn(pr.scale, __ldg(pr.pc + cidx(ci, cj, ck, pr.cny, pr.cnz)));
+    if (sizeof(TP) == 8)
+      v = (TP)__dadd_rn((double)v, (double)corr);
+    else
+      v = (TP)__fadd_rn((float)v, corr);
+  }
+  return (double)v;
+}
+
+// One damped-Jacobi sweep (fluid.py:4224-4273), out of place.
+//   kZero   : the input iterate is identically zero (first sweep of a
+//             V-cycle level), so p is not read.
+//   pr.pc   : fuse the prolongation p += s * p_coarse (fluid.py:5391-5406).
+//   partials: when not null, also reduce sum_fluid out * V (z mean, level 0).
+template <typename TP, bool kNegR, bool kZero>
+__global__ void __launch_bounds__(256) k_sweep(LevelDev L, const TP* __restrict__ p, const void* rhs,
+                                               TP* __restrict__ out, int outlet, double omega, ProlongSrc pr,
+                                               double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  double zv = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    if (m & M_SOLID) {
+      out[c] = (TP)0;
+    } else {
+      double ns, den;
+      if (kZero) {
+        den = 0.0;
+        ns = 0.0;
+        // denominator only (neighbour values are zero)
+        auto zero = [](int64_t, int, int, int) { return 0.0; };
+        stencil(L, zero, i, j, k, c, m, outlet, ns, den);
+      } else {
+        auto val = [&](int64_t cell, int ii, int jj, int kk) { return fused_iterate(p, pr, cell, ii, jj, kk, true); };
+        stencil(L, val, i, j, k, c, m, outlet, ns, den);
+      }
+      den += iface_at<TP>(L, c);
+      TP res;
+      if (den <= 0.0) {
+        res = (TP)0;
+      } else {
+        double jv = (ns - rhs_at<TP, kNegR>(rhs, c, m)) / den;
+        double pc = kZero ? 0.0 : fused_iterate(p, pr, c, i, j, k, (m & M_FLUID) != 0);
+        res = (TP)(pc + omega * (jv - pc));
+      }
+      out[c] = res;
+      if (partials != nullptr && (m & M_FLUID)) zv = (double)res * vol64(L, i, j, k);
+    }
+  }
+  if (partials != nullptr) {
+    double v[1] = {zv}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_z = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->zproj = 1;
+      }
+    }
+  }
+}
+
+// fluid.py:5262-5307 residual of one row (level storage precision).
+template <typename TP, bool kNegR>
+__device__ __forceinline__ TP row_residual(const LevelDev& L, const TP* __restrict__ p, const void* rhs, int i, int j,
+                                           int k, int64_t c, unsigned m, int outlet) {
+  if (m & M_SOLID) return (TP)0;
+  double ns, den;
+  auto val = [&](int64_t cell, int, int, int) { return (double)__ldg(p + cell); };
+  stencil(L, val, i, j, k, c, m, outlet, ns, den);
+  den += iface_at<TP>(L, c);
+  double applied = ns - den * (double)__ldg(p + c);
+  return (TP)(rhs_at<TP, kNegR>(rhs, c, m) - applied);
+}
+
+template <typename TP, bool kNegR>
+__global__ void __launch_bounds__(256) k_residual(LevelDev L, const TP* __restrict__ p, const void* rhs,
+                                                  TP* __restrict__ res, int outlet) {
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const unsigned m = __ldg(L.mask + c);
+  res[c] = row_residual<TP, kNegR>(L, p, rhs, i, j, k, c, m, outlet);
+}
+
+// fluid.py:5310-5388 volume-weighted restriction of the residual, with the
+// fine residual formed on the fly (kFromP) or read from an array.
+template <typename TP, bool kNegR, bool kFromP>
+__global__ void __launch_bounds__(256) k_restrict(LevelDev F, const TP* __restrict__ p_or_res, const void* rhs,
+                                                  int outlet, int cnx, int cny, int cnz, float* __restrict__ crhs) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= cnx || j >= cny || k >= cnz) return;
+  float wres = 0.0f, free_vol = 0.0f;
+  int ocount = 0;
+#pragma unroll
+  for (int oi = 0; oi < 2; ++oi)
+#pragma unroll
+    for (int oj = 0; oj < 2; ++oj)
+#pragma unroll
+      for (int ok = 0; ok < 2; ++ok) {
+        int fi = 2 * i + oi, fj = 2 * j + oj, fk = 2 * k + ok;
+        if (fi < F.nx && fj < F.ny && fk < F.nz) {
+          int64_t f = cidx(fi, fj, fk, F.ny, F.nz);
+          unsigned m = __ldg(F.mask + f);
+          if (m & M_SOLID) {
+            ocount += 1;
+          } else {
+            float vol = __fmul_rn(__fmul_rn(__ldg(F.wx + fi), __ldg(F.wy + fj)), __ldg(F.wz + fk));
+            TP r = kFromP ? row_residual<TP, kNegR>(F, p_or_res, rhs, fi, fj, fk, f, m, outlet) : __ldg(p_or_res + f);
+            if (sizeof(TP) == 8)
+              wres = (float)__dadd_rn((double)wres, __dmul_rn((double)r, (double)vol));
+            else
+              wres = __fadd_rn(wres, __fmul_rn((float)r, vol));
+            free_vol = __fadd_rn(free_vol, vol);
+          }
+        }
+      }
+  crhs[cidx(i, j, k, cny, cnz)] = ocount > 0 ? 0.0f : __fdiv_rn(wres, fmaxf(free_vol, 1.0e-30f));
+}
+
+template <typename TP>
+__global__ void __launch_bounds__(256) k_prolong(LevelDev L, TP* __restrict__ p, ProlongSrc pr) {
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const unsigned m = __ldg(L.mask + c);
+  if (m & M_FLUID) p[c] = (TP)fused_iterate(p, pr, c, i, j, k, true);
+}
+
+// ---------------------------------------------------------------------------
+// Level-0 CG kernels (f64)
+// ---------------------------------------------------------------------------
+
+// z' : the zero-mean projected preconditioned residual (fluid.py:4716-4722),
+// evaluated where it is consumed.
+__device__ __forceinline__ double zp_at(const double* __restrict__ z, const CgScalars& s, int64_t c, unsigned m,
+                                        int zproj) {
+  double zv = __ldg(z + c);
+  if (!zproj) return zv;
+  return (m & M_FLUID) ? zv - s.mean_z : 0.0;
+}
+
+// d_new = z' (copy) or z' + beta d_old (fluid.py:4604-4611, masked), then
+// Ad = A d_new (fluid.py:4312-4345), <d, Ad>_V and alpha (fluid.py:4567-4574).
+template <bool kCopy>
+__global__ void __launch_bounds__(256) k_spmv_dir(LevelDev L, const double* __restrict__ z,
+                                                  const double* __restrict__ d_old, double* __restrict__ d_new,
+                                                  double* __restrict__ Ad, int outlet, double* partials,
+                                                  CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  const double beta = kCopy ? 0.0 : sc->beta;
+  const int zproj = sc->zproj;
+  const double mz = sc->mean_z;
+  CgScalars s;
+  s.mean_z = mz;
+  double part = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    // Neighbours in the stencil are open (obstacle == 0, hence fluid).
+    auto dval = [&](int64_t cell, int, int, int) {
+      double zz = __ldg(z + cell);
+      if (zproj) zz = zz - mz;
+      return kCopy ? zz : zz + beta * __ldg(d_old + cell);
+    };
+    double dc;
+    if (m & M_SOLID) {
+      dc = 0.0;
+    } else {
+      double zz = zp_at(z, s, c, m, zproj);
+      dc = kCopy ? zz : zz + beta * __ldg(d_old + c);
+    }
+    d_new[c] = dc;
+    double out;
+    if (m & M_SOLID) {
+      out = 0.0;
+    } else {
+      double ns, den;
+      stencil(L, dval, i, j, k, c, m, outlet, ns, den);
+      out = (den + iface_at<double>(L, c)) * dc - ns;
+    }
+    Ad[c] = out;
+    if (m & M_FLUID) part = dc * out * vol64(L, i, j, k);
+  }
+  double v[1] = {part}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      double dAd = t[0];
+      sc->dAd = dAd;
+      sc->alpha = 0.0;
+      if (dAd <= 0.0) {
+        if (sc->code == 0) sc->code_dAd = dAd;
+        sc->code = 1;
+      } else {
+        sc->alpha = sc->rz / dAd;
+      }
+    }
+  }
+}
+
+// fluid.py:4577-4587 _cg_apply_alpha_kernel with delta = r_new - r_old
+// (fluid.py:6794) and optional partial sums of x V, r V (mean projection) and
+// r r V (residual check).
+template <bool kDelta>
+__global__ void __launch_bounds__(256) k_cg_update(LevelDev L, double* __restrict__ x, const double* __restrict__ d,
+                                                   double* __restrict__ r, const double* __restrict__ Ad,
+                                                   double* __restrict__ delta, int want_means, int want_rr,
+                                                   double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  const double alpha = sc->alpha;
+  double px = 0.0, pr = 0.0, prr = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    if (m & M_SOLID) {
+      x[c] = 0.0;
+      r[c] = 0.0;
+      if (kDelta) delta[c] = 0.0;
+    } else {
+      double r_old = r[c];
+      double xn = x[c] + alpha * __ldg(d + c);
+      double rn = r_old - alpha * __ldg(Ad + c);
+      x[c] = xn;
+      r[c] = rn;
+      if (kDelta) delta[c] = 1.0 * rn + -1.0 * r_old;
+      if (m & M_FLUID) {
+        double V = vol64(L, i, j, k);
+        px = xn * V;
+        pr = rn * V;
+        prr = rn * rn * V;
+      }
+    }
+  }
+  if (want_means) {
+    double v[2] = {px, pr}, t[2];
+    if (grid_sum<2>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_x = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->mean_r = sc->free_vol > 0.0 ? 1.0 * t[1] / sc->free_vol : 0.0;
+      }
+    }
+  } else if (want_rr) {
+    double v[1] = {prr}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) sc->rr = t[0];
+    }
+  }
+}
+
+// Subtract the means found by k_cg_update from x and r (fluid.py:6685-6689),
+// then reduce r r V for the residual check.
+__global__ void __launch_bounds__(256) k_sub_mean_xr(LevelDev L, double* __restrict__ x, double* __restrict__ r,
+                                                     double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  const double mx = sc->mean_x, mr = sc->mean_r;
+  double prr = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    if (m & M_FLUID) {
+      x[c] = x[c] - mx;
+      double rn = r[c] - mr;
+      r[c] = rn;
+      prr = rn * rn * vol64(L, i, j, k);
+    } else {
+      x[c] = 0.0;
+      r[c] = 0.0;
+    }
+  }
+  double v[1] = {prr}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) sc->rr = t[0];
+  }
+}
+
+// rz_new = <r, z'>_V and (flexible) beta numerator <z', delta>_V, then beta
+// (fluid.py:4590-4601) and rz <- rz_new; kRestart instead stores rz (initial
+// and restarted directions, fluid.py:6662, 6780).
+template <bool kMG, bool kRestart>
+__global__ void __launch_bounds__(256) k_cg_dots(LevelDev L, const double* __restrict__ r,
+                                                 const double* __restrict__ z, const double* __restrict__ delta,
+                                                 double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  CgScalars s;
+  s.mean_z = sc->mean_z;
+  const int zproj = sc->zproj;
+  double a = 0.0, b = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    if (m & M_FLUID) {
+      double V = vol64(L, i, j, k);
+      double zz = zp_at(z, s, c, m, zproj);
+      a = __ldg(r + c) * zz * V;
+      if (kMG && !kRestart) b = zz * __ldg(delta + c) * V;
+    }
+  }
+  double v[2] = {a, b}, t[2];
+  if (grid_sum<2>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      if (kRestart) {
+        sc->rz = t[0];
+      } else {
+        double rz = sc->rz, rz_new = t[0];
+        sc->rz_new = rz_new;
+        sc->beta_num = t[1];
+        double beta = 0.0;
+        if (rz <= 1.0e-300 || rz_new <= 0.0) {
+          sc->code = 2;
+        } else if (kMG) {
+          beta = t[1] / rz;
+          if (beta < 0.0) beta = 0.0;
+        } else {
+          beta = rz_new / rz;
+        }
+        sc->beta = beta;
+        sc->rz = rz_new;
+      }
+    }
+  }
+}
+
+// fluid.py:4503-4516 Jacobi preconditioner, optionally with the z mean sums.
+__global__ void __launch_bounds__(256) k_jacobi_precond(LevelDev L, const double* __restrict__ diag,
+                                                        const double* __restrict__ r, double* __restrict__ z,
+                                                        int want_mean, double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  double pz = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    double zv;
+    if (m & M_SOLID) {
+      zv = 0.0;
+    } else {
+      double dg = __ldg(diag + c);
+      zv = dg > 0.0 ? __ldg(r + c) / dg : 0.0;
+    }
+    z[c] = zv;
+    if (m & M_FLUID) pz = zv * vol64(L, i, j, k);
+  }
+  if (want_mean) {
+    double v[1] = {pz}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_z = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->zproj = 1;
+      }
+    }
+  }
+}
+
+// fluid.py:4677-4693 with multiplier -1 on the level-0 rhs, plus the free
+// volume (computed in the same pass as the reference does).
+__global__ void __launch_bounds__(256) k_rhs_mean(LevelDev L, const double* __restrict__ rhs, double multiplier,
+                                                  double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  double a = 0.0, b = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    if (m & M_FLUID) {
+      double V = vol64(L, i, j, k);
+      a = __ldg(rhs + c) * V;
+      b = V;
+    }
+  }
+  double v[2] = {a, b}, t[2];
+  if (grid_sum<2>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      sc->free_vol = t[1];
+      sc->mean_b = t[1] > 0.0 ? multiplier * t[0] / t[1] : 0.0;
+    }
+  }
+}
+
+// b = -rhs - mean (fluid.py:4472-4482), <b, b>_V.
+__global__ void __launch_bounds__(256) k_build_b(LevelDev L, const double* __restrict__ rhs, int use_mean,
+                                                 double* __restrict__ b, double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  const double mean = use_mean ? sc->mean_b : 0.0;
+  double pb = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    double bv = (m & M_SOLID) ? 0.0 : -__ldg(rhs + c) - mean;
+    b[c] = bv;
+    if (m & M_FLUID) pb = bv * bv * vol64(L, i, j, k);
+  }
+  double v[1] = {pb}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) sc->bnorm2 = t[0];
+  }
+}
+
+// r = b - A x (fluid.py:6613-6614 / 6744-6754), optionally with r V sums
+// (mean) or r r V (no mean projection).
+__global__ void __launch_bounds__(256) k_true_residual(LevelDev L, const double* __restrict__ x,
+                                                       const double* __restrict__ b, double* __restrict__ r,
+                                                       int outlet, int want_mean, double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  double pa = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    double rv;
+    if (m & M_SOLID) {
+      rv = 0.0;
+    } else {
+      double ns, den;
+      auto val = [&](int64_t cell, int, int, int) { return __ldg(x + cell); };
+      stencil(L, val, i, j, k, c, m, outlet, ns, den);
+      double ax = (den + iface_at<double>(L, c)) * __ldg(x + c) - ns;
+      rv = 1.0 * __ldg(b + c) + -1.0 * ax;
+    }
+    r[c] = rv;
+    if (m & M_FLUID) pa = want_mean ? rv * vol64(L, i, j, k) : rv * rv * vol64(L, i, j, k);
+  }
+  double v[1] = {pa}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      if (want_mean)
+        sc->mean_r = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+      else
+        sc->rr = t[0];
+    }
+  }
+}
+
+// r -= mean_r (fluid), then r r V.
+__global__ void __launch_bounds__(256) k_sub_mean_r(LevelDev L, double* __restrict__ r, double* partials,
+                                                    CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  const double mr = sc->mean_r;
+  double prr = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    if (m & M_FLUID) {
+      double rn = r[c] - mr;
+      r[c] = rn;
+      prr = rn * rn * vol64(L, i, j, k);
+    } else {
+      r[c] = 0.0;
+    }
+  }
+  double v[1] = {prr}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) sc->rr = t[0];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_fv_apply(LevelDev L, const double* __restrict__ p, double* __restrict__ out,
+                                                  int outlet) {
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const unsigned m = __ldg(L.mask + c);
+  if (m & M_SOLID) {
+    out[c] = 0.0;
+    return;
+  }
+  double ns, den;
+  auto val = [&](int64_t cell, int, int, int) { return __ldg(p + cell); };
+  stencil(L, val, i, j, k, c, m, outlet, ns, den);
+  out[c] = (den + iface_at<double>(L, c)) * __ldg(p + c) - ns;
+}
+
+__global__ void __launch_bounds__(256) k_fv_diag(LevelDev L, double* __restrict__ diag, int outlet) {
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const unsigned m = __ldg(L.mask + c);
+  if (m & M_SOLID) {
+    diag[c] = 0.0;
+    return;
+  }
+  double ns, den;
+  auto zero = [](int64_t, int, int, int) { return 0.0; };
+  stencil(L, zero, i, j, k, c, m, outlet, ns, den);
+  diag[c] = den + iface_at<double>(L, c);
+}
+
+__global__ void __launch_bounds__(256) k_weighted_dot(LevelDev L, const double* __restrict__ a,
+                                                      const double* __restrict__ b, double* partials, CgScalars* sc) {
+  EFSI_CELL_PROLOGUE(L)
+  double pa = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    if (m & M_FLUID) pa = __ldg(a + c) * __ldg(b + c) * vol64(L, i, j, k);
+  }
+  double v[1] = {pa}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) sc->dot = t[0];
+  }
+}
+
+__global__ void k_set_zproj(CgScalars* sc, int v) {
+  if (threadIdx.x == 0) {
+    sc->zproj = v;
+    if (!v) sc->mean_z = 0.0;
+  }
+}
+
+__global__ void k_reset_scalars(CgScalars* sc) {
+  if (threadIdx.x == 0) {
+    CgScalars z;
+    memset(&z, 0, sizeof(z));
+    *sc = z;
+  }
+}
+
+}  // namespace efsi
+
+namespace efsi {
+
+namespace {
+thread_local std::string g_err;
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+void set_error(const std::string& msg) { g_err = msg; }
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+struct FamilyTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> start, stop;
+  std::vector<double> bytes;
+  size_t used = 0;
+};
+FamilyTimer g_timers[KF_COUNT];
+std::mutex g_timer_mutex;
+}  // namespace
+
+bool timing_enabled(int family) { return family >= 0 && family < KF_COUNT && g_timers[family].on; }
+
+void timing_begin(int family, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  FamilyTimer& T = g_timers[family];
+  if (T.used == T.start.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    T.start.push_back(a);
+    T.stop.push_back(b);
+    T.bytes.push_back(0.0);
+  }
+  cudaEventRecord(T.start[T.used], s);
+}
+
+void timing_end(int family, cudaStream_t s, double bytes) {
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  FamilyTimer& T = g_timers[family];
+  cudaEventRecord(T.stop[T.used], s);
+  T.bytes[T.used] = bytes;
+  T.used += 1;
+}
+
+LevelDev level_dev(const efsi_fv_plan* P, int l) {
+  const LevelBuf& B = P->lv[l];
+  LevelDev L;
+  L.nx = B.nx;
+  L.ny = B.ny;
+  L.nz = B.nz;
+  L.cxm = B.coef;
+  L.cxp = B.coef + B.nx;
+  L.cym = B.coef + 2 * B.nx;
+  L.cyp = B.coef + 2 * B.nx + B.ny;
+  L.czm = B.coef + 2 * B.nx + 2 * B.ny;
+  L.czp = B.coef + 2 * B.nx + 2 * B.ny + B.nz;
+  L.oz = B.oz;
+  L.wx = B.wx;
+  L.wy = B.wy;
+  L.wz = B.wz;
+  L.cdx_f = B.cdx;
+  L.cdy_f = B.cdy;
+  L.cdz_f = B.cdz;
+  L.mask = B.mask;
+  L.fw = P->has_vdir ? B.fw : nullptr;
+  if (l == 0)
+    L.iface = P->has_iface ? (const void*)P->iface0 : nullptr;
+  else
+    L.iface = P->has_iface ? (const void*)B.iface : nullptr;
+  return L;
+}
+
+int level_zero_check(const efsi_fv_plan* P) {
+  EFSI_ARG_CHECK(P != nullptr, "null plan");
+  EFSI_ARG_CHECK(P->lv.size() > 0 && P->lv[0].mask != nullptr, "plan has no masks; call efsi_fv_set_masks first");
+  return EFSI_OK;
+}
+
+}  // namespace efsi
+
+using namespace efsi;
+
+extern "C" {
+
+const char* efsi_last_error(void) { return g_err.c_str(); }
+const char* efsi_version(void) { return "easyfsi_b200 0.1 (sm_100a)"; }
+uint64_t efsi_kernel_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int efsi_kernel_timing_enable(int32_t family, int32_t enable) {
+  EFSI_ARG_CHECK(family >= 0 && family < KF_COUNT, "unknown kernel family");
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  g_timers[family].on = enable != 0;
+  g_timers[family].used = 0;
+  return EFSI_OK;
+}
+
+int efsi_kernel_timing_read(int32_t family, int64_t* launches, double* total_ms, double* total_bytes) {
+  EFSI_ARG_CHECK(family >= 0 && family < KF_COUNT && launches && total_ms && total_bytes, "invalid timing query");
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  FamilyTimer& T = g_timers[family];
+  double ms = 0.0, by = 0.0;
+  for (size_t q = 0; q < T.used; ++q) {
+    EFSI_CUDA_CHECK(cudaEventSynchronize(T.stop[q]));
+    float e = 0.0f;
+    EFSI_CUDA_CHECK(cudaEventElapsedTime(&e, T.start[q], T.stop[q]));
+    ms += e;
+    by += T.bytes[q];
+  }
+  *launches = (int64_t)T.used;
+  *total_ms = ms;
+  *total_bytes = by;
+  return EFSI_OK;
+}
+
+int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t uniform_grid, efsi_fv_plan** out) {
+  EFSI_ARG_CHECK(levels != nullptr && out != nullptr && n_levels >= 1, "invalid plan arguments");
+  efsi_fv_plan* P = new efsi_fv_plan();
+  P->n_levels = n_levels;
+  P->uniform = uniform_grid;
+  P->lv.resize(n_levels);
+  size_t max_blocks = 1;
+  auto fail = [&](int code) {
+    efsi_fv_plan_destroy(P);
+    return code;
+  };
+  for (int l = 0; l < n_levels; ++l) {
+    const efsi_level_desc& D = levels[l];
+    LevelBuf& B = P->lv[l];
+    if (D.nx < 1 || D.ny < 1 || D.nz < 1 || !D.wx || !D.wy || !D.wz || !D.cdx || !D.cdy || !D.cdz) {
+      set_error("invalid level descriptor");
+      return fail(EFSI_ERR_ARG);
+    }
+    B.nx = D.nx;
+    B.ny = D.ny;
+    B.nz = D.nz;
+    B.n = (int64_t)D.nx * D.ny * D.nz;
+    B.wx = D.wx;
+    B.wy = D.wy;
+    B.wz = D.wz;
+    B.cdx = D.cdx;
+    B.cdy = D.cdy;
+    B.cdz = D.cdz;
+    B.shape = shape3(B.nx, B.ny, B.nz);
+    max_blocks = std::max<size_t>(max_blocks, B.shape.nblocks());
+    size_t ncoef = 2 * (size_t)(B.nx + B.ny + B.nz);
+    if (cudaMalloc(&B.coef, ncoef * sizeof(double)) != cudaSuccess || cudaMalloc(&B.mask, B.n) != cudaSuccess) {
+      set_error("cudaMalloc failed for level tables");
+      return fail(EFSI_ERR_CUDA);
+    }
+    EFSI_COUNTED k_axis_coef<<<(B.nx + 127) / 128, 128>>>(D.wx, D.cdx, B.nx, B.coef, B.coef + B.nx);
+    EFSI_COUNTED k_axis_coef<<<(B.ny + 127) / 128, 128>>>(D.wy, D.cdy, B.ny, B.coef + 2 * B.nx, B.coef + 2 * B.nx + B.ny);
+    EFSI_COUNTED k_axis_coef<<<(B.nz + 127) / 128, 128>>>(D.wz, D.cdz, B.nz, B.coef + 2 * B.nx + 2 * B.ny,
+                                             B.coef + 2 * B.nx + 2 * B.ny + B.nz);
+    float wz0 = 0.0f;
+    cudaMemcpy(&wz0, D.wz, sizeof(float), cudaMemcpyDeviceToHost);
+    B.oz = 2.0 / ((double)wz0 * (double)wz0);
+    size_t es = (l == 0) ? sizeof(double) : sizeof(float);
+    if (cudaMalloc(&B.pa, B.n * es) != cudaSuccess || cudaMalloc(&B.pb, B.n * es) != cudaSuccess) {
+      set_error("cudaMalloc failed for level iterates");
+      return fail(EFSI_ERR_CUDA);
+    }
+    if (l > 0) {
+      if (cudaMalloc(&B.rhs, B.n * sizeof(float)) != cudaSuccess ||
+          cudaMalloc(&B.obs, B.n * sizeof(int32_t)) != cudaSuccess) {
+        set_error("cudaMalloc failed for coarse level");
+        return fail(EFSI_ERR_CUDA);
+      }
+    }
+  }
+  const int64_t n0 = P->lv[0].n;
+  double** vecs[] = {&P->r, &P->z, &P->d0, &P->d1, &P->Ad, &P->delta, &P->b, &P->diag};
+  for (double** v : vecs) {
+    if (cudaMalloc(v, n0 * sizeof(double)) != cudaSuccess) {
+      set_error("cudaMalloc failed for CG vectors");
+      return fail(EFSI_ERR_CUDA);
+    }
+  }
+  P->partials_len = 4 * max_blocks;
+  if (cudaMalloc(&P->partials, P->partials_len * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&P->sc, sizeof(CgScalars)) != cudaSuccess || cudaMalloc(&P->aux, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&P->host_sc, sizeof(CgScalars)) != cudaSuccess) {
+    set_error("cudaMalloc failed for reduction scratch");
+    return fail(EFSI_ERR_CUDA);
+  }
+  EFSI_COUNTED k_reset_scalars<<<1, 32>>>(P->sc);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    set_error(std::string("plan setup failed: ") + cudaGetErrorString(e));
+    return fail(EFSI_ERR_CUDA);
+  }
+  *out = P;
+  return EFSI_OK;
+}
+
+int efsi_fv_plan_destroy(efsi_fv_plan* P) {
+  if (P == nullptr) return EFSI_OK;
+  for (LevelBuf& B : P->lv) {
+    cudaFree(B.coef);
+    cudaFree(B.mask);
+    cudaFree(B.fw);
+    cudaFree(B.obs);
+    cudaFree(B.va);
+    cudaFree(B.vw);
+    cudaFree(B.iface);
+    cudaFree(B.pa);
+    cudaFree(B.pb);
+    cudaFree(B.rhs);
+  }
+  double* vecs[] = {P->r, P->z, P->d0, P->d1, P->Ad, P->delta, P->b, P->diag, P->partials};
+  for (double* v : vecs) cudaFree(v);
+  cudaFree(P->sc);
+  cudaFree(P->aux);
+  if (P->host_sc) cudaFreeHost(P->host_sc);
+  delete P;
+  return EFSI_OK;
+}
+
+int efsi_fv_set_masks(efsi_fv_plan* P, const int32_t* obstacle, const int32_t* vdir_active, const float* vdir_weight,
+                      const double* iface_diag, void* stream) {
+  EFSI_ARG_CHECK(P != nullptr && obstacle != nullptr, "null plan or obstacle");
+  EFSI_ARG_CHECK((vdir_active == nullptr) == (vdir_weight == nullptr), "vdir_active and vdir_weight go together");
+  cudaStream_t s = as_stream(stream);
+  P->has_vdir = vdir_active != nullptr;
+  P->has_iface = iface_diag != nullptr;
+  P->iface0 = iface_diag;
+  P->obstacle0 = obstacle;
+  for (int l = 0; l < P->n_levels; ++l) {
+    LevelBuf& B = P->lv[l];
+    if (P->has_vdir && B.fw == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&B.fw, B.n * sizeof(float)));
+    if (l > 0 && P->has_vdir && B.va == nullptr) {
+      EFSI_CUDA_CHECK(cudaMalloc(&B.va, B.n * sizeof(int32_t)));
+      EFSI_CUDA_CHECK(cudaMalloc(&B.vw, B.n * sizeof(float)));
+    }
+    if (l > 0 && P->has_iface && B.iface == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&B.iface, B.n * sizeof(float)));
+  }
+  // level 0
+  {
+    LevelBuf& B = P->lv[0];
+    EFSI_COUNTED k_mask_from_obstacle<<<B.shape.grid, B.shape.block, 0, s>>>(B.nx, B.ny, B.nz, obstacle, vdir_active, vdir_weight,
+                                                                 B.mask, P->has_vdir ? B.fw : nullptr);
+    EFSI_LAUNCH_CHECK();
+  }
+  for (int l = 1; l < P->n_levels; ++l) {
+    LevelBuf& F = P->lv[l - 1];
+    LevelBuf& C = P->lv[l];
+    const int32_t* fobs = (l == 1) ? obstacle : F.obs;
+    const int32_t* fva = P->has_vdir ? ((l == 1) ? vdir_active : F.va) : nullptr;
+    const float* fvw = P->has_vdir ? ((l == 1) ? vdir_weight : F.vw) : nullptr;
+    if (l == 1) {
+      EFSI_COUNTED k_coarsen_structure<double><<<C.shape.grid, C.shape.block, 0, s>>>(
+          F.nx, F.ny, F.nz, fobs, fva, fvw, P->has_iface ? iface_diag : nullptr, F.wx, F.wy, F.wz, C.nx, C.ny, C.nz,
+          C.obs, P->has_vdir ? C.va : nullptr, P->has_vdir ? C.vw : nullptr,
+          P->has_iface ? (float*)C.iface : nullptr);
+    } else {
+      EFSI_COUNTED k_coarsen_structure<float><<<C.shape.grid, C.shape.block, 0, s>>>(
+          F.nx, F.ny, F.nz, fobs, fva, fvw, P->has_iface ? (const float*)F.iface : nullptr, F.wx, F.wy, F.wz, C.nx,
+          C.ny, C.nz, C.obs, P->has_vdir ? C.va : nullptr, P->has_vdir ? C.vw : nullptr,
+          P->has_iface ? (float*)C.iface : nullptr);
+    }
+    EFSI_LAUNCH_CHECK();
+    EFSI_COUNTED k_mask_from_obstacle<<<C.shape.grid, C.shape.block, 0, s>>>(C.nx, C.ny, C.nz, C.obs, P->has_vdir ? C.va : nullptr,
+                                                                 P->has_vdir ? C.vw : nullptr, C.mask,
+                                                                 P->has_vdir ? C.fw : nullptr);
+    EFSI_LAUNCH_CHECK();
+  }
+  return EFSI_OK;
+}
+
+int efsi_fv_apply(efsi_fv_plan* P, const double* p, double* out, int32_t outlet, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  EFSI_COUNTED k_fv_apply<<<S.grid, S.block, 0, as_stream(stream)>>>(L, p, out, outlet);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_fv_diagonal(efsi_fv_plan* P, double* diag, int32_t outlet, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  EFSI_COUNTED k_fv_diag<<<S.grid, S.block, 0, as_stream(stream)>>>(L, diag, outlet);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_apply_jacobi_preconditioner(efsi_fv_plan* P, const double* diag, const double* r, double* z, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  EFSI_COUNTED k_jacobi_precond<<<S.grid, S.block, 0, as_stream(stream)>>>(L, diag, r, z, 0, P->partials, P->sc);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_weighted_dot(efsi_fv_plan* P, const double* a, const double* b, double* result_host, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  cudaStream_t s = as_stream(stream);
+  EFSI_COUNTED k_weighted_dot<<<S.grid, S.block, 0, s>>>(L, a, b, P->partials, P->sc);
+  EFSI_LAUNCH_CHECK();
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(result_host, &P->sc->dot, sizeof(double), cudaMemcpyDeviceToHost, s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  return EFSI_OK;
+}
+
+int efsi_fv_jacobi_sweep(efsi_fv_plan* P, int32_t level, const void* p, const void* rhs, void* tmp, int32_t outlet,
+                         double omega, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(level >= 0 && level < P->n_levels, "level out of range");
+  LevelDev L = level_dev(P, level);
+  const Shape3& S = P->lv[level].shape;
+  ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+  double om = (double)(float)omega;
+  if (level == 0)
+    EFSI_COUNTED k_sweep<double, false, false><<<S.grid, S.block, 0, as_stream(stream)>>>(
+        L, (const double*)p, rhs, (double*)tmp, outlet, om, none, nullptr, P->sc);
+  else
+    EFSI_COUNTED k_sweep<float, false, false><<<S.grid, S.block, 0, as_stream(stream)>>>(L, (const float*)p, rhs, (float*)tmp,
+                                                                            outlet, om, none, nullptr, P->sc);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_fv_residual(efsi_fv_plan* P, int32_t level, const void* p, const void* rhs, void* residual, int32_t outlet,
+                     void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(level >= 0 && level < P->n_levels, "level out of range");
+  LevelDev L = level_dev(P, level);
+  const Shape3& S = P->lv[level].shape;
+  if (level == 0)
+    EFSI_COUNTED k_residual<double, false><<<S.grid, S.block, 0, as_stream(stream)>>>(L, (const double*)p, rhs, (double*)residual,
+                                                                         outlet);
+  else
+    EFSI_COUNTED k_residual<float, false><<<S.grid, S.block, 0, as_stream(stream)>>>(L, (const float*)p, rhs, (float*)residual,
+                                                                        outlet);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_mg_restrict(efsi_fv_plan* P, int32_t level, const void* fine_residual, float* coarse_rhs, float* coarse_iface,
+                     int32_t* coarse_obstacle, int32_t* coarse_vdir_active, float* coarse_vdir_weight, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(level >= 0 && level + 1 < P->n_levels, "level out of range");
+  LevelDev F = level_dev(P, level);
+  const LevelBuf& C = P->lv[level + 1];
+  cudaStream_t s = as_stream(stream);
+  if (level == 0)
+    EFSI_COUNTED k_restrict<double, false, false><<<C.shape.grid, C.shape.block, 0, s>>>(F, (const double*)fine_residual, nullptr,
+                                                                             0, C.nx, C.ny, C.nz, coarse_rhs);
+  else
+    EFSI_COUNTED k_restrict<float, false, false><<<C.shape.grid, C.shape.block, 0, s>>>(F, (const float*)fine_residual, nullptr, 0,
+                                                                            C.nx, C.ny, C.nz, coarse_rhs);
+  EFSI_LAUNCH_CHECK();
+  if (coarse_iface != nullptr) {
+    if (P->has_iface)
+      EFSI_CUDA_CHECK(cudaMemcpyAsync(coarse_iface, C.iface, C.n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    else
+      EFSI_CUDA_CHECK(cudaMemsetAsync(coarse_iface, 0, C.n * sizeof(float), s));
+  }
+  if (coarse_obstacle != nullptr)
+    EFSI_CUDA_CHECK(cudaMemcpyAsync(coarse_obstacle, C.obs, C.n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+  if (coarse_vdir_active != nullptr) {
+    if (P->has_vdir)
+      EFSI_CUDA_CHECK(cudaMemcpyAsync(coarse_vdir_active, C.va, C.n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    else
+      EFSI_CUDA_CHECK(cudaMemsetAsync(coarse_vdir_active, 0, C.n * sizeof(int32_t), s));
+  }
+  if (coarse_vdir_weight != nullptr) {
+    if (P->has_vdir)
+      EFSI_CUDA_CHECK(cudaMemcpyAsync(coarse_vdir_weight, C.vw, C.n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    else
+      EFSI_CUDA_CHECK(cudaMemsetAsync(coarse_vdir_weight, 0, C.n * sizeof(float), s));
+  }
+  return EFSI_OK;
+}
+
+int efsi_mg_prolong(efsi_fv_plan* P, int32_t level, void* fine_p, const float* coarse_p, double scale, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(level >= 0 && level + 1 < P->n_levels, "level out of range");
+  LevelDev L = level_dev(P, level);
+  const LevelBuf& C = P->lv[level + 1];
+  ProlongSrc pr{coarse_p, C.nx, C.ny, C.nz, (float)scale};
+  const Shape3& S = P->lv[level].shape;
+  if (level == 0)
+    EFSI_COUNTED k_prolong<double><<<S.grid, S.block, 0, as_stream(stream)>>>(L, (double*)fine_p, pr);
+  else
+    EFSI_COUNTED k_prolong<float><<<S.grid, S.block, 0, as_stream(stream)>>>(L, (float*)fine_p, pr);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+}  // extern "C"
+
+namespace efsi {
+
+// ---------------------------------------------------------------------------
+// V-cycle (fluid.py:6085-6262), zero initial guess, level-0 rhs = -r.
+// The result lands in z; when `want_mean` the last sweep also reduces the
+// fluid z V sum so consumers can apply the zero-mean projection on the fly.
+// ---------------------------------------------------------------------------
+static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int pre, int coarse, int post,
+                  bool want_mean, cudaStream_t s) {
+  pre = std::max(1, pre);
+  coarse = std::max(1, coarse);
+  post = std::max(1, post);
+  const double om = (double)0.8f;
+  const float scale = P->uniform ? 1.0f : 0.7f;
+  const int nl = P->n_levels;
+  ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+  double* partials = want_mean ? P->partials : nullptr;
+  if (nl <= 1) {
+    LevelDev L = level_dev(P, 0);
+    const Shape3& S = P->lv[0].shape;
+    int n = std::max(pre + post, coarse);
+    double* bufs[2] = {(double*)P->lv[0].pa, (double*)P->lv[0].pb};
+    const double* cur = nullptr;
+    for (int it = 0; it < n; ++it) {
+      double* dst = (it == n - 1) ? z : bufs[it & 1];
+      double* part = (it == n - 1) ? partials : nullptr;
+      if (it == 0)
+        EFSI_COUNTED k_sweep<double, true, true><<<S.grid, S.block, 0, s>>>(L, nullptr, r, dst, outlet, om, none, part, P->sc);
+      else
+        EFSI_COUNTED k_sweep<double, true, false><<<S.grid, S.block, 0, s>>>(L, cur, r, dst, outlet, om, none, part, P->sc);
+      cur = dst;
+    }
+    EFSI_LAUNCH_CHECK();
+    return EFSI_OK;
+  }
+  // Down: level iterate after pre-smoothing lives in cur[l].
+  std::vector<const void*> cur(nl, nullptr);
+  for (int l = 0; l < nl - 1; ++l) {
+    LevelDev L = level_dev(P, l);
+    LevelBuf& B = P->lv[l];
+    const Shape3& S = B.shape;
+    void* bufs[2] = {B.pa, B.pb};
+    const void* c = nullptr;
+    for (int it = 0; it < pre; ++it) {
+      void* dst = bufs[it & 1];
+      if (l == 0) {
+        if (it == 0)
+          EFSI_TIMED(KF_SWEEP_L0, 17.0 * B.n, s,
+                     EFSI_COUNTED k_sweep<double, true, true><<<S.grid, S.block, 0, s>>>(L, nullptr, r, (double*)dst,
+                                                                                         outlet, om, none, nullptr, P->sc));
+        else
+          EFSI_TIMED(KF_SWEEP_L0, 25.0 * B.n, s,
+                     EFSI_COUNTED k_sweep<double, true, false><<<S.grid, S.block, 0, s>>>(
+                         L, (const double*)c, r, (double*)dst, outlet, om, none, nullptr, P->sc));
+      } else {
+        if (it == 0)
+          EFSI_COUNTED k_sweep<float, false, true><<<S.grid, S.block, 0, s>>>(L, nullptr, B.rhs, (float*)dst, outlet, om, none,
+                                                                 nullptr, P->sc);
+        else
+          EFSI_COUNTED k_sweep<float, false, false><<<S.grid, S.block, 0, s>>>(L, (const float*)c, B.rhs, (float*)dst, outlet, om,
+                                                                  none, nullptr, P->sc);
+      }
+      c = dst;
+    }
+    cur[l] = c;
+    const LevelBuf& C = P->lv[l + 1];
+    if (l == 0)
+      EFSI_TIMED(KF_RESTRICT_L0, 17.0 * B.n + 4.0 * C.n, s,
+                 EFSI_COUNTED k_restrict<double, true, true><<<C.shape.grid, C.shape.block, 0, s>>>(
+                     L, (const double*)c, r, outlet, C.nx, C.ny, C.nz, C.rhs));
+    else
+      EFSI_COUNTED k_restrict<float, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, (const float*)c, B.rhs, outlet, C.nx,
+                                                                             C.ny, C.nz, C.rhs);
+  }
+  // Coarsest level: `coarse` sweeps from zero.
+  {
+    const int l = nl - 1;
+    LevelDev L = level_dev(P, l);
+    LevelBuf& B = P->lv[l];
+    const Shape3& S = B.shape;
+    void* bufs[2] = {B.pa, B.pb};
+    const void* c = nullptr;
+    for (int it = 0; it < coarse; ++it) {
+      void* dst = bufs[it & 1];
+      if (it == 0)
+        EFSI_COUNTED k_sweep<float, false, true><<<S.grid, S.block, 0, s>>>(L, nullptr, B.rhs, (float*)dst, outlet, om, none,
+                                                               nullptr, P->sc);
+      else
+        EFSI_COUNTED k_sweep<float, false, false><<<S.grid, S.block, 0, s>>>(L, (const float*)c, B.rhs, (float*)dst, outlet, om,
+                                                                none, nullptr, P->sc);
+      c = dst;
+    }
+    cur[l] = c;
+  }
+  // Up: prolongation fused into the first post sweep.
+  for (int l = nl - 2; l >= 0; --l) {
+    LevelDev L = level_dev(P, l);
+    LevelBuf& B = P->lv[l];
+    const LevelBuf& C = P->lv[l + 1];
+    const Shape3& S = B.shape;
+    ProlongSrc pr{(const float*)cur[l + 1], C.nx, C.ny, C.nz, scale};
+    const void* c = cur[l];
+    // the two ping-pong buffers of this level: the one not holding c first
+    void* other = (c == B.pa) ? B.pb : B.pa;
+    void* seq[2] = {other, const_cast<void*>(c)};
+    for (int it = 0; it < post; ++it) {
+      const bool last = (it == post - 1);
+      void* dst = (l == 0 && last) ? (void*)z : seq[it & 1];
+      ProlongSrc p_use = (it == 0) ? pr : none;
+      double* part = (l == 0 && last) ? partials : nullptr;
+      if (l == 0)
+        EFSI_TIMED(KF_SWEEP_L0, 25.0 * B.n + (it == 0 ? 4.0 * C.n : 0.0), s,
+                   EFSI_COUNTED k_sweep<double, true, false><<<S.grid, S.block, 0, s>>>(
+                       L, (const double*)c, r, (double*)dst, outlet, om, p_use, part, P->sc));
+      else
+        EFSI_COUNTED k_sweep<float, false, false><<<S.grid, S.block, 0, s>>>(L, (const float*)c, B.rhs, (float*)dst, outlet, om,
+                                                                p_use, nullptr, P->sc);
+      c = dst;
+    }
+    cur[l] = c;
+  }
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+}  // namespace efsi
+
+extern "C" {
+
+int efsi_mg_vcycle(efsi_fv_plan* P, const double* r, double* z, int32_t outlet, int32_t pre, int32_t coarse,
+                   int32_t post, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  return vcycle(P, r, z, outlet, pre, coarse, post, false, as_stream(stream));
+}
+
+}  // extern "C"
+
+namespace efsi {
+
+// ---------------------------------------------------------------------------
+// Flexible PCG driver (fluid.py:6535-6811).  All scalars stay on the device;
+// the host reads them where the reference does (b_norm, the initial residual
+// and preconditioner dot, and every 16th iteration's residual).
+// ---------------------------------------------------------------------------
+struct PcgRun {
+  efsi_fv_plan* P;
+  const efsi_pcg_params* prm;
+  cudaStream_t s;
+  LevelDev L;
+  Shape3 S;
+  bool use_mg;
+  int pre, coarse, post;
+  double* d_cur;
+  double* d_nxt;
+  bool copy_next;  // next SpMV starts a fresh direction d = z'
+};
+
+static int read_scalars(PcgRun& R) {
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(R.P->host_sc, R.P->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, R.s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(R.s));
+  return EFSI_OK;
+}
+
+// z = M^-1 r (+ z mean for the on-the-fly projection when remove_mean).
+static int precondition(PcgRun& R) {
+  const bool want_mean = R.prm->remove_mean != 0;
+  if (R.use_mg) {
+    EFSI_TRY(vcycle(R.P, R.P->r, R.P->z, R.prm->outlet, R.pre, R.coarse, R.post, want_mean, R.s));
+  } else {
+    EFSI_COUNTED k_jacobi_precond<<<R.S.grid, R.S.block, 0, R.s>>>(R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
+                                                      R.P->partials, R.P->sc);
+  }
+  if (!want_mean) EFSI_COUNTED k_set_zproj<<<1, 32, 0, R.s>>>(R.P->sc, 0);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+}  // namespace efsi
+
+extern "C" {
+
+int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, const efsi_pcg_params* prm,
+                      efsi_cg_stats* st, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(rhs0 != nullptr && pressure != nullptr && prm != nullptr && st != nullptr, "null argument");
+  cudaStream_t s = as_stream(stream);
+  PcgRun R;
+  R.P = P;
+  R.prm = prm;
+  R.s = s;
+  R.L = level_dev(P, 0);
+  R.S = P->lv[0].shape;
+  const int max_iters = std::max(1, (int)prm->max_iters);
+  const double tol = std::max(0.0, prm->tolerance);
+  std::memset(st, 0, sizeof(*st));
+  st->initial_relative_residual = INFINITY;
+  st->relative_residual = INFINITY;
+  const int outlet = prm->outlet;
+  const bool remove_mean = prm->remove_mean != 0;
+  EFSI_COUNTED k_reset_scalars<<<1, 32, 0, s>>>(P->sc);
+  // fluid.py:6581 diagonal (Jacobi path and fallback).
+  EFSI_COUNTED k_fv_diag<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->diag, outlet);
+  // b = -rhs - V-mean(-rhs)  (fluid.py:6589-6601); the free volume is reduced
+  // in the same pass whether or not the mean is used.
+  EFSI_COUNTED k_rhs_mean<<<R.S.grid, R.S.block, 0, s>>>(R.L, rhs0, -1.0, P->partials, P->sc);
+  if (remove_mean) st->mean_projection_count += 1;
+  EFSI_COUNTED k_build_b<<<R.S.grid, R.S.block, 0, s>>>(R.L, rhs0, remove_mean ? 1 : 0, P->b, P->partials, P->sc);
+  EFSI_LAUNCH_CHECK();
+  EFSI_TRY(read_scalars(R));
+  const double b_norm = std::sqrt(std::max(P->host_sc->bnorm2, 0.0));
+  st->b_norm = b_norm;
+  const int64_t n0 = P->lv[0].n;
+  if (b_norm <= 1.0e-30) {
+    EFSI_CUDA_CHECK(cudaMemsetAsync(pressure, 0, n0 * sizeof(double), s));
+    st->initial_relative_residual = 0.0;
+    st->relative_residual = 0.0;
+    st->converged = 1;
+    return EFSI_OK;
+  }
+  // r = b - A p, mean projection, ||r||  (fluid.py:6613-6622).
+  auto true_residual = [&]() -> int {
+    EFSI_COUNTED k_true_residual<<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, P->b, P->r, outlet, remove_mean ? 1 : 0,
+                                                   P->partials, P->sc);
+    if (remove_mean) {
+      EFSI_COUNTED k_sub_mean_r<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->partials, P->sc);
+      st->mean_projection_count += 1;
+    }
+    EFSI_LAUNCH_CHECK();
+    EFSI_TRY(read_scalars(R));
+    st->host_residual_checks += 1;
+    return EFSI_OK;
+  };
+  EFSI_TRY(true_residual());
+  double r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+  st->initial_relative_residual = r_norm / b_norm;
+  st->relative_residual = st->initial_relative_residual;
+  if (r_norm <= tol * b_norm) {
+    st->converged = 1;
+    return EFSI_OK;
+  }
+  R.use_mg = P->n_levels > 1 && !prm->iface_active && (prm->precond == 1 || prm->precond == 2);
+  R.pre = prm->precond == 2 ? 1 : 2;
+  R.coarse = prm->precond == 2 ? 12 : 24;
+  R.post = prm->precond == 2 ? 1 : 2;
+  R.d_cur = P->d0;
+  R.d_nxt = P->d1;
+  // Initial preconditioning and rz (fluid.py:6644-6673).
+  EFSI_TRY(precondition(R));
+  if (remove_mean) st->mean_projection_count += 1;
+  EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+  EFSI_LAUNCH_CHECK();
+  EFSI_TRY(read_scalars(R));
+  double rz = P->host_sc->rz;
+  if (!std::isfinite(rz) || std::fabs(rz) <= 1.0e-300) {
+    // Downgrade to Jacobi; the reference does not re-project z here.
+    R.use_mg = false;
+    EFSI_COUNTED k_jacobi_precond<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->diag, P->r, P->z, 0, P->partials, P->sc);
+    EFSI_COUNTED k_set_zproj<<<1, 32, 0, s>>>(P->sc, 0);
+    EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+    EFSI_LAUNCH_CHECK();
+    EFSI_TRY(read_scalars(R));
+    rz = P->host_sc->rz;
+  }
+  st->used_mg = R.use_mg ? 1 : 0;
+  if (!std::isfinite(rz) || rz <= 0.0) {
+    st->breakdown_reason = 1;
+    return EFSI_OK;
+  }
+  R.copy_next = true;
+  const int restart_interval = prm->iface_active ? 256 : 512;
+  int code = 0;
+  for (int it = 1; it <= max_iters; ++it) {
+    // SpMV + direction + alpha
+    if (R.copy_next)
+      EFSI_TIMED(KF_SPMV_DIR, 25.0 * n0, s, EFSI_COUNTED k_spmv_dir<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, R.d_cur, R.d_nxt, P->Ad, outlet, P->partials,
+                                                      P->sc));
+    else
+      EFSI_TIMED(KF_SPMV_DIR, 33.0 * n0, s, EFSI_COUNTED k_spmv_dir<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, R.d_cur, R.d_nxt, P->Ad, outlet, P->partials,
+                                                       P->sc));
+    std::swap(R.d_cur, R.d_nxt);
+    R.copy_next = false;
+    const bool mean_now = remove_mean && (it % 16 == 0);
+    const bool check = (it % 16 == 0) || it == max_iters;
+    const int want_rr = (check && !mean_now) ? 1 : 0;
+    if (R.use_mg)
+      EFSI_TIMED(KF_CG_UPDATE, 56.0 * n0, s, EFSI_COUNTED k_cg_update<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, R.d_cur, P->r, P->Ad, P->delta,
+                                                       mean_now ? 1 : 0, want_rr, P->partials, P->sc));
+    else
+      EFSI_TIMED(KF_CG_UPDATE, 48.0 * n0, s, EFSI_COUNTED k_cg_update<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, R.d_cur, P->r, P->Ad, nullptr,
+                                                        mean_now ? 1 : 0, want_rr, P->partials, P->sc));
+    if (mean_now) {
+      EFSI_COUNTED k_sub_mean_xr<<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, P->r, P->partials, P->sc);
+      st->mean_projection_count += 2;
+    }
+    EFSI_LAUNCH_CHECK();
+    st->iterations = it;
+    if (check) {
+      EFSI_TRY(read_scalars(R));
+      st->host_residual_checks += 1;
+      r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+      st->relative_residual = r_norm / b_norm;
+      if (st->relative_residual <= tol) {
+        st->converged = 1;
+        break;
+      }
+      code = P->host_sc->code;
+      if (code != 0) {
+        st->breakdown_dAd = P->host_sc->code_dAd;
+        if (it < max_iters) {
+          EFSI_TRY(true_residual());
+          r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+          st->relative_residual = r_norm / b_norm;
+          if (st->relative_residual <= tol) {
+            st->converged = 1;
+            break;
+          }
+          EFSI_TRY(precondition(R));
+          if (remove_mean) st->mean_projection_count += 1;
+          EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+          EFSI_LAUNCH_CHECK();
+          EFSI_TRY(read_scalars(R));
+          rz = P->host_sc->rz;
+          if (std::isfinite(rz) && rz > 0.0) {
+            // clear the device code (fluid.py:6728-6729)
+            CgScalars* hs = P->host_sc;
+            hs->code = 0;
+            hs->code_dAd = 0.0;
+            EFSI_CUDA_CHECK(cudaMemcpyAsync(&P->sc->code, &hs->code, sizeof(int), cudaMemcpyHostToDevice, s));
+            EFSI_CUDA_CHECK(
+                cudaMemcpyAsync(&P->sc->code_dAd, &hs->code_dAd, sizeof(double), cudaMemcpyHostToDevice, s));
+            EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+            R.copy_next = true;
+            st->restart_count += 1;
+            continue;
+          }
+        }
+        st->breakdown_reason = 2;
+        break;
+      }
+      if (it < max_iters && restart_interval > 0 && it % restart_interval == 0) {
+        EFSI_TRY(true_residual());
+        r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+        st->relative_residual = r_norm / b_norm;
+        if (st->relative_residual <= tol) {
+          st->converged = 1;
+          break;
+        }
+        EFSI_TRY(precondition(R));
+        if (remove_mean) st->mean_projection_count += 1;
+        EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+        EFSI_LAUNCH_CHECK();
+        EFSI_TRY(read_scalars(R));
+        rz = P->host_sc->rz;
+        if (!std::isfinite(rz) || rz <= 0.0) {
+          st->breakdown_reason = 3;
+          break;
+        }
+        R.copy_next = true;
+        st->restart_count += 1;
+        continue;
+      }
+    }
+    EFSI_TRY(precondition(R));
+    if (remove_mean) st->mean_projection_count += 1;
+    if (R.use_mg)
+      EFSI_TIMED(KF_CG_DOTS, 25.0 * n0, s, EFSI_COUNTED k_cg_dots<true, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, P->delta, P->partials, P->sc));
+    else
+      EFSI_TIMED(KF_CG_DOTS, 17.0 * n0, s, EFSI_COUNTED k_cg_dots<false, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc));
+    EFSI_LAUNCH_CHECK();
+  }
+  EFSI_TRY(read_scalars(R));
+  st->breakdown_code = P->host_sc->code;
+  if (st->breakdown_dAd == 0.0) st->breakdown_dAd = P->host_sc->code_dAd;
+  return EFSI_OK;
+}
+
+}  // extern "C"
+
+namespace efsi {
+
+// Sweeps with the reference's "sweep into tmp, copy back" structure
+// (fluid.py:5862-5900); used by the non-PCG pressure solvers.
+template <typename TP>
+static int smooth_copy(efsi_fv_plan* P, int l, TP* p, const void* rhs, int outlet, int iterations, cudaStream_t s) {
+  LevelDev L = level_dev(P, l);
+  LevelBuf& B = P->lv[l];
+  ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+  const double om = (double)0.8f;
+  for (int it = 0; it < std::max(0, iterations); ++it) {
+    EFSI_COUNTED k_sweep<TP, false, false><<<B.shape.grid, B.shape.block, 0, s>>>(L, p, rhs, (TP*)B.pb, outlet, om, none, nullptr,
+                                                                     P->sc);
+    EFSI_CUDA_CHECK(cudaMemcpyAsync(p, B.pb, B.n * sizeof(TP), cudaMemcpyDeviceToDevice, s));
+  }
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+}  // namespace efsi
+
+extern "C" {
+
+int efsi_fv_multigrid_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, int32_t outlet,
+                            int32_t iterations, int32_t cycles, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(cycles > 0, "multigrid_cycles must be positive");
+  cudaStream_t s = as_stream(stream);
+  const int nl = P->n_levels;
+  if (nl <= 1) return smooth_copy<double>(P, 0, pressure, rhs0, outlet, std::max(1, (int)iterations), s);
+  const float scale = P->uniform ? 1.0f : 0.7f;
+  for (int cyc = 0; cyc < cycles; ++cyc) {
+    for (int l = 0; l < nl - 1; ++l) {
+      LevelDev L = level_dev(P, l);
+      LevelBuf& B = P->lv[l];
+      const LevelBuf& C = P->lv[l + 1];
+      if (l == 0) {
+        EFSI_TRY(smooth_copy<double>(P, 0, pressure, rhs0, outlet, 3, s));
+        EFSI_COUNTED k_restrict<double, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, pressure, rhs0, outlet, C.nx, C.ny,
+                                                                                C.nz, C.rhs);
+      } else {
+        EFSI_TRY(smooth_copy<float>(P, l, (float*)B.pa, B.rhs, outlet, 3, s));
+        EFSI_COUNTED k_restrict<float, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, (const float*)B.pa, B.rhs, outlet,
+                                                                               C.nx, C.ny, C.nz, C.rhs);
+      }
+      // the restriction zeroes the coarse iterate (fluid.py:5383-5385)
+      EFSI_CUDA_CHECK(cudaMemsetAsync(C.pa, 0, C.n * sizeof(float), s));
+    }
+    EFSI_TRY(smooth_copy<float>(P, nl - 1, (float*)P->lv[nl - 1].pa, P->lv[nl - 1].rhs, outlet, 36, s));
+    for (int l = nl - 2; l >= 0; --l) {
+      LevelDev L = level_dev(P, l);
+      LevelBuf& B = P->lv[l];
+      const LevelBuf& C = P->lv[l + 1];
+      ProlongSrc pr{(const float*)C.pa, C.nx, C.ny, C.nz, scale};
+      if (l == 0) {
+        EFSI_COUNTED k_prolong<double><<<B.shape.grid, B.shape.block, 0, s>>>(L, pressure, pr);
+        EFSI_TRY(smooth_copy<double>(P, 0, pressure, rhs0, outlet, 3, s));
+      } else {
+        EFSI_COUNTED k_prolong<float><<<B.shape.grid, B.shape.block, 0, s>>>(L, (float*)B.pa, pr);
+        EFSI_TRY(smooth_copy<float>(P, l, (float*)B.pa, B.rhs, outlet, 3, s));
+      }
+    }
+  }
+  if (!P->uniform) EFSI_TRY(smooth_copy<double>(P, 0, pressure, rhs0, outlet, std::max(1, (int)iterations), s));
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_fv_jacobi_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, int32_t outlet, int32_t iterations,
+                         void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  return smooth_copy<double>(P, 0, pressure, rhs0, outlet, (int)iterations, as_stream(stream));
+}
+
+}  // extern "C"

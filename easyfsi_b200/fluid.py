@@ -1,0 +1,1215 @@
+"""Cartesian fluid solver, B200 path (drop-in for simulation_core/fluid.py).
+
+``CartesianFluidSolver`` keeps the reference's constructor, public fields and
+the methods on the coupled-step hot path with their Python signatures:
+``predict`` (fluid.py:2515), ``compute_divergence`` (:3488), ``project``
+(:6889), ``spread_surface_forces`` (:3275), ``apply_body_force`` (:3330),
+``save_state`` / ``restore_state`` (:2266), plus the private kernels the
+reference's tests drive directly (``_fv_laplacian_apply_kernel``,
+``_weighted_dot_kernel``, ``_mg_restrict_residual_kernel``, ...).  Fields are
+torch CUDA tensors behind the ``Field`` adapter; every numerical operation is a
+call into the sm_100a library through the C ABI (``easyfsi_b200._native``).
+
+Out of scope (the HIBM sharp-interface machinery outside the hot path):
+interface row-list / slot couplings, outlet reachability and component
+anchoring, viscous constraint blending and local divergence cleanup.  Their
+fields exist where the plain path reads them; their kernels are not provided.
+"""
+
+from __future__ import annotations
+
+import math
+from ctypes import byref, c_double, c_void_p
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native
+from .field import Field
+from .grid import (
+    CartesianGrid,
+    FluidDomainSpec,
+    GradedGridSpec,
+    RefinementRegion,
+    build_graded_grid,
+    coarsen_axis_widths,
+    multigrid_axis_widths,
+    multigrid_shapes,
+)
+from .runtime import TaichiRuntimeConfig, current_stream_handle, f32, f64, i32, init_runtime
+
+__all__ = [
+    "CG_PRECONDITIONER_CHOICES",
+    "CartesianFluidSolver",
+    "CartesianGrid",
+    "FluidDomainSpec",
+    "ForceSpreadingReport",
+    "FluidImpulseReport",
+    "GradedGridSpec",
+    "RefinementRegion",
+    "VelocityDirichletBoundaryReport",
+    "build_graded_grid",
+]
+
+CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light")
+_PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2}
+_BREAKDOWN_TEXT = {
+    0: "",
+    1: "initial residual/preconditioner dot is not positive finite",
+    2: "device-side CG scalar update failed",
+    3: "restarted residual/preconditioner dot is not positive finite",
+}
+
+
+@dataclass(frozen=True)
+class ForceSpreadingReport:
+    surface_force_n: tuple[float, float, float]
+    grid_force_n: tuple[float, float, float]
+    action_reaction_relative_error: float
+    active_grid_cells: int
+
+
+@dataclass(frozen=True)
+class FluidImpulseReport:
+    grid_impulse_n_s: tuple[float, float, float]
+    momentum_delta_n_s: tuple[float, float, float]
+    impulse_relative_error: float
+    active_velocity_cells: int
+
+
+@dataclass(frozen=True)
+class VelocityDirichletBoundaryReport:
+    active_cells: int
+    max_delta_mps: float
+    mean_delta_mps: float
+    momentum_delta_n_s: tuple[float, float, float] = (0.0, 0.0, 0.0)
+
+
+def _stream():
+    return c_void_p(current_stream_handle())
+
+
+def _ptr(field_or_tensor):
+    t = field_or_tensor.tensor if isinstance(field_or_tensor, Field) else field_or_tensor
+    if not t.is_contiguous():
+        raise RuntimeError("non-contiguous storage cannot cross the C ABI")
+    return c_void_p(t.data_ptr())
+
+
+class CartesianFluidSolver:
+    """Cell-centred 3D Cartesian fluid state for coupled FSI simulations (fluid.py:684)."""
+
+    DEFAULT_MULTIGRID_CYCLES = 12
+    DEFAULT_NONUNIFORM_MULTIGRID_CYCLES = 24
+
+    _build_multigrid_shapes = staticmethod(multigrid_shapes)
+    _coarsen_axis_widths = staticmethod(coarsen_axis_widths)
+    _build_multigrid_axis_widths = staticmethod(multigrid_axis_widths)
+
+    def default_multigrid_cycles(self) -> int:
+        return self.DEFAULT_MULTIGRID_CYCLES if self.grid.is_uniform else self.DEFAULT_NONUNIFORM_MULTIGRID_CYCLES
+
+    def __init__(self, spec: FluidDomainSpec, runtime: TaichiRuntimeConfig | None = None):
+        self.device = init_runtime(runtime)
+        self.spec = spec
+        self.grid = spec.cartesian_grid
+        self.nx, self.ny, self.nz = self.grid.grid_nodes
+        if self.grid.is_uniform:
+            self.dx, self.dy, self.dz = self.grid.uniform_spacing_m
+        else:
+            self.dx, self.dy, self.dz = (
+                min(self.grid.cell_widths_x_m),
+                min(self.grid.cell_widths_y_m),
+                min(self.grid.cell_widths_z_m),
+            )
+        self.bounds_min = tuple(float(v) for v in self.grid.bounds_min_m)
+        self.bounds_max = tuple(float(v) for v in self.grid.bounds_max_m)
+        self.rho = float(spec.density_kgm3)
+        self.mu = float(spec.viscosity_pa_s)
+        self.dt = float(spec.dt_s)
+        shape = self.grid.grid_nodes
+        dev = self.device
+
+        def scalar(dtype, shp=shape):
+            return Field(shp, dtype, device=dev)
+
+        def vector(dtype, shp=shape):
+            return Field(shp, dtype, n=3, device=dev)
+
+        self.velocity = vector(f32)
+        self.velocity_prev = vector(f32)
+        self.saved_velocity = vector(f32)
+        self.pressure = scalar(f64)
+        self.saved_pressure = scalar(f64)
+        self.fsi_pressure = scalar(f64)
+        self.pressure_tmp = scalar(f64)
+        self.pressure_accum = scalar(f64)
+        self.divergence = scalar(f32)
+        self.pressure_interface_projection_divergence_s = scalar(f64)
+        self.volume_source_s = scalar(f32)
+        self.pressure_interface_matrix_diagonal = scalar(f64)
+        self.pressure_interface_matrix_rhs = scalar(f64)
+        self.obstacle = scalar(i32)
+        self.force = vector(f32)
+        self.velocity_dirichlet_boundary_active = scalar(i32)
+        self.velocity_dirichlet_boundary_value_mps = vector(f32)
+        self.velocity_dirichlet_boundary_projection_weight = scalar(f32)
+        self.velocity_dirichlet_boundary_marker_region_id = scalar(i32)
+        self.fv_diag = scalar(f64)
+        self.cg_r = scalar(f64)
+        self.cg_rhs = scalar(f64)
+        self.cg_z = scalar(f64)
+        self.cg_d = scalar(f64)
+        self.cg_Ad = scalar(f64)
+        self.cg_r_old = scalar(f64)
+        self.cg_mg_rhs = scalar(f64)
+        self.cg_mg_residual = scalar(f64)
+        for name in ("cg_rz", "cg_rz_new", "cg_dAd", "cg_rr", "cg_beta_numerator", "cg_alpha", "cg_beta"):
+            setattr(self, name, Field((), f64, device=dev))
+        self.cg_breakdown_code = Field((), i32, device=dev)
+        self.cg_breakdown_dAd = Field((), f64, device=dev)
+
+        # Axis metric fields, f32 on the device like the reference (fluid.py:1013-1024).
+        g = self.grid
+        for axis, name in enumerate("xyz"):
+            n = shape[axis]
+            setattr(self, f"cell_width_{name}_m", self._axis_field(g._widths(axis)))
+            setattr(self, f"cell_face_{name}_m", self._axis_field(g.axis_faces(axis)))
+            setattr(self, f"cell_center_{name}_m", self._axis_field(g.axis_centers(axis)))
+            setattr(self, f"center_distance_{name}_m", self._axis_field(g.axis_center_distances(axis)))
+            assert getattr(self, f"cell_width_{name}_m").shape == (n,)
+
+        # Multigrid hierarchy (fluid.py:1026-1075).
+        self._mg_shapes = multigrid_shapes(shape)
+        self._mg_axis_widths_m = multigrid_axis_widths(self.grid, self._mg_shapes)
+        self._mg_cell_width_x_m = [self.cell_width_x_m]
+        self._mg_cell_width_y_m = [self.cell_width_y_m]
+        self._mg_cell_width_z_m = [self.cell_width_z_m]
+        self._mg_center_distance_x_m = [self.center_distance_x_m]
+        self._mg_center_distance_y_m = [self.center_distance_y_m]
+        self._mg_center_distance_z_m = [self.center_distance_z_m]
+        for level, widths in enumerate(self._mg_axis_widths_m[1:], start=1):
+            for axis, name in enumerate("xyz"):
+                centers = CartesianGrid._axis_centers(self.bounds_min[axis], widths[axis])
+                getattr(self, f"_mg_cell_width_{name}_m").append(self._axis_field(widths[axis]))
+                getattr(self, f"_mg_center_distance_{name}_m").append(
+                    self._axis_field(CartesianGrid._axis_center_distances(centers, widths[axis]))
+                )
+        self._mg_pressure = [self.pressure]
+        self._mg_tmp = [self.pressure_tmp]
+        self._mg_obstacle = [self.obstacle]
+        self._mg_velocity_dirichlet_boundary_active = [self.velocity_dirichlet_boundary_active]
+        self._mg_velocity_dirichlet_boundary_projection_weight = [self.velocity_dirichlet_boundary_projection_weight]
+        self._mg_pressure_interface_matrix_diagonal = [self.pressure_interface_matrix_diagonal]
+        self._mg_rhs = [scalar(f64)]
+        self._mg_residual = [scalar(f64)]
+        self._pcg_mg_rhs = [self.cg_mg_rhs]
+        self._pcg_mg_residual = [self.cg_mg_residual]
+        self._pcg_mg_pressure = [self.cg_z]
+        self._pcg_mg_tmp = [self.cg_Ad]
+        for lshape in self._mg_shapes[1:]:
+            self._mg_rhs.append(scalar(f32, lshape))
+            self._mg_residual.append(scalar(f32, lshape))
+            self._mg_pressure.append(scalar(f32, lshape))
+            self._mg_tmp.append(scalar(f32, lshape))
+            self._mg_obstacle.append(scalar(i32, lshape))
+            self._mg_velocity_dirichlet_boundary_active.append(scalar(i32, lshape))
+            self._mg_velocity_dirichlet_boundary_projection_weight.append(scalar(f32, lshape))
+            self._mg_pressure_interface_matrix_diagonal.append(scalar(f32, lshape))
+            self._pcg_mg_rhs.append(scalar(f32, lshape))
+            self._pcg_mg_residual.append(scalar(f32, lshape))
+            self._pcg_mg_pressure.append(scalar(f32, lshape))
+            self._pcg_mg_tmp.append(scalar(f32, lshape))
+
+        # Native plan: level metric views + f64 face tables + work vectors.
+        self._level_descs = (_native.LevelDesc * len(self._mg_shapes))()
+        for level, lshape in enumerate(self._mg_shapes):
+            d = self._level_descs[level]
+            d.nx, d.ny, d.nz = lshape
+            d.wx = self._mg_cell_width_x_m[level].ptr()
+            d.wy = self._mg_cell_width_y_m[level].ptr()
+            d.wz = self._mg_cell_width_z_m[level].ptr()
+            d.cdx = self._mg_center_distance_x_m[level].ptr()
+            d.cdy = self._mg_center_distance_y_m[level].ptr()
+            d.cdz = self._mg_center_distance_z_m[level].ptr()
+        torch.cuda.synchronize(self.device)
+        handle = c_void_p()
+        _native.call(
+            "efsi_fv_plan_create", self._level_descs, len(self._mg_shapes), 1 if self.grid.is_uniform else 0, byref(handle)
+        )
+        self._plan = handle
+        self._axes = _native.GridAxes(
+            self.cell_face_x_m.ptr(),
+            self.cell_face_y_m.ptr(),
+            self.cell_face_z_m.ptr(),
+            self.cell_center_x_m.ptr(),
+            self.cell_center_y_m.ptr(),
+            self.cell_center_z_m.ptr(),
+        )
+        self._report = torch.zeros(16, dtype=torch.float64, device=dev)
+        self._vdir_active = False
+        self._iface_active = False
+
+        self.last_cg_iterations = 0
+        self.last_cg_initial_relative_residual = math.inf
+        self.last_cg_relative_residual = math.inf
+        self.last_cg_converged = False
+        self.last_cg_breakdown = ""
+        self.last_cg_host_residual_checks = 0
+        self.last_cg_mean_host_reads = 0
+        self.last_cg_mean_projection_count = 0
+        self.last_cg_unreached_set_mean_projection_count = 0
+        self.last_cg_restart_count = 0
+        self.last_cg_restart_count_measured = False
+        self.last_cg_restart_policy = ""
+        self.last_cg_breakdown_dAd = 0.0
+        self.last_cg_used_multigrid = False
+        self._hibm_pressure_unreached_count = 0
+        self.last_divergence_report_host_reads = 0
+        self._reset_project_cg_stats()
+        self.clear()
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value:
+            try:
+                _native.load().efsi_fv_plan_destroy(plan)
+            except Exception:
+                pass
+            self._plan = None
+
+    # ------------------------------------------------------------------
+    # helpers
+    # ------------------------------------------------------------------
+    def _axis_field(self, values) -> Field:
+        field = Field((len(values),), f32, device=self.device)
+        field.tensor.copy_(torch.tensor([float(v) for v in values], dtype=torch.float32))
+        return field
+
+    def _cell_volume_f32(self) -> torch.Tensor:
+        return (
+            self.cell_width_x_m.tensor[:, None, None]
+            * self.cell_width_y_m.tensor[None, :, None]
+            * self.cell_width_z_m.tensor[None, None, :]
+        )
+
+    def _structure_key(self):
+        fields = (
+            self.obstacle,
+            self.velocity_dirichlet_boundary_active,
+            self.velocity_dirichlet_boundary_projection_weight,
+            self.pressure_interface_matrix_diagonal,
+        )
+        return tuple((f.tensor.data_ptr(), f.tensor._version) for f in fields)
+
+    def _refresh_structure(self) -> None:
+        """Rebuild every level's stencil masks from obstacle / Dirichlet rows /
+        interface diagonal when one of them changed since the last build (torch
+        version counters; one host read decides which optional terms are live)."""
+        key = self._structure_key()
+        if key == getattr(self, "_structure_cache", None):
+            return
+        flags = torch.stack(
+            [
+                (self.velocity_dirichlet_boundary_active.tensor != 0).any(),
+                (self.pressure_interface_matrix_diagonal.tensor != 0).any(),
+            ]
+        ).cpu()
+        self._vdir_active = bool(flags[0])
+        self._iface_active = bool(flags[1])
+        _native.call(
+            "efsi_fv_set_masks",
+            self._plan,
+            self.obstacle.ptr(),
+            self.velocity_dirichlet_boundary_active.ptr() if self._vdir_active else None,
+            self.velocity_dirichlet_boundary_projection_weight.ptr() if self._vdir_active else None,
+            self.pressure_interface_matrix_diagonal.ptr() if self._iface_active else None,
+            _stream(),
+        )
+        self._structure_cache = key
+
+    def _as_f64(self, field: Field) -> torch.Tensor:
+        return field.tensor if field.dtype == f64 else field.tensor.to(torch.float64).contiguous()
+
+    # ------------------------------------------------------------------
+    # state management (fluid.py:442-566, 2221-2295)
+    # ------------------------------------------------------------------
+    def clear(self) -> None:
+        for value in self.__dict__.values():
+            if isinstance(value, Field) and value.shape == tuple(self.grid.grid_nodes):
+                value.tensor.zero_()
+        self.velocity_dirichlet_boundary_marker_region_id.fill(-1)
+        for lst in (self._mg_rhs, self._mg_residual, self._mg_pressure, self._mg_tmp):
+            for fld in lst:
+                fld.tensor.zero_()
+
+    def save_state(self) -> None:
+        self.saved_velocity.tensor.copy_(self.velocity.tensor)
+        self.saved_pressure.tensor.copy_(self.pressure.tensor)
+
+    def restore_state(self) -> None:
+        self.velocity.tensor.copy_(self.saved_velocity.tensor)
+        self.velocity_prev.tensor.copy_(self.saved_velocity.tensor)
+        self.pressure.tensor.copy_(self.saved_pressure.tensor)
+        self.pressure_tmp.tensor.copy_(self.saved_pressure.tensor)
+        self.pressure_accum.tensor.copy_(self.saved_pressure.tensor)
+        for fld in (
+            self.volume_source_s,
+            self.pressure_interface_projection_divergence_s,
+            self.pressure_interface_matrix_diagonal,
+            self.pressure_interface_matrix_rhs,
+            self.force,
+            self.velocity_dirichlet_boundary_active,
+            self.velocity_dirichlet_boundary_value_mps,
+            self.velocity_dirichlet_boundary_projection_weight,
+        ):
+            fld.tensor.zero_()
+        self._hibm_pressure_unreached_count = 0
+
+    def clear_force(self) -> None:
+        self.force.tensor.zero_()
+
+    def clear_volume_source(self) -> None:
+        self.volume_source_s.tensor.zero_()
+
+    def _clear_pressure_kernel(self) -> None:
+        self.pressure.tensor.zero_()
+        self.pressure_tmp.tensor.zero_()
+        self.pressure_accum.tensor.zero_()
+
+    def clear_pressure(self) -> None:
+        self._clear_pressure_kernel()
+
+    def snapshot_pressure(self) -> None:
+        self.fsi_pressure.tensor.copy_(self.pressure.tensor)
+
+    def clear_velocity_dirichlet_boundary_rows(self) -> None:
+        self.velocity_dirichlet_boundary_active.tensor.zero_()
+        self.velocity_dirichlet_boundary_value_mps.tensor.zero_()
+        self.velocity_dirichlet_boundary_projection_weight.tensor.zero_()
+
+    def clear_pressure_interface_matrix_terms(self) -> None:
+        self.pressure_interface_matrix_diagonal.tensor.zero_()
+        self.pressure_interface_matrix_rhs.tensor.zero_()
+        self.pressure_interface_projection_divergence_s.tensor.zero_()
+
+    # ------------------------------------------------------------------
+    # predictor (fluid.py:2378-2527)
+    # ------------------------------------------------------------------
+    def _copy_velocity_to_prev_kernel(self) -> None:
+        self.velocity_prev.tensor.copy_(self.velocity.tensor)
+
+    def _predict_kernel(self, dt_s: float, nu_m2_s: float, advection_scheme_code: int) -> None:
+        self._refresh_structure()
+        _native.call(
+            "efsi_predict",
+            self._plan,
+            byref(self._axes),
+            self.velocity_prev.ptr(),
+            float(dt_s),
+            float(nu_m2_s),
+            int(advection_scheme_code),
+            self.velocity.ptr(),
+            _stream(),
+        )
+
+    def predict(self, dt_s: float | None = None, *, advection_scheme: str = "euler") -> None:
+        step_dt_s = self.dt if dt_s is None else float(dt_s)
+        if step_dt_s <= 0.0:
+            raise ValueError("dt_s must be positive")
+        scheme = str(advection_scheme).lower()
+        if scheme not in {"euler", "rk2"}:
+            raise ValueError(f"unsupported advection_scheme: {advection_scheme!r}")
+        # velocity_prev <- velocity by exchanging the two buffers (the
+        # predictor overwrites every cell of velocity).
+        self.velocity.tensor, self.velocity_prev.tensor = self.velocity_prev.tensor, self.velocity.tensor
+        self._predict_kernel(step_dt_s, self.mu / self.rho, 1 if scheme == "rk2" else 0)
+
+    # ------------------------------------------------------------------
+    # divergence and its statistics (fluid.py:3451-3565, 3827-3848)
+    # ------------------------------------------------------------------
+    def _compute_divergence_kernel(self, pressure_outlet_zmin: int) -> None:
+        _native.call(
+            "efsi_compute_divergence", self._plan, self.velocity.ptr(), int(pressure_outlet_zmin), self.divergence.ptr(), _stream()
+        )
+
+    def compute_divergence(self, *, pressure_outlet_zmin: bool = False) -> None:
+        self._refresh_structure()
+        self._compute_divergence_kernel(1 if pressure_outlet_zmin else 0)
+
+    def _div_stats(self, mode: int, interior_only: bool) -> dict[str, float]:
+        out = (c_double * 3)()
+        _native.call(
+            "efsi_divergence_stats",
+            self._plan,
+            self.divergence.ptr(),
+            self.pressure_interface_projection_divergence_s.ptr(),
+            self.volume_source_s.ptr(),
+            int(mode),
+            1 if interior_only else 0,
+            out,
+            _stream(),
+        )
+        self.last_divergence_report_host_reads += 1
+        count = max(1, int(out[2]))
+        return {"max_abs": float(out[0]), "l2": math.sqrt(float(out[1]) / count)}
+
+    def divergence_stats(self, *, interior_only: bool = False) -> dict[str, float]:
+        return self._div_stats(0, interior_only)
+
+    def divergence_residual_stats(self, *, interior_only: bool = False) -> dict[str, float]:
+        return self._div_stats(1, interior_only)
+
+    # ------------------------------------------------------------------
+    # FV operator and pressure-solver kernels (fluid.py:4080-4726, 5228-6262)
+    # ------------------------------------------------------------------
+    def _fv_laplacian_apply_kernel(self, pressure: Field, output: Field, pressure_outlet_zmin: int) -> None:
+        self._refresh_structure()
+        src = self._as_f64(pressure)
+        dst = output.tensor if output.dtype == f64 else torch.empty_like(src)
+        _native.call("efsi_fv_apply", self._plan, _ptr(src), _ptr(dst), int(pressure_outlet_zmin), _stream())
+        if dst is not output.tensor:
+            output.tensor.copy_(dst)
+
+    def _fv_diagonal_kernel(self, diagonal: Field, pressure_outlet_zmin: int) -> None:
+        self._refresh_structure()
+        _native.call("efsi_fv_diagonal", self._plan, diagonal.ptr(), int(pressure_outlet_zmin), _stream())
+
+    def _apply_jacobi_preconditioner_kernel(self, residual: Field, preconditioned: Field) -> None:
+        self._refresh_structure()
+        _native.call(
+            "efsi_apply_jacobi_preconditioner",
+            self._plan,
+            self.fv_diag.ptr(),
+            _ptr(self._as_f64(residual)),
+            preconditioned.ptr(),
+            _stream(),
+        )
+
+    def _weighted_dot_kernel(self, a: Field, b: Field) -> float:
+        self._refresh_structure()
+        out = c_double(0.0)
+        _native.call("efsi_weighted_dot", self._plan, _ptr(self._as_f64(a)), _ptr(self._as_f64(b)), byref(out), _stream())
+        return float(out.value)
+
+    def _weighted_dot_to_field_kernel(self, a: Field, b: Field, out: Field) -> None:
+        out[None] = self._weighted_dot_kernel(a, b)
+
+    def _prepare_fv_multigrid_rhs(self, rhs_scale: float) -> None:
+        self._refresh_structure()
+        _native.call(
+            "efsi_mg_prepare_level0",
+            self._plan,
+            self.divergence.ptr(),
+            self.volume_source_s.ptr(),
+            self.pressure_interface_matrix_rhs.ptr(),
+            float(rhs_scale),
+            self._mg_rhs[0].ptr(),
+            _stream(),
+        )
+        self._mg_residual[0].tensor.zero_()
+        for level in range(1, len(self._mg_shapes)):
+            for lst in (self._mg_pressure, self._mg_tmp, self._mg_rhs, self._mg_residual, self._mg_pressure_interface_matrix_diagonal):
+                lst[level].tensor.zero_()
+
+    def _smooth_fv_pressure_level(self, level: int, *, iterations: int, pressure_outlet_zmin: bool, omega: float) -> None:
+        self._refresh_structure()
+        p = self._mg_pressure[level]
+        tmp = self._mg_tmp[level]
+        for _ in range(max(0, int(iterations))):
+            _native.call(
+                "efsi_fv_jacobi_sweep",
+                self._plan,
+                int(level),
+                p.ptr(),
+                self._mg_rhs[level].ptr(),
+                tmp.ptr(),
+                1 if pressure_outlet_zmin else 0,
+                float(omega),
+                _stream(),
+            )
+            p.tensor.copy_(tmp.tensor)
+
+    def _compute_fv_residual_level(self, level: int, *, pressure_outlet_zmin: bool) -> None:
+        self._refresh_structure()
+        _native.call(
+            "efsi_fv_residual",
+            self._plan,
+            int(level),
+            self._mg_pressure[level].ptr(),
+            self._mg_rhs[level].ptr(),
+            self._mg_residual[level].ptr(),
+            1 if pressure_outlet_zmin else 0,
+            _stream(),
+        )
+
+    def _level_of(self, field: Field, lists) -> int:
+        for lst in lists:
+            for level, fld in enumerate(lst):
+                if fld is field:
+                    return level
+        for level, lshape in enumerate(self._mg_shapes):
+            if tuple(lshape) == tuple(field.shape):
+                return level
+        raise ValueError("field does not belong to a multigrid level of this solver")
+
+    def _mg_restrict_residual_kernel(
+        self,
+        fine_residual,
+        fine_pressure_interface_matrix_diagonal,
+        fine_obstacle,
+        fine_velocity_dirichlet_boundary_active,
+        fine_velocity_dirichlet_boundary_projection_weight,
+        fine_cell_width_x_m,
+        fine_cell_width_y_m,
+        fine_cell_width_z_m,
+        coarse_rhs,
+        coarse_pressure_interface_matrix_diagonal,
+        coarse_pressure,
+        coarse_tmp,
+        coarse_residual,
+        coarse_obstacle,
+        coarse_velocity_dirichlet_boundary_active,
+        coarse_velocity_dirichlet_boundary_projection_weight,
+        fine_nx,
+        fine_ny,
+        fine_nz,
+    ) -> None:
+        level = self._level_of(fine_residual, (self._mg_residual, self._pcg_mg_residual))
+        self._refresh_structure()
+        _native.call(
+            "efsi_mg_restrict",
+            self._plan,
+            int(level),
+            fine_residual.ptr(),
+            coarse_rhs.ptr(),
+            coarse_pressure_interface_matrix_diagonal.ptr(),
+            coarse_obstacle.ptr(),
+            coarse_velocity_dirichlet_boundary_active.ptr(),
+            coarse_velocity_dirichlet_boundary_projection_weight.ptr(),
+            _stream(),
+        )
+        coarse_pressure.tensor.zero_()
+        coarse_tmp.tensor.zero_()
+        coarse_residual.tensor.zero_()
+
+    def _mg_prolongate_add_kernel(
+        self, fine_pressure, fine_obstacle, coarse_pressure, coarse_nx, coarse_ny, coarse_nz, correction_scale
+    ) -> None:
+        level = self._level_of(fine_pressure, (self._mg_pressure, self._pcg_mg_pressure))
+        self._refresh_structure()
+        _native.call(
+            "efsi_mg_prolong", self._plan, int(level), fine_pressure.ptr(), coarse_pressure.ptr(), float(correction_scale), _stream()
+        )
+
+    def _apply_fv_multigrid_preconditioner(
+        self,
+        residual: Field,
+        *,
+        pressure_outlet_zmin: bool,
+        pre_smooth_iterations: int = 2,
+        coarse_smooth_iterations: int = 24,
+        post_smooth_iterations: int = 2,
+    ) -> None:
+        self._refresh_structure()
+        _native.call(
+            "efsi_mg_vcycle",
+            self._plan,
+            _ptr(self._as_f64(residual)),
+            self.cg_z.ptr(),
+            1 if pressure_outlet_zmin else 0,
+            int(pre_smooth_iterations),
+            int(coarse_smooth_iterations),
+            int(post_smooth_iterations),
+            _stream(),
+        )
+
+    def _subtract_pressure_gradient_kernel(self, dt_over_rho: float, pressure_outlet_zmin: int) -> None:
+        self._refresh_structure()
+        vd = self._vdir_active
+        _native.call(
+            "efsi_subtract_pressure_gradient",
+            self._plan,
+            self.pressure.ptr(),
+            self.velocity_dirichlet_boundary_active.ptr() if vd else None,
+            self.velocity_dirichlet_boundary_projection_weight.ptr() if vd else None,
+            self.velocity_dirichlet_boundary_value_mps.ptr() if vd else None,
+            float(dt_over_rho),
+            int(pressure_outlet_zmin),
+            self.velocity.ptr(),
+            _stream(),
+        )
+
+    def _apply_closed_boundary_no_normal_flow_kernel(self, pressure_outlet_zmin: int) -> None:
+        self._refresh_structure()
+        _native.call("efsi_apply_closed_boundary", self._plan, int(pressure_outlet_zmin), self.velocity.ptr(), _stream())
+
+    def _apply_zmin_no_backflow_kernel(self) -> None:
+        _native.call("efsi_apply_zmin_no_backflow", self._plan, self.velocity.ptr(), _stream())
+
+    def apply_velocity_dirichlet_boundary_rows(self, *, read_report: bool = True) -> VelocityDirichletBoundaryReport | None:
+        self._refresh_structure()
+        if not self._vdir_active:
+            return VelocityDirichletBoundaryReport(0, 0.0, 0.0) if read_report else None
+        rep = self._report
+        _native.call(
+            "efsi_apply_velocity_dirichlet_rows",
+            self._plan,
+            self.velocity_dirichlet_boundary_active.ptr(),
+            self.velocity_dirichlet_boundary_value_mps.ptr(),
+            float(self.rho),
+            self.velocity.ptr(),
+            _ptr(rep) if read_report else None,
+            _stream(),
+        )
+        if not read_report:
+            return None
+        r = rep[:6].cpu().tolist()
+        cells = int(r[0])
+        return VelocityDirichletBoundaryReport(
+            active_cells=cells,
+            max_delta_mps=float(r[2]),
+            mean_delta_mps=float(r[1]) / cells if cells > 0 else 0.0,
+            momentum_delta_n_s=(float(r[3]), float(r[4]), float(r[5])),
+        )
+
+    # ------------------------------------------------------------------
+    # pressure solvers (fluid.py:5842-6811)
+    # ------------------------------------------------------------------
+    def _solve_pressure_poisson(self, *, iterations, rhs_scale, inv_dx2, inv_dy2, inv_dz2, pressure_outlet_zmin) -> None:
+        self._refresh_structure()
+        _native.call(
+            "efsi_legacy_jacobi_solve",
+            self._plan,
+            self.divergence.ptr(),
+            self.volume_source_s.ptr(),
+            float(rhs_scale),
+            float(inv_dx2),
+            float(inv_dy2),
+            float(inv_dz2),
+            1 if pressure_outlet_zmin else 0,
+            int(iterations),
+            self.pressure.ptr(),
+            self.pressure_tmp.ptr(),
+            _stream(),
+        )
+
+    def _solve_pressure_poisson_fv_jacobi(self, *, iterations, rhs_scale, pressure_outlet_zmin) -> None:
+        self._prepare_fv_multigrid_rhs(rhs_scale)
+        _native.call(
+            "efsi_fv_jacobi_solve",
+            self._plan,
+            self._mg_rhs[0].ptr(),
+            self.pressure.ptr(),
+            1 if pressure_outlet_zmin else 0,
+            int(iterations),
+            _stream(),
+        )
+
+    def _solve_pressure_poisson_fv_multigrid(self, *, iterations, rhs_scale, pressure_outlet_zmin, multigrid_cycles) -> None:
+        self._prepare_fv_multigrid_rhs(rhs_scale)
+        cycles = int(multigrid_cycles) if multigrid_cycles is not None else self.default_multigrid_cycles()
+        if cycles <= 0:
+            raise ValueError("multigrid_cycles must be positive")
+        _native.call(
+            "efsi_fv_multigrid_solve",
+            self._plan,
+            self._mg_rhs[0].ptr(),
+            self.pressure.ptr(),
+            1 if pressure_outlet_zmin else 0,
+            int(iterations),
+            cycles,
+            _stream(),
+        )
+
+    def _solve_pressure_poisson_fv_cg(
+        self,
+        *,
+        iterations: int,
+        rhs_scale: float,
+        pressure_outlet_zmin: bool,
+        tolerance: float,
+        preconditioner: str = "auto",
+        remove_nullspace_mean: bool = True,
+        pressure_interface_matrix_active: bool = False,
+        use_graphs: bool = True,
+    ) -> None:
+        name = str(preconditioner)
+        if name not in CG_PRECONDITIONER_CHOICES:
+            raise ValueError(f"unsupported cg_preconditioner: {preconditioner!r}")
+        if name == "auto":
+            name = "jacobi" if self.grid.is_uniform else "fv_multigrid"
+        self._prepare_fv_multigrid_rhs(rhs_scale)
+        params = _native.PcgParams(
+            max(1, int(iterations)),
+            _PRECOND_CODE[name],
+            1 if remove_nullspace_mean else 0,
+            1 if pressure_outlet_zmin else 0,
+            1 if pressure_interface_matrix_active else 0,
+            1 if use_graphs else 0,
+            max(0.0, float(tolerance)),
+        )
+        stats = _native.CgStats()
+        _native.call(
+            "efsi_fv_pcg_solve", self._plan, self._mg_rhs[0].ptr(), self.pressure.ptr(), byref(params), byref(stats), _stream()
+        )
+        self.last_cg_iterations = int(stats.iterations)
+        self.last_cg_initial_relative_residual = float(stats.initial_relative_residual)
+        self.last_cg_relative_residual = float(stats.relative_residual)
+        self.last_cg_converged = bool(stats.converged)
+        self.last_cg_breakdown = _BREAKDOWN_TEXT.get(int(stats.breakdown_reason), "")
+        self.last_cg_host_residual_checks = int(stats.host_residual_checks)
+        self.last_cg_mean_host_reads = 0
+        self.last_cg_mean_projection_count = int(stats.mean_projection_count)
+        self.last_cg_unreached_set_mean_projection_count = 0
+        self.last_cg_restart_count = int(stats.restart_count)
+        self.last_cg_restart_count_measured = True
+        self.last_cg_restart_policy = "periodic_exact_residual"
+        self.last_cg_breakdown_dAd = float(stats.breakdown_dAd)
+        self.last_cg_used_multigrid = bool(stats.used_mg)
+        self._last_cg_breakdown_code = int(stats.breakdown_code)
+        if stats.b_norm <= 1.0e-30:
+            self.pressure_tmp.tensor.zero_()
+            self.pressure_accum.tensor.zero_()
+
+    def _solve_pressure_poisson_with_solver(
+        self,
+        *,
+        iterations,
+        rhs_scale,
+        inv_dx2,
+        inv_dy2,
+        inv_dz2,
+        pressure_outlet_zmin,
+        pressure_solver,
+        multigrid_cycles,
+        cg_tolerance,
+        cg_preconditioner="auto",
+        remove_nullspace_mean=True,
+        pressure_interface_matrix_active=False,
+    ) -> None:
+        if pressure_solver in {"jacobi", "compact_jacobi"}:
+            self._solve_pressure_poisson(
+                iterations=int(iterations),
+                rhs_scale=float(rhs_scale),
+                inv_dx2=float(inv_dx2),
+                inv_dy2=float(inv_dy2),
+                inv_dz2=float(inv_dz2),
+                pressure_outlet_zmin=bool(pressure_outlet_zmin),
+            )
+        elif pressure_solver == "fv_jacobi":
+            self._solve_pressure_poisson_fv_jacobi(
+                iterations=int(iterations), rhs_scale=float(rhs_scale), pressure_outlet_zmin=bool(pressure_outlet_zmin)
+            )
+        elif pressure_solver == "fv_multigrid":
+            self._solve_pressure_poisson_fv_multigrid(
+                iterations=int(iterations),
+                rhs_scale=float(rhs_scale),
+                pressure_outlet_zmin=bool(pressure_outlet_zmin),
+                multigrid_cycles=multigrid_cycles,
+            )
+        elif pressure_solver == "fv_cg":
+            self._solve_pressure_poisson_fv_cg(
+                iterations=int(iterations),
+                rhs_scale=float(rhs_scale),
+                pressure_outlet_zmin=bool(pressure_outlet_zmin),
+                tolerance=float(cg_tolerance),
+                preconditioner=str(cg_preconditioner),
+                remove_nullspace_mean=bool(remove_nullspace_mean),
+                pressure_interface_matrix_active=bool(pressure_interface_matrix_active),
+            )
+        else:
+            raise ValueError(f"unsupported pressure_solver: {pressure_solver!r}")
+
+    # ------------------------------------------------------------------
+    # projection (fluid.py:6889-7613)
+    # ------------------------------------------------------------------
+    def _reset_project_cg_stats(self) -> None:
+        self.last_project_cg_project_calls = 0
+        self.last_project_cg_iterations_total = 0
+        self.last_project_cg_iterations_max = 0
+        self.last_project_cg_host_residual_checks = 0
+        self.last_project_cg_mean_host_reads = 0
+        self.last_project_cg_mean_projection_count = 0
+        self.last_project_cg_unreached_set_mean_projection_count = 0
+        self.last_project_cg_restart_count = 0
+        self.last_project_cg_restart_count_measured = False
+        self.last_project_cg_restart_policy = ""
+        self.last_project_cg_initial_relative_residual_max = 0.0
+        self.last_project_cg_relative_residual_max = 0.0
+        self.last_project_cg_converged_all = True
+        self.last_project_cg_breakdown_count = 0
+        self.last_project_cg_breakdown_code = 0
+        self.last_project_cg_breakdown_dAd = 0.0
+        self.last_project_cg_breakdown = ""
+
+    def pressure_interface_matrix_terms_report(self) -> dict[str, float]:
+        diag = self.pressure_interface_matrix_diagonal.tensor
+        rhs = self.pressure_interface_matrix_rhs.tensor
+        vol = self._cell_volume_f32().to(torch.float64)
+        fluid = self.obstacle.tensor == 0
+        vals = torch.stack(
+            [
+                torch.where(fluid, diag * vol, 0.0).sum(),
+                torch.where(fluid, rhs * vol, 0.0).sum(),
+                diag.abs().max(),
+                ((diag != 0) & fluid).sum().to(torch.float64),
+            ]
+        ).cpu().tolist()
+        return {
+            "diagonal_integral": vals[0],
+            "rhs_integral": vals[1],
+            "max_abs_diagonal": vals[2],
+            "active_cells": int(vals[3]),
+            "row_count": 0,
+            "row_active_count": 0,
+        }
+
+    def project(
+        self,
+        iterations: int = 40,
+        pressure_outlet_zmin: bool = False,
+        dt_s: float | None = None,
+        preserve_velocity_constraints: bool = False,
+        velocity_constraint_blend: float = 1.0,
+        velocity_constraint_solid_mobility_ratio: float = 0.0,
+        divergence_cleanup_iterations: int = 0,
+        divergence_cleanup_relaxation: float = 0.7,
+        reset_pressure: bool = False,
+        pressure_solver: str = "jacobi",
+        multigrid_cycles: int | None = None,
+        cg_tolerance: float = 1.0e-6,
+        cg_preconditioner: str = "auto",
+        pressure_solve_failure_policy: str = "report",
+        read_report: bool = True,
+    ) -> dict[str, float]:
+        if iterations <= 0:
+            raise ValueError("iterations must be positive")
+        step_dt_s = self.dt if dt_s is None else float(dt_s)
+        if step_dt_s <= 0.0:
+            raise ValueError("dt_s must be positive")
+        if not 0.0 <= float(velocity_constraint_blend) <= 1.0:
+            raise ValueError("velocity_constraint_blend must be in [0, 1]")
+        ratio = float(velocity_constraint_solid_mobility_ratio)
+        if not math.isfinite(ratio) or ratio < 0.0:
+            raise ValueError("velocity_constraint_solid_mobility_ratio must be a finite non-negative number")
+        if not 0.0 <= float(divergence_cleanup_relaxation) <= 1.0:
+            raise ValueError("divergence_cleanup_relaxation must be in [0, 1]")
+        tol = float(cg_tolerance)
+        if not math.isfinite(tol) or tol < 0.0:
+            raise ValueError("cg_tolerance must be a finite non-negative number")
+        precond = str(cg_preconditioner)
+        if precond not in CG_PRECONDITIONER_CHOICES:
+            raise ValueError(f"unsupported cg_preconditioner: {cg_preconditioner!r}")
+        policy = str(pressure_solve_failure_policy)
+        if policy not in {"report", "raise"}:
+            raise ValueError("pressure_solve_failure_policy must be 'report' or 'raise'")
+        requested = str(pressure_solver)
+        solver = requested
+        if solver not in {"jacobi", "compact_jacobi", "fv_jacobi", "fv_multigrid", "fv_cg"}:
+            raise ValueError(f"unsupported pressure_solver: {pressure_solver!r}")
+        if not self.grid.is_uniform:
+            if solver not in {"fv_jacobi", "fv_multigrid", "fv_cg"}:
+                raise ValueError("non-uniform CartesianGrid projection requires an FV pressure solver")
+            if divergence_cleanup_iterations > 0:
+                raise ValueError("non-uniform CartesianGrid divergence cleanup requires non-uniform cleanup operators")
+        if multigrid_cycles is not None and int(multigrid_cycles) <= 0:
+            raise ValueError("multigrid_cycles must be positive")
+        if preserve_velocity_constraints or int(divergence_cleanup_iterations) > 0:
+            raise NotImplementedError(
+                "velocity-constraint blending and local divergence cleanup are outside the B200 hot path"
+            )
+        report = bool(read_report)
+        outlet = bool(pressure_outlet_zmin)
+        self.last_divergence_report_host_reads = 0
+        self._refresh_structure()
+        iface_active = self._iface_active
+        forced = False
+        force_reason = ""
+        if iface_active and solver == "fv_multigrid":
+            solver, forced, force_reason = "fv_cg", True, "pressure_interface_matrix_requires_rowlist_fv_cg"
+        anchored = (not outlet) and iface_active
+        remove_mean = (not outlet) and solver == "fv_cg" and not anchored
+        if outlet:
+            nullspace_policy, compat = "pressure_outlet_dirichlet", True
+        elif anchored:
+            nullspace_policy, compat = "interface_matrix_anchored", solver == "fv_cg"
+        elif solver == "fv_cg":
+            nullspace_policy, compat = "closed_neumann_fv_cg_zero_mean", True
+        else:
+            nullspace_policy, compat = "closed_neumann_non_cg_unmeasured", False
+        self._reset_project_cg_stats()
+        self.last_project_cg_restart_count_measured = solver == "fv_cg"
+        self.last_project_cg_restart_policy = "periodic_exact_residual" if solver == "fv_cg" else "not_applicable_non_cg"
+        state = {"failed": False, "action": "none"}
+
+        def record_cg_stats() -> None:
+            if solver != "fv_cg":
+                return
+            self.last_project_cg_project_calls += 1
+            self.last_project_cg_iterations_total += int(self.last_cg_iterations)
+            self.last_project_cg_iterations_max = max(self.last_project_cg_iterations_max, int(self.last_cg_iterations))
+            self.last_project_cg_host_residual_checks += int(self.last_cg_host_residual_checks)
+            self.last_project_cg_mean_projection_count += int(self.last_cg_mean_projection_count)
+            self.last_project_cg_restart_count += int(self.last_cg_restart_count)
+            self.last_project_cg_restart_policy = str(self.last_cg_restart_policy)
+            if math.isfinite(self.last_cg_initial_relative_residual):
+                self.last_project_cg_initial_relative_residual_max = max(
+                    self.last_project_cg_initial_relative_residual_max, self.last_cg_initial_relative_residual
+                )
+            if math.isfinite(self.last_cg_relative_residual):
+                self.last_project_cg_relative_residual_max = max(
+                    self.last_project_cg_relative_residual_max, self.last_cg_relative_residual
+                )
+            if not self.last_cg_converged:
+                state["failed"] = True
+                self.last_project_cg_converged_all = False
+                self.last_project_cg_breakdown_count += 1
+                self.last_project_cg_breakdown_code = max(self.last_project_cg_breakdown_code, self._last_cg_breakdown_code)
+                if math.isfinite(self.last_cg_breakdown_dAd):
+                    self.last_project_cg_breakdown_dAd = self.last_cg_breakdown_dAd
+                if self.last_cg_breakdown:
+                    self.last_project_cg_breakdown = self.last_cg_breakdown
+
+        def handle_failure() -> None:
+            if solver != "fv_cg" or self.last_cg_converged:
+                return
+            if policy != "raise":
+                state["action"] = "reported_cleared_pressure_correction"
+                self._clear_pressure_kernel()
+                return
+            raise RuntimeError(
+                "FV-CG pressure solve did not converge before pressure-gradient velocity correction "
+                f"(iterations={self.last_cg_iterations}, relative_residual={self.last_cg_relative_residual:.6g}, "
+                f"breakdown={self.last_cg_breakdown!r})"
+            )
+
+        vdir_calls = {"n": 0, "cells": 0, "cells_max": 0, "dsum": 0.0, "dmax": 0.0, "mom": [0.0, 0.0, 0.0]}
+
+        def apply_bc() -> None:
+            if self._vdir_active:
+                rep = self.apply_velocity_dirichlet_boundary_rows(read_report=report)
+                if report and rep is not None:
+                    vdir_calls["n"] += 1
+                    vdir_calls["cells"] += rep.active_cells
+                    vdir_calls["cells_max"] = max(vdir_calls["cells_max"], rep.active_cells)
+                    vdir_calls["dsum"] += rep.mean_delta_mps * rep.active_cells
+                    vdir_calls["dmax"] = max(vdir_calls["dmax"], rep.max_delta_mps)
+                    for a in range(3):
+                        vdir_calls["mom"][a] += rep.momentum_delta_n_s[a]
+            elif report:
+                vdir_calls["n"] += 1
+            if outlet:
+                self._apply_zmin_no_backflow_kernel()
+                self._apply_closed_boundary_no_normal_flow_kernel(1)
+
+        nan_stats = {"max_abs": math.nan, "l2": math.nan}
+        self.pressure_interface_projection_divergence_s.tensor.zero_()
+        apply_bc()
+        self._compute_divergence_kernel(1 if outlet else 0)
+        pre_raw = self.divergence_stats() if report else nan_stats
+        pre = self.divergence_residual_stats() if report else nan_stats
+        if reset_pressure:
+            self._clear_pressure_kernel()
+        rhs_scale = self.rho / step_dt_s
+        solve_kwargs = dict(
+            iterations=int(iterations),
+            rhs_scale=float(rhs_scale),
+            inv_dx2=1.0 / (self.dx * self.dx),
+            inv_dy2=1.0 / (self.dy * self.dy),
+            inv_dz2=1.0 / (self.dz * self.dz),
+            pressure_outlet_zmin=outlet,
+            pressure_solver=solver,
+            multigrid_cycles=multigrid_cycles,
+            cg_tolerance=tol,
+            cg_preconditioner=precond,
+            remove_nullspace_mean=remove_mean,
+            pressure_interface_matrix_active=iface_active,
+        )
+        self._solve_pressure_poisson_with_solver(**solve_kwargs)
+        record_cg_stats()
+        handle_failure()
+        self._subtract_pressure_gradient_kernel(step_dt_s / self.rho, 1 if outlet else 0)
+        apply_bc()
+        self._compute_divergence_kernel(1 if outlet else 0)
+        proj_raw = self.divergence_stats() if report else nan_stats
+        proj = self.divergence_residual_stats() if report else nan_stats
+        post_raw, post = proj_raw, proj
+        if outlet:
+            # fluid.py:7259-7318: up to three cleanup re-solves while the
+            # residual divergence grew more than 5 % over the projection's.
+            self.pressure_accum.tensor.copy_(self.pressure.tensor)
+            target_stats = self.divergence_residual_stats()
+            target_l2 = max(float(target_stats["l2"]) * 1.05, 1.0e-8)
+            apply_bc()
+            self._compute_divergence_kernel(1)
+            current = self.divergence_residual_stats()
+            post_raw = self.divergence_stats() if report else nan_stats
+            post = current if report else nan_stats
+            cleanup_iterations = max(1, min(int(iterations), 256))
+            for _ in range(3):
+                if current["l2"] <= target_l2:
+                    break
+                self.pressure.tensor.zero_()
+                self.pressure_interface_matrix_rhs.tensor.zero_()
+                self._solve_pressure_poisson_with_solver(**{**solve_kwargs, "iterations": cleanup_iterations})
+                record_cg_stats()
+                handle_failure()
+                self._subtract_pressure_gradient_kernel(step_dt_s / self.rho, 1)
+                corrected = self.pressure_accum.tensor + self.pressure.tensor
+                self.pressure_accum.tensor.copy_(corrected)
+                self.pressure.tensor.copy_(corrected)
+                self.pressure_tmp.tensor.copy_(corrected)
+                apply_bc()
+                self._compute_divergence_kernel(1)
+                current = self.divergence_residual_stats()
+                post_raw = self.divergence_stats() if report else nan_stats
+                post = current if report else nan_stats
+        else:
+            self._apply_closed_boundary_no_normal_flow_kernel(0)
+        if not report:
+            return {}
+        self._compute_divergence_kernel(1 if outlet else 0)
+        final_raw = self.divergence_stats()
+        final = self.divergence_residual_stats()
+        final_int_raw = self.divergence_stats(interior_only=True)
+        final_int = self.divergence_residual_stats(interior_only=True)
+        iface = self.pressure_interface_matrix_terms_report()
+        n_vdir = vdir_calls["cells"]
+        return {
+            "pressure_solver_requested": requested,
+            "pressure_solver": solver,
+            "pressure_solver_forced_to_fv_cg": forced,
+            "pressure_solver_force_reason": force_reason,
+            "l2": final["l2"],
+            "max_abs": final["max_abs"],
+            "raw_l2": final_raw["l2"],
+            "raw_max_abs": final_raw["max_abs"],
+            "interior_l2": final_int["l2"],
+            "interior_max_abs": final_int["max_abs"],
+            "interior_raw_l2": final_int_raw["l2"],
+            "interior_raw_max_abs": final_int_raw["max_abs"],
+            "pre_projection_l2": pre["l2"],
+            "pre_projection_max_abs": pre["max_abs"],
+            "pre_projection_raw_l2": pre_raw["l2"],
+            "pre_projection_raw_max_abs": pre_raw["max_abs"],
+            "projection_l2": proj["l2"],
+            "projection_max_abs": proj["max_abs"],
+            "projection_raw_l2": proj_raw["l2"],
+            "projection_raw_max_abs": proj_raw["max_abs"],
+            "post_boundary_l2": post["l2"],
+            "post_boundary_max_abs": post["max_abs"],
+            "post_boundary_raw_l2": post_raw["l2"],
+            "post_boundary_raw_max_abs": post_raw["max_abs"],
+            "post_constraint_l2": post["l2"],
+            "post_constraint_max_abs": post["max_abs"],
+            "post_constraint_raw_l2": post_raw["l2"],
+            "post_constraint_raw_max_abs": post_raw["max_abs"],
+            "velocity_dirichlet_boundary_apply_calls": vdir_calls["n"],
+            "velocity_dirichlet_boundary_active_cells_total": n_vdir,
+            "velocity_dirichlet_boundary_active_cells_max": vdir_calls["cells_max"],
+            "velocity_dirichlet_boundary_max_delta_mps": vdir_calls["dmax"],
+            "velocity_dirichlet_boundary_mean_delta_mps": vdir_calls["dsum"] / n_vdir if n_vdir > 0 else 0.0,
+            "velocity_dirichlet_boundary_momentum_delta_n_s": tuple(vdir_calls["mom"]),
+            "pressure_interface_matrix_diagonal_integral": iface["diagonal_integral"],
+            "pressure_interface_matrix_rhs_integral": iface["rhs_integral"],
+            "pressure_interface_matrix_max_abs_diagonal": iface["max_abs_diagonal"],
+            "pressure_interface_matrix_active_cells": iface["active_cells"],
+            "pressure_interface_matrix_active": iface_active,
+            "pressure_interface_matrix_row_count": 0,
+            "pressure_interface_matrix_row_active_count": 0,
+            "pressure_nullspace_policy": nullspace_policy,
+            "pressure_nullspace_compatibility_measured": compat,
+            "pressure_nullspace_zero_mean_projection_applied": remove_mean,
+            "pressure_system_anchored_by_interface_matrix": anchored,
+            "pressure_solve_failure_policy": policy,
+            "pressure_solve_failed": state["failed"],
+            "pressure_solve_failure_action": state["action"],
+            "pressure_projection_physical_failure": False,
+            "pressure_projection_physical_failure_reason": "",
+            "pressure_projection_physical_failure_action": "none",
+            "cg_project_calls": self.last_project_cg_project_calls,
+            "cg_iterations_total": self.last_project_cg_iterations_total,
+            "cg_iterations_max": self.last_project_cg_iterations_max,
+            "cg_host_residual_checks": self.last_project_cg_host_residual_checks,
+            "cg_mean_host_reads": 0,
+            "cg_mean_projection_count": self.last_project_cg_mean_projection_count,
+            "cg_unreached_set_mean_projection_count": 0,
+            "cg_restart_count": self.last_project_cg_restart_count,
+            "cg_restart_count_measured": self.last_project_cg_restart_count_measured,
+            "cg_restart_policy": self.last_project_cg_restart_policy,
+            "cg_initial_relative_residual_max": self.last_project_cg_initial_relative_residual_max,
+            "cg_relative_residual_max": self.last_project_cg_relative_residual_max,
+            "cg_converged_all": self.last_project_cg_converged_all,
+            "cg_breakdown_count": self.last_project_cg_breakdown_count,
+            "cg_breakdown_code": self.last_project_cg_breakdown_code,
+            "cg_breakdown": self.last_project_cg_breakdown,
+        }
+
+    # ------------------------------------------------------------------
+    # body-force spreading (fluid.py:3196-3345)
+    # ------------------------------------------------------------------
+    def spread_surface_forces(
+        self, surface_position_m, surface_force_n, vertex_count: int, center_m, force_sign: float = -1.0
+    ) -> ForceSpreadingReport:
+        if vertex_count <= 0:
+            raise ValueError("vertex_count must be positive")
+        self._refresh_structure()
+        pos = surface_position_m.tensor if isinstance(surface_position_m, Field) else surface_position_m
+        frc = surface_force_n.tensor if isinstance(surface_force_n, Field) else surface_force_n
+        pos = pos.to(self.device, torch.float32).contiguous()
+        frc = frc.to(self.device, torch.float32).contiguous()
+        rep = self._report
+        _native.call(
+            "efsi_spread_surface_forces",
+            self._plan,
+            byref(self._axes),
+            _ptr(pos),
+            _ptr(frc),
+            int(vertex_count),
+            float(center_m[0]),
+            float(center_m[1]),
+            float(center_m[2]),
+            float(force_sign),
+            self.force.ptr(),
+            _ptr(rep),
+            _stream(),
+        )
+        r = rep[:6].cpu().numpy().astype(np.float32)
+        surface = tuple(float(v) for v in r[:3])
+        grid_force = tuple(float(v) for v in r[3:6])
+        expected = np.float32(force_sign) * r[:3]
+        denom = max(float(np.linalg.norm(expected)), 1.0e-12)
+        err = float(np.linalg.norm(r[3:6] - expected)) / denom
+        active = int((self.force.tensor.norm(dim=-1) > 0).sum().item())
+        return ForceSpreadingReport(surface, grid_force, err, active)
+
+    def apply_body_force(self, dt_s: float | None = None, *, read_report: bool = True) -> FluidImpulseReport | None:
+        step_dt_s = self.dt if dt_s is None else float(dt_s)
+        if step_dt_s <= 0.0:
+            raise ValueError("dt_s must be positive")
+        self._refresh_structure()
+        rep = self._report
+        _native.call(
+            "efsi_apply_body_force",
+            self._plan,
+            self.force.ptr(),
+            float(step_dt_s),
+            float(self.rho),
+            self.velocity.ptr(),
+            _ptr(rep),
+            _stream(),
+        )
+        if not read_report:
+            return None
+        r = rep[:7].cpu().tolist()
+        impulse = np.asarray(r[:3])
+        momentum = np.asarray(r[3:6])
+        denom = max(float(np.linalg.norm(impulse)), 1.0e-12)
+        return FluidImpulseReport(
+            grid_impulse_n_s=tuple(float(v) for v in impulse),
+            momentum_delta_n_s=tuple(float(v) for v in momentum),
+            impulse_relative_error=float(np.linalg.norm(momentum - impulse)) / denom,
+            active_velocity_cells=int(r[6]),
+        )

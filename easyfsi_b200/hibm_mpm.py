@@ -1,0 +1,512 @@
+"""HIBM surface markers, B200 path (drop-in for the marker part of
+simulation_core/hibm_mpm.py, class HibmMpmSurfaceMarkers :279).
+
+Provides the coupled-step members of the reference class with their
+signatures: ``load_markers`` (:553), ``set_marker_tractions_pa`` (:893),
+``compute_marker_forces`` (:908), the pressure-only fast path of
+``sample_fluid_stress_to_marker_tractions`` (:3710 -> :2253),
+``aggregate_region_forces`` (:5291), ``clear_mpm_external_forces`` (:4880),
+``scatter_marker_forces_to_mpm_particles`` (:4961) and the two surface-feedback
+updates (:5055, :5182).  Every method accepts an extra ``read_report=False``
+keyword that skips the host read of its report (the report is then ``None``).
+
+The viscous / closure stress sampler, projection triangles and the IB node
+search of the reference are outside the hot path and not provided.
+"""
+
+from __future__ import annotations
+
+import math
+from ctypes import byref, c_float, c_void_p
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native
+from .field import Field
+from .runtime import TaichiRuntimeConfig, current_stream_handle, f32, f64, i32, init_runtime
+
+
+def _vector3(value, *, name: str) -> tuple[float, float, float]:
+    if len(value) != 3:
+        raise ValueError(f"{name} must contain exactly 3 components")
+    out = tuple(float(v) for v in value)
+    if not all(math.isfinite(v) for v in out):
+        raise ValueError(f"{name} must contain finite values")
+    return out  # type: ignore[return-value]
+
+
+def _normalize_vector3(value, *, name: str) -> tuple[float, float, float]:
+    v = _vector3(value, name=name)
+    n = math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    if n <= 1.0e-12:
+        raise ValueError(f"{name} must be non-zero")
+    return (v[0] / n, v[1] / n, v[2] / n)
+
+
+@dataclass(frozen=True)
+class HibmMpmFluidStressSampleReport:
+    valid_marker_count: int
+    invalid_marker_count: int
+    max_abs_traction_pa: float
+    two_sided_pressure_marker_count: int = 0
+    one_sided_pressure_marker_count: int = 0
+
+
+@dataclass(frozen=True)
+class HibmMpmSurfaceMarkerForceReport:
+    primary_marker_force_n: tuple[float, float, float]
+    secondary_marker_force_n: tuple[float, float, float]
+    total_marker_force_n: tuple[float, float, float]
+    primary_marker_count: int
+    secondary_marker_count: int
+    total_marker_count: int
+    fluid_reaction_force_n: tuple[float, float, float]
+    action_reaction_residual_n: float
+    primary_stress_valid_marker_count: int = 0
+    primary_stress_invalid_marker_count: int = 0
+    secondary_stress_valid_marker_count: int = 0
+    secondary_stress_invalid_marker_count: int = 0
+    primary_marker_force_norm_sum_n: float = 0.0
+    secondary_marker_force_norm_sum_n: float = 0.0
+    total_marker_force_norm_sum_n: float = 0.0
+    primary_marker_force_norm_max_n: float = 0.0
+    secondary_marker_force_norm_max_n: float = 0.0
+    total_marker_force_norm_max_n: float = 0.0
+
+
+@dataclass(frozen=True)
+class HibmMpmExternalForceClearReport:
+    cleared_particle_count: int
+    max_abs_external_force_before_n: float
+
+
+@dataclass(frozen=True)
+class HibmMpmMpmForceScatterReport:
+    active_marker_count: int
+    invalid_marker_count: int
+    active_particle_count: int
+    total_marker_force_n: tuple[float, float, float]
+    total_mpm_external_force_n: tuple[float, float, float]
+    action_reaction_residual_n: float
+
+
+@dataclass(frozen=True)
+class HibmMpmSurfaceUpdateReport:
+    updated_marker_count: int
+    invalid_marker_count: int
+    max_marker_displacement_m: float
+    max_marker_speed_mps: float
+    geometry_updated_marker_count: int = 0
+    geometry_invalid_marker_count: int = 0
+    max_marker_normal_change: float = 0.0
+    max_marker_area_change_m2: float = 0.0
+
+
+def _tensor(field_or_tensor) -> torch.Tensor:
+    return field_or_tensor.tensor if isinstance(field_or_tensor, Field) else field_or_tensor
+
+
+class HibmMpmSurfaceMarkers:
+    def __init__(self, marker_capacity: int, projection_triangle_capacity: int | None = None, runtime: TaichiRuntimeConfig | None = None) -> None:
+        self.device = init_runtime(runtime)
+        if int(marker_capacity) <= 0:
+            raise ValueError("marker_capacity must be positive")
+        self.marker_capacity = int(marker_capacity)
+        if projection_triangle_capacity is None:
+            projection_triangle_capacity = self.marker_capacity
+        if int(projection_triangle_capacity) <= 0:
+            raise ValueError("projection_triangle_capacity must be positive")
+        self.projection_triangle_capacity = int(projection_triangle_capacity)
+        self.marker_count = 0
+        self.projection_triangle_count = 0
+        cap, dev = self.marker_capacity, self.device
+        self.x_gamma_m = Field((cap,), f32, n=3, device=dev)
+        self.v_gamma_mps = Field((cap,), f32, n=3, device=dev)
+        self.n_gamma = Field((cap,), f32, n=3, device=dev)
+        self.A_gamma_m2 = Field((cap,), f32, device=dev)
+        self.region_id = Field((cap,), i32, device=dev)
+        self.t_gamma_pa = Field((cap,), f64, n=3, device=dev)
+        self._stress_pressure_valid = Field((cap,), i32, device=dev)
+        self.F_gamma_n = Field((cap,), f64, n=3, device=dev)
+        self._report = torch.zeros(16, dtype=torch.float64, device=dev)
+        self._bins: dict = {}
+
+    def __del__(self):
+        for plan in getattr(self, "_bins", {}).values():
+            try:
+                _native.load().efsi_bin_plan_destroy(plan[0])
+            except Exception:
+                pass
+
+    # ------------------------------------------------------------------
+    def load_markers(self, *, positions_m, velocities_mps, normals, areas_m2, region_ids) -> None:
+        count = len(positions_m)
+        if count > self.marker_capacity:
+            raise ValueError("marker count exceeds marker_capacity")
+        if not (len(velocities_mps) == len(normals) == len(areas_m2) == len(region_ids) == count):
+            raise ValueError("marker inputs must have matching lengths")
+        pos = np.zeros((self.marker_capacity, 3), dtype=np.float32)
+        vel = np.zeros_like(pos)
+        nor = np.zeros_like(pos)
+        area = np.zeros(self.marker_capacity, dtype=np.float32)
+        reg = np.zeros(self.marker_capacity, dtype=np.int32)
+        for m in range(count):
+            pos[m] = _vector3(positions_m[m], name="positions_m")
+            vel[m] = _vector3(velocities_mps[m], name="velocities_mps")
+            nor[m] = _normalize_vector3(normals[m], name="normals")
+            a = float(areas_m2[m])
+            if not math.isfinite(a) or a < 0.0:
+                raise ValueError("areas_m2 must contain finite non-negative values")
+            area[m] = a
+            reg[m] = int(region_ids[m])
+        self.marker_count = int(count)
+        self.projection_triangle_count = 0
+        self.x_gamma_m.from_numpy(pos)
+        self.v_gamma_mps.from_numpy(vel)
+        self.n_gamma.from_numpy(nor)
+        self.A_gamma_m2.from_numpy(area)
+        self.region_id.from_numpy(reg)
+        self.t_gamma_pa.tensor.zero_()
+        self.F_gamma_n.tensor.zero_()
+
+    def set_marker_tractions_pa(self, tractions_pa) -> None:
+        if len(tractions_pa) != self.marker_count:
+            raise ValueError("tractions_pa must match marker_count")
+        t = np.zeros((self.marker_capacity, 3), dtype=np.float64)
+        for m in range(self.marker_count):
+            t[m] = _vector3(tractions_pa[m], name="tractions_pa")
+        self.t_gamma_pa.from_numpy(t)
+
+    def compute_marker_forces(self) -> None:
+        _native.call(
+            "efsi_compute_marker_forces",
+            int(self.marker_count),
+            self.t_gamma_pa.ptr(),
+            self.A_gamma_m2.ptr(),
+            self.F_gamma_n.ptr(),
+            c_void_p(current_stream_handle()),
+        )
+
+    # ------------------------------------------------------------------
+    def sample_fluid_stress_to_marker_tractions(
+        self,
+        velocity_field,
+        pressure_field,
+        obstacle_field,
+        cell_face_x_m,
+        cell_face_y_m,
+        cell_face_z_m,
+        cell_center_x_m,
+        cell_center_y_m,
+        cell_center_z_m,
+        cell_width_x_m,
+        cell_width_y_m,
+        cell_width_z_m,
+        grid_nodes,
+        *,
+        viscosity_pa_s: float,
+        two_sided_pressure: bool = False,
+        far_pressure_region_id: int = -1,
+        far_pressure_pa: float = 0.0,
+        far_pressure_side_normal_sign: float = 0.0,
+        far_pressure_inside_probe_max_multiplier: float = 3.0,
+        two_sided_probe_max_multiplier: float = 3.0,
+        one_sided_pressure_region_id: int = -1,
+        one_sided_reference_pressure_pa: float = 0.0,
+        one_sided_probe_max_multiplier: float = 3.0,
+        use_pressure_anchor_fallback: bool = False,
+        node_anchor_cell=None,
+        sampling_obstacle_field=None,
+        read_report: bool = True,
+    ) -> HibmMpmFluidStressSampleReport | None:
+        nodes = tuple(int(v) for v in grid_nodes)
+        if len(nodes) != 3 or any(v < 2 for v in nodes):
+            raise ValueError("grid_nodes must contain three values >= 2")
+        viscosity = float(viscosity_pa_s)
+        if not math.isfinite(viscosity) or viscosity < 0.0:
+            raise ValueError("viscosity_pa_s must be a finite non-negative number")
+        if not math.isfinite(float(far_pressure_pa)):
+            raise ValueError("far_pressure_pa must be a finite number")
+        if float(far_pressure_side_normal_sign) not in (-1.0, 0.0, 1.0):
+            raise ValueError("far_pressure_side_normal_sign must be -1.0, 0.0, or 1.0")
+        for value, name in (
+            (far_pressure_inside_probe_max_multiplier, "far_pressure_inside_probe_max_multiplier"),
+            (two_sided_probe_max_multiplier, "two_sided_probe_max_multiplier"),
+            (one_sided_probe_max_multiplier, "one_sided_probe_max_multiplier"),
+        ):
+            if not math.isfinite(float(value)) or float(value) < 3.0:
+                raise ValueError(f"{name} must be finite and >= 3.0")
+        if not math.isfinite(float(one_sided_reference_pressure_pa)):
+            raise ValueError("one_sided_reference_pressure_pa must be a finite number")
+        fast_path = (
+            viscosity == 0.0
+            and int(far_pressure_region_id) < 0
+            and not bool(use_pressure_anchor_fallback)
+            and node_anchor_cell is None
+            and sampling_obstacle_field is None
+        )
+        if not fast_path:
+            raise NotImplementedError(
+                "only the pressure-only traction sampler (hibm_mpm.py:2253) is on the B200 hot path"
+            )
+        p = _tensor(pressure_field)
+        if p.dtype != torch.float64:
+            p = p.to(torch.float64)
+        p = p.contiguous()
+        axes = _native.GridAxes(
+            _tensor(cell_face_x_m).data_ptr(),
+            _tensor(cell_face_y_m).data_ptr(),
+            _tensor(cell_face_z_m).data_ptr(),
+            _tensor(cell_center_x_m).data_ptr(),
+            _tensor(cell_center_y_m).data_ptr(),
+            _tensor(cell_center_z_m).data_ptr(),
+        )
+        rep = self._report
+        _native.call(
+            "efsi_sample_pressure_tractions",
+            nodes[0],
+            nodes[1],
+            nodes[2],
+            byref(axes),
+            c_void_p(_tensor(cell_width_x_m).data_ptr()),
+            c_void_p(_tensor(cell_width_y_m).data_ptr()),
+            c_void_p(_tensor(cell_width_z_m).data_ptr()),
+            c_void_p(_tensor(obstacle_field).data_ptr()),
+            c_void_p(p.data_ptr()),
+            int(self.marker_count),
+            self.x_gamma_m.ptr(),
+            self.n_gamma.ptr(),
+            self.region_id.ptr(),
+            1 if two_sided_pressure else 0,
+            int(one_sided_pressure_region_id),
+            float(one_sided_reference_pressure_pa),
+            self.t_gamma_pa.ptr(),
+            self._stress_pressure_valid.ptr(),
+            c_void_p(rep.data_ptr()),
+            c_void_p(current_stream_handle()),
+        )
+        if not read_report:
+            return None
+        r = rep[:5].cpu().tolist()
+        return HibmMpmFluidStressSampleReport(
+            valid_marker_count=int(r[0]),
+            invalid_marker_count=int(r[1]),
+            max_abs_traction_pa=float(r[4]),
+            two_sided_pressure_marker_count=int(r[2]),
+            one_sided_pressure_marker_count=int(r[3]),
+        )
+
+    def aggregate_region_forces(self, *, primary_region_id: int, secondary_region_id: int) -> HibmMpmSurfaceMarkerForceReport:
+        n = int(self.marker_count)
+        F = self.F_gamma_n.tensor[:n]
+        reg = self.region_id.tensor[:n]
+        valid = self._stress_pressure_valid.tensor[:n] != 0
+        norms = F.norm(dim=1)
+
+        def part(mask):
+            if mask is None:
+                mask = torch.ones(n, dtype=torch.bool, device=F.device)
+            return torch.cat(
+                [
+                    torch.where(mask[:, None], F, 0.0).sum(dim=0),
+                    torch.where(mask, norms, 0.0).sum()[None],
+                    torch.where(mask, norms, 0.0).max()[None] if n else torch.zeros(1, dtype=F.dtype, device=F.device),
+                    mask.sum()[None].to(F.dtype),
+                    (mask & valid).sum()[None].to(F.dtype),
+                    (mask & ~valid).sum()[None].to(F.dtype),
+                ]
+            )
+
+        pm, sm = reg == int(primary_region_id), reg == int(secondary_region_id)
+        vals = torch.stack([part(pm), part(sm), part(None)]).cpu().numpy()
+        p, s, t = vals
+        total = tuple(float(v) for v in t[:3])
+        reaction = tuple(-v for v in total)
+        resid = math.sqrt(sum((a + b) * (a + b) for a, b in zip(total, reaction)))
+        return HibmMpmSurfaceMarkerForceReport(
+            primary_marker_force_n=tuple(float(v) for v in p[:3]),
+            secondary_marker_force_n=tuple(float(v) for v in s[:3]),
+            total_marker_force_n=total,
+            primary_marker_count=int(p[5]),
+            secondary_marker_count=int(s[5]),
+            total_marker_count=int(t[5]),
+            fluid_reaction_force_n=reaction,
+            action_reaction_residual_n=resid,
+            primary_stress_valid_marker_count=int(p[6]),
+            primary_stress_invalid_marker_count=int(p[7]),
+            secondary_stress_valid_marker_count=int(s[6]),
+            secondary_stress_invalid_marker_count=int(s[7]),
+            primary_marker_force_norm_sum_n=float(p[3]),
+            secondary_marker_force_norm_sum_n=float(s[3]),
+            total_marker_force_norm_sum_n=float(t[3]),
+            primary_marker_force_norm_max_n=float(p[4]),
+            secondary_marker_force_norm_max_n=float(s[4]),
+            total_marker_force_norm_max_n=float(t[4]),
+        )
+
+    # ------------------------------------------------------------------
+    def clear_mpm_external_forces(self, external_force_n, *, particle_count: int, read_report: bool = True):
+        particles = int(particle_count)
+        if particles <= 0:
+            raise ValueError("particle_count must be positive")
+        rep = self._report
+        _native.call(
+            "efsi_clear_external_forces",
+            particles,
+            c_void_p(_tensor(external_force_n).data_ptr()),
+            c_void_p(rep.data_ptr()) if read_report else None,
+            c_void_p(current_stream_handle()),
+        )
+        if not read_report:
+            return None
+        r = rep[:2].cpu().tolist()
+        return HibmMpmExternalForceClearReport(cleared_particle_count=int(r[0]), max_abs_external_force_before_n=float(r[1]))
+
+    def _bin_plan(self, particle_x: torch.Tensor, particle_count: int, support_radius: float):
+        key = (int(particle_x.shape[0]), float(support_radius))
+        plan = self._bins.get(key)
+        if plan is None:
+            pts = particle_x[:particle_count]
+            mk = self.x_gamma_m.tensor[: max(int(self.marker_count), 1)]
+            allp = torch.cat([pts, mk], dim=0)
+            finite = torch.isfinite(allp).all(dim=1)
+            allp = allp[finite] if bool(finite.any()) else torch.zeros(1, 3, device=allp.device)
+            lo = allp.min(dim=0).values.cpu().numpy().astype(np.float64)
+            hi = allp.max(dim=0).values.cpu().numpy().astype(np.float64)
+            pad = np.maximum(0.5 * (hi - lo), 4.0 * support_radius)
+            lo, hi = lo - pad, hi + pad
+            bmin = (c_float * 3)(*[float(v) for v in lo])
+            bmax = (c_float * 3)(*[float(v) for v in hi])
+            handle = c_void_p()
+            _native.call("efsi_bin_plan_create", key[0], bmin, bmax, float(support_radius), byref(handle))
+            plan = (handle,)
+            self._bins[key] = plan
+        _native.call(
+            "efsi_bin_particles", plan[0], c_void_p(particle_x.data_ptr()), int(particle_count), c_void_p(current_stream_handle())
+        )
+        return plan[0]
+
+    def scatter_marker_forces_to_mpm_particles(
+        self, external_force_n, particle_position_m, *, particle_count: int, support_radius_m: float, read_report: bool = True
+    ) -> HibmMpmMpmForceScatterReport | None:
+        particles = int(particle_count)
+        if particles <= 0:
+            raise ValueError("particle_count must be positive")
+        radius = float(support_radius_m)
+        if not math.isfinite(radius) or radius <= 0.0:
+            raise ValueError("support_radius_m must be a finite positive number")
+        xp = _tensor(particle_position_m)
+        plan = self._bin_plan(xp, particles, radius)
+        rep = self._report
+        _native.call(
+            "efsi_scatter_marker_forces",
+            plan,
+            int(self.marker_count),
+            self.x_gamma_m.ptr(),
+            self.F_gamma_n.ptr(),
+            c_void_p(xp.data_ptr()),
+            c_void_p(_tensor(external_force_n).data_ptr()),
+            c_void_p(rep.data_ptr()),
+            c_void_p(current_stream_handle()),
+        )
+        if not read_report:
+            return None
+        r = rep[:9].cpu().tolist()
+        marker = tuple(float(v) for v in r[3:6])
+        ext = tuple(float(v) for v in r[6:9])
+        resid = math.sqrt(sum((a - b) * (a - b) for a, b in zip(marker, ext)))
+        return HibmMpmMpmForceScatterReport(
+            active_marker_count=int(r[0]),
+            invalid_marker_count=int(r[1]),
+            active_particle_count=int(r[2]),
+            total_marker_force_n=marker,
+            total_mpm_external_force_n=ext,
+            action_reaction_residual_n=resid,
+        )
+
+    def _feedback(self, xp, vp, np_, ap, particle_count, support_radius_m, dt_s, read_report):
+        particles = int(particle_count)
+        if particles <= 0:
+            raise ValueError("particle_count must be positive")
+        radius = float(support_radius_m)
+        if not math.isfinite(radius) or radius <= 0.0:
+            raise ValueError("support_radius_m must be a finite positive number")
+        dt = float(dt_s)
+        if not math.isfinite(dt) or dt <= 0.0:
+            raise ValueError("dt_s must be a finite positive number")
+        xp = _tensor(xp)
+        plan = self._bin_plan(xp, particles, radius)
+        rep = self._report
+        _native.call(
+            "efsi_surface_feedback",
+            plan,
+            int(self.marker_count),
+            self.x_gamma_m.ptr(),
+            self.v_gamma_mps.ptr(),
+            self.n_gamma.ptr(),
+            self.A_gamma_m2.ptr(),
+            c_void_p(xp.data_ptr()),
+            c_void_p(_tensor(vp).data_ptr()),
+            None if np_ is None else c_void_p(_tensor(np_).data_ptr()),
+            None if ap is None else c_void_p(_tensor(ap).data_ptr()),
+            dt,
+            c_void_p(rep.data_ptr()),
+            c_void_p(current_stream_handle()),
+        )
+        if not read_report:
+            return None
+        r = rep[:8].cpu().tolist()
+        return HibmMpmSurfaceUpdateReport(
+            updated_marker_count=int(r[0]),
+            invalid_marker_count=int(r[1]),
+            max_marker_displacement_m=float(r[4]),
+            max_marker_speed_mps=float(r[5]),
+            geometry_updated_marker_count=int(r[2]),
+            geometry_invalid_marker_count=int(r[3]),
+            max_marker_normal_change=float(r[6]),
+            max_marker_area_change_m2=float(r[7]),
+        )
+
+    def update_surface_feedback_from_mpm_particles(
+        self, particle_position_m, particle_velocity_mps, *, particle_count: int, support_radius_m: float, dt_s: float, read_report: bool = True
+    ):
+        return self._feedback(particle_position_m, particle_velocity_mps, None, None, particle_count, support_radius_m, dt_s, read_report)
+
+    def update_surface_feedback_from_mpm_surface_particles(
+        self,
+        particle_position_m,
+        particle_velocity_mps,
+        particle_normal,
+        particle_area_m2,
+        *,
+        particle_count: int,
+        support_radius_m: float,
+        dt_s: float,
+        read_report: bool = True,
+    ):
+        return self._feedback(
+            particle_position_m, particle_velocity_mps, particle_normal, particle_area_m2, particle_count, support_radius_m, dt_s, read_report
+        )
+
+    # ------------------------------------------------------------------
+    @staticmethod
+    def _vector_value_tuple(field: Field, index: int) -> tuple[float, float, float]:
+        v = field[int(index)]
+        return (float(v[0]), float(v[1]), float(v[2]))
+
+    def marker_force_n(self, marker_index: int):
+        return self._vector_value_tuple(self.F_gamma_n, marker_index)
+
+    def marker_traction_pa(self, marker_index: int):
+        return self._vector_value_tuple(self.t_gamma_pa, marker_index)
+
+    def marker_normal(self, marker_index: int):
+        return self._vector_value_tuple(self.n_gamma, marker_index)
+
+    def marker_velocity_mps(self, marker_index: int):
+        return self._vector_value_tuple(self.v_gamma_mps, marker_index)
+
+    def marker_region_id(self, marker_index: int) -> int:
+        return int(self.region_id[int(marker_index)])

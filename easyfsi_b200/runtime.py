@@ -1,0 +1,70 @@
+"""Process-wide runtime of the B200 path (replaces simulation_core/runtime.py).
+
+``TaichiRuntimeConfig`` keeps the reference's name and fields so callers that
+build one keep working; here it selects the CUDA device instead of a Taichi
+backend.  Like the reference (runtime.py:24-59) the first initialisation wins,
+the CPU backend is refused and a different ``default_fp`` later is an error.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+
+from . import _native
+
+_SUPPORTED_ARCHS = ("cuda", "gpu")
+_SUPPORTED_FPS = ("f32", "f64")
+
+# dtype tokens (the reference compares field dtypes against ti.f32 / ti.f64 / ti.i32)
+f32 = torch.float32
+f64 = torch.float64
+i32 = torch.int32
+
+
+@dataclass(frozen=True)
+class TaichiRuntimeConfig:
+    arch: str = "cuda"
+    default_fp: str = "f32"
+    random_seed: int = 0
+
+
+RuntimeConfig = TaichiRuntimeConfig
+
+_STATE = {"initialized": False, "fp": None, "device": None}
+
+
+def init_runtime(config: TaichiRuntimeConfig | None = None) -> torch.device:
+    """Initialise once; return the CUDA device all fields live on."""
+    cfg = config or TaichiRuntimeConfig()
+    arch = str(cfg.arch).lower()
+    if arch == "cpu":
+        raise ValueError("easyfsi_b200 is GPU-only; use arch='cuda' or arch='gpu'")
+    if arch not in _SUPPORTED_ARCHS:
+        raise ValueError(f"unsupported arch: {cfg.arch!r}")
+    fp = str(cfg.default_fp)
+    if fp not in _SUPPORTED_FPS:
+        raise ValueError(f"unsupported default_fp: {cfg.default_fp!r}; expected one of {_SUPPORTED_FPS}")
+    if _STATE["initialized"]:
+        if _STATE["fp"] != fp:
+            raise ValueError(
+                f"runtime is already initialized with default_fp={_STATE['fp']!r}; "
+                f"cannot re-initialize with default_fp={fp!r}"
+            )
+        return _STATE["device"]
+    if not torch.cuda.is_available():
+        raise RuntimeError("easyfsi_b200 requires a CUDA device (B200, sm_100a); none is visible")
+    _native.load()
+    torch.manual_seed(int(cfg.random_seed))
+    device = torch.device("cuda", torch.cuda.current_device())
+    _STATE.update(initialized=True, fp=fp, device=device)
+    return device
+
+
+# The reference's entry point name.
+init_taichi = init_runtime
+
+
+def current_stream_handle() -> int:
+    return torch.cuda.current_stream().cuda_stream

@@ -1,0 +1,322 @@
+/*
+ * easyfsi_b200 C ABI -- the drop-in boundary of the B200 implementation of the
+ * EasyFsi coupled-step hot path.
+ *
+ * Every entry point takes plain device pointers (CUDA global memory, C order
+ * (nx, ny, nz) with k fastest, vector fields stored as (n, 3) and matrices as
+ * (n, 3, 3) rows), plain sizes and a cudaStream_t passed as void*.  Every entry
+ * point returns an int status (EFSI_OK on success); a failing status leaves
+ * the message in efsi_last_error().  No entry point takes ownership of caller
+ * memory.  Plans (efsi_fv_plan, efsi_mpm_plan, efsi_bin_plan) own their
+ * derived tables and work buffers.
+ *
+ * Each declaration names the reference function it replaces as
+ * file:line in lizhuoh9/EasyFsi (simulation_core/...).
+ */
+#ifndef EASYFSI_B200_H
+#define EASYFSI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define EFSI_OK 0
+#define EFSI_ERR_ARG 1
+#define EFSI_ERR_CUDA 2
+#define EFSI_ERR_STATE 3
+
+/* Last error message of the calling thread (never NULL). */
+const char* efsi_last_error(void);
+/* Library version string. */
+const char* efsi_version(void);
+/* Number of kernels this library has launched in the process so far. */
+uint64_t efsi_kernel_launch_count(void);
+
+/* Benchmark instrumentation (no counterpart in the reference): bracket every
+ * launch of a kernel family with CUDA events on its stream and accumulate the
+ * family's algorithmic bytes.  Families: 0 SpMV+direction, 1 level-0 smoother
+ * sweeps, 2 CG update, 3 level-0 residual+restriction, 4 CG dots, 5 MPM P2G,
+ * 6 predictor.  Enabling resets the family's record; reading synchronises. */
+int efsi_kernel_timing_enable(int32_t family, int32_t enable);
+int efsi_kernel_timing_read(int32_t family, int64_t* launches, double* total_ms, double* total_bytes);
+
+/* ------------------------------------------------------------------------ */
+/* Fluid grid / multigrid hierarchy                                          */
+/* ------------------------------------------------------------------------ */
+
+/* One multigrid level: f32 device axis arrays exactly as the reference loads
+ * them into cell_width_*_m / center_distance_*_m (fluid.py:1013-1024,
+ * 1161-1199; coarse levels fluid.py:692-729). */
+typedef struct efsi_level_desc {
+  int32_t nx, ny, nz;
+  const float* wx;
+  const float* wy;
+  const float* wz;
+  const float* cdx;
+  const float* cdy;
+  const float* cdz;
+} efsi_level_desc;
+
+typedef struct efsi_fv_plan efsi_fv_plan;
+
+/* Builds the per-level f64 face-coefficient tables and allocates the solver
+ * work vectors for the hierarchy (replaces the field allocation of
+ * CartesianFluidSolver.__init__, fluid.py:736-1075). */
+int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t uniform_grid, efsi_fv_plan** out);
+int efsi_fv_plan_destroy(efsi_fv_plan* plan);
+
+/* Rebuilds the per-cell stencil masks of every level from the obstacle, the
+ * velocity-Dirichlet rows and the interface diagonal (the coarse part replaces
+ * the obstacle / Dirichlet / interface-diagonal half of
+ * _mg_restrict_residual_kernel, fluid.py:5310-5388).  vdir_active, vdir_weight
+ * and iface_diag may be NULL (inactive). */
+int efsi_fv_set_masks(efsi_fv_plan* plan, const int32_t* obstacle, const int32_t* vdir_active,
+                      const float* vdir_weight, const double* iface_diag, void* stream);
+
+/* fluid.py:3451-3486 _compute_divergence_kernel. velocity (n,3) f32 -> div f32. */
+int efsi_compute_divergence(efsi_fv_plan* plan, const float* velocity, int32_t outlet, float* divergence,
+                            void* stream);
+
+/* fluid.py:5228-5243 _mg_prepare_level0_kernel: rhs = s (div - src) - iface_rhs (f64 out).
+ * iface_rhs may be NULL. */
+int efsi_mg_prepare_level0(efsi_fv_plan* plan, const float* divergence, const float* volume_source,
+                           const double* iface_rhs, float rhs_scale, double* rhs, void* stream);
+
+/* fluid.py:4312-4345 _fv_laplacian_apply_kernel (level 0, f64). */
+int efsi_fv_apply(efsi_fv_plan* plan, const double* p, double* out, int32_t outlet, void* stream);
+
+/* fluid.py:4280-4309 _fv_diagonal_kernel. */
+int efsi_fv_diagonal(efsi_fv_plan* plan, double* diag, int32_t outlet, void* stream);
+
+/* fluid.py:4503-4516 _apply_jacobi_preconditioner_kernel. */
+int efsi_apply_jacobi_preconditioner(efsi_fv_plan* plan, const double* diag, const double* r, double* z,
+                                     void* stream);
+
+/* fluid.py:4534-4546 _weighted_dot_kernel: sum over fluid cells of a b V (f64,
+ * deterministic order).  Synchronises the stream and writes the host result. */
+int efsi_weighted_dot(efsi_fv_plan* plan, const double* a, const double* b, double* result_host, void* stream);
+
+/* fluid.py:4224-4273 _pressure_fv_jacobi_kernel, one out-of-place sweep on
+ * level `level` (level 0: double arrays, coarse levels: float arrays).  rhs
+ * and iface follow the level's storage type. */
+int efsi_fv_jacobi_sweep(efsi_fv_plan* plan, int32_t level, const void* p, const void* rhs, void* tmp,
+                         int32_t outlet, double omega, void* stream);
+
+/* fluid.py:5262-5307 _mg_compute_residual_kernel on `level`. */
+int efsi_fv_residual(efsi_fv_plan* plan, int32_t level, const void* p, const void* rhs, void* residual,
+                     int32_t outlet, void* stream);
+
+/* fluid.py:5310-5388 _mg_restrict_residual_kernel: coarse_rhs of level+1
+ * (float) from the fine residual of `level`; the optional outputs receive the
+ * coarse interface diagonal, obstacle and Dirichlet flag / weight views. */
+int efsi_mg_restrict(efsi_fv_plan* plan, int32_t level, const void* fine_residual, float* coarse_rhs,
+                     float* coarse_iface, int32_t* coarse_obstacle, int32_t* coarse_vdir_active,
+                     float* coarse_vdir_weight, void* stream);
+
+/* fluid.py:5391-5406 _mg_prolongate_add_kernel: fine(level) += s * coarse(level+1). */
+int efsi_mg_prolong(efsi_fv_plan* plan, int32_t level, void* fine_p, const float* coarse_p, double scale,
+                    void* stream);
+
+/* fluid.py:6085-6262 _apply_fv_multigrid_preconditioner: z = V-cycle(r), zero
+ * initial guess. */
+int efsi_mg_vcycle(efsi_fv_plan* plan, const double* r, double* z, int32_t outlet, int32_t pre, int32_t coarse,
+                   int32_t post, void* stream);
+
+typedef struct efsi_pcg_params {
+  int32_t max_iters;
+  int32_t precond;      /* 0 jacobi, 1 fv_multigrid (2/24/2), 2 fv_multigrid_light (1/12/1) */
+  int32_t remove_mean;  /* closed-domain zero-mean projection */
+  int32_t outlet;       /* pressure_outlet_zmin */
+  int32_t iface_active; /* interface terms present: MG disabled, restart every 256 */
+  int32_t use_graphs;   /* capture the 16-iteration blocks into CUDA graphs */
+  double tolerance;
+} efsi_pcg_params;
+
+typedef struct efsi_cg_stats {
+  int32_t iterations;
+  int32_t converged;
+  int32_t breakdown_code;
+  int32_t breakdown_reason; /* 0 none, 1 initial dot, 2 device scalar, 3 restart dot */
+  int32_t host_residual_checks;
+  int32_t restart_count;
+  int32_t mean_projection_count;
+  int32_t used_mg;
+  double initial_relative_residual;
+  double relative_residual;
+  double breakdown_dAd;
+  double b_norm;
+} efsi_cg_stats;
+
+/* fluid.py:6535-6811 _solve_pressure_poisson_fv_cg: flexible MG/Jacobi PCG on
+ * A p = b in the cell-volume inner product, from the f64 level-0 rhs built by
+ * efsi_mg_prepare_level0.  pressure is the warm start and the solution. */
+int efsi_fv_pcg_solve(efsi_fv_plan* plan, const double* rhs0, double* pressure, const efsi_pcg_params* params,
+                      efsi_cg_stats* stats, void* stream);
+
+/* fluid.py:5992-6083 _solve_pressure_poisson_fv_multigrid (standalone cycles). */
+int efsi_fv_multigrid_solve(efsi_fv_plan* plan, const double* rhs0, double* pressure, int32_t outlet,
+                            int32_t iterations, int32_t cycles, void* stream);
+
+/* fluid.py:5977-5990 _solve_pressure_poisson_fv_jacobi (omega 0.8 sweeps on level 0). */
+int efsi_fv_jacobi_solve(efsi_fv_plan* plan, const double* rhs0, double* pressure, int32_t outlet,
+                         int32_t iterations, void* stream);
+
+/* fluid.py:3997-4059 _pressure_jacobi_kernel + _copy_pressure_kernel, `iterations`
+ * times (the legacy uniform-grid solver "jacobi"); tmp is an f64 scratch field. */
+int efsi_legacy_jacobi_solve(efsi_fv_plan* plan, const float* divergence, const float* volume_source,
+                             float rhs_scale, float inv_dx2, float inv_dy2, float inv_dz2, int32_t outlet,
+                             int32_t iterations, double* pressure, double* tmp, void* stream);
+
+/* fluid.py:5538-5582 _subtract_pressure_gradient_kernel.  vdir_* may be NULL. */
+int efsi_subtract_pressure_gradient(efsi_fv_plan* plan, const double* pressure, const int32_t* vdir_active,
+                                    const float* vdir_weight, const float* vdir_value, float dt_over_rho,
+                                    int32_t outlet, float* velocity, void* stream);
+
+/* fluid.py:5529-5536 _apply_closed_boundary_no_normal_flow_kernel. */
+int efsi_apply_closed_boundary(efsi_fv_plan* plan, int32_t outlet, float* velocity, void* stream);
+
+/* fluid.py:5762-5766 _apply_zmin_no_backflow_kernel. */
+int efsi_apply_zmin_no_backflow(efsi_fv_plan* plan, float* velocity, void* stream);
+
+/* fluid.py:2549-2593 _apply_velocity_dirichlet_boundary_rows_kernel.
+ * report_device (may be NULL): double[6] = cells, delta_sum, delta_max, momentum xyz. */
+int efsi_apply_velocity_dirichlet_rows(efsi_fv_plan* plan, const int32_t* vdir_active, const float* vdir_value,
+                                       float density, float* velocity, double* report_device, void* stream);
+
+/* Fluid grid faces / centres (device f32) used by the predictor and samplers. */
+typedef struct efsi_grid_axes {
+  const float* fx;
+  const float* fy;
+  const float* fz;
+  const float* cx;
+  const float* cy;
+  const float* cz;
+} efsi_grid_axes;
+
+/* fluid.py:2447-2527 _predict_kernel (velocity_prev is read, velocity written). */
+int efsi_predict(efsi_fv_plan* plan, const efsi_grid_axes* axes, const float* velocity_prev, float dt, float nu,
+                 int32_t rk2, float* velocity, void* stream);
+
+/* fluid.py:3494-3565 _divergence_stats_kernel / _divergence_residual_stats_kernel.
+ * mode 0 raw, 1 residual (minus volume source).  out_host: max_abs, sum_sq, count. */
+int efsi_divergence_stats(efsi_fv_plan* plan, const float* divergence, const double* iface_div,
+                          const float* volume_source, int32_t mode, int32_t interior_only, double* out_host,
+                          void* stream);
+
+/* fluid.py:3196-3273 _spread_surface_forces_kernel.  report_device: double[6]
+ * (surface force xyz, grid force xyz). */
+int efsi_spread_surface_forces(efsi_fv_plan* plan, const efsi_grid_axes* axes, const float* position,
+                               const float* force, int32_t vertex_count, float cx, float cy, float cz,
+                               float force_sign, float* grid_force_density, double* report_device, void* stream);
+
+/* fluid.py:3301-3328 _apply_body_force_kernel.  report_device: double[7]
+ * (impulse xyz, momentum xyz, active cells). */
+int efsi_apply_body_force(efsi_fv_plan* plan, const float* grid_force_density, float dt, float density,
+                          float* velocity, double* report_device, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Neo-Hookean MLS/APIC-MPM                                                  */
+/* ------------------------------------------------------------------------ */
+
+typedef struct efsi_mpm_plan efsi_mpm_plan;
+
+/* Scratch for particle binning on the MPM node grid (replaces nothing in the
+ * reference, which scatters with per-particle global atomics). */
+int efsi_mpm_plan_create(int32_t particle_capacity, int32_t nx, int32_t ny, int32_t nz, efsi_mpm_plan** out);
+int efsi_mpm_plan_destroy(efsi_mpm_plan* plan);
+
+typedef struct efsi_mpm_state {
+  int32_t particle_count;
+  int32_t nx, ny, nz;
+  float bmin[3];
+  float dx[3];
+  float* x;
+  float* v;
+  float* C;
+  float* F;
+  const float* mass;
+  const float* volume;
+  const float* fext;
+  const int32_t* fixed;
+  const int32_t* region;
+  const float* rest_x;
+  float* normal;
+  float* area;
+  const float* rest_normal;
+  const float* rest_area;
+  float* grid_mass;
+  float* grid_velocity;
+  float* grid_force;
+} efsi_mpm_state;
+
+/* neo_hookean_mpm.py:696-959 _step_kernel (clear, P2G, grid update, G2P,
+ * surface geometry, diagnostics).  report_device: double[34] in the layout of
+ * report_host_snapshot (neo_hookean_mpm.py:909-958), or NULL. */
+int efsi_mpm_step(efsi_mpm_plan* plan, const efsi_mpm_state* state, float dt, float mu, float lambda_,
+                  float velocity_damping, int32_t primary_region, int32_t secondary_region,
+                  double* report_device, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* HIBM surface markers                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* hibm_mpm.py:2253-2432 _sample_pressure_only_marker_tractions_kernel.
+ * report_device: double[5] = valid, invalid, two_sided, one_sided, max |t|. */
+int efsi_sample_pressure_tractions(int32_t nx, int32_t ny, int32_t nz, const efsi_grid_axes* axes,
+                                   const float* wx, const float* wy, const float* wz, const int32_t* obstacle,
+                                   const double* pressure, int32_t marker_count, const float* x_gamma,
+                                   const float* n_gamma, const int32_t* region, int32_t two_sided,
+                                   int32_t one_sided_region, float one_sided_reference, double* t_gamma,
+                                   int32_t* valid, double* report_device, void* stream);
+
+/* hibm_mpm.py:903-909 _compute_marker_forces_kernel: F = t A. */
+int efsi_compute_marker_forces(int32_t marker_count, const double* t_gamma, const float* area, double* f_gamma,
+                               void* stream);
+
+/* hibm_mpm.py:4861-4878 _clear_mpm_external_forces_kernel.
+ * report_device: double[2] = cleared count, max |f| before. */
+int efsi_clear_external_forces(int32_t particle_count, float* external_force, double* report_device,
+                               void* stream);
+
+typedef struct efsi_bin_plan efsi_bin_plan;
+
+/* Uniform binning of particles with bin edge = support radius over a box;
+ * used by the spreading and feedback entry points below. */
+int efsi_bin_plan_create(int32_t particle_capacity, const float* box_min, const float* box_max,
+                         float support_radius, efsi_bin_plan** out);
+int efsi_bin_plan_destroy(efsi_bin_plan* plan);
+/* Sorts particle indices into bins (stable: particle order within a bin). */
+int efsi_bin_particles(efsi_bin_plan* plan, const float* particle_x, int32_t particle_count, void* stream);
+
+/* hibm_mpm.py:4899-4959 _scatter_marker_forces_to_mpm_particles_kernel over the
+ * binned particles (the reference loops over all particles per marker).
+ * report_device: double[9] = active markers, invalid markers, active
+ * contributions, marker force xyz, external force xyz. */
+int efsi_scatter_marker_forces(efsi_bin_plan* plan, int32_t marker_count, const float* x_gamma,
+                               const double* f_gamma, const float* particle_x, float* external_force,
+                               double* report_device, void* stream);
+
+/* hibm_mpm.py:5097-5180 _update_surface_feedback_from_mpm_surface_particles_kernel
+ * (particle_normal / particle_area NULL: velocity-only variant hibm_mpm.py:5012-5053).
+ * report_device: double[8] = updated, invalid, geometry updated, geometry
+ * invalid, max displacement, max speed, max normal change, max area change. */
+int efsi_surface_feedback(efsi_bin_plan* plan, int32_t marker_count, float* x_gamma, float* v_gamma,
+                          float* n_gamma, float* area_gamma, const float* particle_x, const float* particle_v,
+                          const float* particle_normal, const float* particle_area, float dt,
+                          double* report_device, void* stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EASYFSI_B200_H */

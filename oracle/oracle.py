@@ -1,0 +1,392 @@
+"""Python binding of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads ``liboracle_mirror.so`` (the reference's f32/f64 precision mix) or
+``liboracle_fp64.so`` (all FP64) built from the C++ restatement in this
+directory, and exposes numpy-level wrappers plus ``OracleScene``, the coupled
+step of the reference's marker-MPM runner on host arrays.  Only the tests,
+``__graft_entry__.smoke`` and the CPU legs of ``bench.py`` use this module; the
+product path never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from ctypes import POINTER, Structure, byref, c_double, c_float, c_int, c_int32, c_int64, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIBS: dict[str, ctypes.CDLL] = {}
+
+
+def build(force: bool = False) -> None:
+    """Compile both oracle variants with the Makefile in this directory."""
+    args = ["make", "-C", str(HERE)]
+    if force:
+        args.append("-B")
+    subprocess.run(args, check=True, capture_output=True)
+
+
+def load(variant: str = "mirror") -> ctypes.CDLL:
+    if variant not in ("mirror", "fp64"):
+        raise ValueError("variant must be 'mirror' or 'fp64'")
+    if variant not in _LIBS:
+        path = HERE / f"liboracle_{variant}.so"
+        if not path.exists():
+            build()
+        _LIBS[variant] = ctypes.CDLL(str(path))
+    return _LIBS[variant]
+
+
+def r32_dtype(variant: str):
+    return np.float32 if variant == "mirror" else np.float64
+
+
+class Level(Structure):
+    _fields_ = [("nx", c_int32), ("ny", c_int32), ("nz", c_int32)] + [
+        (n, c_void_p) for n in ("wx", "wy", "wz", "cdx", "cdy", "cdz")
+    ]
+
+
+class Grid(Structure):
+    _fields_ = [("l0", Level)] + [(n, c_void_p) for n in ("fx", "fy", "fz", "cx", "cy", "cz")]
+
+
+class CgStats(Structure):
+    _fields_ = [
+        ("iterations", c_int32),
+        ("converged", c_int32),
+        ("breakdown_code", c_int32),
+        ("breakdown_reason", c_int32),
+        ("host_residual_checks", c_int32),
+        ("restart_count", c_int32),
+        ("mean_projection_count", c_int32),
+        ("used_mg", c_int32),
+        ("initial_relative_residual", c_double),
+        ("relative_residual", c_double),
+        ("breakdown_dAd", c_double),
+        ("b_norm", c_double),
+    ]
+
+
+class MpmState(Structure):
+    _fields_ = [
+        ("particle_count", c_int32),
+        ("nx", c_int32),
+        ("ny", c_int32),
+        ("nz", c_int32),
+        ("bmin", c_double * 3),
+        ("dx", c_double * 3),
+    ] + [(n, c_void_p) for n in (
+        "x", "v", "C", "F", "mass", "volume", "fext", "fixed", "region", "rest_x", "normal", "area",
+        "rest_normal", "rest_area", "grid_mass", "grid_vel", "grid_force")]
+
+
+class MpmReport(Structure):
+    _fields_ = [("values", c_double * 28), ("counts", c_int64 * 6)]
+
+
+class TractionReport(Structure):
+    _fields_ = [("valid", c_int64), ("invalid", c_int64), ("two_sided", c_int64), ("one_sided", c_int64), ("max_abs_traction", c_double)]
+
+
+class ScatterReport(Structure):
+    _fields_ = [("active_markers", c_int64), ("invalid_markers", c_int64), ("active_particle_contributions", c_int64),
+                ("marker_force", c_double * 3), ("external_force", c_double * 3)]
+
+
+class FeedbackReport(Structure):
+    _fields_ = [("updated", c_int64), ("invalid", c_int64), ("geometry_updated", c_int64), ("geometry_invalid", c_int64),
+                ("max_displacement", c_double), ("max_speed", c_double), ("max_normal_change", c_double),
+                ("max_area_change", c_double)]
+
+
+def _p(a: np.ndarray | None):
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("oracle arrays must be C-contiguous")
+    return c_void_p(a.ctypes.data)
+
+
+# ---------------------------------------------------------------------------
+# host grid metrics (same order of operations as the reference: running sums)
+# ---------------------------------------------------------------------------
+
+
+def axis_metrics(origin: float, widths) -> dict[str, np.ndarray]:
+    widths = [float(w) for w in widths]
+    faces = [float(origin)]
+    centers = []
+    face = float(origin)
+    for w in widths:
+        centers.append(face + 0.5 * w)
+        face += w
+        faces.append(faces[-1] + w)
+    dist = [widths[0]] + [centers[n] - centers[n - 1] for n in range(1, len(centers))]
+    return {"w": np.asarray(widths), "faces": np.asarray(faces), "centers": np.asarray(centers), "cd": np.asarray(dist)}
+
+
+def multigrid_levels(grid) -> list[list[dict]]:
+    """Per-level per-axis metrics (fluid.py:692-729, 1161-1199)."""
+    shape = grid.grid_nodes
+    shapes = [tuple(shape)]
+    cur = shapes[0]
+    while min(cur) > 3:
+        nxt = tuple(max(2, (n + 1) // 2) for n in cur)
+        if nxt == cur:
+            break
+        shapes.append(nxt)
+        cur = nxt
+    axes = [list(grid.cell_widths_x_m), list(grid.cell_widths_y_m), list(grid.cell_widths_z_m)]
+    levels = []
+    for _ in shapes:
+        levels.append([axis_metrics(grid.bounds_min_m[a], axes[a]) for a in range(3)])
+        axes = [[sum(w[n : min(n + 2, len(w))]) for n in range(0, len(w), 2)] for w in axes]
+    return levels
+
+
+class OracleFluid:
+    """Fluid state on host arrays (reference layouts) driven by the oracle."""
+
+    def __init__(self, grid, *, rho: float, mu: float, variant: str = "mirror"):
+        self.lib = load(variant)
+        self.variant = variant
+        self.rt = r32_dtype(variant)
+        self.grid = grid
+        self.nx, self.ny, self.nz = grid.grid_nodes
+        self.rho, self.mu = float(rho), float(mu)
+        self.uniform = bool(grid.is_uniform)
+        self.metrics = multigrid_levels(grid)
+        self._arrays = []
+        self.levels = (Level * len(self.metrics))()
+        for level, axes in enumerate(self.metrics):
+            L = self.levels[level]
+            L.nx, L.ny, L.nz = (len(a["w"]) for a in axes)
+            for a, name in enumerate("xyz"):
+                w = np.ascontiguousarray(axes[a]["w"].astype(np.float32).astype(self.rt))
+                cd = np.ascontiguousarray(axes[a]["cd"].astype(np.float32).astype(self.rt))
+                self._arrays += [w, cd]
+                setattr(L, "w" + name, _p(w))
+                setattr(L, "cd" + name, _p(cd))
+        m0 = self.metrics[0]
+        self.axes_f = []
+        for a in range(3):
+            fa = np.ascontiguousarray(m0[a]["faces"].astype(np.float32).astype(self.rt))
+            ce = np.ascontiguousarray(m0[a]["centers"].astype(np.float32).astype(self.rt))
+            self.axes_f.append((fa, ce))
+        self.gridstruct = Grid()
+        self.gridstruct.l0 = self.levels[0]
+        self.gridstruct.fx, self.gridstruct.fy, self.gridstruct.fz = (_p(self.axes_f[a][0]) for a in range(3))
+        self.gridstruct.cx, self.gridstruct.cy, self.gridstruct.cz = (_p(self.axes_f[a][1]) for a in range(3))
+        shape = (self.nx, self.ny, self.nz)
+        self.velocity = np.zeros(shape + (3,), dtype=self.rt)
+        self.velocity_prev = np.zeros_like(self.velocity)
+        self.pressure = np.zeros(shape, dtype=np.float64)
+        self.divergence = np.zeros(shape, dtype=self.rt)
+        self.volume_source = np.zeros(shape, dtype=self.rt)
+        self.obstacle = np.zeros(shape, dtype=np.int32)
+        self.rhs0 = np.zeros(shape, dtype=np.float64)
+        self.last_stats = CgStats()
+
+    # single kernels -------------------------------------------------------
+    def compute_divergence(self, outlet: int = 0) -> None:
+        self.lib.efo_compute_divergence(byref(self.levels[0]), _p(self.obstacle), _p(self.velocity), c_int(outlet), _p(self.divergence))
+
+    def prepare_rhs(self, rhs_scale: float) -> None:
+        self.lib.efo_mg_prepare_level0(byref(self.levels[0]), _p(self.obstacle), _p(self.divergence), _p(self.volume_source), None,
+                                       c_float(rhs_scale), _p(self.rhs0))
+
+    def fv_apply(self, p: np.ndarray, outlet: int = 0, vdir_active=None, vdir_weight=None, iface=None) -> np.ndarray:
+        out = np.zeros_like(p, dtype=np.float64)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        self.lib.efo_fv_apply(byref(self.levels[0]), _p(self.obstacle), _p(vdir_active), _p(vdir_weight), _p(iface), _p(p), _p(out), c_int(outlet))
+        return out
+
+    def fv_diagonal(self, outlet: int = 0, vdir_active=None, vdir_weight=None, iface=None) -> np.ndarray:
+        out = np.zeros((self.nx, self.ny, self.nz), dtype=np.float64)
+        self.lib.efo_fv_diagonal(byref(self.levels[0]), _p(self.obstacle), _p(vdir_active), _p(vdir_weight), _p(iface), _p(out), c_int(outlet))
+        return out
+
+    def weighted_dot(self, a: np.ndarray, b: np.ndarray) -> float:
+        self.lib.efo_weighted_dot.restype = c_double
+        return float(self.lib.efo_weighted_dot(byref(self.levels[0]), _p(self.obstacle), _p(np.ascontiguousarray(a, dtype=np.float64)),
+                                               _p(np.ascontiguousarray(b, dtype=np.float64))))
+
+    def vcycle(self, r: np.ndarray, outlet: int = 0, pre: int = 2, coarse: int = 24, post: int = 2) -> np.ndarray:
+        z = np.zeros_like(r, dtype=np.float64)
+        self.lib.efo_mg_vcycle(c_int(len(self.metrics)), self.levels, _p(self.obstacle), None, None, None,
+                               _p(np.ascontiguousarray(r, dtype=np.float64)), _p(z), c_int(outlet), c_int(pre), c_int(coarse),
+                               c_int(post), c_int(1 if self.uniform else 0))
+        return z
+
+    def pcg_solve(self, *, outlet: int, max_iters: int, tol: float, precond: int, remove_mean: bool) -> CgStats:
+        st = CgStats()
+        self.lib.efo_fv_pcg_solve(c_int(len(self.metrics)), self.levels, _p(self.obstacle), None, None, None, _p(self.rhs0),
+                                  _p(self.pressure), c_int(outlet), c_int(max_iters), c_double(tol), c_int(precond),
+                                  c_int(1 if remove_mean else 0), c_int(1 if self.uniform else 0), c_int(0), byref(st))
+        self.last_stats = st
+        return st
+
+    def predict(self, dt: float) -> None:
+        self.velocity_prev[...] = self.velocity
+        self.lib.efo_predict(byref(self.gridstruct), _p(self.obstacle), _p(self.velocity_prev), c_float(dt),
+                             c_float(self.mu / self.rho), c_int(0), _p(self.velocity))
+
+    def project(self, *, dt: float, max_iters: int = 400, tol: float = 1.0e-8, precond: int = 1) -> CgStats:
+        """Plain closed-box fv_cg projection (fluid.py:6889-7340 without Dirichlet rows)."""
+        self.compute_divergence(0)
+        self.prepare_rhs(self.rho / dt)
+        st = self.pcg_solve(outlet=0, max_iters=max_iters, tol=tol, precond=precond, remove_mean=True)
+        if not st.converged:
+            self.pressure[...] = 0.0
+        self.lib.efo_subtract_pressure_gradient(byref(self.levels[0]), _p(self.obstacle), None, None, None, _p(self.pressure),
+                                                c_float(dt / self.rho), c_int(0), _p(self.velocity))
+        self.compute_divergence(0)
+        self.lib.efo_apply_closed_boundary(byref(self.levels[0]), c_int(0), _p(self.velocity))
+        return st
+
+
+class OracleSolid:
+    def __init__(self, *, capacity: int, grid_nodes, bounds_min=(0.0, 0.0, 0.0), bounds_max=(1.0, 1.0, 1.0), variant="mirror"):
+        self.lib = load(variant)
+        self.rt = r32_dtype(variant)
+        self.nodes = tuple(int(n) for n in grid_nodes)
+        self.bmin = tuple(float(v) for v in bounds_min)
+        self.dx = tuple((float(bounds_max[a]) - self.bmin[a]) / self.nodes[a] for a in range(3))
+        P = int(capacity)
+        rt = self.rt
+        self.count = 0
+        self.x = np.zeros((P, 3), rt)
+        self.v = np.zeros((P, 3), rt)
+        self.C = np.zeros((P, 3, 3), rt)
+        self.F = np.tile(np.eye(3, dtype=rt), (P, 1, 1))
+        self.mass = np.zeros(P, rt)
+        self.volume = np.zeros(P, rt)
+        self.fext = np.zeros((P, 3), rt)
+        self.fixed = np.zeros(P, np.int32)
+        self.region = np.zeros(P, np.int32)
+        self.rest_x = np.zeros((P, 3), rt)
+        self.normal = np.zeros((P, 3), rt)
+        self.area = np.zeros(P, rt)
+        self.rest_normal = np.zeros((P, 3), rt)
+        self.rest_area = np.zeros(P, rt)
+        self.grid_mass = np.zeros(self.nodes, rt)
+        self.grid_vel = np.zeros(self.nodes + (3,), rt)
+        self.grid_force = np.zeros(self.nodes + (3,), rt)
+
+    def load(self, *, x, volume, mass, region=None, normal=None, area=None, fixed=None) -> None:
+        n = x.shape[0]
+        self.count = n
+        self.x[:n] = x
+        self.rest_x[:n] = x
+        self.volume[:n] = volume
+        self.mass[:n] = mass
+        if region is not None:
+            self.region[:n] = region
+        if normal is not None:
+            self.normal[:n] = normal
+            self.rest_normal[:n] = normal
+        if area is not None:
+            self.area[:n] = area
+            self.rest_area[:n] = area
+        if fixed is not None:
+            self.fixed[:n] = fixed
+
+    def step(self, *, dt: float, mu: float, lam: float, damping: float = 1.0, primary: int = 101, secondary: int = 202):
+        s = MpmState()
+        s.particle_count = self.count
+        s.nx, s.ny, s.nz = self.nodes
+        for a in range(3):
+            s.bmin[a] = float(np.float32(self.bmin[a]))
+            s.dx[a] = float(np.float32(self.dx[a]))
+        for name in ("x", "v", "C", "F", "mass", "volume", "fext", "fixed", "region", "rest_x", "normal", "area",
+                     "rest_normal", "rest_area", "grid_mass", "grid_vel", "grid_force"):
+            setattr(s, name, _p(getattr(self, name)))
+        rep = MpmReport()
+        self.lib.efo_mpm_step(byref(s), c_float(dt), c_float(mu), c_float(lam), c_float(damping), c_int(primary), c_int(secondary), byref(rep))
+        return rep
+
+
+class OracleMarkers:
+    def __init__(self, *, x, normal, area, region, variant="mirror"):
+        self.lib = load(variant)
+        rt = r32_dtype(variant)
+        self.count = x.shape[0]
+        self.x = np.ascontiguousarray(x, dtype=rt)
+        self.v = np.zeros_like(self.x)
+        self.n = np.ascontiguousarray(normal, dtype=rt)
+        self.A = np.ascontiguousarray(area, dtype=rt)
+        self.region = np.ascontiguousarray(region, dtype=np.int32)
+        self.t = np.zeros((self.count, 3), np.float64)
+        self.F = np.zeros((self.count, 3), np.float64)
+        self.valid = np.zeros(self.count, np.int32)
+
+    def sample_tractions(self, fluid: OracleFluid, *, two_sided: int = 0, one_sided_region: int = -1, one_sided_ref: float = 0.0):
+        rep = TractionReport()
+        self.lib.efo_sample_pressure_tractions(byref(fluid.gridstruct), _p(fluid.obstacle), _p(fluid.pressure), c_int(self.count),
+                                               _p(self.x), _p(self.n), _p(self.region), c_int(two_sided), c_int(one_sided_region),
+                                               c_float(one_sided_ref), _p(self.t), _p(self.valid), byref(rep))
+        return rep
+
+    def compute_forces(self) -> None:
+        self.lib.efo_compute_marker_forces(c_int(self.count), _p(self.t), _p(self.A), _p(self.F))
+
+    def clear(self, solid: OracleSolid):
+        cleared, mx = c_int64(0), c_double(0.0)
+        self.lib.efo_clear_external_forces(c_int(solid.count), _p(solid.fext), byref(cleared), byref(mx))
+        return cleared.value, mx.value
+
+    def scatter(self, solid: OracleSolid, radius: float):
+        rep = ScatterReport()
+        self.lib.efo_scatter_marker_forces(c_int(self.count), _p(self.x), _p(self.F), c_int(solid.count), _p(solid.x),
+                                           c_float(radius), _p(solid.fext), byref(rep))
+        return rep
+
+    def feedback(self, solid: OracleSolid, radius: float, dt: float, geometry: bool = True):
+        rep = FeedbackReport()
+        self.lib.efo_surface_feedback(c_int(self.count), _p(self.x), _p(self.v), _p(self.n), _p(self.A), c_int(solid.count),
+                                      _p(solid.x), _p(solid.v), _p(solid.normal) if geometry else None,
+                                      _p(solid.area) if geometry else None, c_float(radius), c_float(dt), byref(rep))
+        return rep
+
+
+class OracleScene:
+    """The coupled step of easyfsi_b200.scenarios.CoupledScene on host arrays."""
+
+    def __init__(self, cfg, *, variant: str = "mirror", initial_velocity=None, project_initial: bool = True):
+        from easyfsi_b200 import scenarios as sc
+
+        self.cfg = cfg
+        self.grid = sc.build_grid(cfg)
+        self.fluid = OracleFluid(self.grid, rho=cfg.density_kgm3, mu=cfg.viscosity_pa_s, variant=variant)
+        self.fluid.obstacle[...] = sc.obstacle_mask(self.grid, cfg.bodies)
+        u0 = initial_velocity if initial_velocity is not None else sc.fourier_velocity(
+            self.grid, cfg.velocity_seed, cfg.amplitude_mps, cfg.max_wavenumber)
+        self.fluid.velocity[...] = u0
+        if project_initial:
+            self.fluid.project(dt=cfg.dt_s, max_iters=cfg.cg_max_iterations, tol=cfg.cg_tolerance)
+            self.fluid.pressure[...] = 0.0
+        part = sc.particles(cfg)
+        self.solid = OracleSolid(capacity=part["x"].shape[0], grid_nodes=cfg.mpm_nodes, variant=variant)
+        self.solid.load(x=part["x"], volume=part["volume"], mass=part["mass"], region=part["region"], normal=part["normal"],
+                        area=part["area"])
+        mk = sc.markers(cfg)
+        self.markers = OracleMarkers(x=mk["x"], normal=mk["normal"], area=mk["area"], region=mk["region"], variant=variant)
+        self.mu, self.lam = sc.material(cfg)
+        self.radius = sc.support_radius(cfg)
+        self.last_stats = None
+
+    def step(self) -> None:
+        cfg = self.cfg
+        self.fluid.predict(cfg.dt_s)
+        self.last_stats = self.fluid.project(dt=cfg.dt_s, max_iters=cfg.cg_max_iterations, tol=cfg.cg_tolerance)
+        self.markers.sample_tractions(self.fluid, two_sided=0)
+        self.markers.compute_forces()
+        self.markers.clear(self.solid)
+        self.markers.scatter(self.solid, self.radius)
+        for _ in range(cfg.solid_substeps):
+            self.solid.step(dt=cfg.dt_s / cfg.solid_substeps, mu=self.mu, lam=self.lam)
+        self.markers.feedback(self.solid, self.radius, cfg.dt_s, geometry=True)

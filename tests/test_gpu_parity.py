@@ -1,0 +1,190 @@
+"""CUDA path vs the CPU oracle on identical seeded inputs (mirror precision).
+
+Tolerances: f64 quantities (pressure, CG vectors, tractions) relative L2
+<= 1e-10 (the operator itself to 1e-13); f32 quantities (velocity,
+divergence, MPM state, marker geometry) relative L2 <= 1e-5.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = max(np.linalg.norm(b.ravel()), 1e-300)
+    return float(np.linalg.norm((a - b).ravel()) / den)
+
+
+def _graded_grid(n=(14, 12, 18)):
+    from easyfsi_b200.scenarios import graded_axis_widths
+    from easyfsi_b200.grid import CartesianGrid
+
+    return CartesianGrid(
+        bounds_min_m=(0.0, 0.0, 0.0),
+        cell_widths_x_m=graded_axis_widths(n[0], 0.0, 1.0, 0.3, 0.7),
+        cell_widths_y_m=graded_axis_widths(n[1], 0.0, 1.0, 0.3, 0.7),
+        cell_widths_z_m=graded_axis_widths(n[2], 0.0, 1.0, 0.2, 0.8),
+    )
+
+
+def _solver(grid):
+    from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
+
+    spec = FluidDomainSpec((0, 0, 0), grid.bounds_max_m, None, 1000.0, 1.0e-3, 1.0e-3, cartesian_grid=grid)
+    return CartesianFluidSolver(spec)
+
+
+def _obstacle(grid, seed=3):
+    rng = np.random.default_rng(seed)
+    obs = np.zeros(grid.grid_nodes, dtype=np.int32)
+    nx, ny, nz = grid.grid_nodes
+    obs[nx // 3 : nx // 3 + 3, ny // 2 - 1 : ny // 2 + 2, nz // 2 : nz // 2 + 4] = 1
+    obs[rng.random(obs.shape) < 0.03] = 1
+    return obs
+
+
+@pytest.fixture(scope="module")
+def case():
+    grid = _graded_grid()
+    fl = _solver(grid)
+    ofl = orc.OracleFluid(grid, rho=1000.0, mu=1.0e-3, variant="mirror")
+    obs = _obstacle(grid)
+    fl.obstacle.from_numpy(obs)
+    ofl.obstacle[...] = obs
+    rng = np.random.default_rng(11)
+    vel = rng.normal(size=grid.grid_nodes + (3,)).astype(np.float32)
+    fl.velocity.from_numpy(vel)
+    ofl.velocity[...] = vel
+    return grid, fl, ofl, rng
+
+
+def test_divergence(case):
+    grid, fl, ofl, _ = case
+    fl.compute_divergence()
+    ofl.compute_divergence(0)
+    assert rel_l2(fl.divergence.to_numpy(), ofl.divergence) <= 1e-6
+
+
+def test_operator_diagonal_and_dot(case):
+    grid, fl, ofl, rng = case
+    p = rng.normal(size=grid.grid_nodes)
+    fl.pressure_tmp.from_numpy(p)
+    fl._fv_laplacian_apply_kernel(fl.pressure_tmp, fl.cg_r, 0)
+    assert rel_l2(fl.cg_r.to_numpy(), ofl.fv_apply(p, 0)) <= 1e-13
+    fl._fv_diagonal_kernel(fl.fv_diag, 0)
+    assert rel_l2(fl.fv_diag.to_numpy(), ofl.fv_diagonal(0)) <= 1e-14
+    q = rng.normal(size=grid.grid_nodes)
+    fl.cg_d.from_numpy(q)
+    got = fl._weighted_dot_kernel(fl.pressure_tmp, fl.cg_d)
+    assert got == pytest.approx(ofl.weighted_dot(p, q), rel=1e-12)
+    # outlet variant
+    fl._fv_laplacian_apply_kernel(fl.pressure_tmp, fl.cg_r, 1)
+    assert rel_l2(fl.cg_r.to_numpy(), ofl.fv_apply(p, 1)) <= 1e-13
+
+
+def test_vcycle_matches_oracle(case):
+    grid, fl, ofl, rng = case
+    r = rng.normal(size=grid.grid_nodes)
+    r[ofl.obstacle == 1] = 0.0
+    fl.cg_r.from_numpy(r)
+    fl._apply_fv_multigrid_preconditioner(fl.cg_r, pressure_outlet_zmin=False)
+    z_gpu = fl.cg_z.to_numpy()
+    z_ref = ofl.vcycle(r, 0)
+    assert rel_l2(z_gpu, z_ref) <= 1e-6
+
+
+@pytest.mark.parametrize("precond", ["fv_multigrid", "jacobi", "fv_multigrid_light"])
+def test_pcg_solve_matches_oracle(case, precond):
+    grid, fl, ofl, rng = case
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    fl.divergence.from_numpy(div)
+    ofl.divergence[...] = div
+    fl.pressure.tensor.zero_()
+    ofl.pressure[...] = 0.0
+    fl._solve_pressure_poisson_fv_cg(
+        iterations=300, rhs_scale=1000.0 / 1.0e-3, pressure_outlet_zmin=False, tolerance=1e-8, preconditioner=precond
+    )
+    ofl.prepare_rhs(1000.0 / 1.0e-3)
+    code = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2}[precond]
+    st = ofl.pcg_solve(outlet=0, max_iters=300, tol=1e-8, precond=code, remove_mean=True)
+    assert fl.last_cg_converged and st.converged
+    assert fl.last_cg_iterations == st.iterations
+    tol = 1e-10 if precond == "jacobi" else 1e-7
+    assert rel_l2(fl.pressure.to_numpy(), ofl.pressure) <= tol
+    # true residual of the GPU solution, measured by the oracle operator
+    rhs = ofl.rhs0.copy()
+    b = np.where(ofl.obstacle == 1, 0.0, -rhs)
+    vol = np.einsum("i,j,k->ijk", *[np.asarray(m["w"], np.float32).astype(np.float64) for m in ofl.metrics[0]])
+    fluid = ofl.obstacle == 0
+    b -= (b * vol)[fluid].sum() / vol[fluid].sum()
+    b[~fluid] = 0.0
+    res = b - ofl.fv_apply(fl.pressure.to_numpy(), 0)
+    res[~fluid] = 0.0
+    res -= (res * vol)[fluid].sum() / vol[fluid].sum()
+    res[~fluid] = 0.0
+    assert np.sqrt((res * res * vol).sum() / (b * b * vol).sum()) <= 1.1e-8
+
+
+def test_projection_gradient_and_predict(case):
+    grid, fl, ofl, rng = case
+    vel = (0.1 * rng.normal(size=grid.grid_nodes + (3,))).astype(np.float32)
+    fl.velocity.from_numpy(vel)
+    ofl.velocity[...] = vel
+    fl.pressure.tensor.zero_()
+    ofl.pressure[...] = 0.0
+    fl.project(iterations=300, dt_s=1e-3, pressure_solver="fv_cg", cg_tolerance=1e-8, cg_preconditioner="fv_multigrid", read_report=False)
+    ofl.project(dt=1e-3, max_iters=300, tol=1e-8)
+    assert rel_l2(fl.pressure.to_numpy(), ofl.pressure) <= 1e-7
+    assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) <= 1e-5
+    fl.predict(1e-3)
+    ofl.predict(1e-3)
+    assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) <= 1e-5
+
+
+def test_mpm_step_matches_oracle():
+    from easyfsi_b200.neo_hookean_mpm import NeoHookeanMpmState
+
+    rng = np.random.default_rng(5)
+    n = 2000
+    x = (0.35 + 0.3 * rng.random((n, 3))).astype(np.float32)
+    vol = np.full(n, 1.0e-6, np.float32)
+    mass = vol * 1100.0
+    gpu = NeoHookeanMpmState(particle_capacity=n, bounds_min_m=(0, 0, 0), bounds_max_m=(1, 1, 1), grid_nodes=(24, 24, 24))
+    gpu.load_particles(positions_m=x, volumes_m3=vol, masses_kg=mass, region_ids=np.full(n, 101, np.int32))
+    v0 = (0.05 * rng.normal(size=(n, 3))).astype(np.float32)
+    gpu.v.tensor[:n] = torch.as_tensor(v0, device=gpu.device)
+    ref = orc.OracleSolid(capacity=n, grid_nodes=(24, 24, 24), variant="mirror")
+    ref.load(x=x, volume=vol, mass=mass, region=np.full(n, 101, np.int32))
+    ref.v[:n] = v0
+    for _ in range(20):
+        rep = gpu.step(dt_s=1e-4, mu_pa=1.7e4, lambda_pa=1.6e5, primary_region_id=101, secondary_region_id=202)
+        ref.step(dt=1e-4, mu=1.7e4, lam=1.6e5)
+    assert rel_l2(gpu.x.to_numpy()[:n], ref.x[:n]) <= 1e-5
+    assert rel_l2(gpu.v.to_numpy()[:n], ref.v[:n]) <= 1e-4
+    assert rel_l2(gpu.F.to_numpy()[:n], ref.F[:n]) <= 1e-5
+    assert rep.transfer_relative_error < 2e-5
+
+
+def test_coupled_scene_matches_oracle():
+    from easyfsi_b200.scenarios import CoupledScene, tiny_config
+
+    cfg = tiny_config()
+    gpu = CoupledScene(cfg)
+    u0 = gpu.fluid.velocity.to_numpy()
+    ref = orc.OracleScene(cfg, variant="mirror", initial_velocity=u0, project_initial=False)
+    for _ in range(cfg.steps):
+        gpu.step()
+        ref.step()
+        assert gpu.last_cg_iterations == ref.last_stats.iterations
+    assert rel_l2(gpu.fluid.pressure.to_numpy(), ref.fluid.pressure) <= 1e-6
+    assert rel_l2(gpu.fluid.velocity.to_numpy(), ref.fluid.velocity) <= 1e-5
+    n = gpu.solid.particle_count
+    assert rel_l2(gpu.solid.x.to_numpy()[:n], ref.solid.x[:n]) <= 1e-5
+    assert rel_l2(gpu.markers.x_gamma_m.to_numpy()[: ref.markers.count], ref.markers.x) <= 1e-5
+    assert rel_l2(gpu.solid.external_force_n.to_numpy()[:n], ref.solid.fext[:n]) <= 1e-5
