@@ -52,6 +52,8 @@ class CgStats(Structure):
         ("restart_count", c_int32),
         ("mean_projection_count", c_int32),
         ("used_mg", c_int32),
+        ("used_graphs", c_int32),
+        ("reserved", c_int32),
         ("initial_relative_residual", c_double),
         ("relative_residual", c_double),
         ("breakdown_dAd", c_double),
@@ -100,6 +102,7 @@ D = c_double
 _PROTOTYPES: dict[str, list] = {
     "efsi_kernel_timing_enable": [I, I],
     "efsi_kernel_timing_read": [I, POINTER(ctypes.c_int64), POINTER(c_double), POINTER(c_double)],
+    "efsi_fv_kernel_replay": [P, I, I, POINTER(c_double), POINTER(c_double), P],
     "efsi_fv_plan_create": [POINTER(LevelDesc), I, I, POINTER(c_void_p)],
     "efsi_fv_plan_destroy": [P],
     "efsi_fv_set_masks": [P, P, P, P, P, P],
@@ -164,6 +167,8 @@ def load():
     lib.efsi_version.argtypes = []
     lib.efsi_kernel_launch_count.restype = ctypes.c_uint64
     lib.efsi_kernel_launch_count.argtypes = []
+    lib.efsi_fv_graph_error.restype = c_char_p
+    lib.efsi_fv_graph_error.argtypes = [c_void_p]
     for name, args in _PROTOTYPES.items():
         fn = getattr(lib, name)
         fn.restype = c_int32
@@ -173,7 +178,7 @@ def load():
 
 
 def exported_names() -> list[str]:
-    return ["efsi_last_error", "efsi_version", "efsi_kernel_launch_count", *_PROTOTYPES.keys()]
+    return ["efsi_last_error", "efsi_version", "efsi_kernel_launch_count", "efsi_fv_graph_error", *_PROTOTYPES.keys()]
 
 
 class NativeError(RuntimeError):
@@ -199,6 +204,14 @@ KERNEL_FAMILIES = {
     "p2g": 5,
     "predict": 6,
 }
+
+
+def kernel_replay(plan, family: str, reps: int = 50) -> tuple[float, float]:
+    """Mean ms per launch and algorithmic bytes per launch of a level-0 family."""
+    ms, nbytes = c_double(0.0), c_double(0.0)
+    stream = c_void_p(__import__("torch").cuda.current_stream().cuda_stream)
+    call("efsi_fv_kernel_replay", plan, KERNEL_FAMILIES[family], int(reps), ctypes.byref(ms), ctypes.byref(nbytes), stream)
+    return float(ms.value), float(nbytes.value)
 
 
 def kernel_timing_enable(family: str, enable: bool = True) -> None:

@@ -182,9 +182,18 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double* partials, unsi
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
-    double s = 0.0;
-    for (unsigned b = tid; b < nb; b += nt) s += ((volatile double*)partials)[(size_t)q * nb + b];
-    acc[q] = s;
+    // four independent L2 loads in flight per thread; fixed summation order
+    const double* part = partials + (size_t)q * nb;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    unsigned b = tid;
+    for (; b + 3 * nt < nb; b += 4 * nt) {
+      s0 += __ldcg(part + b);
+      s1 += __ldcg(part + b + nt);
+      s2 += __ldcg(part + b + 2 * nt);
+      s3 += __ldcg(part + b + 3 * nt);
+    }
+    for (; b < nb; b += nt) s0 += __ldcg(part + b);
+    acc[q] = (s0 + s1) + (s2 + s3);
   }
   block_sum<NV>(acc);
   if (tid == 0) {

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -285,6 +286,575 @@ __global__ void __launch_bounds__(256) k_prolong(LevelDev L, TP* __restrict__ p,
   if (!active) return;
   const unsigned m = __ldg(L.mask + c);
   if (m & M_FLUID) p[c] = (TP)fused_iterate(p, pr, c, i, j, k, true);
+}
+
+// ---------------------------------------------------------------------------
+// Tiled level kernels.  A block of 32 (k) x 8 (j) threads walks tiles of
+// 32 x 8 x kCI cells (grid-stride over tiles, about four resident blocks per
+// SM); each thread marches kCI consecutive cells along i.  All stencil inputs
+// of the kCI cells -- the i-column from i0-1 to i0+kCI and the four lateral
+// neighbours of every cell -- are loaded before any arithmetic, which keeps
+// ~25 independent loads per thread in flight.  Reductions keep one partial per
+// block, so the last-block finisher handles a few hundred partials.
+// ---------------------------------------------------------------------------
+constexpr int kTK = 32, kTJ = 8, kCI = 4;
+
+__host__ __device__ __forceinline__ int tiles_of(int nx, int ny, int nz) {
+  return ((nz + kTK - 1) / kTK) * ((ny + kTJ - 1) / kTJ) * ((nx + kCI - 1) / kCI);
+}
+
+__device__ __forceinline__ bool tile_coords(const LevelDev& L, int tile, int& i0, int& j, int& k) {
+  const int ntk = (L.nz + kTK - 1) / kTK, ntj = (L.ny + kTJ - 1) / kTJ;
+  const int tk = tile % ntk, rest = tile / ntk;
+  const int tj = rest % ntj, ti = rest / ntj;
+  k = tk * kTK + (int)threadIdx.x;
+  j = tj * kTJ + (int)threadIdx.y;
+  i0 = ti * kCI;
+  return j < L.ny && k < L.nz;
+}
+
+// Neighbour sum / denominator from pre-loaded neighbour values (same order
+// and arithmetic as `stencil`).
+__device__ __forceinline__ void stencil_vals(const LevelDev& L, int i, int j, int k, int64_t c, unsigned m, int outlet,
+                                             double vxm, double vxp, double vym, double vyp, double vzm, double vzp,
+                                             double& ns, double& den) {
+  double kxm = __ldg(L.cxm + i), kxp = __ldg(L.cxp + i);
+  double kym = __ldg(L.cym + j), kyp = __ldg(L.cyp + j);
+  double kzm = __ldg(L.czm + k), kzp = __ldg(L.czp + k);
+  if (L.fw != nullptr) {
+    const int64_t sx = (int64_t)L.ny * L.nz, sy = L.nz;
+    const double fc = (double)__ldg(L.fw + c);
+    kxm *= fc;
+    kxp *= (double)__ldg(L.fw + (i < L.nx - 1 ? c + sx : c));
+    kym *= fc;
+    kyp *= (double)__ldg(L.fw + (j < L.ny - 1 ? c + sy : c));
+    kzm *= fc;
+    kzp *= (double)__ldg(L.fw + (k < L.nz - 1 ? c + 1 : c));
+  }
+  ns = 0.0;
+  den = 0.0;
+  if (m & M_XM) {
+    ns += kxm * vxm;
+    den += kxm;
+  }
+  if (m & M_XP) {
+    ns += kxp * vxp;
+    den += kxp;
+  }
+  if (m & M_YM) {
+    ns += kym * vym;
+    den += kym;
+  }
+  if (m & M_YP) {
+    ns += kyp * vyp;
+    den += kyp;
+  }
+  if (m & M_ZM) {
+    ns += kzm * vzm;
+    den += kzm;
+  }
+  if (m & M_ZP) {
+    ns += kzp * vzp;
+    den += kzp;
+  }
+  if (outlet && k == 0) den += L.oz;
+}
+
+// Loads the i-column (i0-1 .. i0+kCI) and the lateral neighbours of the kCI
+// cells through `val(cell, i, j, k)`; out-of-domain positions read an
+// in-domain cell (their faces are closed, the value is never used).
+template <class VAL>
+__device__ __forceinline__ void load_column(const LevelDev& L, const VAL& val, int i0, int j, int k,
+                                            double (&col)[kCI + 2], double (&lat)[kCI][4]) {
+  const int64_t sx = (int64_t)L.ny * L.nz, sy = L.nz;
+  const int64_t base = (int64_t)j * L.nz + k;
+  const int nx1 = L.nx - 1;
+  const bool hym = j > 0, hyp = j < L.ny - 1, hzm = k > 0, hzp = k < L.nz - 1;
+#pragma unroll
+  for (int q = 0; q < kCI + 2; ++q) {
+    const int ii = min(max(i0 - 1 + q, 0), nx1);
+    col[q] = val(ii * sx + base, ii, j, k);
+  }
+#pragma unroll
+  for (int q = 0; q < kCI; ++q) {
+    const int ii = min(i0 + q, nx1);
+    const int64_t c = ii * sx + base;
+    lat[q][0] = val(hym ? c - sy : c, ii, hym ? j - 1 : j, k);
+    lat[q][1] = val(hyp ? c + sy : c, ii, hyp ? j + 1 : j, k);
+    lat[q][2] = val(hzm ? c - 1 : c, ii, j, hzm ? k - 1 : k);
+    lat[q][3] = val(hzp ? c + 1 : c, ii, j, hzp ? k + 1 : k);
+  }
+}
+
+// Tiled damped-Jacobi sweep (see k_sweep).
+template <typename TP, bool kNegR, bool kZero>
+__global__ void __launch_bounds__(256) kt_sweep(LevelDev L, const TP* __restrict__ p, const void* rhs,
+                                                TP* __restrict__ out, int outlet, double omega, ProlongSrc pr,
+                                                double* partials, CgScalars* sc) {
+  const int nt = tiles_of(L.nx, L.ny, L.nz);
+  const int64_t sx = (int64_t)L.ny * L.nz;
+  double zsum = 0.0;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    int i0, j, k;
+    if (!tile_coords(L, tile, i0, j, k)) continue;
+    const int64_t base = (int64_t)j * L.nz + k;
+    unsigned msk[kCI];
+    double rv[kCI];
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      const int64_t c = (int64_t)min(i0 + q, L.nx - 1) * sx + base;
+      msk[q] = __ldg(L.mask + c);
+      rv[q] = rhs_at<TP, kNegR>(rhs, c, msk[q]);
+    }
+    double col[kCI + 2], lat[kCI][4];
+    if (!kZero) {
+      auto val = [&](int64_t cell, int ii, int jj, int kk) { return fused_iterate(p, pr, cell, ii, jj, kk, true); };
+      load_column(L, val, i0, j, k, col, lat);
+    } else {
+#pragma unroll
+      for (int q = 0; q < kCI + 2; ++q) col[q] = 0.0;
+#pragma unroll
+      for (int q = 0; q < kCI; ++q) lat[q][0] = lat[q][1] = lat[q][2] = lat[q][3] = 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      const int i = i0 + q;
+      if (i >= L.nx) break;
+      const int64_t c = (int64_t)i * sx + base;
+      const unsigned m = msk[q];
+      if (m & M_SOLID) {
+        out[c] = (TP)0;
+        continue;
+      }
+      double ns, den;
+      stencil_vals(L, i, j, k, c, m, outlet, col[q], col[q + 2], lat[q][0], lat[q][1], lat[q][2], lat[q][3], ns, den);
+      den += iface_at<TP>(L, c);
+      TP res;
+      if (den <= 0.0) {
+        res = (TP)0;
+      } else {
+        const double jv = (ns - rv[q]) / den;
+        double pc = 0.0;
+        if (!kZero) pc = (m & M_FLUID) || pr.pc == nullptr ? col[q + 1] : (double)__ldg(p + c);
+        res = (TP)(pc + omega * (jv - pc));
+      }
+      out[c] = res;
+      if (partials != nullptr && (m & M_FLUID)) zsum += (double)res * vol64(L, i, j, k);
+    }
+  }
+  if (partials != nullptr) {
+    double v[1] = {zsum}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_z = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->zproj = 1;
+      }
+    }
+  }
+}
+
+// Tiled d_new = z' (+ beta d_old), Ad = A d_new, <d, Ad>_V and alpha (see k_spmv_dir).
+template <bool kCopy>
+__global__ void __launch_bounds__(256) kt_spmv_dir(LevelDev L, const double* __restrict__ z,
+                                                   const double* __restrict__ d_old, double* __restrict__ d_new,
+                                                   double* __restrict__ Ad, int outlet, double* partials,
+                                                   CgScalars* sc) {
+  const int nt = tiles_of(L.nx, L.ny, L.nz);
+  const int64_t sx = (int64_t)L.ny * L.nz;
+  const double beta = kCopy ? 0.0 : sc->beta;
+  const int zproj = sc->zproj;
+  const double mz = sc->mean_z;
+  double part = 0.0;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    int i0, j, k;
+    if (!tile_coords(L, tile, i0, j, k)) continue;
+    const int64_t base = (int64_t)j * L.nz + k;
+    unsigned msk[kCI];
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) msk[q] = __ldg(L.mask + (int64_t)min(i0 + q, L.nx - 1) * sx + base);
+    // Neighbours in the stencil are open (obstacle == 0, hence fluid).
+    auto dval = [&](int64_t cell, int, int, int) {
+      double zz = __ldg(z + cell);
+      if (zproj) zz = zz - mz;
+      return kCopy ? zz : zz + beta * __ldg(d_old + cell);
+    };
+    double col[kCI + 2], lat[kCI][4];
+    load_column(L, dval, i0, j, k, col, lat);
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      const int i = i0 + q;
+      if (i >= L.nx) break;
+      const int64_t c = (int64_t)i * sx + base;
+      const unsigned m = msk[q];
+      double dc;
+      if (m & M_SOLID) {
+        dc = 0.0;
+      } else if (!(m & M_FLUID) && zproj) {
+        dc = kCopy ? 0.0 : 0.0 + beta * __ldg(d_old + c);  // z' = 0 off the fluid set
+      } else {
+        dc = col[q + 1];
+      }
+      d_new[c] = dc;
+      double o;
+      if (m & M_SOLID) {
+        o = 0.0;
+      } else {
+        double ns, den;
+        stencil_vals(L, i, j, k, c, m, outlet, col[q], col[q + 2], lat[q][0], lat[q][1], lat[q][2], lat[q][3], ns,
+                     den);
+        o = (den + iface_at<double>(L, c)) * dc - ns;
+      }
+      Ad[c] = o;
+      if (m & M_FLUID) part += dc * o * vol64(L, i, j, k);
+    }
+  }
+  double v[1] = {part}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      const double dAd = t[0];
+      sc->dAd = dAd;
+      sc->alpha = 0.0;
+      if (dAd <= 0.0) {
+        if (sc->code == 0) sc->code_dAd = dAd;
+        sc->code = 1;
+      } else {
+        sc->alpha = sc->rz / dAd;
+      }
+    }
+  }
+}
+
+// Tiled CG update (see k_cg_update).
+template <bool kDelta>
+__global__ void __launch_bounds__(256) kt_cg_update(LevelDev L, double* __restrict__ x, const double* __restrict__ d,
+                                                    double* __restrict__ r, const double* __restrict__ Ad,
+                                                    double* __restrict__ delta, int want_means, int want_rr,
+                                                    double* partials, CgScalars* sc) {
+  const int nt = tiles_of(L.nx, L.ny, L.nz);
+  const int64_t sx = (int64_t)L.ny * L.nz;
+  const double alpha = sc->alpha;
+  double px = 0.0, pr = 0.0, prr = 0.0;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    int i0, j, k;
+    if (!tile_coords(L, tile, i0, j, k)) continue;
+    const int64_t base = (int64_t)j * L.nz + k;
+    const int qn = min(kCI, L.nx - i0);
+    unsigned msk[kCI];
+    double xv[kCI], dv[kCI], rv[kCI], av[kCI];
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      if (q >= qn) break;
+      const int64_t c = (int64_t)(i0 + q) * sx + base;
+      msk[q] = __ldg(L.mask + c);
+      xv[q] = x[c];
+      dv[q] = __ldg(d + c);
+      rv[q] = r[c];
+      av[q] = __ldg(Ad + c);
+    }
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      if (q >= qn) break;
+      const int i = i0 + q;
+      const int64_t c = (int64_t)i * sx + base;
+      if (msk[q] & M_SOLID) {
+        x[c] = 0.0;
+        r[c] = 0.0;
+        if (kDelta) delta[c] = 0.0;
+      } else {
+        const double xn = xv[q] + alpha * dv[q];
+        const double rn = rv[q] - alpha * av[q];
+        x[c] = xn;
+        r[c] = rn;
+        if (kDelta) delta[c] = 1.0 * rn + -1.0 * rv[q];
+        if (msk[q] & M_FLUID) {
+          const double V = vol64(L, i, j, k);
+          px += xn * V;
+          pr += rn * V;
+          prr += rn * rn * V;
+        }
+      }
+    }
+  }
+  if (want_means) {
+    double v[2] = {px, pr}, t[2];
+    if (grid_sum<2>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_x = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->mean_r = sc->free_vol > 0.0 ? 1.0 * t[1] / sc->free_vol : 0.0;
+      }
+    }
+  } else if (want_rr) {
+    double v[1] = {prr}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) sc->rr = t[0];
+    }
+  }
+}
+
+// Tiled rz_new / beta numerator / beta (see k_cg_dots).
+template <bool kMG, bool kRestart>
+__global__ void __launch_bounds__(256) kt_cg_dots(LevelDev L, const double* __restrict__ r,
+                                                  const double* __restrict__ z, const double* __restrict__ delta,
+                                                  double* partials, CgScalars* sc) {
+  const int nt = tiles_of(L.nx, L.ny, L.nz);
+  const int64_t sx = (int64_t)L.ny * L.nz;
+  CgScalars s;
+  s.mean_z = sc->mean_z;
+  const int zproj = sc->zproj;
+  double a = 0.0, b = 0.0;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    int i0, j, k;
+    if (!tile_coords(L, tile, i0, j, k)) continue;
+    const int64_t base = (int64_t)j * L.nz + k;
+    const int qn = min(kCI, L.nx - i0);
+    unsigned msk[kCI];
+    double rv[kCI], zv[kCI], dv[kCI];
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      if (q >= qn) break;
+      const int64_t c = (int64_t)(i0 + q) * sx + base;
+      msk[q] = __ldg(L.mask + c);
+      rv[q] = __ldg(r + c);
+      zv[q] = __ldg(z + c);
+      dv[q] = (kMG && !kRestart) ? __ldg(delta + c) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      if (q >= qn) break;
+      if (!(msk[q] & M_FLUID)) continue;
+      const double V = vol64(L, i0 + q, j, k);
+      const double zz = zproj ? zv[q] - s.mean_z : zv[q];
+      a += rv[q] * zz * V;
+      if (kMG && !kRestart) b += zz * dv[q] * V;
+    }
+  }
+  double v[2] = {a, b}, t[2];
+  if (grid_sum<2>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      if (kRestart) {
+        sc->rz = t[0];
+      } else {
+        const double rz = sc->rz, rz_new = t[0];
+        sc->rz_new = rz_new;
+        sc->beta_num = t[1];
+        double beta = 0.0;
+        if (rz <= 1.0e-300 || rz_new <= 0.0) {
+          sc->code = 2;
+        } else if (kMG) {
+          beta = t[1] / rz;
+          if (beta < 0.0) beta = 0.0;
+        } else {
+          beta = rz_new / rz;
+        }
+        sc->beta = beta;
+        sc->rz = rz_new;
+      }
+    }
+  }
+}
+
+// Tiled x -= mean_x, r -= mean_r and <r, r>_V (see k_sub_mean_xr).
+__global__ void __launch_bounds__(256) kt_sub_mean_xr(LevelDev L, double* __restrict__ x, double* __restrict__ r,
+                                                      double* partials, CgScalars* sc) {
+  const int nt = tiles_of(L.nx, L.ny, L.nz);
+  const int64_t sx = (int64_t)L.ny * L.nz;
+  const double mx = sc->mean_x, mr = sc->mean_r;
+  double prr = 0.0;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    int i0, j, k;
+    if (!tile_coords(L, tile, i0, j, k)) continue;
+    const int64_t base = (int64_t)j * L.nz + k;
+    const int qn = min(kCI, L.nx - i0);
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      if (q >= qn) break;
+      const int64_t c = (int64_t)(i0 + q) * sx + base;
+      if (__ldg(L.mask + c) & M_FLUID) {
+        x[c] = x[c] - mx;
+        const double rn = r[c] - mr;
+        r[c] = rn;
+        prr += rn * rn * vol64(L, i0 + q, j, k);
+      } else {
+        x[c] = 0.0;
+        r[c] = 0.0;
+      }
+    }
+  }
+  double v[1] = {prr}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) sc->rr = t[0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle tail: all coarse levels from `lt` down to the coarsest run inside one
+// CTA, iterates / rhs / masks in shared memory, with the same per-row
+// arithmetic as k_sweep / k_restrict (f32 storage, f64 row arithmetic).  One
+// launch replaces the per-level launches of the small levels.
+// ---------------------------------------------------------------------------
+constexpr int kTailMaxLevels = 12;
+constexpr int kTailThreads = 512;
+
+struct TailDesc {
+  int lt, nl;
+  int outlet, pre, coarse, post;
+  float scale;
+  double omega;
+  LevelDev L[kTailMaxLevels];
+  int foff[kTailMaxLevels];  // float offset of level l's block (pA, pB, rhs) in shared memory
+  int moff[kTailMaxLevels];  // byte offset of level l's mask copy
+  const float* rhs_in;       // rhs of level lt (written by the restriction from lt - 1)
+  float* p_out;              // final iterate of level lt
+};
+
+__device__ __forceinline__ void tail_ijk(const LevelDev& L, int t, int& i, int& j, int& k) {
+  k = t % L.nz;
+  const int ij = t / L.nz;
+  j = ij % L.ny;
+  i = ij / L.ny;
+}
+
+// One Jacobi sweep of level l: src -> dst (src null: zero initial guess),
+// optionally fusing the prolongation from the coarse iterate pc of level l+1.
+__device__ void tail_sweep(const TailDesc& T, int l, const float* src, float* dst, const float* rhs,
+                           const uint8_t* mask, const float* pc) {
+  const LevelDev& L = T.L[l];
+  const int n = L.nx * L.ny * L.nz;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    int i, j, k;
+    tail_ijk(L, t, i, j, k);
+    const unsigned m = mask[t];
+    if (m & M_SOLID) {
+      dst[t] = 0.0f;
+      continue;
+    }
+    auto it_at = [&](int cell, int ii, int jj, int kk, bool fluid) -> double {
+      if (src == nullptr) return 0.0;
+      float v = src[cell];
+      if (pc != nullptr && fluid) {
+        const LevelDev& C = T.L[l + 1];
+        const int ci = min(ii / 2, C.nx - 1), cj = min(jj / 2, C.ny - 1), ck = min(kk / 2, C.nz - 1);
+        v = __fadd_rn(v, __fmul_rn(T.scale, pc[(ci * C.ny + cj) * C.nz + ck]));
+      }
+      return (double)v;
+    };
+    auto val = [&](int64_t cell, int ii, int jj, int kk) { return it_at((int)cell, ii, jj, kk, true); };
+    double ns, den;
+    stencil(L, val, i, j, k, t, m, T.outlet, ns, den);
+    den += iface_at<float>(L, t);
+    float res;
+    if (den <= 0.0) {
+      res = 0.0f;
+    } else {
+      const double jv = (ns - (double)rhs[t]) / den;
+      const double pcur = it_at(t, i, j, k, (m & M_FLUID) != 0);
+      res = (float)(pcur + T.omega * (jv - pcur));
+    }
+    dst[t] = res;
+  }
+  __syncthreads();
+}
+
+// Residual of level l formed on the fly and volume-weighted into the rhs of l+1.
+__device__ void tail_restrict(const TailDesc& T, int l, const float* p, const float* rhs, const uint8_t* mask,
+                              float* crhs) {
+  const LevelDev& F = T.L[l];
+  const LevelDev& C = T.L[l + 1];
+  const int nc = C.nx * C.ny * C.nz;
+  for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+    int i, j, k;
+    tail_ijk(C, t, i, j, k);
+    float wres = 0.0f, free_vol = 0.0f;
+    int ocount = 0;
+    for (int oi = 0; oi < 2; ++oi)
+      for (int oj = 0; oj < 2; ++oj)
+        for (int ok = 0; ok < 2; ++ok) {
+          const int fi = 2 * i + oi, fj = 2 * j + oj, fk = 2 * k + ok;
+          if (fi < F.nx && fj < F.ny && fk < F.nz) {
+            const int f = (fi * F.ny + fj) * F.nz + fk;
+            const unsigned m = mask[f];
+            if (m & M_SOLID) {
+              ocount += 1;
+            } else {
+              const float vol = __fmul_rn(__fmul_rn(__ldg(F.wx + fi), __ldg(F.wy + fj)), __ldg(F.wz + fk));
+              double ns, den;
+              auto val = [&](int64_t cell, int, int, int) { return (double)p[cell]; };
+              stencil(F, val, fi, fj, fk, f, m, T.outlet, ns, den);
+              den += iface_at<float>(F, f);
+              const float r = (float)((double)rhs[f] - (ns - den * (double)p[f]));
+              wres = __fadd_rn(wres, __fmul_rn(r, vol));
+              free_vol = __fadd_rn(free_vol, vol);
+            }
+          }
+        }
+    crhs[t] = ocount > 0 ? 0.0f : __fdiv_rn(wres, fmaxf(free_vol, 1.0e-30f));
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  float* fpool = reinterpret_cast<float*>(tail_smem);
+  // masks and the rhs of level lt into shared memory
+  for (int l = T.lt; l < T.nl; ++l) {
+    const LevelDev& L = T.L[l];
+    const int n = L.nx * L.ny * L.nz;
+    uint8_t* ms = tail_smem + T.moff[l];
+    for (int t = threadIdx.x; t < n; t += blockDim.x) ms[t] = L.mask[t];
+  }
+  {
+    const LevelDev& L = T.L[T.lt];
+    const int n = L.nx * L.ny * L.nz;
+    float* rhs = fpool + T.foff[T.lt] + 2 * n;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) rhs[t] = T.rhs_in[t];
+  }
+  __syncthreads();
+  int cur[kTailMaxLevels];  // 0: pA holds the iterate, 1: pB
+  for (int l = T.lt; l < T.nl; ++l) {
+    const LevelDev& L = T.L[l];
+    const int n = L.nx * L.ny * L.nz;
+    float* pa = fpool + T.foff[l];
+    float* buf[2] = {pa, pa + n};
+    const float* rhs = pa + 2 * n;
+    const uint8_t* ms = tail_smem + T.moff[l];
+    const bool coarsest = (l == T.nl - 1);
+    const int sweeps = coarsest ? T.coarse : T.pre;
+    int c = -1;
+    for (int it = 0; it < sweeps; ++it) {
+      const int d = (it & 1);
+      tail_sweep(T, l, c < 0 ? nullptr : buf[c], buf[d], rhs, ms, nullptr);
+      c = d;
+    }
+    cur[l] = c;
+    if (!coarsest) {
+      const LevelDev& C = T.L[l + 1];
+      float* crhs = fpool + T.foff[l + 1] + 2 * (C.nx * C.ny * C.nz);
+      tail_restrict(T, l, buf[c], rhs, ms, crhs);
+    }
+  }
+  for (int l = T.nl - 2; l >= T.lt; --l) {
+    const LevelDev& L = T.L[l];
+    const int n = L.nx * L.ny * L.nz;
+    float* pa = fpool + T.foff[l];
+    float* buf[2] = {pa, pa + n};
+    const float* rhs = pa + 2 * n;
+    const uint8_t* ms = tail_smem + T.moff[l];
+    const LevelDev& C = T.L[l + 1];
+    const float* pc = fpool + T.foff[l + 1] + cur[l + 1] * (C.nx * C.ny * C.nz);
+    int c = cur[l];
+    for (int it = 0; it < T.post; ++it) {
+      const int d = 1 - c;
+      tail_sweep(T, l, buf[c], buf[d], rhs, ms, it == 0 ? pc : nullptr);
+      c = d;
+    }
+    cur[l] = c;
+  }
+  {
+    const LevelDev& L = T.L[T.lt];
+    const int n = L.nx * L.ny * L.nz;
+    const float* res = fpool + T.foff[T.lt] + cur[T.lt] * n;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) T.p_out[t] = res[t];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -669,7 +1239,20 @@ std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
 void set_error(const std::string& msg) { g_err = msg; }
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+thread_local unsigned long long g_capture_count = 0;
+extern thread_local bool g_capturing;
+void count_launch() {
+  if (g_capturing)
+    ++g_capture_count;  // a captured launch runs once per graph replay
+  else
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+void count_graph_launch(unsigned long long nodes) { g_launches.fetch_add(nodes, std::memory_order_relaxed); }
+unsigned long long take_capture_count() {
+  unsigned long long v = g_capture_count;
+  g_capture_count = 0;
+  return v;
+}
 
 namespace {
 struct FamilyTimer {
@@ -682,7 +1265,9 @@ FamilyTimer g_timers[KF_COUNT];
 std::mutex g_timer_mutex;
 }  // namespace
 
-bool timing_enabled(int family) { return family >= 0 && family < KF_COUNT && g_timers[family].on; }
+thread_local bool g_capturing = false;  // defined here, declared above
+void set_capturing(bool on) { g_capturing = on; }
+bool timing_enabled(int family) { return !g_capturing && family >= 0 && family < KF_COUNT && g_timers[family].on; }
 
 void timing_begin(int family, cudaStream_t s) {
   std::lock_guard<std::mutex> lock(g_timer_mutex);
@@ -740,6 +1325,78 @@ int level_zero_check(const efsi_fv_plan* P) {
   return EFSI_OK;
 }
 
+}  // namespace efsi
+
+namespace efsi {
+// Load every kernel of the solver into the context up front: with lazy module
+// loading a kernel's first launch would otherwise happen inside a stream
+// capture (16-iteration PCG blocks are captured into CUDA graphs).
+static void preload_kernels() {
+  cudaFuncAttributes a;
+  const void* fns[] = {
+      (const void*)k_sweep<double, true, true>,   (const void*)k_sweep<double, true, false>,
+      (const void*)k_sweep<double, false, false>, (const void*)k_sweep<float, false, true>,
+      (const void*)k_sweep<float, false, false>,  (const void*)k_restrict<double, true, true>,
+      (const void*)k_restrict<float, false, true>, (const void*)k_restrict<double, false, true>,
+      (const void*)k_spmv_dir<true>,              (const void*)k_spmv_dir<false>,
+      (const void*)k_cg_update<true>,             (const void*)k_cg_update<false>,
+      (const void*)k_cg_dots<true, false>,        (const void*)k_cg_dots<false, false>,
+      (const void*)k_cg_dots<false, true>,        (const void*)k_sub_mean_xr,
+      (const void*)k_jacobi_precond,              (const void*)k_set_zproj,
+      (const void*)k_true_residual,               (const void*)k_sub_mean_r,
+      (const void*)k_rhs_mean,                    (const void*)k_build_b,
+      (const void*)k_fv_diag,                     (const void*)k_reset_scalars,
+      (const void*)kt_sweep<double, true, true>,  (const void*)kt_sweep<double, true, false>,
+      (const void*)kt_sweep<float, false, true>,  (const void*)kt_sweep<float, false, false>,
+      (const void*)kt_spmv_dir<true>,             (const void*)kt_spmv_dir<false>,
+      (const void*)kt_cg_update<true>,            (const void*)kt_cg_update<false>,
+      (const void*)kt_cg_dots<true, false>,       (const void*)kt_cg_dots<false, false>,
+      (const void*)kt_sub_mean_xr,                (const void*)k_mg_tail,
+  };
+  for (const void* f : fns) cudaFuncGetAttributes(&a, f);
+  cudaGetLastError();
+}
+}  // namespace efsi
+
+
+namespace efsi {
+// Picks the first coarse level from which every level fits the tail kernel's
+// shared memory (13 bytes per cell) and has at most EFSI_TAIL_MAX_CELLS cells
+// (default 4096; 0 disables the tail).
+static void configure_tail(efsi_fv_plan* P) {
+  P->tail_level = P->n_levels;
+  int max_cells = 4096;
+  if (const char* env = std::getenv("EFSI_TAIL_MAX_CELLS")) max_cells = std::atoi(env);
+  if (max_cells <= 0 || P->n_levels < 2 || P->n_levels > kTailMaxLevels) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int smem_optin = 0;
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  for (int lt = 1; lt < P->n_levels; ++lt) {
+    if (P->lv[lt].n > max_cells) continue;
+    size_t floats = 0, bytes_mask = 0;
+    for (int l = lt; l < P->n_levels; ++l) {
+      floats += 3 * (size_t)P->lv[l].n;
+      bytes_mask += ((size_t)P->lv[l].n + 15) / 16 * 16;
+    }
+    const size_t total = floats * sizeof(float) + bytes_mask;
+    if ((int64_t)total > (int64_t)smem_optin) continue;
+    size_t fo = 0, mo = floats * sizeof(float);
+    for (int l = lt; l < P->n_levels; ++l) {
+      P->tail_foff[l] = (int)fo;
+      fo += 3 * (size_t)P->lv[l].n;
+      P->tail_moff[l] = (int)mo;
+      mo += ((size_t)P->lv[l].n + 15) / 16 * 16;
+    }
+    if (cudaFuncSetAttribute(k_mg_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    P->tail_level = lt;
+    P->tail_smem_bytes = total;
+    return;
+  }
+}
 }  // namespace efsi
 
 using namespace efsi;
@@ -806,6 +1463,16 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
     B.cdz = D.cdz;
     B.shape = shape3(B.nx, B.ny, B.nz);
     max_blocks = std::max<size_t>(max_blocks, B.shape.nblocks());
+    {
+      int dev = 0, nsm = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      int per_sm = 4;
+      if (const char* env = std::getenv("EFSI_TILED_BLOCKS_PER_SM")) per_sm = std::max(1, std::atoi(env));
+      const int nt = tiles_of(B.nx, B.ny, B.nz);
+      B.tiled = B.nz >= 16 && B.ny >= 8 && std::getenv("EFSI_NO_TILED") == nullptr;
+      B.tgrid = (unsigned)std::max(1, std::min(nt, nsm * per_sm));
+    }
     size_t ncoef = 2 * (size_t)(B.nx + B.ny + B.nz);
     if (cudaMalloc(&B.coef, ncoef * sizeof(double)) != cudaSuccess || cudaMalloc(&B.mask, B.n) != cudaSuccess) {
       set_error("cudaMalloc failed for level tables");
@@ -846,6 +1513,12 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
     set_error("cudaMalloc failed for reduction scratch");
     return fail(EFSI_ERR_CUDA);
   }
+  preload_kernels();
+  configure_tail(P);
+  if (cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cannot create the capture stream");
+    return fail(EFSI_ERR_CUDA);
+  }
   EFSI_COUNTED k_reset_scalars<<<1, 32>>>(P->sc);
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
@@ -858,6 +1531,9 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
 
 int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   if (P == nullptr) return EFSI_OK;
+  for (PcgGraph& g : P->graphs) cudaGraphExecDestroy(g.exec);
+  P->graphs.clear();
+  if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
   for (LevelBuf& B : P->lv) {
     cudaFree(B.coef);
     cudaFree(B.mask);
@@ -1059,6 +1735,21 @@ int efsi_mg_prolong(efsi_fv_plan* P, int32_t level, void* fine_p, const float* c
 
 namespace efsi {
 
+
+// One smoother sweep of level l (tiled kernel when the level is tiled).
+template <typename TP, bool kNegR, bool kZero>
+static void launch_sweep(efsi_fv_plan* P, int l, const TP* p, const void* rhs, TP* out, int outlet, double om,
+                         ProlongSrc pr, double* partials, cudaStream_t s) {
+  LevelDev L = level_dev(P, l);
+  const LevelBuf& B = P->lv[l];
+  if (B.tiled)
+    EFSI_COUNTED kt_sweep<TP, kNegR, kZero><<<B.tgrid, dim3(kTK, kTJ), 0, s>>>(L, p, rhs, out, outlet, om, pr, partials,
+                                                                              P->sc);
+  else
+    EFSI_COUNTED k_sweep<TP, kNegR, kZero><<<B.shape.grid, B.shape.block, 0, s>>>(L, p, rhs, out, outlet, om, pr,
+                                                                                   partials, P->sc);
+}
+
 // ---------------------------------------------------------------------------
 // V-cycle (fluid.py:6085-6262), zero initial guess, level-0 rhs = -r.
 // The result lands in z; when `want_mean` the last sweep also reduces the
@@ -1072,52 +1763,50 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
   const double om = (double)0.8f;
   const float scale = P->uniform ? 1.0f : 0.7f;
   const int nl = P->n_levels;
+  const double n0 = (double)P->lv[0].n;
   ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
   double* partials = want_mean ? P->partials : nullptr;
   if (nl <= 1) {
-    LevelDev L = level_dev(P, 0);
-    const Shape3& S = P->lv[0].shape;
-    int n = std::max(pre + post, coarse);
+    const int n = std::max(pre + post, coarse);
     double* bufs[2] = {(double*)P->lv[0].pa, (double*)P->lv[0].pb};
     const double* cur = nullptr;
     for (int it = 0; it < n; ++it) {
       double* dst = (it == n - 1) ? z : bufs[it & 1];
       double* part = (it == n - 1) ? partials : nullptr;
       if (it == 0)
-        EFSI_COUNTED k_sweep<double, true, true><<<S.grid, S.block, 0, s>>>(L, nullptr, r, dst, outlet, om, none, part, P->sc);
+        launch_sweep<double, true, true>(P, 0, nullptr, r, dst, outlet, om, none, part, s);
       else
-        EFSI_COUNTED k_sweep<double, true, false><<<S.grid, S.block, 0, s>>>(L, cur, r, dst, outlet, om, none, part, P->sc);
+        launch_sweep<double, true, false>(P, 0, cur, r, dst, outlet, om, none, part, s);
       cur = dst;
     }
     EFSI_LAUNCH_CHECK();
     return EFSI_OK;
   }
-  // Down: level iterate after pre-smoothing lives in cur[l].
+  // Down: the iterate after pre-smoothing of level l lives in cur[l].  Levels
+  // from P->tail_level on run inside k_mg_tail.
+  const int lt = P->tail_level;
   std::vector<const void*> cur(nl, nullptr);
-  for (int l = 0; l < nl - 1; ++l) {
+  const int down_end = (lt < nl) ? lt : nl - 1;
+  for (int l = 0; l < down_end; ++l) {
     LevelDev L = level_dev(P, l);
     LevelBuf& B = P->lv[l];
-    const Shape3& S = B.shape;
     void* bufs[2] = {B.pa, B.pb};
     const void* c = nullptr;
     for (int it = 0; it < pre; ++it) {
       void* dst = bufs[it & 1];
       if (l == 0) {
         if (it == 0)
-          EFSI_TIMED(KF_SWEEP_L0, 17.0 * B.n, s,
-                     EFSI_COUNTED k_sweep<double, true, true><<<S.grid, S.block, 0, s>>>(L, nullptr, r, (double*)dst,
-                                                                                         outlet, om, none, nullptr, P->sc));
+          EFSI_TIMED(KF_SWEEP_L0, 17.0 * n0, s,
+                     (launch_sweep<double, true, true>(P, 0, nullptr, r, (double*)dst, outlet, om, none, nullptr, s)));
         else
-          EFSI_TIMED(KF_SWEEP_L0, 25.0 * B.n, s,
-                     EFSI_COUNTED k_sweep<double, true, false><<<S.grid, S.block, 0, s>>>(
-                         L, (const double*)c, r, (double*)dst, outlet, om, none, nullptr, P->sc));
+          EFSI_TIMED(KF_SWEEP_L0, 25.0 * n0, s,
+                     (launch_sweep<double, true, false>(P, 0, (const double*)c, r, (double*)dst, outlet, om, none,
+                                                        nullptr, s)));
       } else {
         if (it == 0)
-          EFSI_COUNTED k_sweep<float, false, true><<<S.grid, S.block, 0, s>>>(L, nullptr, B.rhs, (float*)dst, outlet, om, none,
-                                                                 nullptr, P->sc);
+          launch_sweep<float, false, true>(P, l, nullptr, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
         else
-          EFSI_COUNTED k_sweep<float, false, false><<<S.grid, S.block, 0, s>>>(L, (const float*)c, B.rhs, (float*)dst, outlet, om,
-                                                                  none, nullptr, P->sc);
+          launch_sweep<float, false, false>(P, l, (const float*)c, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
       }
       c = dst;
     }
@@ -1128,38 +1817,52 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
                  EFSI_COUNTED k_restrict<double, true, true><<<C.shape.grid, C.shape.block, 0, s>>>(
                      L, (const double*)c, r, outlet, C.nx, C.ny, C.nz, C.rhs));
     else
-      EFSI_COUNTED k_restrict<float, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, (const float*)c, B.rhs, outlet, C.nx,
-                                                                             C.ny, C.nz, C.rhs);
+      EFSI_COUNTED k_restrict<float, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, (const float*)c, B.rhs,
+                                                                                          outlet, C.nx, C.ny, C.nz,
+                                                                                          C.rhs);
   }
-  // Coarsest level: `coarse` sweeps from zero.
-  {
+  if (lt < nl) {
+    TailDesc T;
+    T.lt = lt;
+    T.nl = nl;
+    T.outlet = outlet;
+    T.pre = pre;
+    T.coarse = coarse;
+    T.post = post;
+    T.scale = scale;
+    T.omega = om;
+    for (int l = lt; l < nl; ++l) {
+      T.L[l] = level_dev(P, l);
+      T.foff[l] = P->tail_foff[l];
+      T.moff[l] = P->tail_moff[l];
+    }
+    T.rhs_in = P->lv[lt].rhs;
+    T.p_out = (float*)P->lv[lt].pa;
+    EFSI_COUNTED k_mg_tail<<<1, kTailThreads, P->tail_smem_bytes, s>>>(T);
+    cur[lt] = P->lv[lt].pa;
+  } else {
+    // Coarsest level: `coarse` sweeps from zero.
     const int l = nl - 1;
-    LevelDev L = level_dev(P, l);
     LevelBuf& B = P->lv[l];
-    const Shape3& S = B.shape;
     void* bufs[2] = {B.pa, B.pb};
     const void* c = nullptr;
     for (int it = 0; it < coarse; ++it) {
       void* dst = bufs[it & 1];
       if (it == 0)
-        EFSI_COUNTED k_sweep<float, false, true><<<S.grid, S.block, 0, s>>>(L, nullptr, B.rhs, (float*)dst, outlet, om, none,
-                                                               nullptr, P->sc);
+        launch_sweep<float, false, true>(P, l, nullptr, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
       else
-        EFSI_COUNTED k_sweep<float, false, false><<<S.grid, S.block, 0, s>>>(L, (const float*)c, B.rhs, (float*)dst, outlet, om,
-                                                                none, nullptr, P->sc);
+        launch_sweep<float, false, false>(P, l, (const float*)c, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
       c = dst;
     }
     cur[l] = c;
   }
   // Up: prolongation fused into the first post sweep.
-  for (int l = nl - 2; l >= 0; --l) {
-    LevelDev L = level_dev(P, l);
+  const int up_start = (lt < nl) ? lt - 1 : nl - 2;
+  for (int l = up_start; l >= 0; --l) {
     LevelBuf& B = P->lv[l];
     const LevelBuf& C = P->lv[l + 1];
-    const Shape3& S = B.shape;
     ProlongSrc pr{(const float*)cur[l + 1], C.nx, C.ny, C.nz, scale};
     const void* c = cur[l];
-    // the two ping-pong buffers of this level: the one not holding c first
     void* other = (c == B.pa) ? B.pb : B.pa;
     void* seq[2] = {other, const_cast<void*>(c)};
     for (int it = 0; it < post; ++it) {
@@ -1168,12 +1871,11 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       ProlongSrc p_use = (it == 0) ? pr : none;
       double* part = (l == 0 && last) ? partials : nullptr;
       if (l == 0)
-        EFSI_TIMED(KF_SWEEP_L0, 25.0 * B.n + (it == 0 ? 4.0 * C.n : 0.0), s,
-                   EFSI_COUNTED k_sweep<double, true, false><<<S.grid, S.block, 0, s>>>(
-                       L, (const double*)c, r, (double*)dst, outlet, om, p_use, part, P->sc));
+        EFSI_TIMED(KF_SWEEP_L0, 25.0 * n0 + (it == 0 ? 4.0 * C.n : 0.0), s,
+                   (launch_sweep<double, true, false>(P, 0, (const double*)c, r, (double*)dst, outlet, om, p_use, part,
+                                                      s)));
       else
-        EFSI_COUNTED k_sweep<float, false, false><<<S.grid, S.block, 0, s>>>(L, (const float*)c, B.rhs, (float*)dst, outlet, om,
-                                                                p_use, nullptr, P->sc);
+        launch_sweep<float, false, false>(P, l, (const float*)c, B.rhs, (float*)dst, outlet, om, p_use, nullptr, s);
       c = dst;
     }
     cur[l] = c;
@@ -1201,6 +1903,10 @@ namespace efsi {
 // the host reads them where the reference does (b_norm, the initial residual
 // and preconditioner dot, and every 16th iteration's residual).
 // ---------------------------------------------------------------------------
+void set_capturing(bool on);
+void count_graph_launch(unsigned long long nodes);
+unsigned long long take_capture_count();
+
 struct PcgRun {
   efsi_fv_plan* P;
   const efsi_pcg_params* prm;
@@ -1327,76 +2033,185 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   }
   R.copy_next = true;
   const int restart_interval = prm->iface_active ? 256 : 512;
-  int code = 0;
-  for (int it = 1; it <= max_iters; ++it) {
-    // SpMV + direction + alpha
-    if (R.copy_next)
-      EFSI_TIMED(KF_SPMV_DIR, 25.0 * n0, s, EFSI_COUNTED k_spmv_dir<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, R.d_cur, R.d_nxt, P->Ad, outlet, P->partials,
-                                                      P->sc));
+  const double n0d = (double)n0;
+  // --- launch pieces of one iteration -------------------------------------
+  const bool tiled0 = P->lv[0].tiled;
+  const unsigned tg0 = P->lv[0].tgrid;
+  const dim3 tblk(kTK, kTJ);
+  auto launch_spmv = [&](bool copy, double* d_old, double* d_new) {
+    if (tiled0) {
+      if (copy)
+        EFSI_TIMED(KF_SPMV_DIR, 25.0 * n0d, s,
+                   EFSI_COUNTED kt_spmv_dir<true><<<tg0, tblk, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                                                                       P->partials, P->sc));
+      else
+        EFSI_TIMED(KF_SPMV_DIR, 33.0 * n0d, s,
+                   EFSI_COUNTED kt_spmv_dir<false><<<tg0, tblk, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                                                                        P->partials, P->sc));
+      return;
+    }
+    if (copy)
+      EFSI_TIMED(KF_SPMV_DIR, 25.0 * n0d, s,
+                 EFSI_COUNTED k_spmv_dir<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                                                                              P->partials, P->sc));
     else
-      EFSI_TIMED(KF_SPMV_DIR, 33.0 * n0, s, EFSI_COUNTED k_spmv_dir<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, R.d_cur, R.d_nxt, P->Ad, outlet, P->partials,
-                                                       P->sc));
-    std::swap(R.d_cur, R.d_nxt);
-    R.copy_next = false;
-    const bool mean_now = remove_mean && (it % 16 == 0);
-    const bool check = (it % 16 == 0) || it == max_iters;
-    const int want_rr = (check && !mean_now) ? 1 : 0;
+      EFSI_TIMED(KF_SPMV_DIR, 33.0 * n0d, s,
+                 EFSI_COUNTED k_spmv_dir<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                                                                               P->partials, P->sc));
+  };
+  auto launch_update = [&](double* d, bool mean_now, bool want_rr) {
+    if (tiled0) {
+      if (R.use_mg)
+        EFSI_TIMED(KF_CG_UPDATE, 56.0 * n0d, s,
+                   EFSI_COUNTED kt_cg_update<true><<<tg0, tblk, 0, s>>>(R.L, pressure, d, P->r, P->Ad, P->delta,
+                                                                        mean_now ? 1 : 0, want_rr ? 1 : 0,
+                                                                        P->partials, P->sc));
+      else
+        EFSI_TIMED(KF_CG_UPDATE, 48.0 * n0d, s,
+                   EFSI_COUNTED kt_cg_update<false><<<tg0, tblk, 0, s>>>(R.L, pressure, d, P->r, P->Ad, nullptr,
+                                                                         mean_now ? 1 : 0, want_rr ? 1 : 0,
+                                                                         P->partials, P->sc));
+      if (mean_now) EFSI_COUNTED kt_sub_mean_xr<<<tg0, tblk, 0, s>>>(R.L, pressure, P->r, P->partials, P->sc);
+      return;
+    }
     if (R.use_mg)
-      EFSI_TIMED(KF_CG_UPDATE, 56.0 * n0, s, EFSI_COUNTED k_cg_update<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, R.d_cur, P->r, P->Ad, P->delta,
-                                                       mean_now ? 1 : 0, want_rr, P->partials, P->sc));
+      EFSI_TIMED(KF_CG_UPDATE, 56.0 * n0d, s,
+                 EFSI_COUNTED k_cg_update<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, d, P->r, P->Ad, P->delta,
+                                                                               mean_now ? 1 : 0, want_rr ? 1 : 0,
+                                                                               P->partials, P->sc));
     else
-      EFSI_TIMED(KF_CG_UPDATE, 48.0 * n0, s, EFSI_COUNTED k_cg_update<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, R.d_cur, P->r, P->Ad, nullptr,
-                                                        mean_now ? 1 : 0, want_rr, P->partials, P->sc));
-    if (mean_now) {
+      EFSI_TIMED(KF_CG_UPDATE, 48.0 * n0d, s,
+                 EFSI_COUNTED k_cg_update<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, d, P->r, P->Ad, nullptr,
+                                                                                mean_now ? 1 : 0, want_rr ? 1 : 0,
+                                                                                P->partials, P->sc));
+    if (mean_now)
       EFSI_COUNTED k_sub_mean_xr<<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, P->r, P->partials, P->sc);
-      st->mean_projection_count += 2;
+  };
+  auto launch_precond_dots = [&]() -> int {
+    EFSI_TRY(precondition(R));
+    if (tiled0) {
+      if (R.use_mg)
+        EFSI_TIMED(KF_CG_DOTS, 25.0 * n0d, s,
+                   EFSI_COUNTED kt_cg_dots<true, false><<<tg0, tblk, 0, s>>>(R.L, P->r, P->z, P->delta, P->partials,
+                                                                             P->sc));
+      else
+        EFSI_TIMED(KF_CG_DOTS, 17.0 * n0d, s,
+                   EFSI_COUNTED kt_cg_dots<false, false><<<tg0, tblk, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials,
+                                                                              P->sc));
+      return EFSI_OK;
+    }
+    if (R.use_mg)
+      EFSI_TIMED(KF_CG_DOTS, 25.0 * n0d, s,
+                 EFSI_COUNTED k_cg_dots<true, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, P->delta,
+                                                                                    P->partials, P->sc));
+    else
+      EFSI_TIMED(KF_CG_DOTS, 17.0 * n0d, s,
+                 EFSI_COUNTED k_cg_dots<false, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr,
+                                                                                     P->partials, P->sc));
+    return EFSI_OK;
+  };
+  // --- one 16-iteration block (iterations 16k+1 .. 16k+16), optionally as a
+  // CUDA graph.  `cont`: the block starts with the preconditioner and dots of
+  // the previous block's last iteration; otherwise it starts a new direction.
+  auto launch_block = [&](bool cont) -> int {
+    if (cont) EFSI_TRY(launch_precond_dots());
+    double* d[2] = {P->d0, P->d1};
+    for (int j = 0; j < 16; ++j) {
+      launch_spmv(!cont && j == 0, d[j & 1], d[(j + 1) & 1]);
+      const bool last = (j == 15);
+      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean);
+      if (!last) EFSI_TRY(launch_precond_dots());
     }
     EFSI_LAUNCH_CHECK();
+    return EFSI_OK;
+  };
+  auto run_block = [&](bool cont) -> int {
+    if (!prm->use_graphs || P->graphs_disabled) return launch_block(cont);
+    const PcgGraphKey key{cont, R.use_mg, remove_mean, outlet, R.pre, R.coarse, R.post, pressure};
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : P->graphs)
+      if (g.key == key) exec = g.exec;
+    if (exec == nullptr) {
+      // Capture on the plan's private stream (the caller's may be the legacy
+      // default stream, which cannot be captured); the graph runs on `s`.
+      cudaGraph_t graph = nullptr;
+      const cudaStream_t launch_stream = s;
+      s = P->cap_stream;
+      R.s = P->cap_stream;
+      set_capturing(true);
+      take_capture_count();
+      cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      int rc = e == cudaSuccess ? launch_block(cont) : EFSI_ERR_CUDA;
+      cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      set_capturing(false);
+      const unsigned long long nodes = take_capture_count();
+      s = launch_stream;
+      R.s = launch_stream;
+      cudaError_t e3 = cudaSuccess;
+      if (e == cudaSuccess && rc == EFSI_OK && e2 == cudaSuccess) e3 = cudaGraphInstantiate(&exec, graph, 0);
+      if (graph != nullptr) cudaGraphDestroy(graph);
+      if (e != cudaSuccess || rc != EFSI_OK || e2 != cudaSuccess || e3 != cudaSuccess) {
+        // Record why and run this block with direct launches instead.
+        P->graph_error = std::string("begin: ") + cudaGetErrorString(e) + "; block: " + std::to_string(rc) + " (" +
+                         g_err + "); end: " + cudaGetErrorString(e2) + "; instantiate: " + cudaGetErrorString(e3);
+        cudaGetLastError();
+        P->graphs_disabled = true;
+        return launch_block(cont);
+      }
+      P->graphs.push_back({key, exec, nodes});
+    }
+    unsigned long long nodes_now = 0;
+    for (auto& g : P->graphs)
+      if (g.exec == exec) nodes_now = g.nodes;
+    EFSI_CUDA_CHECK(cudaGraphLaunch(exec, s));
+    count_graph_launch(nodes_now);
+    return EFSI_OK;
+  };
+  bool pending = false;  // preconditioner + dots of the previous iteration not launched yet
+  int n_precond = 0;     // preconditioner applications inside the loop
+  int it = 1;
+  while (it <= max_iters) {
+    const bool block = ((it - 1) % 16 == 0) && (it + 15 <= max_iters) && (pending || R.copy_next);
+    if (block) {
+      // d0 holds the current direction at every block start (16 swaps per block)
+      EFSI_TRY(run_block(pending));
+      n_precond += 15;
+      it += 15;
+      pending = false;
+      R.copy_next = false;
+    } else {
+      if (pending) EFSI_TRY(launch_precond_dots());
+      pending = false;
+      double* d_old = ((it - 1) & 1) ? P->d1 : P->d0;
+      double* d_new = ((it - 1) & 1) ? P->d0 : P->d1;
+      launch_spmv(R.copy_next, d_old, d_new);
+      R.copy_next = false;
+      const bool mean_now = remove_mean && (it % 16 == 0);
+      const bool check_now = (it % 16 == 0) || it == max_iters;
+      launch_update(d_new, mean_now, check_now && !mean_now);
+      EFSI_LAUNCH_CHECK();
+    }
+    if (remove_mean && it % 16 == 0) st->mean_projection_count += 2;
     st->iterations = it;
-    if (check) {
-      EFSI_TRY(read_scalars(R));
-      st->host_residual_checks += 1;
-      r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
-      st->relative_residual = r_norm / b_norm;
-      if (st->relative_residual <= tol) {
-        st->converged = 1;
-        break;
-      }
-      code = P->host_sc->code;
-      if (code != 0) {
-        st->breakdown_dAd = P->host_sc->code_dAd;
-        if (it < max_iters) {
-          EFSI_TRY(true_residual());
-          r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
-          st->relative_residual = r_norm / b_norm;
-          if (st->relative_residual <= tol) {
-            st->converged = 1;
-            break;
-          }
-          EFSI_TRY(precondition(R));
-          if (remove_mean) st->mean_projection_count += 1;
-          EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
-          EFSI_LAUNCH_CHECK();
-          EFSI_TRY(read_scalars(R));
-          rz = P->host_sc->rz;
-          if (std::isfinite(rz) && rz > 0.0) {
-            // clear the device code (fluid.py:6728-6729)
-            CgScalars* hs = P->host_sc;
-            hs->code = 0;
-            hs->code_dAd = 0.0;
-            EFSI_CUDA_CHECK(cudaMemcpyAsync(&P->sc->code, &hs->code, sizeof(int), cudaMemcpyHostToDevice, s));
-            EFSI_CUDA_CHECK(
-                cudaMemcpyAsync(&P->sc->code_dAd, &hs->code_dAd, sizeof(double), cudaMemcpyHostToDevice, s));
-            EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
-            R.copy_next = true;
-            st->restart_count += 1;
-            continue;
-          }
-        }
-        st->breakdown_reason = 2;
-        break;
-      }
-      if (it < max_iters && restart_interval > 0 && it % restart_interval == 0) {
+    const bool check = (it % 16 == 0) || it == max_iters;
+    if (!check) {
+      pending = true;
+      ++n_precond;
+      ++it;
+      continue;
+    }
+    EFSI_TRY(read_scalars(R));
+    st->host_residual_checks += 1;
+    r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+    st->relative_residual = r_norm / b_norm;
+    if (st->relative_residual <= tol) {
+      st->converged = 1;
+      break;
+    }
+    const int code = P->host_sc->code;
+    if (code != 0) {
+      st->breakdown_dAd = P->host_sc->code_dAd;
+      if (it < max_iters) {
         EFSI_TRY(true_residual());
         r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
         st->relative_residual = r_norm / b_norm;
@@ -1410,24 +2225,56 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
         EFSI_LAUNCH_CHECK();
         EFSI_TRY(read_scalars(R));
         rz = P->host_sc->rz;
-        if (!std::isfinite(rz) || rz <= 0.0) {
-          st->breakdown_reason = 3;
-          break;
+        if (std::isfinite(rz) && rz > 0.0) {
+          // clear the device code (fluid.py:6728-6729)
+          CgScalars* hs = P->host_sc;
+          hs->code = 0;
+          hs->code_dAd = 0.0;
+          EFSI_CUDA_CHECK(cudaMemcpyAsync(&P->sc->code, &hs->code, sizeof(int), cudaMemcpyHostToDevice, s));
+          EFSI_CUDA_CHECK(cudaMemcpyAsync(&P->sc->code_dAd, &hs->code_dAd, sizeof(double), cudaMemcpyHostToDevice, s));
+          EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+          R.copy_next = true;
+          pending = false;
+          st->restart_count += 1;
+          ++it;
+          continue;
         }
-        R.copy_next = true;
-        st->restart_count += 1;
-        continue;
       }
+      st->breakdown_reason = 2;
+      break;
     }
-    EFSI_TRY(precondition(R));
-    if (remove_mean) st->mean_projection_count += 1;
-    if (R.use_mg)
-      EFSI_TIMED(KF_CG_DOTS, 25.0 * n0, s, EFSI_COUNTED k_cg_dots<true, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, P->delta, P->partials, P->sc));
-    else
-      EFSI_TIMED(KF_CG_DOTS, 17.0 * n0, s, EFSI_COUNTED k_cg_dots<false, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc));
-    EFSI_LAUNCH_CHECK();
+    if (it < max_iters && restart_interval > 0 && it % restart_interval == 0) {
+      EFSI_TRY(true_residual());
+      r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+      st->relative_residual = r_norm / b_norm;
+      if (st->relative_residual <= tol) {
+        st->converged = 1;
+        break;
+      }
+      EFSI_TRY(precondition(R));
+      if (remove_mean) st->mean_projection_count += 1;
+      EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+      EFSI_LAUNCH_CHECK();
+      EFSI_TRY(read_scalars(R));
+      rz = P->host_sc->rz;
+      if (!std::isfinite(rz) || rz <= 0.0) {
+        st->breakdown_reason = 3;
+        break;
+      }
+      R.copy_next = true;
+      pending = false;
+      st->restart_count += 1;
+      ++it;
+      continue;
+    }
+    pending = true;
+    ++n_precond;
+    ++it;
   }
+  // mean projections of z: one per preconditioner application
+  if (remove_mean) st->mean_projection_count += n_precond;
   EFSI_TRY(read_scalars(R));
+  st->used_graphs = (prm->use_graphs && !P->graphs_disabled) ? 1 : 0;
   st->breakdown_code = P->host_sc->code;
   if (st->breakdown_dAd == 0.0) st->breakdown_dAd = P->host_sc->code_dAd;
   return EFSI_OK;
@@ -1510,3 +2357,92 @@ int efsi_fv_jacobi_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, 
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Benchmark helper (no counterpart in the reference): launch one level-0
+// kernel family `reps` times back to back on the plan's own work buffers and
+// report the mean CUDA-event duration per launch and its algorithmic bytes.
+int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double* avg_ms, double* bytes_per_launch,
+                          void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(reps > 0 && avg_ms && bytes_per_launch, "invalid replay arguments");
+  cudaStream_t s = as_stream(stream);
+  LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  const double n0 = (double)P->lv[0].n;
+  ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+  const double om = (double)0.8f;
+  double bytes = 0.0;
+  auto one = [&]() -> int {
+    switch (family) {
+      case KF_SPMV_DIR:
+        bytes = 33.0 * n0;
+        if (P->lv[0].tiled)
+          EFSI_COUNTED kt_spmv_dir<false><<<P->lv[0].tgrid, dim3(kTK, kTJ), 0, s>>>(L, P->z, P->d0, P->d1, P->Ad, 0,
+                                                                                    P->partials, P->sc);
+        else
+          EFSI_COUNTED k_spmv_dir<false><<<S.grid, S.block, 0, s>>>(L, P->z, P->d0, P->d1, P->Ad, 0, P->partials,
+                                                                    P->sc);
+        break;
+      case KF_SWEEP_L0:
+        bytes = 25.0 * n0;
+        launch_sweep<double, true, false>(P, 0, (const double*)P->lv[0].pa, P->r, (double*)P->lv[0].pb, 0, om, none,
+                                          nullptr, s);
+        break;
+      case KF_CG_UPDATE:
+        bytes = 56.0 * n0;
+        if (P->lv[0].tiled)
+          EFSI_COUNTED kt_cg_update<true><<<P->lv[0].tgrid, dim3(kTK, kTJ), 0, s>>>(L, P->b, P->d0, P->diag, P->Ad,
+                                                                                    P->delta, 0, 0, P->partials,
+                                                                                    P->sc);
+        else
+          EFSI_COUNTED k_cg_update<true><<<S.grid, S.block, 0, s>>>(L, P->b, P->d0, P->diag, P->Ad, P->delta, 0, 0,
+                                                                    P->partials, P->sc);
+        break;
+      case KF_RESTRICT_L0: {
+        if (P->n_levels < 2) {
+          set_error("replay of the restriction needs two levels");
+          return EFSI_ERR_ARG;
+        }
+        const LevelBuf& C = P->lv[1];
+        bytes = 17.0 * n0 + 4.0 * (double)C.n;
+        EFSI_COUNTED k_restrict<double, true, true><<<C.shape.grid, C.shape.block, 0, s>>>(
+            L, (const double*)P->lv[0].pa, P->r, 0, C.nx, C.ny, C.nz, C.rhs);
+        break;
+      }
+      case KF_CG_DOTS:
+        bytes = 25.0 * n0;
+        if (P->lv[0].tiled)
+          EFSI_COUNTED kt_cg_dots<true, false><<<P->lv[0].tgrid, dim3(kTK, kTJ), 0, s>>>(L, P->r, P->z, P->delta,
+                                                                                         P->partials, P->sc);
+        else
+          EFSI_COUNTED k_cg_dots<true, false><<<S.grid, S.block, 0, s>>>(L, P->r, P->z, P->delta, P->partials, P->sc);
+        break;
+      default:
+        set_error("family not supported by the replay");
+        return EFSI_ERR_ARG;
+    }
+    return EFSI_OK;
+  };
+  EFSI_TRY(one());  // warm-up
+  cudaEvent_t a, b;
+  EFSI_CUDA_CHECK(cudaEventCreate(&a));
+  EFSI_CUDA_CHECK(cudaEventCreate(&b));
+  EFSI_CUDA_CHECK(cudaEventRecord(a, s));
+  for (int q = 0; q < reps; ++q) EFSI_TRY(one());
+  EFSI_CUDA_CHECK(cudaEventRecord(b, s));
+  EFSI_CUDA_CHECK(cudaEventSynchronize(b));
+  float ms = 0.0f;
+  EFSI_CUDA_CHECK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  EFSI_LAUNCH_CHECK();
+  *avg_ms = (double)ms / reps;
+  *bytes_per_launch = bytes;
+  return EFSI_OK;
+}
+
+}  // extern "C"
+
+extern "C" const char* efsi_fv_graph_error(efsi_fv_plan* P) { return P ? P->graph_error.c_str() : ""; }

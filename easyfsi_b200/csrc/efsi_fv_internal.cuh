@@ -2,6 +2,7 @@
 // easyfsi_b200 library (plan layout, per-level device view, mask bits).
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "efsi_common.cuh"
@@ -64,50 +65,63 @@ __device__ __forceinline__ double iface_at(const LevelDev& L, int64_t c) {
   return (double)__ldg(reinterpret_cast<const TP*>(L.iface) + c);
 }
 
-// fluid.py:4080-4221: neighbour sum and denominator of one row.  `val(cell)`
-// returns the (possibly on-the-fly) iterate at a neighbour.
+// fluid.py:4080-4221: neighbour sum and denominator of one row.  `val(cell,
+// i, j, k)` returns the (possibly on-the-fly) iterate at a neighbour.  All six
+// neighbour values, coefficients and face weights are loaded unconditionally
+// (a wall face reads the cell itself) so the loads do not wait for the mask;
+// the mask then selects the open faces in the reference's order x-, x+, y-,
+// y+, z-, z+.
 template <class V>
 __device__ __forceinline__ void stencil(const LevelDev& L, const V& val, int i, int j, int k, int64_t c, unsigned m,
                                         int outlet, double& ns, double& den) {
   const int64_t sx = (int64_t)L.ny * L.nz, sy = L.nz;
+  const bool hxm = i > 0, hxp = i < L.nx - 1, hym = j > 0, hyp = j < L.ny - 1, hzm = k > 0, hzp = k < L.nz - 1;
+  const int64_t cxm = hxm ? c - sx : c, cxp = hxp ? c + sx : c;
+  const int64_t cym = hym ? c - sy : c, cyp = hyp ? c + sy : c;
+  const int64_t czm = hzm ? c - 1 : c, czp = hzp ? c + 1 : c;
+  const double vxm = val(cxm, hxm ? i - 1 : i, j, k);
+  const double vxp = val(cxp, hxp ? i + 1 : i, j, k);
+  const double vym = val(cym, i, hym ? j - 1 : j, k);
+  const double vyp = val(cyp, i, hyp ? j + 1 : j, k);
+  const double vzm = val(czm, i, j, hzm ? k - 1 : k);
+  const double vzp = val(czp, i, j, hzp ? k + 1 : k);
+  double kxm = __ldg(L.cxm + i), kxp = __ldg(L.cxp + i);
+  double kym = __ldg(L.cym + j), kyp = __ldg(L.cyp + j);
+  double kzm = __ldg(L.czm + k), kzp = __ldg(L.czp + k);
+  if (L.fw != nullptr) {
+    const double fc = (double)__ldg(L.fw + c);
+    kxm *= fc;
+    kxp *= (double)__ldg(L.fw + cxp);
+    kym *= fc;
+    kyp *= (double)__ldg(L.fw + cyp);
+    kzm *= fc;
+    kzp *= (double)__ldg(L.fw + czp);
+  }
   ns = 0.0;
   den = 0.0;
-  const float* fw = L.fw;
   if (m & M_XM) {
-    double co = __ldg(L.cxm + i);
-    if (fw) co *= (double)__ldg(fw + c);
-    ns += co * val(c - sx, i - 1, j, k);
-    den += co;
+    ns += kxm * vxm;
+    den += kxm;
   }
   if (m & M_XP) {
-    double co = __ldg(L.cxp + i);
-    if (fw) co *= (double)__ldg(fw + c + sx);
-    ns += co * val(c + sx, i + 1, j, k);
-    den += co;
+    ns += kxp * vxp;
+    den += kxp;
   }
   if (m & M_YM) {
-    double co = __ldg(L.cym + j);
-    if (fw) co *= (double)__ldg(fw + c);
-    ns += co * val(c - sy, i, j - 1, k);
-    den += co;
+    ns += kym * vym;
+    den += kym;
   }
   if (m & M_YP) {
-    double co = __ldg(L.cyp + j);
-    if (fw) co *= (double)__ldg(fw + c + sy);
-    ns += co * val(c + sy, i, j + 1, k);
-    den += co;
+    ns += kyp * vyp;
+    den += kyp;
   }
   if (m & M_ZM) {
-    double co = __ldg(L.czm + k);
-    if (fw) co *= (double)__ldg(fw + c);
-    ns += co * val(c - 1, i, j, k - 1);
-    den += co;
+    ns += kzm * vzm;
+    den += kzm;
   }
   if (m & M_ZP) {
-    double co = __ldg(L.czp + k);
-    if (fw) co *= (double)__ldg(fw + c + 1);
-    ns += co * val(c + 1, i, j, k + 1);
-    den += co;
+    ns += kzp * vzp;
+    den += kzp;
   }
   if (outlet && k == 0) den += L.oz;
 }
@@ -137,9 +151,27 @@ struct LevelBuf {
   const float *cdx, *cdy, *cdz;
   double oz = 0.0;
   Shape3 shape;
+  bool tiled = false;  // the tiled 32 x 8 x 4 kernels run on this level
+  unsigned tgrid = 1;  // their grid-stride grid size
 };
 
 }  // namespace efsi
+
+struct PcgGraphKey {
+  bool cont, use_mg, remove_mean;
+  int outlet, pre, coarse, post;
+  const double* pressure;
+  bool operator==(const PcgGraphKey& o) const {
+    return cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
+           pre == o.pre && coarse == o.coarse && post == o.post && pressure == o.pressure;
+  }
+};
+
+struct PcgGraph {
+  PcgGraphKey key;
+  cudaGraphExec_t exec;
+  unsigned long long nodes;  // kernel launches per replay
+};
 
 struct efsi_fv_plan {
   int n_levels = 0;
@@ -157,6 +189,14 @@ struct efsi_fv_plan {
   bool has_iface = false;
   const double* iface0 = nullptr;  // caller's level-0 interface diagonal
   const int32_t* obstacle0 = nullptr;  // caller's level-0 obstacle (legacy Jacobi)
+  std::vector<PcgGraph> graphs;        // instantiated 16-iteration PCG blocks
+  cudaStream_t cap_stream = nullptr;   // private stream used for graph capture
+  bool graphs_disabled = false;        // a capture failed; blocks run as direct launches
+  int tail_level = 1 << 30;            // first level run by the single-CTA V-cycle tail
+  size_t tail_smem_bytes = 0;
+  int tail_foff[12] = {0};
+  int tail_moff[12] = {0};
+  std::string graph_error;
 };
 
 

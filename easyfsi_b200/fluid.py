@@ -768,6 +768,9 @@ class CartesianFluidSolver:
         self.last_cg_restart_policy = "periodic_exact_residual"
         self.last_cg_breakdown_dAd = float(stats.breakdown_dAd)
         self.last_cg_used_multigrid = bool(stats.used_mg)
+        self.last_cg_used_graphs = bool(stats.used_graphs)
+        if use_graphs and not stats.used_graphs:
+            self.last_cg_graph_error = _native.load().efsi_fv_graph_error(self._plan).decode(errors="replace")
         self._last_cg_breakdown_code = int(stats.breakdown_code)
         if stats.b_norm <= 1.0e-30:
             self.pressure_tmp.tensor.zero_()

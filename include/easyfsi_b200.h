@@ -31,6 +31,10 @@ extern "C" {
 #define EFSI_ERR_CUDA 2
 #define EFSI_ERR_STATE 3
 
+typedef struct efsi_fv_plan efsi_fv_plan;
+typedef struct efsi_mpm_plan efsi_mpm_plan;
+typedef struct efsi_bin_plan efsi_bin_plan;
+
 /* Last error message of the calling thread (never NULL). */
 const char* efsi_last_error(void);
 /* Library version string. */
@@ -45,6 +49,13 @@ uint64_t efsi_kernel_launch_count(void);
  * 6 predictor.  Enabling resets the family's record; reading synchronises. */
 int efsi_kernel_timing_enable(int32_t family, int32_t enable);
 int efsi_kernel_timing_read(int32_t family, int64_t* launches, double* total_ms, double* total_bytes);
+
+/* Benchmark helper (no counterpart in the reference): launch one level-0
+ * kernel family (0 SpMV+direction, 1 smoother sweep, 2 CG update, 3 residual +
+ * restriction, 4 CG dots) `reps` times back to back on the plan's work buffers;
+ * returns the mean CUDA-event time per launch and its algorithmic bytes. */
+int efsi_fv_kernel_replay(efsi_fv_plan* plan, int32_t family, int32_t reps, double* avg_ms,
+                          double* bytes_per_launch, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Fluid grid / multigrid hierarchy                                          */
@@ -62,8 +73,6 @@ typedef struct efsi_level_desc {
   const float* cdy;
   const float* cdz;
 } efsi_level_desc;
-
-typedef struct efsi_fv_plan efsi_fv_plan;
 
 /* Builds the per-level f64 face-coefficient tables and allocates the solver
  * work vectors for the hierarchy (replaces the field allocation of
@@ -147,6 +156,8 @@ typedef struct efsi_cg_stats {
   int32_t restart_count;
   int32_t mean_projection_count;
   int32_t used_mg;
+  int32_t used_graphs; /* the 16-iteration blocks ran as CUDA graphs */
+  int32_t reserved;
   double initial_relative_residual;
   double relative_residual;
   double breakdown_dAd;
@@ -158,6 +169,9 @@ typedef struct efsi_cg_stats {
  * efsi_mg_prepare_level0.  pressure is the warm start and the solution. */
 int efsi_fv_pcg_solve(efsi_fv_plan* plan, const double* rhs0, double* pressure, const efsi_pcg_params* params,
                       efsi_cg_stats* stats, void* stream);
+
+/* Why CUDA-graph capture was abandoned for this plan ("" when it was not). */
+const char* efsi_fv_graph_error(efsi_fv_plan* plan);
 
 /* fluid.py:5992-6083 _solve_pressure_poisson_fv_multigrid (standalone cycles). */
 int efsi_fv_multigrid_solve(efsi_fv_plan* plan, const double* rhs0, double* pressure, int32_t outlet,
@@ -224,8 +238,6 @@ int efsi_apply_body_force(efsi_fv_plan* plan, const float* grid_force_density, f
 /* Neo-Hookean MLS/APIC-MPM                                                  */
 /* ------------------------------------------------------------------------ */
 
-typedef struct efsi_mpm_plan efsi_mpm_plan;
-
 /* Scratch for particle binning on the MPM node grid (replaces nothing in the
  * reference, which scatters with per-particle global atomics). */
 int efsi_mpm_plan_create(int32_t particle_capacity, int32_t nx, int32_t ny, int32_t nz, efsi_mpm_plan** out);
@@ -283,8 +295,6 @@ int efsi_compute_marker_forces(int32_t marker_count, const double* t_gamma, cons
  * report_device: double[2] = cleared count, max |f| before. */
 int efsi_clear_external_forces(int32_t particle_count, float* external_force, double* report_device,
                                void* stream);
-
-typedef struct efsi_bin_plan efsi_bin_plan;
 
 /* Uniform binning of particles with bin edge = support radius over a box;
  * used by the spreading and feedback entry points below. */

@@ -188,3 +188,23 @@ def test_coupled_scene_matches_oracle():
     assert rel_l2(gpu.solid.x.to_numpy()[:n], ref.solid.x[:n]) <= 1e-5
     assert rel_l2(gpu.markers.x_gamma_m.to_numpy()[: ref.markers.count], ref.markers.x) <= 1e-5
     assert rel_l2(gpu.solid.external_force_n.to_numpy()[:n], ref.solid.fext[:n]) <= 1e-5
+
+
+def test_graph_blocks_match_direct_launches(case):
+    """The CUDA-graph 16-iteration blocks replay exactly the direct launches."""
+    grid, fl, ofl, rng = case
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    out = []
+    for graphs in (False, True, True):
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(
+            iterations=300, rhs_scale=1.0e6, pressure_outlet_zmin=False, tolerance=1e-9, preconditioner="fv_multigrid",
+            use_graphs=graphs,
+        )
+        out.append((fl.last_cg_iterations, fl.pressure.to_numpy()))
+        if graphs:
+            assert fl.last_cg_used_graphs, getattr(fl, "last_cg_graph_error", "")
+    assert out[0][0] == out[1][0] == out[2][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[1][1], out[2][1])
