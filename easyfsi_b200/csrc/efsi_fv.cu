@@ -27,6 +27,7 @@
 //   * every scalar reduction is a deterministic two-stage block reduction whose
 //     last block also evaluates alpha / beta / means (no extra launches).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -38,6 +39,7 @@
 #include <vector>
 
 #include "efsi_fv_internal.cuh"
+#include "efsi_march.cuh"
 
 namespace efsi {
 
@@ -148,11 +150,6 @@ __device__ __forceinline__ double rhs_at(const void* rhs, int64_t c, unsigned m)
   return (double)__ldg(reinterpret_cast<const TP*>(rhs) + c);
 }
 
-struct ProlongSrc {
-  const float* pc;  // coarse iterate, null when no prolongation is fused
-  int cnx, cny, cnz;
-  float scale;
-};
 
 template <typename TP>
 __device__ __forceinline__ double fused_iterate(const TP* __restrict__ p, const ProlongSrc& pr, int64_t cell, int ii,
@@ -1352,6 +1349,16 @@ static void preload_kernels() {
       (const void*)kt_cg_update<true>,            (const void*)kt_cg_update<false>,
       (const void*)kt_cg_dots<true, false>,       (const void*)kt_cg_dots<false, false>,
       (const void*)kt_sub_mean_xr,                (const void*)k_mg_tail,
+#define EFSI_MARCH_FNS(A)                                                                              \
+      (const void*)km_sweep<double, true, false, A>, (const void*)km_sweep<double, true, true, A>,         \
+      (const void*)km_sweep<double, false, false, A>, (const void*)km_sweep<float, false, false, A>,       \
+      (const void*)km_sweep<float, false, true, A>, (const void*)km_sweep0<double, true, A>,               \
+      (const void*)km_sweep0<double, false, A>, (const void*)km_sweep0<float, false, A>,                   \
+      (const void*)km_restrict<double, true, A>, (const void*)km_restrict<double, false, A>,               \
+      (const void*)km_restrict<float, false, A>, (const void*)km_spmv_dir<true, A>,                        \
+      (const void*)km_spmv_dir<false, A>
+      EFSI_MARCH_FNS(false), EFSI_MARCH_FNS(true),
+#undef EFSI_MARCH_FNS
   };
   for (const void* f : fns) cudaFuncGetAttributes(&a, f);
   cudaGetLastError();
@@ -1472,6 +1479,10 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
       const int nt = tiles_of(B.nx, B.ny, B.nz);
       B.tiled = B.nz >= 16 && B.ny >= 8 && std::getenv("EFSI_NO_TILED") == nullptr;
       B.tgrid = (unsigned)std::max(1, std::min(nt, nsm * per_sm));
+      const MarchCfg mc = march_cfg(B.nx, B.ny, B.nz, nsm * 4);
+      B.march = B.nz >= 16 && B.ny >= 8 && std::getenv("EFSI_NO_MARCH") == nullptr;
+      B.mchunk = mc.chunk;
+      B.mgrid = mc.grid;
     }
     size_t ncoef = 2 * (size_t)(B.nx + B.ny + B.nz);
     if (cudaMalloc(&B.coef, ncoef * sizeof(double)) != cudaSuccess || cudaMalloc(&B.mask, B.n) != cudaSuccess) {
@@ -1736,18 +1747,162 @@ int efsi_mg_prolong(efsi_fv_plan* P, int32_t level, void* fine_p, const float* c
 namespace efsi {
 
 
-// One smoother sweep of level l (tiled kernel when the level is tiled).
+// ---------------------------------------------------------------------------
+// TMA descriptors of level fields for the plane-marching kernels
+// ---------------------------------------------------------------------------
+enum : int { MAP_VALUE = 0, MAP_RHS = 1, MAP_MASK = 2 };
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// Descriptor of field `ptr` of level l (f64 at level 0, f32 on coarse levels;
+// the mask is u8): value tiles are (8 + 2) rows x (32 + 2 x 16 bytes) with
+// their origin 16 bytes left of and one row above the column tile, rhs and
+// mask tiles are 8 x 32 at the tile origin.  Null when the field cannot be
+// described (misaligned base or row pitch, or no encoder).
+static const CUtensorMap* plane_map(efsi_fv_plan* P, int l, const void* ptr, int kind) {
+  for (const PlaneMap& m : P->maps)
+    if (m.ptr == ptr && m.level == l && m.kind == kind) return &m.map;
+  auto enc = tensor_map_encoder();
+  if (enc == nullptr || ptr == nullptr || (reinterpret_cast<uintptr_t>(ptr) & 15u) != 0) return nullptr;
+  const LevelBuf& B = P->lv[l];
+  const int es = kind == MAP_MASK ? 1 : (l == 0 ? 8 : 4);
+  if (((size_t)B.nz * es) % 16 != 0) return nullptr;
+  const CUtensorMapDataType dt = kind == MAP_MASK ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                 : l == 0         ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[3] = {(cuuint64_t)B.nz, (cuuint64_t)B.ny, (cuuint64_t)B.nx};
+  const cuuint64_t strides[2] = {(cuuint64_t)B.nz * es, (cuuint64_t)B.nz * B.ny * es};
+  cuuint32_t box[3] = {(cuuint32_t)kMK, (cuuint32_t)kMJ, 1u};
+  if (kind == MAP_VALUE) {
+    box[0] = (cuuint32_t)(kMK + 2 * (16 / es));
+    box[1] = (cuuint32_t)(kMJ + 2);
+  }
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  PlaneMap pm;
+  pm.ptr = ptr;
+  pm.level = l;
+  pm.kind = kind;
+  if (enc(&pm.map, dt, 3, const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return nullptr;
+  P->maps.push_back(pm);
+  return &P->maps.back().map;
+}
+
+// d_new = z' (+ beta d_old), Ad = A d_new, <d, Ad>_V and alpha (marching
+// kernel); false when the fields cannot be streamed with TMA.
+static bool launch_march_spmv(efsi_fv_plan* P, const LevelDev& L, bool copy, const double* z, const double* d_old,
+                              double* d_new, double* Ad, int outlet, double* partials, CgScalars* sc,
+                              cudaStream_t s) {
+  const LevelBuf& B = P->lv[0];
+  const CUtensorMap* mz = plane_map(P, 0, z, MAP_VALUE);
+  const CUtensorMap* mm = plane_map(P, 0, B.mask, MAP_MASK);
+  const CUtensorMap* md = copy ? mz : plane_map(P, 0, d_old, MAP_VALUE);
+  if (!mz || !mm || !md) return false;
+  const dim3 blk(kMK, kMJ);
+  const bool aux = L.fw != nullptr || L.iface != nullptr;
+  const int sm1 = march_smem<double, 1, double, false>(), sm2 = march_smem<double, 2, double, false>();
+  if (copy && aux)
+    EFSI_COUNTED km_spmv_dir<true, true><<<B.mgrid, blk, sm1, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+                                                                    partials, sc);
+  else if (copy)
+    EFSI_COUNTED km_spmv_dir<true, false><<<B.mgrid, blk, sm1, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+                                                                     partials, sc);
+  else if (aux)
+    EFSI_COUNTED km_spmv_dir<false, true><<<B.mgrid, blk, sm2, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+                                                                     partials, sc);
+  else
+    EFSI_COUNTED km_spmv_dir<false, false><<<B.mgrid, blk, sm2, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+                                                                      partials, sc);
+  return true;
+}
+
+// One sweep with the marching kernels; false when the fields cannot be
+// streamed with TMA (the caller then runs the per-cell kernel).
+template <typename TP, bool kNegR, bool kZero, bool kAux>
+static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const TP* p, const void* rhs, TP* out,
+                               int outlet, double om, ProlongSrc pr, double* partials, cudaStream_t s) {
+  using TR = typename std::conditional<kNegR, double, TP>::type;
+  const LevelBuf& B = P->lv[l];
+  const dim3 blk(kMK, kMJ);
+  if (kZero) {
+    EFSI_COUNTED km_sweep0<TP, kNegR, kAux><<<B.mgrid, blk, 0, s>>>(L, B.mchunk, rhs, out, outlet, om, partials,
+                                                                     P->sc);
+    return true;
+  }
+  const CUtensorMap* mp = plane_map(P, l, p, MAP_VALUE);
+  const CUtensorMap* mr = plane_map(P, l, rhs, MAP_RHS);
+  const CUtensorMap* mm = plane_map(P, l, B.mask, MAP_MASK);
+  if (!mp || !mr || !mm) return false;
+  const int sm = march_smem<TP, 1, TR, true>();
+  if (pr.pc != nullptr)
+    EFSI_COUNTED km_sweep<TP, kNegR, true, kAux><<<B.mgrid, blk, sm, s>>>(L, B.mchunk, *mp, *mr, *mm, out, outlet, om,
+                                                                           pr, partials, P->sc);
+  else
+    EFSI_COUNTED km_sweep<TP, kNegR, false, kAux><<<B.mgrid, blk, sm, s>>>(L, B.mchunk, *mp, *mr, *mm, out, outlet,
+                                                                            om, pr, partials, P->sc);
+  return true;
+}
+
+// One smoother sweep of level l (plane-marching kernel when the level is
+// large enough, else the per-cell kernel).
 template <typename TP, bool kNegR, bool kZero>
 static void launch_sweep(efsi_fv_plan* P, int l, const TP* p, const void* rhs, TP* out, int outlet, double om,
                          ProlongSrc pr, double* partials, cudaStream_t s) {
   LevelDev L = level_dev(P, l);
   const LevelBuf& B = P->lv[l];
+  if (B.march) {
+    const bool done = (L.fw != nullptr || L.iface != nullptr)
+                          ? launch_march_sweep<TP, kNegR, kZero, true>(P, l, L, p, rhs, out, outlet, om, pr, partials, s)
+                          : launch_march_sweep<TP, kNegR, kZero, false>(P, l, L, p, rhs, out, outlet, om, pr, partials,
+                                                                         s);
+    if (done) return;
+  }
   if (B.tiled)
     EFSI_COUNTED kt_sweep<TP, kNegR, kZero><<<B.tgrid, dim3(kTK, kTJ), 0, s>>>(L, p, rhs, out, outlet, om, pr, partials,
                                                                               P->sc);
   else
     EFSI_COUNTED k_sweep<TP, kNegR, kZero><<<B.shape.grid, B.shape.block, 0, s>>>(L, p, rhs, out, outlet, om, pr,
                                                                                    partials, P->sc);
+}
+
+// Residual of level l's iterate p restricted into level l+1's rhs.
+template <typename TP, bool kNegR>
+static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs, int outlet, cudaStream_t s) {
+  LevelDev L = level_dev(P, l);
+  const LevelBuf& B = P->lv[l];
+  const LevelBuf& C = P->lv[l + 1];
+  if (B.march) {
+    using TR = typename std::conditional<kNegR, double, TP>::type;
+    const CUtensorMap* mp = plane_map(P, l, p, MAP_VALUE);
+    const CUtensorMap* mr = plane_map(P, l, rhs, MAP_RHS);
+    const CUtensorMap* mm = plane_map(P, l, B.mask, MAP_MASK);
+    if (mp && mr && mm) {
+      const int sm = march_smem<TP, 1, TR, true>();
+      if (L.fw != nullptr || L.iface != nullptr)
+        EFSI_COUNTED km_restrict<TP, kNegR, true><<<B.mgrid, dim3(kMK, kMJ), sm, s>>>(
+            L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
+      else
+        EFSI_COUNTED km_restrict<TP, kNegR, false><<<B.mgrid, dim3(kMK, kMJ), sm, s>>>(
+            L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
+      return;
+    }
+  }
+  EFSI_COUNTED k_restrict<TP, kNegR, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, p, rhs, outlet, C.nx, C.ny,
+                                                                                 C.nz, C.rhs);
 }
 
 // ---------------------------------------------------------------------------
@@ -1814,12 +1969,9 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     const LevelBuf& C = P->lv[l + 1];
     if (l == 0)
       EFSI_TIMED(KF_RESTRICT_L0, 17.0 * B.n + 4.0 * C.n, s,
-                 EFSI_COUNTED k_restrict<double, true, true><<<C.shape.grid, C.shape.block, 0, s>>>(
-                     L, (const double*)c, r, outlet, C.nx, C.ny, C.nz, C.rhs));
+                 (launch_restrict<double, true>(P, 0, (const double*)c, r, outlet, s)));
     else
-      EFSI_COUNTED k_restrict<float, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, (const float*)c, B.rhs,
-                                                                                          outlet, C.nx, C.ny, C.nz,
-                                                                                          C.rhs);
+      launch_restrict<float, false>(P, l, (const float*)c, B.rhs, outlet, s);
   }
   if (lt < nl) {
     TailDesc T;
@@ -2038,7 +2190,14 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   const bool tiled0 = P->lv[0].tiled;
   const unsigned tg0 = P->lv[0].tgrid;
   const dim3 tblk(kTK, kTJ);
+  const bool march0 = P->lv[0].march;
   auto launch_spmv = [&](bool copy, double* d_old, double* d_new) {
+    if (march0) {
+      bool done = false;
+      EFSI_TIMED(KF_SPMV_DIR, (copy ? 25.0 : 33.0) * n0d, s,
+                 done = launch_march_spmv(P, R.L, copy, P->z, d_old, d_new, P->Ad, outlet, P->partials, P->sc, s));
+      if (done) return;
+    }
     if (tiled0) {
       if (copy)
         EFSI_TIMED(KF_SPMV_DIR, 25.0 * n0d, s,
@@ -2288,13 +2447,11 @@ namespace efsi {
 // (fluid.py:5862-5900); used by the non-PCG pressure solvers.
 template <typename TP>
 static int smooth_copy(efsi_fv_plan* P, int l, TP* p, const void* rhs, int outlet, int iterations, cudaStream_t s) {
-  LevelDev L = level_dev(P, l);
   LevelBuf& B = P->lv[l];
   ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
   const double om = (double)0.8f;
   for (int it = 0; it < std::max(0, iterations); ++it) {
-    EFSI_COUNTED k_sweep<TP, false, false><<<B.shape.grid, B.shape.block, 0, s>>>(L, p, rhs, (TP*)B.pb, outlet, om, none, nullptr,
-                                                                     P->sc);
+    launch_sweep<TP, false, false>(P, l, p, rhs, (TP*)B.pb, outlet, om, none, nullptr, s);
     EFSI_CUDA_CHECK(cudaMemcpyAsync(p, B.pb, B.n * sizeof(TP), cudaMemcpyDeviceToDevice, s));
   }
   EFSI_LAUNCH_CHECK();
@@ -2320,12 +2477,10 @@ int efsi_fv_multigrid_solve(efsi_fv_plan* P, const double* rhs0, double* pressur
       const LevelBuf& C = P->lv[l + 1];
       if (l == 0) {
         EFSI_TRY(smooth_copy<double>(P, 0, pressure, rhs0, outlet, 3, s));
-        EFSI_COUNTED k_restrict<double, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, pressure, rhs0, outlet, C.nx, C.ny,
-                                                                                C.nz, C.rhs);
+        launch_restrict<double, false>(P, 0, pressure, rhs0, outlet, s);
       } else {
         EFSI_TRY(smooth_copy<float>(P, l, (float*)B.pa, B.rhs, outlet, 3, s));
-        EFSI_COUNTED k_restrict<float, false, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, (const float*)B.pa, B.rhs, outlet,
-                                                                               C.nx, C.ny, C.nz, C.rhs);
+        launch_restrict<float, false>(P, l, (const float*)B.pa, B.rhs, outlet, s);
       }
       // the restriction zeroes the coarse iterate (fluid.py:5383-5385)
       EFSI_CUDA_CHECK(cudaMemsetAsync(C.pa, 0, C.n * sizeof(float), s));
@@ -2378,6 +2533,8 @@ int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double*
     switch (family) {
       case KF_SPMV_DIR:
         bytes = 33.0 * n0;
+        if (P->lv[0].march && launch_march_spmv(P, L, false, P->z, P->d0, P->d1, P->Ad, 0, P->partials, P->sc, s))
+          break;
         if (P->lv[0].tiled)
           EFSI_COUNTED kt_spmv_dir<false><<<P->lv[0].tgrid, dim3(kTK, kTJ), 0, s>>>(L, P->z, P->d0, P->d1, P->Ad, 0,
                                                                                     P->partials, P->sc);
@@ -2407,8 +2564,7 @@ int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double*
         }
         const LevelBuf& C = P->lv[1];
         bytes = 17.0 * n0 + 4.0 * (double)C.n;
-        EFSI_COUNTED k_restrict<double, true, true><<<C.shape.grid, C.shape.block, 0, s>>>(
-            L, (const double*)P->lv[0].pa, P->r, 0, C.nx, C.ny, C.nz, C.rhs);
+        launch_restrict<double, true>(P, 0, (const double*)P->lv[0].pa, P->r, 0, s);
         break;
       }
       case KF_CG_DOTS:

@@ -2,8 +2,11 @@
 // easyfsi_b200 library (plan layout, per-level device view, mask bits).
 #pragma once
 
+#include <deque>
 #include <string>
 #include <vector>
+
+#include <cuda.h>
 
 #include "efsi_common.cuh"
 
@@ -49,6 +52,14 @@ struct CgScalars {
   int code;
   int zproj;  // 1: consumers of z apply the zero-mean projection on the fly
   unsigned ticket;
+  int fault;  // a plane-marching kernel's stage copy did not complete in time
+};
+
+// Coarse iterate whose prolongation p += scale * p_coarse is fused into a sweep.
+struct ProlongSrc {
+  const float* pc;  // coarse iterate, null when no prolongation is fused
+  int cnx, cny, cnz;
+  float scale;
 };
 
 __device__ __forceinline__ int64_t cidx(int i, int j, int k, int ny, int nz) {
@@ -153,6 +164,9 @@ struct LevelBuf {
   Shape3 shape;
   bool tiled = false;  // the tiled 32 x 8 x 4 kernels run on this level
   unsigned tgrid = 1;  // their grid-stride grid size
+  bool march = false;  // the plane-marching stencil kernels run on this level
+  int mchunk = 2;      // their planes per block
+  unsigned mgrid = 1;  // and grid size
 };
 
 }  // namespace efsi
@@ -171,6 +185,15 @@ struct PcgGraph {
   PcgGraphKey key;
   cudaGraphExec_t exec;
   unsigned long long nodes;  // kernel launches per replay
+};
+
+// A TMA descriptor of one level field, cached per plan (encoded on the host
+// at first use; the plane-marching kernels take it by value).
+struct PlaneMap {
+  const void* ptr;
+  int level;
+  int kind;  // 0: value tile with halo, 1: right-hand side tile, 2: mask tile
+  alignas(64) CUtensorMap map;
 };
 
 struct efsi_fv_plan {
@@ -197,6 +220,7 @@ struct efsi_fv_plan {
   int tail_foff[12] = {0};
   int tail_moff[12] = {0};
   std::string graph_error;
+  std::deque<PlaneMap> maps;  // deque: descriptors stay in place as the cache grows
 };
 
 

@@ -1,0 +1,638 @@
+// Plane-marching stencil kernels of the graded-grid pressure solver: damped
+// Jacobi sweeps of every level, the CG direction update + SpMV, and the
+// residual restriction.
+//
+// A block of 32 (k) x 8 (j) threads owns a 32 x 8 column tile of a level and
+// a chunk of planes [ib, ie) along i (the slowest-varying axis).  One elected
+// thread streams every plane the chunk needs (ib-1 .. ie) into a ring of
+// kStages shared-memory stages with TMA (cp.async.bulk.tensor, no multicast):
+// the swept field as a (8 + 2) x (32 + 2 pad) tile with its one-cell halo,
+// and the plane's right-hand side and stencil-mask tiles.  Each stage has an
+// mbarrier that completes when its bytes have landed.  The block computes
+// plane i from the stages of planes i-1, i and i+1 while the copies of planes
+// i+2 .. i+kStages-2 are in flight, then releases stage i-1 at the plane's
+// block barrier and the elected thread refills it.  HBM is read once per
+// value (halo rows come from L2); registers hold no prefetched data.
+//
+// The per-cell arithmetic is the same expression, in the same order, as the
+// per-cell kernels (`stencil`, `row_residual`): open faces are selected from
+// the stencil mask, closed faces contribute exact zeros.
+//
+// TMA rules honoured here: every copy starts at an x (k) coordinate that is a
+// multiple of 16 bytes (the value tile starts 16 bytes left of the tile, the
+// rhs / mask tiles at the tile edge, k0 a multiple of 32); rows outside the
+// level read the zero fill value and are only used behind closed faces;
+// destinations are 128-byte aligned.  The host only selects these kernels
+// for levels whose row pitch is a multiple of 16 bytes for every field.
+#pragma once
+
+#include <cuda.h>
+
+#include <type_traits>
+
+#include "efsi_fv_internal.cuh"
+
+namespace efsi {
+
+constexpr int kMK = 32, kMJ = 8;
+constexpr int kStages = 6;
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s: a stage that never lands is reported, not waited on forever
+
+// Launch configuration of the marching kernels of one level: `chunk` planes
+// (even, so a plane pair of the restriction never straddles two blocks) per
+// block, blocks = column tiles x ceil(nx / chunk).
+struct MarchCfg {
+  int chunk = 2;
+  unsigned grid = 1;
+};
+
+inline MarchCfg march_cfg(int nx, int ny, int nz, int slots) {
+  const int tiles = ((nz + kMK - 1) / kMK) * ((ny + kMJ - 1) / kMJ);
+  int nsplit = slots / tiles;
+  if (nsplit < 1) nsplit = 1;
+  int chunk = (nx + nsplit - 1) / nsplit;
+  if (chunk < 2) chunk = 2;
+  chunk += chunk & 1;
+  MarchCfg c;
+  c.chunk = chunk;
+  c.grid = (unsigned)(tiles * ((nx + chunk - 1) / chunk));
+  return c;
+}
+
+struct MarchGeom {
+  int tx, ty;
+  int j0, k0;      // tile origin
+  int j, k;        // this thread's column (may lie outside the level)
+  int jc, kc;      // clamped into the level
+  bool active;     // the column lies inside the level
+  int ib, ie;      // planes of this block
+  int off;         // in-plane offset of (jc, kc)
+};
+
+__device__ __forceinline__ bool march_geom(const LevelDev& L, int chunk, MarchGeom& g) {
+  const int ntk = (L.nz + kMK - 1) / kMK, ntj = (L.ny + kMJ - 1) / kMJ;
+  int b = (int)blockIdx.x;
+  const int tk = b % ntk;
+  b /= ntk;
+  const int tj = b % ntj;
+  const int sp = b / ntj;
+  g.ib = sp * chunk;
+  g.ie = min(L.nx, g.ib + chunk);
+  g.tx = (int)threadIdx.x;
+  g.ty = (int)threadIdx.y;
+  g.k0 = tk * kMK;
+  g.j0 = tj * kMJ;
+  g.k = g.k0 + g.tx;
+  g.j = g.j0 + g.ty;
+  g.active = g.j < L.ny && g.k < L.nz;
+  g.jc = min(g.j, L.ny - 1);
+  g.kc = min(g.k, L.nz - 1);
+  g.off = g.jc * L.nz + g.kc;
+  return g.ib < g.ie;
+}
+
+// Axis coefficients of the thread's column that do not change along i.
+struct ColumnCoef {
+  double kym, kyp, kzm, kzp;
+};
+
+__device__ __forceinline__ ColumnCoef column_coef(const LevelDev& L, int jc, int kc) {
+  ColumnCoef c;
+  c.kym = __ldg(L.cym + jc);
+  c.kyp = __ldg(L.cyp + jc);
+  c.kzm = __ldg(L.czm + kc);
+  c.kzp = __ldg(L.czp + kc);
+  return c;
+}
+
+// Neighbour sum and denominator of row (i, j, k) (fluid.py:4080-4221): the
+// mask selects the open faces in the order x-, x+, y-, y+, z-, z+; a closed
+// face adds exact zeros.  kAux: the level may carry Dirichlet face weights
+// (and an interface diagonal); without them the kernels skip those loads.
+template <bool kAux>
+__device__ __forceinline__ void stencil_sel(const LevelDev& L, const ColumnCoef& cc, double kxm, double kxp, int i,
+                                            int j, int k, int64_t c, unsigned m, int outlet, double vxm, double vxp,
+                                            double vym, double vyp, double vzm, double vzp, double& ns, double& den) {
+  double kym = cc.kym, kyp = cc.kyp, kzm = cc.kzm, kzp = cc.kzp;
+  if (kAux && L.fw != nullptr) {
+    const int64_t sx = (int64_t)L.ny * L.nz, sy = L.nz;
+    const double fc = (double)__ldg(L.fw + c);
+    kxm *= fc;
+    kxp *= (double)__ldg(L.fw + (i < L.nx - 1 ? c + sx : c));
+    kym *= fc;
+    kyp *= (double)__ldg(L.fw + (j < L.ny - 1 ? c + sy : c));
+    kzm *= fc;
+    kzp *= (double)__ldg(L.fw + (k < L.nz - 1 ? c + 1 : c));
+  }
+  const double axm = (m & M_XM) ? kxm : 0.0;
+  const double axp = (m & M_XP) ? kxp : 0.0;
+  const double aym = (m & M_YM) ? kym : 0.0;
+  const double ayp = (m & M_YP) ? kyp : 0.0;
+  const double azm = (m & M_ZM) ? kzm : 0.0;
+  const double azp = (m & M_ZP) ? kzp : 0.0;
+  ns = fma(axm, vxm, 0.0);
+  ns = fma(axp, vxp, ns);
+  ns = fma(aym, vym, ns);
+  ns = fma(ayp, vyp, ns);
+  ns = fma(azm, vzm, ns);
+  ns = fma(azp, vzp, ns);
+  den = 0.0 + axm;
+  den += axp;
+  den += aym;
+  den += ayp;
+  den += azm;
+  den += azp;
+  if (outlet && k == 0) den += L.oz;
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier / TMA primitives (inline PTX)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity; false if it did not complete
+// within kWaitCycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+constexpr int round128(int b) { return (b + 127) & ~127; }
+
+// Shared-memory stage of the pipeline: NV value tiles of TV (with halo, the
+// left pad is 16 bytes so the copy's x coordinate stays 16-byte aligned), an
+// optional right-hand-side tile of TR and the mask tile.
+template <typename TV, int NV, typename TR, bool kR>
+struct StageLayout {
+  static constexpr int kPad = 16 / (int)sizeof(TV);
+  static constexpr int kW = kMK + 2 * kPad;  // value row width (elements)
+  static constexpr int kVBytes = (kMJ + 2) * kW * (int)sizeof(TV);
+  static constexpr int kRBytes = kR ? kMJ * kMK * (int)sizeof(TR) : 0;
+  static constexpr int kMBytes = kMJ * kMK;
+  static constexpr int kVStride = round128(kVBytes);
+  static constexpr int kROff = NV * kVStride;
+  static constexpr int kMOff = kROff + round128(kRBytes);
+  static constexpr int kStage = round128(kMOff + kMBytes);
+  static constexpr int kBarOff = kStages * kStage;
+  static constexpr int kSmem = kBarOff + kStages * 8;
+};
+
+// The pipeline of one block: stage bookkeeping, the elected thread's copies
+// and the consumers' bounded waits.
+template <typename TV, int NV, typename TR, bool kR>
+struct PlanePipe {
+  using Lay = StageLayout<TV, NV, TR, kR>;
+  unsigned char* base;
+  uint64_t* bar;
+  const CUtensorMap* mv[NV];
+  const CUtensorMap* mr;
+  const CUtensorMap* mm;
+  int k0, j0, ib, ie;
+
+  __device__ __forceinline__ int stage_of(int plane) const { return (plane - ib + 1) % kStages; }
+  __device__ __forceinline__ unsigned parity_of(int plane) const { return ((plane - ib + 1) / kStages) & 1u; }
+  __device__ __forceinline__ const TV* val(int plane, int v) const {
+    return reinterpret_cast<const TV*>(base + stage_of(plane) * Lay::kStage + v * Lay::kVStride);
+  }
+  __device__ __forceinline__ const TR* rhs(int plane) const {
+    return reinterpret_cast<const TR*>(base + stage_of(plane) * Lay::kStage + Lay::kROff);
+  }
+  __device__ __forceinline__ const uint8_t* mask(int plane) const {
+    return reinterpret_cast<const uint8_t*>(base + stage_of(plane) * Lay::kStage + Lay::kMOff);
+  }
+  // Elected thread: copy plane `plane` into its stage.  Halo planes (ib-1,
+  // ie) carry only the value tiles.
+  __device__ __forceinline__ void issue(int plane) {
+    const int s = stage_of(plane);
+    unsigned char* st = base + s * Lay::kStage;
+    const bool interior = plane >= ib && plane < ie;
+    const unsigned bytes = NV * Lay::kVBytes + (interior ? Lay::kRBytes + Lay::kMBytes : 0);
+    mbar_expect_tx(&bar[s], bytes);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) tma_load_3d(st + v * Lay::kVStride, mv[v], k0 - Lay::kPad, j0 - 1, plane, &bar[s]);
+    if (interior) {
+      if (kR) tma_load_3d(st + Lay::kROff, mr, k0, j0, plane, &bar[s]);
+      tma_load_3d(st + Lay::kMOff, mm, k0, j0, plane, &bar[s]);
+    }
+  }
+  __device__ __forceinline__ bool wait(int plane) { return mbar_wait(&bar[stage_of(plane)], parity_of(plane)); }
+};
+
+// The march.  `Op::cell(i, j, k, c, m, rhs, kxm, kxp, val)` computes one row,
+// reading the field through val(v, di, dj, dk) (value tile v at (i+di, j+dj,
+// k+dk)); `Op::plane_end(g, i)` is the per-plane epilogue (it may use
+// __syncthreads).  Returns false (in every thread) if a stage did not land in
+// time; the kernel then reports it through `sc->fault`.
+template <typename TV, int NV, typename TR, bool kR, class Op>
+__device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, const CUtensorMap* const (&mv)[NV],
+                                      const CUtensorMap* mr, const CUtensorMap* mm, Op& op) {
+  extern __shared__ unsigned char dsmem[];  // launched with march_smem() bytes (128 of slack for the alignment)
+  using Pipe = PlanePipe<TV, NV, TR, kR>;
+  using Lay = typename Pipe::Lay;
+  Pipe pp;
+  pp.base = dsmem + ((128u - (smem_addr(dsmem) & 127u)) & 127u);
+  pp.bar = reinterpret_cast<uint64_t*>(pp.base + Lay::kBarOff);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) pp.mv[v] = mv[v];
+  pp.mr = mr;
+  pp.mm = mm;
+  pp.k0 = g.k0;
+  pp.j0 = g.j0;
+  pp.ib = g.ib;
+  pp.ie = g.ie;
+  const bool leader = g.tx == 0 && g.ty == 0;
+  if (leader) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&pp.bar[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int issued = min(g.ie, g.ib - 1 + kStages - 1);  // last plane in flight
+  if (leader)
+    for (int p = g.ib - 1; p <= issued; ++p) pp.issue(p);
+  bool fail = !pp.wait(g.ib - 1);
+  if (!fail) fail = !pp.wait(g.ib);
+  const int64_t sx = (int64_t)L.ny * L.nz;
+  const int row = g.ty + 1, col = g.tx + Lay::kPad, W = Lay::kW;
+  for (int i = g.ib; i < g.ie; ++i) {
+    if (!fail) fail = !pp.wait(i + 1);
+    if (!fail && g.active) {
+      const double kxm = __ldg(L.cxm + i), kxp = __ldg(L.cxp + i);
+      const int t = g.ty * kMK + g.tx;
+      const double e = kR ? (double)pp.rhs(i)[t] : 0.0;
+      const TV* vt[3][NV];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) vt[d][v] = pp.val(i - 1 + d, v) + row * W + col;
+      op.cell(i, g.j, g.k, (int64_t)i * sx + g.off, (unsigned)pp.mask(i)[t], e, kxm, kxp,
+              [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][dj * W + dk]; });
+    }
+    op.plane_end(g, i);
+    if (__syncthreads_or(fail)) {
+      // let the copies in flight land before the block exits
+      if (leader)
+        for (int p = i + 2; p <= issued; ++p) pp.wait(p);
+      __syncthreads();
+      return false;
+    }
+    if (leader && i - 1 + kStages <= g.ie) {
+      fence_proxy_async_smem();
+      issued = i - 1 + kStages;
+      pp.issue(issued);
+    }
+  }
+  return true;
+}
+
+template <typename TV, int NV, typename TR, bool kR>
+constexpr int march_smem() {
+  return StageLayout<TV, NV, TR, kR>::kSmem + 128;
+}
+
+__device__ __forceinline__ void report_fault(CgScalars* sc) {
+  if (flat_tid() == 0) atomicExch(&sc->fault, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Damped-Jacobi sweep (fluid.py:4224-4273), out of place, with the
+// prolongation p += s * p_coarse of fluid cells fused in when kProlong
+// (fluid.py:5391-5406) and, when `partials`, the fluid sum of out * V.
+// ---------------------------------------------------------------------------
+template <typename TP, bool kNegR, bool kProlong, bool kAux>
+struct SweepOp {
+  const LevelDev& L;
+  ColumnCoef cc;
+  TP* __restrict__ out;
+  int outlet;
+  double omega;
+  ProlongSrc pr;
+  bool want_sum;
+  double zsum;
+
+  // p + s * p_coarse at (i, j, k) in the level's storage precision
+  __device__ __forceinline__ double prolonged(double v, int i, int j, int k) const {
+    const float corr = __fmul_rn(
+        pr.scale,
+        __ldg(pr.pc + cidx(min(i / 2, pr.cnx - 1), min(j / 2, pr.cny - 1), min(k / 2, pr.cnz - 1), pr.cny, pr.cnz)));
+    if (sizeof(TP) == 8) return __dadd_rn(v, (double)corr);
+    return (double)__fadd_rn((float)v, corr);
+  }
+
+  template <class V>
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, unsigned m, double e, double kxm, double kxp,
+                                       const V& val) {
+    TP res = (TP)0;
+    if (!(m & M_SOLID)) {
+      double x0 = val(0, 0, 0, 0), xm = val(0, -1, 0, 0), xp = val(0, 1, 0, 0);
+      double ym = val(0, 0, -1, 0), yp = val(0, 0, 1, 0), zm = val(0, 0, 0, -1), zp = val(0, 0, 0, 1);
+      if (kProlong) {
+        // neighbours behind open faces are fluid; the centre by its own mask
+        // (indices are clamped, so a closed face at the level edge reads an
+        // in-level coarse value that is never used)
+        if (m & M_FLUID) x0 = prolonged(x0, i, j, k);
+        xm = prolonged(xm, max(i - 1, 0), j, k);
+        xp = prolonged(xp, i + 1, j, k);
+        ym = prolonged(ym, i, max(j - 1, 0), k);
+        yp = prolonged(yp, i, j + 1, k);
+        zm = prolonged(zm, i, j, max(k - 1, 0));
+        zp = prolonged(zp, i, j, k + 1);
+      }
+      double ns, den;
+      stencil_sel<kAux>(L, cc, kxm, kxp, i, j, k, c, m, outlet, xm, xp, ym, yp, zm, zp, ns, den);
+      if (kAux) den += iface_at<TP>(L, c);
+      if (den > 0.0) {
+        const double rv = kNegR ? -e : e;
+        const double jv = (ns - rv) / den;
+        res = (TP)(x0 + omega * (jv - x0));
+      }
+      if (want_sum && (m & M_FLUID)) zsum += (double)res * vol64(L, i, j, k);
+    }
+    out[c] = res;
+  }
+  __device__ __forceinline__ void plane_end(const MarchGeom&, int) {}
+};
+
+template <typename TP, bool kNegR, bool kProlong, bool kAux>
+__global__ void __launch_bounds__(kMK* kMJ)
+    km_sweep(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
+             const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
+             TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc) {
+  using TR = typename std::conditional<kNegR, double, TP>::type;
+  MarchGeom g;
+  const bool any = march_geom(L, chunk, g);
+  SweepOp<TP, kNegR, kProlong, kAux> op{L, column_coef(L, g.jc, g.kc), out, outlet, omega, pr,
+                                        partials != nullptr, 0.0};
+  const CUtensorMap* const mv[1] = {&map_p};
+  if (any && !march<TP, 1, TR, true>(L, g, mv, &map_r, &map_m, op)) report_fault(sc);
+  if (partials != nullptr) {
+    double v[1] = {op.zsum}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_z = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->zproj = 1;
+      }
+    }
+  }
+}
+
+// First sweep from a zero iterate: out = omega * (0 - rhs) / den per row; no
+// neighbour values are needed, so this is a plain streaming pass.
+template <typename TP, bool kNegR, bool kAux>
+__global__ void __launch_bounds__(kMK* kMJ)
+    km_sweep0(LevelDev L, int chunk, const void* rhs, TP* __restrict__ out, int outlet, double omega,
+              double* partials, CgScalars* sc) {
+  MarchGeom g;
+  double zsum = 0.0;
+  if (march_geom(L, chunk, g) && g.active) {
+    const int64_t sx = (int64_t)L.ny * L.nz;
+    const ColumnCoef cc = column_coef(L, g.jc, g.kc);
+#pragma unroll 4
+    for (int i = g.ib; i < g.ie; ++i) {
+      const int64_t c = (int64_t)i * sx + g.off;
+      const unsigned m = __ldg(L.mask + c);
+      const double e = kNegR ? __ldg(reinterpret_cast<const double*>(rhs) + c)
+                             : (double)__ldg(reinterpret_cast<const TP*>(rhs) + c);
+      TP res = (TP)0;
+      if (!(m & M_SOLID)) {
+        double ns, den;
+        stencil_sel<kAux>(L, cc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, g.j, g.k, c, m, outlet, 0.0, 0.0, 0.0, 0.0,
+                          0.0, 0.0, ns, den);
+        if (kAux) den += iface_at<TP>(L, c);
+        if (den > 0.0) {
+          const double rv = kNegR ? -e : e;
+          const double jv = (ns - rv) / den;
+          res = (TP)(0.0 + omega * (jv - 0.0));
+        }
+        if (partials != nullptr && (m & M_FLUID)) zsum += (double)res * vol64(L, i, g.j, g.k);
+      }
+      out[c] = res;
+    }
+  }
+  if (partials != nullptr) {
+    double v[1] = {zsum}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_z = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->zproj = 1;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CG direction and SpMV: d_new = z' (copy) or z' + beta d_old (fluid.py:
+// 4604-4611, masked; z' the zero-mean projected z of fluid.py:4716-4722),
+// Ad = A d_new (fluid.py:4312-4345), <d, Ad>_V and alpha (fluid.py:4567-4574).
+// The direction of every stencil point is formed from the z and d_old tiles.
+// ---------------------------------------------------------------------------
+template <bool kCopy, bool kAux>
+struct SpmvOp {
+  const LevelDev& L;
+  ColumnCoef cc;
+  double* __restrict__ d_new;
+  double* __restrict__ Ad;
+  int outlet;
+  double beta, mz;
+  int zproj;
+  double part;
+
+  // direction at a neighbour behind an open face (a fluid cell)
+  template <class V>
+  __device__ __forceinline__ double dir(const V& val, int dp, int dj, int dk) const {
+    double zz = val(0, dp, dj, dk);
+    if (zproj) zz = zz - mz;
+    return kCopy ? zz : zz + beta * val(1, dp, dj, dk);
+  }
+
+  template <class V>
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, unsigned m, double, double kxm, double kxp,
+                                       const V& val) {
+    double x0;
+    if (m & M_SOLID)
+      x0 = 0.0;
+    else if (!(m & M_FLUID) && zproj)
+      x0 = kCopy ? 0.0 : 0.0 + beta * val(1, 0, 0, 0);
+    else
+      x0 = dir(val, 0, 0, 0);
+    d_new[c] = x0;
+    double o = 0.0;
+    if (!(m & M_SOLID)) {
+      double ns, den;
+      stencil_sel<kAux>(L, cc, kxm, kxp, i, j, k, c, m, outlet, dir(val, -1, 0, 0), dir(val, 1, 0, 0),
+                        dir(val, 0, -1, 0), dir(val, 0, 1, 0), dir(val, 0, 0, -1), dir(val, 0, 0, 1), ns, den);
+      o = (den + (kAux ? iface_at<double>(L, c) : 0.0)) * x0 - ns;
+    }
+    Ad[c] = o;
+    if (m & M_FLUID) part += x0 * o * vol64(L, i, j, k);
+  }
+  __device__ __forceinline__ void plane_end(const MarchGeom&, int) {}
+};
+
+template <bool kCopy, bool kAux>
+__global__ void __launch_bounds__(kMK* kMJ)
+    km_spmv_dir(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_z,
+                const __grid_constant__ CUtensorMap map_d, const __grid_constant__ CUtensorMap map_m,
+                double* __restrict__ d_new, double* __restrict__ Ad, int outlet, double* partials, CgScalars* sc) {
+  MarchGeom g;
+  const bool any = march_geom(L, chunk, g);
+  SpmvOp<kCopy, kAux> op{L, column_coef(L, g.jc, g.kc), d_new, Ad, outlet, kCopy ? 0.0 : sc->beta, sc->mean_z,
+                         sc->zproj, 0.0};
+  bool ok = true;
+  if (any) {
+    if (kCopy) {
+      const CUtensorMap* const mv[1] = {&map_z};
+      ok = march<double, 1, double, false>(L, g, mv, nullptr, &map_m, op);
+    } else {
+      const CUtensorMap* const mv[2] = {&map_z, &map_d};
+      ok = march<double, 2, double, false>(L, g, mv, nullptr, &map_m, op);
+    }
+  }
+  if (!ok) report_fault(sc);
+  double v[1] = {op.part}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      const double dAd = t[0];
+      sc->dAd = dAd;
+      sc->alpha = 0.0;
+      if (dAd <= 0.0) {
+        if (sc->code == 0) sc->code_dAd = dAd;
+        sc->code = 1;
+      } else {
+        sc->alpha = sc->rz / dAd;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Residual restriction (fluid.py:5262-5388): the fine residual of every row
+// is formed in the march and staged in shared memory; the threads owning a
+// coarse cell accumulate its 2 x 2 x 2 children in the reference's order
+// (i-pair outer, then j, then k) with the f32 volume weights, across the two
+// planes of the pair.
+// ---------------------------------------------------------------------------
+template <typename TP, bool kNegR, bool kAux>
+struct RestrictOp {
+  const LevelDev& L;
+  ColumnCoef cc;
+  int outlet;
+  int cnx, cny, cnz;
+  float* __restrict__ crhs;
+  double (*rs)[kMK];
+  unsigned char (*rsolid)[kMK];
+  float wres, free_vol;
+  int ocount;
+
+  template <class V>
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, unsigned m, double e, double kxm, double kxp,
+                                       const V& val) {
+    const int ty = (int)threadIdx.y, tx = (int)threadIdx.x;
+    if (m & M_SOLID) {
+      rsolid[ty][tx] = 1;
+      rs[ty][tx] = 0.0;
+      return;
+    }
+    double ns, den;
+    stencil_sel<kAux>(L, cc, kxm, kxp, i, j, k, c, m, outlet, val(0, -1, 0, 0), val(0, 1, 0, 0), val(0, 0, -1, 0),
+                      val(0, 0, 1, 0), val(0, 0, 0, -1), val(0, 0, 0, 1), ns, den);
+    if (kAux) den += iface_at<TP>(L, c);
+    const double applied = ns - den * val(0, 0, 0, 0);
+    const double rv = kNegR ? -e : e;
+    rsolid[ty][tx] = 0;
+    rs[ty][tx] = (double)(TP)(rv - applied);
+  }
+  __device__ __forceinline__ void plane_end(const MarchGeom& g, int i) {
+    __syncthreads();
+    if (g.tx < kMK / 2 && g.ty < kMJ / 2) {
+      const int fj0 = g.j0 + 2 * g.ty, fk0 = g.k0 + 2 * g.tx;
+#pragma unroll
+      for (int oj = 0; oj < 2; ++oj)
+#pragma unroll
+        for (int ok = 0; ok < 2; ++ok) {
+          const int fj = fj0 + oj, fk = fk0 + ok;
+          if (fj < L.ny && fk < L.nz) {
+            if (rsolid[2 * g.ty + oj][2 * g.tx + ok]) {
+              ocount += 1;
+            } else {
+              const float vol = __fmul_rn(__fmul_rn(__ldg(L.wx + i), __ldg(L.wy + fj)), __ldg(L.wz + fk));
+              const double r = rs[2 * g.ty + oj][2 * g.tx + ok];
+              if (sizeof(TP) == 8)
+                wres = (float)__dadd_rn((double)wres, __dmul_rn(r, (double)vol));
+              else
+                wres = __fadd_rn(wres, __fmul_rn((float)r, vol));
+              free_vol = __fadd_rn(free_vol, vol);
+            }
+          }
+        }
+      if ((i & 1) || i == L.nx - 1) {
+        const int ci = i >> 1, cj = fj0 >> 1, ck = fk0 >> 1;
+        if (ci < cnx && cj < cny && ck < cnz)
+          crhs[cidx(ci, cj, ck, cny, cnz)] = ocount > 0 ? 0.0f : __fdiv_rn(wres, fmaxf(free_vol, 1.0e-30f));
+        wres = 0.0f;
+        free_vol = 0.0f;
+        ocount = 0;
+      }
+    }
+  }
+};
+
+template <typename TP, bool kNegR, bool kAux>
+__global__ void __launch_bounds__(kMK* kMJ)
+    km_restrict(LevelDev F, int chunk, const __grid_constant__ CUtensorMap map_p,
+                const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m, int outlet,
+                int cnx, int cny, int cnz, float* __restrict__ crhs, CgScalars* sc) {
+  using TR = typename std::conditional<kNegR, double, TP>::type;
+  __shared__ double rs[kMJ][kMK];
+  __shared__ unsigned char rsolid[kMJ][kMK];
+  MarchGeom g;
+  const bool any = march_geom(F, chunk, g);
+  RestrictOp<TP, kNegR, kAux> op{F, column_coef(F, g.jc, g.kc), outlet, cnx, cny, cnz, crhs, rs, rsolid,
+                                 0.0f, 0.0f, 0};
+  const CUtensorMap* const mv[1] = {&map_p};
+  if (any && !march<TP, 1, TR, true>(F, g, mv, &map_r, &map_m, op)) report_fault(sc);
+}
+
+}  // namespace efsi

@@ -208,3 +208,74 @@ def test_graph_blocks_match_direct_launches(case):
     assert out[0][0] == out[1][0] == out[2][0]
     assert np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[1][1], out[2][1])
+
+
+def _paired_solvers(n, aux=False):
+    """The same graded grid and obstacle built twice: plane-marching kernels
+    (default) and the per-cell kernels (selected at plan creation).  With
+    `aux`, Dirichlet velocity rows and an interface diagonal are live too."""
+    import os
+
+    grid = _graded_grid(n)
+    obs = _obstacle(grid, seed=7)
+    rng = np.random.default_rng(23)
+    va = (rng.random(grid.grid_nodes) < 0.05).astype(np.int32)
+    vw = rng.random(grid.grid_nodes).astype(np.float32)
+    iface = np.where(rng.random(grid.grid_nodes) < 0.05, rng.random(grid.grid_nodes), 0.0)
+    out = []
+    for env in ({}, {"EFSI_NO_MARCH": "1", "EFSI_NO_TILED": "1"}):
+        saved = {k: os.environ.get(k) for k in ("EFSI_NO_MARCH", "EFSI_NO_TILED")}
+        os.environ.update(env)
+        try:
+            fl = _solver(grid)
+            fl.obstacle.from_numpy(obs)
+            if aux:
+                fl.velocity_dirichlet_boundary_active.from_numpy(va)
+                fl.velocity_dirichlet_boundary_projection_weight.from_numpy(vw)
+                fl.pressure_interface_matrix_diagonal.from_numpy(iface)
+            fl._refresh_structure()
+        finally:
+            for k, v in saved.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        out.append(fl)
+    return grid, out
+
+
+@pytest.mark.parametrize("n,aux", [((40, 24, 48), False), ((14, 12, 18), False), ((40, 24, 48), True)])
+def test_march_kernels_match_per_cell_kernels(n, aux):
+    """Plane-marching sweeps / restriction / SpMV reproduce the per-cell
+    kernels: same arithmetic per row, so the V-cycle agrees to rounding of the
+    z-mean reduction order only (none here), and PCG takes the same path."""
+    grid, (fm, fc) = _paired_solvers(n, aux)
+    rng = np.random.default_rng(17)
+    r = rng.normal(size=grid.grid_nodes)
+    r[fm.obstacle.to_numpy() == 1] = 0.0
+    zs = []
+    for fl in (fm, fc):
+        fl.cg_r.from_numpy(r)
+        fl._apply_fv_multigrid_preconditioner(fl.cg_r, pressure_outlet_zmin=False)
+        zs.append(fl.cg_z.to_numpy())
+    assert rel_l2(zs[0], zs[1]) <= 1e-13
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    res = []
+    for fl in (fm, fc):
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(
+            iterations=300, rhs_scale=1.0e6, pressure_outlet_zmin=False, tolerance=1e-9, preconditioner="fv_multigrid"
+        )
+        res.append((fl.last_cg_iterations, fl.pressure.to_numpy()))
+    assert res[0][0] == res[1][0]
+    # the dot products sum their block partials over different partitions, so
+    # the two solves agree to well below their 1e-9 residual tolerance
+    assert rel_l2(res[0][1], res[1][1]) <= 1e-8
+    for fl in (fm, fc):
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_multigrid(
+            iterations=4, rhs_scale=1.0e6, pressure_outlet_zmin=True, multigrid_cycles=2
+        )
+    assert rel_l2(fm.pressure.to_numpy(), fc.pressure.to_numpy()) <= 1e-12
