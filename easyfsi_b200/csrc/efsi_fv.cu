@@ -1361,6 +1361,21 @@ static void preload_kernels() {
 #undef EFSI_MARCH_FNS
   };
   for (const void* f : fns) cudaFuncGetAttributes(&a, f);
+  // the plane-marching kernels take up to ~70 KB of dynamic shared memory
+#define EFSI_MARCH_SMEM(A)                                                                                        \
+  {(const void*)km_sweep<double, true, false, A>, march_smem<double, 1, double, true>()},                         \
+      {(const void*)km_sweep<double, true, true, A>, march_smem<double, 1, double, true>()},                      \
+      {(const void*)km_sweep<double, false, false, A>, march_smem<double, 1, double, true>()},                    \
+      {(const void*)km_sweep<float, false, false, A>, march_smem<float, 1, float, true>()},                       \
+      {(const void*)km_sweep<float, false, true, A>, march_smem<float, 1, float, true>()},                        \
+      {(const void*)km_restrict<double, true, A>, march_smem<double, 1, double, true>()},                         \
+      {(const void*)km_restrict<double, false, A>, march_smem<double, 1, double, true>()},                        \
+      {(const void*)km_restrict<float, false, A>, march_smem<float, 1, float, true>()},                           \
+      {(const void*)km_spmv_dir<true, A>, march_smem<double, 1, double, false>()},                                \
+      {(const void*)km_spmv_dir<false, A>, march_smem<double, 2, double, false>()}
+  const std::pair<const void*, int> dyn[] = {EFSI_MARCH_SMEM(false), EFSI_MARCH_SMEM(true)};
+#undef EFSI_MARCH_SMEM
+  for (const auto& d : dyn) cudaFuncSetAttribute(d.first, cudaFuncAttributeMaxDynamicSharedMemorySize, d.second);
   cudaGetLastError();
 }
 }  // namespace efsi
@@ -1479,7 +1494,7 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
       const int nt = tiles_of(B.nx, B.ny, B.nz);
       B.tiled = B.nz >= 16 && B.ny >= 8 && std::getenv("EFSI_NO_TILED") == nullptr;
       B.tgrid = (unsigned)std::max(1, std::min(nt, nsm * per_sm));
-      const MarchCfg mc = march_cfg(B.nx, B.ny, B.nz, nsm * 4);
+      const MarchCfg mc = march_cfg(B.nx, B.ny, B.nz, nsm * 3);
       B.march = B.nz >= 16 && B.ny >= 8 && std::getenv("EFSI_NO_MARCH") == nullptr;
       B.mchunk = mc.chunk;
       B.mgrid = mc.grid;
@@ -1812,7 +1827,7 @@ static bool launch_march_spmv(efsi_fv_plan* P, const LevelDev& L, bool copy, con
   const CUtensorMap* mm = plane_map(P, 0, B.mask, MAP_MASK);
   const CUtensorMap* md = copy ? mz : plane_map(P, 0, d_old, MAP_VALUE);
   if (!mz || !mm || !md) return false;
-  const dim3 blk(kMK, kMJ);
+  const dim3 blk(kMK, kTY);
   const bool aux = L.fw != nullptr || L.iface != nullptr;
   const int sm1 = march_smem<double, 1, double, false>(), sm2 = march_smem<double, 2, double, false>();
   if (copy && aux)
@@ -1837,7 +1852,7 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
                                int outlet, double om, ProlongSrc pr, double* partials, cudaStream_t s) {
   using TR = typename std::conditional<kNegR, double, TP>::type;
   const LevelBuf& B = P->lv[l];
-  const dim3 blk(kMK, kMJ);
+  const dim3 blk(kMK, kTY);
   if (kZero) {
     EFSI_COUNTED km_sweep0<TP, kNegR, kAux><<<B.mgrid, blk, 0, s>>>(L, B.mchunk, rhs, out, outlet, om, partials,
                                                                      P->sc);
@@ -1893,10 +1908,10 @@ static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs
     if (mp && mr && mm) {
       const int sm = march_smem<TP, 1, TR, true>();
       if (L.fw != nullptr || L.iface != nullptr)
-        EFSI_COUNTED km_restrict<TP, kNegR, true><<<B.mgrid, dim3(kMK, kMJ), sm, s>>>(
+        EFSI_COUNTED km_restrict<TP, kNegR, true><<<B.mgrid, dim3(kMK, kTY), sm, s>>>(
             L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
       else
-        EFSI_COUNTED km_restrict<TP, kNegR, false><<<B.mgrid, dim3(kMK, kMJ), sm, s>>>(
+        EFSI_COUNTED km_restrict<TP, kNegR, false><<<B.mgrid, dim3(kMK, kTY), sm, s>>>(
             L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
       return;
     }

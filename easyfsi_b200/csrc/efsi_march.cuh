@@ -34,7 +34,10 @@
 
 namespace efsi {
 
-constexpr int kMK = 32, kMJ = 8;
+constexpr int kMK = 32;           // tile width along k (one warp)
+constexpr int kTY = 8;            // thread rows per block
+constexpr int kRows = 2;          // tile rows per thread row
+constexpr int kMJ = kTY * kRows;  // tile height along j
 constexpr int kStages = 6;
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s: a stage that never lands is reported, not waited on forever
 
@@ -59,14 +62,16 @@ inline MarchCfg march_cfg(int nx, int ny, int nz, int slots) {
   return c;
 }
 
+// Thread (tx, ty) of a block owns the cells (j0 + ty + r * kTY, k0 + tx),
+// r < kRows, of every plane of the block's chunk.
 struct MarchGeom {
   int tx, ty;
-  int j0, k0;      // tile origin
-  int j, k;        // this thread's column (may lie outside the level)
-  int jc, kc;      // clamped into the level
-  bool active;     // the column lies inside the level
-  int ib, ie;      // planes of this block
-  int off;         // in-plane offset of (jc, kc)
+  int j0, k0;             // tile origin
+  int k, kc;              // this thread's k (may lie outside the level) and its clamp
+  int ib, ie;             // planes of this block
+  int j[kRows];           // the thread's rows
+  bool active[kRows];     // (j, k) lies inside the level
+  int off[kRows];         // in-plane offset of (j, k), clamped into the level
 };
 
 __device__ __forceinline__ bool march_geom(const LevelDev& L, int chunk, MarchGeom& g) {
@@ -83,21 +88,24 @@ __device__ __forceinline__ bool march_geom(const LevelDev& L, int chunk, MarchGe
   g.k0 = tk * kMK;
   g.j0 = tj * kMJ;
   g.k = g.k0 + g.tx;
-  g.j = g.j0 + g.ty;
-  g.active = g.j < L.ny && g.k < L.nz;
-  g.jc = min(g.j, L.ny - 1);
   g.kc = min(g.k, L.nz - 1);
-  g.off = g.jc * L.nz + g.kc;
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    g.j[r] = g.j0 + g.ty + r * kTY;
+    g.active[r] = g.j[r] < L.ny && g.k < L.nz;
+    g.off[r] = min(g.j[r], L.ny - 1) * L.nz + g.kc;
+  }
   return g.ib < g.ie;
 }
 
-// Axis coefficients of the thread's column that do not change along i.
-struct ColumnCoef {
+// Axis coefficients of one row that do not change along i.
+struct RowCoef {
   double kym, kyp, kzm, kzp;
 };
 
-__device__ __forceinline__ ColumnCoef column_coef(const LevelDev& L, int jc, int kc) {
-  ColumnCoef c;
+__device__ __forceinline__ RowCoef row_coef(const LevelDev& L, int j, int kc) {
+  const int jc = min(j, L.ny - 1);
+  RowCoef c;
   c.kym = __ldg(L.cym + jc);
   c.kyp = __ldg(L.cyp + jc);
   c.kzm = __ldg(L.czm + kc);
@@ -110,7 +118,7 @@ __device__ __forceinline__ ColumnCoef column_coef(const LevelDev& L, int jc, int
 // face adds exact zeros.  kAux: the level may carry Dirichlet face weights
 // (and an interface diagonal); without them the kernels skip those loads.
 template <bool kAux>
-__device__ __forceinline__ void stencil_sel(const LevelDev& L, const ColumnCoef& cc, double kxm, double kxp, int i,
+__device__ __forceinline__ void stencil_sel(const LevelDev& L, const RowCoef& cc, double kxm, double kxp, int i,
                                             int j, int k, int64_t c, unsigned m, int outlet, double vxm, double vxp,
                                             double vym, double vyp, double vzm, double vzp, double& ns, double& den) {
   double kym = cc.kym, kyp = cc.kyp, kzm = cc.kzm, kzp = cc.kzp;
@@ -220,110 +228,96 @@ struct StageLayout {
   static constexpr int kSmem = kBarOff + kStages * 8;
 };
 
-// The pipeline of one block: stage bookkeeping, the elected thread's copies
-// and the consumers' bounded waits.
-template <typename TV, int NV, typename TR, bool kR>
-struct PlanePipe {
-  using Lay = StageLayout<TV, NV, TR, kR>;
-  unsigned char* base;
-  uint64_t* bar;
-  const CUtensorMap* mv[NV];
-  const CUtensorMap* mr;
-  const CUtensorMap* mm;
-  int k0, j0, ib, ie;
-
-  __device__ __forceinline__ int stage_of(int plane) const { return (plane - ib + 1) % kStages; }
-  __device__ __forceinline__ unsigned parity_of(int plane) const { return ((plane - ib + 1) / kStages) & 1u; }
-  __device__ __forceinline__ const TV* val(int plane, int v) const {
-    return reinterpret_cast<const TV*>(base + stage_of(plane) * Lay::kStage + v * Lay::kVStride);
-  }
-  __device__ __forceinline__ const TR* rhs(int plane) const {
-    return reinterpret_cast<const TR*>(base + stage_of(plane) * Lay::kStage + Lay::kROff);
-  }
-  __device__ __forceinline__ const uint8_t* mask(int plane) const {
-    return reinterpret_cast<const uint8_t*>(base + stage_of(plane) * Lay::kStage + Lay::kMOff);
-  }
-  // Elected thread: copy plane `plane` into its stage.  Halo planes (ib-1,
-  // ie) carry only the value tiles.
-  __device__ __forceinline__ void issue(int plane) {
-    const int s = stage_of(plane);
-    unsigned char* st = base + s * Lay::kStage;
-    const bool interior = plane >= ib && plane < ie;
-    const unsigned bytes = NV * Lay::kVBytes + (interior ? Lay::kRBytes + Lay::kMBytes : 0);
-    mbar_expect_tx(&bar[s], bytes);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) tma_load_3d(st + v * Lay::kVStride, mv[v], k0 - Lay::kPad, j0 - 1, plane, &bar[s]);
-    if (interior) {
-      if (kR) tma_load_3d(st + Lay::kROff, mr, k0, j0, plane, &bar[s]);
-      tma_load_3d(st + Lay::kMOff, mm, k0, j0, plane, &bar[s]);
-    }
-  }
-  __device__ __forceinline__ bool wait(int plane) { return mbar_wait(&bar[stage_of(plane)], parity_of(plane)); }
-};
-
-// The march.  `Op::cell(i, j, k, c, m, rhs, kxm, kxp, val)` computes one row,
-// reading the field through val(v, di, dj, dk) (value tile v at (i+di, j+dj,
-// k+dk)); `Op::plane_end(g, i)` is the per-plane epilogue (it may use
-// __syncthreads).  Returns false (in every thread) if a stage did not land in
-// time; the kernel then reports it through `sc->fault`.
+// The march.  Per plane i and owned row r, `Op::cell(i, j, k, c, t, m, rhs,
+// kxm, kxp, rc, val)` computes one cell (t: its index in the tile), reading
+// the field through val(v, di, dj, dk) (value tile v at (i+di, j+dj, k+dk));
+// `Op::plane_end(g, i)` runs before the plane's block barrier and
+// `Op::finish(g)` after the last plane.  Returns false (in every thread) if a
+// stage did not land in time; the kernel then reports it through
+// `sc->fault`.
 template <typename TV, int NV, typename TR, bool kR, class Op>
 __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, const CUtensorMap* const (&mv)[NV],
                                       const CUtensorMap* mr, const CUtensorMap* mm, Op& op) {
   extern __shared__ unsigned char dsmem[];  // launched with march_smem() bytes (128 of slack for the alignment)
-  using Pipe = PlanePipe<TV, NV, TR, kR>;
-  using Lay = typename Pipe::Lay;
-  Pipe pp;
-  pp.base = dsmem + ((128u - (smem_addr(dsmem) & 127u)) & 127u);
-  pp.bar = reinterpret_cast<uint64_t*>(pp.base + Lay::kBarOff);
-#pragma unroll
-  for (int v = 0; v < NV; ++v) pp.mv[v] = mv[v];
-  pp.mr = mr;
-  pp.mm = mm;
-  pp.k0 = g.k0;
-  pp.j0 = g.j0;
-  pp.ib = g.ib;
-  pp.ie = g.ie;
+  using Lay = StageLayout<TV, NV, TR, kR>;
+  unsigned char* base = dsmem + ((128u - (smem_addr(dsmem) & 127u)) & 127u);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + Lay::kBarOff);
   const bool leader = g.tx == 0 && g.ty == 0;
+  // Elected thread: copy plane p into stage s.  Halo planes (ib-1, ie) carry
+  // only the value tiles.
+  auto issue = [&](int p, int s) {
+    unsigned char* st = base + s * Lay::kStage;
+    const bool interior = p >= g.ib && p < g.ie;
+    mbar_expect_tx(&bar[s], NV * Lay::kVBytes + (interior ? Lay::kRBytes + Lay::kMBytes : 0));
+#pragma unroll
+    for (int v = 0; v < NV; ++v) tma_load_3d(st + v * Lay::kVStride, mv[v], g.k0 - Lay::kPad, g.j0 - 1, p, &bar[s]);
+    if (interior) {
+      if (kR) tma_load_3d(st + Lay::kROff, mr, g.k0, g.j0, p, &bar[s]);
+      tma_load_3d(st + Lay::kMOff, mm, g.k0, g.j0, p, &bar[s]);
+    }
+  };
   if (leader) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&pp.bar[s], 1);
+    for (int s = 0; s < kStages; ++s) mbar_init(&bar[s], 1);
     mbar_fence_init();
   }
   __syncthreads();
+  // plane p lives in stage (p - ib + 1) % kStages, phase ((p - ib + 1) / kStages) & 1
   int issued = min(g.ie, g.ib - 1 + kStages - 1);  // last plane in flight
   if (leader)
-    for (int p = g.ib - 1; p <= issued; ++p) pp.issue(p);
-  bool fail = !pp.wait(g.ib - 1);
-  if (!fail) fail = !pp.wait(g.ib);
+    for (int p = g.ib - 1; p <= issued; ++p) issue(p, p - g.ib + 1);
+  bool fail = !mbar_wait(&bar[0], 0u);
+  if (!fail) fail = !mbar_wait(&bar[1], 0u);
+  int s_m = 0, s_0 = 1, s_p = 2 % kStages;  // stages of planes i-1, i, i+1
+  unsigned ph_p = 0;                        // phase parity of plane i+1
   const int64_t sx = (int64_t)L.ny * L.nz;
-  const int row = g.ty + 1, col = g.tx + Lay::kPad, W = Lay::kW;
-  for (int i = g.ib; i < g.ie; ++i) {
-    if (!fail) fail = !pp.wait(i + 1);
-    if (!fail && g.active) {
+  const int col = g.tx + Lay::kPad, W = Lay::kW;
+  RowCoef rc[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) rc[r] = row_coef(L, g.j[r], g.kc);
+  int64_t pbase = (int64_t)g.ib * sx;
+  for (int i = g.ib; i < g.ie; ++i, pbase += sx) {
+    if (!fail) fail = !mbar_wait(&bar[s_p], ph_p);
+    if (!fail) {
       const double kxm = __ldg(L.cxm + i), kxp = __ldg(L.cxp + i);
-      const int t = g.ty * kMK + g.tx;
-      const double e = kR ? (double)pp.rhs(i)[t] : 0.0;
       const TV* vt[3][NV];
 #pragma unroll
-      for (int d = 0; d < 3; ++d)
+      for (int v = 0; v < NV; ++v) {
+        vt[0][v] = reinterpret_cast<const TV*>(base + s_m * Lay::kStage + v * Lay::kVStride) + col;
+        vt[1][v] = reinterpret_cast<const TV*>(base + s_0 * Lay::kStage + v * Lay::kVStride) + col;
+        vt[2][v] = reinterpret_cast<const TV*>(base + s_p * Lay::kStage + v * Lay::kVStride) + col;
+      }
+      const TR* rt = reinterpret_cast<const TR*>(base + s_0 * Lay::kStage + Lay::kROff);
+      const uint8_t* mt = base + s_0 * Lay::kStage + Lay::kMOff;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) vt[d][v] = pp.val(i - 1 + d, v) + row * W + col;
-      op.cell(i, g.j, g.k, (int64_t)i * sx + g.off, (unsigned)pp.mask(i)[t], e, kxm, kxp,
-              [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][dj * W + dk]; });
+      for (int r = 0; r < kRows; ++r) {
+        if (!g.active[r]) continue;
+        const int t = (g.ty + r * kTY) * kMK + g.tx;
+        const int row = (g.ty + r * kTY + 1) * W;
+        op.cell(i, g.j[r], g.k, pbase + g.off[r], t, (unsigned)mt[t], kR ? (double)rt[t] : 0.0, kxm, kxp, rc[r],
+                [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][row + dj * W + dk]; });
+      }
     }
     op.plane_end(g, i);
     if (__syncthreads_or(fail)) {
       // let the copies in flight land before the block exits
       if (leader)
-        for (int p = i + 2; p <= issued; ++p) pp.wait(p);
+        for (int p = i + 2; p <= issued; ++p) mbar_wait(&bar[(p - g.ib + 1) % kStages], ((p - g.ib + 1) / kStages) & 1u);
       __syncthreads();
       return false;
     }
     if (leader && i - 1 + kStages <= g.ie) {
       fence_proxy_async_smem();
       issued = i - 1 + kStages;
-      pp.issue(issued);
+      issue(issued, s_m);
+    }
+    s_m = s_0;
+    s_0 = s_p;
+    if (++s_p == kStages) {
+      s_p = 0;
+      ph_p ^= 1u;
     }
   }
+  op.finish(g);
   return true;
 }
 
@@ -344,7 +338,6 @@ __device__ __forceinline__ void report_fault(CgScalars* sc) {
 template <typename TP, bool kNegR, bool kProlong, bool kAux>
 struct SweepOp {
   const LevelDev& L;
-  ColumnCoef cc;
   TP* __restrict__ out;
   int outlet;
   double omega;
@@ -362,8 +355,8 @@ struct SweepOp {
   }
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, unsigned m, double e, double kxm, double kxp,
-                                       const V& val) {
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, unsigned m, double e, double kxm,
+                                       double kxp, const RowCoef& rc, const V& val) {
     TP res = (TP)0;
     if (!(m & M_SOLID)) {
       double x0 = val(0, 0, 0, 0), xm = val(0, -1, 0, 0), xp = val(0, 1, 0, 0);
@@ -381,7 +374,7 @@ struct SweepOp {
         zp = prolonged(zp, i, j, k + 1);
       }
       double ns, den;
-      stencil_sel<kAux>(L, cc, kxm, kxp, i, j, k, c, m, outlet, xm, xp, ym, yp, zm, zp, ns, den);
+      stencil_sel<kAux>(L, rc, kxm, kxp, i, j, k, c, m, outlet, xm, xp, ym, yp, zm, zp, ns, den);
       if (kAux) den += iface_at<TP>(L, c);
       if (den > 0.0) {
         const double rv = kNegR ? -e : e;
@@ -393,18 +386,18 @@ struct SweepOp {
     out[c] = res;
   }
   __device__ __forceinline__ void plane_end(const MarchGeom&, int) {}
+  __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
 template <typename TP, bool kNegR, bool kProlong, bool kAux>
-__global__ void __launch_bounds__(kMK* kMJ)
+__global__ void __launch_bounds__(kMK* kTY)
     km_sweep(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
              const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
              TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc) {
   using TR = typename std::conditional<kNegR, double, TP>::type;
   MarchGeom g;
   const bool any = march_geom(L, chunk, g);
-  SweepOp<TP, kNegR, kProlong, kAux> op{L, column_coef(L, g.jc, g.kc), out, outlet, omega, pr,
-                                        partials != nullptr, 0.0};
+  SweepOp<TP, kNegR, kProlong, kAux> op{L, out, outlet, omega, pr, partials != nullptr, 0.0};
   const CUtensorMap* const mv[1] = {&map_p};
   if (any && !march<TP, 1, TR, true>(L, g, mv, &map_r, &map_m, op)) report_fault(sc);
   if (partials != nullptr) {
@@ -421,34 +414,38 @@ __global__ void __launch_bounds__(kMK* kMJ)
 // First sweep from a zero iterate: out = omega * (0 - rhs) / den per row; no
 // neighbour values are needed, so this is a plain streaming pass.
 template <typename TP, bool kNegR, bool kAux>
-__global__ void __launch_bounds__(kMK* kMJ)
+__global__ void __launch_bounds__(kMK* kTY)
     km_sweep0(LevelDev L, int chunk, const void* rhs, TP* __restrict__ out, int outlet, double omega,
               double* partials, CgScalars* sc) {
   MarchGeom g;
   double zsum = 0.0;
-  if (march_geom(L, chunk, g) && g.active) {
+  if (march_geom(L, chunk, g)) {
     const int64_t sx = (int64_t)L.ny * L.nz;
-    const ColumnCoef cc = column_coef(L, g.jc, g.kc);
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      if (!g.active[r]) continue;
+      const RowCoef rc = row_coef(L, g.j[r], g.kc);
 #pragma unroll 4
-    for (int i = g.ib; i < g.ie; ++i) {
-      const int64_t c = (int64_t)i * sx + g.off;
-      const unsigned m = __ldg(L.mask + c);
-      const double e = kNegR ? __ldg(reinterpret_cast<const double*>(rhs) + c)
-                             : (double)__ldg(reinterpret_cast<const TP*>(rhs) + c);
-      TP res = (TP)0;
-      if (!(m & M_SOLID)) {
-        double ns, den;
-        stencil_sel<kAux>(L, cc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, g.j, g.k, c, m, outlet, 0.0, 0.0, 0.0, 0.0,
-                          0.0, 0.0, ns, den);
-        if (kAux) den += iface_at<TP>(L, c);
-        if (den > 0.0) {
-          const double rv = kNegR ? -e : e;
-          const double jv = (ns - rv) / den;
-          res = (TP)(0.0 + omega * (jv - 0.0));
+      for (int i = g.ib; i < g.ie; ++i) {
+        const int64_t c = (int64_t)i * sx + g.off[r];
+        const unsigned m = __ldg(L.mask + c);
+        const double e = kNegR ? __ldg(reinterpret_cast<const double*>(rhs) + c)
+                               : (double)__ldg(reinterpret_cast<const TP*>(rhs) + c);
+        TP res = (TP)0;
+        if (!(m & M_SOLID)) {
+          double ns, den;
+          stencil_sel<kAux>(L, rc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, g.j[r], g.k, c, m, outlet, 0.0, 0.0, 0.0,
+                            0.0, 0.0, 0.0, ns, den);
+          if (kAux) den += iface_at<TP>(L, c);
+          if (den > 0.0) {
+            const double rv = kNegR ? -e : e;
+            const double jv = (ns - rv) / den;
+            res = (TP)(0.0 + omega * (jv - 0.0));
+          }
+          if (partials != nullptr && (m & M_FLUID)) zsum += (double)res * vol64(L, i, g.j[r], g.k);
         }
-        if (partials != nullptr && (m & M_FLUID)) zsum += (double)res * vol64(L, i, g.j, g.k);
+        out[c] = res;
       }
-      out[c] = res;
     }
   }
   if (partials != nullptr) {
@@ -471,7 +468,6 @@ __global__ void __launch_bounds__(kMK* kMJ)
 template <bool kCopy, bool kAux>
 struct SpmvOp {
   const LevelDev& L;
-  ColumnCoef cc;
   double* __restrict__ d_new;
   double* __restrict__ Ad;
   int outlet;
@@ -488,8 +484,8 @@ struct SpmvOp {
   }
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, unsigned m, double, double kxm, double kxp,
-                                       const V& val) {
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, unsigned m, double, double kxm,
+                                       double kxp, const RowCoef& rc, const V& val) {
     double x0;
     if (m & M_SOLID)
       x0 = 0.0;
@@ -501,7 +497,7 @@ struct SpmvOp {
     double o = 0.0;
     if (!(m & M_SOLID)) {
       double ns, den;
-      stencil_sel<kAux>(L, cc, kxm, kxp, i, j, k, c, m, outlet, dir(val, -1, 0, 0), dir(val, 1, 0, 0),
+      stencil_sel<kAux>(L, rc, kxm, kxp, i, j, k, c, m, outlet, dir(val, -1, 0, 0), dir(val, 1, 0, 0),
                         dir(val, 0, -1, 0), dir(val, 0, 1, 0), dir(val, 0, 0, -1), dir(val, 0, 0, 1), ns, den);
       o = (den + (kAux ? iface_at<double>(L, c) : 0.0)) * x0 - ns;
     }
@@ -509,17 +505,17 @@ struct SpmvOp {
     if (m & M_FLUID) part += x0 * o * vol64(L, i, j, k);
   }
   __device__ __forceinline__ void plane_end(const MarchGeom&, int) {}
+  __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
 template <bool kCopy, bool kAux>
-__global__ void __launch_bounds__(kMK* kMJ)
+__global__ void __launch_bounds__(kMK* kTY)
     km_spmv_dir(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_z,
                 const __grid_constant__ CUtensorMap map_d, const __grid_constant__ CUtensorMap map_m,
                 double* __restrict__ d_new, double* __restrict__ Ad, int outlet, double* partials, CgScalars* sc) {
   MarchGeom g;
   const bool any = march_geom(L, chunk, g);
-  SpmvOp<kCopy, kAux> op{L, column_coef(L, g.jc, g.kc), d_new, Ad, outlet, kCopy ? 0.0 : sc->beta, sc->mean_z,
-                         sc->zproj, 0.0};
+  SpmvOp<kCopy, kAux> op{L, d_new, Ad, outlet, kCopy ? 0.0 : sc->beta, sc->mean_z, sc->zproj, 0.0};
   bool ok = true;
   if (any) {
     if (kCopy) {
@@ -549,88 +545,94 @@ __global__ void __launch_bounds__(kMK* kMJ)
 
 // ---------------------------------------------------------------------------
 // Residual restriction (fluid.py:5262-5388): the fine residual of every row
-// is formed in the march and staged in shared memory; the threads owning a
-// coarse cell accumulate its 2 x 2 x 2 children in the reference's order
-// (i-pair outer, then j, then k) with the f32 volume weights, across the two
-// planes of the pair.
+// is formed in the march and staged in shared memory (double-buffered by
+// plane parity); one plane behind, the threads owning a coarse cell
+// accumulate its 2 x 2 x 2 children in the reference's order (i-pair outer,
+// then j, then k) with the f32 volume weights, across the two planes of the
+// pair.
 // ---------------------------------------------------------------------------
 template <typename TP, bool kNegR, bool kAux>
 struct RestrictOp {
   const LevelDev& L;
-  ColumnCoef cc;
   int outlet;
   int cnx, cny, cnz;
   float* __restrict__ crhs;
-  double (*rs)[kMK];
-  unsigned char (*rsolid)[kMK];
+  double (*rs)[kMJ * kMK];          // [2][tile]: fine residuals of planes by parity
+  unsigned char (*rsolid)[kMJ * kMK];
   float wres, free_vol;
   int ocount;
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, unsigned m, double e, double kxm, double kxp,
-                                       const V& val) {
-    const int ty = (int)threadIdx.y, tx = (int)threadIdx.x;
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int t, unsigned m, double e, double kxm,
+                                       double kxp, const RowCoef& rc, const V& val) {
     if (m & M_SOLID) {
-      rsolid[ty][tx] = 1;
-      rs[ty][tx] = 0.0;
+      rsolid[i & 1][t] = 1;
+      rs[i & 1][t] = 0.0;
       return;
     }
     double ns, den;
-    stencil_sel<kAux>(L, cc, kxm, kxp, i, j, k, c, m, outlet, val(0, -1, 0, 0), val(0, 1, 0, 0), val(0, 0, -1, 0),
+    stencil_sel<kAux>(L, rc, kxm, kxp, i, j, k, c, m, outlet, val(0, -1, 0, 0), val(0, 1, 0, 0), val(0, 0, -1, 0),
                       val(0, 0, 1, 0), val(0, 0, 0, -1), val(0, 0, 0, 1), ns, den);
     if (kAux) den += iface_at<TP>(L, c);
     const double applied = ns - den * val(0, 0, 0, 0);
     const double rv = kNegR ? -e : e;
-    rsolid[ty][tx] = 0;
-    rs[ty][tx] = (double)(TP)(rv - applied);
+    rsolid[i & 1][t] = 0;
+    rs[i & 1][t] = (double)(TP)(rv - applied);
   }
-  __device__ __forceinline__ void plane_end(const MarchGeom& g, int i) {
-    __syncthreads();
-    if (g.tx < kMK / 2 && g.ty < kMJ / 2) {
-      const int fj0 = g.j0 + 2 * g.ty, fk0 = g.k0 + 2 * g.tx;
+  // Owners (tx < 16, every thread row) fold fine plane q into their coarse cell.
+  __device__ __forceinline__ void accumulate(const MarchGeom& g, int q) {
+    if (g.tx >= kMK / 2) return;
+    const int fj0 = g.j0 + 2 * g.ty, fk0 = g.k0 + 2 * g.tx;
 #pragma unroll
-      for (int oj = 0; oj < 2; ++oj)
+    for (int oj = 0; oj < 2; ++oj)
 #pragma unroll
-        for (int ok = 0; ok < 2; ++ok) {
-          const int fj = fj0 + oj, fk = fk0 + ok;
-          if (fj < L.ny && fk < L.nz) {
-            if (rsolid[2 * g.ty + oj][2 * g.tx + ok]) {
-              ocount += 1;
-            } else {
-              const float vol = __fmul_rn(__fmul_rn(__ldg(L.wx + i), __ldg(L.wy + fj)), __ldg(L.wz + fk));
-              const double r = rs[2 * g.ty + oj][2 * g.tx + ok];
-              if (sizeof(TP) == 8)
-                wres = (float)__dadd_rn((double)wres, __dmul_rn(r, (double)vol));
-              else
-                wres = __fadd_rn(wres, __fmul_rn((float)r, vol));
-              free_vol = __fadd_rn(free_vol, vol);
-            }
+      for (int ok = 0; ok < 2; ++ok) {
+        const int fj = fj0 + oj, fk = fk0 + ok;
+        if (fj < L.ny && fk < L.nz) {
+          const int t = (2 * g.ty + oj) * kMK + 2 * g.tx + ok;
+          if (rsolid[q & 1][t]) {
+            ocount += 1;
+          } else {
+            const float vol = __fmul_rn(__fmul_rn(__ldg(L.wx + q), __ldg(L.wy + fj)), __ldg(L.wz + fk));
+            const double r = rs[q & 1][t];
+            if (sizeof(TP) == 8)
+              wres = (float)__dadd_rn((double)wres, __dmul_rn(r, (double)vol));
+            else
+              wres = __fadd_rn(wres, __fmul_rn((float)r, vol));
+            free_vol = __fadd_rn(free_vol, vol);
           }
         }
-      if ((i & 1) || i == L.nx - 1) {
-        const int ci = i >> 1, cj = fj0 >> 1, ck = fk0 >> 1;
-        if (ci < cnx && cj < cny && ck < cnz)
-          crhs[cidx(ci, cj, ck, cny, cnz)] = ocount > 0 ? 0.0f : __fdiv_rn(wres, fmaxf(free_vol, 1.0e-30f));
-        wres = 0.0f;
-        free_vol = 0.0f;
-        ocount = 0;
       }
+    if ((q & 1) || q == L.nx - 1) {
+      const int ci = q >> 1, cj = fj0 >> 1, ck = fk0 >> 1;
+      if (ci < cnx && cj < cny && ck < cnz)
+        crhs[cidx(ci, cj, ck, cny, cnz)] = ocount > 0 ? 0.0f : __fdiv_rn(wres, fmaxf(free_vol, 1.0e-30f));
+      wres = 0.0f;
+      free_vol = 0.0f;
+      ocount = 0;
     }
+  }
+  // plane i-1 was staged before the previous block barrier
+  __device__ __forceinline__ void plane_end(const MarchGeom& g, int i) {
+    if (i > g.ib) accumulate(g, i - 1);
+  }
+  __device__ __forceinline__ void finish(const MarchGeom& g) {
+    __syncthreads();
+    accumulate(g, g.ie - 1);
   }
 };
 
 template <typename TP, bool kNegR, bool kAux>
-__global__ void __launch_bounds__(kMK* kMJ)
+__global__ void __launch_bounds__(kMK* kTY)
     km_restrict(LevelDev F, int chunk, const __grid_constant__ CUtensorMap map_p,
                 const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m, int outlet,
                 int cnx, int cny, int cnz, float* __restrict__ crhs, CgScalars* sc) {
   using TR = typename std::conditional<kNegR, double, TP>::type;
-  __shared__ double rs[kMJ][kMK];
-  __shared__ unsigned char rsolid[kMJ][kMK];
+  __shared__ double rs[2][kMJ * kMK];
+  __shared__ unsigned char rsolid[2][kMJ * kMK];
   MarchGeom g;
   const bool any = march_geom(F, chunk, g);
-  RestrictOp<TP, kNegR, kAux> op{F, column_coef(F, g.jc, g.kc), outlet, cnx, cny, cnz, crhs, rs, rsolid,
-                                 0.0f, 0.0f, 0};
+  RestrictOp<TP, kNegR, kAux> op{F, outlet, cnx, cny, cnz, crhs, rs, rsolid, 0.0f, 0.0f, 0};
   const CUtensorMap* const mv[1] = {&map_p};
   if (any && !march<TP, 1, TR, true>(F, g, mv, &map_r, &map_m, op)) report_fault(sc);
 }
