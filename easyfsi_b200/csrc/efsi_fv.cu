@@ -1486,6 +1486,10 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
     B.shape = shape3(B.nx, B.ny, B.nz);
     max_blocks = std::max<size_t>(max_blocks, B.shape.nblocks());
     {
+      const dim3 g0 = sweep0_grid(B.nx, B.ny, B.nz);
+      max_blocks = std::max<size_t>(max_blocks, (size_t)g0.x * g0.y * g0.z);
+    }
+    {
       int dev = 0, nsm = 148;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1854,8 +1858,8 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   const LevelBuf& B = P->lv[l];
   const dim3 blk(kMK, kTY);
   if (kZero) {
-    EFSI_COUNTED km_sweep0<TP, kNegR, kAux><<<B.mgrid, blk, 0, s>>>(L, B.mchunk, rhs, out, outlet, om, partials,
-                                                                     P->sc);
+    EFSI_COUNTED km_sweep0<TP, kNegR, kAux><<<sweep0_grid(B.nx, B.ny, B.nz), blk, 0, s>>>(L, rhs, out, outlet, om,
+                                                                                           partials, P->sc);
     return true;
   }
   const CUtensorMap* mp = plane_map(P, l, p, MAP_VALUE);

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <utility>
 
 #include "efsi_common.cuh"
 
@@ -29,6 +30,7 @@ struct efsi_bin_plan {
   int32_t* count = nullptr;
   int32_t* offset = nullptr;
   int32_t* cursor = nullptr;
+  int32_t* tile_sums = nullptr;  // per-tile bin counts of the offset scan
 };
 
 namespace efsi {
@@ -222,28 +224,75 @@ __global__ void k_bin_count(BinView B, const float* x, int P, int32_t* key, int3
   if ((threadIdx.x & 31) == leader) atomicAdd(count + kk, __popc(peers));
 }
 
-__global__ void k_bin_scan(const int32_t* count, int n, int32_t* offset, int32_t* cursor) {
-  __shared__ int32_t part[1024];
-  const int t = threadIdx.x;
-  const int per = (n + 1023) / 1024;
-  const int lo = t * per, hi = min(n, lo + per);
-  int32_t s = 0;
-  for (int q = lo; q < hi; ++q) s += count[q];
-  part[t] = s;
+// Bin offsets by a two-pass scan over tiles of kScanTile counts: per-tile
+// totals, then every tile scans itself after summing the totals before it.
+constexpr int kScanThreads = 1024, kScanPer = 4, kScanTile = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int32_t block_exclusive_scan(int32_t v, int32_t* warp_tot, int32_t& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[w] = x;
   __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {
-    int32_t v = t >= o ? part[t - o] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
+  if (w == 0) {
+    int32_t t = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    warp_tot[lane] = t;  // inclusive over warps
   }
-  int32_t run = part[t] - s;
-  for (int q = lo; q < hi; ++q) {
-    offset[q] = run;
-    cursor[q] = 0;
-    run += count[q];
+  __syncthreads();
+  total = warp_tot[31];
+  const int32_t before = w > 0 ? warp_tot[w - 1] : 0;
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_bin_tile_sums(const int32_t* count, int n, int32_t* tile_sums) {
+  __shared__ int32_t warp_tot[32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
+  int32_t s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanPer; ++q) s += base + q < n ? count[base + q] : 0;
+  int32_t total;
+  block_exclusive_scan(s, warp_tot, total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_bin_offsets(const int32_t* count, int n, const int32_t* tile_sums,
+                                                              int32_t* offset, int32_t* cursor) {
+  __shared__ int32_t warp_tot[32];
+  __shared__ int32_t carry;
+  if (threadIdx.x < 32) {
+    int32_t c = 0;
+    for (int t = threadIdx.x; t < (int)blockIdx.x; t += 32) c += tile_sums[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (threadIdx.x == 0) carry = c;
   }
-  if (t == 1023) offset[n] = part[1023];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
+  int32_t v[kScanPer], s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanPer; ++q) {
+    v[q] = base + q < n ? count[base + q] : 0;
+    s += v[q];
+  }
+  int32_t total;
+  int32_t run = block_exclusive_scan(s, warp_tot, total) + carry;
+#pragma unroll
+  for (int q = 0; q < kScanPer; ++q) {
+    if (base + q < n) {
+      offset[base + q] = run;
+      cursor[base + q] = 0;
+    }
+    run += v[q];
+  }
+  if (base <= n - 1 && n - 1 < base + kScanPer) offset[n] = run;  // the grand total
 }
 
 __global__ void k_bin_fill(int P, const int32_t* key, const int32_t* offset, int32_t* cursor, int32_t* sorted) {
@@ -254,19 +303,18 @@ __global__ void k_bin_fill(int P, const int32_t* key, const int32_t* offset, int
   sorted[offset[kk] + slot] = p;
 }
 
-// Restores particle order inside every bin (insertion sort; bins are small),
-// so the spreading sums are reproducible run to run.
-__global__ void k_bin_order(int nbins, const int32_t* offset, int32_t* sorted) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+// Restores particle order inside every bin, so the spreading sums are
+// reproducible run to run: one warp per bin places each entry at its rank
+// (the number of smaller particle indices in the bin).
+__global__ void k_bin_rank(int nbins, const int32_t* offset, const int32_t* in, int32_t* out) {
+  const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
   if (b >= nbins) return;
   const int lo = offset[b], hi = offset[b + 1];
-  for (int q = lo + 1; q < hi; ++q) {
-    int v = sorted[q], r = q - 1;
-    while (r >= lo && sorted[r] > v) {
-      sorted[r + 1] = sorted[r];
-      --r;
-    }
-    sorted[r + 1] = v;
+  for (int q = lo + lane; q < hi; q += 32) {
+    const int32_t v = in[q];
+    int rank = 0;
+    for (int r = lo; r < hi; ++r) rank += in[r] < v;
+    out[lo + rank] = v;
   }
 }
 
@@ -278,8 +326,10 @@ __device__ __forceinline__ float tent(const float* xm, const float* xp, float R)
   return w;
 }
 
+// Visits the particles of the 3 x 3 x 3 bins around xm; lane `lane` of the
+// calling warp takes every 32nd particle of each bin (in bin order).
 template <class Fn>
-__device__ __forceinline__ void for_near(const BinView& B, const float* xm, Fn fn) {
+__device__ __forceinline__ void for_near(const BinView& B, const float* xm, int lane, Fn fn) {
   int c[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) c[a] = bin_axis(xm[a], B.bmin[a], B.invR, B.nb[a]);
@@ -293,31 +343,43 @@ __device__ __forceinline__ void for_near(const BinView& B, const float* xm, Fn f
         int b2 = c[2] + d2;
         if (b2 < 0 || b2 >= B.nb[2]) continue;
         const int bin = (b0 * B.nb[1] + b1) * B.nb[2] + b2;
-        const int lo = B.offset[bin], hi = B.offset[bin + 1];
-        for (int q = lo; q < hi; ++q) fn(B.sorted[q]);
+        const int lo = __ldg(B.offset + bin), hi = __ldg(B.offset + bin + 1);
+        for (int q = lo + lane; q < hi; q += 32) fn(__ldg(B.sorted + q));
       }
     }
   }
 }
 
-// hibm_mpm.py:4899-4959 _scatter_marker_forces_to_mpm_particles_kernel.
+// Butterfly sums over the warp: every lane gets the same total, summed in a
+// fixed order (reproducible run to run).
+__device__ __forceinline__ float warp_allsum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// hibm_mpm.py:4899-4959 _scatter_marker_forces_to_mpm_particles_kernel: one
+// warp per marker; the tent-weight sum over the marker's neighbourhood is a
+// warp reduction, then every lane spreads F * w / wsum to its particles.
 __global__ void k_scatter(BinView B, int M, const float* xg, const double* Fg, const float* xp, float* fext,
                           double* rep) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= M) return;
-  const float* xm = xg + 3 * m;
-  const double* Fm = Fg + 3 * m;
+  const int m = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
+  if (m >= M) return;  // uniform over the warp
+  const float xm[3] = {__ldg(xg + 3 * m), __ldg(xg + 3 * m + 1), __ldg(xg + 3 * m + 2)};
+  const double Fm[3] = {__ldg(Fg + 3 * m), __ldg(Fg + 3 * m + 1), __ldg(Fg + 3 * m + 2)};
   const bool valid = finite3(xm) && isfinite(Fm[0]) && isfinite(Fm[1]) && isfinite(Fm[2]);
-  float wsum = 0.0f;
   const float R = B.R;
-  if (valid) for_near(B, xm, [&](int p) { wsum += tent(xm, xp + 3 * p, R); });
+  float wl = 0.0f;
+  if (valid) for_near(B, xm, lane, [&](int p) { wl += tent(xm, xp + 3 * p, R); });
+  const float wsum = warp_allsum(wl);
   if (valid && wsum > 1.0e-12f) {
-    atomicAdd(rep + 0, 1.0);
-    atomicAdd(rep + 3, Fm[0]);
-    atomicAdd(rep + 4, Fm[1]);
-    atomicAdd(rep + 5, Fm[2]);
     double e0 = 0, e1 = 0, e2 = 0, contrib = 0;
-    for_near(B, xm, [&](int p) {
+    for_near(B, xm, lane, [&](int p) {
       float w = tent(xm, xp + 3 * p, R);
       if (w > 0.0f) {
         const double ratio = (double)(w / wsum);
@@ -331,32 +393,44 @@ __global__ void k_scatter(BinView B, int M, const float* xg, const double* Fg, c
         contrib += 1.0;
       }
     });
-    atomicAdd(rep + 2, contrib);
-    atomicAdd(rep + 6, e0);
-    atomicAdd(rep + 7, e1);
-    atomicAdd(rep + 8, e2);
-  } else {
+    e0 = warp_allsum(e0);
+    e1 = warp_allsum(e1);
+    e2 = warp_allsum(e2);
+    contrib = warp_allsum(contrib);
+    if (lane == 0) {
+      atomicAdd(rep + 0, 1.0);
+      atomicAdd(rep + 3, Fm[0]);
+      atomicAdd(rep + 4, Fm[1]);
+      atomicAdd(rep + 5, Fm[2]);
+      atomicAdd(rep + 2, contrib);
+      atomicAdd(rep + 6, e0);
+      atomicAdd(rep + 7, e1);
+      atomicAdd(rep + 8, e2);
+    }
+  } else if (lane == 0) {
     atomicAdd(rep + 1, 1.0);
   }
 }
 
-// hibm_mpm.py:5097-5180 / 5012-5053 surface feedback.
+// hibm_mpm.py:5097-5180 / 5012-5053 surface feedback: one warp per marker,
+// tent-weighted sums of particle velocity (and normal / area) as warp
+// reductions.
 __global__ void k_feedback(BinView B, int M, float* xg, float* vg, float* ng, float* Ag, const float* xp,
                            const float* vp, const float* np_, const float* ap, float dt, double* rep) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= M) return;
+  const int m = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
+  if (m >= M) return;  // uniform over the warp
   const bool geometry = np_ != nullptr && ap != nullptr;
   const float xo[3] = {xg[3 * m], xg[3 * m + 1], xg[3 * m + 2]};
   const float no[3] = {ng[3 * m], ng[3 * m + 1], ng[3 * m + 2]};
   const float ao = Ag[m];
   float vs[3] = {0, 0, 0}, ns[3] = {0, 0, 0}, as = 0.0f, ws = 0.0f, gs = 0.0f;
   const float R = B.R;
-  for_near(B, xo, [&](int p) {
+  for_near(B, xo, lane, [&](int p) {
     float w = tent(xo, xp + 3 * p, R);
     if (w > 0.0f) {
-      vs[0] += w * vp[3 * p];
-      vs[1] += w * vp[3 * p + 1];
-      vs[2] += w * vp[3 * p + 2];
+      vs[0] += w * __ldg(vp + 3 * p);
+      vs[1] += w * __ldg(vp + 3 * p + 1);
+      vs[2] += w * __ldg(vp + 3 * p + 2);
       ws += w;
       if (geometry) {
         const float* pn = np_ + 3 * p;
@@ -370,6 +444,15 @@ __global__ void k_feedback(BinView B, int M, float* xg, float* vg, float* ng, fl
       }
     }
   });
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    vs[a] = warp_allsum(vs[a]);
+    ns[a] = warp_allsum(ns[a]);
+  }
+  as = warp_allsum(as);
+  ws = warp_allsum(ws);
+  gs = warp_allsum(gs);
+  if (lane != 0) return;
   if (ws > 1.0e-12f) {
     float nv[3], nx[3];
     for (int a = 0; a < 3; ++a) {
@@ -490,7 +573,8 @@ int efsi_bin_plan_create(int32_t capacity, const float* box_min, const float* bo
       cudaMalloc(&P->sorted, capacity * sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&P->count, (P->nbins + 1) * sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&P->offset, (P->nbins + 2) * sizeof(int32_t)) != cudaSuccess ||
-      cudaMalloc(&P->cursor, (P->nbins + 1) * sizeof(int32_t)) != cudaSuccess) {
+      cudaMalloc(&P->cursor, (P->nbins + 1) * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&P->tile_sums, ((P->nbins + 1) / kScanTile + 1) * sizeof(int32_t)) != cudaSuccess) {
     efsi_bin_plan_destroy(P);
     set_error("cudaMalloc failed for the bin plan");
     return EFSI_ERR_CUDA;
@@ -506,6 +590,7 @@ int efsi_bin_plan_destroy(efsi_bin_plan* P) {
   cudaFree(P->count);
   cudaFree(P->offset);
   cudaFree(P->cursor);
+  cudaFree(P->tile_sums);
   delete P;
   return EFSI_OK;
 }
@@ -518,9 +603,15 @@ int efsi_bin_particles(efsi_bin_plan* P, const float* particle_x, int32_t partic
   EFSI_CUDA_CHECK(cudaMemsetAsync(P->count, 0, (P->nbins + 1) * sizeof(int32_t), s));
   const unsigned pb = (particle_count + 255) / 256;
   EFSI_COUNTED k_bin_count<<<pb, 256, 0, s>>>(B, particle_x, particle_count, P->key, P->count);
-  EFSI_COUNTED k_bin_scan<<<1, 1024, 0, s>>>(P->count, P->nbins + 1, P->offset, P->cursor);
+  const int nc = P->nbins + 1;
+  const unsigned tiles = (unsigned)((nc + kScanTile - 1) / kScanTile);
+  EFSI_COUNTED k_bin_tile_sums<<<tiles, kScanThreads, 0, s>>>(P->count, nc, P->tile_sums);
+  EFSI_COUNTED k_bin_offsets<<<tiles, kScanThreads, 0, s>>>(P->count, nc, P->tile_sums, P->offset, P->cursor);
+  // unordered fill into the key buffer (no longer needed), ordered copy into `sorted`
   EFSI_COUNTED k_bin_fill<<<pb, 256, 0, s>>>(particle_count, P->key, P->offset, P->cursor, P->sorted);
-  EFSI_COUNTED k_bin_order<<<(P->nbins + 255) / 256, 256, 0, s>>>(P->nbins, P->offset, P->sorted);
+  std::swap(P->key, P->sorted);
+  EFSI_COUNTED k_bin_rank<<<(unsigned)(((int64_t)P->nbins * 32 + 255) / 256), 256, 0, s>>>(P->nbins, P->offset,
+                                                                                          P->key, P->sorted);
   EFSI_LAUNCH_CHECK();
   P->count_last = particle_count;
   return EFSI_OK;
@@ -533,8 +624,8 @@ int efsi_scatter_marker_forces(efsi_bin_plan* P, int32_t marker_count, const flo
   cudaStream_t s = as_stream(stream);
   EFSI_CUDA_CHECK(cudaMemsetAsync(report_device, 0, 9 * sizeof(double), s));
   if (marker_count <= 0) return EFSI_OK;
-  EFSI_COUNTED k_scatter<<<(marker_count + 127) / 128, 128, 0, s>>>(bin_view(P), marker_count, x_gamma, f_gamma, particle_x,
-                                                       external_force, report_device);
+  EFSI_COUNTED k_scatter<<<(marker_count + 7) / 8, 256, 0, s>>>(bin_view(P), marker_count, x_gamma, f_gamma,
+                                                                  particle_x, external_force, report_device);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
@@ -548,9 +639,9 @@ int efsi_surface_feedback(efsi_bin_plan* P, int32_t marker_count, float* x_gamma
   cudaStream_t s = as_stream(stream);
   EFSI_CUDA_CHECK(cudaMemsetAsync(report_device, 0, 8 * sizeof(double), s));
   if (marker_count <= 0) return EFSI_OK;
-  EFSI_COUNTED k_feedback<<<(marker_count + 127) / 128, 128, 0, s>>>(bin_view(P), marker_count, x_gamma, v_gamma, n_gamma,
-                                                        area_gamma, particle_x, particle_v, particle_normal,
-                                                        particle_area, dt, report_device);
+  EFSI_COUNTED k_feedback<<<(marker_count + 7) / 8, 256, 0, s>>>(bin_view(P), marker_count, x_gamma, v_gamma,
+                                                                   n_gamma, area_gamma, particle_x, particle_v,
+                                                                   particle_normal, particle_area, dt, report_device);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }

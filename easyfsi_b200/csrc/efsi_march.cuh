@@ -232,7 +232,9 @@ struct StageLayout {
 // kxm, kxp, rc, val)` computes one cell (t: its index in the tile), reading
 // the field through val(v, di, dj, dk) (value tile v at (i+di, j+dj, k+dk));
 // `Op::plane_end(g, i)` runs before the plane's block barrier and
-// `Op::finish(g)` after the last plane.  Returns false (in every thread) if a
+// `Op::finish(g)` after the last plane.  With Op::kPrepare, every stage is
+// first passed to `Op::prepare(g, value_tile, mask_tile, plane)` (all threads,
+// in place; the mask tile is null for the halo planes) once it has landed.  Returns false (in every thread) if a
 // stage did not land in time; the kernel then reports it through
 // `sc->fault`.
 template <typename TV, int NV, typename TR, bool kR, class Op>
@@ -265,8 +267,19 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
   int issued = min(g.ie, g.ib - 1 + kStages - 1);  // last plane in flight
   if (leader)
     for (int p = g.ib - 1; p <= issued; ++p) issue(p, p - g.ib + 1);
+  auto vtile = [&](int s) { return reinterpret_cast<TV*>(base + s * Lay::kStage); };
+  auto mtile = [&](int s) { return reinterpret_cast<const uint8_t*>(base + s * Lay::kStage + Lay::kMOff); };
   bool fail = !mbar_wait(&bar[0], 0u);
   if (!fail) fail = !mbar_wait(&bar[1], 0u);
+  if (Op::kPrepare) {
+    // planes ib-1 (a halo plane: no mask tile) and ib
+    if (!fail) {
+      op.prepare(g, vtile(0), nullptr, g.ib - 1);
+      op.prepare(g, vtile(1), mtile(1), g.ib);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+  }
   int s_m = 0, s_0 = 1, s_p = 2 % kStages;  // stages of planes i-1, i, i+1
   unsigned ph_p = 0;                        // phase parity of plane i+1
   const int64_t sx = (int64_t)L.ny * L.nz;
@@ -277,6 +290,11 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
   int64_t pbase = (int64_t)g.ib * sx;
   for (int i = g.ib; i < g.ie; ++i, pbase += sx) {
     if (!fail) fail = !mbar_wait(&bar[s_p], ph_p);
+    if (Op::kPrepare) {
+      if (!fail) op.prepare(g, vtile(s_p), i + 1 < g.ie ? mtile(s_p) : nullptr, i + 1);
+      fence_proxy_async_smem();  // these generic writes precede the stage's next TMA refill
+      __syncthreads();
+    }
     if (!fail) {
       const double kxm = __ldg(L.cxm + i), kxp = __ldg(L.cxp + i);
       const TV* vt[3][NV];
@@ -354,25 +372,31 @@ struct SweepOp {
     return (double)__fadd_rn((float)v, corr);
   }
 
+  // The prolongation is applied to each landed value tile once: tile cells
+  // by their own mask, halo cells (reached only through open faces, hence
+  // fluid) unconditionally.  Coarse indices are clamped, so cells outside the
+  // level take an in-level coarse value that is never used.
+  static constexpr bool kPrepare = kProlong;
+  __device__ __forceinline__ void prepare(const MarchGeom& g, TP* tile, const uint8_t* mtile, int plane) const {
+    using Lay = StageLayout<TP, 1, TP, true>;
+    constexpr int kCols = kMK + 2, kCells = (kMJ + 2) * kCols;
+    const int ip = min(max(plane, 0), L.nx - 1);
+    for (int e = g.ty * kMK + g.tx; e < kCells; e += kMK * kTY) {
+      const int r = e / kCols, cc = e - r * kCols;
+      const bool inner = r >= 1 && r <= kMJ && cc >= 1 && cc <= kMK;
+      if (inner && mtile != nullptr && !(mtile[(r - 1) * kMK + cc - 1] & M_FLUID)) continue;
+      TP* v = tile + r * Lay::kW + Lay::kPad - 1 + cc;
+      *v = (TP)prolonged((double)*v, ip, max(g.j0 - 1 + r, 0), max(g.k0 - 1 + cc, 0));
+    }
+  }
+
   template <class V>
   __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, unsigned m, double e, double kxm,
                                        double kxp, const RowCoef& rc, const V& val) {
     TP res = (TP)0;
     if (!(m & M_SOLID)) {
-      double x0 = val(0, 0, 0, 0), xm = val(0, -1, 0, 0), xp = val(0, 1, 0, 0);
-      double ym = val(0, 0, -1, 0), yp = val(0, 0, 1, 0), zm = val(0, 0, 0, -1), zp = val(0, 0, 0, 1);
-      if (kProlong) {
-        // neighbours behind open faces are fluid; the centre by its own mask
-        // (indices are clamped, so a closed face at the level edge reads an
-        // in-level coarse value that is never used)
-        if (m & M_FLUID) x0 = prolonged(x0, i, j, k);
-        xm = prolonged(xm, max(i - 1, 0), j, k);
-        xp = prolonged(xp, i + 1, j, k);
-        ym = prolonged(ym, i, max(j - 1, 0), k);
-        yp = prolonged(yp, i, j + 1, k);
-        zm = prolonged(zm, i, j, max(k - 1, 0));
-        zp = prolonged(zp, i, j, k + 1);
-      }
+      const double x0 = val(0, 0, 0, 0), xm = val(0, -1, 0, 0), xp = val(0, 1, 0, 0);
+      const double ym = val(0, 0, -1, 0), yp = val(0, 0, 1, 0), zm = val(0, 0, 0, -1), zp = val(0, 0, 0, 1);
       double ns, den;
       stencil_sel<kAux>(L, rc, kxm, kxp, i, j, k, c, m, outlet, xm, xp, ym, yp, zm, zp, ns, den);
       if (kAux) den += iface_at<TP>(L, c);
@@ -412,40 +436,56 @@ __global__ void __launch_bounds__(kMK* kTY)
 }
 
 // First sweep from a zero iterate: out = omega * (0 - rhs) / den per row; no
-// neighbour values are needed, so this is a plain streaming pass.
+// neighbour values are needed, so this is a plain streaming pass: a 32 x 8
+// block per (k, j) tile and four planes, every thread's loads issued before
+// its arithmetic.
+constexpr int kSweep0Planes = 4;
+
+inline dim3 sweep0_grid(int nx, int ny, int nz) {
+  return dim3((unsigned)((nz + kMK - 1) / kMK), (unsigned)((ny + kTY - 1) / kTY),
+              (unsigned)((nx + kSweep0Planes - 1) / kSweep0Planes));
+}
+
 template <typename TP, bool kNegR, bool kAux>
 __global__ void __launch_bounds__(kMK* kTY)
-    km_sweep0(LevelDev L, int chunk, const void* rhs, TP* __restrict__ out, int outlet, double omega,
-              double* partials, CgScalars* sc) {
-  MarchGeom g;
+    km_sweep0(LevelDev L, const void* rhs, TP* __restrict__ out, int outlet, double omega, double* partials,
+              CgScalars* sc) {
+  const int k = (int)(blockIdx.x * kMK + threadIdx.x), j = (int)(blockIdx.y * kTY + threadIdx.y);
+  const int i0 = (int)blockIdx.z * kSweep0Planes;
   double zsum = 0.0;
-  if (march_geom(L, chunk, g)) {
+  if (j < L.ny && k < L.nz) {
     const int64_t sx = (int64_t)L.ny * L.nz;
+    const int64_t c0 = (int64_t)i0 * sx + (int64_t)j * L.nz + k;
+    const RowCoef rc = row_coef(L, j, k);
+    const int n = min(kSweep0Planes, L.nx - i0);
+    unsigned m[kSweep0Planes];
+    double e[kSweep0Planes];
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      if (!g.active[r]) continue;
-      const RowCoef rc = row_coef(L, g.j[r], g.kc);
-#pragma unroll 4
-      for (int i = g.ib; i < g.ie; ++i) {
-        const int64_t c = (int64_t)i * sx + g.off[r];
-        const unsigned m = __ldg(L.mask + c);
-        const double e = kNegR ? __ldg(reinterpret_cast<const double*>(rhs) + c)
-                               : (double)__ldg(reinterpret_cast<const TP*>(rhs) + c);
-        TP res = (TP)0;
-        if (!(m & M_SOLID)) {
-          double ns, den;
-          stencil_sel<kAux>(L, rc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, g.j[r], g.k, c, m, outlet, 0.0, 0.0, 0.0,
-                            0.0, 0.0, 0.0, ns, den);
-          if (kAux) den += iface_at<TP>(L, c);
-          if (den > 0.0) {
-            const double rv = kNegR ? -e : e;
-            const double jv = (ns - rv) / den;
-            res = (TP)(0.0 + omega * (jv - 0.0));
-          }
-          if (partials != nullptr && (m & M_FLUID)) zsum += (double)res * vol64(L, i, g.j[r], g.k);
+    for (int q = 0; q < kSweep0Planes; ++q) {
+      if (q >= n) break;
+      m[q] = __ldg(L.mask + c0 + q * sx);
+      e[q] = kNegR ? __ldg(reinterpret_cast<const double*>(rhs) + c0 + q * sx)
+                   : (double)__ldg(reinterpret_cast<const TP*>(rhs) + c0 + q * sx);
+    }
+#pragma unroll
+    for (int q = 0; q < kSweep0Planes; ++q) {
+      if (q >= n) break;
+      const int i = i0 + q;
+      const int64_t c = c0 + q * sx;
+      TP res = (TP)0;
+      if (!(m[q] & M_SOLID)) {
+        double ns, den;
+        stencil_sel<kAux>(L, rc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, j, k, c, m[q], outlet, 0.0, 0.0, 0.0, 0.0,
+                          0.0, 0.0, ns, den);
+        if (kAux) den += iface_at<TP>(L, c);
+        if (den > 0.0) {
+          const double rv = kNegR ? -e[q] : e[q];
+          const double jv = (ns - rv) / den;
+          res = (TP)(0.0 + omega * (jv - 0.0));
         }
-        out[c] = res;
+        if (partials != nullptr && (m[q] & M_FLUID)) zsum += (double)res * vol64(L, i, j, k);
       }
+      out[c] = res;
     }
   }
   if (partials != nullptr) {
@@ -467,6 +507,9 @@ __global__ void __launch_bounds__(kMK* kTY)
 // ---------------------------------------------------------------------------
 template <bool kCopy, bool kAux>
 struct SpmvOp {
+  static constexpr bool kPrepare = false;
+  template <typename T>
+  __device__ __forceinline__ void prepare(const MarchGeom&, T*, const uint8_t*, int) const {}
   const LevelDev& L;
   double* __restrict__ d_new;
   double* __restrict__ Ad;
@@ -553,6 +596,9 @@ __global__ void __launch_bounds__(kMK* kTY)
 // ---------------------------------------------------------------------------
 template <typename TP, bool kNegR, bool kAux>
 struct RestrictOp {
+  static constexpr bool kPrepare = false;
+  template <typename T>
+  __device__ __forceinline__ void prepare(const MarchGeom&, T*, const uint8_t*, int) const {}
   const LevelDev& L;
   int outlet;
   int cnx, cny, cnz;
