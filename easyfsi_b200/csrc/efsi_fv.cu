@@ -2094,6 +2094,10 @@ struct PcgRun {
 static int read_scalars(PcgRun& R) {
   EFSI_CUDA_CHECK(cudaMemcpyAsync(R.P->host_sc, R.P->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, R.s));
   EFSI_CUDA_CHECK(cudaStreamSynchronize(R.s));
+  if (R.P->host_sc->fault) {
+    set_error("a plane-marching kernel's TMA stage did not complete in time");
+    return EFSI_ERR_CUDA;
+  }
   return EFSI_OK;
 }
 
