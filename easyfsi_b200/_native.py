@@ -112,6 +112,7 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_fv_diagonal": [P, P, I, P],
     "efsi_apply_jacobi_preconditioner": [P, P, P, P, P],
     "efsi_weighted_dot": [P, P, P, POINTER(c_double), P],
+    "efsi_weighted_dot_noalloc": [I, I, I, P, P, P, P, P, P, P, P],
     "efsi_fv_jacobi_sweep": [P, I, P, P, P, I, D, P],
     "efsi_fv_residual": [P, I, P, P, P, I, P],
     "efsi_mg_restrict": [P, I, P, P, P, P, P, P, P],

@@ -111,6 +111,17 @@ int efsi_apply_jacobi_preconditioner(efsi_fv_plan* plan, const double* diag, con
  * deterministic order).  Synchronises the stream and writes the host result. */
 int efsi_weighted_dot(efsi_fv_plan* plan, const double* a, const double* b, double* result_host, void* stream);
 
+/* No counterpart in the reference: the same fluid-weighted dot (fluid =
+ * obstacle == 0, V = wx[i] wy[j] wz[k]) with no plan and no allocation; its
+ * reduction scratch is a static device array of the library, so at most
+ * 268435456 cells (larger grids return EFSI_ERR_ARG) and calls on one device
+ * must not overlap.  The first call on a device resolves that scratch (and
+ * may load the module): make it before any stream capture.  Writes the total
+ * to result_device without synchronising. */
+int efsi_weighted_dot_noalloc(int32_t nx, int32_t ny, int32_t nz, const int32_t* obstacle, const float* wx,
+                              const float* wy, const float* wz, const double* a, const double* b,
+                              double* result_device, void* stream);
+
 /* fluid.py:4224-4273 _pressure_fv_jacobi_kernel, one out-of-place sweep on
  * level `level` (level 0: double arrays, coarse levels: float arrays).  rhs
  * and iface follow the level's storage type. */
