@@ -115,6 +115,24 @@ class ClockSampler:
         }
 
 
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """Largest per-rank time over all ranks (every rank calls this in the same
+    order; a no-op for one rank)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_steps_per_s(world: int, steps: int, max_ms: float) -> float:
+    """Whole-job throughput of `world` independent replicas that each ran
+    `steps` steps, timed by the slowest rank."""
+    return world * steps / (max_ms / 1000.0)
+
+
 def cpu_reference(cfg, steps: int, warmup: int, initial_velocity=None) -> dict:
     """Time the CPU oracle's coupled step (all host threads)."""
     from oracle import oracle as orc
@@ -242,11 +260,8 @@ def main() -> None:
             "launches_per_step": per_it * iters_mean,
             "ms_per_step": avg_ms * per_it * iters_mean,
         }
-    t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps / (max_ms / 1000.0)
+    max_ms = max_over_ranks(elapsed_ms, world, "cuda")
+    value = replica_steps_per_s(world, args.steps, max_ms)
 
     # --- e2e through the public API with host-resident state ---
     e2e = None
@@ -293,11 +308,9 @@ def main() -> None:
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        te = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
         e2e = {
-            "value": world * args.steps / (float(te.item()) / 1000.0),
+            "value": replica_steps_per_s(world, args.steps, e2e_ms),
             "unit": "steps/s",
             "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h),

@@ -215,6 +215,30 @@ class OracleFluid:
         return float(self.lib.efo_weighted_dot(byref(self.levels[0]), _p(self.obstacle), _p(np.ascontiguousarray(a, dtype=np.float64)),
                                                _p(np.ascontiguousarray(b, dtype=np.float64))))
 
+    def restrict(self, res: np.ndarray, iface=None, vdir_active=None, vdir_weight=None):
+        """Level 0 -> 1 restriction of a fine residual (fluid.py:5310-5388):
+        coarse rhs, interface diagonal, obstacle, Dirichlet flag and weight."""
+        C = self.levels[1]
+        shape = (C.nx, C.ny, C.nz)
+        crhs = np.zeros(shape, self.rt)
+        ciface = np.zeros(shape, self.rt)
+        cobs = np.zeros(shape, np.int32)
+        cva = np.zeros(shape, np.int32)
+        cvw = np.zeros(shape, self.rt)
+        self.lib.efo_mg_restrict_f64(byref(self.levels[0]), _p(np.ascontiguousarray(res, dtype=np.float64)), _p(iface),
+                                     _p(self.obstacle), _p(vdir_active), _p(vdir_weight), byref(C), _p(crhs), _p(ciface),
+                                     _p(cobs), _p(cva), _p(cvw))
+        return {"rhs": crhs, "iface": ciface, "obstacle": cobs, "vdir_active": cva, "vdir_weight": cvw}
+
+    def jacobi_sweep_coarse(self, level: int, p, rhs, iface, obstacle, omega: float, outlet: int = 0) -> np.ndarray:
+        """One damped-Jacobi sweep (fluid.py:4224-4273) on a coarse (f32) level."""
+        L = self.levels[level]
+        out = np.zeros((L.nx, L.ny, L.nz), self.rt)
+        args = [np.ascontiguousarray(a, dtype=self.rt) for a in (p, rhs, iface)]
+        self.lib.efo_jacobi_sweep_r32(byref(L), *(_p(a) for a in args), _p(np.ascontiguousarray(obstacle, dtype=np.int32)),
+                                      None, None, _p(out), c_int(outlet), c_double(omega))
+        return out
+
     def vcycle(self, r: np.ndarray, outlet: int = 0, pre: int = 2, coarse: int = 24, post: int = 2) -> np.ndarray:
         z = np.zeros_like(r, dtype=np.float64)
         self.lib.efo_mg_vcycle(c_int(len(self.metrics)), self.levels, _p(self.obstacle), None, None, None,

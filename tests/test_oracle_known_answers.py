@@ -1,0 +1,221 @@
+"""The reference's own known-answer cases, restated against the CPU oracle.
+
+Each case names the reference test it restates (tests/<file>:<line> in the
+reference tree) and keeps that test's inputs and bounds; where the oracle is
+exact in f64 the bound is tightened beside the reference's.  These pin the
+oracle before it is used as the GPU path's checker.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from easyfsi_b200.grid import CartesianGrid
+from easyfsi_b200.scenarios import graded_axis_widths
+from oracle import oracle as orc
+
+
+def _uniform_box(n):
+    w = [1.0 / n] * n
+    return CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=w, cell_widths_y_m=w, cell_widths_z_m=w)
+
+
+def _fluid(grid, variant="mirror"):
+    return orc.OracleFluid(grid, rho=1000.0, mu=1.0e-3, variant=variant)
+
+
+# test_core_fluid.py:1677 interface diagonal enters operator, diagonal and Jacobi
+def test_interface_diagonal_enters_operator_and_jacobi():
+    fl = _fluid(_uniform_box(5))
+    p = np.ones((5, 5, 5))
+    iface = np.zeros((5, 5, 5))
+    iface[2, 2, 2] = 7.5
+    applied = fl.fv_apply(p, 0, iface=iface)
+    diag = fl.fv_diagonal(0, iface=iface)
+    base = 6.0 / (0.2 * 0.2)
+    assert applied[2, 2, 2] == pytest.approx(7.5, abs=1e-5)
+    assert diag[2, 2, 2] == pytest.approx(base + 7.5, abs=3e-5)
+    # Jacobi preconditioner z = r / D (fluid.py:4503-4516)
+    assert 15.0 / diag[2, 2, 2] == pytest.approx(15.0 / (base + 7.5), abs=1e-6)
+    # rows away from the interface: A 1 = 0 on a closed box
+    assert np.abs(applied[np.arange(5) != 2]).max() < 1e-9
+
+
+# test_core_fluid.py:1206 restriction volume-averages the interface diagonal
+def test_restriction_volume_averages_interface_diagonal():
+    fl = _fluid(_uniform_box(8))
+    iface = np.zeros((8, 8, 8))
+    iface[2, 2, 2] = 80.0
+    out = fl.restrict(np.zeros((8, 8, 8)), iface=iface)
+    assert float(out["iface"][1, 1, 1]) == pytest.approx(10.0, abs=1e-5)
+    assert float(out["iface"][0, 0, 0]) == pytest.approx(0.0, abs=1e-6)
+
+
+# test_core_fluid.py:1166 mixed obstacle blocks are blocked on the coarse level
+def test_restriction_marks_mixed_obstacle_blocks_blocked():
+    fl = _fluid(_uniform_box(8))
+    fl.obstacle[1, 1, 1] = 1
+    va = np.zeros((8, 8, 8), np.int32)
+    va[2, 2, 2] = 1
+    vw = np.full((8, 8, 8), 0.5, np.float32)
+    out = fl.restrict(np.zeros((8, 8, 8)), vdir_active=va, vdir_weight=vw)
+    assert int(out["obstacle"][0, 0, 0]) == 1
+    assert int(out["vdir_active"][1, 1, 1]) == 1
+    assert int(out["obstacle"].sum()) == 1
+
+
+# test_core_fluid.py:1242 the coarse smoother reads the coarse interface diagonal
+def test_coarse_smoother_uses_the_coarse_interface_diagonal():
+    fl = _fluid(_uniform_box(8))
+    iface = np.zeros((8, 8, 8))
+    iface[1, 1, 1] = 1.0e8
+    coarse = fl.restrict(np.zeros((8, 8, 8)), iface=iface)
+    rhs = np.zeros((4, 4, 4), np.float32)
+    rhs[1, 1, 1] = 1.0
+    p = fl.jacobi_sweep_coarse(1, np.zeros((4, 4, 4)), rhs, coarse["iface"], coarse["obstacle"], omega=1.0)
+    assert float(p[1, 1, 1]) < -1.0e-3
+    assert float(coarse["iface"][0, 0, 0]) == pytest.approx(1.0e8 / 8.0, rel=1e-6)
+
+
+def _graded_obstacle_grid():
+    grid = CartesianGrid(
+        bounds_min_m=(0.0, 0.0, 0.0),
+        cell_widths_x_m=graded_axis_widths(16, 0.0, 1.0, 0.3, 0.7),
+        cell_widths_y_m=graded_axis_widths(14, 0.0, 1.0, 0.3, 0.7),
+        cell_widths_z_m=graded_axis_widths(20, 0.0, 1.0, 0.2, 0.8),
+    )
+    obs = np.zeros(grid.grid_nodes, np.int32)
+    obs[6:10, 5:9, 8:13] = 1
+    return grid, obs
+
+
+# test_core_fluid.py:1648 the weighted operator is self-adjoint on a graded obstacle grid
+@pytest.mark.parametrize("outlet", [0, 1])
+def test_operator_is_self_adjoint_on_graded_obstacle_grid(outlet):
+    grid, obs = _graded_obstacle_grid()
+    fl = _fluid(grid, variant="fp64")
+    fl.obstacle[...] = obs
+    rng = np.random.default_rng(17)
+    x = rng.normal(size=grid.grid_nodes).astype(np.float32).astype(np.float64)
+    y = rng.normal(size=grid.grid_nodes).astype(np.float32).astype(np.float64)
+    x[obs == 1] = 0.0
+    y[obs == 1] = 0.0
+    lhs = fl.weighted_dot(fl.fv_apply(x, outlet), y)
+    rhs = fl.weighted_dot(x, fl.fv_apply(y, outlet))
+    rel = abs(lhs - rhs) / max(abs(lhs), abs(rhs), 1e-30)
+    assert rel < 1.0e-5  # the reference's bound
+    assert rel < 1.0e-12  # exact in f64
+
+
+# test_core_fluid.py:1377 monotone Richardson convergence on a non-uniform grid
+def test_nonuniform_operator_converges_monotonically():
+    errors = []
+    for n in (12, 18, 24):
+        q = (np.arange(n, dtype=np.float64) + 0.5) / n
+        raw = 1.0 + 0.3 * np.sin(2.0 * np.pi * q)
+        widths = tuple(float(v) for v in raw / raw.sum())
+        grid = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=widths, cell_widths_y_m=widths,
+                             cell_widths_z_m=widths)
+        fl = _fluid(grid)
+        c = [np.asarray(a, np.float64) for a in (grid.cell_centers_x_m, grid.cell_centers_y_m, grid.cell_centers_z_m)]
+        p = (np.sin(np.pi * c[0])[:, None, None] * np.sin(np.pi * c[1])[None, :, None]
+             * np.sin(np.pi * c[2])[None, None, :]).astype(np.float32)
+        expected = 3.0 * np.pi * np.pi * p.astype(np.float64)
+        applied = fl.fv_apply(p.astype(np.float64), 0)
+        inner = (slice(2, -2),) * 3
+        err = applied[inner] - expected[inner]
+        errors.append(float(np.sqrt(np.mean(err * err)) / np.sqrt(np.mean(expected[inner] ** 2))))
+    assert errors[1] < errors[0]
+    assert errors[2] < errors[1]
+    assert errors[2] < 4.0e-3
+
+
+def _box_particles(counts, lo, hi, density):
+    nxp, nyp, nzp = counts
+    n = nxp * nyp * nzp
+    lo = np.asarray(lo, np.float32)
+    hi = np.asarray(hi, np.float32)
+    p = np.arange(n)
+    idx = np.stack([p % nxp, (p // nxp) % nyp, p // (nxp * nyp)], axis=1).astype(np.float32)
+    x = (lo + (idx + np.float32(0.5)) * (hi - lo) / np.asarray(counts, np.float32)).astype(np.float32)
+    vol = np.float32(np.prod(hi - lo) / n)
+    return x, np.full(n, vol, np.float32), np.full(n, np.float32(density) * vol, np.float32)
+
+
+# test_neo_hookean_mpm.py:102 a uniform velocity transfers conservatively, J stays 1
+@pytest.mark.parametrize("variant", ["mirror", "fp64"])
+def test_uniform_velocity_transfer_is_conservative(variant):
+    x, vol, mass = _box_particles((4, 4, 4), (-0.005,) * 3, (0.005,) * 3, 1100.0)
+    s = orc.OracleSolid(capacity=64, grid_nodes=(12, 12, 12), bounds_min=(-0.02,) * 3, bounds_max=(0.02,) * 3,
+                        variant=variant)
+    s.load(x=x, volume=vol, mass=mass, region=np.full(64, 101, np.int32))
+    s.v[:64] = (0.02, -0.01, 0.03)
+    e, nu = 1.0e5, 0.45
+    mu, lam = e / (2 * (1 + nu)), e * nu / ((1 + nu) * (1 - 2 * nu))
+    rep = s.step(dt=1.0e-5, mu=mu, lam=lam)
+    assert rep.counts[0] > 0  # active grid nodes
+    assert rep.values[11] < 2.0e-5  # transfer relative error
+    assert rep.values[13] == pytest.approx(1.0, abs=1e-4)  # max |J|
+    assert rep.values[0] > 0.0  # total mass
+
+
+# test_neo_hookean_mpm.py:38 surface area and normal follow F (Nanson)
+def test_surface_geometry_follows_the_deformation_gradient():
+    s = orc.OracleSolid(capacity=1, grid_nodes=(12, 12, 12), bounds_min=(-1.0,) * 3, bounds_max=(1.0,) * 3)
+    s.load(x=np.array([[1.0 / 3.0, 1.0 / 3.0, 0.0]], np.float32), volume=np.array([1.0e-3], np.float32),
+           mass=np.array([1.0], np.float32), region=np.array([1], np.int32),
+           normal=np.array([[0.0, 0.0, 1.0]], np.float32), area=np.array([0.5], np.float32))
+    s.F[0] = np.array([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.5, 0.0, 1.0]], np.float32)
+    s.step(dt=0.0, mu=0.0, lam=0.0, primary=1, secondary=2)
+    expected = np.array([-0.5, 0.0, 1.0]) / math.sqrt(1.25)
+    assert float(s.area[0]) == pytest.approx(0.5 * math.sqrt(1.25), abs=1e-5)
+    np.testing.assert_allclose(s.normal[0], expected, atol=1e-5)
+
+
+def _one_marker(position, traction, normal, area):
+    m = orc.OracleMarkers(x=np.array([position], np.float32), normal=np.array([normal], np.float32),
+                          area=np.array([area], np.float32), region=np.array([101], np.int32))
+    m.t[0] = traction
+    m.compute_forces()
+    return m
+
+
+# test_hibm.py:605 a marker over one particle hands it its whole force
+def test_scatter_gives_the_single_particle_the_marker_force():
+    m = _one_marker((0.5, 0.5, 0.5), (2.0, -4.0, 6.0), (1.0, 0.0, 0.0), 0.5)
+    x, vol, mass = _box_particles((1, 1, 1), (0.0,) * 3, (1.0,) * 3, 1000.0)
+    s = orc.OracleSolid(capacity=1, grid_nodes=(4, 4, 4))
+    s.load(x=x, volume=vol, mass=mass)
+    rep = m.scatter(s, 0.25)
+    assert rep.active_markers == 1 and rep.invalid_markers == 0 and rep.active_particle_contributions == 1
+    assert tuple(s.fext[0]) == (1.0, -2.0, 3.0)
+    assert tuple(rep.marker_force) == (1.0, -2.0, 3.0)
+    assert tuple(rep.external_force) == (1.0, -2.0, 3.0)
+
+
+# test_hibm.py:645 the force is partitioned across the supported particles
+def test_scatter_partitions_force_across_supported_particles():
+    m = _one_marker((0.5, 0.5, 0.5), (0.0, 0.0, 4.0), (0.0, 0.0, 1.0), 1.0)
+    x, vol, mass = _box_particles((2, 1, 1), (0.25, 0.0, 0.0), (0.75, 1.0, 1.0), 1000.0)
+    s = orc.OracleSolid(capacity=2, grid_nodes=(4, 4, 4))
+    s.load(x=x, volume=vol, mass=mass)
+    rep = m.scatter(s, 0.4)
+    assert rep.active_markers == 1 and rep.active_particle_contributions == 2
+    assert float(s.fext[0, 2]) == pytest.approx(2.0, abs=1e-5)
+    assert float(s.fext[1, 2]) == pytest.approx(2.0, abs=1e-5)
+    assert rep.external_force[2] == pytest.approx(4.0, abs=1e-5)
+    assert rep.external_force[2] - rep.marker_force[2] == pytest.approx(0.0, abs=1e-5)
+
+
+# test_hibm.py:684 clear-then-scatter replaces a stale external force
+def test_clear_then_scatter_replaces_stale_force():
+    m = _one_marker((0.5, 0.5, 0.5), (2.0, -4.0, 6.0), (1.0, 0.0, 0.0), 0.5)
+    x, vol, mass = _box_particles((1, 1, 1), (0.0,) * 3, (1.0,) * 3, 1000.0)
+    s = orc.OracleSolid(capacity=1, grid_nodes=(4, 4, 4))
+    s.load(x=x, volume=vol, mass=mass)
+    s.fext[0] = (99.0, 0.0, 0.0)
+    cleared, largest = m.clear(s)
+    assert cleared == 1 and largest == pytest.approx(99.0)
+    m.scatter(s, 0.25)
+    assert tuple(s.fext[0]) == (1.0, -2.0, 3.0)
