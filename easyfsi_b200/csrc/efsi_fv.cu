@@ -1499,7 +1499,10 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
       B.tiled = B.nz >= 16 && B.ny >= 8 && std::getenv("EFSI_NO_TILED") == nullptr;
       B.tgrid = (unsigned)std::max(1, std::min(nt, nsm * per_sm));
       const MarchCfg mc = march_cfg(B.nx, B.ny, B.nz, nsm * 3);
-      B.march = B.nz >= 16 && B.ny >= 8 && std::getenv("EFSI_NO_MARCH") == nullptr;
+      // levels below EFSI_MARCH_MIN_CELLS (default 0) keep the per-cell kernels
+      int64_t march_min = 0;
+      if (const char* env = std::getenv("EFSI_MARCH_MIN_CELLS")) march_min = std::atoll(env);
+      B.march = B.nz >= 16 && B.ny >= 8 && B.n >= march_min && std::getenv("EFSI_NO_MARCH") == nullptr;
       B.mchunk = mc.chunk;
       B.mgrid = mc.grid;
     }

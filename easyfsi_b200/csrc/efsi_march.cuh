@@ -9,9 +9,9 @@
 // the swept field as a (8 + 2) x (32 + 2 pad) tile with its one-cell halo,
 // and the plane's right-hand side and stencil-mask tiles.  Each stage has an
 // mbarrier that completes when its bytes have landed.  The block computes
-// plane i from the stages of planes i-1, i and i+1 while the copies of planes
-// i+2 .. i+kStages-2 are in flight, then releases stage i-1 at the plane's
-// block barrier and the elected thread refills it.  HBM is read once per
+// planes i and i+1 from the stages of planes i-1 .. i+2 while the copies of
+// planes i+3 and i+4 are in flight, then releases the stages of i-1 and i at
+// the iteration's block barrier and the elected thread refills them.  HBM is read once per
 // value (halo rows come from L2); registers hold no prefetched data.
 //
 // The per-cell arithmetic is the same expression, in the same order, as the
@@ -228,15 +228,16 @@ struct StageLayout {
   static constexpr int kSmem = kBarOff + kStages * 8;
 };
 
-// The march.  Per plane i and owned row r, `Op::cell(i, j, k, c, t, m, rhs,
-// kxm, kxp, rc, val)` computes one cell (t: its index in the tile), reading
-// the field through val(v, di, dj, dk) (value tile v at (i+di, j+dj, k+dk));
-// `Op::plane_end(g, i)` runs before the plane's block barrier and
+// The march, two planes per iteration.  Per plane i and owned row r,
+// `Op::cell(i, j, k, c, t, m, rhs, kxm, kxp, rc, val)` computes one cell (t:
+// its index in the tile), reading the field through val(v, di, dj, dk) (value
+// tile v at (i+di, j+dj, k+dk)); `Op::plane_end(g, i, np)` runs after the np
+// planes i .. i+np-1 of an iteration, before its block barrier, and
 // `Op::finish(g)` after the last plane.  With Op::kPrepare, every stage is
-// first passed to `Op::prepare(g, value_tile, mask_tile, plane)` (all threads,
-// in place; the mask tile is null for the halo planes) once it has landed.  Returns false (in every thread) if a
-// stage did not land in time; the kernel then reports it through
-// `sc->fault`.
+// first passed to `Op::prepare(g, value_tile, mask_tile, plane)` (all
+// threads, in place; the mask tile is null for the halo planes) once it has
+// landed.  Returns false (in every thread) if a stage did not land in time;
+// the kernel then reports it through `sc->fault`.
 template <typename TV, int NV, typename TR, bool kR, class Op>
 __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, const CUtensorMap* const (&mv)[NV],
                                       const CUtensorMap* mr, const CUtensorMap* mm, Op& op) {
@@ -280,60 +281,77 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
     fence_proxy_async_smem();
     __syncthreads();
   }
-  int s_m = 0, s_0 = 1, s_p = 2 % kStages;  // stages of planes i-1, i, i+1
-  unsigned ph_p = 0;                        // phase parity of plane i+1
+  // Two planes per iteration: planes i-1 .. i+2 resident, the next two in
+  // flight.  sb is the stage of plane i-1; plane p's phase parity is
+  // ((p - ib + 1) / kStages) & 1.
+  int sb = 0;
+  auto stage_at = [&](int q) {  // stage of plane i - 1 + q
+    const int st = sb + q;
+    return st >= kStages ? st - kStages : st;
+  };
+  auto phase_of = [&](int p) { return (unsigned)(((p - g.ib + 1) / kStages) & 1); };
   const int64_t sx = (int64_t)L.ny * L.nz;
   const int col = g.tx + Lay::kPad, W = Lay::kW;
   RowCoef rc[kRows];
 #pragma unroll
   for (int r = 0; r < kRows; ++r) rc[r] = row_coef(L, g.j[r], g.kc);
   int64_t pbase = (int64_t)g.ib * sx;
-  for (int i = g.ib; i < g.ie; ++i, pbase += sx) {
-    if (!fail) fail = !mbar_wait(&bar[s_p], ph_p);
+  for (int i = g.ib; i < g.ie; i += 2, pbase += 2 * sx) {
+    const int np = min(2, g.ie - i);  // planes computed in this iteration
+#pragma unroll
+    for (int q = 1; q <= 2; ++q) {
+      if (q > np) break;
+      const int st = stage_at(q + 1);  // plane i + q
+      if (!fail) fail = !mbar_wait(&bar[st], phase_of(i + q));
+      if (Op::kPrepare && !fail) op.prepare(g, vtile(st), i + q < g.ie ? mtile(st) : nullptr, i + q);
+    }
     if (Op::kPrepare) {
-      if (!fail) op.prepare(g, vtile(s_p), i + 1 < g.ie ? mtile(s_p) : nullptr, i + 1);
-      fence_proxy_async_smem();  // these generic writes precede the stage's next TMA refill
+      fence_proxy_async_smem();  // these generic writes precede the stages' next TMA refill
       __syncthreads();
     }
     if (!fail) {
-      const double kxm = __ldg(L.cxm + i), kxp = __ldg(L.cxp + i);
-      const TV* vt[3][NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        vt[0][v] = reinterpret_cast<const TV*>(base + s_m * Lay::kStage + v * Lay::kVStride) + col;
-        vt[1][v] = reinterpret_cast<const TV*>(base + s_0 * Lay::kStage + v * Lay::kVStride) + col;
-        vt[2][v] = reinterpret_cast<const TV*>(base + s_p * Lay::kStage + v * Lay::kVStride) + col;
-      }
-      const TR* rt = reinterpret_cast<const TR*>(base + s_0 * Lay::kStage + Lay::kROff);
-      const uint8_t* mt = base + s_0 * Lay::kStage + Lay::kMOff;
+      for (int d = 0; d < 2; ++d) {
+        if (d >= np) break;
+        const int ip = i + d;
+        const double kxm = __ldg(L.cxm + ip), kxp = __ldg(L.cxp + ip);
+        const int sm = stage_at(d), s0 = stage_at(d + 1), sp = stage_at(d + 2);
+        const TV* vt[3][NV];
 #pragma unroll
-      for (int r = 0; r < kRows; ++r) {
-        if (!g.active[r]) continue;
-        const int t = (g.ty + r * kTY) * kMK + g.tx;
-        const int row = (g.ty + r * kTY + 1) * W;
-        op.cell(i, g.j[r], g.k, pbase + g.off[r], t, (unsigned)mt[t], kR ? (double)rt[t] : 0.0, kxm, kxp, rc[r],
-                [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][row + dj * W + dk]; });
+        for (int v = 0; v < NV; ++v) {
+          vt[0][v] = reinterpret_cast<const TV*>(base + sm * Lay::kStage + v * Lay::kVStride) + col;
+          vt[1][v] = reinterpret_cast<const TV*>(base + s0 * Lay::kStage + v * Lay::kVStride) + col;
+          vt[2][v] = reinterpret_cast<const TV*>(base + sp * Lay::kStage + v * Lay::kVStride) + col;
+        }
+        const TR* rt = reinterpret_cast<const TR*>(base + s0 * Lay::kStage + Lay::kROff);
+        const uint8_t* mt = base + s0 * Lay::kStage + Lay::kMOff;
+        const int64_t pb = pbase + d * sx;
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+          if (!g.active[r]) continue;
+          const int t = (g.ty + r * kTY) * kMK + g.tx;
+          const int row = (g.ty + r * kTY + 1) * W;
+          op.cell(ip, g.j[r], g.k, pb + g.off[r], t, (unsigned)mt[t], kR ? (double)rt[t] : 0.0, kxm, kxp, rc[r],
+                  [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][row + dj * W + dk]; });
+        }
       }
     }
-    op.plane_end(g, i);
+    op.plane_end(g, i, np);
     if (__syncthreads_or(fail)) {
       // let the copies in flight land before the block exits
       if (leader)
-        for (int p = i + 2; p <= issued; ++p) mbar_wait(&bar[(p - g.ib + 1) % kStages], ((p - g.ib + 1) / kStages) & 1u);
+        for (int p = i + np + 1; p <= issued; ++p)
+          mbar_wait(&bar[(p - g.ib + 1) % kStages], ((p - g.ib + 1) / kStages) & 1u);
       __syncthreads();
       return false;
     }
-    if (leader && i - 1 + kStages <= g.ie) {
+    // planes i-1 and i are no longer needed: refill their stages
+    if (leader) {
       fence_proxy_async_smem();
-      issued = i - 1 + kStages;
-      issue(issued, s_m);
+      if (i - 1 + kStages <= g.ie) issue(issued = i - 1 + kStages, stage_at(0));
+      if (np == 2 && i + kStages <= g.ie) issue(issued = i + kStages, stage_at(1));
     }
-    s_m = s_0;
-    s_0 = s_p;
-    if (++s_p == kStages) {
-      s_p = 0;
-      ph_p ^= 1u;
-    }
+    sb = stage_at(2);
   }
   op.finish(g);
   return true;
@@ -409,7 +427,7 @@ struct SweepOp {
     }
     out[c] = res;
   }
-  __device__ __forceinline__ void plane_end(const MarchGeom&, int) {}
+  __device__ __forceinline__ void plane_end(const MarchGeom&, int, int) {}
   __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
@@ -547,7 +565,7 @@ struct SpmvOp {
     Ad[c] = o;
     if (m & M_FLUID) part += x0 * o * vol64(L, i, j, k);
   }
-  __device__ __forceinline__ void plane_end(const MarchGeom&, int) {}
+  __device__ __forceinline__ void plane_end(const MarchGeom&, int, int) {}
   __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
@@ -588,11 +606,10 @@ __global__ void __launch_bounds__(kMK* kTY)
 
 // ---------------------------------------------------------------------------
 // Residual restriction (fluid.py:5262-5388): the fine residual of every row
-// is formed in the march and staged in shared memory (double-buffered by
-// plane parity); one plane behind, the threads owning a coarse cell
-// accumulate its 2 x 2 x 2 children in the reference's order (i-pair outer,
-// then j, then k) with the f32 volume weights, across the two planes of the
-// pair.
+// is formed in the march and staged in shared memory (one buffer per plane of
+// the iteration's pair); the threads owning a coarse cell then accumulate its
+// 2 x 2 x 2 children in the reference's order (i-pair outer, then j, then k)
+// with the f32 volume weights.
 // ---------------------------------------------------------------------------
 template <typename TP, bool kNegR, bool kAux>
 struct RestrictOp {
@@ -625,10 +642,22 @@ struct RestrictOp {
     rsolid[i & 1][t] = 0;
     rs[i & 1][t] = (double)(TP)(rv - applied);
   }
+  float wy[2], wz[2];  // the owner's fine widths along j and k (0 outside the level)
+
+  __device__ __forceinline__ void load_widths(const MarchGeom& g) {
+    const int fj0 = g.j0 + 2 * g.ty, fk0 = g.k0 + 2 * g.tx;
+#pragma unroll
+    for (int o = 0; o < 2; ++o) {
+      wy[o] = fj0 + o < L.ny ? __ldg(L.wy + fj0 + o) : 0.0f;
+      wz[o] = fk0 + o < L.nz ? __ldg(L.wz + fk0 + o) : 0.0f;
+    }
+  }
+
   // Owners (tx < 16, every thread row) fold fine plane q into their coarse cell.
   __device__ __forceinline__ void accumulate(const MarchGeom& g, int q) {
     if (g.tx >= kMK / 2) return;
     const int fj0 = g.j0 + 2 * g.ty, fk0 = g.k0 + 2 * g.tx;
+    const float wxq = __ldg(L.wx + q);
 #pragma unroll
     for (int oj = 0; oj < 2; ++oj)
 #pragma unroll
@@ -639,7 +668,7 @@ struct RestrictOp {
           if (rsolid[q & 1][t]) {
             ocount += 1;
           } else {
-            const float vol = __fmul_rn(__fmul_rn(__ldg(L.wx + q), __ldg(L.wy + fj)), __ldg(L.wz + fk));
+            const float vol = __fmul_rn(__fmul_rn(wxq, wy[oj]), wz[ok]);
             const double r = rs[q & 1][t];
             if (sizeof(TP) == 8)
               wres = (float)__dadd_rn((double)wres, __dmul_rn(r, (double)vol));
@@ -658,14 +687,14 @@ struct RestrictOp {
       ocount = 0;
     }
   }
-  // plane i-1 was staged before the previous block barrier
-  __device__ __forceinline__ void plane_end(const MarchGeom& g, int i) {
-    if (i > g.ib) accumulate(g, i - 1);
-  }
-  __device__ __forceinline__ void finish(const MarchGeom& g) {
+  // An iteration's planes are the pair (2c, 2c+1) of coarse plane c (ib and
+  // the chunk are even): fold them in order once both are staged.
+  __device__ __forceinline__ void plane_end(const MarchGeom& g, int i, int np) {
     __syncthreads();
-    accumulate(g, g.ie - 1);
+    accumulate(g, i);
+    if (np == 2) accumulate(g, i + 1);
   }
+  __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
 template <typename TP, bool kNegR, bool kAux>
@@ -678,7 +707,8 @@ __global__ void __launch_bounds__(kMK* kTY)
   __shared__ unsigned char rsolid[2][kMJ * kMK];
   MarchGeom g;
   const bool any = march_geom(F, chunk, g);
-  RestrictOp<TP, kNegR, kAux> op{F, outlet, cnx, cny, cnz, crhs, rs, rsolid, 0.0f, 0.0f, 0};
+  RestrictOp<TP, kNegR, kAux> op{F, outlet, cnx, cny, cnz, crhs, rs, rsolid, 0.0f, 0.0f, 0, {0.0f, 0.0f}, {0.0f, 0.0f}};
+  op.load_widths(g);
   const CUtensorMap* const mv[1] = {&map_p};
   if (any && !march<TP, 1, TR, true>(F, g, mv, &map_r, &map_m, op)) report_fault(sc);
 }
