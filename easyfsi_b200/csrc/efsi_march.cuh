@@ -229,8 +229,9 @@ struct StageLayout {
 };
 
 // The march, two planes per iteration.  Per plane i and owned row r,
-// `Op::cell(i, j, k, c, t, m, rhs, kxm, kxp, rc, val)` computes one cell (t:
-// its index in the tile), reading the field through val(v, di, dj, dk) (value
+// `Op::cell(i, j, k, c, t, active, m, rhs, kxm, kxp, rc, val)` computes one
+// cell (t: its index in the tile; an inactive row lies outside the level and
+// must not store), reading the field through val(v, di, dj, dk) (value
 // tile v at (i+di, j+dj, k+dk)); `Op::plane_end(g, i, np)` runs after the np
 // planes i .. i+np-1 of an iteration, before its block barrier, and
 // `Op::finish(g)` after the last plane.  With Op::kPrepare, every stage is
@@ -298,6 +299,14 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
   int64_t pbase = (int64_t)g.ib * sx;
   for (int i = g.ib; i < g.ie; i += 2, pbase += 2 * sx) {
     const int np = min(2, g.ie - i);  // planes computed in this iteration
+    // x-face coefficients of the iteration's planes, loaded ahead of the waits
+    double kx[4];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      const int ip = min(i + d, L.nx - 1);
+      kx[2 * d] = __ldg(L.cxm + ip);
+      kx[2 * d + 1] = __ldg(L.cxp + ip);
+    }
 #pragma unroll
     for (int q = 1; q <= 2; ++q) {
       if (q > np) break;
@@ -310,31 +319,38 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
       __syncthreads();
     }
     if (!fail) {
+      // all cells of the iteration in one branch-free block (inactive rows
+      // compute on clamped data and only skip their stores)
+      auto run = [&](auto planes) {
+        constexpr int ND = decltype(planes)::value;
 #pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        if (d >= np) break;
-        const int ip = i + d;
-        const double kxm = __ldg(L.cxm + ip), kxp = __ldg(L.cxp + ip);
-        const int sm = stage_at(d), s0 = stage_at(d + 1), sp = stage_at(d + 2);
-        const TV* vt[3][NV];
+        for (int d = 0; d < ND; ++d) {
+          const int ip = i + d;
+          const int sm = stage_at(d), s0 = stage_at(d + 1), sp = stage_at(d + 2);
+          const TV* vt[3][NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          vt[0][v] = reinterpret_cast<const TV*>(base + sm * Lay::kStage + v * Lay::kVStride) + col;
-          vt[1][v] = reinterpret_cast<const TV*>(base + s0 * Lay::kStage + v * Lay::kVStride) + col;
-          vt[2][v] = reinterpret_cast<const TV*>(base + sp * Lay::kStage + v * Lay::kVStride) + col;
+          for (int v = 0; v < NV; ++v) {
+            vt[0][v] = reinterpret_cast<const TV*>(base + sm * Lay::kStage + v * Lay::kVStride) + col;
+            vt[1][v] = reinterpret_cast<const TV*>(base + s0 * Lay::kStage + v * Lay::kVStride) + col;
+            vt[2][v] = reinterpret_cast<const TV*>(base + sp * Lay::kStage + v * Lay::kVStride) + col;
+          }
+          const TR* rt = reinterpret_cast<const TR*>(base + s0 * Lay::kStage + Lay::kROff);
+          const uint8_t* mt = base + s0 * Lay::kStage + Lay::kMOff;
+          const int64_t pb = pbase + d * sx;
+#pragma unroll
+          for (int r = 0; r < kRows; ++r) {
+            const int t = (g.ty + r * kTY) * kMK + g.tx;
+            const int row = (g.ty + r * kTY + 1) * W;
+            op.cell(ip, g.j[r], g.k, pb + g.off[r], t, g.active[r], (unsigned)mt[t], kR ? (double)rt[t] : 0.0,
+                    kx[2 * d], kx[2 * d + 1], rc[r],
+                    [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][row + dj * W + dk]; });
+          }
         }
-        const TR* rt = reinterpret_cast<const TR*>(base + s0 * Lay::kStage + Lay::kROff);
-        const uint8_t* mt = base + s0 * Lay::kStage + Lay::kMOff;
-        const int64_t pb = pbase + d * sx;
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-          if (!g.active[r]) continue;
-          const int t = (g.ty + r * kTY) * kMK + g.tx;
-          const int row = (g.ty + r * kTY + 1) * W;
-          op.cell(ip, g.j[r], g.k, pb + g.off[r], t, (unsigned)mt[t], kR ? (double)rt[t] : 0.0, kxm, kxp, rc[r],
-                  [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][row + dj * W + dk]; });
-        }
-      }
+      };
+      if (np == 2)
+        run(std::integral_constant<int, 2>{});
+      else
+        run(std::integral_constant<int, 1>{});
     }
     op.plane_end(g, i, np);
     if (__syncthreads_or(fail)) {
@@ -409,8 +425,9 @@ struct SweepOp {
   }
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, unsigned m, double e, double kxm,
-                                       double kxp, const RowCoef& rc, const V& val) {
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, bool active, unsigned m, double e,
+                                       double kxm, double kxp, const RowCoef& rc, const V& val) {
+    if (!active) return;
     TP res = (TP)0;
     if (!(m & M_SOLID)) {
       const double x0 = val(0, 0, 0, 0), xm = val(0, -1, 0, 0), xp = val(0, 1, 0, 0);
@@ -545,25 +562,21 @@ struct SpmvOp {
   }
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, unsigned m, double, double kxm,
-                                       double kxp, const RowCoef& rc, const V& val) {
-    double x0;
-    if (m & M_SOLID)
-      x0 = 0.0;
-    else if (!(m & M_FLUID) && zproj)
-      x0 = kCopy ? 0.0 : 0.0 + beta * val(1, 0, 0, 0);
-    else
-      x0 = dir(val, 0, 0, 0);
-    d_new[c] = x0;
-    double o = 0.0;
-    if (!(m & M_SOLID)) {
-      double ns, den;
-      stencil_sel<kAux>(L, rc, kxm, kxp, i, j, k, c, m, outlet, dir(val, -1, 0, 0), dir(val, 1, 0, 0),
-                        dir(val, 0, -1, 0), dir(val, 0, 1, 0), dir(val, 0, 0, -1), dir(val, 0, 0, 1), ns, den);
-      o = (den + (kAux ? iface_at<double>(L, c) : 0.0)) * x0 - ns;
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, bool active, unsigned m, double,
+                                       double kxm, double kxp, const RowCoef& rc, const V& val) {
+    const bool solid = (m & M_SOLID) != 0;
+    double x0 = dir(val, 0, 0, 0);
+    if (!(m & M_FLUID) && zproj) x0 = kCopy ? 0.0 : 0.0 + beta * val(1, 0, 0, 0);
+    if (solid) x0 = 0.0;
+    double ns, den;
+    stencil_sel<kAux>(L, rc, kxm, kxp, i, j, k, c, m, outlet, dir(val, -1, 0, 0), dir(val, 1, 0, 0),
+                      dir(val, 0, -1, 0), dir(val, 0, 1, 0), dir(val, 0, 0, -1), dir(val, 0, 0, 1), ns, den);
+    const double o = solid ? 0.0 : (den + (kAux ? iface_at<double>(L, c) : 0.0)) * x0 - ns;
+    if (active) {
+      d_new[c] = x0;
+      Ad[c] = o;
+      if (m & M_FLUID) part += x0 * o * vol64(L, i, j, k);
     }
-    Ad[c] = o;
-    if (m & M_FLUID) part += x0 * o * vol64(L, i, j, k);
   }
   __device__ __forceinline__ void plane_end(const MarchGeom&, int, int) {}
   __device__ __forceinline__ void finish(const MarchGeom&) {}
@@ -626,7 +639,7 @@ struct RestrictOp {
   int ocount;
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int t, unsigned m, double e, double kxm,
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int t, bool, unsigned m, double e, double kxm,
                                        double kxp, const RowCoef& rc, const V& val) {
     if (m & M_SOLID) {
       rsolid[i & 1][t] = 1;
