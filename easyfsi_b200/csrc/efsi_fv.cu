@@ -1350,9 +1350,10 @@ static void preload_kernels() {
       (const void*)kt_cg_dots<true, false>,       (const void*)kt_cg_dots<false, false>,
       (const void*)kt_sub_mean_xr,                (const void*)k_mg_tail,
 #define EFSI_MARCH_FNS(A)                                                                              \
-      (const void*)km_sweep<double, true, false, A>, (const void*)km_sweep<double, true, true, A>,         \
-      (const void*)km_sweep<double, false, false, A>, (const void*)km_sweep<float, false, false, A>,       \
-      (const void*)km_sweep<float, false, true, A>, (const void*)km_sweep0<double, true, A>,               \
+      (const void*)km_sweep<double, true, false, A, false>, (const void*)km_sweep<double, true, true, A, false>, \
+      (const void*)km_sweep<double, true, false, A, true>, (const void*)km_sweep<double, true, true, A, true>,   \
+      (const void*)km_sweep<double, false, false, A, false>, (const void*)km_sweep<float, false, false, A, false>, \
+      (const void*)km_sweep<float, false, true, A, false>, (const void*)km_sweep0<double, true, A>,        \
       (const void*)km_sweep0<double, false, A>, (const void*)km_sweep0<float, false, A>,                   \
       (const void*)km_restrict<double, true, A>, (const void*)km_restrict<double, false, A>,               \
       (const void*)km_restrict<float, false, A>, (const void*)km_spmv_dir<true, A>,                        \
@@ -1363,11 +1364,13 @@ static void preload_kernels() {
   for (const void* f : fns) cudaFuncGetAttributes(&a, f);
   // the plane-marching kernels take up to ~70 KB of dynamic shared memory
 #define EFSI_MARCH_SMEM(A)                                                                                        \
-  {(const void*)km_sweep<double, true, false, A>, march_smem<double, 1, double, true>()},                         \
-      {(const void*)km_sweep<double, true, true, A>, march_smem<double, 1, double, true>()},                      \
-      {(const void*)km_sweep<double, false, false, A>, march_smem<double, 1, double, true>()},                    \
-      {(const void*)km_sweep<float, false, false, A>, march_smem<float, 1, float, true>()},                       \
-      {(const void*)km_sweep<float, false, true, A>, march_smem<float, 1, float, true>()},                        \
+  {(const void*)km_sweep<double, true, false, A, false>, march_smem<double, 1, double, true>()},                  \
+      {(const void*)km_sweep<double, true, true, A, false>, march_smem<double, 1, double, true>()},               \
+      {(const void*)km_sweep<double, true, false, A, true>, march_smem<double, 1, double, true>()},               \
+      {(const void*)km_sweep<double, true, true, A, true>, march_smem<double, 1, double, true>()},                \
+      {(const void*)km_sweep<double, false, false, A, false>, march_smem<double, 1, double, true>()},             \
+      {(const void*)km_sweep<float, false, false, A, false>, march_smem<float, 1, float, true>()},                \
+      {(const void*)km_sweep<float, false, true, A, false>, march_smem<float, 1, float, true>()},                 \
       {(const void*)km_restrict<double, true, A>, march_smem<double, 1, double, true>()},                         \
       {(const void*)km_restrict<double, false, A>, march_smem<double, 1, double, true>()},                        \
       {(const void*)km_restrict<float, false, A>, march_smem<float, 1, float, true>()},                           \
@@ -1856,7 +1859,8 @@ static bool launch_march_spmv(efsi_fv_plan* P, const LevelDev& L, bool copy, con
 // streamed with TMA (the caller then runs the per-cell kernel).
 template <typename TP, bool kNegR, bool kZero, bool kAux>
 static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const TP* p, const void* rhs, TP* out,
-                               int outlet, double om, ProlongSrc pr, double* partials, cudaStream_t s) {
+                               int outlet, double om, ProlongSrc pr, double* partials, cudaStream_t s,
+                               const double* dots_delta) {
   using TR = typename std::conditional<kNegR, double, TP>::type;
   const LevelBuf& B = P->lv[l];
   const dim3 blk(kMK, kTY);
@@ -1870,28 +1874,47 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   const CUtensorMap* mm = plane_map(P, l, B.mask, MAP_MASK);
   if (!mp || !mr || !mm) return false;
   const int sm = march_smem<TP, 1, TR, true>();
+  if constexpr (std::is_same<TP, double>::value && kNegR && !kZero) {
+    if (dots_delta != nullptr) {
+      if (pr.pc != nullptr)
+        EFSI_COUNTED km_sweep<TP, kNegR, true, kAux, true><<<B.mgrid, blk, sm, s>>>(
+            L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dots_delta);
+      else
+        EFSI_COUNTED km_sweep<TP, kNegR, false, kAux, true><<<B.mgrid, blk, sm, s>>>(
+            L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dots_delta);
+      return true;
+    }
+  }
   if (pr.pc != nullptr)
-    EFSI_COUNTED km_sweep<TP, kNegR, true, kAux><<<B.mgrid, blk, sm, s>>>(L, B.mchunk, *mp, *mr, *mm, out, outlet, om,
-                                                                           pr, partials, P->sc);
+    EFSI_COUNTED km_sweep<TP, kNegR, true, kAux, false><<<B.mgrid, blk, sm, s>>>(
+        L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr);
   else
-    EFSI_COUNTED km_sweep<TP, kNegR, false, kAux><<<B.mgrid, blk, sm, s>>>(L, B.mchunk, *mp, *mr, *mm, out, outlet,
-                                                                            om, pr, partials, P->sc);
+    EFSI_COUNTED km_sweep<TP, kNegR, false, kAux, false><<<B.mgrid, blk, sm, s>>>(
+        L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr);
   return true;
 }
 
 // One smoother sweep of level l (plane-marching kernel when the level is
 // large enough, else the per-cell kernel).
+// With dots_delta (level 0, the last sweep of the PCG's V-cycle, partials
+// given) the march kernel also finishes the PCG dots and *dots_done is set;
+// the per-cell fallback leaves them to the dots kernel.
 template <typename TP, bool kNegR, bool kZero>
 static void launch_sweep(efsi_fv_plan* P, int l, const TP* p, const void* rhs, TP* out, int outlet, double om,
-                         ProlongSrc pr, double* partials, cudaStream_t s) {
+                         ProlongSrc pr, double* partials, cudaStream_t s, const double* dots_delta = nullptr,
+                         bool* dots_done = nullptr) {
   LevelDev L = level_dev(P, l);
   const LevelBuf& B = P->lv[l];
   if (B.march) {
     const bool done = (L.fw != nullptr || L.iface != nullptr)
-                          ? launch_march_sweep<TP, kNegR, kZero, true>(P, l, L, p, rhs, out, outlet, om, pr, partials, s)
-                          : launch_march_sweep<TP, kNegR, kZero, false>(P, l, L, p, rhs, out, outlet, om, pr, partials,
-                                                                         s);
-    if (done) return;
+                          ? launch_march_sweep<TP, kNegR, kZero, true>(P, l, L, p, rhs, out, outlet, om, pr, partials,
+                                                                        s, dots_delta)
+                          : launch_march_sweep<TP, kNegR, kZero, false>(P, l, L, p, rhs, out, outlet, om, pr,
+                                                                         partials, s, dots_delta);
+    if (done) {
+      if (dots_done != nullptr && dots_delta != nullptr && !kZero) *dots_done = true;
+      return;
+    }
   }
   if (B.tiled)
     EFSI_COUNTED kt_sweep<TP, kNegR, kZero><<<B.tgrid, dim3(kTK, kTJ), 0, s>>>(L, p, rhs, out, outlet, om, pr, partials,
@@ -1933,7 +1956,7 @@ static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs
 // fluid z V sum so consumers can apply the zero-mean projection on the fly.
 // ---------------------------------------------------------------------------
 static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int pre, int coarse, int post,
-                  bool want_mean, cudaStream_t s) {
+                  bool want_mean, cudaStream_t s, const double* dots_delta = nullptr, bool* dots_done = nullptr) {
   pre = std::max(1, pre);
   coarse = std::max(1, coarse);
   post = std::max(1, post);
@@ -1953,7 +1976,8 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       if (it == 0)
         launch_sweep<double, true, true>(P, 0, nullptr, r, dst, outlet, om, none, part, s);
       else
-        launch_sweep<double, true, false>(P, 0, cur, r, dst, outlet, om, none, part, s);
+        launch_sweep<double, true, false>(P, 0, cur, r, dst, outlet, om, none, part, s,
+                                          it == n - 1 ? dots_delta : nullptr, dots_done);
       cur = dst;
     }
     EFSI_LAUNCH_CHECK();
@@ -2047,7 +2071,7 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       if (l == 0)
         EFSI_TIMED(KF_SWEEP_L0, 25.0 * n0 + (it == 0 ? 4.0 * C.n : 0.0), s,
                    (launch_sweep<double, true, false>(P, 0, (const double*)c, r, (double*)dst, outlet, om, p_use, part,
-                                                      s)));
+                                                      s, last ? dots_delta : nullptr, dots_done)));
       else
         launch_sweep<float, false, false>(P, l, (const float*)c, B.rhs, (float*)dst, outlet, om, p_use, nullptr, s);
       c = dst;
@@ -2092,6 +2116,7 @@ struct PcgRun {
   double* d_cur;
   double* d_nxt;
   bool copy_next;  // next SpMV starts a fresh direction d = z'
+  bool dots_fused;  // the last preconditioner sweep also finished the PCG dots
 };
 
 static int read_scalars(PcgRun& R) {
@@ -2107,8 +2132,11 @@ static int read_scalars(PcgRun& R) {
 // z = M^-1 r (+ z mean for the on-the-fly projection when remove_mean).
 static int precondition(PcgRun& R) {
   const bool want_mean = R.prm->remove_mean != 0;
+  R.dots_fused = false;
   if (R.use_mg) {
-    EFSI_TRY(vcycle(R.P, R.P->r, R.P->z, R.prm->outlet, R.pre, R.coarse, R.post, want_mean, R.s));
+    // with the zero-mean projection the V-cycle's last sweep finishes the dots
+    EFSI_TRY(vcycle(R.P, R.P->r, R.P->z, R.prm->outlet, R.pre, R.coarse, R.post, want_mean, R.s,
+                    want_mean ? R.P->delta : nullptr, &R.dots_fused));
   } else {
     EFSI_COUNTED k_jacobi_precond<<<R.S.grid, R.S.block, 0, R.s>>>(R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
                                                       R.P->partials, R.P->sc);
@@ -2274,6 +2302,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   };
   auto launch_precond_dots = [&]() -> int {
     EFSI_TRY(precondition(R));
+    if (R.dots_fused) return EFSI_OK;
     if (tiled0) {
       if (R.use_mg)
         EFSI_TIMED(KF_CG_DOTS, 25.0 * n0d, s,

@@ -387,7 +387,7 @@ __device__ __forceinline__ void report_fault(CgScalars* sc) {
 // prolongation p += s * p_coarse of fluid cells fused in when kProlong
 // (fluid.py:5391-5406) and, when `partials`, the fluid sum of out * V.
 // ---------------------------------------------------------------------------
-template <typename TP, bool kNegR, bool kProlong, bool kAux>
+template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots>
 struct SweepOp {
   const LevelDev& L;
   TP* __restrict__ out;
@@ -396,6 +396,11 @@ struct SweepOp {
   ProlongSrc pr;
   bool want_sum;
   double zsum;
+  // kDots (the V-cycle's last level-0 sweep inside the flexible PCG): the
+  // sums behind <r, z'>_V and <delta, z'>_V with z' = z - mean_z, i.e.
+  // sum r z V, sum r V, sum delta z V and sum delta V over fluid rows.
+  const double* __restrict__ delta;
+  double srz, sr, sdz, sd;
 
   // p + s * p_coarse at (i, j, k) in the level's storage precision
   __device__ __forceinline__ double prolonged(double v, int i, int j, int k) const {
@@ -440,7 +445,17 @@ struct SweepOp {
         const double jv = (ns - rv) / den;
         res = (TP)(x0 + omega * (jv - x0));
       }
-      if (want_sum && (m & M_FLUID)) zsum += (double)res * vol64(L, i, j, k);
+      if ((want_sum || kDots) && (m & M_FLUID)) {
+        const double V = vol64(L, i, j, k);
+        zsum += (double)res * V;
+        if (kDots) {  // rhs e is r (level 0 of the PCG's V-cycle)
+          const double dl = __ldg(delta + c);
+          srz += e * (double)res * V;
+          sr += e * V;
+          sdz += (double)res * dl * V;
+          sd += dl * V;
+        }
+      }
     }
     out[c] = res;
   }
@@ -448,17 +463,45 @@ struct SweepOp {
   __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
-template <typename TP, bool kNegR, bool kProlong, bool kAux>
+// kDots: also finish the flexible PCG's preconditioned dots of this
+// iteration (what the dots kernel computes, fluid.py:4604-4611 / 4590-4601):
+// rz_new = <r, z'>_V, beta_num = <delta, z'>_V and beta, from the five sums.
+template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots>
 __global__ void __launch_bounds__(kMK* kTY)
     km_sweep(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
              const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
-             TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc) {
+             TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc,
+             const double* __restrict__ delta) {
   using TR = typename std::conditional<kNegR, double, TP>::type;
   MarchGeom g;
   const bool any = march_geom(L, chunk, g);
-  SweepOp<TP, kNegR, kProlong, kAux> op{L, out, outlet, omega, pr, partials != nullptr, 0.0};
+  SweepOp<TP, kNegR, kProlong, kAux, kDots> op{L, out, outlet, omega, pr, partials != nullptr, 0.0,
+                                               delta, 0.0, 0.0, 0.0, 0.0};
   const CUtensorMap* const mv[1] = {&map_p};
   if (any && !march<TP, 1, TR, true>(L, g, mv, &map_r, &map_m, op)) report_fault(sc);
+  if (kDots) {
+    double v[5] = {op.zsum, op.srz, op.sr, op.sdz, op.sd}, t[5];
+    if (grid_sum<5>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        const double mz = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->mean_z = mz;
+        sc->zproj = 1;
+        const double rz = sc->rz, rz_new = t[1] - mz * t[2], bnum = t[3] - mz * t[4];
+        sc->rz_new = rz_new;
+        sc->beta_num = bnum;
+        double beta = 0.0;
+        if (rz <= 1.0e-300 || rz_new <= 0.0) {
+          sc->code = 2;
+        } else {
+          beta = bnum / rz;
+          if (beta < 0.0) beta = 0.0;
+        }
+        sc->beta = beta;
+        sc->rz = rz_new;
+      }
+    }
+    return;
+  }
   if (partials != nullptr) {
     double v[1] = {op.zsum}, t[1];
     if (grid_sum<1>(v, partials, &sc->ticket, t)) {
