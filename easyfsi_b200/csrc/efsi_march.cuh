@@ -229,15 +229,17 @@ struct StageLayout {
 };
 
 // The march, two planes per iteration.  Per plane i and owned row r,
-// `Op::cell(i, j, k, c, t, active, m, rhs, kxm, kxp, rc, val)` computes one
-// cell (t: its index in the tile; an inactive row lies outside the level and
-// must not store), reading the field through val(v, di, dj, dk) (value
+// `Op::cell(i, j, k, c, t, slot, active, m, rhs, kxm, kxp, rc, val)` computes
+// one cell (t: its index in the tile; slot = d * kRows + r for plane i + d of
+// the iteration; an inactive row lies outside the level and must not store), reading the field through val(v, di, dj, dk) (value
 // tile v at (i+di, j+dj, k+dk)); `Op::plane_end(g, i, np)` runs after the np
 // planes i .. i+np-1 of an iteration, before its block barrier, and
-// `Op::finish(g)` after the last plane.  With Op::kPrepare, every stage is
-// first passed to `Op::prepare(g, value_tile, mask_tile, plane)` (all
-// threads, in place; the mask tile is null for the halo planes) once it has
-// landed.  Returns false (in every thread) if a stage did not land in time;
+// `Op::finish(g)` after the last plane.  `Op::prefetch(g, i, pbase, sx)`
+// (and `prefetch_prologue(g)` for planes ib-1, ib) issue the op's own global
+// loads of an iteration before its stage waits.  With Op::kPrepare, every
+// stage is first passed to `Op::prepare(g, value_tile, mask_tile, plane,
+// slot)` (all threads, in place; the mask tile is null for the halo planes;
+// slot 0 / 1 for planes i+1 / i+2, or ib-1 / ib) once it has landed.  Returns false (in every thread) if a stage did not land in time;
 // the kernel then reports it through `sc->fault`.
 template <typename TV, int NV, typename TR, bool kR, class Op>
 __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, const CUtensorMap* const (&mv)[NV],
@@ -271,13 +273,14 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
     for (int p = g.ib - 1; p <= issued; ++p) issue(p, p - g.ib + 1);
   auto vtile = [&](int s) { return reinterpret_cast<TV*>(base + s * Lay::kStage); };
   auto mtile = [&](int s) { return reinterpret_cast<const uint8_t*>(base + s * Lay::kStage + Lay::kMOff); };
+  op.prefetch_prologue(g);  // the op's own loads for planes ib-1 and ib, ahead of the waits
   bool fail = !mbar_wait(&bar[0], 0u);
   if (!fail) fail = !mbar_wait(&bar[1], 0u);
   if (Op::kPrepare) {
     // planes ib-1 (a halo plane: no mask tile) and ib
     if (!fail) {
-      op.prepare(g, vtile(0), nullptr, g.ib - 1);
-      op.prepare(g, vtile(1), mtile(1), g.ib);
+      op.prepare(g, vtile(0), nullptr, g.ib - 1, 0);
+      op.prepare(g, vtile(1), mtile(1), g.ib, 1);
     }
     fence_proxy_async_smem();
     __syncthreads();
@@ -307,12 +310,13 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
       kx[2 * d] = __ldg(L.cxm + ip);
       kx[2 * d + 1] = __ldg(L.cxp + ip);
     }
+    op.prefetch(g, i, pbase, sx);  // the op's own loads for this iteration, ahead of the waits
 #pragma unroll
     for (int q = 1; q <= 2; ++q) {
       if (q > np) break;
       const int st = stage_at(q + 1);  // plane i + q
       if (!fail) fail = !mbar_wait(&bar[st], phase_of(i + q));
-      if (Op::kPrepare && !fail) op.prepare(g, vtile(st), i + q < g.ie ? mtile(st) : nullptr, i + q);
+      if (Op::kPrepare && !fail) op.prepare(g, vtile(st), i + q < g.ie ? mtile(st) : nullptr, i + q, q - 1);
     }
     if (Op::kPrepare) {
       fence_proxy_async_smem();  // these generic writes precede the stages' next TMA refill
@@ -341,8 +345,8 @@ __device__ __forceinline__ bool march(const LevelDev& L, const MarchGeom& g, con
           for (int r = 0; r < kRows; ++r) {
             const int t = (g.ty + r * kTY) * kMK + g.tx;
             const int row = (g.ty + r * kTY + 1) * W;
-            op.cell(ip, g.j[r], g.k, pb + g.off[r], t, g.active[r], (unsigned)mt[t], kR ? (double)rt[t] : 0.0,
-                    kx[2 * d], kx[2 * d + 1], rc[r],
+            op.cell(ip, g.j[r], g.k, pb + g.off[r], t, d * kRows + r, g.active[r], (unsigned)mt[t],
+                    kR ? (double)rt[t] : 0.0, kx[2 * d], kx[2 * d + 1], rc[r],
                     [&](int v, int dp, int dj, int dk) -> double { return (double)vt[dp + 1][v][row + dj * W + dk]; });
           }
         }
@@ -401,37 +405,72 @@ struct SweepOp {
   // sum r z V, sum r V, sum delta z V and sum delta V over fluid rows.
   const double* __restrict__ delta;
   double srz, sr, sdz, sd;
+  double dl[2 * kRows];  // kDots: delta of the iteration's cells, prefetched
 
-  // p + s * p_coarse at (i, j, k) in the level's storage precision
-  __device__ __forceinline__ double prolonged(double v, int i, int j, int k) const {
-    const float corr = __fmul_rn(
-        pr.scale,
-        __ldg(pr.pc + cidx(min(i / 2, pr.cnx - 1), min(j / 2, pr.cny - 1), min(k / 2, pr.cnz - 1), pr.cny, pr.cnz)));
-    if (sizeof(TP) == 8) return __dadd_rn(v, (double)corr);
-    return (double)__fadd_rn((float)v, corr);
+  // kProlong: every thread prolongs up to kPCells cells of each landed value
+  // tile (the (kMJ + 2) x (kMK + 2) cells with halo, strided by the block);
+  // their coarse values are loaded ahead of the stage waits.
+  static constexpr int kCols = kMK + 2, kCells = (kMJ + 2) * kCols;
+  static constexpr int kPCells = (kCells + kMK * kTY - 1) / (kMK * kTY);
+  float pcv[2][kPCells];
+
+  __device__ __forceinline__ void load_coarse(const MarchGeom& g, int plane, int slot) {
+    const int ci = min(min(max(plane, 0), L.nx - 1) / 2, pr.cnx - 1);
+#pragma unroll
+    for (int q = 0; q < kPCells; ++q) {
+      const int e = min(g.ty * kMK + g.tx + q * kMK * kTY, kCells - 1);
+      const int r = e / kCols, cc = e - r * kCols;
+      const int cj = min(max(g.j0 - 1 + r, 0) / 2, pr.cny - 1), ck = min(max(g.k0 - 1 + cc, 0) / 2, pr.cnz - 1);
+      pcv[slot][q] = __ldg(pr.pc + cidx(ci, cj, ck, pr.cny, pr.cnz));
+    }
+  }
+  __device__ __forceinline__ void prefetch_prologue(const MarchGeom& g) {
+    if (kProlong) {
+      load_coarse(g, g.ib - 1, 0);
+      load_coarse(g, g.ib, 1);
+    }
+  }
+  __device__ __forceinline__ void prefetch(const MarchGeom& g, int i, int64_t pbase, int64_t sx) {
+    if (kProlong) {
+      load_coarse(g, i + 1, 0);
+      load_coarse(g, i + 2, 1);
+    }
+    if (kDots) {
+#pragma unroll
+      for (int d = 0; d < 2; ++d)
+#pragma unroll
+        for (int r = 0; r < kRows; ++r)
+          dl[d * kRows + r] = __ldg(delta + min(pbase + d * sx, (int64_t)(L.nx - 1) * sx) + g.off[r]);
+    }
   }
 
-  // The prolongation is applied to each landed value tile once: tile cells
-  // by their own mask, halo cells (reached only through open faces, hence
-  // fluid) unconditionally.  Coarse indices are clamped, so cells outside the
-  // level take an in-level coarse value that is never used.
+  // The prolongation p + s * p_coarse (in the level's storage precision) is
+  // applied to each landed value tile once: tile cells by their own mask,
+  // halo cells (reached only through open faces, hence fluid)
+  // unconditionally.  Coarse indices are clamped, so cells outside the level
+  // take an in-level coarse value that is never used.
   static constexpr bool kPrepare = kProlong;
-  __device__ __forceinline__ void prepare(const MarchGeom& g, TP* tile, const uint8_t* mtile, int plane) const {
+  __device__ __forceinline__ void prepare(const MarchGeom& g, TP* tile, const uint8_t* mtile, int, int slot) const {
     using Lay = StageLayout<TP, 1, TP, true>;
-    constexpr int kCols = kMK + 2, kCells = (kMJ + 2) * kCols;
-    const int ip = min(max(plane, 0), L.nx - 1);
-    for (int e = g.ty * kMK + g.tx; e < kCells; e += kMK * kTY) {
+#pragma unroll
+    for (int q = 0; q < kPCells; ++q) {
+      const int e = g.ty * kMK + g.tx + q * kMK * kTY;
+      if (e >= kCells) break;
       const int r = e / kCols, cc = e - r * kCols;
       const bool inner = r >= 1 && r <= kMJ && cc >= 1 && cc <= kMK;
       if (inner && mtile != nullptr && !(mtile[(r - 1) * kMK + cc - 1] & M_FLUID)) continue;
       TP* v = tile + r * Lay::kW + Lay::kPad - 1 + cc;
-      *v = (TP)prolonged((double)*v, ip, max(g.j0 - 1 + r, 0), max(g.k0 - 1 + cc, 0));
+      const float corr = __fmul_rn(pr.scale, pcv[slot][q]);
+      if (sizeof(TP) == 8)
+        *v = (TP)__dadd_rn((double)*v, (double)corr);
+      else
+        *v = (TP)__fadd_rn((float)*v, corr);
     }
   }
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, bool active, unsigned m, double e,
-                                       double kxm, double kxp, const RowCoef& rc, const V& val) {
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, int slot, bool active, unsigned m,
+                                       double e, double kxm, double kxp, const RowCoef& rc, const V& val) {
     if (!active) return;
     TP res = (TP)0;
     if (!(m & M_SOLID)) {
@@ -449,11 +488,11 @@ struct SweepOp {
         const double V = vol64(L, i, j, k);
         zsum += (double)res * V;
         if (kDots) {  // rhs e is r (level 0 of the PCG's V-cycle)
-          const double dl = __ldg(delta + c);
+          const double dlc = dl[slot];
           srz += e * (double)res * V;
           sr += e * V;
-          sdz += (double)res * dl * V;
-          sd += dl * V;
+          sdz += (double)res * dlc * V;
+          sd += dlc * V;
         }
       }
     }
@@ -463,11 +502,12 @@ struct SweepOp {
   __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
+// Three blocks per SM (the shared-memory ring allows three).
 // kDots: also finish the flexible PCG's preconditioned dots of this
 // iteration (what the dots kernel computes, fluid.py:4604-4611 / 4590-4601):
 // rz_new = <r, z'>_V, beta_num = <delta, z'>_V and beta, from the five sums.
 template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots>
-__global__ void __launch_bounds__(kMK* kTY)
+__global__ void __launch_bounds__(kMK* kTY, 3)
     km_sweep(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
              const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
              TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc,
@@ -587,7 +627,9 @@ template <bool kCopy, bool kAux>
 struct SpmvOp {
   static constexpr bool kPrepare = false;
   template <typename T>
-  __device__ __forceinline__ void prepare(const MarchGeom&, T*, const uint8_t*, int) const {}
+  __device__ __forceinline__ void prepare(const MarchGeom&, T*, const uint8_t*, int, int) const {}
+  __device__ __forceinline__ void prefetch_prologue(const MarchGeom&) {}
+  __device__ __forceinline__ void prefetch(const MarchGeom&, int, int64_t, int64_t) {}
   const LevelDev& L;
   double* __restrict__ d_new;
   double* __restrict__ Ad;
@@ -605,7 +647,7 @@ struct SpmvOp {
   }
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, bool active, unsigned m, double,
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, int, bool active, unsigned m, double,
                                        double kxm, double kxp, const RowCoef& rc, const V& val) {
     const bool solid = (m & M_SOLID) != 0;
     double x0 = dir(val, 0, 0, 0);
@@ -626,7 +668,7 @@ struct SpmvOp {
 };
 
 template <bool kCopy, bool kAux>
-__global__ void __launch_bounds__(kMK* kTY)
+__global__ void __launch_bounds__(kMK* kTY, 3)
     km_spmv_dir(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_z,
                 const __grid_constant__ CUtensorMap map_d, const __grid_constant__ CUtensorMap map_m,
                 double* __restrict__ d_new, double* __restrict__ Ad, int outlet, double* partials, CgScalars* sc) {
@@ -671,7 +713,9 @@ template <typename TP, bool kNegR, bool kAux>
 struct RestrictOp {
   static constexpr bool kPrepare = false;
   template <typename T>
-  __device__ __forceinline__ void prepare(const MarchGeom&, T*, const uint8_t*, int) const {}
+  __device__ __forceinline__ void prepare(const MarchGeom&, T*, const uint8_t*, int, int) const {}
+  __device__ __forceinline__ void prefetch_prologue(const MarchGeom&) {}
+  __device__ __forceinline__ void prefetch(const MarchGeom&, int, int64_t, int64_t) {}
   const LevelDev& L;
   int outlet;
   int cnx, cny, cnz;
@@ -682,8 +726,8 @@ struct RestrictOp {
   int ocount;
 
   template <class V>
-  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int t, bool, unsigned m, double e, double kxm,
-                                       double kxp, const RowCoef& rc, const V& val) {
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int t, int, bool, unsigned m, double e,
+                                       double kxm, double kxp, const RowCoef& rc, const V& val) {
     if (m & M_SOLID) {
       rsolid[i & 1][t] = 1;
       rs[i & 1][t] = 0.0;
@@ -754,7 +798,7 @@ struct RestrictOp {
 };
 
 template <typename TP, bool kNegR, bool kAux>
-__global__ void __launch_bounds__(kMK* kTY)
+__global__ void __launch_bounds__(kMK* kTY, 3)
     km_restrict(LevelDev F, int chunk, const __grid_constant__ CUtensorMap map_p,
                 const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m, int outlet,
                 int cnx, int cny, int cnz, float* __restrict__ crhs, CgScalars* sc) {
