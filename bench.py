@@ -253,7 +253,8 @@ def main() -> None:
     iters_mean = float(np.mean(iters)) if iters else 0.0
     # (the CG dots are finished inside the V-cycle's last level-0 sweep, so
     # their stand-alone kernel is not on the path)
-    per_iteration = {"sweep_l0": 4, "spmv_dir": 1, "cg_update": 1, "restrict_l0": 1}
+    per_iteration = {"sweep0_l0": 1, "sweep_l0": 1, "sweep_prolong_l0": 1, "sweep_dots_l0": 1, "spmv_dir": 1,
+                     "cg_update": 1, "restrict_l0": 1}
     fam_stats = {}
     for fam, per_it in per_iteration.items():
         avg_ms, nbytes = _native.kernel_replay(scene.fluid._plan, fam, reps=args.replay_reps)
@@ -264,6 +265,12 @@ def main() -> None:
             "launches_per_step": per_it * iters_mean,
             "ms_per_step": avg_ms * per_it * iters_mean,
         }
+    # the whole preconditioner (levels 0-6 of the V-cycle, dots included), time only
+    vc_ms, _ = _native.kernel_replay(scene.fluid._plan, "vcycle", reps=max(1, args.replay_reps // 5))
+    level0_us = sum(fam_stats[f]["avg_launch_us"] for f in ("sweep0_l0", "sweep_l0", "sweep_prolong_l0",
+                                                            "sweep_dots_l0", "restrict_l0"))
+    vcycle_stats = {"avg_us": 1000.0 * vc_ms, "level0_kernels_us": level0_us,
+                    "coarse_levels_us": 1000.0 * vc_ms - level0_us, "per_step_ms": vc_ms * iters_mean}
     max_ms = max_over_ranks(elapsed_ms, world, "cuda")
     value = replica_steps_per_s(world, args.steps, max_ms)
 
@@ -383,6 +390,7 @@ def main() -> None:
                 "cg_iterations": iters,
             },
             "kernel_families": fam_stats,
+            "preconditioner": vcycle_stats,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -204,6 +204,11 @@ KERNEL_FAMILIES = {
     "cg_dots": 4,
     "p2g": 5,
     "predict": 6,
+    # replay only
+    "sweep0_l0": 16,
+    "sweep_prolong_l0": 17,
+    "sweep_dots_l0": 18,
+    "vcycle": 19,
 }
 
 

@@ -78,6 +78,32 @@ void timing_end(int family, cudaStream_t s, double bytes);
     if (_t) ::efsi::timing_end(family, stream, (double)(bytes));  \
   } while (0)
 
+// Programmatic dependent launch.  Kernels of the PCG loop are launched with
+// programmatic stream serialization (launch_pdl), so their launch and block
+// set-up overlap the drain of the kernel before them; each of them calls
+// pdl_wait() before its first global-memory access, which waits for the
+// previous grid to complete and its writes to be visible.  For a kernel
+// launched without the attribute pdl_wait() returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+bool pdl_enabled();  // false when EFSI_NO_PDL is set
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 inline unsigned next_pow2(unsigned v) {
   unsigned p = 1;
   while (p < v) p <<= 1;

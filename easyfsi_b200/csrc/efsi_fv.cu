@@ -176,6 +176,7 @@ template <typename TP, bool kNegR, bool kZero>
 __global__ void __launch_bounds__(256) k_sweep(LevelDev L, const TP* __restrict__ p, const void* rhs,
                                                TP* __restrict__ out, int outlet, double omega, ProlongSrc pr,
                                                double* partials, CgScalars* sc) {
+  pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   double zv = 0.0;
   if (active) {
@@ -245,6 +246,7 @@ __global__ void __launch_bounds__(256) k_residual(LevelDev L, const TP* __restri
 template <typename TP, bool kNegR, bool kFromP>
 __global__ void __launch_bounds__(256) k_restrict(LevelDev F, const TP* __restrict__ p_or_res, const void* rhs,
                                                   int outlet, int cnx, int cny, int cnz, float* __restrict__ crhs) {
+  pdl_wait();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z * blockDim.z + threadIdx.z;
@@ -388,6 +390,7 @@ template <typename TP, bool kNegR, bool kZero>
 __global__ void __launch_bounds__(256) kt_sweep(LevelDev L, const TP* __restrict__ p, const void* rhs,
                                                 TP* __restrict__ out, int outlet, double omega, ProlongSrc pr,
                                                 double* partials, CgScalars* sc) {
+  pdl_wait();
   const int nt = tiles_of(L.nx, L.ny, L.nz);
   const int64_t sx = (int64_t)L.ny * L.nz;
   double zsum = 0.0;
@@ -456,6 +459,7 @@ __global__ void __launch_bounds__(256) kt_spmv_dir(LevelDev L, const double* __r
                                                    const double* __restrict__ d_old, double* __restrict__ d_new,
                                                    double* __restrict__ Ad, int outlet, double* partials,
                                                    CgScalars* sc) {
+  pdl_wait();
   const int nt = tiles_of(L.nx, L.ny, L.nz);
   const int64_t sx = (int64_t)L.ny * L.nz;
   const double beta = kCopy ? 0.0 : sc->beta;
@@ -527,6 +531,7 @@ __global__ void __launch_bounds__(256) kt_cg_update(LevelDev L, double* __restri
                                                     double* __restrict__ r, const double* __restrict__ Ad,
                                                     double* __restrict__ delta, int want_means, int want_rr,
                                                     double* partials, CgScalars* sc) {
+  pdl_wait();
   const int nt = tiles_of(L.nx, L.ny, L.nz);
   const int64_t sx = (int64_t)L.ny * L.nz;
   const double alpha = sc->alpha;
@@ -593,6 +598,7 @@ template <bool kMG, bool kRestart>
 __global__ void __launch_bounds__(256) kt_cg_dots(LevelDev L, const double* __restrict__ r,
                                                   const double* __restrict__ z, const double* __restrict__ delta,
                                                   double* partials, CgScalars* sc) {
+  pdl_wait();
   const int nt = tiles_of(L.nx, L.ny, L.nz);
   const int64_t sx = (int64_t)L.ny * L.nz;
   CgScalars s;
@@ -653,6 +659,7 @@ __global__ void __launch_bounds__(256) kt_cg_dots(LevelDev L, const double* __re
 // Tiled x -= mean_x, r -= mean_r and <r, r>_V (see k_sub_mean_xr).
 __global__ void __launch_bounds__(256) kt_sub_mean_xr(LevelDev L, double* __restrict__ x, double* __restrict__ r,
                                                       double* partials, CgScalars* sc) {
+  pdl_wait();
   const int nt = tiles_of(L.nx, L.ny, L.nz);
   const int64_t sx = (int64_t)L.ny * L.nz;
   const double mx = sc->mean_x, mr = sc->mean_r;
@@ -790,6 +797,7 @@ __device__ void tail_restrict(const TailDesc& T, int l, const float* p, const fl
 }
 
 __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char tail_smem[];
   float* fpool = reinterpret_cast<float*>(tail_smem);
   // masks and the rhs of level lt into shared memory
@@ -874,6 +882,7 @@ __global__ void __launch_bounds__(256) k_spmv_dir(LevelDev L, const double* __re
                                                   const double* __restrict__ d_old, double* __restrict__ d_new,
                                                   double* __restrict__ Ad, int outlet, double* partials,
                                                   CgScalars* sc) {
+  pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   const double beta = kCopy ? 0.0 : sc->beta;
   const int zproj = sc->zproj;
@@ -932,6 +941,7 @@ __global__ void __launch_bounds__(256) k_cg_update(LevelDev L, double* __restric
                                                    double* __restrict__ r, const double* __restrict__ Ad,
                                                    double* __restrict__ delta, int want_means, int want_rr,
                                                    double* partials, CgScalars* sc) {
+  pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   const double alpha = sc->alpha;
   double px = 0.0, pr = 0.0, prr = 0.0;
@@ -976,6 +986,7 @@ __global__ void __launch_bounds__(256) k_cg_update(LevelDev L, double* __restric
 // then reduce r r V for the residual check.
 __global__ void __launch_bounds__(256) k_sub_mean_xr(LevelDev L, double* __restrict__ x, double* __restrict__ r,
                                                      double* partials, CgScalars* sc) {
+  pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   const double mx = sc->mean_x, mr = sc->mean_r;
   double prr = 0.0;
@@ -1004,6 +1015,7 @@ template <bool kMG, bool kRestart>
 __global__ void __launch_bounds__(256) k_cg_dots(LevelDev L, const double* __restrict__ r,
                                                  const double* __restrict__ z, const double* __restrict__ delta,
                                                  double* partials, CgScalars* sc) {
+  pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   CgScalars s;
   s.mean_z = sc->mean_z;
@@ -1047,6 +1059,7 @@ __global__ void __launch_bounds__(256) k_cg_dots(LevelDev L, const double* __res
 __global__ void __launch_bounds__(256) k_jacobi_precond(LevelDev L, const double* __restrict__ diag,
                                                         const double* __restrict__ r, double* __restrict__ z,
                                                         int want_mean, double* partials, CgScalars* sc) {
+  pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   double pz = 0.0;
   if (active) {
@@ -1212,6 +1225,7 @@ __global__ void __launch_bounds__(256) k_weighted_dot(LevelDev L, const double* 
 }
 
 __global__ void k_set_zproj(CgScalars* sc, int v) {
+  pdl_wait();
   if (threadIdx.x == 0) {
     sc->zproj = v;
     if (!v) sc->mean_z = 0.0;
@@ -1249,6 +1263,10 @@ unsigned long long take_capture_count() {
   unsigned long long v = g_capture_count;
   g_capture_count = 0;
   return v;
+}
+bool pdl_enabled() {
+  static const bool on = std::getenv("EFSI_NO_PDL") == nullptr;
+  return on;
 }
 
 namespace {
@@ -1841,16 +1859,16 @@ static bool launch_march_spmv(efsi_fv_plan* P, const LevelDev& L, bool copy, con
   const bool aux = L.fw != nullptr || L.iface != nullptr;
   const int sm1 = march_smem<double, 1, double, false>(), sm2 = march_smem<double, 2, double, false>();
   if (copy && aux)
-    EFSI_COUNTED km_spmv_dir<true, true><<<B.mgrid, blk, sm1, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<true, true>, B.mgrid, blk, sm1, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                     partials, sc);
   else if (copy)
-    EFSI_COUNTED km_spmv_dir<true, false><<<B.mgrid, blk, sm1, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<true, false>, B.mgrid, blk, sm1, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                      partials, sc);
   else if (aux)
-    EFSI_COUNTED km_spmv_dir<false, true><<<B.mgrid, blk, sm2, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<false, true>, B.mgrid, blk, sm2, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                      partials, sc);
   else
-    EFSI_COUNTED km_spmv_dir<false, false><<<B.mgrid, blk, sm2, s>>>(L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<false, false>, B.mgrid, blk, sm2, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                       partials, sc);
   return true;
 }
@@ -1865,7 +1883,7 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   const LevelBuf& B = P->lv[l];
   const dim3 blk(kMK, kTY);
   if (kZero) {
-    EFSI_COUNTED km_sweep0<TP, kNegR, kAux><<<sweep0_grid(B.nx, B.ny, B.nz), blk, 0, s>>>(L, rhs, out, outlet, om,
+    EFSI_COUNTED launch_pdl(km_sweep0<TP, kNegR, kAux>, sweep0_grid(B.nx, B.ny, B.nz), blk, 0, s, L, rhs, out, outlet, om,
                                                                                            partials, P->sc);
     return true;
   }
@@ -1877,19 +1895,19 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   if constexpr (std::is_same<TP, double>::value && kNegR && !kZero) {
     if (dots_delta != nullptr) {
       if (pr.pc != nullptr)
-        EFSI_COUNTED km_sweep<TP, kNegR, true, kAux, true><<<B.mgrid, blk, sm, s>>>(
+        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, true>, B.mgrid, blk, sm, s, 
             L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dots_delta);
       else
-        EFSI_COUNTED km_sweep<TP, kNegR, false, kAux, true><<<B.mgrid, blk, sm, s>>>(
+        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, true>, B.mgrid, blk, sm, s, 
             L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dots_delta);
       return true;
     }
   }
   if (pr.pc != nullptr)
-    EFSI_COUNTED km_sweep<TP, kNegR, true, kAux, false><<<B.mgrid, blk, sm, s>>>(
+    EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, false>, B.mgrid, blk, sm, s, 
         L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr);
   else
-    EFSI_COUNTED km_sweep<TP, kNegR, false, kAux, false><<<B.mgrid, blk, sm, s>>>(
+    EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, false>, B.mgrid, blk, sm, s, 
         L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr);
   return true;
 }
@@ -1917,10 +1935,10 @@ static void launch_sweep(efsi_fv_plan* P, int l, const TP* p, const void* rhs, T
     }
   }
   if (B.tiled)
-    EFSI_COUNTED kt_sweep<TP, kNegR, kZero><<<B.tgrid, dim3(kTK, kTJ), 0, s>>>(L, p, rhs, out, outlet, om, pr, partials,
+    EFSI_COUNTED launch_pdl(kt_sweep<TP, kNegR, kZero>, B.tgrid, dim3(kTK, kTJ), 0, s, L, p, rhs, out, outlet, om, pr, partials,
                                                                               P->sc);
   else
-    EFSI_COUNTED k_sweep<TP, kNegR, kZero><<<B.shape.grid, B.shape.block, 0, s>>>(L, p, rhs, out, outlet, om, pr,
+    EFSI_COUNTED launch_pdl(k_sweep<TP, kNegR, kZero>, B.shape.grid, B.shape.block, 0, s, L, p, rhs, out, outlet, om, pr,
                                                                                    partials, P->sc);
 }
 
@@ -1938,15 +1956,15 @@ static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs
     if (mp && mr && mm) {
       const int sm = march_smem<TP, 1, TR, true>();
       if (L.fw != nullptr || L.iface != nullptr)
-        EFSI_COUNTED km_restrict<TP, kNegR, true><<<B.mgrid, dim3(kMK, kTY), sm, s>>>(
+        EFSI_COUNTED launch_pdl(km_restrict<TP, kNegR, true>, B.mgrid, dim3(kMK, kTY), sm, s, 
             L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
       else
-        EFSI_COUNTED km_restrict<TP, kNegR, false><<<B.mgrid, dim3(kMK, kTY), sm, s>>>(
+        EFSI_COUNTED launch_pdl(km_restrict<TP, kNegR, false>, B.mgrid, dim3(kMK, kTY), sm, s, 
             L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
       return;
     }
   }
-  EFSI_COUNTED k_restrict<TP, kNegR, true><<<C.shape.grid, C.shape.block, 0, s>>>(L, p, rhs, outlet, C.nx, C.ny,
+  EFSI_COUNTED launch_pdl(k_restrict<TP, kNegR, true>, C.shape.grid, C.shape.block, 0, s, L, p, rhs, outlet, C.nx, C.ny,
                                                                                  C.nz, C.rhs);
 }
 
@@ -2036,7 +2054,7 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     }
     T.rhs_in = P->lv[lt].rhs;
     T.p_out = (float*)P->lv[lt].pa;
-    EFSI_COUNTED k_mg_tail<<<1, kTailThreads, P->tail_smem_bytes, s>>>(T);
+    EFSI_COUNTED launch_pdl(k_mg_tail, 1, kTailThreads, P->tail_smem_bytes, s, T);
     cur[lt] = P->lv[lt].pa;
   } else {
     // Coarsest level: `coarse` sweeps from zero.
@@ -2138,10 +2156,10 @@ static int precondition(PcgRun& R) {
     EFSI_TRY(vcycle(R.P, R.P->r, R.P->z, R.prm->outlet, R.pre, R.coarse, R.post, want_mean, R.s,
                     want_mean ? R.P->delta : nullptr, &R.dots_fused));
   } else {
-    EFSI_COUNTED k_jacobi_precond<<<R.S.grid, R.S.block, 0, R.s>>>(R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
+    EFSI_COUNTED launch_pdl(k_jacobi_precond, R.S.grid, R.S.block, 0, R.s, R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
                                                       R.P->partials, R.P->sc);
   }
-  if (!want_mean) EFSI_COUNTED k_set_zproj<<<1, 32, 0, R.s>>>(R.P->sc, 0);
+  if (!want_mean) EFSI_COUNTED launch_pdl(k_set_zproj, 1, 32, 0, R.s, R.P->sc, 0);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
@@ -2218,16 +2236,16 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   // Initial preconditioning and rz (fluid.py:6644-6673).
   EFSI_TRY(precondition(R));
   if (remove_mean) st->mean_projection_count += 1;
-  EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+  EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
   EFSI_LAUNCH_CHECK();
   EFSI_TRY(read_scalars(R));
   double rz = P->host_sc->rz;
   if (!std::isfinite(rz) || std::fabs(rz) <= 1.0e-300) {
     // Downgrade to Jacobi; the reference does not re-project z here.
     R.use_mg = false;
-    EFSI_COUNTED k_jacobi_precond<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->diag, P->r, P->z, 0, P->partials, P->sc);
-    EFSI_COUNTED k_set_zproj<<<1, 32, 0, s>>>(P->sc, 0);
-    EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+    EFSI_COUNTED launch_pdl(k_jacobi_precond, R.S.grid, R.S.block, 0, s, R.L, P->diag, P->r, P->z, 0, P->partials, P->sc);
+    EFSI_COUNTED launch_pdl(k_set_zproj, 1, 32, 0, s, P->sc, 0);
+    EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
     EFSI_LAUNCH_CHECK();
     EFSI_TRY(read_scalars(R));
     rz = P->host_sc->rz;
@@ -2255,50 +2273,50 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     if (tiled0) {
       if (copy)
         EFSI_TIMED(KF_SPMV_DIR, 25.0 * n0d, s,
-                   EFSI_COUNTED kt_spmv_dir<true><<<tg0, tblk, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                   EFSI_COUNTED launch_pdl(kt_spmv_dir<true>, tg0, tblk, 0, s, R.L, P->z, d_old, d_new, P->Ad, outlet,
                                                                        P->partials, P->sc));
       else
         EFSI_TIMED(KF_SPMV_DIR, 33.0 * n0d, s,
-                   EFSI_COUNTED kt_spmv_dir<false><<<tg0, tblk, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                   EFSI_COUNTED launch_pdl(kt_spmv_dir<false>, tg0, tblk, 0, s, R.L, P->z, d_old, d_new, P->Ad, outlet,
                                                                         P->partials, P->sc));
       return;
     }
     if (copy)
       EFSI_TIMED(KF_SPMV_DIR, 25.0 * n0d, s,
-                 EFSI_COUNTED k_spmv_dir<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                 EFSI_COUNTED launch_pdl(k_spmv_dir<true>, R.S.grid, R.S.block, 0, s, R.L, P->z, d_old, d_new, P->Ad, outlet,
                                                                               P->partials, P->sc));
     else
       EFSI_TIMED(KF_SPMV_DIR, 33.0 * n0d, s,
-                 EFSI_COUNTED k_spmv_dir<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->z, d_old, d_new, P->Ad, outlet,
+                 EFSI_COUNTED launch_pdl(k_spmv_dir<false>, R.S.grid, R.S.block, 0, s, R.L, P->z, d_old, d_new, P->Ad, outlet,
                                                                                P->partials, P->sc));
   };
   auto launch_update = [&](double* d, bool mean_now, bool want_rr) {
     if (tiled0) {
       if (R.use_mg)
         EFSI_TIMED(KF_CG_UPDATE, 56.0 * n0d, s,
-                   EFSI_COUNTED kt_cg_update<true><<<tg0, tblk, 0, s>>>(R.L, pressure, d, P->r, P->Ad, P->delta,
+                   EFSI_COUNTED launch_pdl(kt_cg_update<true>, tg0, tblk, 0, s, R.L, pressure, d, P->r, P->Ad, P->delta,
                                                                         mean_now ? 1 : 0, want_rr ? 1 : 0,
                                                                         P->partials, P->sc));
       else
         EFSI_TIMED(KF_CG_UPDATE, 48.0 * n0d, s,
-                   EFSI_COUNTED kt_cg_update<false><<<tg0, tblk, 0, s>>>(R.L, pressure, d, P->r, P->Ad, nullptr,
+                   EFSI_COUNTED launch_pdl(kt_cg_update<false>, tg0, tblk, 0, s, R.L, pressure, d, P->r, P->Ad, nullptr,
                                                                          mean_now ? 1 : 0, want_rr ? 1 : 0,
                                                                          P->partials, P->sc));
-      if (mean_now) EFSI_COUNTED kt_sub_mean_xr<<<tg0, tblk, 0, s>>>(R.L, pressure, P->r, P->partials, P->sc);
+      if (mean_now) EFSI_COUNTED launch_pdl(kt_sub_mean_xr, tg0, tblk, 0, s, R.L, pressure, P->r, P->partials, P->sc);
       return;
     }
     if (R.use_mg)
       EFSI_TIMED(KF_CG_UPDATE, 56.0 * n0d, s,
-                 EFSI_COUNTED k_cg_update<true><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, d, P->r, P->Ad, P->delta,
+                 EFSI_COUNTED launch_pdl(k_cg_update<true>, R.S.grid, R.S.block, 0, s, R.L, pressure, d, P->r, P->Ad, P->delta,
                                                                                mean_now ? 1 : 0, want_rr ? 1 : 0,
                                                                                P->partials, P->sc));
     else
       EFSI_TIMED(KF_CG_UPDATE, 48.0 * n0d, s,
-                 EFSI_COUNTED k_cg_update<false><<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, d, P->r, P->Ad, nullptr,
+                 EFSI_COUNTED launch_pdl(k_cg_update<false>, R.S.grid, R.S.block, 0, s, R.L, pressure, d, P->r, P->Ad, nullptr,
                                                                                 mean_now ? 1 : 0, want_rr ? 1 : 0,
                                                                                 P->partials, P->sc));
     if (mean_now)
-      EFSI_COUNTED k_sub_mean_xr<<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, P->r, P->partials, P->sc);
+      EFSI_COUNTED launch_pdl(k_sub_mean_xr, R.S.grid, R.S.block, 0, s, R.L, pressure, P->r, P->partials, P->sc);
   };
   auto launch_precond_dots = [&]() -> int {
     EFSI_TRY(precondition(R));
@@ -2306,21 +2324,21 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     if (tiled0) {
       if (R.use_mg)
         EFSI_TIMED(KF_CG_DOTS, 25.0 * n0d, s,
-                   EFSI_COUNTED kt_cg_dots<true, false><<<tg0, tblk, 0, s>>>(R.L, P->r, P->z, P->delta, P->partials,
+                   EFSI_COUNTED launch_pdl(kt_cg_dots<true, false>, tg0, tblk, 0, s, R.L, P->r, P->z, P->delta, P->partials,
                                                                              P->sc));
       else
         EFSI_TIMED(KF_CG_DOTS, 17.0 * n0d, s,
-                   EFSI_COUNTED kt_cg_dots<false, false><<<tg0, tblk, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials,
+                   EFSI_COUNTED launch_pdl(kt_cg_dots<false, false>, tg0, tblk, 0, s, R.L, P->r, P->z, nullptr, P->partials,
                                                                               P->sc));
       return EFSI_OK;
     }
     if (R.use_mg)
       EFSI_TIMED(KF_CG_DOTS, 25.0 * n0d, s,
-                 EFSI_COUNTED k_cg_dots<true, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, P->delta,
+                 EFSI_COUNTED launch_pdl(k_cg_dots<true, false>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, P->delta,
                                                                                     P->partials, P->sc));
     else
       EFSI_TIMED(KF_CG_DOTS, 17.0 * n0d, s,
-                 EFSI_COUNTED k_cg_dots<false, false><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr,
+                 EFSI_COUNTED launch_pdl(k_cg_dots<false, false>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr,
                                                                                      P->partials, P->sc));
     return EFSI_OK;
   };
@@ -2435,7 +2453,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
         }
         EFSI_TRY(precondition(R));
         if (remove_mean) st->mean_projection_count += 1;
-        EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+        EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
         EFSI_LAUNCH_CHECK();
         EFSI_TRY(read_scalars(R));
         rz = P->host_sc->rz;
@@ -2467,7 +2485,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       }
       EFSI_TRY(precondition(R));
       if (remove_mean) st->mean_projection_count += 1;
-      EFSI_COUNTED k_cg_dots<false, true><<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->z, nullptr, P->partials, P->sc);
+      EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
       EFSI_LAUNCH_CHECK();
       EFSI_TRY(read_scalars(R));
       rz = P->host_sc->rz;
@@ -2591,10 +2609,10 @@ int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double*
         if (P->lv[0].march && launch_march_spmv(P, L, false, P->z, P->d0, P->d1, P->Ad, 0, P->partials, P->sc, s))
           break;
         if (P->lv[0].tiled)
-          EFSI_COUNTED kt_spmv_dir<false><<<P->lv[0].tgrid, dim3(kTK, kTJ), 0, s>>>(L, P->z, P->d0, P->d1, P->Ad, 0,
+          EFSI_COUNTED launch_pdl(kt_spmv_dir<false>, P->lv[0].tgrid, dim3(kTK, kTJ), 0, s, L, P->z, P->d0, P->d1, P->Ad, 0,
                                                                                     P->partials, P->sc);
         else
-          EFSI_COUNTED k_spmv_dir<false><<<S.grid, S.block, 0, s>>>(L, P->z, P->d0, P->d1, P->Ad, 0, P->partials,
+          EFSI_COUNTED launch_pdl(k_spmv_dir<false>, S.grid, S.block, 0, s, L, P->z, P->d0, P->d1, P->Ad, 0, P->partials,
                                                                     P->sc);
         break;
       case KF_SWEEP_L0:
@@ -2605,11 +2623,11 @@ int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double*
       case KF_CG_UPDATE:
         bytes = 56.0 * n0;
         if (P->lv[0].tiled)
-          EFSI_COUNTED kt_cg_update<true><<<P->lv[0].tgrid, dim3(kTK, kTJ), 0, s>>>(L, P->b, P->d0, P->diag, P->Ad,
+          EFSI_COUNTED launch_pdl(kt_cg_update<true>, P->lv[0].tgrid, dim3(kTK, kTJ), 0, s, L, P->b, P->d0, P->diag, P->Ad,
                                                                                     P->delta, 0, 0, P->partials,
                                                                                     P->sc);
         else
-          EFSI_COUNTED k_cg_update<true><<<S.grid, S.block, 0, s>>>(L, P->b, P->d0, P->diag, P->Ad, P->delta, 0, 0,
+          EFSI_COUNTED launch_pdl(k_cg_update<true>, S.grid, S.block, 0, s, L, P->b, P->d0, P->diag, P->Ad, P->delta, 0, 0,
                                                                     P->partials, P->sc);
         break;
       case KF_RESTRICT_L0: {
@@ -2625,11 +2643,40 @@ int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double*
       case KF_CG_DOTS:
         bytes = 25.0 * n0;
         if (P->lv[0].tiled)
-          EFSI_COUNTED kt_cg_dots<true, false><<<P->lv[0].tgrid, dim3(kTK, kTJ), 0, s>>>(L, P->r, P->z, P->delta,
+          EFSI_COUNTED launch_pdl(kt_cg_dots<true, false>, P->lv[0].tgrid, dim3(kTK, kTJ), 0, s, L, P->r, P->z, P->delta,
                                                                                          P->partials, P->sc);
         else
-          EFSI_COUNTED k_cg_dots<true, false><<<S.grid, S.block, 0, s>>>(L, P->r, P->z, P->delta, P->partials, P->sc);
+          EFSI_COUNTED launch_pdl(k_cg_dots<true, false>, S.grid, S.block, 0, s, L, P->r, P->z, P->delta, P->partials, P->sc);
         break;
+      case 16:  // zero-guess level-0 sweep
+        bytes = 17.0 * n0;
+        launch_sweep<double, true, true>(P, 0, nullptr, P->r, (double*)P->lv[0].pb, 0, om, none, nullptr, s);
+        break;
+      case 17: {  // level-0 sweep with the prolongation from level 1 fused in
+        if (P->n_levels < 2) {
+          set_error("replay of the prolongation sweep needs two levels");
+          return EFSI_ERR_ARG;
+        }
+        const LevelBuf& C = P->lv[1];
+        ProlongSrc pr{(const float*)C.pa, C.nx, C.ny, C.nz, P->uniform ? 1.0f : 0.7f};
+        bytes = 25.0 * n0 + 4.0 * (double)C.n;
+        launch_sweep<double, true, false>(P, 0, (const double*)P->lv[0].pa, P->r, (double*)P->lv[0].pb, 0, om, pr,
+                                          nullptr, s);
+        break;
+      }
+      case 18: {  // the V-cycle's last level-0 sweep with the PCG dots finished in it
+        bool fused = false;
+        bytes = 33.0 * n0;
+        launch_sweep<double, true, false>(P, 0, (const double*)P->lv[0].pa, P->r, (double*)P->lv[0].pb, 0, om, none,
+                                          P->partials, s, P->delta, &fused);
+        break;
+      }
+      case 19: {  // one whole MG preconditioner application (2 / 24 / 2), dots included
+        bool fused = false;
+        bytes = 0.0;  // time only
+        EFSI_TRY(vcycle(P, P->r, P->z, 0, 2, 24, 2, true, s, P->delta, &fused));
+        break;
+      }
       default:
         set_error("family not supported by the replay");
         return EFSI_ERR_ARG;

@@ -413,27 +413,36 @@ struct SweepOp {
   static constexpr int kCols = kMK + 2, kCells = (kMJ + 2) * kCols;
   static constexpr int kPCells = (kCells + kMK * kTY - 1) / (kMK * kTY);
   float pcv[2][kPCells];
+  // per-thread constants of those cells: in-plane coarse offset, offset in
+  // the value tile, and mask-tile index (-1: halo cell, prolonged always)
+  int coff[kPCells], toff[kPCells], moff[kPCells];
 
-  __device__ __forceinline__ void load_coarse(const MarchGeom& g, int plane, int slot) {
-    const int ci = min(min(max(plane, 0), L.nx - 1) / 2, pr.cnx - 1);
+  __device__ __forceinline__ void load_coarse(int plane, int slot) {
+    const int64_t cplane = (int64_t)min(min(max(plane, 0), L.nx - 1) / 2, pr.cnx - 1) * pr.cny * pr.cnz;
 #pragma unroll
-    for (int q = 0; q < kPCells; ++q) {
-      const int e = min(g.ty * kMK + g.tx + q * kMK * kTY, kCells - 1);
-      const int r = e / kCols, cc = e - r * kCols;
-      const int cj = min(max(g.j0 - 1 + r, 0) / 2, pr.cny - 1), ck = min(max(g.k0 - 1 + cc, 0) / 2, pr.cnz - 1);
-      pcv[slot][q] = __ldg(pr.pc + cidx(ci, cj, ck, pr.cny, pr.cnz));
-    }
+    for (int q = 0; q < kPCells; ++q) pcv[slot][q] = __ldg(pr.pc + cplane + coff[q]);
   }
   __device__ __forceinline__ void prefetch_prologue(const MarchGeom& g) {
     if (kProlong) {
-      load_coarse(g, g.ib - 1, 0);
-      load_coarse(g, g.ib, 1);
+      using Lay = StageLayout<TP, 1, TP, true>;
+#pragma unroll
+      for (int q = 0; q < kPCells; ++q) {
+        const int e = g.ty * kMK + g.tx + q * kMK * kTY;
+        const int ec = min(e, kCells - 1);
+        const int r = ec / kCols, cc = ec - r * kCols;
+        const int cj = min(max(g.j0 - 1 + r, 0) / 2, pr.cny - 1), ck = min(max(g.k0 - 1 + cc, 0) / 2, pr.cnz - 1);
+        coff[q] = cj * pr.cnz + ck;
+        toff[q] = e < kCells ? r * Lay::kW + Lay::kPad - 1 + cc : -1;
+        moff[q] = (r >= 1 && r <= kMJ && cc >= 1 && cc <= kMK) ? (r - 1) * kMK + cc - 1 : -1;
+      }
+      load_coarse(g.ib - 1, 0);
+      load_coarse(g.ib, 1);
     }
   }
   __device__ __forceinline__ void prefetch(const MarchGeom& g, int i, int64_t pbase, int64_t sx) {
     if (kProlong) {
-      load_coarse(g, i + 1, 0);
-      load_coarse(g, i + 2, 1);
+      load_coarse(i + 1, 0);
+      load_coarse(i + 2, 1);
     }
     if (kDots) {
 #pragma unroll
@@ -450,16 +459,12 @@ struct SweepOp {
   // unconditionally.  Coarse indices are clamped, so cells outside the level
   // take an in-level coarse value that is never used.
   static constexpr bool kPrepare = kProlong;
-  __device__ __forceinline__ void prepare(const MarchGeom& g, TP* tile, const uint8_t* mtile, int, int slot) const {
-    using Lay = StageLayout<TP, 1, TP, true>;
+  __device__ __forceinline__ void prepare(const MarchGeom&, TP* tile, const uint8_t* mtile, int, int slot) const {
 #pragma unroll
     for (int q = 0; q < kPCells; ++q) {
-      const int e = g.ty * kMK + g.tx + q * kMK * kTY;
-      if (e >= kCells) break;
-      const int r = e / kCols, cc = e - r * kCols;
-      const bool inner = r >= 1 && r <= kMJ && cc >= 1 && cc <= kMK;
-      if (inner && mtile != nullptr && !(mtile[(r - 1) * kMK + cc - 1] & M_FLUID)) continue;
-      TP* v = tile + r * Lay::kW + Lay::kPad - 1 + cc;
+      if (toff[q] < 0) break;
+      if (moff[q] >= 0 && mtile != nullptr && !(mtile[moff[q]] & M_FLUID)) continue;
+      TP* v = tile + toff[q];
       const float corr = __fmul_rn(pr.scale, pcv[slot][q]);
       if (sizeof(TP) == 8)
         *v = (TP)__dadd_rn((double)*v, (double)corr);
@@ -485,14 +490,14 @@ struct SweepOp {
         res = (TP)(x0 + omega * (jv - x0));
       }
       if ((want_sum || kDots) && (m & M_FLUID)) {
-        const double V = vol64(L, i, j, k);
-        zsum += (double)res * V;
+        const double vol = vol64(L, i, j, k);
+        zsum += (double)res * vol;
         if (kDots) {  // rhs e is r (level 0 of the PCG's V-cycle)
           const double dlc = dl[slot];
-          srz += e * (double)res * V;
-          sr += e * V;
-          sdz += (double)res * dlc * V;
-          sd += dlc * V;
+          srz += e * (double)res * vol;
+          sr += e * vol;
+          sdz += (double)res * dlc * vol;
+          sd += dlc * vol;
         }
       }
     }
@@ -512,6 +517,7 @@ __global__ void __launch_bounds__(kMK* kTY, 3)
              const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
              TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc,
              const double* __restrict__ delta) {
+  pdl_wait();
   using TR = typename std::conditional<kNegR, double, TP>::type;
   MarchGeom g;
   const bool any = march_geom(L, chunk, g);
@@ -568,6 +574,7 @@ template <typename TP, bool kNegR, bool kAux>
 __global__ void __launch_bounds__(kMK* kTY)
     km_sweep0(LevelDev L, const void* rhs, TP* __restrict__ out, int outlet, double omega, double* partials,
               CgScalars* sc) {
+  pdl_wait();
   const int k = (int)(blockIdx.x * kMK + threadIdx.x), j = (int)(blockIdx.y * kTY + threadIdx.y);
   const int i0 = (int)blockIdx.z * kSweep0Planes;
   double zsum = 0.0;
@@ -672,6 +679,7 @@ __global__ void __launch_bounds__(kMK* kTY, 3)
     km_spmv_dir(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_z,
                 const __grid_constant__ CUtensorMap map_d, const __grid_constant__ CUtensorMap map_m,
                 double* __restrict__ d_new, double* __restrict__ Ad, int outlet, double* partials, CgScalars* sc) {
+  pdl_wait();
   MarchGeom g;
   const bool any = march_geom(L, chunk, g);
   SpmvOp<kCopy, kAux> op{L, d_new, Ad, outlet, kCopy ? 0.0 : sc->beta, sc->mean_z, sc->zproj, 0.0};
@@ -802,6 +810,7 @@ __global__ void __launch_bounds__(kMK* kTY, 3)
     km_restrict(LevelDev F, int chunk, const __grid_constant__ CUtensorMap map_p,
                 const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m, int outlet,
                 int cnx, int cny, int cnz, float* __restrict__ crhs, CgScalars* sc) {
+  pdl_wait();
   using TR = typename std::conditional<kNegR, double, TP>::type;
   __shared__ double rs[2][kMJ * kMK];
   __shared__ unsigned char rsolid[2][kMJ * kMK];

@@ -1,0 +1,73 @@
+"""The c2 workload at full size (128 x 128 x 256 graded grid, ~201k particles,
+8066 markers) through the drop-in API, checked by properties that hold at any
+size: the pressure solve reaches its true-residual tolerance and removes the
+divergence, the MPM transfer conserves momentum with det F ~ 1, and the marker
+force spreading conserves force (action = reaction).  The oracle checks the
+same kernels element by element on smaller grids (test_gpu_parity.py).
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scene():
+    from easyfsi_b200.scenarios import CONFIGS, CoupledScene
+
+    return CoupledScene(CONFIGS["c2"])
+
+
+def test_c2_projection_reaches_tolerance_and_removes_divergence(scene):
+    cfg, fl = scene.cfg, scene.fluid
+    fl.predict(cfg.dt_s)
+    fl.compute_divergence()
+    before = fl.divergence_stats()["l2"]
+    fl.project(iterations=cfg.cg_max_iterations, dt_s=cfg.dt_s, pressure_solver="fv_cg",
+               cg_tolerance=cfg.cg_tolerance, cg_preconditioner="fv_multigrid", read_report=False)
+    assert fl.last_cg_converged
+    assert fl.last_cg_used_multigrid
+    assert fl.last_cg_relative_residual <= cfg.cg_tolerance * (1.0 + 1e-6)
+    assert 0 < fl.last_cg_iterations < cfg.cg_max_iterations
+    fl.compute_divergence()
+    after = fl.divergence_stats()["l2"]
+    # velocity is f32 (as in the reference), so what remains is f32 rounding
+    # of the face velocities (~1e-7 |u| / h); the reference's own test asks
+    # for a reduction to 0.45 (tests/test_fluid.py:46-57)
+    assert before > 0.0
+    assert after <= 1.0e-2 * before
+
+
+def test_c2_marker_forces_spread_conservatively(scene):
+    fl, mk, so = scene.fluid, scene.markers, scene.solid
+    mk.sample_fluid_stress_to_marker_tractions(
+        fl.velocity, fl.pressure, fl.obstacle,
+        fl.cell_face_x_m, fl.cell_face_y_m, fl.cell_face_z_m,
+        fl.cell_center_x_m, fl.cell_center_y_m, fl.cell_center_z_m,
+        fl.cell_width_x_m, fl.cell_width_y_m, fl.cell_width_z_m,
+        fl.grid.grid_nodes, viscosity_pa_s=0.0, two_sided_pressure=False, read_report=False,
+    )
+    mk.compute_marker_forces()
+    mk.clear_mpm_external_forces(so.external_force_n, particle_count=so.particle_count, read_report=False)
+    rep = mk.scatter_marker_forces_to_mpm_particles(
+        so.external_force_n, so.x, particle_count=so.particle_count, support_radius_m=scene.radius
+    )
+    assert rep.active_marker_count > 0 and rep.invalid_marker_count == 0
+    total = np.asarray(rep.total_marker_force_n)
+    spread = so.external_force_n.to_numpy()[: so.particle_count].astype(np.float64).sum(axis=0)
+    scale = max(np.abs(total).max(), 1e-30)
+    assert np.abs(np.asarray(rep.total_mpm_external_force_n) - total).max() <= 1e-5 * scale
+    assert np.abs(spread - total).max() <= 1e-4 * scale
+
+
+def test_c2_mpm_substep_conserves_momentum(scene):
+    from easyfsi_b200.scenarios import PRIMARY_REGION_ID, SECONDARY_REGION_ID
+
+    cfg, so = scene.cfg, scene.solid
+    rep = so.step(dt_s=cfg.dt_s / cfg.solid_substeps, mu_pa=scene.mu_pa, lambda_pa=scene.lambda_pa,
+                  primary_region_id=PRIMARY_REGION_ID, secondary_region_id=SECONDARY_REGION_ID)
+    assert rep.particle_count == so.particle_count
+    assert rep.active_grid_nodes > 0
+    assert rep.transfer_relative_error < 2.0e-5
+    assert rep.max_abs_j == pytest.approx(1.0, abs=1e-3)
