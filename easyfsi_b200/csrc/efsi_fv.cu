@@ -707,6 +707,8 @@ struct TailDesc {
   LevelDev L[kTailMaxLevels];
   int foff[kTailMaxLevels];  // float offset of level l's block (pA, pB, rhs) in shared memory
   int moff[kTailMaxLevels];  // byte offset of level l's mask copy
+  int coff[kTailMaxLevels];  // byte offset of level l's row table: 6 face coefficients + denominator (f64, SoA)
+  int noff[kTailMaxLevels];  // byte offset of level l's neighbour table: 6 cell indices (int, SoA)
   const float* rhs_in;       // rhs of level lt (written by the restriction from lt - 1)
   float* p_out;              // final iterate of level lt
 };
@@ -718,50 +720,118 @@ __device__ __forceinline__ void tail_ijk(const LevelDev& L, int t, int& i, int& 
   i = ij / L.ny;
 }
 
-// One Jacobi sweep of level l: src -> dst (src null: zero initial guess),
-// optionally fusing the prolongation from the coarse iterate pc of level l+1.
-__device__ void tail_sweep(const TailDesc& T, int l, const float* src, float* dst, const float* rhs,
-                           const uint8_t* mask, const float* pc) {
+// Row tables of a tail level, built once per launch: for every cell the six
+// face coefficients behind open faces (0 behind closed ones; Dirichlet face
+// weights applied), the denominator (fluid.py:4080-4221, summed in the order
+// x-, x+, y-, y+, z-, z+, then the outlet term and the interface diagonal)
+// and the six neighbour indices (the cell itself behind a closed face).  The
+// sweeps and residuals then read only shared memory; the arithmetic is that of
+// `stencil`, with closed faces contributing exact zeros.
+struct TailTables {
+  const double* a;  // [6][n]
+  const double* den;  // [n]
+  const int* nb;  // [6][n]
+  int n;
+};
+
+__device__ __forceinline__ TailTables tail_tables(const TailDesc& T, int l, unsigned char* smem) {
+  const LevelDev& L = T.L[l];
+  TailTables tb;
+  tb.n = L.nx * L.ny * L.nz;
+  tb.a = reinterpret_cast<const double*>(smem + T.coff[l]);
+  tb.den = tb.a + 6 * tb.n;
+  tb.nb = reinterpret_cast<const int*>(smem + T.noff[l]);
+  return tb;
+}
+
+__device__ void tail_build_tables(const TailDesc& T, int l, unsigned char* smem, uint8_t* ms) {
   const LevelDev& L = T.L[l];
   const int n = L.nx * L.ny * L.nz;
+  double* a = reinterpret_cast<double*>(smem + T.coff[l]);
+  double* den = a + 6 * n;
+  int* nb = reinterpret_cast<int*>(smem + T.noff[l]);
+  const int sx = L.ny * L.nz, sy = L.nz;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
     int i, j, k;
     tail_ijk(L, t, i, j, k);
-    const unsigned m = mask[t];
-    if (m & M_SOLID) {
-      dst[t] = 0.0f;
-      continue;
+    const unsigned m = L.mask[t];
+    ms[t] = (uint8_t)m;
+    const int c[6] = {i > 0 ? t - sx : t, i < L.nx - 1 ? t + sx : t, j > 0 ? t - sy : t,
+                      j < L.ny - 1 ? t + sy : t, k > 0 ? t - 1 : t, k < L.nz - 1 ? t + 1 : t};
+    double kf[6] = {__ldg(L.cxm + i), __ldg(L.cxp + i), __ldg(L.cym + j),
+                    __ldg(L.cyp + j), __ldg(L.czm + k), __ldg(L.czp + k)};
+    if (L.fw != nullptr) {
+      const double fc = (double)__ldg(L.fw + t);
+      kf[0] *= fc;
+      kf[1] *= (double)__ldg(L.fw + c[1]);
+      kf[2] *= fc;
+      kf[3] *= (double)__ldg(L.fw + c[3]);
+      kf[4] *= fc;
+      kf[5] *= (double)__ldg(L.fw + c[5]);
     }
-    auto it_at = [&](int cell, int ii, int jj, int kk, bool fluid) -> double {
-      if (src == nullptr) return 0.0;
-      float v = src[cell];
-      if (pc != nullptr && fluid) {
-        const LevelDev& C = T.L[l + 1];
-        const int ci = min(ii / 2, C.nx - 1), cj = min(jj / 2, C.ny - 1), ck = min(kk / 2, C.nz - 1);
-        v = __fadd_rn(v, __fmul_rn(T.scale, pc[(ci * C.ny + cj) * C.nz + ck]));
+    const unsigned bit[6] = {M_XM, M_XP, M_YM, M_YP, M_ZM, M_ZP};
+    double d = 0.0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const double af = (m & bit[f]) ? kf[f] : 0.0;
+      a[f * n + t] = af;
+      nb[f * n + t] = c[f];
+      d = d + af;
+    }
+    if (T.outlet && k == 0) d += L.oz;
+    d += iface_at<float>(L, t);
+    den[t] = d;
+  }
+}
+
+// Neighbour sum of row t from the tables (same order and fused multiply-adds
+// as `stencil`).
+__device__ __forceinline__ double tail_ns(const TailTables& tb, const float* p, int t) {
+  double ns = fma(tb.a[t], (double)p[tb.nb[t]], 0.0);
+#pragma unroll
+  for (int f = 1; f < 6; ++f) ns = fma(tb.a[f * tb.n + t], (double)p[tb.nb[f * tb.n + t]], ns);
+  return ns;
+}
+
+// One Jacobi sweep of level l: src -> dst (src null: zero initial guess).
+__device__ void tail_sweep(const TailTables& tb, const float* src, float* dst, const float* rhs, const uint8_t* mask,
+                           double omega) {
+  for (int t = threadIdx.x; t < tb.n; t += blockDim.x) {
+    const unsigned m = mask[t];
+    float res = 0.0f;
+    if (!(m & M_SOLID)) {
+      const double den = tb.den[t];
+      if (den > 0.0) {
+        const double ns = src != nullptr ? tail_ns(tb, src, t) : 0.0;
+        const double jv = (ns - (double)rhs[t]) / den;
+        const double pcur = src != nullptr ? (double)src[t] : 0.0;
+        res = (float)(pcur + omega * (jv - pcur));
       }
-      return (double)v;
-    };
-    auto val = [&](int64_t cell, int ii, int jj, int kk) { return it_at((int)cell, ii, jj, kk, true); };
-    double ns, den;
-    stencil(L, val, i, j, k, t, m, T.outlet, ns, den);
-    den += iface_at<float>(L, t);
-    float res;
-    if (den <= 0.0) {
-      res = 0.0f;
-    } else {
-      const double jv = (ns - (double)rhs[t]) / den;
-      const double pcur = it_at(t, i, j, k, (m & M_FLUID) != 0);
-      res = (float)(pcur + T.omega * (jv - pcur));
     }
     dst[t] = res;
   }
   __syncthreads();
 }
 
-// Residual of level l formed on the fly and volume-weighted into the rhs of l+1.
-__device__ void tail_restrict(const TailDesc& T, int l, const float* p, const float* rhs, const uint8_t* mask,
-                              float* crhs) {
+// p += s * p_coarse on the fluid cells of level l (fluid.py:5391-5406).
+__device__ void tail_prolong(const TailDesc& T, int l, float* p, const uint8_t* mask, const float* pc) {
+  const LevelDev& L = T.L[l];
+  const LevelDev& C = T.L[l + 1];
+  const int n = L.nx * L.ny * L.nz;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    if (!(mask[t] & M_FLUID)) continue;
+    int i, j, k;
+    tail_ijk(L, t, i, j, k);
+    const int ci = min(i / 2, C.nx - 1), cj = min(j / 2, C.ny - 1), ck = min(k / 2, C.nz - 1);
+    p[t] = __fadd_rn(p[t], __fmul_rn(T.scale, pc[(ci * C.ny + cj) * C.nz + ck]));
+  }
+  __syncthreads();
+}
+
+// Residual of level l formed from the tables and volume-weighted into the
+// rhs of l+1 (fluid.py:5262-5388).
+__device__ void tail_restrict(const TailDesc& T, int l, const TailTables& tb, const float* p, const float* rhs,
+                              const uint8_t* mask, float* crhs) {
   const LevelDev& F = T.L[l];
   const LevelDev& C = T.L[l + 1];
   const int nc = C.nx * C.ny * C.nz;
@@ -776,16 +846,12 @@ __device__ void tail_restrict(const TailDesc& T, int l, const float* p, const fl
           const int fi = 2 * i + oi, fj = 2 * j + oj, fk = 2 * k + ok;
           if (fi < F.nx && fj < F.ny && fk < F.nz) {
             const int f = (fi * F.ny + fj) * F.nz + fk;
-            const unsigned m = mask[f];
-            if (m & M_SOLID) {
+            if (mask[f] & M_SOLID) {
               ocount += 1;
             } else {
               const float vol = __fmul_rn(__fmul_rn(__ldg(F.wx + fi), __ldg(F.wy + fj)), __ldg(F.wz + fk));
-              double ns, den;
-              auto val = [&](int64_t cell, int, int, int) { return (double)p[cell]; };
-              stencil(F, val, fi, fj, fk, f, m, T.outlet, ns, den);
-              den += iface_at<float>(F, f);
-              const float r = (float)((double)rhs[f] - (ns - den * (double)p[f]));
+              const double ns = tail_ns(tb, p, f);
+              const float r = (float)((double)rhs[f] - (ns - tb.den[f] * (double)p[f]));
               wres = __fadd_rn(wres, __fmul_rn(r, vol));
               free_vol = __fadd_rn(free_vol, vol);
             }
@@ -800,13 +866,8 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
   pdl_wait();
   extern __shared__ __align__(16) unsigned char tail_smem[];
   float* fpool = reinterpret_cast<float*>(tail_smem);
-  // masks and the rhs of level lt into shared memory
-  for (int l = T.lt; l < T.nl; ++l) {
-    const LevelDev& L = T.L[l];
-    const int n = L.nx * L.ny * L.nz;
-    uint8_t* ms = tail_smem + T.moff[l];
-    for (int t = threadIdx.x; t < n; t += blockDim.x) ms[t] = L.mask[t];
-  }
+  // row tables and masks of every tail level, the rhs of level lt
+  for (int l = T.lt; l < T.nl; ++l) tail_build_tables(T, l, tail_smem, tail_smem + T.moff[l]);
   {
     const LevelDev& L = T.L[T.lt];
     const int n = L.nx * L.ny * L.nz;
@@ -822,19 +883,20 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
     float* buf[2] = {pa, pa + n};
     const float* rhs = pa + 2 * n;
     const uint8_t* ms = tail_smem + T.moff[l];
+    const TailTables tb = tail_tables(T, l, tail_smem);
     const bool coarsest = (l == T.nl - 1);
     const int sweeps = coarsest ? T.coarse : T.pre;
     int c = -1;
     for (int it = 0; it < sweeps; ++it) {
       const int d = (it & 1);
-      tail_sweep(T, l, c < 0 ? nullptr : buf[c], buf[d], rhs, ms, nullptr);
+      tail_sweep(tb, c < 0 ? nullptr : buf[c], buf[d], rhs, ms, T.omega);
       c = d;
     }
     cur[l] = c;
     if (!coarsest) {
       const LevelDev& C = T.L[l + 1];
       float* crhs = fpool + T.foff[l + 1] + 2 * (C.nx * C.ny * C.nz);
-      tail_restrict(T, l, buf[c], rhs, ms, crhs);
+      tail_restrict(T, l, tb, buf[c], rhs, ms, crhs);
     }
   }
   for (int l = T.nl - 2; l >= T.lt; --l) {
@@ -844,12 +906,14 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
     float* buf[2] = {pa, pa + n};
     const float* rhs = pa + 2 * n;
     const uint8_t* ms = tail_smem + T.moff[l];
+    const TailTables tb = tail_tables(T, l, tail_smem);
     const LevelDev& C = T.L[l + 1];
     const float* pc = fpool + T.foff[l + 1] + cur[l + 1] * (C.nx * C.ny * C.nz);
     int c = cur[l];
+    tail_prolong(T, l, buf[c], ms, pc);
     for (int it = 0; it < T.post; ++it) {
       const int d = 1 - c;
-      tail_sweep(T, l, buf[c], buf[d], rhs, ms, it == 0 ? pc : nullptr);
+      tail_sweep(tb, buf[c], buf[d], rhs, ms, T.omega);
       c = d;
     }
     cur[l] = c;
@@ -1417,19 +1481,26 @@ static void configure_tail(efsi_fv_plan* P) {
   cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   for (int lt = 1; lt < P->n_levels; ++lt) {
     if (P->lv[lt].n > max_cells) continue;
-    size_t floats = 0, bytes_mask = 0;
+    // layout: row tables (7 f64 per cell), iterates + rhs (3 f32 per cell),
+    // neighbour tables (6 int per cell), masks (1 byte per cell, 16-aligned)
+    size_t cells = 0, bytes_mask = 0;
     for (int l = lt; l < P->n_levels; ++l) {
-      floats += 3 * (size_t)P->lv[l].n;
+      cells += (size_t)P->lv[l].n;
       bytes_mask += ((size_t)P->lv[l].n + 15) / 16 * 16;
     }
-    const size_t total = floats * sizeof(float) + bytes_mask;
+    const size_t total = cells * (7 * sizeof(double) + 3 * sizeof(float) + 6 * sizeof(int)) + bytes_mask;
     if ((int64_t)total > (int64_t)smem_optin) continue;
-    size_t fo = 0, mo = floats * sizeof(float);
+    size_t co = 0, fo = cells * 7 * sizeof(double), no = fo + cells * 3 * sizeof(float), mo = no + cells * 6 * sizeof(int);
     for (int l = lt; l < P->n_levels; ++l) {
-      P->tail_foff[l] = (int)fo;
-      fo += 3 * (size_t)P->lv[l].n;
+      const size_t n = (size_t)P->lv[l].n;
+      P->tail_coff[l] = (int)co;
+      co += n * 7 * sizeof(double);
+      P->tail_foff[l] = (int)(fo / sizeof(float));
+      fo += n * 3 * sizeof(float);
+      P->tail_noff[l] = (int)no;
+      no += n * 6 * sizeof(int);
       P->tail_moff[l] = (int)mo;
-      mo += ((size_t)P->lv[l].n + 15) / 16 * 16;
+      mo += (n + 15) / 16 * 16;
     }
     if (cudaFuncSetAttribute(k_mg_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin) != cudaSuccess) {
       cudaGetLastError();
@@ -2051,6 +2122,8 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       T.L[l] = level_dev(P, l);
       T.foff[l] = P->tail_foff[l];
       T.moff[l] = P->tail_moff[l];
+      T.coff[l] = P->tail_coff[l];
+      T.noff[l] = P->tail_noff[l];
     }
     T.rhs_in = P->lv[lt].rhs;
     T.p_out = (float*)P->lv[lt].pa;

@@ -219,6 +219,8 @@ struct efsi_fv_plan {
   size_t tail_smem_bytes = 0;
   int tail_foff[12] = {0};
   int tail_moff[12] = {0};
+  int tail_coff[12] = {0};
+  int tail_noff[12] = {0};
   std::string graph_error;
   std::deque<PlaneMap> maps;  // deque: descriptors stay in place as the cache grows
 };
