@@ -2226,8 +2226,10 @@ static int precondition(PcgRun& R) {
   R.dots_fused = false;
   if (R.use_mg) {
     // with the zero-mean projection the V-cycle's last sweep finishes the dots
+    // (EFSI_SEPARATE_DOTS keeps them in their own kernel)
+    static const bool separate = std::getenv("EFSI_SEPARATE_DOTS") != nullptr;
     EFSI_TRY(vcycle(R.P, R.P->r, R.P->z, R.prm->outlet, R.pre, R.coarse, R.post, want_mean, R.s,
-                    want_mean ? R.P->delta : nullptr, &R.dots_fused));
+                    want_mean && !separate ? R.P->delta : nullptr, &R.dots_fused));
   } else {
     EFSI_COUNTED launch_pdl(k_jacobi_precond, R.S.grid, R.S.block, 0, R.s, R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
                                                       R.P->partials, R.P->sc);
