@@ -192,6 +192,7 @@ def main() -> None:
     ap.add_argument("--config", default="c2")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the fv_multigrid_mixed measurement")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-reps", type=int, default=50)
@@ -273,6 +274,36 @@ def main() -> None:
                     "coarse_levels_us": 1000.0 * vc_ms - level0_us, "per_step_ms": vc_ms * iters_mean}
     max_ms = max_over_ranks(elapsed_ms, world, "cuda")
     value = replica_steps_per_s(world, args.steps, max_ms)
+
+    # --- the same coupled step with the mixed-precision preconditioner (FP32
+    # level-0 V-cycle inside the FP64 flexible CG), continuing the scene ---
+    mixed = None
+    if not args.no_mixed:
+        scene.preconditioner = "fv_multigrid_mixed"
+        for _ in range(args.warmup):  # the first step captures its PCG graphs
+            scene.step()
+        torch.cuda.synchronize()
+        barrier()
+        m_iters, m_res = [], []
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            scene.step()
+            m_iters.append(scene.last_cg_iterations)
+            m_res.append(scene.fluid.last_cg_relative_residual)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        m_value = replica_steps_per_s(world, args.steps, max_over_ranks(m0.elapsed_time(m1), world, "cuda"))
+        mixed = {
+            "value": m_value,
+            "unit": "steps/s",
+            "preconditioner": "fv_multigrid_mixed: FP32 level-0 V-cycle; CG, residual, dots and scalars FP64",
+            "cg_iterations_mean": float(np.mean(m_iters)),
+            "max_relative_residual": float(max(m_res)),
+            "ratio_to_fv_multigrid": m_value / value,
+        }
+        scene.preconditioner = "fv_multigrid"
 
     # --- e2e through the public API with host-resident state ---
     e2e = None
@@ -391,6 +422,7 @@ def main() -> None:
             },
             "kernel_families": fam_stats,
             "preconditioner": vcycle_stats,
+            "mixed_precision": mixed,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

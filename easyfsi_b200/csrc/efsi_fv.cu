@@ -1442,6 +1442,12 @@ static void preload_kernels() {
       (const void*)km_spmv_dir<false, A>
       EFSI_MARCH_FNS(false), EFSI_MARCH_FNS(true),
 #undef EFSI_MARCH_FNS
+#define EFSI_MIXED_FNS(A)                                                                                       \
+  (const void*)km_sweep32<false, A, false>, (const void*)km_sweep32<false, A, true>,                           \
+      (const void*)km_sweep32<true, A, false>, (const void*)km_sweep32<true, A, true>,                         \
+      (const void*)km_sweep0<float, true, A>, (const void*)km_restrict<float, true, A>
+      EFSI_MIXED_FNS(false), EFSI_MIXED_FNS(true),
+#undef EFSI_MIXED_FNS
   };
   for (const void* f : fns) cudaFuncGetAttributes(&a, f);
   // the plane-marching kernels take up to ~70 KB of dynamic shared memory
@@ -1458,8 +1464,16 @@ static void preload_kernels() {
       {(const void*)km_restrict<float, false, A>, march_smem<float, 1, float, true>()},                           \
       {(const void*)km_spmv_dir<true, A>, march_smem<double, 1, double, false>()},                                \
       {(const void*)km_spmv_dir<false, A>, march_smem<double, 2, double, false>()}
-  const std::pair<const void*, int> dyn[] = {EFSI_MARCH_SMEM(false), EFSI_MARCH_SMEM(true)};
+#define EFSI_MIXED_SMEM(A)                                                                                        \
+  {(const void*)km_sweep32<false, A, false>, march_smem<float, 1, double, true>()},                              \
+      {(const void*)km_sweep32<false, A, true>, march_smem<float, 1, double, true>()},                           \
+      {(const void*)km_sweep32<true, A, false>, march_smem<float, 1, double, true>()},                           \
+      {(const void*)km_sweep32<true, A, true>, march_smem<float, 1, double, true>()},                            \
+      {(const void*)km_restrict<float, true, A>, march_smem<float, 1, double, true>()}
+  const std::pair<const void*, int> dyn[] = {EFSI_MARCH_SMEM(false), EFSI_MARCH_SMEM(true), EFSI_MIXED_SMEM(false),
+                                             EFSI_MIXED_SMEM(true)};
 #undef EFSI_MARCH_SMEM
+#undef EFSI_MIXED_SMEM
   for (const auto& d : dyn) cudaFuncSetAttribute(d.first, cudaFuncAttributeMaxDynamicSharedMemorySize, d.second);
   cudaGetLastError();
 }
@@ -1615,6 +1629,11 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
       set_error("cudaMalloc failed for level iterates");
       return fail(EFSI_ERR_CUDA);
     }
+    if (l == 0 && (cudaMalloc(&B.pa32, B.n * sizeof(float)) != cudaSuccess ||
+                   cudaMalloc(&B.pb32, B.n * sizeof(float)) != cudaSuccess)) {
+      set_error("cudaMalloc failed for the mixed-precision level-0 iterates");
+      return fail(EFSI_ERR_CUDA);
+    }
     if (l > 0) {
       if (cudaMalloc(&B.rhs, B.n * sizeof(float)) != cudaSuccess ||
           cudaMalloc(&B.obs, B.n * sizeof(int32_t)) != cudaSuccess) {
@@ -1669,6 +1688,8 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
     cudaFree(B.iface);
     cudaFree(B.pa);
     cudaFree(B.pb);
+    cudaFree(B.pa32);
+    cudaFree(B.pb32);
     cudaFree(B.rhs);
   }
   double* vecs[] = {P->r, P->z, P->d0, P->d1, P->Ad, P->delta, P->b, P->diag, P->partials};
@@ -1864,7 +1885,8 @@ namespace efsi {
 // ---------------------------------------------------------------------------
 // TMA descriptors of level fields for the plane-marching kernels
 // ---------------------------------------------------------------------------
-enum : int { MAP_VALUE = 0, MAP_RHS = 1, MAP_MASK = 2 };
+// MAP_VALUE32: an FP32 value tile on level 0 (the mixed-precision V-cycle)
+enum : int { MAP_VALUE = 0, MAP_RHS = 1, MAP_MASK = 2, MAP_VALUE32 = 3 };
 
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -1891,15 +1913,15 @@ static const CUtensorMap* plane_map(efsi_fv_plan* P, int l, const void* ptr, int
   auto enc = tensor_map_encoder();
   if (enc == nullptr || ptr == nullptr || (reinterpret_cast<uintptr_t>(ptr) & 15u) != 0) return nullptr;
   const LevelBuf& B = P->lv[l];
-  const int es = kind == MAP_MASK ? 1 : (l == 0 ? 8 : 4);
+  const int es = kind == MAP_MASK ? 1 : (l == 0 && kind != MAP_VALUE32 ? 8 : 4);
   if (((size_t)B.nz * es) % 16 != 0) return nullptr;
   const CUtensorMapDataType dt = kind == MAP_MASK ? CU_TENSOR_MAP_DATA_TYPE_UINT8
-                                 : l == 0         ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                 : es == 8        ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   const cuuint64_t dims[3] = {(cuuint64_t)B.nz, (cuuint64_t)B.ny, (cuuint64_t)B.nx};
   const cuuint64_t strides[2] = {(cuuint64_t)B.nz * es, (cuuint64_t)B.nz * B.ny * es};
   cuuint32_t box[3] = {(cuuint32_t)kMK, (cuuint32_t)kMJ, 1u};
-  if (kind == MAP_VALUE) {
+  if (kind == MAP_VALUE || kind == MAP_VALUE32) {
     box[0] = (cuuint32_t)(kMK + 2 * (16 / es));
     box[1] = (cuuint32_t)(kMJ + 2);
   }
@@ -1983,6 +2005,35 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   return true;
 }
 
+// Level-0 sweep of the mixed-precision V-cycle (FP32 iterate and arithmetic);
+// out64 (with partials, and dots_delta when the PCG dots are finished in it)
+// receives the f64 result.  False when the fields cannot be streamed.
+static bool launch_sweep32(efsi_fv_plan* P, const float* p, const double* r, float* out, double* out64, int outlet,
+                           double om, ProlongSrc pr, double* partials, const double* dots_delta, cudaStream_t s) {
+  LevelDev L = level_dev(P, 0);
+  const LevelBuf& B = P->lv[0];
+  const CUtensorMap* mp = plane_map(P, 0, p, MAP_VALUE32);
+  const CUtensorMap* mr = plane_map(P, 0, r, MAP_RHS);
+  const CUtensorMap* mm = plane_map(P, 0, B.mask, MAP_MASK);
+  if (!B.march || !mp || !mr || !mm) return false;
+  const dim3 blk(kMK, kTY);
+  const int sm = march_smem<float, 1, double, true>();
+  const bool aux = L.fw != nullptr || L.iface != nullptr, pro = pr.pc != nullptr, dots = dots_delta != nullptr;
+#define EFSI_SWEEP32(PRO, AUX, DOTS)                                                                              \
+  EFSI_COUNTED launch_pdl(km_sweep32<PRO, AUX, DOTS>, B.mgrid, blk, sm, s, L, B.mchunk, *mp, *mr, *mm, out, out64, \
+                          outlet, om, pr, partials, P->sc, dots_delta)
+  if (pro && aux && dots) EFSI_SWEEP32(true, true, true);
+  else if (pro && aux) EFSI_SWEEP32(true, true, false);
+  else if (pro && dots) EFSI_SWEEP32(true, false, true);
+  else if (pro) EFSI_SWEEP32(true, false, false);
+  else if (aux && dots) EFSI_SWEEP32(false, true, true);
+  else if (aux) EFSI_SWEEP32(false, true, false);
+  else if (dots) EFSI_SWEEP32(false, false, true);
+  else EFSI_SWEEP32(false, false, false);
+#undef EFSI_SWEEP32
+  return true;
+}
+
 // One smoother sweep of level l (plane-marching kernel when the level is
 // large enough, else the per-cell kernel).
 // With dots_delta (level 0, the last sweep of the PCG's V-cycle, partials
@@ -2021,7 +2072,7 @@ static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs
   const LevelBuf& C = P->lv[l + 1];
   if (B.march) {
     using TR = typename std::conditional<kNegR, double, TP>::type;
-    const CUtensorMap* mp = plane_map(P, l, p, MAP_VALUE);
+    const CUtensorMap* mp = plane_map(P, l, p, (l == 0 && sizeof(TP) == 4) ? MAP_VALUE32 : MAP_VALUE);
     const CUtensorMap* mr = plane_map(P, l, rhs, MAP_RHS);
     const CUtensorMap* mm = plane_map(P, l, B.mask, MAP_MASK);
     if (mp && mr && mm) {
@@ -2044,8 +2095,11 @@ static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs
 // The result lands in z; when `want_mean` the last sweep also reduces the
 // fluid z V sum so consumers can apply the zero-mean projection on the fly.
 // ---------------------------------------------------------------------------
+// mixed: level 0 runs in FP32 (fv_multigrid_mixed; the caller checks that
+// level 0 has the plane-marching kernels and more than one level exists).
 static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int pre, int coarse, int post,
-                  bool want_mean, cudaStream_t s, const double* dots_delta = nullptr, bool* dots_done = nullptr) {
+                  bool want_mean, cudaStream_t s, const double* dots_delta = nullptr, bool* dots_done = nullptr,
+                  bool mixed = false) {
   pre = std::max(1, pre);
   coarse = std::max(1, coarse);
   post = std::max(1, post);
@@ -2081,10 +2135,21 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     LevelDev L = level_dev(P, l);
     LevelBuf& B = P->lv[l];
     void* bufs[2] = {B.pa, B.pb};
+    if (l == 0 && mixed) {
+      bufs[0] = B.pa32;
+      bufs[1] = B.pb32;
+    }
     const void* c = nullptr;
     for (int it = 0; it < pre; ++it) {
       void* dst = bufs[it & 1];
-      if (l == 0) {
+      if (l == 0 && mixed) {
+        if (it == 0)
+          launch_sweep<float, true, true>(P, 0, nullptr, r, (float*)dst, outlet, om, none, nullptr, s);
+        else if (!launch_sweep32(P, (const float*)c, r, (float*)dst, nullptr, outlet, om, none, nullptr, nullptr, s)) {
+          set_error("the mixed-precision V-cycle needs the plane-marching kernels on level 0");
+          return EFSI_ERR_ARG;
+        }
+      } else if (l == 0) {
         if (it == 0)
           EFSI_TIMED(KF_SWEEP_L0, 17.0 * n0, s,
                      (launch_sweep<double, true, true>(P, 0, nullptr, r, (double*)dst, outlet, om, none, nullptr, s)));
@@ -2102,7 +2167,9 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     }
     cur[l] = c;
     const LevelBuf& C = P->lv[l + 1];
-    if (l == 0)
+    if (l == 0 && mixed)
+      launch_restrict<float, true>(P, 0, (const float*)c, r, outlet, s);
+    else if (l == 0)
       EFSI_TIMED(KF_RESTRICT_L0, 17.0 * B.n + 4.0 * C.n, s,
                  (launch_restrict<double, true>(P, 0, (const double*)c, r, outlet, s)));
     else
@@ -2152,14 +2219,22 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     const LevelBuf& C = P->lv[l + 1];
     ProlongSrc pr{(const float*)cur[l + 1], C.nx, C.ny, C.nz, scale};
     const void* c = cur[l];
-    void* other = (c == B.pa) ? B.pb : B.pa;
+    void* other = (l == 0 && mixed) ? (void*)((c == B.pa32) ? B.pb32 : B.pa32) : ((c == B.pa) ? B.pb : B.pa);
     void* seq[2] = {other, const_cast<void*>(c)};
     for (int it = 0; it < post; ++it) {
       const bool last = (it == post - 1);
       void* dst = (l == 0 && last) ? (void*)z : seq[it & 1];
       ProlongSrc p_use = (it == 0) ? pr : none;
       double* part = (l == 0 && last) ? partials : nullptr;
-      if (l == 0)
+      if (l == 0 && mixed) {
+        const double* dd = last ? dots_delta : nullptr;
+        if (!launch_sweep32(P, (const float*)c, r, last ? nullptr : (float*)dst, last ? z : nullptr, outlet, om,
+                            p_use, part, dd, s)) {
+          set_error("the mixed-precision V-cycle needs the plane-marching kernels on level 0");
+          return EFSI_ERR_ARG;
+        }
+        if (dd != nullptr && dots_done != nullptr) *dots_done = true;
+      } else if (l == 0)
         EFSI_TIMED(KF_SWEEP_L0, 25.0 * n0 + (it == 0 ? 4.0 * C.n : 0.0), s,
                    (launch_sweep<double, true, false>(P, 0, (const double*)c, r, (double*)dst, outlet, om, p_use, part,
                                                       s, last ? dots_delta : nullptr, dots_done)));
@@ -2208,6 +2283,7 @@ struct PcgRun {
   double* d_nxt;
   bool copy_next;  // next SpMV starts a fresh direction d = z'
   bool dots_fused;  // the last preconditioner sweep also finished the PCG dots
+  bool mixed;       // FP32 level-0 V-cycle
 };
 
 static int read_scalars(PcgRun& R) {
@@ -2229,7 +2305,7 @@ static int precondition(PcgRun& R) {
     // (EFSI_SEPARATE_DOTS keeps them in their own kernel)
     static const bool separate = std::getenv("EFSI_SEPARATE_DOTS") != nullptr;
     EFSI_TRY(vcycle(R.P, R.P->r, R.P->z, R.prm->outlet, R.pre, R.coarse, R.post, want_mean, R.s,
-                    want_mean && !separate ? R.P->delta : nullptr, &R.dots_fused));
+                    want_mean && !separate ? R.P->delta : nullptr, &R.dots_fused, R.mixed));
   } else {
     EFSI_COUNTED launch_pdl(k_jacobi_precond, R.S.grid, R.S.block, 0, R.s, R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
                                                       R.P->partials, R.P->sc);
@@ -2249,6 +2325,8 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   EFSI_ARG_CHECK(rhs0 != nullptr && pressure != nullptr && prm != nullptr && st != nullptr, "null argument");
   cudaStream_t s = as_stream(stream);
   PcgRun R;
+  R.mixed = false;
+  R.dots_fused = false;
   R.P = P;
   R.prm = prm;
   R.s = s;
@@ -2302,7 +2380,11 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     st->converged = 1;
     return EFSI_OK;
   }
-  R.use_mg = P->n_levels > 1 && !prm->iface_active && (prm->precond == 1 || prm->precond == 2);
+  R.use_mg = P->n_levels > 1 && !prm->iface_active && (prm->precond == 1 || prm->precond == 2 || prm->precond == 3);
+  // 3: the FP32 level-0 V-cycle.  It needs the plane-marching kernels on
+  // level 0 with TMA maps of all three fields (mask rows of 16-byte multiples:
+  // nz % 16 == 0) and no interface diagonal; otherwise the f64 V-cycle runs.
+  R.mixed = R.use_mg && prm->precond == 3 && P->lv[0].march && P->lv[0].nz % 16 == 0 && !P->has_iface;
   R.pre = prm->precond == 2 ? 1 : 2;
   R.coarse = prm->precond == 2 ? 12 : 24;
   R.post = prm->precond == 2 ? 1 : 2;
@@ -2434,7 +2516,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   };
   auto run_block = [&](bool cont) -> int {
     if (!prm->use_graphs || P->graphs_disabled) return launch_block(cont);
-    const PcgGraphKey key{cont, R.use_mg, remove_mean, outlet, R.pre, R.coarse, R.post, pressure};
+    const PcgGraphKey key{cont, R.use_mg, remove_mean, outlet, R.pre, R.coarse, R.post, pressure, R.mixed};
     cudaGraphExec_t exec = nullptr;
     for (auto& g : P->graphs)
       if (g.key == key) exec = g.exec;

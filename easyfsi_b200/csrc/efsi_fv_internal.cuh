@@ -157,6 +157,8 @@ struct LevelBuf {
   // V-cycle work: three iterate buffers and the rhs (coarse) of the level.
   void* pa = nullptr;
   void* pb = nullptr;
+  float* pa32 = nullptr;    // level 0: FP32 iterates of the mixed-precision V-cycle
+  float* pb32 = nullptr;
   float* rhs = nullptr;     // coarse rhs (levels >= 1)
   const float *wx, *wy, *wz;
   const float *cdx, *cdy, *cdz;
@@ -175,9 +177,10 @@ struct PcgGraphKey {
   bool cont, use_mg, remove_mean;
   int outlet, pre, coarse, post;
   const double* pressure;
+  bool mixed;  // FP32 level-0 V-cycle
   bool operator==(const PcgGraphKey& o) const {
     return cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
-           pre == o.pre && coarse == o.coarse && post == o.post && pressure == o.pressure;
+           pre == o.pre && coarse == o.coarse && post == o.post && pressure == o.pressure && mixed == o.mixed;
   }
 };
 

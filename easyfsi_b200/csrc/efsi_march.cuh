@@ -507,24 +507,12 @@ struct SweepOp {
   __device__ __forceinline__ void finish(const MarchGeom&) {}
 };
 
-// Three blocks per SM (the shared-memory ring allows three).
-// kDots: also finish the flexible PCG's preconditioned dots of this
-// iteration (what the dots kernel computes, fluid.py:4604-4611 / 4590-4601):
-// rz_new = <r, z'>_V, beta_num = <delta, z'>_V and beta, from the five sums.
-template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots>
-__global__ void __launch_bounds__(kMK* kTY, 3)
-    km_sweep(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
-             const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
-             TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc,
-             const double* __restrict__ delta) {
-  pdl_wait();
-  using TR = typename std::conditional<kNegR, double, TP>::type;
-  MarchGeom g;
-  const bool any = march_geom(L, chunk, g);
-  SweepOp<TP, kNegR, kProlong, kAux, kDots> op{L, out, outlet, omega, pr, partials != nullptr, 0.0,
-                                               delta, 0.0, 0.0, 0.0, 0.0};
-  const CUtensorMap* const mv[1] = {&map_p};
-  if (any && !march<TP, 1, TR, true>(L, g, mv, &map_r, &map_m, op)) report_fault(sc);
+// Epilogue of a sweep that reduces: with kDots the z-mean and the flexible
+// PCG's preconditioned dots of this iteration (what the dots kernel computes,
+// fluid.py:4604-4611 / 4590-4601): rz_new = <r, z'>_V, beta_num = <delta,
+// z'>_V and beta, from the five sums; otherwise (partials given) the z-mean.
+template <bool kDots, class Op>
+__device__ __forceinline__ void sweep_epilogue(const Op& op, double* partials, CgScalars* sc) {
   if (kDots) {
     double v[5] = {op.zsum, op.srz, op.sr, op.sdz, op.sd}, t[5];
     if (grid_sum<5>(v, partials, &sc->ticket, t)) {
@@ -557,6 +545,120 @@ __global__ void __launch_bounds__(kMK* kTY, 3)
       }
     }
   }
+}
+
+// Three blocks per SM (the shared-memory ring allows three).
+template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots>
+__global__ void __launch_bounds__(kMK* kTY, 3)
+    km_sweep(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
+             const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
+             TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc,
+             const double* __restrict__ delta) {
+  pdl_wait();
+  using TR = typename std::conditional<kNegR, double, TP>::type;
+  MarchGeom g;
+  const bool any = march_geom(L, chunk, g);
+  SweepOp<TP, kNegR, kProlong, kAux, kDots> op{L, out, outlet, omega, pr, partials != nullptr, 0.0,
+                                               delta, 0.0, 0.0, 0.0, 0.0};
+  const CUtensorMap* const mv[1] = {&map_p};
+  if (any && !march<TP, 1, TR, true>(L, g, mv, &map_r, &map_m, op)) report_fault(sc);
+  sweep_epilogue<kDots>(op, partials, sc);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision level-0 sweep of the fv_multigrid_mixed preconditioner: the
+// iterate tiles are FP32 and the row arithmetic is FP32 (face coefficients
+// rounded from the f64 tables); the right-hand side is the FP64 CG residual.
+// The outer flexible CG, its inner products and scalars, and the z-mean /
+// dot sums stay FP64.  No counterpart in the reference (its V-cycle is f64 on
+// level 0); the outer CG still stops on its f64 true residual.  With out64
+// the result is written as the f64 preconditioned residual z.
+// ---------------------------------------------------------------------------
+template <bool kAux>
+__device__ __forceinline__ void stencil_sel32(const LevelDev& L, const RowCoef& cc, float kxm, float kxp, int i,
+                                              int j, int k, int64_t c, unsigned m, int outlet, float vxm, float vxp,
+                                              float vym, float vyp, float vzm, float vzp, float& ns, float& den) {
+  float kym = (float)cc.kym, kyp = (float)cc.kyp, kzm = (float)cc.kzm, kzp = (float)cc.kzp;
+  if (kAux && L.fw != nullptr) {
+    const int64_t sx = (int64_t)L.ny * L.nz, sy = L.nz;
+    const float fc = __ldg(L.fw + c);
+    kxm *= fc;
+    kxp *= __ldg(L.fw + (i < L.nx - 1 ? c + sx : c));
+    kym *= fc;
+    kyp *= __ldg(L.fw + (j < L.ny - 1 ? c + sy : c));
+    kzm *= fc;
+    kzp *= __ldg(L.fw + (k < L.nz - 1 ? c + 1 : c));
+  }
+  const float axm = (m & M_XM) ? kxm : 0.0f;
+  const float axp = (m & M_XP) ? kxp : 0.0f;
+  const float aym = (m & M_YM) ? kym : 0.0f;
+  const float ayp = (m & M_YP) ? kyp : 0.0f;
+  const float azm = (m & M_ZM) ? kzm : 0.0f;
+  const float azp = (m & M_ZP) ? kzp : 0.0f;
+  ns = axm * vxm;
+  ns = fmaf(axp, vxp, ns);
+  ns = fmaf(aym, vym, ns);
+  ns = fmaf(ayp, vyp, ns);
+  ns = fmaf(azm, vzm, ns);
+  ns = fmaf(azp, vzp, ns);
+  den = ((((axm + axp) + aym) + ayp) + azm) + azp;
+  if (outlet && k == 0) den += (float)L.oz;
+}
+
+template <bool kProlong, bool kAux, bool kDots>
+struct Sweep32Op : SweepOp<float, true, kProlong, kAux, kDots> {
+  double* __restrict__ out64;  // when set, z is written here in f64 instead of the f32 output
+
+  template <class V>
+  __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int, int slot, bool active, unsigned m,
+                                       double e, double kxm, double kxp, const RowCoef& rc, const V& val) {
+    if (!active) return;
+    const LevelDev& L = this->L;
+    float res = 0.0f;
+    if (!(m & M_SOLID)) {
+      const float x0 = (float)val(0, 0, 0, 0);
+      float ns, den;
+      stencil_sel32<kAux>(L, rc, (float)kxm, (float)kxp, i, j, k, c, m, this->outlet, (float)val(0, -1, 0, 0),
+                          (float)val(0, 1, 0, 0), (float)val(0, 0, -1, 0), (float)val(0, 0, 1, 0),
+                          (float)val(0, 0, 0, -1), (float)val(0, 0, 0, 1), ns, den);
+      if (kAux) den += (float)iface_at<double>(L, c);
+      if (den > 0.0f) {
+        const float jv = (ns + (float)e) / den;  // the level-0 rhs is -r
+        res = x0 + (float)this->omega * (jv - x0);
+      }
+      if ((this->want_sum || kDots) && (m & M_FLUID)) {
+        const double vol = vol64(L, i, j, k), rd = (double)res;
+        this->zsum += rd * vol;
+        if (kDots) {
+          const double dlc = this->dl[slot];
+          this->srz += e * rd * vol;
+          this->sr += e * vol;
+          this->sdz += rd * dlc * vol;
+          this->sd += dlc * vol;
+        }
+      }
+    }
+    if (out64 != nullptr)
+      out64[c] = (double)res;
+    else
+      this->out[c] = res;
+  }
+};
+
+template <bool kProlong, bool kAux, bool kDots>
+__global__ void __launch_bounds__(kMK* kTY, 3)
+    km_sweep32(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
+               const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
+               float* __restrict__ out, double* __restrict__ out64, int outlet, double omega, ProlongSrc pr,
+               double* partials, CgScalars* sc, const double* __restrict__ delta) {
+  pdl_wait();
+  MarchGeom g;
+  const bool any = march_geom(L, chunk, g);
+  Sweep32Op<kProlong, kAux, kDots> op{{L, out, outlet, omega, pr, partials != nullptr, 0.0, delta, 0.0, 0.0, 0.0, 0.0},
+                                      out64};
+  const CUtensorMap* const mv[1] = {&map_p};
+  if (any && !march<float, 1, double, true>(L, g, mv, &map_r, &map_m, op)) report_fault(sc);
+  sweep_epilogue<kDots>(op, partials, sc);
 }
 
 // First sweep from a zero iterate: out = omega * (0 - rhs) / den per row; no

@@ -52,8 +52,11 @@ __all__ = [
     "build_graded_grid",
 ]
 
-CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light")
-_PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2}
+# "fv_multigrid_mixed" (no reference counterpart): the fv_multigrid V-cycle
+# with FP32 storage and arithmetic on level 0, inside the same FP64 flexible CG
+# (true residual, inner products and scalars in FP64).
+CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light", "fv_multigrid_mixed")
+_PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2, "fv_multigrid_mixed": 3}
 _BREAKDOWN_TEXT = {
     0: "",
     1: "initial residual/preconditioner dot is not positive finite",

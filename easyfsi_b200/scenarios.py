@@ -384,13 +384,15 @@ class CoupledScene:
         self.mu_pa, self.lambda_pa = material(cfg)
         self.radius = support_radius(cfg)
         self.last_cg_iterations = 0
+        # "fv_multigrid" (the reference's) or "fv_multigrid_mixed" (FP32 level-0 V-cycle)
+        self.preconditioner = "fv_multigrid"
 
     def step(self) -> None:
         cfg, fluid, solid, mk = self.cfg, self.fluid, self.solid, self.markers
         fluid.predict(cfg.dt_s)
         fluid.project(
             iterations=cfg.cg_max_iterations, dt_s=cfg.dt_s, pressure_solver="fv_cg", cg_tolerance=cfg.cg_tolerance,
-            cg_preconditioner="fv_multigrid", read_report=False,
+            cg_preconditioner=self.preconditioner, read_report=False,
         )
         self.last_cg_iterations = fluid.last_cg_iterations
         mk.sample_fluid_stress_to_marker_tractions(

@@ -150,7 +150,9 @@ int efsi_mg_vcycle(efsi_fv_plan* plan, const double* r, double* z, int32_t outle
 
 typedef struct efsi_pcg_params {
   int32_t max_iters;
-  int32_t precond;      /* 0 jacobi, 1 fv_multigrid (2/24/2), 2 fv_multigrid_light (1/12/1) */
+  int32_t precond;      /* 0 jacobi, 1 fv_multigrid (2/24/2), 2 fv_multigrid_light (1/12/1),
+                           3 fv_multigrid_mixed: the 2/24/2 V-cycle with FP32 level-0 iterates and
+                           arithmetic (no reference counterpart; the CG stays FP64) */
   int32_t remove_mean;  /* closed-domain zero-mean projection */
   int32_t outlet;       /* pressure_outlet_zmin */
   int32_t iface_active; /* interface terms present: MG disabled, restart every 256 */

@@ -71,3 +71,27 @@ def test_c2_mpm_substep_conserves_momentum(scene):
     assert rep.active_grid_nodes > 0
     assert rep.transfer_relative_error < 2.0e-5
     assert rep.max_abs_j == pytest.approx(1.0, abs=1e-3)
+
+
+def test_c2_mixed_precision_vcycle_solves_to_the_same_tolerance(scene):
+    """fv_multigrid_mixed at full size: the FP64 outer CG reaches the same
+    true-residual tolerance, in about as many iterations, and the pressure
+    stays close to the FP64 V-cycle's solution of the same system."""
+    cfg, fl = scene.cfg, scene.fluid
+    fl.predict(cfg.dt_s)
+    fl.compute_divergence()
+    out = {}
+    for name in ("fv_multigrid", "fv_multigrid_mixed"):
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(iterations=cfg.cg_max_iterations, rhs_scale=cfg.density_kgm3 / cfg.dt_s,
+                                         pressure_outlet_zmin=False, tolerance=cfg.cg_tolerance, preconditioner=name)
+        assert fl.last_cg_converged and fl.last_cg_used_multigrid
+        assert fl.last_cg_relative_residual <= cfg.cg_tolerance * (1.0 + 1e-6)
+        out[name] = (fl.last_cg_iterations, fl.pressure.to_numpy().astype(np.float64))
+    (it32, a), (it64, b) = out["fv_multigrid_mixed"], out["fv_multigrid"]
+    assert it32 <= it64 + 5
+    # the FP32 V-cycle ran: the FP64 one is deterministic and would repeat b bit for bit
+    assert not np.array_equal(a, b)
+    # both stop at relative residual 1e-8: the solutions agree to the
+    # condition number times that
+    assert np.linalg.norm((a - b).ravel()) <= 1e-3 * np.linalg.norm(b.ravel())

@@ -283,3 +283,53 @@ def test_march_kernels_match_per_cell_kernels(n, aux):
             iterations=4, rhs_scale=1.0e6, pressure_outlet_zmin=True, multigrid_cycles=2
         )
     assert rel_l2(fm.pressure.to_numpy(), fc.pressure.to_numpy()) <= 1e-12
+
+
+# (level 0 streams its mask rows by TMA only when nz % 16 == 0; below that
+# the preconditioner runs the f64 V-cycle)
+@pytest.mark.parametrize("n", [(40, 24, 48), (14, 12, 32)])
+def test_mixed_precision_vcycle_pcg_reaches_the_same_solution(n):
+    """fv_multigrid_mixed (FP32 level-0 V-cycle inside the FP64 flexible CG)
+    converges to the same true residual as the FP64 V-cycle, measured by the
+    oracle's operator, and its pressure matches the FP64 V-cycle's to 1e-5."""
+    grid = _graded_grid(n)
+    obs = _obstacle(grid, seed=9)
+    fl = _solver(grid)
+    fl.obstacle.from_numpy(obs)
+    ofl = orc.OracleFluid(grid, rho=1000.0, mu=1.0e-3, variant="mirror")
+    ofl.obstacle[...] = obs
+    div = np.random.default_rng(31).normal(size=grid.grid_nodes).astype(np.float32)
+    out = {}
+    for name in ("fv_multigrid", "fv_multigrid_mixed"):
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(
+            iterations=300, rhs_scale=1.0e6, pressure_outlet_zmin=False, tolerance=1e-10, preconditioner=name
+        )
+        assert fl.last_cg_converged and fl.last_cg_used_multigrid
+        out[name] = (fl.last_cg_iterations, fl.pressure.to_numpy())
+    it64, p64 = out["fv_multigrid"]
+    it32, p32 = out["fv_multigrid_mixed"]
+    assert it32 <= it64 + 3
+    # the FP32 V-cycle ran: the FP64 one is deterministic and would repeat p64 bit for bit
+    assert not np.array_equal(p32, p64)
+    # both stop at relative residual 1e-10; their difference is bounded by the
+    # operator's condition number times that
+    assert rel_l2(p32, p64) <= 1e-5
+    # true residuals of both solutions with the oracle's operator (the
+    # reference's f32-loaded metrics, f64 arithmetic)
+    ofl.divergence[...] = div
+    ofl.prepare_rhs(1.0e6)
+    fluid = ofl.obstacle == 0
+    vol = np.einsum("i,j,k->ijk", *[np.asarray(m["w"], np.float32).astype(np.float64) for m in ofl.metrics[0]])
+    b = np.where(fluid, -ofl.rhs0, 0.0)
+    b -= (b * vol)[fluid].sum() / vol[fluid].sum()
+    b[~fluid] = 0.0
+    # (the CG stops on its recurrence residual; the oracle's own PCG solution
+    # of this system has a true residual of 8.8e-11 at tolerance 1e-10)
+    for p in (p64, p32):
+        res = b - ofl.fv_apply(p, 0)
+        res[~fluid] = 0.0
+        res -= (res * vol)[fluid].sum() / vol[fluid].sum()
+        res[~fluid] = 0.0
+        assert np.sqrt((res * res * vol).sum() / (b * b * vol).sum()) <= 2.0e-10
