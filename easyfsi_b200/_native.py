@@ -65,6 +65,26 @@ class GridAxes(Structure):
     _fields_ = [("fx", c_void_p), ("fy", c_void_p), ("fz", c_void_p), ("cx", c_void_p), ("cy", c_void_p), ("cz", c_void_p)]
 
 
+class IbSearchParams(Structure):  # efsi_ib_search_params
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
+        ("marker_count", c_int32), ("triangle_count", c_int32), ("classify_far_internal_nodes", c_int32),
+        ("search_radius_m", c_float), ("interior_probe_distance_m", c_float), ("sign_tolerance_m", c_float),
+        ("cell_center_x_m", c_void_p), ("cell_center_y_m", c_void_p), ("cell_center_z_m", c_void_p),
+        ("bounds_min_m", c_float * 3), ("spacing_m", c_float * 3),
+        ("box_min_m", c_float * 3), ("box_max_m", c_float * 3),
+        ("marker_x", c_void_p), ("marker_n", c_void_p), ("triangles", c_void_p),
+    ]
+
+
+class IbSearchFields(Structure):  # efsi_ib_search_fields
+    _fields_ = [
+        ("node_kind", c_void_p), ("nearest_marker", c_void_p), ("signed_distance_m", c_void_p),
+        ("boundary_point_m", c_void_p), ("interior_fluid_point_m", c_void_p),
+        ("projection_marker_indices", c_void_p), ("projection_marker_weights", c_void_p), ("report", c_void_p),
+    ]
+
+
 class MpmState(Structure):
     _fields_ = [
         ("particle_count", c_int32),
@@ -141,6 +161,10 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_bin_particles": [P, P, I, P],
     "efsi_scatter_marker_forces": [P, I, P, P, P, P, P, P],
     "efsi_surface_feedback": [P, I, P, P, P, P, P, P, P, P, F, P, P],
+    "efsi_ib_search_plan_create": [POINTER(c_void_p)],
+    "efsi_ib_search_plan_destroy": [P],
+    "efsi_ib_node_search": [P, POINTER(IbSearchParams), POINTER(IbSearchFields), P],
+    "efsi_ib_reset_anchor_cells": [P, ctypes.c_int64, P],
 }
 
 _lib = None

@@ -33,6 +33,11 @@ NVCC_FLAGS = [
 ]
 
 
+# Per-source extra flags.  The node search keeps the reference's f32
+# expressions unfused, so its geometry rounds as the expressions read.
+EXTRA_FLAGS = {"efsi_ibsearch.cu": ["-fmad=false"]}
+
+
 def _nvcc() -> str:
     candidates = [os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"]
     for cand in candidates:
@@ -70,7 +75,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     objects = []
     for src in sources():
         obj = BUILD_DIR / (src.stem + ".o")
-        cmd = [nvcc, *_host_compiler(), *NVCC_FLAGS, f"-I{INCLUDE_DIR}", "-c", str(src), "-o", str(obj)]
+        cmd = [nvcc, *_host_compiler(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src.name, []), f"-I{INCLUDE_DIR}", "-c",
+               str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

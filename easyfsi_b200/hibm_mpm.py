@@ -10,8 +10,10 @@ signatures: ``load_markers`` (:553), ``set_marker_tractions_pa`` (:893),
 updates (:5055, :5182).  Every method accepts an extra ``read_report=False``
 keyword that skips the host read of its report (the report is then ``None``).
 
-The viscous / closure stress sampler, projection triangles and the IB node
-search of the reference are outside the hot path and not provided.
+Projection triangles (``set_projection_triangles`` :590) and the IB node
+search (class ``HibmMpmIbNodeSearch`` :5385) are provided too.  The viscous /
+closure stress sampler of the reference is outside the hot path and not
+provided.
 """
 
 from __future__ import annotations
@@ -130,6 +132,7 @@ class HibmMpmSurfaceMarkers:
         self.t_gamma_pa = Field((cap,), f64, n=3, device=dev)
         self._stress_pressure_valid = Field((cap,), i32, device=dev)
         self.F_gamma_n = Field((cap,), f64, n=3, device=dev)
+        self.projection_triangle_indices = Field((self.projection_triangle_capacity,), i32, n=3, device=dev)
         self._report = torch.zeros(16, dtype=torch.float64, device=dev)
         self._bins: dict = {}
 
@@ -170,6 +173,25 @@ class HibmMpmSurfaceMarkers:
         self.region_id.from_numpy(reg)
         self.t_gamma_pa.tensor.zero_()
         self.F_gamma_n.tensor.zero_()
+
+    def set_projection_triangles(self, triangle_indices) -> int:
+        """hibm_mpm.py:590-615: marker-index triangles used by the IB node
+        search's closest-point projection."""
+        count = len(triangle_indices)
+        if count > self.projection_triangle_capacity:
+            raise ValueError("projection triangle count exceeds projection_triangle_capacity")
+        marker_count = int(self.marker_count)
+        tri = np.zeros((self.projection_triangle_capacity, 3), dtype=np.int32)
+        for t, triangle in enumerate(triangle_indices):
+            if len(triangle) != 3:
+                raise ValueError("projection triangles must contain three indices")
+            ia, ib, ic = (int(triangle[0]), int(triangle[1]), int(triangle[2]))
+            if min(ia, ib, ic) < 0 or max(ia, ib, ic) >= marker_count:
+                raise ValueError("projection triangle index out of marker range")
+            tri[t] = (ia, ib, ic)
+        self.projection_triangle_indices.from_numpy(tri)
+        self.projection_triangle_count = int(count)
+        return self.projection_triangle_count
 
     def set_marker_tractions_pa(self, tractions_pa) -> None:
         if len(tractions_pa) != self.marker_count:
@@ -510,3 +532,188 @@ class HibmMpmSurfaceMarkers:
 
     def marker_region_id(self, marker_index: int) -> int:
         return int(self.region_id[int(marker_index)])
+
+
+@dataclass(frozen=True)
+class HibmMpmIbNodeSearchReport:
+    near_boundary_node_count: int
+    external_ib_node_count: int
+    internal_node_count: int
+    invalid_projection_count: int
+
+
+class HibmMpmIbNodeSearch:
+    """Immersed-boundary node search and in/out classification (drop-in for
+    simulation_core/hibm_mpm.py:5385 HibmMpmIbNodeSearch).
+
+    Every node finds the nearest projection triangle (or marker) within the
+    search radius, records its boundary point, projection weights and the
+    interior fluid probe point, and is classified external IB (some candidate
+    sees it outside), internal, or none; with ``classify_far_internal_nodes``
+    a node outside the radius of every candidate is internal when no
+    candidate at all sees it outside.  The search runs in
+    ``efsi_ib_node_search`` (binned triangles on the device); the fields and
+    report counts are the reference's.
+    """
+
+    _NODE_NONE = 0
+    _NODE_EXTERNAL_IB = 1
+    _NODE_INTERNAL = 2
+    _F32_EPSILON = 1.1920928955078125e-7
+
+    def __init__(self, *, grid_nodes, bounds_min_m, bounds_max_m, marker_capacity: int,
+                 runtime: TaichiRuntimeConfig | None = None) -> None:
+        self.device = init_runtime(runtime)
+        nodes = tuple(int(v) for v in grid_nodes)
+        if len(nodes) != 3 or any(v <= 0 for v in nodes):
+            raise ValueError("grid_nodes must contain three positive integers")
+        bounds_min = _vector3(bounds_min_m, name="bounds_min_m")
+        bounds_max = _vector3(bounds_max_m, name="bounds_max_m")
+        if any(hi <= lo for lo, hi in zip(bounds_min, bounds_max)):
+            raise ValueError("bounds_max_m must be greater than bounds_min_m")
+        if int(marker_capacity) <= 0:
+            raise ValueError("marker_capacity must be positive")
+        self.grid_nodes = nodes
+        self.bounds_min_m = bounds_min
+        self.bounds_max_m = bounds_max
+        self.spacing_m = tuple((hi - lo) / float(n) for lo, hi, n in zip(bounds_min, bounds_max, nodes))
+        self.marker_capacity = int(marker_capacity)
+        dev = self.device
+        self.node_kind_code = Field(nodes, i32, device=dev)
+        self.nearest_marker = Field(nodes, i32, device=dev)
+        self.node_signed_distance_m = Field(nodes, f32, device=dev)
+        self.node_boundary_point_m = Field(nodes, f32, n=3, device=dev)
+        self.node_interior_fluid_point_m = Field(nodes, f32, n=3, device=dev)
+        self.node_projection_marker_indices = Field(nodes, i32, n=3, device=dev)
+        self.node_projection_marker_weights = Field(nodes, f32, n=3, device=dev)
+        self.node_anchor_cell = Field(nodes, i32, n=3, device=dev)
+        self._report = torch.zeros(4, dtype=torch.int32, device=dev)
+        handle = c_void_p()
+        _native.call("efsi_ib_search_plan_create", byref(handle))
+        self._plan = handle
+        self.reset_node_anchor_cells()
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None:
+            try:
+                _native.load().efsi_ib_search_plan_destroy(plan)
+            except Exception:
+                pass
+
+    def reset_node_anchor_cells(self) -> None:
+        """hibm_mpm.py:5463-5475: every node's anchor cell to (-1, -1, -1)."""
+        n = int(np.prod(self.grid_nodes))
+        _native.call("efsi_ib_reset_anchor_cells", self.node_anchor_cell.ptr(), n, current_stream_handle())
+
+    def _default_sign_tolerance_m(self) -> float:
+        """hibm_mpm.py:5477-5492."""
+        min_spacing = max(min(self.spacing_m), 1.0e-12)
+        max_extent = max(hi - lo for lo, hi in zip(self.bounds_min_m, self.bounds_max_m))
+        max_coordinate = max(max(abs(v) for v in self.bounds_min_m), max(abs(v) for v in self.bounds_max_m))
+        coordinate_scale = max(max_extent, max_coordinate, min_spacing, 1.0)
+        return max(1.0e-12, 1.0e-6 * min_spacing, 2.0 * self._F32_EPSILON * coordinate_scale)
+
+    def _validate_search_inputs(self, markers, *, search_radius_m, interior_probe_distance_m, sign_tolerance_m):
+        """hibm_mpm.py:6069-6094."""
+        if int(markers.marker_count) > self.marker_capacity:
+            raise ValueError("markers.marker_count exceeds marker_capacity")
+        radius = float(search_radius_m)
+        if not math.isfinite(radius) or radius <= 0.0:
+            raise ValueError("search_radius_m must be a finite positive number")
+        probe = float(interior_probe_distance_m)
+        if not math.isfinite(probe) or probe <= 0.0:
+            raise ValueError("interior_probe_distance_m must be a finite positive number")
+        tol = self._default_sign_tolerance_m() if sign_tolerance_m is None else float(sign_tolerance_m)
+        if not math.isfinite(tol) or tol < 0.0:
+            raise ValueError("sign_tolerance_m must be a finite non-negative number")
+        return radius, probe, tol
+
+    def _run(self, markers, centres, radius, probe, tol, classify_far) -> HibmMpmIbNodeSearchReport:
+        prm = _native.IbSearchParams()
+        prm.nx, prm.ny, prm.nz = self.grid_nodes
+        prm.marker_count = int(markers.marker_count)
+        prm.triangle_count = int(getattr(markers, "projection_triangle_count", 0))
+        prm.classify_far_internal_nodes = 1 if classify_far else 0
+        prm.search_radius_m = radius
+        prm.interior_probe_distance_m = probe
+        prm.sign_tolerance_m = tol
+        keep = []
+        if centres is not None:
+            axes = []
+            for c, count in zip(centres, self.grid_nodes):
+                t = (c.tensor if isinstance(c, Field) else torch.as_tensor(c))
+                t = t.to(device=self.device, dtype=torch.float32).contiguous()
+                if t.numel() < count:
+                    raise ValueError("cell centre fields must cover grid_nodes")
+                keep.append(t)
+                axes.append(t.data_ptr())
+            prm.cell_center_x_m, prm.cell_center_y_m, prm.cell_center_z_m = axes
+        for a in range(3):
+            prm.bounds_min_m[a] = self.bounds_min_m[a]
+            prm.spacing_m[a] = self.spacing_m[a]
+            prm.box_min_m[a] = self.bounds_min_m[a]
+            prm.box_max_m[a] = self.bounds_max_m[a]
+        prm.marker_x = markers.x_gamma_m.ptr()
+        prm.marker_n = markers.n_gamma.ptr()
+        prm.triangles = markers.projection_triangle_indices.ptr() if prm.triangle_count > 0 else None
+        out = _native.IbSearchFields()
+        out.node_kind = self.node_kind_code.ptr()
+        out.nearest_marker = self.nearest_marker.ptr()
+        out.signed_distance_m = self.node_signed_distance_m.ptr()
+        out.boundary_point_m = self.node_boundary_point_m.ptr()
+        out.interior_fluid_point_m = self.node_interior_fluid_point_m.ptr()
+        out.projection_marker_indices = self.node_projection_marker_indices.ptr()
+        out.projection_marker_weights = self.node_projection_marker_weights.ptr()
+        out.report = self._report.data_ptr()
+        _native.call("efsi_ib_node_search", self._plan, byref(prm), byref(out), current_stream_handle())
+        counts = [int(v) for v in self._report.cpu()]
+        del keep
+        return HibmMpmIbNodeSearchReport(*counts)
+
+    def search_and_classify(self, markers, *, search_radius_m: float, interior_probe_distance_m: float,
+                            sign_tolerance_m: float | None = None,
+                            classify_far_internal_nodes: bool = False) -> HibmMpmIbNodeSearchReport:
+        """hibm_mpm.py:6096-6133: nodes at the uniform cell centres of the
+        search box."""
+        radius, probe, tol = self._validate_search_inputs(
+            markers, search_radius_m=search_radius_m, interior_probe_distance_m=interior_probe_distance_m,
+            sign_tolerance_m=sign_tolerance_m)
+        return self._run(markers, None, radius, probe, tol, classify_far_internal_nodes)
+
+    def search_and_classify_grid_fields(self, markers, *, cell_center_x_m, cell_center_y_m, cell_center_z_m,
+                                        search_radius_m: float, interior_probe_distance_m: float,
+                                        sign_tolerance_m: float | None = None,
+                                        classify_far_internal_nodes: bool = False) -> HibmMpmIbNodeSearchReport:
+        """hibm_mpm.py:6135-6170: nodes at the fluid's (graded) cell centres."""
+        radius, probe, tol = self._validate_search_inputs(
+            markers, search_radius_m=search_radius_m, interior_probe_distance_m=interior_probe_distance_m,
+            sign_tolerance_m=sign_tolerance_m)
+        return self._run(markers, (cell_center_x_m, cell_center_y_m, cell_center_z_m), radius, probe, tol,
+                         classify_far_internal_nodes)
+
+    def node_kind(self, node_index) -> str:
+        code = int(self.node_kind_code[self._node_index(node_index)])
+        if code == self._NODE_EXTERNAL_IB:
+            return "external_ib"
+        if code == self._NODE_INTERNAL:
+            return "internal"
+        return "none"
+
+    def nearest_marker_index(self, node_index) -> int:
+        return int(self.nearest_marker[self._node_index(node_index)])
+
+    def signed_distance_m(self, node_index) -> float:
+        return float(self.node_signed_distance_m[self._node_index(node_index)])
+
+    def boundary_point_m(self, node_index) -> tuple[float, float, float]:
+        return tuple(float(v) for v in self.node_boundary_point_m[self._node_index(node_index)])
+
+    def interior_fluid_point_m(self, node_index) -> tuple[float, float, float]:
+        return tuple(float(v) for v in self.node_interior_fluid_point_m[self._node_index(node_index)])
+
+    def _node_index(self, node_index) -> tuple[int, int, int]:
+        index = tuple(int(v) for v in node_index)
+        if len(index) != 3 or any(v < 0 or v >= n for v, n in zip(index, self.grid_nodes)):
+            raise IndexError("node_index out of range")
+        return index

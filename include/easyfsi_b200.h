@@ -34,6 +34,7 @@ extern "C" {
 typedef struct efsi_fv_plan efsi_fv_plan;
 typedef struct efsi_mpm_plan efsi_mpm_plan;
 typedef struct efsi_bin_plan efsi_bin_plan;
+typedef struct efsi_ib_search_plan efsi_ib_search_plan;
 
 /* Last error message of the calling thread (never NULL). */
 const char* efsi_last_error(void);
@@ -333,6 +334,60 @@ int efsi_surface_feedback(efsi_bin_plan* plan, int32_t marker_count, float* x_ga
                           float* n_gamma, float* area_gamma, const float* particle_x, const float* particle_v,
                           const float* particle_normal, const float* particle_area, float dt,
                           double* report_device, void* stream);
+
+/* Immersed-boundary node search (hibm_mpm.py:5385-6220 HibmMpmIbNodeSearch). */
+typedef struct efsi_ib_search_params {
+  int32_t nx, ny, nz;            /* nodes */
+  int32_t marker_count;
+  int32_t triangle_count;        /* projection triangles; 0: search the markers */
+  int32_t classify_far_internal_nodes;
+  float search_radius_m, interior_probe_distance_m, sign_tolerance_m;
+  /* node positions: the three centre arrays (nx, ny, nz floats) when given
+     (search_and_classify_grid_fields), else bounds_min + (i + 0.5) * spacing
+     per axis in f32 (search_and_classify) */
+  const float* cell_center_x_m;
+  const float* cell_center_y_m;
+  const float* cell_center_z_m;
+  float bounds_min_m[3];
+  float spacing_m[3];
+  float box_min_m[3], box_max_m[3]; /* box of the node positions, for the triangle bins */
+  const float* marker_x;         /* marker positions, 3 floats each */
+  const float* marker_n;         /* marker normals */
+  const int32_t* triangles;      /* 3 marker indices each */
+} efsi_ib_search_params;
+
+/* Per-node output fields (hibm_mpm.py:5418-5436), C order over (nx, ny, nz):
+   node kind (0 none, 1 external IB, 2 internal), nearest marker, signed
+   distance, boundary point (3), interior fluid point (3), projection marker
+   indices (3) and weights (3); report: int32[4] = near-boundary, external IB,
+   internal and invalid-projection node counts (written on the device). */
+typedef struct efsi_ib_search_fields {
+  int32_t* node_kind;
+  int32_t* nearest_marker;
+  float* signed_distance_m;
+  float* boundary_point_m;
+  float* interior_fluid_point_m;
+  int32_t* projection_marker_indices;
+  float* projection_marker_weights;
+  int32_t* report;
+} efsi_ib_search_fields;
+
+/* Work buffers of the node search (triangle bins), grown on demand. */
+int efsi_ib_search_plan_create(efsi_ib_search_plan** out);
+int efsi_ib_search_plan_destroy(efsi_ib_search_plan* plan);
+
+/* hibm_mpm.py:5601-5835 _search_and_classify_kernel and 5837-6068
+ * _search_and_classify_grid_fields_kernel (argument checks of
+ * hibm_mpm.py:6069-6094).  Same fields and counts as the reference's
+ * all-pairs loop; the triangles are binned by their box widened by the
+ * search radius, so a near node visits only its bin.  Synchronises the
+ * stream once (the bin entry total). */
+int efsi_ib_node_search(efsi_ib_search_plan* plan, const efsi_ib_search_params* params,
+                        const efsi_ib_search_fields* fields, void* stream);
+
+/* hibm_mpm.py:5463-5475 _reset_node_anchor_cells_kernel: every node's
+ * anchor cell (3 int32 each) to (-1, -1, -1). */
+int efsi_ib_reset_anchor_cells(int32_t* anchor_cells, int64_t node_count, void* stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

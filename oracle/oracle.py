@@ -377,6 +377,51 @@ class OracleMarkers:
         return rep
 
 
+def ib_node_search(*, grid_nodes, markers_x, markers_n, triangles=None, search_radius: float,
+                   interior_probe_distance: float, sign_tolerance: float, classify_far: bool = False,
+                   centers=None, bounds_min=None, spacing=None, variant: str = "mirror") -> dict:
+    """Immersed-boundary node search and classification of every node
+    (oracle_ibsearch.cpp; hibm_mpm.py:5603-6068).  Node positions are the
+    centre arrays ``centers = (cx, cy, cz)`` when given, else ``bounds_min +
+    (i + 0.5) * spacing``.  Returns the per-node fields and the four report
+    counts."""
+    lib = load(variant)
+    rt = r32_dtype(variant)
+    nx, ny, nz = (int(v) for v in grid_nodes)
+    mx = np.ascontiguousarray(markers_x, dtype=rt).reshape(-1, 3)
+    mn = np.ascontiguousarray(markers_n, dtype=rt).reshape(-1, 3)
+    tri = np.zeros((0, 3), np.int32) if triangles is None else np.ascontiguousarray(triangles, dtype=np.int32).reshape(-1, 3)
+    if centers is not None:
+        cx, cy, cz = (np.ascontiguousarray(c, dtype=rt) for c in centers)
+        bmin = sp = None
+    else:
+        cx = cy = cz = None
+        bmin = np.ascontiguousarray(bounds_min, dtype=rt)
+        sp = np.ascontiguousarray(spacing, dtype=rt)
+    shape = (nx, ny, nz)
+    out = {
+        "kind": np.zeros(shape, np.int32),
+        "nearest_marker": np.zeros(shape, np.int32),
+        "signed_distance": np.zeros(shape, rt),
+        "boundary_point": np.zeros(shape + (3,), rt),
+        "interior_point": np.zeros(shape + (3,), rt),
+        "projection_indices": np.zeros(shape + (3,), np.int32),
+        "projection_weights": np.zeros(shape + (3,), rt),
+    }
+    report = np.zeros(4, np.int64)
+    real = c_float if rt == np.float32 else c_double
+    lib.efo_ib_node_search(
+        c_int(nx), c_int(ny), c_int(nz), _p(cx), _p(cy), _p(cz), _p(bmin), _p(sp), _p(mx), _p(mn), c_int(mx.shape[0]),
+        _p(tri), c_int(tri.shape[0]), real(search_radius), real(interior_probe_distance), real(sign_tolerance),
+        c_int(1 if classify_far else 0), _p(out["kind"]), _p(out["nearest_marker"]), _p(out["signed_distance"]),
+        _p(out["boundary_point"]), _p(out["interior_point"]), _p(out["projection_indices"]),
+        _p(out["projection_weights"]), _p(report),
+    )
+    out["report"] = dict(zip(("near_boundary_node_count", "external_ib_node_count", "internal_node_count",
+                              "invalid_projection_count"), (int(v) for v in report)))
+    return out
+
+
 class OracleScene:
     """The coupled step of easyfsi_b200.scenarios.CoupledScene on host arrays."""
 

@@ -209,3 +209,162 @@ def test_clear_then_scatter_replaces_stale_force():
                                       stale=(99.0, 0.0, 0.0))
     assert solid.external_force_n[0] == (1.0, -2.0, 3.0)
     assert rep.total_mpm_external_force_n == (1.0, -2.0, 3.0)
+
+
+# --------------------------------------------------------------------------
+# IB node search (HibmMpmIbNodeSearch, hibm_mpm.py:5385-6220), the reference's
+# HibmMpmIbNodeSearchTests through the drop-in classes.
+# --------------------------------------------------------------------------
+def _markers(positions, normals, triangles=None):
+    from easyfsi_b200.hibm_mpm import HibmMpmSurfaceMarkers
+
+    n = len(positions)
+    m = HibmMpmSurfaceMarkers(marker_capacity=n, projection_triangle_capacity=len(triangles) if triangles else None)
+    m.load_markers(positions_m=positions, velocities_mps=((0.0, 0.0, 0.0),) * n, normals=normals,
+                   areas_m2=(1.0,) * n, region_ids=(7,) * n)
+    if triangles:
+        m.set_projection_triangles(triangles)
+    return m
+
+
+def _node_search(nodes, capacity, bmin=(0.0, 0.0, 0.0), bmax=(1.0, 1.0, 1.0)):
+    from easyfsi_b200.hibm_mpm import HibmMpmIbNodeSearch
+
+    return HibmMpmIbNodeSearch(grid_nodes=nodes, bounds_min_m=bmin, bounds_max_m=bmax, marker_capacity=capacity)
+
+
+_CLOSED_X = ((0.25, 0.5, 0.5), (0.75, 0.5, 0.5), (0.5, 0.25, 0.5), (0.5, 0.75, 0.5), (0.5, 0.5, 0.25), (0.5, 0.5, 0.75))
+_CLOSED_N = ((-1.0, 0.0, 0.0), (1.0, 0.0, 0.0), (0.0, -1.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, -1.0), (0.0, 0.0, 1.0))
+
+
+# test_hibm.py:904
+def test_ib_search_plane_classifies_external_and_internal_nodes():
+    mk = _markers(((0.5, 0.5, 0.5),), ((0.0, 0.0, 1.0),))
+    search = _node_search((1, 1, 4), 1)
+    rep = search.search_and_classify(mk, search_radius_m=0.26, interior_probe_distance_m=0.125)
+    assert (rep.near_boundary_node_count, rep.external_ib_node_count, rep.internal_node_count,
+            rep.invalid_projection_count) == (2, 1, 1, 0)
+    assert search.node_kind((0, 0, 2)) == "external_ib" and search.node_kind((0, 0, 1)) == "internal"
+    assert search.nearest_marker_index((0, 0, 2)) == 0 and search.nearest_marker_index((0, 0, 1)) == 0
+    assert search.boundary_point_m((0, 0, 2)) == (0.5, 0.5, 0.5)
+    assert search.interior_fluid_point_m((0, 0, 2)) == (0.5, 0.5, 0.75)
+    assert search.signed_distance_m((0, 0, 2)) > 0.0 and search.signed_distance_m((0, 0, 1)) < 0.0
+
+
+# test_hibm.py:939
+def test_ib_search_triangle_projection_between_markers():
+    mk = _markers(((0.25, 0.25, 0.5), (0.75, 0.25, 0.5), (0.25, 0.75, 0.5)), ((0.0, 0.0, 1.0),) * 3, [(0, 1, 2)])
+    search = _node_search((8, 8, 8), 3)
+    rep = search.search_and_classify(mk, search_radius_m=0.08, interior_probe_distance_m=0.05)
+    assert rep.near_boundary_node_count >= 1 and rep.external_ib_node_count >= 1
+    assert search.node_kind((2, 2, 4)) == "external_ib"
+    np.testing.assert_allclose(search.boundary_point_m((2, 2, 4)), (0.3125, 0.3125, 0.5), atol=1e-6)
+    assert search.signed_distance_m((2, 2, 4)) == pytest.approx(0.0625)
+    np.testing.assert_allclose(search.interior_fluid_point_m((2, 2, 4)), (0.3125, 0.3125, 0.6125), atol=1e-6)
+
+
+# test_hibm.py:987
+def test_ib_search_closed_surface_deep_internal_node():
+    search = _node_search((1, 1, 1), 6)
+    rep = search.search_and_classify(_markers(_CLOSED_X, _CLOSED_N), search_radius_m=0.1,
+                                     interior_probe_distance_m=0.125, classify_far_internal_nodes=True)
+    assert (rep.near_boundary_node_count, rep.external_ib_node_count, rep.internal_node_count) == (0, 0, 1)
+    assert search.node_kind((0, 0, 0)) == "internal" and search.nearest_marker_index((0, 0, 0)) >= 0
+
+
+# test_hibm.py:1030
+def test_ib_search_closed_surface_grid_fields_deep_internal_nodes():
+    fluid = _unit_solver(4)
+    search = _node_search(fluid.grid.grid_nodes, 6, fluid.grid.bounds_min_m, fluid.grid.bounds_max_m)
+    rep = search.search_and_classify_grid_fields(
+        _markers(_CLOSED_X, _CLOSED_N), cell_center_x_m=fluid.cell_center_x_m, cell_center_y_m=fluid.cell_center_y_m,
+        cell_center_z_m=fluid.cell_center_z_m, search_radius_m=0.08, interior_probe_distance_m=0.125,
+        classify_far_internal_nodes=True)
+    assert rep.near_boundary_node_count == 0 and rep.internal_node_count == 8
+    assert search.node_kind((1, 1, 1)) == "internal" and search.node_kind((2, 2, 2)) == "internal"
+    assert search.node_kind((0, 0, 0)) == "none"
+
+
+# test_hibm.py:1088
+def test_ib_search_default_sign_tolerance_flags_ambiguous_node():
+    search = _node_search((1, 1, 1), 1)
+    rep = search.search_and_classify(_markers(((0.5, 0.5, 0.5 - 5.0e-8),), ((0.0, 0.0, 1.0),)), search_radius_m=0.01,
+                                     interior_probe_distance_m=0.125)
+    assert rep.near_boundary_node_count == 1 and rep.invalid_projection_count == 1
+    assert search.node_kind((0, 0, 0)) == "internal" and search.signed_distance_m((0, 0, 0)) > 0.0
+
+
+# test_hibm.py:1115
+def test_ib_search_nonuniform_cell_centres():
+    from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
+    from easyfsi_b200.grid import CartesianGrid
+
+    grid = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=(0.25,) * 4, cell_widths_y_m=(0.25,) * 4,
+                         cell_widths_z_m=(0.1, 0.1, 0.2, 0.6))
+    fluid = CartesianFluidSolver(FluidDomainSpec(bounds_min_m=(0.0, 0.0, 0.0), bounds_max_m=(1.0, 1.0, 1.0),
+                                                 grid_nodes=(4, 4, 4), density_kgm3=1000.0, viscosity_pa_s=1.0e-3,
+                                                 dt_s=1.0e-3, cartesian_grid=grid))
+    search = _node_search(fluid.grid.grid_nodes, 1, fluid.grid.bounds_min_m, fluid.grid.bounds_max_m)
+    rep = search.search_and_classify_grid_fields(
+        _markers(((0.625, 0.625, 0.28),), ((0.0, 0.0, 1.0),)), cell_center_x_m=fluid.cell_center_x_m,
+        cell_center_y_m=fluid.cell_center_y_m, cell_center_z_m=fluid.cell_center_z_m, search_radius_m=0.04,
+        interior_probe_distance_m=0.05)
+    assert (rep.near_boundary_node_count, rep.external_ib_node_count, rep.internal_node_count) == (1, 1, 0)
+    assert search.node_kind((2, 2, 2)) == "external_ib" and search.node_kind((2, 2, 1)) == "none"
+    assert search.signed_distance_m((2, 2, 2)) == pytest.approx(0.02, abs=1e-6)
+    np.testing.assert_allclose(search.boundary_point_m((2, 2, 2)), (0.625, 0.625, 0.28), atol=1e-6)
+    assert search.interior_fluid_point_m((2, 2, 2))[2] == pytest.approx(0.35, abs=1e-6)
+
+
+# test_hibm.py:1174
+def test_ib_search_external_if_any_local_normal_is_positive():
+    search = _node_search((1, 1, 1), 2)
+    rep = search.search_and_classify(_markers(((0.5, 0.5, 0.55), (0.5, 0.5, 0.45)), ((0.0, 0.0, -1.0), (0.0, 0.0, 1.0))),
+                                     search_radius_m=0.08, interior_probe_distance_m=0.05)
+    assert (rep.near_boundary_node_count, rep.external_ib_node_count, rep.internal_node_count) == (1, 1, 0)
+    assert search.node_kind((0, 0, 0)) == "external_ib"
+
+
+# test_hibm.py:1201
+def test_ib_search_stores_the_external_candidate():
+    search = _node_search((1, 1, 1), 2)
+    rep = search.search_and_classify(_markers(((0.5, 0.5, 0.49), (0.5, 0.5, 0.46)), ((0.0, 0.0, -1.0), (0.0, 0.0, 1.0))),
+                                     search_radius_m=0.05, interior_probe_distance_m=0.05, sign_tolerance_m=1.0e-8)
+    assert (rep.near_boundary_node_count, rep.external_ib_node_count, rep.internal_node_count) == (1, 1, 0)
+    assert search.node_kind((0, 0, 0)) == "external_ib" and search.nearest_marker_index((0, 0, 0)) == 1
+    assert search.signed_distance_m((0, 0, 0)) > 0.0
+    assert search.boundary_point_m((0, 0, 0))[2] == pytest.approx(0.46, abs=1e-6)
+    assert search.interior_fluid_point_m((0, 0, 0))[2] > 0.5
+
+
+# test_hibm.py:1240
+def test_ib_search_radial_marker_inside_and_outside():
+    search = _node_search((4, 1, 1), 1)
+    rep = search.search_and_classify(_markers(((0.75, 0.5, 0.5),), ((1.0, 0.0, 0.0),)), search_radius_m=0.14,
+                                     interior_probe_distance_m=0.125)
+    assert (rep.near_boundary_node_count, rep.external_ib_node_count, rep.internal_node_count) == (2, 1, 1)
+    assert search.node_kind((3, 0, 0)) == "external_ib" and search.node_kind((2, 0, 0)) == "internal"
+    assert search.signed_distance_m((3, 0, 0)) > 0.0 and search.signed_distance_m((2, 0, 0)) < 0.0
+
+
+# test_hibm.py:1270
+def test_ib_search_tangent_projection_records_invalid():
+    search = _node_search((1, 1, 1), 1)
+    rep = search.search_and_classify(_markers(((0.5, 0.5, 0.5),), ((0.0, 0.0, 1.0),)), search_radius_m=0.1,
+                                     interior_probe_distance_m=0.125, sign_tolerance_m=1.0e-9)
+    assert rep.near_boundary_node_count == 1 and rep.invalid_projection_count == 1
+    assert search.nearest_marker_index((0, 0, 0)) == 0
+    assert search.boundary_point_m((0, 0, 0)) == (0.5, 0.5, 0.5)
+    assert search.interior_fluid_point_m((0, 0, 0)) == (0.5, 0.5, 0.625)
+
+
+def test_ib_search_rejects_bad_arguments():
+    """hibm_mpm.py:6069-6094 argument errors."""
+    mk = _markers(((0.5, 0.5, 0.5),), ((0.0, 0.0, 1.0),))
+    search = _node_search((2, 2, 2), 1)
+    for kwargs in ({"search_radius_m": 0.0, "interior_probe_distance_m": 0.1},
+                   {"search_radius_m": math.inf, "interior_probe_distance_m": 0.1},
+                   {"search_radius_m": 0.1, "interior_probe_distance_m": -1.0},
+                   {"search_radius_m": 0.1, "interior_probe_distance_m": 0.1, "sign_tolerance_m": -1.0}):
+        with pytest.raises(ValueError):
+            search.search_and_classify(mk, **kwargs)

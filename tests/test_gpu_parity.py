@@ -359,3 +359,87 @@ def test_mixed_precision_vcycle_with_dirichlet_rows_or_outlet(aux, outlet):
     assert it32 <= it64 + 5
     assert not np.array_equal(p32, p64)
     assert rel_l2(p32, p64) <= 1e-5
+
+
+def _sphere_surface(center, radius, n_theta=9, n_phi=14, seed=5):
+    """Markers on a slightly perturbed UV sphere, outward normals, and its
+    triangles (pole fans and split quads)."""
+    rng = np.random.default_rng(seed)
+    pts = [(0.0, 0.0, 1.0)]
+    for i in range(1, n_theta):
+        th = np.pi * i / n_theta
+        for j in range(n_phi):
+            ph = 2.0 * np.pi * j / n_phi
+            pts.append((np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)))
+    pts.append((0.0, 0.0, -1.0))
+    unit = np.asarray(pts) * (1.0 + 0.02 * rng.standard_normal((len(pts), 1)))
+    x = np.asarray(center) + radius * unit
+    n = unit / np.linalg.norm(unit, axis=1, keepdims=True)
+    ring = lambda i, j: 1 + (i - 1) * n_phi + (j % n_phi)  # noqa: E731
+    tri = [(0, ring(1, j), ring(1, j + 1)) for j in range(n_phi)]
+    for i in range(1, n_theta - 1):
+        for j in range(n_phi):
+            a, b, c, d = ring(i, j), ring(i, j + 1), ring(i + 1, j), ring(i + 1, j + 1)
+            tri += [(a, c, b), (b, c, d)]
+    south = len(pts) - 1
+    tri += [(south, ring(n_theta - 1, j + 1), ring(n_theta - 1, j)) for j in range(n_phi)]
+    return x, n, np.asarray(tri, np.int32)
+
+
+def test_ib_node_search_matches_oracle():
+    """The binned node search against the oracle's all-pairs loop on a closed
+    triangulated surface: node kinds, nearest markers and projection indices
+    identical; distances, points and weights within 1e-6 (the same f32
+    expressions, unfused, on both sides); same report counts.  One search
+    object runs every case, so its bin buffers are rebuilt between them."""
+    from easyfsi_b200.hibm_mpm import HibmMpmIbNodeSearch, HibmMpmSurfaceMarkers
+
+    grid = _graded_grid((24, 20, 28))
+    nodes = grid.grid_nodes
+    x, n, tri = _sphere_surface((0.45, 0.5, 0.55), 0.28)
+    mk = HibmMpmSurfaceMarkers(marker_capacity=len(x), projection_triangle_capacity=len(tri))
+    mk.load_markers(positions_m=x, velocities_mps=np.zeros_like(x), normals=n, areas_m2=np.ones(len(x)),
+                    region_ids=np.full(len(x), 7))
+    search = HibmMpmIbNodeSearch(grid_nodes=nodes, bounds_min_m=grid.bounds_min_m, bounds_max_m=grid.bounds_max_m,
+                                 marker_capacity=len(x))
+    centres_np = [np.asarray(c, np.float32) for c in (grid.cell_centers_x_m, grid.cell_centers_y_m,
+                                                      grid.cell_centers_z_m)]
+    centres = [torch.as_tensor(c, device="cuda") for c in centres_np]
+    mx = mk.x_gamma_m.to_numpy()[: len(x)]
+    mn = mk.n_gamma.to_numpy()[: len(x)]
+    tol = search._default_sign_tolerance_m()
+    cases = [  # (node positions, classify far, triangles, radius)
+        ("grid", False, True, 0.07),
+        ("grid", True, True, 0.07),
+        ("uniform", True, True, 0.05),
+        ("grid", True, False, 0.07),
+        ("grid", False, True, 0.6),
+    ]
+    for where, far, use_tri, radius in cases:
+        mk.projection_triangle_count = 0
+        if use_tri:
+            mk.set_projection_triangles(tri.tolist())
+        kwargs = dict(search_radius_m=radius, interior_probe_distance_m=0.03, classify_far_internal_nodes=far)
+        if where == "grid":
+            rep = search.search_and_classify_grid_fields(mk, cell_center_x_m=centres[0], cell_center_y_m=centres[1],
+                                                         cell_center_z_m=centres[2], **kwargs)
+        else:
+            rep = search.search_and_classify(mk, **kwargs)
+        ref = orc.ib_node_search(
+            grid_nodes=nodes, markers_x=mx, markers_n=mn, triangles=tri if use_tri else None, search_radius=radius,
+            interior_probe_distance=0.03, sign_tolerance=tol, classify_far=far,
+            centers=centres_np if where == "grid" else None, bounds_min=grid.bounds_min_m, spacing=search.spacing_m)
+        case = (where, far, use_tri, radius)
+        assert rep.__dict__ == ref["report"], case
+        assert ref["report"]["near_boundary_node_count"] > 0, case
+        if far:
+            assert ref["report"]["internal_node_count"] > ref["report"]["near_boundary_node_count"] // 4, case
+        np.testing.assert_array_equal(search.node_kind_code.to_numpy(), ref["kind"], err_msg=str(case))
+        np.testing.assert_array_equal(search.nearest_marker.to_numpy(), ref["nearest_marker"], err_msg=str(case))
+        np.testing.assert_array_equal(search.node_projection_marker_indices.to_numpy(), ref["projection_indices"],
+                                      err_msg=str(case))
+        for got, key in ((search.node_signed_distance_m, "signed_distance"), (search.node_boundary_point_m,
+                         "boundary_point"), (search.node_interior_fluid_point_m, "interior_point"),
+                         (search.node_projection_marker_weights, "projection_weights")):
+            np.testing.assert_allclose(got.to_numpy(), ref[key], rtol=0.0, atol=1e-6, err_msg=f"{case} {key}")
+    assert (search.node_anchor_cell.to_numpy() == -1).all()

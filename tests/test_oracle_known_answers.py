@@ -219,3 +219,136 @@ def test_clear_then_scatter_replaces_stale_force():
     assert cleared == 1 and largest == pytest.approx(99.0)
     m.scatter(s, 0.25)
     assert tuple(s.fext[0]) == (1.0, -2.0, 3.0)
+
+
+# --------------------------------------------------------------------------
+# IB node search and classification (hibm_mpm.py:5385-6220), the reference's
+# HibmMpmIbNodeSearchTests (tests/test_hibm.py:903-1297) on the oracle.
+# --------------------------------------------------------------------------
+def _default_sign_tolerance(bmin, bmax, nodes):
+    """hibm_mpm.py:5477-5492 for a search box."""
+    spacing = [(hi - lo) / n for lo, hi, n in zip(bmin, bmax, nodes)]
+    min_spacing = max(min(spacing), 1.0e-12)
+    max_extent = max(hi - lo for lo, hi in zip(bmin, bmax))
+    max_coord = max(max(abs(v) for v in bmin), max(abs(v) for v in bmax))
+    scale = max(max_extent, max_coord, min_spacing, 1.0)
+    return max(1.0e-12, 1.0e-6 * min_spacing, 2.0 * 1.1920928955078125e-7 * scale)
+
+
+def _search(nodes, x, n, *, radius, probe, tol=None, far=False, triangles=None, centers=None,
+            bmin=(0.0, 0.0, 0.0), bmax=(1.0, 1.0, 1.0)):
+    spacing = [(hi - lo) / k for lo, hi, k in zip(bmin, bmax, nodes)]
+    nn = np.asarray(n, np.float64)
+    nn = nn / np.linalg.norm(nn, axis=1, keepdims=True)  # load_markers normalises (hibm_mpm.py:553)
+    return orc.ib_node_search(
+        grid_nodes=nodes, markers_x=np.asarray(x, np.float64), markers_n=nn, triangles=triangles,
+        search_radius=radius, interior_probe_distance=probe,
+        sign_tolerance=_default_sign_tolerance(bmin, bmax, nodes) if tol is None else tol, classify_far=far,
+        centers=centers, bounds_min=bmin, spacing=spacing)
+
+
+def _report(r, near, ext, internal, invalid=None):
+    rep = r["report"]
+    assert rep["near_boundary_node_count"] == near
+    assert rep["external_ib_node_count"] == ext
+    assert rep["internal_node_count"] == internal
+    if invalid is not None:
+        assert rep["invalid_projection_count"] == invalid
+
+
+# test_hibm.py:904 plane search classifies external and internal nodes
+def test_ib_search_plane_classifies_external_and_internal_nodes():
+    r = _search((1, 1, 4), [(0.5, 0.5, 0.5)], [(0.0, 0.0, 1.0)], radius=0.26, probe=0.125)
+    _report(r, 2, 1, 1, 0)
+    assert r["kind"][0, 0, 2] == 1 and r["kind"][0, 0, 1] == 2
+    assert r["nearest_marker"][0, 0, 2] == 0 and r["nearest_marker"][0, 0, 1] == 0
+    assert tuple(r["boundary_point"][0, 0, 2]) == (0.5, 0.5, 0.5)
+    assert tuple(r["interior_point"][0, 0, 2]) == (0.5, 0.5, 0.75)
+    assert r["signed_distance"][0, 0, 2] > 0.0 and r["signed_distance"][0, 0, 1] < 0.0
+
+
+# test_hibm.py:939 triangle projection finds the closest surface point between markers
+def test_ib_search_triangle_projection_between_markers():
+    x = [(0.25, 0.25, 0.5), (0.75, 0.25, 0.5), (0.25, 0.75, 0.5)]
+    r = _search((8, 8, 8), x, [(0.0, 0.0, 1.0)] * 3, triangles=[(0, 1, 2)], radius=0.08, probe=0.05)
+    assert r["report"]["near_boundary_node_count"] >= 1 and r["report"]["external_ib_node_count"] >= 1
+    assert r["kind"][2, 2, 4] == 1
+    np.testing.assert_allclose(r["boundary_point"][2, 2, 4], (0.3125, 0.3125, 0.5), atol=1e-6)
+    assert r["signed_distance"][2, 2, 4] == pytest.approx(0.0625)
+    np.testing.assert_allclose(r["interior_point"][2, 2, 4], (0.3125, 0.3125, 0.6125), atol=1e-6)
+
+
+_CLOSED_X = [(0.25, 0.5, 0.5), (0.75, 0.5, 0.5), (0.5, 0.25, 0.5), (0.5, 0.75, 0.5), (0.5, 0.5, 0.25), (0.5, 0.5, 0.75)]
+_CLOSED_N = [(-1.0, 0.0, 0.0), (1.0, 0.0, 0.0), (0.0, -1.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, -1.0), (0.0, 0.0, 1.0)]
+
+
+# test_hibm.py:987 closed surface search classifies deep internal nodes
+def test_ib_search_closed_surface_deep_internal_node():
+    r = _search((1, 1, 1), _CLOSED_X, _CLOSED_N, radius=0.1, probe=0.125, far=True)
+    _report(r, 0, 0, 1)
+    assert r["kind"][0, 0, 0] == 2 and r["nearest_marker"][0, 0, 0] >= 0
+
+
+# test_hibm.py:1030 closed surface grid-field search classifies deep internal nodes
+def test_ib_search_closed_surface_grid_fields_deep_internal_nodes():
+    grid = _uniform_box(4)
+    centers = (grid.cell_centers_x_m, grid.cell_centers_y_m, grid.cell_centers_z_m)
+    r = _search((4, 4, 4), _CLOSED_X, _CLOSED_N, radius=0.08, probe=0.125, far=True, centers=centers)
+    assert r["report"]["near_boundary_node_count"] == 0 and r["report"]["internal_node_count"] == 8
+    assert r["kind"][1, 1, 1] == 2 and r["kind"][2, 2, 2] == 2 and r["kind"][0, 0, 0] == 0
+
+
+# test_hibm.py:1088 default sign tolerance flags f32-scale ambiguous nodes
+def test_ib_search_default_sign_tolerance_flags_ambiguous_node():
+    r = _search((1, 1, 1), [(0.5, 0.5, 0.5 - 5.0e-8)], [(0.0, 0.0, 1.0)], radius=0.01, probe=0.125)
+    assert r["report"]["near_boundary_node_count"] == 1 and r["report"]["invalid_projection_count"] == 1
+    assert r["kind"][0, 0, 0] == 2 and r["signed_distance"][0, 0, 0] > 0.0
+
+
+# test_hibm.py:1115 search uses non-uniform fluid cell-centre fields
+def test_ib_search_nonuniform_cell_centres():
+    grid = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=(0.25,) * 4, cell_widths_y_m=(0.25,) * 4,
+                         cell_widths_z_m=(0.1, 0.1, 0.2, 0.6))
+    centers = (grid.cell_centers_x_m, grid.cell_centers_y_m, grid.cell_centers_z_m)
+    r = _search((4, 4, 4), [(0.625, 0.625, 0.28)], [(0.0, 0.0, 1.0)], radius=0.04, probe=0.05, centers=centers)
+    _report(r, 1, 1, 0)
+    assert r["kind"][2, 2, 2] == 1 and r["kind"][2, 2, 1] == 0
+    assert r["signed_distance"][2, 2, 2] == pytest.approx(0.02, abs=1e-6)
+    np.testing.assert_allclose(r["boundary_point"][2, 2, 2], (0.625, 0.625, 0.28), atol=1e-6)
+    assert r["interior_point"][2, 2, 2][2] == pytest.approx(0.35, abs=1e-6)
+
+
+# test_hibm.py:1174 a node is external if any local normal sees it outside
+def test_ib_search_external_if_any_local_normal_is_positive():
+    r = _search((1, 1, 1), [(0.5, 0.5, 0.55), (0.5, 0.5, 0.45)], [(0.0, 0.0, -1.0), (0.0, 0.0, 1.0)],
+                radius=0.08, probe=0.05)
+    _report(r, 1, 1, 0)
+    assert r["kind"][0, 0, 0] == 1
+
+
+# test_hibm.py:1201 external search stores the external projection candidate
+def test_ib_search_stores_the_external_candidate():
+    r = _search((1, 1, 1), [(0.5, 0.5, 0.49), (0.5, 0.5, 0.46)], [(0.0, 0.0, -1.0), (0.0, 0.0, 1.0)],
+                radius=0.05, probe=0.05, tol=1.0e-8)
+    _report(r, 1, 1, 0)
+    assert r["kind"][0, 0, 0] == 1 and r["nearest_marker"][0, 0, 0] == 1
+    assert r["signed_distance"][0, 0, 0] > 0.0
+    assert r["boundary_point"][0, 0, 0][2] == pytest.approx(0.46, abs=1e-6)
+    assert r["interior_point"][0, 0, 0][2] > 0.5
+
+
+# test_hibm.py:1240 radial marker classifies inside and outside nodes
+def test_ib_search_radial_marker_inside_and_outside():
+    r = _search((4, 1, 1), [(0.75, 0.5, 0.5)], [(1.0, 0.0, 0.0)], radius=0.14, probe=0.125)
+    _report(r, 2, 1, 1)
+    assert r["kind"][3, 0, 0] == 1 and r["kind"][2, 0, 0] == 2
+    assert r["signed_distance"][3, 0, 0] > 0.0 and r["signed_distance"][2, 0, 0] < 0.0
+
+
+# test_hibm.py:1270 tangent projection fallback records the invalid count
+def test_ib_search_tangent_projection_records_invalid():
+    r = _search((1, 1, 1), [(0.5, 0.5, 0.5)], [(0.0, 0.0, 1.0)], radius=0.1, probe=0.125, tol=1.0e-9)
+    assert r["report"]["near_boundary_node_count"] == 1 and r["report"]["invalid_projection_count"] == 1
+    assert r["nearest_marker"][0, 0, 0] == 0
+    assert tuple(r["boundary_point"][0, 0, 0]) == (0.5, 0.5, 0.5)
+    assert tuple(r["interior_point"][0, 0, 0]) == (0.5, 0.5, 0.625)
