@@ -115,6 +115,46 @@ class ClockSampler:
         }
 
 
+def ib_node_search_stats(scene, reps: int) -> dict:
+    """The IB node search (HibmMpmIbNodeSearch.search_and_classify_grid_fields)
+    over the scene's fluid cell centres against its markers (the scene has no
+    projection triangles, so the markers are the candidates), radius two of
+    the finest cells, far nodes classified.  CUDA events around `reps` calls;
+    each call includes its two small host reads (bin entry total, report).
+    `pairs_per_s` counts the node-marker pairs the reference's all-pairs loop
+    would evaluate for the same result."""
+    import torch
+
+    from easyfsi_b200.hibm_mpm import HibmMpmIbNodeSearch
+
+    fl, mk = scene.fluid, scene.markers
+    g = fl.grid
+    search = HibmMpmIbNodeSearch(grid_nodes=g.grid_nodes, bounds_min_m=g.bounds_min_m, bounds_max_m=g.bounds_max_m,
+                                 marker_capacity=mk.marker_capacity)
+    radius = 2.0 * min(min(g._widths(a)) for a in range(3))
+    kwargs = dict(cell_center_x_m=fl.cell_center_x_m, cell_center_y_m=fl.cell_center_y_m,
+                  cell_center_z_m=fl.cell_center_z_m, search_radius_m=radius, interior_probe_distance_m=radius,
+                  classify_far_internal_nodes=True)
+    rep = search.search_and_classify_grid_fields(mk, **kwargs)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        rep = search.search_and_classify_grid_fields(mk, **kwargs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    nodes = int(np.prod(g.grid_nodes))
+    return {
+        "ms_per_call": ms,
+        "nodes": nodes,
+        "markers": int(mk.marker_count),
+        "search_radius_m": radius,
+        "report": dict(rep.__dict__),
+        "pairs_per_s": nodes * int(mk.marker_count) / (ms * 1e-3),
+    }
+
+
 def max_over_ranks(ms: float, world: int, device) -> float:
     """Largest per-rank time over all ranks (every rank calls this in the same
     order; a no-op for one rank)."""
@@ -193,6 +233,7 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the fv_multigrid_mixed measurement")
+    ap.add_argument("--no-ib-search", action="store_true", help="skip the IB node search measurement")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-reps", type=int, default=50)
@@ -304,6 +345,14 @@ def main() -> None:
             "ratio_to_fv_multigrid": m_value / value,
         }
         scene.preconditioner = "fv_multigrid"
+
+    # --- the IB node search on the same grid and markers (not part of the step) ---
+    ib_search = None
+    if not args.no_ib_search:
+        try:
+            ib_search = ib_node_search_stats(scene, reps=5)
+        except Exception as exc:  # reported, never fatal to the step's line
+            ib_search = {"error": f"{type(exc).__name__}: {exc}"}
 
     # --- e2e through the public API with host-resident state ---
     e2e = None
@@ -423,6 +472,7 @@ def main() -> None:
             "kernel_families": fam_stats,
             "preconditioner": vcycle_stats,
             "mixed_precision": mixed,
+            "ib_node_search": ib_search,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
