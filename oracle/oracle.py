@@ -422,6 +422,37 @@ def ib_node_search(*, grid_nodes, markers_x, markers_n, triangles=None, search_r
     return out
 
 
+def ib_build_boundary_conditions(search: dict, *, markers_v, markers_n, marker_gradients,
+                                 variant: str = "mirror") -> dict:
+    """hibm_mpm.py:6499-6577 on the fields of ``ib_node_search``: per-node
+    no-slip velocity, Neumann normal and gradient targets of the external IB
+    nodes, and the report (no-slip rows, Neumann rows, inactive internal
+    nodes, max |v|)."""
+    lib = load(variant)
+    rt = r32_dtype(variant)
+    kind = np.ascontiguousarray(search["kind"], np.int32)
+    shape = kind.shape
+    n = int(kind.size)
+    mv = np.ascontiguousarray(markers_v, dtype=rt).reshape(-1, 3)
+    mn = np.ascontiguousarray(markers_n, dtype=rt).reshape(-1, 3)
+    mg = np.ascontiguousarray(marker_gradients, dtype=rt).reshape(-1)
+    out = {
+        "active": np.zeros(shape, np.int32),
+        "velocity": np.zeros(shape + (3,), rt),
+        "normal": np.zeros(shape + (3,), rt),
+        "gradient": np.zeros(shape, rt),
+    }
+    report = np.zeros(4, np.float64)
+    lib.efo_ib_build_boundary_conditions(
+        c_int64(n), _p(kind), _p(np.ascontiguousarray(search["nearest_marker"], np.int32)),
+        _p(np.ascontiguousarray(search["projection_indices"], np.int32)),
+        _p(np.ascontiguousarray(search["projection_weights"], rt)), _p(mv), _p(mn), _p(mg), c_int(mv.shape[0]),
+        _p(out["active"]), _p(out["velocity"]), _p(out["normal"]), _p(out["gradient"]), _p(report))
+    out["report"] = {"no_slip_dirichlet_count": int(report[0]), "pressure_neumann_count": int(report[1]),
+                     "inactive_internal_node_count": int(report[2]), "max_abs_velocity_mps": float(report[3])}
+    return out
+
+
 class OracleScene:
     """The coupled step of easyfsi_b200.scenarios.CoupledScene on host arrays."""
 

@@ -268,3 +268,67 @@ EFO_API void efo_ib_node_search(int nx, int ny, int nz, const r32* cx, const r32
   report[2] = int_count;
   report[3] = invalid_count;
 }
+
+// hibm_mpm.py:6499-6577 HibmMpmIbBoundaryConditions._build_from_search_kernel:
+// per external IB node, the no-slip velocity, Neumann normal and Neumann
+// gradient targets interpolated from the projection markers (weights > 0,
+// renormalised; the nearest marker's values when no weight is usable); the
+// normal is renormalised.  f32 throughout, as the reference's fields.
+// Outputs per node: active (0/1), velocity (3), normal (3), gradient;
+// report[4] = no-slip rows, Neumann rows, inactive internal nodes, max |v|.
+EFO_API void efo_ib_build_boundary_conditions(int64_t n, const int32_t* kind, const int32_t* nearest,
+                                              const int32_t* pidx, const r32* pw, const r32* mv, const r32* mn,
+                                              const r32* mgrad, int marker_count, int32_t* active, r32* vel,
+                                              r32* nrm, r32* grad, double* report) {
+  int64_t rows = 0, inactive = 0;
+  r32 vmax = 0;
+  for (int64_t c = 0; c < n; ++c) {
+    active[c] = 0;
+    store3(vel, c, v3(0, 0, 0));
+    store3(nrm, c, v3(0, 0, 0));
+    grad[c] = 0;
+    if (kind[c] == 1) {
+      const int marker = nearest[c];
+      if (!(0 <= marker && marker < marker_count)) continue;
+      V3 tv = v3(0, 0, 0), tn = v3(0, 0, 0);
+      r32 tg = 0, total = 0;
+      for (int q = 0; q < 3; ++q) {
+        const int pm = pidx[3 * c + q];
+        const r32 w = pw[3 * c + q];
+        if (0 <= pm && pm < marker_count && w > 0) {
+          tv = add(tv, scale(load3(mv, pm), w));
+          tn = add(tn, scale(load3(mn, pm), w));
+          tg = tg + w * mgrad[pm];
+          total = total + w;
+        }
+      }
+      if (total > (r32)1.0e-12) {
+        const r32 inv = (r32)1 / total;
+        tv = scale(tv, inv);
+        tn = scale(tn, inv);
+        tg = tg * inv;
+        const r32 nn = norm(tn);
+        if (nn > (r32)1.0e-12)
+          tn = divide(tn, nn);
+        else
+          tn = load3(mn, marker);
+      } else {
+        tv = load3(mv, marker);
+        tn = load3(mn, marker);
+        tg = mgrad[marker];
+      }
+      active[c] = 1;
+      store3(vel, c, tv);
+      store3(nrm, c, tn);
+      grad[c] = tg;
+      rows += 1;
+      vmax = std::max(vmax, std::max(std::max(std::fabs(tv.x), std::fabs(tv.y)), std::fabs(tv.z)));
+    } else if (kind[c] == 2) {
+      inactive += 1;
+    }
+  }
+  report[0] = (double)rows;
+  report[1] = (double)rows;
+  report[2] = (double)inactive;
+  report[3] = (double)vmax;
+}

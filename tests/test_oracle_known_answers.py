@@ -352,3 +352,32 @@ def test_ib_search_tangent_projection_records_invalid():
     assert r["nearest_marker"][0, 0, 0] == 0
     assert tuple(r["boundary_point"][0, 0, 0]) == (0.5, 0.5, 0.5)
     assert tuple(r["interior_point"][0, 0, 0]) == (0.5, 0.5, 0.625)
+
+
+# test_hibm.py:1301 builds external-IB no-slip and pressure-Neumann targets
+# (HibmMpmIbBoundaryConditions.build_from_search, hibm_mpm.py:6499-6605)
+def test_ib_boundary_targets_from_the_plane_search():
+    s = _search((1, 1, 4), [(0.5, 0.5, 0.5)], [(0.0, 0.0, 2.0)], radius=0.26, probe=0.125)
+    bc = orc.ib_build_boundary_conditions(s, markers_v=[(1.25, -0.5, 0.75)], markers_n=[(0.0, 0.0, 1.0)],
+                                          marker_gradients=[42.0])
+    rep = bc["report"]
+    assert (rep["no_slip_dirichlet_count"], rep["pressure_neumann_count"], rep["inactive_internal_node_count"]) == (1, 1, 1)
+    assert rep["max_abs_velocity_mps"] == pytest.approx(1.25, abs=1e-6)
+    assert bc["active"][0, 0, 2] == 1 and bc["active"][0, 0, 1] == 0
+    assert tuple(bc["velocity"][0, 0, 2]) == (1.25, -0.5, 0.75)
+    assert tuple(bc["normal"][0, 0, 2]) == (0.0, 0.0, 1.0)
+    assert bc["gradient"][0, 0, 2] == pytest.approx(42.0)
+
+
+# test_hibm.py:1343 triangle projection interpolates curved-surface targets
+def test_ib_boundary_targets_interpolate_over_the_projection_triangle():
+    x = [(0.25, 0.25, 0.5), (0.75, 0.25, 0.5), (0.25, 0.75, 0.5)]
+    eye = [(1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0)]
+    s = _search((8, 8, 8), x, eye, triangles=[(0, 1, 2)], radius=0.08, probe=0.05)
+    bc = orc.ib_build_boundary_conditions(s, markers_v=eye, markers_n=eye, marker_gradients=[100.0, 200.0, 300.0])
+    w = np.array((0.75, 0.125, 0.125))
+    assert bc["report"]["no_slip_dirichlet_count"] == bc["report"]["pressure_neumann_count"]
+    assert bc["active"][2, 2, 4] == 1
+    np.testing.assert_allclose(bc["velocity"][2, 2, 4], w, atol=1e-6)
+    np.testing.assert_allclose(bc["normal"][2, 2, 4], w / np.linalg.norm(w), atol=1e-6)
+    assert bc["gradient"][2, 2, 4] == pytest.approx(137.5, abs=1e-5)
