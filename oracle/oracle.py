@@ -205,6 +205,33 @@ class OracleFluid:
         self.lib.efo_fv_apply(byref(self.levels[0]), _p(self.obstacle), _p(vdir_active), _p(vdir_weight), _p(iface), _p(p), _p(out), c_int(outlet))
         return out
 
+    def fv_apply_coupled(self, p: np.ndarray, outlet: int = 0, iface=None, *, slots=None, rows=None) -> np.ndarray:
+        """The FV operator plus the interface-coupling terms (fluid.py:4345-4456):
+        ``slots = (active, neighbor, coefficient, extra_neighbor,
+        extra_coefficient)`` per cell, or ``rows = (owner, neighbor,
+        transmissibility)``, which take precedence when non-empty."""
+        out = self.fv_apply(p, outlet, iface=iface)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        shape = (self.nx, self.ny, self.nz)
+        if slots is None:
+            slots = (np.zeros(shape, np.int32), np.zeros(shape + (3,), np.int32), np.zeros(shape),
+                     np.zeros(shape + (15, 3), np.int32), np.zeros(shape + (15,)))
+        active, nb, coef, xnb, xcoef = (np.ascontiguousarray(a, dt) for a, dt in zip(
+            slots, (np.int32, np.int32, np.float64, np.int32, np.float64)))
+        n_extra = int(xcoef.shape[-1])
+        if rows is None or len(rows[2]) == 0:
+            owner = nbr = np.zeros((1, 3), np.int32)
+            trans = np.zeros(1)
+            count = 0
+        else:
+            owner, nbr = (np.ascontiguousarray(a, np.int32).reshape(-1, 3) for a in rows[:2])
+            trans = np.ascontiguousarray(rows[2], np.float64)
+            count = len(trans)
+        self.lib.efo_fv_interface_coupling(byref(self.levels[0]), _p(self.obstacle), _p(p), _p(out), _p(active),
+                                           _p(nb), _p(coef), _p(xnb), _p(xcoef), c_int(n_extra), c_int(count),
+                                           _p(owner), _p(nbr), _p(trans))
+        return out
+
     def fv_diagonal(self, outlet: int = 0, vdir_active=None, vdir_weight=None, iface=None) -> np.ndarray:
         out = np.zeros((self.nx, self.ny, self.nz), dtype=np.float64)
         self.lib.efo_fv_diagonal(byref(self.levels[0]), _p(self.obstacle), _p(vdir_active), _p(vdir_weight), _p(iface), _p(out), c_int(outlet))

@@ -1026,3 +1026,55 @@ EFO_API void efo_apply_body_force(const efo_level* Lp, const int32_t* obs, const
           for (int a = 0; a < 3; ++a) vel[3 * c + a] += force[3 * c + a] * (dt / rho);
       }
 }
+
+// fluid.py:4345-4456, the interface-coupling terms of
+// _fv_laplacian_apply_kernel, added to `out` after the FV operator: each
+// coupling (owner, neighbour, transmissibility T > 0) between two fluid cells
+// subtracts T / V_owner * p[neighbour] from the owner's row and
+// T / V_neighbour * p[owner] from the neighbour's.  The explicit row list is
+// used when row_count > 0, else the per-cell slots (active count, first
+// neighbour / coefficient, then n_extra extra slots; at most 16 slots in
+// all).  Cell volumes are the f32 products of the widths
+// (fluid.py:2861-2862).  Sequential order here; the reference adds atomically.
+EFO_API void efo_fv_interface_coupling(const efo_level* Lp, const int32_t* obs, const double* p, double* out,
+                                       const int32_t* active, const int32_t* nb, const double* coef,
+                                       const int32_t* extra_nb, const double* extra_coef, int n_extra,
+                                       int row_count, const int32_t* row_owner, const int32_t* row_neighbor,
+                                       const double* row_t) {
+  const efo_level& L = *Lp;
+  auto inside = [&](int i, int j, int k) { return 0 <= i && i < L.nx && 0 <= j && j < L.ny && 0 <= k && k < L.nz; };
+  auto vol = [&](int i, int j, int k) {
+    const r32 v = L.wx[i] * L.wy[j] * L.wz[k];
+    return (double)std::max(v, (r32)1.0e-30);
+  };
+  auto couple = [&](int i, int j, int k, int ni, int nj, int nk, double t) {
+    const int64_t c = efo_idx(i, j, k, L.ny, L.nz), cn = efo_idx(ni, nj, nk, L.ny, L.nz);
+    out[c] += -(t / vol(i, j, k)) * p[cn];
+    out[cn] += -(t / vol(ni, nj, nk)) * p[c];
+  };
+  if (row_count > 0) {
+    const int limit = std::min(row_count, L.nx * L.ny * L.nz);
+    for (int r = 0; r < limit; ++r) {
+      const int i = row_owner[3 * r], j = row_owner[3 * r + 1], k = row_owner[3 * r + 2];
+      const int ni = row_neighbor[3 * r], nj = row_neighbor[3 * r + 1], nk = row_neighbor[3 * r + 2];
+      const double t = row_t[r];
+      if (inside(i, j, k) && inside(ni, nj, nk) && obs[efo_idx(i, j, k, L.ny, L.nz)] == 0 &&
+          obs[efo_idx(ni, nj, nk, L.ny, L.nz)] == 0 && t > 0.0)
+        couple(i, j, k, ni, nj, nk, t);
+    }
+    return;
+  }
+  for (int i = 0; i < L.nx; ++i)
+    for (int j = 0; j < L.ny; ++j)
+      for (int k = 0; k < L.nz; ++k) {
+        const int64_t c = efo_idx(i, j, k, L.ny, L.nz);
+        if (!(active[c] > 0 && obs[c] == 0)) continue;
+        const int slots = std::min(active[c], 1 + n_extra);
+        for (int s = 0; s < slots; ++s) {
+          const int32_t* q = s == 0 ? nb + 3 * c : extra_nb + 3 * (c * n_extra + (s - 1));
+          const double t = s == 0 ? coef[c] : extra_coef[c * n_extra + (s - 1)];
+          const int ni = q[0], nj = q[1], nk = q[2];
+          if (inside(ni, nj, nk) && obs[efo_idx(ni, nj, nk, L.ny, L.nz)] == 0 && t > 0.0) couple(i, j, k, ni, nj, nk, t);
+        }
+      }
+}

@@ -381,3 +381,77 @@ def test_ib_boundary_targets_interpolate_over_the_projection_triangle():
     np.testing.assert_allclose(bc["velocity"][2, 2, 4], w, atol=1e-6)
     np.testing.assert_allclose(bc["normal"][2, 2, 4], w / np.linalg.norm(w), atol=1e-6)
     assert bc["gradient"][2, 2, 4] == pytest.approx(137.5, abs=1e-5)
+
+
+# --------------------------------------------------------------------------
+# Interface-coupling operator terms (fluid.py:4345-4456), the reference's
+# tests/test_core_fluid.py:1756-1897 on the oracle.
+# --------------------------------------------------------------------------
+def _slots(shape):
+    return [np.zeros(shape, np.int32), np.zeros(shape + (3,), np.int32), np.zeros(shape),
+            np.zeros(shape + (15, 3), np.int32), np.zeros(shape + (15,))]
+
+
+# test_core_fluid.py:1756 interface coupling enters the operator symmetrically
+def test_interface_coupling_enters_operator_symmetrically():
+    fl = _fluid(_uniform_box(5))
+    p = np.ones((5, 5, 5))
+    p[2, 2, 2], p[2, 2, 3] = 3.0, 1.0
+    base = fl.fv_apply(p, 0)
+    diag = np.zeros((5, 5, 5))
+    diag[2, 2, 2] = diag[2, 2, 3] = 4.0
+    slots = _slots((5, 5, 5))
+    slots[0][2, 2, 2] = 1
+    slots[1][2, 2, 2] = (2, 2, 3)
+    slots[2][2, 2, 2] = 4.0 * 0.2 ** 3
+    coupled = fl.fv_apply_coupled(p, 0, iface=diag, slots=slots)
+    assert coupled[2, 2, 2] - base[2, 2, 2] == pytest.approx(8.0, abs=1e-5)
+    assert coupled[2, 2, 3] - base[2, 2, 3] == pytest.approx(-8.0, abs=1e-5)
+    # the same coupling as one explicit row gives the same operator
+    rows = (np.array([(2, 2, 2)]), np.array([(2, 2, 3)]), np.array([4.0 * 0.2 ** 3]))
+    np.testing.assert_allclose(fl.fv_apply_coupled(p, 0, iface=diag, rows=rows), coupled, rtol=0, atol=1e-12)
+
+
+# test_core_fluid.py:1792 interface coupling uses the transmissibility on non-uniform cells
+def test_interface_coupling_is_self_adjoint_on_nonuniform_cells():
+    grid = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=(0.1, 0.2, 0.35, 0.35),
+                         cell_widths_y_m=(0.25,) * 4, cell_widths_z_m=(0.25,) * 4)
+    fl = _fluid(grid)
+    rng = np.random.default_rng(41)
+    x = rng.normal(size=grid.grid_nodes).astype(np.float32).astype(np.float64)
+    y = rng.normal(size=grid.grid_nodes).astype(np.float32).astype(np.float64)
+    t, left, right = 0.375, (1, 2, 2), (2, 2, 2)
+    diag = np.zeros(grid.grid_nodes)
+    diag[left] = np.float32(t / (0.2 * 0.25 * 0.25))
+    diag[right] = np.float32(t / (0.35 * 0.25 * 0.25))
+    slots = _slots(grid.grid_nodes)
+    slots[0][left] = 1
+    slots[1][left] = right
+    slots[2][left] = t
+    ax = fl.fv_apply_coupled(x, 0, iface=diag, slots=slots)
+    ay = fl.fv_apply_coupled(y, 0, iface=diag, slots=slots)
+    lhs, rhs = fl.weighted_dot(ax, y), fl.weighted_dot(x, ay)
+    assert abs(lhs - rhs) / max(abs(lhs), abs(rhs), 1e-30) < 1.0e-5
+
+
+# test_core_fluid.py:1839 interface coupling applies multiple owner slots
+def test_interface_coupling_applies_multiple_owner_slots():
+    fl = _fluid(_uniform_box(5))
+    owner, n0, n1 = (2, 2, 2), (2, 2, 3), (2, 3, 2)
+    p = np.ones((5, 5, 5))
+    p[owner], p[n0], p[n1] = 3.0, 1.0, 2.0
+    base = fl.fv_apply(p, 0)
+    v = 0.2 ** 3
+    c0, c1 = 4.0 * v, 7.0 * v
+    diag = np.zeros((5, 5, 5))
+    diag[owner], diag[n0], diag[n1] = (c0 + c1) / v, c0 / v, c1 / v
+    slots = _slots((5, 5, 5))
+    slots[0][owner] = 2
+    slots[1][owner] = n0
+    slots[2][owner] = c0
+    slots[3][owner + (0,)] = n1
+    slots[4][owner + (0,)] = c1
+    op = fl.fv_apply_coupled(p, 0, iface=diag, slots=slots)
+    assert op[owner] - base[owner] == pytest.approx(15.0, abs=5e-5)
+    assert op[n0] - base[n0] == pytest.approx(-8.0, abs=5e-5)
+    assert op[n1] - base[n1] == pytest.approx(-7.0, abs=5e-5)
