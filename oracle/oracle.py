@@ -480,6 +480,56 @@ def ib_build_boundary_conditions(search: dict, *, markers_v, markers_n, marker_g
     return out
 
 
+VD_REPORT_KEYS = (
+    "active_velocity_dirichlet_rows", "inactive_obstacle_rows", "max_abs_velocity_mps",
+    "invalid_reconstruction_row_count", "invalid_no_fluid_sample_row_count", "invalid_nonpositive_gap_row_count",
+    "invalid_node_behind_boundary_row_count", "invalid_node_beyond_interior_row_count",
+    "narrow_gap_boundary_velocity_row_count", "relocated_row_count", "relocation_merged_row_count",
+    "relocation_blocked_row_count", "min_projection_weight", "max_projection_weight",
+)
+
+
+def ib_velocity_dirichlet_rows(grid, *, active_ib, bc_velocity, bc_normal, boundary_point, interior_point,
+                               obstacle, velocity, nearest_marker=None, marker_region=None, region_out=None,
+                               variant: str = "mirror") -> dict:
+    """assemble_velocity_dirichlet_reconstructed_boundary_rows
+    (hibm_mpm.py:7655-7800) on host arrays: ``grid`` is a CartesianGrid
+    (faces and centres as the fluid's f32 fields); the boundary fields come
+    from ``ib_build_boundary_conditions`` and the points from
+    ``ib_node_search``.  ``region_out`` (int32 per node) is stamped in place
+    when ``marker_region`` is given."""
+    lib = load(variant)
+    rt = r32_dtype(variant)
+    nx, ny, nz = grid.grid_nodes
+    shape = (nx, ny, nz)
+    faces = [np.ascontiguousarray(grid.axis_faces(a), rt) for a in range(3)]
+    centres = [np.ascontiguousarray(grid.axis_centers(a), rt) for a in range(3)]
+    f32 = lambda a, extra=(): np.ascontiguousarray(np.broadcast_to(np.asarray(a, rt), shape + extra))  # noqa: E731
+    i32 = lambda a, extra=(): np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.int32), shape + extra))  # noqa: E731
+    act, obs = i32(active_ib), i32(obstacle)
+    bv, bn, bp, ip, vel = (f32(a, (3,)) for a in (bc_velocity, bc_normal, boundary_point, interior_point, velocity))
+    near = i32(-1 if nearest_marker is None else nearest_marker)
+    regions = None if marker_region is None else np.ascontiguousarray(marker_region, np.int32)
+    out = {
+        "active": np.zeros(shape, np.int32),
+        "value": np.zeros(shape + (3,), rt),
+        "weight": np.zeros(shape, rt),
+        "anchor": np.zeros(shape + (3,), np.int32),
+    }
+    if regions is not None and region_out is None:
+        region_out = np.zeros(shape, np.int32)
+    report = np.zeros(14, np.float64)
+    lib.efo_ib_velocity_dirichlet_rows(
+        c_int(nx), c_int(ny), c_int(nz), *(_p(a) for a in faces), *(_p(a) for a in centres), _p(act), _p(bv), _p(bn),
+        _p(bp), _p(ip), _p(near), _p(obs), _p(vel), _p(regions), c_int(0 if regions is None else len(regions)),
+        _p(out["active"]), _p(out["value"]), _p(out["weight"]), _p(out["anchor"]),
+        _p(region_out) if regions is not None else None, _p(report))
+    out["region"] = region_out
+    out["report"] = {k: (float(v) if k in ("max_abs_velocity_mps", "min_projection_weight", "max_projection_weight")
+                         else int(v)) for k, v in zip(VD_REPORT_KEYS, report)}
+    return out
+
+
 class OracleScene:
     """The coupled step of easyfsi_b200.scenarios.CoupledScene on host arrays."""
 

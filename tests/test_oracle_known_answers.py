@@ -369,7 +369,7 @@ def test_ib_boundary_targets_from_the_plane_search():
     assert bc["gradient"][0, 0, 2] == pytest.approx(42.0)
 
 
-# test_hibm.py:1343 triangle projection interpolates curved-surface targets
+# test_hibm.py:1345 triangle projection interpolates curved-surface targets
 def test_ib_boundary_targets_interpolate_over_the_projection_triangle():
     x = [(0.25, 0.25, 0.5), (0.75, 0.25, 0.5), (0.25, 0.75, 0.5)]
     eye = [(1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0)]
@@ -455,3 +455,115 @@ def test_interface_coupling_applies_multiple_owner_slots():
     assert op[owner] - base[owner] == pytest.approx(15.0, abs=5e-5)
     assert op[n0] - base[n0] == pytest.approx(-8.0, abs=5e-5)
     assert op[n1] - base[n1] == pytest.approx(-7.0, abs=5e-5)
+
+
+# --------------------------------------------------------------------------
+# Velocity-Dirichlet reconstructed rows (hibm_mpm.py:6714-7800), the
+# reference's tests/test_hibm.py:3337-3753 on the oracle.
+# --------------------------------------------------------------------------
+def _one_node_rows(node, bv, n, bp, ip, *, obstacle=None, velocity=(0.0, 0.0, 0.0)):
+    grid = _uniform_box(4)
+    act = np.zeros((4, 4, 4), np.int32)
+    act[node] = 1
+    fields = {}
+    for name, value in (("bc_velocity", bv), ("bc_normal", n), ("boundary_point", bp), ("interior_point", ip)):
+        a = np.zeros((4, 4, 4, 3))
+        a[node] = value
+        fields[name] = a
+    obs = np.zeros((4, 4, 4), np.int32) if obstacle is None else obstacle
+    return orc.ib_velocity_dirichlet_rows(grid, active_ib=act, obstacle=obs, velocity=velocity, **fields)
+
+
+# test_hibm.py:3337 no-slip rows reconstruct along the surface normal
+def test_vd_rows_reconstruct_along_the_surface_normal():
+    s = _search((4, 4, 4), [(0.625, 0.625, 0.5)], [(0.0, 0.0, 1.0)], radius=0.13, probe=0.125)
+    bc = orc.ib_build_boundary_conditions(s, markers_v=[(0.0, 0.0, 0.1)], markers_n=[(0.0, 0.0, 1.0)],
+                                          marker_gradients=[0.0])
+    r = orc.ib_velocity_dirichlet_rows(
+        _uniform_box(4), active_ib=bc["active"], bc_velocity=bc["velocity"], bc_normal=bc["normal"],
+        boundary_point=s["boundary_point"], interior_point=s["interior_point"], obstacle=np.zeros((4, 4, 4)),
+        velocity=(0.0, 0.0, 0.4), nearest_marker=s["nearest_marker"], marker_region=[7])
+    rep = r["report"]
+    assert rep["active_velocity_dirichlet_rows"] == 1 and rep["invalid_reconstruction_row_count"] == 0
+    assert rep["min_projection_weight"] == pytest.approx(0.5, abs=1e-6)
+    assert rep["max_projection_weight"] == pytest.approx(0.5, abs=1e-6)
+    assert r["active"][2, 2, 2] == 1 and r["region"][2, 2, 2] == 7
+    assert r["value"][2, 2, 2][2] == pytest.approx(0.25, abs=1e-6)
+    assert r["weight"][2, 2, 2] == pytest.approx(0.5, abs=1e-6)
+
+
+# test_hibm.py:3411 reconstruction falls back to the nearest marker velocity
+def test_vd_rows_zero_gap_falls_back_to_the_boundary_velocity():
+    node = (2, 2, 2)
+    r = _one_node_rows(node, (0.1, 0.0, 0.0), (1.0, 0.0, 0.0), (0.625,) * 3, (0.625,) * 3)
+    rep = r["report"]
+    assert rep["active_velocity_dirichlet_rows"] == 1 and rep["invalid_reconstruction_row_count"] == 1
+    assert rep["invalid_no_fluid_sample_row_count"] == 0 and rep["invalid_nonpositive_gap_row_count"] == 1
+    assert rep["invalid_node_behind_boundary_row_count"] == 0 and rep["invalid_node_beyond_interior_row_count"] == 0
+    assert rep["min_projection_weight"] == 0.0 and rep["max_projection_weight"] == 0.0
+    assert r["active"][node] == 1 and r["weight"][node] == 0.0
+    np.testing.assert_allclose(r["value"][node], (0.1, 0.0, 0.0), atol=1e-7)
+
+
+# test_hibm.py:3478 a masked node's row relocates to the first fluid cell
+def test_vd_rows_relocate_a_masked_node_to_the_first_fluid_cell():
+    obs = np.zeros((4, 4, 4), np.int32)
+    obs[2, 2, 2] = 1
+    r = _one_node_rows((2, 2, 2), (0.2, 0.0, 0.0), (1.0, 0.0, 0.0), (0.5, 0.625, 0.625), (0.875, 0.625, 0.625),
+                       obstacle=obs)
+    rep = r["report"]
+    assert rep["active_velocity_dirichlet_rows"] == 1 and rep["relocated_row_count"] == 1
+    assert rep["relocation_blocked_row_count"] == 0 and rep["inactive_obstacle_rows"] == 0
+    assert rep["invalid_reconstruction_row_count"] == 0
+    assert r["active"][2, 2, 2] == 0 and r["active"][3, 2, 2] == 1
+    np.testing.assert_allclose(r["value"][3, 2, 2], (0.08, 0.0, 0.0), atol=1e-6)
+    assert r["weight"][3, 2, 2] == pytest.approx(0.6, abs=1e-6)
+
+
+# test_hibm.py:3540 relocation to the opposite fluid side when the normal side is solid
+def test_vd_rows_relocate_to_the_opposite_side():
+    obs = np.zeros((4, 4, 4), np.int32)
+    obs[2:, :, :] = 1
+    r = _one_node_rows((2, 2, 2), (0.2, 0.0, 0.0), (1.0, 0.0, 0.0), (0.5, 0.625, 0.625), (0.875, 0.625, 0.625),
+                       obstacle=obs)
+    rep = r["report"]
+    assert rep["active_velocity_dirichlet_rows"] == 1 and rep["relocated_row_count"] == 1
+    assert rep["relocation_blocked_row_count"] == 0
+    assert r["active"][2, 2, 2] == 0 and r["active"][1, 2, 2] == 1
+    np.testing.assert_allclose(r["value"][1, 2, 2], (0.13333334, 0.0, 0.0), atol=1e-7)
+
+
+# test_hibm.py:3597 a wall-limited gap is a narrow-gap row
+def test_vd_rows_wall_limited_gap_is_a_narrow_gap_row():
+    obs = np.zeros((4, 4, 4), np.int32)
+    obs[3, :, :] = 1
+    node = (2, 2, 2)
+    r = _one_node_rows(node, (0.3, 0.0, 0.0), (1.0, 0.0, 0.0), (0.5, 0.625, 0.625), (0.875, 0.625, 0.625),
+                       obstacle=obs)
+    rep = r["report"]
+    assert rep["active_velocity_dirichlet_rows"] == 1 and rep["narrow_gap_boundary_velocity_row_count"] == 1
+    assert rep["invalid_reconstruction_row_count"] == 0 and rep["invalid_no_fluid_sample_row_count"] == 0
+    assert r["active"][node] == 1 and r["weight"][node] == 0.0
+    np.testing.assert_allclose(r["value"][node], (0.3, 0.0, 0.0), atol=1e-7)
+
+
+# test_hibm.py:3658 fallback for a node beyond the interior segment
+def test_vd_rows_fall_back_for_a_node_beyond_the_interior_segment():
+    node = (2, 2, 2)
+    r = _one_node_rows(node, (0.2, 0.0, 0.0), (1.0, 0.0, 0.0), (0.25, 0.625, 0.625), (0.375, 0.625, 0.625),
+                       velocity=(0.4, 0.0, 0.0))
+    rep = r["report"]
+    assert rep["active_velocity_dirichlet_rows"] == 1 and rep["invalid_reconstruction_row_count"] == 0
+    assert r["weight"][node] > 0.0
+    np.testing.assert_allclose(r["value"][node], (0.35, 0.0, 0.0), atol=1e-6)
+
+
+# test_hibm.py:3718 fallback for a node behind the boundary plane
+def test_vd_rows_fall_back_for_a_node_behind_the_boundary_plane():
+    node = (1, 2, 2)
+    r = _one_node_rows(node, (0.2, 0.0, 0.0), (1.0, 0.0, 0.0), (0.5, 0.625, 0.625), (0.625, 0.625, 0.625),
+                       velocity=(0.4, 0.0, 0.0))
+    rep = r["report"]
+    assert rep["active_velocity_dirichlet_rows"] == 1 and rep["invalid_reconstruction_row_count"] == 0
+    assert r["weight"][node] == pytest.approx(0.5, abs=1e-6)
+    np.testing.assert_allclose(r["value"][node], (0.3, 0.0, 0.0), atol=1e-6)
