@@ -85,6 +85,35 @@ class IbSearchFields(Structure):  # efsi_ib_search_fields
     ]
 
 
+class IbBcReport(Structure):  # efsi_ib_bc_report
+    _fields_ = [("no_slip_dirichlet_count", c_int32), ("pressure_neumann_count", c_int32),
+                ("inactive_internal_node_count", c_int32), ("max_abs_velocity_mps", c_float)]
+
+
+class IbVdParams(Structure):  # efsi_ib_vd_params
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
+        ("face_x_m", c_void_p), ("face_y_m", c_void_p), ("face_z_m", c_void_p),
+        ("center_x_m", c_void_p), ("center_y_m", c_void_p), ("center_z_m", c_void_p),
+        ("active_ib_node", c_void_p), ("target_velocity", c_void_p), ("target_normal", c_void_p),
+        ("boundary_point_m", c_void_p), ("interior_fluid_point_m", c_void_p), ("nearest_marker", c_void_p),
+        ("obstacle", c_void_p), ("velocity", c_void_p), ("marker_region_id", c_void_p), ("marker_count", c_int32),
+    ]
+
+
+class IbVdReport(Structure):  # efsi_ib_vd_report
+    _fields_ = [(name, c_int32) for name in (
+        "active_rows", "blocked_rows", "invalid_rows", "invalid_no_fluid_sample_rows", "invalid_nonpositive_gap_rows",
+        "invalid_node_behind_boundary_rows", "invalid_node_beyond_interior_rows", "narrow_gap_rows",
+        "relocated_rows", "merged_rows")] + [
+        ("max_abs_velocity_mps", c_float), ("min_projection_weight", c_float), ("max_projection_weight", c_float)]
+
+
+class IbVdFields(Structure):  # efsi_ib_vd_fields
+    _fields_ = [("active", c_void_p), ("value_mps", c_void_p), ("projection_weight", c_void_p),
+                ("anchor_cell", c_void_p), ("marker_region_id", c_void_p), ("report", c_void_p)]
+
+
 class MpmState(Structure):
     _fields_ = [
         ("particle_count", c_int32),
@@ -165,6 +194,8 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_ib_search_plan_destroy": [P],
     "efsi_ib_node_search": [P, POINTER(IbSearchParams), POINTER(IbSearchFields), P],
     "efsi_ib_reset_anchor_cells": [P, ctypes.c_int64, P],
+    "efsi_ib_build_boundary_conditions": [ctypes.c_int64, P, P, P, P, P, P, P, I, P, P, P, P, P, P],
+    "efsi_ib_velocity_dirichlet_rows": [P, POINTER(IbVdParams), POINTER(IbVdFields), I, P],
 }
 
 _lib = None

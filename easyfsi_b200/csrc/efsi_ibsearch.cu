@@ -32,6 +32,8 @@ struct efsi_ib_search_plan {
   int64_t entry_cap = 0;
   unsigned long long* total = nullptr;       // entry total (device)
   unsigned long long* host_total = nullptr;  // and its pinned readback
+  int32_t* claim = nullptr;  // per fluid cell: relocation claims, then region writers
+  int64_t claim_cap = 0;
 };
 
 namespace efsi {
@@ -41,6 +43,7 @@ constexpr int kNodeNone = 0, kNodeExternal = 1, kNodeInternal = 2;  // hibm_mpm.
 constexpr int kMaxBinsPerAxis = 128;
 constexpr int64_t kMaxEntries = int64_t(1) << 27;  // beyond this the nodes scan every item
 constexpr int kScanThreads = 1024, kScanPer = 4, kScanTile = kScanThreads * kScanPer;
+constexpr int kRelocationWalkSteps = 24;  // HIBM_OWNER_RELOCATION_WALK_STEPS (hibm_mpm.py:23)
 
 struct F3 {
   float x, y, z;
@@ -55,7 +58,7 @@ __device__ __forceinline__ F3 cross(F3 a, F3 b) {
   return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 __device__ __forceinline__ float norm(F3 a) { return sqrtf(dot(a, a)); }
-__device__ __forceinline__ F3 ld3(const float* p, int i) {
+__device__ __forceinline__ F3 ld3(const float* p, int64_t i) {
   return f3(__ldg(p + 3 * i), __ldg(p + 3 * i + 1), __ldg(p + 3 * i + 2));
 }
 __device__ __forceinline__ void st3(float* p, int64_t i, F3 v) {
@@ -480,6 +483,439 @@ __global__ void k_ibs_fill_anchor(int32_t* anchor, int64_t n3) {
   if (q < n3) anchor[q] = -1;
 }
 
+// ---------------------------------------------------------------------------
+// Boundary-condition targets (hibm_mpm.py:6499-6577)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float max_abs3(F3 v) { return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fabsf(v.z)); }
+
+// atomic max / min of non-negative floats through their ordered bit patterns
+__device__ __forceinline__ void atomic_max_nonneg(float* a, float v) { atomicMax((int*)a, __float_as_int(v)); }
+__device__ __forceinline__ void atomic_min_nonneg(float* a, float v) { atomicMin((int*)a, __float_as_int(v)); }
+
+__global__ void __launch_bounds__(256) k_ib_build_bc(int64_t n, const int32_t* __restrict__ kind,
+                                                     const int32_t* __restrict__ nearest,
+                                                     const int32_t* __restrict__ pidx, const float* __restrict__ pw,
+                                                     const float* __restrict__ mv, const float* __restrict__ mn,
+                                                     const float* __restrict__ mg, int marker_count,
+                                                     int32_t* __restrict__ active, float* __restrict__ vel,
+                                                     float* __restrict__ nrm, float* __restrict__ grad,
+                                                     efsi_ib_bc_report* rep) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  int act = 0;
+  F3 tv = f3(0.0f, 0.0f, 0.0f), tn = f3(0.0f, 0.0f, 0.0f);
+  float tg = 0.0f;
+  const int k = kind[c];
+  if (k == kNodeExternal) {
+    const int marker = nearest[c];
+    if (0 <= marker && marker < marker_count) {
+      float total = 0.0f;
+      for (int q = 0; q < 3; ++q) {
+        const int pm = pidx[3 * c + q];
+        const float w = pw[3 * c + q];
+        if (0 <= pm && pm < marker_count && w > 0.0f) {
+          tv = add(tv, scale(ld3(mv, pm), w));
+          tn = add(tn, scale(ld3(mn, pm), w));
+          tg = tg + w * __ldg(mg + pm);
+          total = total + w;
+        }
+      }
+      if (total > 1.0e-12f) {
+        const float inv = 1.0f / total;
+        tv = scale(tv, inv);
+        tn = scale(tn, inv);
+        tg = tg * inv;
+        const float nn = norm(tn);
+        tn = nn > 1.0e-12f ? divide(tn, nn) : ld3(mn, marker);
+      } else {
+        tv = ld3(mv, marker);
+        tn = ld3(mn, marker);
+        tg = __ldg(mg + marker);
+      }
+      act = 1;
+      atomicAdd(&rep->no_slip_dirichlet_count, 1);
+      atomicAdd(&rep->pressure_neumann_count, 1);
+      atomic_max_nonneg(&rep->max_abs_velocity_mps, max_abs3(tv));
+    }
+  } else if (k == kNodeInternal) {
+    atomicAdd(&rep->inactive_internal_node_count, 1);
+  }
+  active[c] = act;
+  st3(vel, c, tv);
+  st3(nrm, c, tn);
+  grad[c] = tg;
+}
+
+// ---------------------------------------------------------------------------
+// Velocity-Dirichlet rows (hibm_mpm.py:6649-7800)
+// ---------------------------------------------------------------------------
+struct VdArgs {
+  int n[3];
+  int64_t ncell;
+  const float* f[3];  // faces, n + 1
+  const float* c[3];  // centres
+  const int32_t* act;
+  const float* bv;
+  const float* bn;
+  const float* bp;
+  const float* ip;
+  const int32_t* nearest;
+  const int32_t* obs;
+  const float* vel;
+  const int32_t* mreg;
+  int mcount;
+  int32_t* vd_active;
+  float* vd_value;
+  float* vd_weight;
+  int32_t* anchor;
+  int32_t* region;
+  efsi_ib_vd_report* rep;
+  int32_t* claim;
+};
+
+__device__ __forceinline__ int64_t vidx(const VdArgs& A, int i, int j, int k) {
+  return ((int64_t)i * A.n[1] + j) * A.n[2] + k;
+}
+
+// hibm_mpm.py:6714-6743
+__device__ float axis_coordinate(float value, const float* faces, const float* centers, int count) {
+  if (value <= centers[0]) {
+    const float half = fmaxf(centers[0] - faces[0], 1.0e-18f);
+    return -0.5f * (centers[0] - value) / half;
+  }
+  if (value >= centers[count - 1]) {
+    const float half = fmaxf(faces[count] - centers[count - 1], 1.0e-18f);
+    return (float)(count - 1) + 0.5f * (value - centers[count - 1]) / half;
+  }
+  int lower = 0, upper = count - 1;
+  while (upper - lower > 1) {
+    const int middle = (lower + upper) / 2;
+    if (value >= centers[middle])
+      lower = middle;
+    else
+      upper = middle;
+  }
+  upper = min(lower + 1, count - 1);
+  const float distance = fmaxf(centers[upper] - centers[lower], 1.0e-18f);
+  return (float)lower + (value - centers[lower]) / distance;
+}
+
+__device__ __forceinline__ F3 grid_coordinate(const VdArgs& A, F3 p) {
+  return f3(axis_coordinate(p.x, A.f[0], A.c[0], A.n[0]), axis_coordinate(p.y, A.f[1], A.c[1], A.n[1]),
+            axis_coordinate(p.z, A.f[2], A.c[2], A.n[2]));
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+__device__ __forceinline__ void nearest_cell(const VdArgs& A, F3 g, int& i, int& j, int& k) {
+  i = clampi((int)floorf(g.x + 0.5f), 0, A.n[0] - 1);
+  j = clampi((int)floorf(g.y + 0.5f), 0, A.n[1] - 1);
+  k = clampi((int)floorf(g.z + 0.5f), 0, A.n[2] - 1);
+}
+
+// hibm_mpm.py:6782-6812
+__device__ F3 sample_velocity(const VdArgs& A, F3 g, float& fluid_weight) {
+  const int i0 = clampi((int)floorf(g.x), 0, A.n[0] - 2);
+  const int j0 = clampi((int)floorf(g.y), 0, A.n[1] - 2);
+  const int k0 = clampi((int)floorf(g.z), 0, A.n[2] - 2);
+  const float tx = fminf(fmaxf(g.x - (float)i0, 0.0f), 1.0f);
+  const float ty = fminf(fmaxf(g.y - (float)j0, 0.0f), 1.0f);
+  const float tz = fminf(fmaxf(g.z - (float)k0, 0.0f), 1.0f);
+  F3 value = f3(0.0f, 0.0f, 0.0f);
+  fluid_weight = 0.0f;
+  for (int oi = 0; oi < 2; ++oi)
+    for (int oj = 0; oj < 2; ++oj)
+      for (int ok = 0; ok < 2; ++ok) {
+        const float wx = oi == 0 ? 1.0f - tx : tx, wy = oj == 0 ? 1.0f - ty : ty, wz = ok == 0 ? 1.0f - tz : tz;
+        const float w = wx * wy * wz;
+        const int64_t c = vidx(A, i0 + oi, j0 + oj, k0 + ok);
+        if (__ldg(A.obs + c) == 0) {
+          value = add(value, scale(ld3(A.vel, c), w));
+          fluid_weight = fluid_weight + w;
+        }
+      }
+  if (fluid_weight > 1.0e-12f) value = divide(value, fluid_weight);
+  return value;
+}
+
+// hibm_mpm.py:6846-6902
+__device__ F3 walk_sample(const VdArgs& A, F3 bp, F3 normal, float base, float step, float& weight, float& distance) {
+  weight = 0.0f;
+  distance = base;
+  for (int s = 0; s < 5; ++s) {
+    const float cd = base + step * (float)s;
+    float w;
+    const F3 v = sample_velocity(A, grid_coordinate(A, add(bp, scale(normal, cd))), w);
+    if (w > 1.0e-12f) {
+      weight = w;
+      distance = cd;
+      return v;
+    }
+  }
+  return f3(0.0f, 0.0f, 0.0f);
+}
+
+__device__ __forceinline__ float walk_step(F3 n, float wx, float wy, float wz) {
+  const float s = fabsf(n.x) / fmaxf(wx, 1.0e-12f) + fabsf(n.y) / fmaxf(wy, 1.0e-12f) + fabsf(n.z) / fmaxf(wz, 1.0e-12f);
+  return 0.5f / fmaxf(s, 1.0e-12f);
+}
+
+__device__ __forceinline__ void decode(const VdArgs& A, int64_t c, int& i, int& j, int& k) {
+  k = (int)(c % A.n[2]);
+  j = (int)((c / A.n[2]) % A.n[1]);
+  i = (int)(c / ((int64_t)A.n[1] * A.n[2]));
+}
+
+__device__ __forceinline__ void report_row(const VdArgs& A, float alpha, F3 v, bool max_weight) {
+  atomicAdd(&A.rep->active_rows, 1);
+  atomic_min_nonneg(&A.rep->min_projection_weight, alpha);
+  if (max_weight) atomic_max_nonneg(&A.rep->max_projection_weight, alpha);
+  atomic_max_nonneg(&A.rep->max_abs_velocity_mps, max_abs3(v));
+}
+
+__global__ void k_vd_report_init(efsi_ib_vd_report* rep) {
+  efsi_ib_vd_report r{};
+  r.min_projection_weight = 1.0e30f;
+  *rep = r;
+}
+
+__global__ void k_vd_fill(int32_t* a, int64_t n, int32_t v) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) a[q] = v;
+}
+
+// anchor reset and prefill from the interior probe point (hibm_mpm.py:7551-7616)
+__global__ void __launch_bounds__(256) k_vd_prefill(VdArgs A) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.ncell) return;
+  int ai = -1, aj = -1, ak = -1;
+  if (A.act[c] == 1) {
+    int i, j, k;
+    nearest_cell(A, grid_coordinate(A, ld3(A.ip, c)), i, j, k);
+    if (__ldg(A.obs + vidx(A, i, j, k)) == 0) ai = i, aj = j, ak = k;
+  }
+  A.anchor[3 * c] = ai;
+  A.anchor[3 * c + 1] = aj;
+  A.anchor[3 * c + 2] = ak;
+}
+
+// row reconstruction (hibm_mpm.py:6904-7335)
+__global__ void __launch_bounds__(256) k_vd_reconstruct(VdArgs A) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.ncell) return;
+  int act = 0;
+  F3 value = f3(0.0f, 0.0f, 0.0f);
+  float weight = 0.0f;
+  if (A.act[c] == 1 && __ldg(A.obs + c) == 0) {
+    int i, j, k;
+    decode(A, c, i, j, k);
+    const F3 bv = ld3(A.bv, c), normal = ld3(A.bn, c), bp = ld3(A.bp, c), ip = ld3(A.ip, c);
+    const F3 node = f3(__ldg(A.c[0] + i), __ldg(A.c[1] + j), __ldg(A.c[2] + k));
+    const float normal_den = dot(sub(ip, bp), normal);
+    const float normal_dist = dot(sub(node, bp), normal);
+    const float wx = __ldg(A.f[0] + i + 1) - __ldg(A.f[0] + i);
+    const float wy = __ldg(A.f[1] + j + 1) - __ldg(A.f[1] + j);
+    const float wz = __ldg(A.f[2] + k + 1) - __ldg(A.f[2] + k);
+    float fw, sample_den;
+    const F3 iv = walk_sample(A, bp, normal, normal_den, walk_step(normal, wx, wy, wz), fw, sample_den);
+    F3 fb_vel = iv;
+    float fb_alpha = 0.0f;
+    int fai = -1, faj = -1, fak = -1;
+    const bool segment = fw > 1.0e-12f && sample_den > 1.0e-12f && normal_dist >= 0.0f && normal_dist <= sample_den;
+    bool fallback = false;
+    if (!segment && fw > 1.0e-12f && sample_den > 1.0e-12f && normal_den > 1.0e-12f) {
+      const F3 off = sub(node, bp);
+      const float line = sqrtf(fmaxf(dot(off, off), 0.0f));
+      if (line > 1.0e-12f) {
+        const F3 fn = divide(off, line);
+        const float fstep = walk_step(fn, wx, wy, wz);
+        float fbw, fb_den;
+        fb_vel = walk_sample(A, bp, fn, line + fstep, fstep, fbw, fb_den);
+        if (fbw > 1.0e-12f && fb_den > line + 1.0e-12f) {
+          fb_alpha = fminf(fmaxf(line / fmaxf(fb_den, 1.0e-12f), 0.0f), 1.0f);
+          nearest_cell(A, grid_coordinate(A, add(bp, scale(fn, fb_den))), fai, faj, fak);
+          fallback = __ldg(A.obs + vidx(A, fai, faj, fak)) == 0;
+        }
+      }
+    }
+    act = 1;
+    if (segment) {
+      const float alpha = fminf(fmaxf(normal_dist / sample_den, 0.0f), 1.0f);
+      value = add(bv, scale(sub(iv, bv), alpha));
+      weight = alpha;
+      int ai, aj, ak;
+      nearest_cell(A, grid_coordinate(A, add(bp, scale(normal, sample_den))), ai, aj, ak);
+      if (__ldg(A.obs + vidx(A, ai, aj, ak)) == 0) {
+        A.anchor[3 * c] = ai;
+        A.anchor[3 * c + 1] = aj;
+        A.anchor[3 * c + 2] = ak;
+      }
+      report_row(A, alpha, value, true);
+    } else if (fallback) {
+      value = add(bv, scale(sub(fb_vel, bv), fb_alpha));
+      weight = fb_alpha;
+      A.anchor[3 * c] = fai;
+      A.anchor[3 * c + 1] = faj;
+      A.anchor[3 * c + 2] = fak;
+      report_row(A, fb_alpha, value, true);
+    } else {
+      value = bv;
+      if (fw <= 1.0e-12f && normal_den > 1.0e-12f && normal_dist >= 0.0f) {
+        atomicAdd(&A.rep->narrow_gap_rows, 1);
+      } else {
+        atomicAdd(&A.rep->invalid_rows, 1);
+        if (fw <= 1.0e-12f)
+          atomicAdd(&A.rep->invalid_no_fluid_sample_rows, 1);
+        else if (normal_den <= 1.0e-12f)
+          atomicAdd(&A.rep->invalid_nonpositive_gap_rows, 1);
+        else if (normal_dist < 0.0f)
+          atomicAdd(&A.rep->invalid_node_behind_boundary_rows, 1);
+        else if (normal_dist > normal_den)
+          atomicAdd(&A.rep->invalid_node_beyond_interior_rows, 1);
+      }
+      report_row(A, 0.0f, bv, false);
+    }
+  }
+  A.vd_active[c] = act;
+  st3(A.vd_value, c, value);
+  A.vd_weight[c] = weight;
+}
+
+// The first fluid cell along the walk from a masked node's boundary point
+// (its own side first, then the other; hibm_mpm.py:7359-7438); false if none.
+__device__ bool relocation_target(const VdArgs& A, int64_t c, int& ti, int& tj, int& tk, float& tdist, F3& twn,
+                                  float& tstep) {
+  int i, j, k;
+  decode(A, c, i, j, k);
+  const F3 normal = ld3(A.bn, c), bp = ld3(A.bp, c);
+  const F3 node = f3(__ldg(A.c[0] + i), __ldg(A.c[1] + j), __ldg(A.c[2] + k));
+  const float side = dot(sub(node, bp), normal);
+  const F3 primary = side < 0.0f ? f3(-normal.x, -normal.y, -normal.z) : normal;
+  const float node_dist = fabsf(side);
+  const float wx = __ldg(A.f[0] + i + 1) - __ldg(A.f[0] + i);
+  const float wy = __ldg(A.f[1] + j + 1) - __ldg(A.f[1] + j);
+  const float wz = __ldg(A.f[2] + k + 1) - __ldg(A.f[2] + k);
+  for (int s = 0; s < 2; ++s) {
+    const F3 wn = s == 0 ? primary : f3(-primary.x, -primary.y, -primary.z);
+    const float start = s == 0 ? node_dist : 0.0f;
+    const float step = walk_step(wn, wx, wy, wz);
+    for (int q = 0; q < kRelocationWalkSteps; ++q) {
+      const float cd = start + step * (float)(q + 1);
+      int ci, cj, ck;
+      nearest_cell(A, grid_coordinate(A, add(bp, scale(wn, cd))), ci, cj, ck);
+      if (__ldg(A.obs + vidx(A, ci, cj, ck)) != 0) continue;
+      const float ccd = dot(sub(f3(__ldg(A.c[0] + ci), __ldg(A.c[1] + cj), __ldg(A.c[2] + ck)), bp), wn);
+      if (ccd > 1.0e-12f) {
+        ti = ci;
+        tj = cj;
+        tk = ck;
+        tdist = ccd;
+        twn = wn;
+        tstep = step;
+        return true;
+      }
+    }
+  }
+  return false;
+}
+
+// Relocation, pass 1: every masked node claims its target cell unless a row
+// sits there already; the lowest node index wins, as the first claim of the
+// nodes visited in order.
+__global__ void __launch_bounds__(256) k_vd_relocate_claim(VdArgs A) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.ncell || !(A.act[c] == 1 && __ldg(A.obs + c) != 0)) return;
+  int ti, tj, tk;
+  float tdist, tstep;
+  F3 twn;
+  if (!relocation_target(A, c, ti, tj, tk, tdist, twn, tstep)) return;
+  const int64_t t = vidx(A, ti, tj, tk);
+  if (A.vd_active[t] == 0) atomicMin(A.claim + t, (int32_t)c);
+}
+
+// Relocation, pass 2 (hibm_mpm.py:7439-7549): the winner writes the row.
+__global__ void __launch_bounds__(256) k_vd_relocate_apply(VdArgs A) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.ncell || !(A.act[c] == 1 && __ldg(A.obs + c) != 0)) return;
+  int ti, tj, tk;
+  float tdist, tstep;
+  F3 twn;
+  if (!relocation_target(A, c, ti, tj, tk, tdist, twn, tstep)) {
+    atomicAdd(&A.rep->blocked_rows, 1);
+    return;
+  }
+  const int64_t t = vidx(A, ti, tj, tk);
+  if (A.claim[t] != (int32_t)c) {
+    atomicAdd(&A.rep->merged_rows, 1);
+    return;
+  }
+  const F3 bp = ld3(A.bp, c), bv = ld3(A.bv, c);
+  float sw, sd;
+  const F3 sv = walk_sample(A, bp, twn, tdist + 2.0f * tstep, tstep, sw, sd);
+  F3 tv = bv;
+  float alpha = 0.0f;
+  if (sw > 1.0e-12f && sd > tdist) {
+    alpha = fminf(fmaxf(tdist / sd, 0.0f), 1.0f);
+    tv = add(bv, scale(sub(sv, bv), alpha));
+  }
+  A.vd_active[t] = 1;
+  st3(A.vd_value, t, tv);
+  A.vd_weight[t] = alpha;
+  A.anchor[3 * c] = ti;
+  A.anchor[3 * c + 1] = tj;
+  A.anchor[3 * c + 2] = tk;
+  atomicAdd(&A.rep->relocated_rows, 1);
+  report_row(A, alpha, tv, true);
+}
+
+// Region stamp (hibm_mpm.py:7618-7653): a cell written by several nodes
+// keeps the region of the highest node index, as the last write of the nodes
+// visited in order.  pass 0: record writers, pass 1: the writers write.
+__device__ __forceinline__ bool stamp_anchor(const VdArgs& A, int64_t c, int64_t& a) {
+  const int ai = A.anchor[3 * c], aj = A.anchor[3 * c + 1], ak = A.anchor[3 * c + 2];
+  if (!(ai >= 0 && ai < A.n[0] && aj >= 0 && aj < A.n[1] && ak >= 0 && ak < A.n[2])) return false;
+  a = vidx(A, ai, aj, ak);
+  return A.vd_active[a] != 0;
+}
+
+__global__ void __launch_bounds__(256) k_vd_stamp(VdArgs A, int pass) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.ncell || A.act[c] != 1) return;
+  const int marker = A.nearest[c];
+  if (marker < 0 || marker >= A.mcount) return;
+  const int32_t region = __ldg(A.mreg + marker);
+  int64_t a;
+  const bool own = A.vd_active[c] != 0, anc = stamp_anchor(A, c, a);
+  if (pass == 0) {
+    if (own) atomicMax(A.claim + c, (int32_t)c);
+    if (anc) atomicMax(A.claim + a, (int32_t)c);
+  } else {
+    if (own && A.claim[c] == (int32_t)c) A.region[c] = region;
+    if (anc && A.claim[a] == (int32_t)c) A.region[a] = region;
+  }
+}
+
+// hibm_mpm.py:6649-6688 _assemble_velocity_dirichlet_boundary_rows_kernel:
+// the target velocity itself on every active IB node that is not masked.
+__global__ void __launch_bounds__(256) k_vd_direct(VdArgs A) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.ncell) return;
+  int act = 0;
+  F3 value = f3(0.0f, 0.0f, 0.0f);
+  if (A.act[c] == 1) {
+    if (__ldg(A.obs + c) == 0) {
+      act = 1;
+      value = ld3(A.bv, c);
+      atomicAdd(&A.rep->active_rows, 1);
+      atomic_max_nonneg(&A.rep->max_abs_velocity_mps, max_abs3(value));
+    } else {
+      atomicAdd(&A.rep->blocked_rows, 1);
+    }
+  }
+  A.vd_active[c] = act;
+  st3(A.vd_value, c, value);
+}
+
 template <typename T>
 int grow(T*& buf, int64_t& cap, int64_t need) {
   if (need <= cap) return EFSI_OK;
@@ -519,6 +955,7 @@ int efsi_ib_search_plan_destroy(efsi_ib_search_plan* P) {
   cudaFree(P->cursor);
   cudaFree(P->tile_sums);
   cudaFree(P->entries);
+  cudaFree(P->claim);
   cudaFree(P->total);
   cudaFreeHost(P->host_total);
   delete P;
@@ -649,6 +1086,93 @@ int efsi_ib_node_search(efsi_ib_search_plan* P, const efsi_ib_search_params* prm
     }
   }
   EFSI_COUNTED k_ibs_search<<<(unsigned)((A.n + 255) / 256), 256, 0, s>>>(A);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_ib_build_boundary_conditions(int64_t node_count, const int32_t* node_kind, const int32_t* nearest_marker,
+                                      const int32_t* projection_marker_indices,
+                                      const float* projection_marker_weights, const float* marker_velocity,
+                                      const float* marker_normal, const float* marker_gradient, int32_t marker_count,
+                                      int32_t* active, float* velocity, float* normal, float* gradient,
+                                      efsi_ib_bc_report* report_device, void* stream) {
+  EFSI_ARG_CHECK(node_count >= 0 && marker_count >= 0, "negative node or marker count");
+  EFSI_ARG_CHECK(node_kind && nearest_marker && projection_marker_indices && projection_marker_weights && active &&
+                     velocity && normal && gradient && report_device,
+                 "null argument");
+  EFSI_ARG_CHECK(marker_count == 0 || (marker_velocity && marker_normal && marker_gradient), "marker arrays missing");
+  cudaStream_t s = as_stream(stream);
+  EFSI_CUDA_CHECK(cudaMemsetAsync(report_device, 0, sizeof(efsi_ib_bc_report), s));
+  if (node_count == 0) return EFSI_OK;
+  EFSI_COUNTED k_ib_build_bc<<<(unsigned)((node_count + 255) / 256), 256, 0, s>>>(
+      node_count, node_kind, nearest_marker, projection_marker_indices, projection_marker_weights, marker_velocity,
+      marker_normal, marker_gradient, marker_count, active, velocity, normal, gradient, report_device);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_ib_velocity_dirichlet_rows(efsi_ib_search_plan* P, const efsi_ib_vd_params* prm,
+                                    const efsi_ib_vd_fields* out, int32_t reconstruct, void* stream) {
+  EFSI_ARG_CHECK(P != nullptr && prm != nullptr && out != nullptr, "null argument");
+  EFSI_ARG_CHECK(prm->nx >= 2 && prm->ny >= 2 && prm->nz >= 2, "grid_nodes must contain three values >= 2");
+  EFSI_ARG_CHECK(prm->active_ib_node && prm->target_velocity && prm->obstacle && out->active && out->value_mps &&
+                     out->report,
+                 "null argument");
+  if (reconstruct) {
+    EFSI_ARG_CHECK(prm->face_x_m && prm->face_y_m && prm->face_z_m && prm->center_x_m && prm->center_y_m &&
+                       prm->center_z_m && prm->target_normal && prm->boundary_point_m &&
+                       prm->interior_fluid_point_m && prm->velocity && out->projection_weight && out->anchor_cell,
+                   "reconstructed rows need the grid axes, targets, node points, velocity and anchor fields");
+    EFSI_ARG_CHECK(prm->marker_region_id == nullptr || (out->marker_region_id && prm->nearest_marker),
+                   "the region stamp needs the nearest markers and the region output");
+  }
+  cudaStream_t s = as_stream(stream);
+  VdArgs A{};
+  A.n[0] = prm->nx;
+  A.n[1] = prm->ny;
+  A.n[2] = prm->nz;
+  A.ncell = (int64_t)prm->nx * prm->ny * prm->nz;
+  A.f[0] = prm->face_x_m;
+  A.f[1] = prm->face_y_m;
+  A.f[2] = prm->face_z_m;
+  A.c[0] = prm->center_x_m;
+  A.c[1] = prm->center_y_m;
+  A.c[2] = prm->center_z_m;
+  A.act = prm->active_ib_node;
+  A.bv = prm->target_velocity;
+  A.bn = prm->target_normal;
+  A.bp = prm->boundary_point_m;
+  A.ip = prm->interior_fluid_point_m;
+  A.nearest = prm->nearest_marker;
+  A.obs = prm->obstacle;
+  A.vel = prm->velocity;
+  A.mreg = prm->marker_region_id;
+  A.mcount = prm->marker_count;
+  A.vd_active = out->active;
+  A.vd_value = out->value_mps;
+  A.vd_weight = out->projection_weight;
+  A.anchor = out->anchor_cell;
+  A.region = out->marker_region_id;
+  A.rep = out->report;
+  const unsigned grid = (unsigned)((A.ncell + 255) / 256);
+  EFSI_COUNTED k_vd_report_init<<<1, 1, 0, s>>>(out->report);
+  if (!reconstruct) {
+    EFSI_COUNTED k_vd_direct<<<grid, 256, 0, s>>>(A);
+    EFSI_LAUNCH_CHECK();
+    return EFSI_OK;
+  }
+  EFSI_TRY(grow(P->claim, P->claim_cap, A.ncell));
+  A.claim = P->claim;
+  EFSI_COUNTED k_vd_prefill<<<grid, 256, 0, s>>>(A);
+  EFSI_COUNTED k_vd_reconstruct<<<grid, 256, 0, s>>>(A);
+  EFSI_COUNTED k_vd_fill<<<grid, 256, 0, s>>>(A.claim, A.ncell, INT32_MAX);
+  EFSI_COUNTED k_vd_relocate_claim<<<grid, 256, 0, s>>>(A);
+  EFSI_COUNTED k_vd_relocate_apply<<<grid, 256, 0, s>>>(A);
+  if (A.mreg != nullptr) {
+    EFSI_COUNTED k_vd_fill<<<grid, 256, 0, s>>>(A.claim, A.ncell, -1);
+    EFSI_COUNTED k_vd_stamp<<<grid, 256, 0, s>>>(A, 0);
+    EFSI_COUNTED k_vd_stamp<<<grid, 256, 0, s>>>(A, 1);
+  }
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }

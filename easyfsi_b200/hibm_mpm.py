@@ -717,3 +717,232 @@ class HibmMpmIbNodeSearch:
         if len(index) != 3 or any(v < 0 or v >= n for v, n in zip(index, self.grid_nodes)):
             raise IndexError("node_index out of range")
         return index
+
+
+@dataclass(frozen=True)
+class HibmMpmIbBoundaryConditionReport:
+    no_slip_dirichlet_count: int
+    pressure_neumann_count: int
+    inactive_internal_node_count: int
+    max_abs_velocity_mps: float = 0.0
+
+
+@dataclass(frozen=True)
+class HibmMpmVelocityDirichletBoundaryReport:
+    active_velocity_dirichlet_rows: int
+    inactive_obstacle_rows: int
+    max_abs_velocity_mps: float
+    invalid_reconstruction_row_count: int = 0
+    invalid_no_fluid_sample_row_count: int = 0
+    invalid_nonpositive_gap_row_count: int = 0
+    invalid_node_behind_boundary_row_count: int = 0
+    invalid_node_beyond_interior_row_count: int = 0
+    narrow_gap_boundary_velocity_row_count: int = 0
+    relocated_row_count: int = 0
+    relocation_merged_row_count: int = 0
+    relocation_blocked_row_count: int = 0
+    min_projection_weight: float = 0.0
+    max_projection_weight: float = 0.0
+
+
+class HibmMpmIbBoundaryConditions:
+    """External-IB boundary conditions from the node search (drop-in for
+    simulation_core/hibm_mpm.py:6222 HibmMpmIbBoundaryConditions, the
+    build-from-search and velocity-Dirichlet row members).
+
+    ``build_from_search`` interpolates each external IB node's no-slip
+    velocity, Neumann normal and Neumann gradient from its projection markers
+    (``efsi_ib_build_boundary_conditions``); the two row assemblies write the
+    fluid's velocity-Dirichlet row fields (``efsi_ib_velocity_dirichlet_rows``):
+    the target velocity itself, or the reconstruction along the surface normal
+    with its fallbacks and the relocation of rows whose node is masked.  The
+    pressure-Neumann row assembly of the reference class is not provided.
+    """
+
+    _NODE_EXTERNAL_IB = HibmMpmIbNodeSearch._NODE_EXTERNAL_IB
+    _NODE_INTERNAL = HibmMpmIbNodeSearch._NODE_INTERNAL
+
+    def __init__(self, *, grid_nodes, marker_capacity: int, runtime: TaichiRuntimeConfig | None = None) -> None:
+        self.device = init_runtime(runtime)
+        nodes = tuple(int(v) for v in grid_nodes)
+        if len(nodes) != 3 or any(v <= 0 for v in nodes):
+            raise ValueError("grid_nodes must contain three positive integers")
+        if int(marker_capacity) <= 0:
+            raise ValueError("marker_capacity must be positive")
+        self.grid_nodes = nodes
+        self.marker_capacity = int(marker_capacity)
+        dev = self.device
+        self.active_ib_node = Field(nodes, i32, device=dev)
+        self.velocity_dirichlet_mps_field = Field(nodes, f32, n=3, device=dev)
+        self.pressure_neumann_normal_field = Field(nodes, f32, n=3, device=dev)
+        self.pressure_neumann_gradient_field = Field(nodes, f32, device=dev)
+        self.marker_pressure_neumann_gradient_field = Field((self.marker_capacity,), f32, device=dev)
+        self._bc_report = torch.zeros(4, dtype=torch.int32, device=dev)
+        self._vd_report = torch.zeros(13, dtype=torch.int32, device=dev)
+        handle = c_void_p()
+        _native.call("efsi_ib_search_plan_create", byref(handle))
+        self._plan = handle
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None:
+            try:
+                _native.load().efsi_ib_search_plan_destroy(plan)
+            except Exception:
+                pass
+
+    def _validate_search_and_markers(self, search, markers) -> None:
+        """hibm_mpm.py:6636-6647."""
+        if tuple(search.grid_nodes) != self.grid_nodes:
+            raise ValueError("search.grid_nodes must match boundary grid_nodes")
+        if int(markers.marker_count) > self.marker_capacity:
+            raise ValueError("markers.marker_count exceeds marker_capacity")
+        if int(search.marker_capacity) > self.marker_capacity:
+            raise ValueError("search.marker_capacity exceeds marker_capacity")
+
+    def build_from_search(self, search, markers, *,
+                          marker_pressure_neumann_gradient_pa_per_m) -> HibmMpmIbBoundaryConditionReport:
+        """hibm_mpm.py:6579-6605."""
+        self._validate_search_and_markers(search, markers)
+        if len(marker_pressure_neumann_gradient_pa_per_m) != markers.marker_count:
+            raise ValueError("marker_pressure_neumann_gradient_pa_per_m must match marker_count")
+        grad = np.zeros(self.marker_capacity, dtype=np.float32)
+        for m, g in enumerate(marker_pressure_neumann_gradient_pa_per_m):
+            v = float(g)
+            if not math.isfinite(v):
+                raise ValueError("marker_pressure_neumann_gradient_pa_per_m must be finite")
+            grad[m] = v
+        self.marker_pressure_neumann_gradient_field.from_numpy(grad)
+        return self.build_from_search_device_fields(
+            search, markers, marker_pressure_neumann_gradient_pa_per_m_field=self.marker_pressure_neumann_gradient_field)
+
+    def build_from_search_device_fields(self, search, markers, *,
+                                        marker_pressure_neumann_gradient_pa_per_m_field
+                                        ) -> HibmMpmIbBoundaryConditionReport:
+        """hibm_mpm.py:6607-6634 over the search's fields."""
+        self._validate_search_and_markers(search, markers)
+        grad = _tensor(marker_pressure_neumann_gradient_pa_per_m_field)
+        _native.call(
+            "efsi_ib_build_boundary_conditions", int(np.prod(self.grid_nodes)), search.node_kind_code.ptr(),
+            search.nearest_marker.ptr(), search.node_projection_marker_indices.ptr(),
+            search.node_projection_marker_weights.ptr(), markers.v_gamma_mps.ptr(), markers.n_gamma.ptr(),
+            grad.data_ptr(), int(markers.marker_count), self.active_ib_node.ptr(),
+            self.velocity_dirichlet_mps_field.ptr(), self.pressure_neumann_normal_field.ptr(),
+            self.pressure_neumann_gradient_field.ptr(), self._bc_report.data_ptr(), current_stream_handle())
+        rep = self._bc_report.cpu()
+        return HibmMpmIbBoundaryConditionReport(int(rep[0]), int(rep[1]), int(rep[2]),
+                                                float(rep[3:4].view(torch.float32)[0]))
+
+    def _vd_call(self, prm, fields, reconstruct: int, written) -> torch.Tensor:
+        _native.call("efsi_ib_velocity_dirichlet_rows", self._plan, byref(prm), byref(fields), reconstruct,
+                     current_stream_handle())
+        # the kernels write through raw pointers: bump the fields' versions so
+        # the fluid rebuilds its stencil masks from the new rows
+        for field in written:
+            _tensor(field).add_(0)
+        return self._vd_report.cpu()
+
+    def assemble_velocity_dirichlet_boundary_rows(self, velocity_dirichlet_active, velocity_dirichlet_value_mps,
+                                                  obstacle_field) -> HibmMpmVelocityDirichletBoundaryReport:
+        """hibm_mpm.py:6690-6712: the target velocity on every unmasked active IB node."""
+        prm = _native.IbVdParams()
+        prm.nx, prm.ny, prm.nz = self.grid_nodes
+        prm.active_ib_node = self.active_ib_node.ptr()
+        prm.target_velocity = self.velocity_dirichlet_mps_field.ptr()
+        prm.obstacle = _tensor(obstacle_field).data_ptr()
+        out = _native.IbVdFields()
+        out.active = _tensor(velocity_dirichlet_active).data_ptr()
+        out.value_mps = _tensor(velocity_dirichlet_value_mps).data_ptr()
+        out.report = self._vd_report.data_ptr()
+        rep = self._vd_call(prm, out, 0, (velocity_dirichlet_active, velocity_dirichlet_value_mps))
+        return HibmMpmVelocityDirichletBoundaryReport(int(rep[0]), int(rep[1]), float(rep[10:11].view(torch.float32)[0]))
+
+    def assemble_velocity_dirichlet_reconstructed_boundary_rows(
+        self, velocity_dirichlet_active, velocity_dirichlet_value_mps, velocity_dirichlet_projection_weight,
+        obstacle_field, velocity_field, search, *, cell_face_x_m, cell_face_y_m, cell_face_z_m, cell_center_x_m,
+        cell_center_y_m, cell_center_z_m, grid_nodes, velocity_dirichlet_marker_region_id=None, marker_region_id=None,
+    ) -> HibmMpmVelocityDirichletBoundaryReport:
+        """hibm_mpm.py:7655-7800: anchor prefill, row reconstruction along the
+        surface normal (with the line-of-sight fallback, narrow-gap and invalid
+        rows), relocation of rows whose node is masked, and the region stamp
+        when both region fields are given."""
+        if tuple(search.grid_nodes) != self.grid_nodes:
+            raise ValueError("search.grid_nodes must match boundary grid_nodes")
+        nodes = tuple(int(v) for v in grid_nodes)
+        if len(nodes) != 3 or any(v < 2 for v in nodes):
+            raise ValueError("grid_nodes must contain three values >= 2")
+        if nodes != self.grid_nodes:
+            raise ValueError("grid_nodes must match boundary grid_nodes")
+        if (velocity_dirichlet_marker_region_id is None) != (marker_region_id is None):
+            raise ValueError("velocity_dirichlet_marker_region_id and marker_region_id must be provided together")
+        region_out = None
+        if velocity_dirichlet_marker_region_id is not None:
+            region_out = _tensor(velocity_dirichlet_marker_region_id)
+            if tuple(region_out.shape) != tuple(_tensor(velocity_dirichlet_active).shape):
+                raise ValueError("velocity_dirichlet_marker_region_id shape must match velocity_dirichlet_active")
+        keep = []
+
+        def f32_ptr(field, count):
+            t = _tensor(field).to(device=self.device, dtype=torch.float32).contiguous()
+            if t.numel() < count:
+                raise ValueError("grid axis fields must cover grid_nodes")
+            keep.append(t)
+            return t.data_ptr()
+
+        prm = _native.IbVdParams()
+        prm.nx, prm.ny, prm.nz = nodes
+        prm.face_x_m, prm.face_y_m, prm.face_z_m = (f32_ptr(f, n + 1) for f, n in zip(
+            (cell_face_x_m, cell_face_y_m, cell_face_z_m), nodes))
+        prm.center_x_m, prm.center_y_m, prm.center_z_m = (f32_ptr(f, n) for f, n in zip(
+            (cell_center_x_m, cell_center_y_m, cell_center_z_m), nodes))
+        prm.active_ib_node = self.active_ib_node.ptr()
+        prm.target_velocity = self.velocity_dirichlet_mps_field.ptr()
+        prm.target_normal = self.pressure_neumann_normal_field.ptr()
+        prm.boundary_point_m = search.node_boundary_point_m.ptr()
+        prm.interior_fluid_point_m = search.node_interior_fluid_point_m.ptr()
+        prm.nearest_marker = search.nearest_marker.ptr()
+        prm.obstacle = _tensor(obstacle_field).data_ptr()
+        prm.velocity = _tensor(velocity_field).data_ptr()
+        if marker_region_id is not None:
+            regions = _tensor(marker_region_id).to(device=self.device, dtype=torch.int32).contiguous()
+            keep.append(regions)
+            prm.marker_region_id = regions.data_ptr()
+            prm.marker_count = int(regions.shape[0])
+        out = _native.IbVdFields()
+        out.active = _tensor(velocity_dirichlet_active).data_ptr()
+        out.value_mps = _tensor(velocity_dirichlet_value_mps).data_ptr()
+        out.projection_weight = _tensor(velocity_dirichlet_projection_weight).data_ptr()
+        out.anchor_cell = search.node_anchor_cell.ptr()
+        out.marker_region_id = region_out.data_ptr() if region_out is not None else None
+        out.report = self._vd_report.data_ptr()
+        rep = self._vd_call(prm, out, 1, (velocity_dirichlet_active, velocity_dirichlet_value_mps,
+                                          velocity_dirichlet_projection_weight))
+        del keep
+        counts = [int(v) for v in rep[:10]]
+        vmax, wmin, wmax = (float(v) for v in rep[10:13].view(torch.float32))
+        return HibmMpmVelocityDirichletBoundaryReport(
+            active_velocity_dirichlet_rows=counts[0], inactive_obstacle_rows=counts[1], max_abs_velocity_mps=vmax,
+            invalid_reconstruction_row_count=counts[2], invalid_no_fluid_sample_row_count=counts[3],
+            invalid_nonpositive_gap_row_count=counts[4], invalid_node_behind_boundary_row_count=counts[5],
+            invalid_node_beyond_interior_row_count=counts[6], narrow_gap_boundary_velocity_row_count=counts[7],
+            relocated_row_count=counts[8], relocation_merged_row_count=counts[9],
+            relocation_blocked_row_count=counts[1], min_projection_weight=wmin if counts[0] > 0 else 0.0,
+            max_projection_weight=wmax)
+
+    def is_active(self, node_index) -> bool:
+        return bool(int(self.active_ib_node[self._node_index(node_index)]))
+
+    def velocity_dirichlet_mps(self, node_index) -> tuple[float, float, float]:
+        return tuple(float(v) for v in self.velocity_dirichlet_mps_field[self._node_index(node_index)])
+
+    def pressure_neumann_normal(self, node_index) -> tuple[float, float, float]:
+        return tuple(float(v) for v in self.pressure_neumann_normal_field[self._node_index(node_index)])
+
+    def pressure_neumann_gradient_pa_per_m(self, node_index) -> float:
+        return float(self.pressure_neumann_gradient_field[self._node_index(node_index)])
+
+    def _node_index(self, node_index) -> tuple[int, int, int]:
+        index = tuple(int(v) for v in node_index)
+        if len(index) != 3 or any(v < 0 or v >= n for v, n in zip(index, self.grid_nodes)):
+            raise IndexError("node_index out of range")
+        return index

@@ -385,6 +385,93 @@ int efsi_ib_search_plan_destroy(efsi_ib_search_plan* plan);
 int efsi_ib_node_search(efsi_ib_search_plan* plan, const efsi_ib_search_params* params,
                         const efsi_ib_search_fields* fields, void* stream);
 
+/* Report of efsi_ib_build_boundary_conditions (HibmMpmIbBoundaryConditionReport). */
+typedef struct efsi_ib_bc_report {
+  int32_t no_slip_dirichlet_count;
+  int32_t pressure_neumann_count;
+  int32_t inactive_internal_node_count;
+  float max_abs_velocity_mps;
+} efsi_ib_bc_report;
+
+/* hibm_mpm.py:6499-6577 HibmMpmIbBoundaryConditions._build_from_search_kernel:
+ * per external IB node of the search, the no-slip velocity, Neumann normal
+ * and Neumann gradient targets interpolated from the projection markers
+ * (3 floats per node for velocity and normal).  report_device is written on
+ * the device. */
+int efsi_ib_build_boundary_conditions(int64_t node_count, const int32_t* node_kind, const int32_t* nearest_marker,
+                                      const int32_t* projection_marker_indices,
+                                      const float* projection_marker_weights, const float* marker_velocity,
+                                      const float* marker_normal, const float* marker_gradient, int32_t marker_count,
+                                      int32_t* active, float* velocity, float* normal, float* gradient,
+                                      efsi_ib_bc_report* report_device, void* stream);
+
+/* Inputs of efsi_ib_velocity_dirichlet_rows: the fluid grid (faces n + 1 and
+   centres n per axis, f32), the boundary targets (active IB flag, target
+   velocity and normal), the node search's boundary / interior points and
+   nearest markers, the obstacle and cell velocity (3 floats per cell), and
+   optionally the markers' region ids for the region stamp. */
+typedef struct efsi_ib_vd_params {
+  int32_t nx, ny, nz;
+  const float* face_x_m;
+  const float* face_y_m;
+  const float* face_z_m;
+  const float* center_x_m;
+  const float* center_y_m;
+  const float* center_z_m;
+  const int32_t* active_ib_node;
+  const float* target_velocity;
+  const float* target_normal;
+  const float* boundary_point_m;
+  const float* interior_fluid_point_m;
+  const int32_t* nearest_marker;
+  const int32_t* obstacle;
+  const float* velocity;
+  const int32_t* marker_region_id; /* NULL: no region stamp */
+  int32_t marker_count;
+} efsi_ib_vd_params;
+
+/* Report of the velocity-Dirichlet rows (HibmMpmVelocityDirichletBoundaryReport;
+   blocked_rows is both its inactive_obstacle_rows and relocation_blocked_row_count). */
+typedef struct efsi_ib_vd_report {
+  int32_t active_rows;
+  int32_t blocked_rows;
+  int32_t invalid_rows;
+  int32_t invalid_no_fluid_sample_rows;
+  int32_t invalid_nonpositive_gap_rows;
+  int32_t invalid_node_behind_boundary_rows;
+  int32_t invalid_node_beyond_interior_rows;
+  int32_t narrow_gap_rows;
+  int32_t relocated_rows;
+  int32_t merged_rows;
+  float max_abs_velocity_mps;
+  float min_projection_weight; /* 1e30 when no row was written */
+  float max_projection_weight;
+} efsi_ib_vd_report;
+
+/* Outputs: the fluid's row fields (active, value 3 per cell, projection
+   weight), the search's anchor cells (3 int32 per node), the region ids (in
+   place) and the report (device). */
+typedef struct efsi_ib_vd_fields {
+  int32_t* active;
+  float* value_mps;
+  float* projection_weight;
+  int32_t* anchor_cell;
+  int32_t* marker_region_id;
+  efsi_ib_vd_report* report;
+} efsi_ib_vd_fields;
+
+/* reconstruct = 0: hibm_mpm.py:6649-6688 _assemble_velocity_dirichlet_boundary_rows_kernel
+ * (the target velocity on every unmasked active IB node; only the active and
+ * value fields are written).  reconstruct = 1: hibm_mpm.py:7655-7800
+ * assemble_velocity_dirichlet_reconstructed_boundary_rows: anchor prefill
+ * (7551-7616), row reconstruction along the normal with its fallbacks
+ * (6904-7335), relocation of masked rows (7337-7549) and the region stamp
+ * (7618-7653).  Where the reference's parallel loops race (relocation claims,
+ * region writes), the node visited first in C order claims a cell and the
+ * one visited last stamps it. */
+int efsi_ib_velocity_dirichlet_rows(efsi_ib_search_plan* plan, const efsi_ib_vd_params* params,
+                                    const efsi_ib_vd_fields* fields, int32_t reconstruct, void* stream);
+
 /* hibm_mpm.py:5463-5475 _reset_node_anchor_cells_kernel: every node's
  * anchor cell (3 int32 each) to (-1, -1, -1). */
 int efsi_ib_reset_anchor_cells(int32_t* anchor_cells, int64_t node_count, void* stream);

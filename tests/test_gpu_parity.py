@@ -443,3 +443,77 @@ def test_ib_node_search_matches_oracle():
                          (search.node_projection_marker_weights, "projection_weights")):
             np.testing.assert_allclose(got.to_numpy(), ref[key], rtol=0.0, atol=1e-6, err_msg=f"{case} {key}")
     assert (search.node_anchor_cell.to_numpy() == -1).all()
+
+
+@pytest.mark.skip(reason="boundary-condition kernels not yet run on a B200")
+def test_ib_boundary_rows_match_oracle():
+    """Node search -> boundary targets -> reconstructed velocity-Dirichlet
+    rows on a closed surface over a graded grid with masked cells and a
+    random velocity field, each stage against the oracle on the same inputs:
+    flags, anchors and regions identical (the oracle visits nodes in C order;
+    the kernels resolve claims to the first node and region writes to the
+    last), values and weights within 1e-6, report counts equal."""
+    from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
+    from easyfsi_b200.hibm_mpm import HibmMpmIbBoundaryConditions, HibmMpmIbNodeSearch, HibmMpmSurfaceMarkers
+
+    grid = _graded_grid((24, 20, 28))
+    nodes = grid.grid_nodes
+    x, n, tri = _sphere_surface((0.45, 0.5, 0.55), 0.28)
+    rng = np.random.default_rng(12)
+    mk = HibmMpmSurfaceMarkers(marker_capacity=len(x), projection_triangle_capacity=len(tri))
+    mk.load_markers(positions_m=x, velocities_mps=rng.normal(size=x.shape) * 0.1, normals=n,
+                    areas_m2=np.ones(len(x)), region_ids=rng.integers(1, 5, len(x)))
+    mk.set_projection_triangles(tri.tolist())
+    fluid = CartesianFluidSolver(FluidDomainSpec((0, 0, 0), grid.bounds_max_m, None, 1000.0, 1.0e-3, 1.0e-3,
+                                                 cartesian_grid=grid))
+    obs = (rng.random(nodes) < 0.08).astype(np.int32)
+    fluid.obstacle.from_numpy(obs)
+    vel = rng.normal(size=nodes + (3,)).astype(np.float32)
+    fluid.velocity.from_numpy(vel)
+    search = HibmMpmIbNodeSearch(grid_nodes=nodes, bounds_min_m=grid.bounds_min_m, bounds_max_m=grid.bounds_max_m,
+                                 marker_capacity=len(x))
+    search.search_and_classify_grid_fields(
+        mk, cell_center_x_m=fluid.cell_center_x_m, cell_center_y_m=fluid.cell_center_y_m,
+        cell_center_z_m=fluid.cell_center_z_m, search_radius_m=0.07, interior_probe_distance_m=0.04)
+    grads = rng.normal(size=len(x)) * 10.0
+    boundary = HibmMpmIbBoundaryConditions(grid_nodes=nodes, marker_capacity=len(x))
+    rep = boundary.build_from_search(search, mk, marker_pressure_neumann_gradient_pa_per_m=grads.tolist())
+    s = {"kind": search.node_kind_code.to_numpy(), "nearest_marker": search.nearest_marker.to_numpy(),
+         "projection_indices": search.node_projection_marker_indices.to_numpy(),
+         "projection_weights": search.node_projection_marker_weights.to_numpy()}
+    mv, mn = mk.v_gamma_mps.to_numpy()[: len(x)], mk.n_gamma.to_numpy()[: len(x)]
+    bc = orc.ib_build_boundary_conditions(s, markers_v=mv, markers_n=mn, marker_gradients=grads.astype(np.float32))
+    assert rep.__dict__ == pytest.approx(bc["report"])
+    assert bc["report"]["no_slip_dirichlet_count"] > 50
+    np.testing.assert_array_equal(boundary.active_ib_node.to_numpy(), bc["active"])
+    for got, key in ((boundary.velocity_dirichlet_mps_field, "velocity"),
+                     (boundary.pressure_neumann_normal_field, "normal"),
+                     (boundary.pressure_neumann_gradient_field, "gradient")):
+        np.testing.assert_allclose(got.to_numpy(), bc[key], rtol=0.0, atol=1e-5, err_msg=key)
+
+    regions = fluid.velocity_dirichlet_boundary_marker_region_id
+    vrep = boundary.assemble_velocity_dirichlet_reconstructed_boundary_rows(
+        fluid.velocity_dirichlet_boundary_active, fluid.velocity_dirichlet_boundary_value_mps,
+        fluid.velocity_dirichlet_boundary_projection_weight, fluid.obstacle, fluid.velocity, search,
+        cell_face_x_m=fluid.cell_face_x_m, cell_face_y_m=fluid.cell_face_y_m, cell_face_z_m=fluid.cell_face_z_m,
+        cell_center_x_m=fluid.cell_center_x_m, cell_center_y_m=fluid.cell_center_y_m,
+        cell_center_z_m=fluid.cell_center_z_m, grid_nodes=nodes, velocity_dirichlet_marker_region_id=regions,
+        marker_region_id=mk.region_id)
+    ref = orc.ib_velocity_dirichlet_rows(
+        grid, active_ib=boundary.active_ib_node.to_numpy(),
+        bc_velocity=boundary.velocity_dirichlet_mps_field.to_numpy(),
+        bc_normal=boundary.pressure_neumann_normal_field.to_numpy(),
+        boundary_point=search.node_boundary_point_m.to_numpy(),
+        interior_point=search.node_interior_fluid_point_m.to_numpy(), obstacle=obs, velocity=vel,
+        nearest_marker=s["nearest_marker"], marker_region=mk.region_id.to_numpy()[: len(x)],
+        region_out=np.full(nodes, -1, np.int32))
+    assert vrep.relocated_row_count > 0 and vrep.active_velocity_dirichlet_rows > 50
+    for key, value in ref["report"].items():
+        assert getattr(vrep, key) == pytest.approx(value, abs=1e-6), key
+    np.testing.assert_array_equal(fluid.velocity_dirichlet_boundary_active.to_numpy(), ref["active"])
+    np.testing.assert_array_equal(search.node_anchor_cell.to_numpy(), ref["anchor"])
+    np.testing.assert_array_equal(regions.to_numpy(), ref["region"])
+    np.testing.assert_allclose(fluid.velocity_dirichlet_boundary_value_mps.to_numpy(), ref["value"], rtol=0.0,
+                               atol=1e-6)
+    np.testing.assert_allclose(fluid.velocity_dirichlet_boundary_projection_weight.to_numpy(), ref["weight"],
+                               rtol=0.0, atol=1e-6)
