@@ -43,3 +43,41 @@ def test_argument_validation_without_gpu():
     assert status == 1
     assert b"invalid plan arguments" in lib.efsi_last_error()
     assert lib.efsi_mpm_plan_create(0, 4, 4, 4, None) == 1
+
+
+def test_ib_entry_points_reject_bad_arguments_without_gpu():
+    """The IB node search, boundary-condition and row entry points check
+    their arguments before any device work (hibm_mpm.py:6069-6094, 7673-7678)."""
+    from ctypes import byref, c_void_p
+
+    lib = _native.load()
+    fake_plan = c_void_p(1)  # never dereferenced: every call below fails an argument check first
+    prm = _native.IbSearchParams()
+    out = _native.IbSearchFields()
+    assert lib.efsi_ib_node_search(None, byref(prm), byref(out), None) == 1
+    assert b"null argument" in lib.efsi_last_error()
+    prm.nx = prm.ny = prm.nz = 2
+    prm.search_radius_m = 0.0
+    prm.interior_probe_distance_m = 0.1
+    assert lib.efsi_ib_node_search(fake_plan, byref(prm), byref(out), None) == 1
+    assert b"search_radius_m" in lib.efsi_last_error()
+    prm.search_radius_m = float("inf")
+    assert lib.efsi_ib_node_search(fake_plan, byref(prm), byref(out), None) == 1
+    assert b"search_radius_m" in lib.efsi_last_error()
+    prm.search_radius_m = 0.1
+    prm.sign_tolerance_m = -1.0
+    assert lib.efsi_ib_node_search(fake_plan, byref(prm), byref(out), None) == 1
+    assert b"sign_tolerance_m" in lib.efsi_last_error()
+    prm.sign_tolerance_m = 0.0
+    prm.marker_count = 3  # marker arrays missing
+    assert lib.efsi_ib_node_search(fake_plan, byref(prm), byref(out), None) == 1
+    assert b"marker arrays" in lib.efsi_last_error()
+
+    assert lib.efsi_ib_build_boundary_conditions(-1, None, None, None, None, None, None, None, 0, None, None, None,
+                                                 None, None, None) == 1
+    vd = _native.IbVdParams()
+    vd.nx, vd.ny, vd.nz = 1, 4, 4
+    fields = _native.IbVdFields()
+    assert lib.efsi_ib_velocity_dirichlet_rows(fake_plan, byref(vd), byref(fields), 1, None) == 1
+    assert b">= 2" in lib.efsi_last_error()
+    assert lib.efsi_ib_reset_anchor_cells(None, 4, None) == 1
