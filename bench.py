@@ -155,6 +155,52 @@ def ib_node_search_stats(scene, reps: int) -> dict:
     }
 
 
+def pressure_solve_stats(scene, reps: int, jacobi_max_iterations: int = 20000) -> dict:
+    """One c2 pressure solve to the scene's relative-residual tolerance (the
+    Poisson system of a predicted, not yet projected velocity), timed with
+    CUDA events per preconditioner: the reference's MG V-cycle, the FP32
+    level-0 V-cycle, and Jacobi (plain diagonally preconditioned CG, with a
+    larger iteration budget).  The first solve of each captures its graphs
+    and is not timed.  The scene's velocity and pressure are restored."""
+    import torch
+
+    fl, cfg = scene.fluid, scene.cfg
+    saved = (fl.velocity.tensor.clone(), fl.pressure.tensor.clone())
+    stream = torch.cuda.current_stream()
+    out = {}
+    try:
+        fl.predict(cfg.dt_s)
+        fl.compute_divergence()
+        for name, iters in (("fv_multigrid", cfg.cg_max_iterations), ("fv_multigrid_mixed", cfg.cg_max_iterations),
+                            ("jacobi", jacobi_max_iterations)):
+            times = []
+            for r in range(reps + 1):
+                fl.pressure.tensor.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fl._solve_pressure_poisson_fv_cg(iterations=iters, rhs_scale=cfg.density_kgm3 / cfg.dt_s,
+                                                 pressure_outlet_zmin=False, tolerance=cfg.cg_tolerance,
+                                                 preconditioner=name)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if r > 0:
+                    times.append(e0.elapsed_time(e1))
+            out[name] = {
+                "ms": float(np.median(times)),
+                "iterations": int(fl.last_cg_iterations),
+                "converged": bool(fl.last_cg_converged),
+                "relative_residual": float(fl.last_cg_relative_residual),
+            }
+        base = out["jacobi"]["ms"]
+        for name in ("fv_multigrid", "fv_multigrid_mixed"):
+            out[name]["speedup_vs_jacobi"] = base / out[name]["ms"]
+        out["tolerance"] = cfg.cg_tolerance
+    finally:
+        fl.velocity.tensor.copy_(saved[0])
+        fl.pressure.tensor.copy_(saved[1])
+    return out
+
+
 def max_over_ranks(ms: float, world: int, device) -> float:
     """Largest per-rank time over all ranks (every rank calls this in the same
     order; a no-op for one rank)."""
@@ -234,6 +280,7 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the fv_multigrid_mixed measurement")
     ap.add_argument("--no-ib-search", action="store_true", help="skip the IB node search measurement")
+    ap.add_argument("--no-pressure-solve", action="store_true", help="skip the per-preconditioner solve timing")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-reps", type=int, default=50)
@@ -354,6 +401,14 @@ def main() -> None:
         except Exception as exc:  # reported, never fatal to the step's line
             ib_search = {"error": f"{type(exc).__name__}: {exc}"}
 
+    # --- one pressure solve per preconditioner (not part of the step) ---
+    psolve = None
+    if not args.no_pressure_solve:
+        try:
+            psolve = pressure_solve_stats(scene, reps=2)
+        except Exception as exc:  # reported, never fatal to the step's line
+            psolve = {"error": f"{type(exc).__name__}: {exc}"}
+
     # --- e2e through the public API with host-resident state ---
     e2e = None
     if not args.no_e2e:
@@ -473,6 +528,7 @@ def main() -> None:
             "preconditioner": vcycle_stats,
             "mixed_precision": mixed,
             "ib_node_search": ib_search,
+            "pressure_solve": psolve,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
