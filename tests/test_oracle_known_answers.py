@@ -567,3 +567,58 @@ def test_vd_rows_fall_back_for_a_node_behind_the_boundary_plane():
     assert rep["active_velocity_dirichlet_rows"] == 1 and rep["invalid_reconstruction_row_count"] == 0
     assert r["weight"][node] == pytest.approx(0.5, abs=1e-6)
     np.testing.assert_allclose(r["value"][node], (0.3, 0.0, 0.0), atol=1e-6)
+
+
+def _ecoflex_0010():
+    """hyperelastic.py:143-165 / :111-140: Ecoflex 00-10, mu from the 100 %
+    modulus (8 psi) of a uniaxial neo-Hookean bar, nu = 0.49, 1040 kg/m^3."""
+    mu = 8.0 * 6894.757293168361 / (2.0 - 2.0 ** -2)
+    nu = 0.49
+    e = 2.0 * mu * (1.0 + nu)
+    k = e / (3.0 * (1.0 - 2.0 * nu))
+    return 1040.0, mu, k - 2.0 * mu / 3.0
+
+
+# test_neo_hookean_mpm.py:133 a non-cubic grid maps particles with its own axis spacing
+def test_mpm_non_cubic_grid_uses_axis_spacing():
+    rho, mu, lam = _ecoflex_0010()
+    x, vol, mass = _box_particles((2, 2, 2), (-0.002, -0.002, 0.024), (0.002, 0.002, 0.030), rho)
+    s = orc.OracleSolid(capacity=8, grid_nodes=(12, 12, 12), bounds_min=(-0.01, -0.01, -0.04),
+                        bounds_max=(0.01, 0.01, 0.04))
+    s.load(x=x, volume=vol, mass=mass, region=np.ones(8, np.int32))
+    s.v[:8] = (0.0, 0.0, 0.01)
+    rep = s.step(dt=1.0e-5, mu=mu, lam=lam, primary=1, secondary=2)
+    assert rep.counts[0] > 0
+    assert rep.values[11] < 2.0e-5
+    assert rep.values[13] == pytest.approx(1.0, abs=1e-4)
+
+
+# test_neo_hookean_mpm.py:163 an external force changes the grid momentum consistently
+def test_mpm_external_force_changes_grid_momentum():
+    rho, mu, lam = _ecoflex_0010()
+    x, vol, mass = _box_particles((2, 2, 2), (-0.004,) * 3, (0.004,) * 3, rho)
+    s = orc.OracleSolid(capacity=8, grid_nodes=(12, 12, 12), bounds_min=(-0.02,) * 3, bounds_max=(0.02,) * 3)
+    s.load(x=x, volume=vol, mass=mass, region=np.ones(8, np.int32))
+    s.fext[:8] = (0.0, 0.0, -1.0e-4)
+    rep = s.step(dt=1.0e-5, mu=mu, lam=lam, primary=1, secondary=2)
+    assert rep.values[10] < 0.0  # external force z
+    assert rep.values[7] < 0.0  # grid momentum z
+    assert rep.values[11] < 2.0e-5
+
+
+# test_neo_hookean_mpm.py:411 a particle next to the boundary deposits no partial stencil
+def test_mpm_near_boundary_particle_deposits_nothing():
+    rho, mu, lam = _ecoflex_0010()
+    x, vol, mass = _box_particles((2, 2, 2), (-0.004,) * 3, (0.004,) * 3, rho)
+    dx = 0.04 / 8
+    x[0, 0] = np.float32(-0.02 + 0.25 * dx)
+    s = orc.OracleSolid(capacity=8, grid_nodes=(8, 8, 8), bounds_min=(-0.02,) * 3, bounds_max=(0.02,) * 3)
+    s.load(x=x, volume=vol, mass=mass, region=np.ones(8, np.int32))
+    rep = s.step(dt=0.0, mu=mu, lam=lam, primary=1, secondary=2)
+    assert rep.counts[1] == 1  # grid out-of-bounds particles
+    assert float(np.sum(s.grid_mass, dtype=np.float64)) == pytest.approx(float(np.sum(mass[1:], dtype=np.float64)),
+                                                                         abs=1e-8)
+    mean_stretch = rep.values[14] / rep.counts[3]
+    assert math.isfinite(mean_stretch) and math.isfinite(rep.values[15])
+    assert mean_stretch == pytest.approx(1.0, abs=1e-6)
+    assert rep.values[15] == pytest.approx(0.0, abs=5e-6)
