@@ -622,3 +622,29 @@ def test_mpm_near_boundary_particle_deposits_nothing():
     assert math.isfinite(mean_stretch) and math.isfinite(rep.values[15])
     assert mean_stretch == pytest.approx(1.0, abs=1e-6)
     assert rep.values[15] == pytest.approx(0.0, abs=5e-6)
+
+
+def _one_particle_with_f(f):
+    rho, mu, lam = _ecoflex_0010()
+    x, vol, mass = _box_particles((1, 1, 1), (-0.001,) * 3, (0.001,) * 3, rho)
+    s = orc.OracleSolid(capacity=1, grid_nodes=(8, 8, 8), bounds_min=(-0.01,) * 3, bounds_max=(0.01,) * 3)
+    s.load(x=x, volume=vol, mass=mass, region=np.ones(1, np.int32))
+    s.F[0] = np.asarray(f, np.float32)
+    return s, s.step(dt=0.0, mu=mu, lam=lam, primary=1, secondary=2)
+
+
+# test_neo_hookean_mpm.py:543 an inverted deformation gradient triggers the SVD clamp
+def test_mpm_inverted_deformation_gradient_is_clamped():
+    s, rep = _one_particle_with_f([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, -1.0]])
+    assert rep.counts[2] == 1  # deformation clamps
+    assert rep.values[13] > 0.0 and abs(rep.values[13] - 1.0) < 1.0e-5
+
+
+# test_neo_hookean_mpm.py:581 the clamp persists the corrected deformation gradient
+def test_mpm_clamp_persists_the_corrected_deformation_gradient():
+    s, rep = _one_particle_with_f([[-2.0, 0.0, 0.0], [0.0, 0.5, 0.0], [0.0, 0.0, 0.5]])
+    corrected = np.asarray(s.F[0], np.float64).reshape(3, 3)
+    assert rep.counts[2] == 1
+    assert np.linalg.det(corrected) > 0.0
+    sv = np.linalg.svd(corrected, compute_uv=False)
+    assert sv.min() >= 1.0e-2 and sv.max() <= 1.0e2
