@@ -648,3 +648,62 @@ def test_mpm_clamp_persists_the_corrected_deformation_gradient():
     assert np.linalg.det(corrected) > 0.0
     sv = np.linalg.svd(corrected, compute_uv=False)
     assert sv.min() >= 1.0e-2 and sv.max() <= 1.0e2
+
+
+# --------------------------------------------------------------------------
+# Divergence and projection (tests/test_fluid.py:28-58 of the reference)
+# --------------------------------------------------------------------------
+def _divergence_stats(fl, interior_only=False):
+    """fluid.py:3494-3522 / 3827-3835: max |div| and RMS over fluid cells."""
+    d = np.abs(np.asarray(fl.divergence, np.float64))
+    mask = fl.obstacle == 0
+    if interior_only:
+        inner = np.zeros_like(mask)
+        inner[1:-1, 1:-1, 1:-1] = True
+        mask &= inner
+    vals = d[mask]
+    return {"max_abs": float(vals.max(initial=0.0)), "l2": math.sqrt(float((vals * vals).sum()) / max(1, vals.size))}
+
+
+def _centres(n):
+    return (np.arange(n, dtype=np.float32) + np.float32(0.5)) / np.float32(n)
+
+
+# test_fluid.py:28 a uniform velocity has near-zero divergence
+def test_uniform_velocity_has_near_zero_divergence():
+    fl = _fluid(_uniform_box(16))
+    fl.velocity[...] = (0.2, -0.1, 0.05)
+    fl.compute_divergence(0)
+    st = _divergence_stats(fl, interior_only=True)
+    assert st["max_abs"] < 1.0e-5 and st["l2"] < 1.0e-5
+
+
+# test_fluid.py:37 a simple shear velocity has near-zero divergence
+def test_simple_shear_velocity_has_near_zero_divergence():
+    fl = _fluid(_uniform_box(21))
+    y = _centres(21)
+    fl.velocity[...] = 0.0
+    fl.velocity[:, :, :, 0] = (np.float32(75.0) * (y - np.float32(0.5)))[None, :, None]
+    fl.compute_divergence(0)
+    st = _divergence_stats(fl, interior_only=True)
+    assert st["max_abs"] < 1.0e-5 and st["l2"] < 1.0e-5
+
+
+# test_fluid.py:46 the projection reduces the divergence (the reference's
+# default legacy Jacobi solve; here the oracle's MG-PCG, which reduces it further)
+def test_projection_reduces_divergence():
+    n = 24
+    fl = _fluid(_uniform_box(n))
+    c = _centres(n)
+    two_pi = np.float32(2.0 * math.pi)
+    fl.velocity[..., 0] = (np.float32(0.15) * np.sin(two_pi * c))[:, None, None]
+    fl.velocity[..., 1] = (np.float32(0.075) * np.sin(two_pi * c))[None, :, None]
+    fl.velocity[..., 2] = (np.float32(-0.0375) * np.sin(two_pi * c))[None, None, :]
+    fl.compute_divergence(0)
+    before = _divergence_stats(fl)
+    fl.project(dt=2.0e-3, max_iters=240, tol=1.0e-8)
+    fl.compute_divergence(0)
+    after = _divergence_stats(fl)
+    assert before["l2"] > 0.1
+    assert after["l2"] < before["l2"] * 0.45
+    assert after["max_abs"] < before["max_abs"] * 0.55
