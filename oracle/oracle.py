@@ -232,6 +232,24 @@ class OracleFluid:
                                            _p(owner), _p(nbr), _p(trans))
         return out
 
+    def spread_surface_forces(self, positions, forces, *, center=(0.0, 0.0, 0.0), force_sign: float = -1.0):
+        """fluid.py:3196-3273: surface forces spread trilinearly onto the fluid
+        cells as force densities (renormalised over the fluid corners).
+        Returns the report: surface force sum (3), grid force sum (3)."""
+        pos = np.ascontiguousarray(positions, self.rt).reshape(-1, 3)
+        f = np.ascontiguousarray(forces, self.rt).reshape(-1, 3)
+        self.force = np.zeros((self.nx, self.ny, self.nz, 3), self.rt)
+        report = np.zeros(6)
+        self.lib.efo_spread_surface_forces(byref(self.gridstruct), _p(self.obstacle), _p(pos), _p(f), c_int(len(pos)),
+                                           c_float(center[0]), c_float(center[1]), c_float(center[2]),
+                                           c_float(force_sign), _p(self.force), _p(report))
+        return report
+
+    def apply_body_force(self, dt: float) -> None:
+        """fluid.py:3301-3328: u += f dt / rho on the fluid cells."""
+        self.lib.efo_apply_body_force(byref(self.levels[0]), _p(self.obstacle), _p(self.force), c_float(dt),
+                                      c_float(self.rho), _p(self.velocity))
+
     def fv_diagonal(self, outlet: int = 0, vdir_active=None, vdir_weight=None, iface=None) -> np.ndarray:
         out = np.zeros((self.nx, self.ny, self.nz), dtype=np.float64)
         self.lib.efo_fv_diagonal(byref(self.levels[0]), _p(self.obstacle), _p(vdir_active), _p(vdir_weight), _p(iface), _p(out), c_int(outlet))

@@ -707,3 +707,45 @@ def test_projection_reduces_divergence():
     assert before["l2"] > 0.1
     assert after["l2"] < before["l2"] * 0.45
     assert after["max_abs"] < before["max_abs"] * 0.55
+
+
+def _cell_volumes(fl):
+    w = [np.asarray(m["w"], np.float32).astype(np.float64) for m in fl.metrics[0]]
+    return np.einsum("i,j,k->ijk", *w)
+
+
+def _momentum_change(fl, before):
+    """sum rho V du over the fluid cells (the impulse of the body force)."""
+    du = np.asarray(fl.velocity, np.float64) - before
+    return fl.rho * np.einsum("ijk,ijkc->c", _cell_volumes(fl), du)
+
+
+# test_fluid.py:85 surface-force spreading conserves action and reaction on the grid
+def test_surface_force_spreading_conserves_action_reaction():
+    fl = _fluid(_uniform_box(32))
+    pos = [(-0.02, 0.0, 0.0), (0.02, 0.0, 0.0), (0.0, -0.02, 0.0), (0.0, 0.02, 0.0)]
+    forces = [(0.0, 0.0, -0.25), (0.0, 0.0, -0.5), (0.0, 0.0, -0.75), (0.0, 0.0, -1.0)]
+    rep = fl.spread_surface_forces(pos, forces, center=(0.5, 0.5, 0.5), force_sign=-1.0)
+    surface, grid = rep[:3], rep[3:]
+    assert np.count_nonzero(np.abs(fl.force).sum(axis=-1)) > 0
+    assert surface[2] == pytest.approx(-2.5, abs=1e-6)
+    assert grid[2] == pytest.approx(-surface[2], abs=abs(surface[2]) * 1e-5)
+    # the force densities integrate to the grid force
+    np.testing.assert_allclose(np.einsum("ijk,ijkc->c", _cell_volumes(fl), fl.force), grid, rtol=1e-5, atol=1e-9)
+    before = np.asarray(fl.velocity, np.float64).copy()
+    fl.apply_body_force(2.5e-3)
+    assert _momentum_change(fl, before)[2] == pytest.approx(grid[2] * 2.5e-3, rel=1e-5)
+
+
+# test_fluid.py:139 spreading renormalises around obstacles
+def test_surface_force_spreading_renormalises_around_obstacles():
+    fl = _fluid(_uniform_box(8))
+    fl.obstacle[3, 4, 4] = 1
+    c = _centres(8)
+    pos = [(0.5 * (c[3] + c[4]), c[4], c[4])]
+    rep = fl.spread_surface_forces(pos, [(0.0, 0.0, -2.0)], center=(0.0, 0.0, 0.0), force_sign=-1.0)
+    assert np.count_nonzero(np.abs(fl.force).sum(axis=-1)) == 1
+    assert rep[5] == pytest.approx(2.0, abs=2e-5)
+    before = np.asarray(fl.velocity, np.float64).copy()
+    fl.apply_body_force(2.5e-3)
+    assert _momentum_change(fl, before)[2] == pytest.approx(rep[5] * 2.5e-3, rel=1e-5)
