@@ -232,6 +232,13 @@ class OracleFluid:
                                            _p(owner), _p(nbr), _p(trans))
         return out
 
+    def subtract_pressure_gradient(self, dt_over_rho: float, outlet: int = 0) -> None:
+        """fluid.py:5538-5582 _subtract_pressure_gradient_kernel on the current
+        pressure (no Dirichlet rows)."""
+        self.lib.efo_subtract_pressure_gradient(byref(self.levels[0]), _p(self.obstacle), None, None, None,
+                                                _p(self.pressure), c_float(dt_over_rho), c_int(outlet),
+                                                _p(self.velocity))
+
     def spread_surface_forces(self, positions, forces, *, center=(0.0, 0.0, 0.0), force_sign: float = -1.0):
         """fluid.py:3196-3273: surface forces spread trilinearly onto the fluid
         cells as force densities (renormalised over the fluid corners).

@@ -749,3 +749,75 @@ def test_surface_force_spreading_renormalises_around_obstacles():
     before = np.asarray(fl.velocity, np.float64).copy()
     fl.apply_body_force(2.5e-3)
     assert _momentum_change(fl, before)[2] == pytest.approx(rep[5] * 2.5e-3, rel=1e-5)
+
+
+# --------------------------------------------------------------------------
+# FV divergence and pressure gradient next to obstacles (tests/test_core_fluid.py:1038-1146)
+# --------------------------------------------------------------------------
+def _fluid_with(nodes, obstacle, pressure=None, velocity=None):
+    w = [[1.0 / n] * n for n in nodes]
+    fl = _fluid(CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=w[0], cell_widths_y_m=w[1],
+                              cell_widths_z_m=w[2]))
+    fl.obstacle[...] = obstacle
+    fl.velocity[...] = 0.0 if velocity is None else velocity
+    if pressure is not None:
+        fl.pressure[...] = pressure
+    return fl
+
+
+# test_core_fluid.py:1038 the divergence has zero flux through obstacle faces
+def test_divergence_uses_zero_flux_on_obstacle_faces():
+    obs = np.zeros((4, 4, 4), np.int32)
+    obs[2, 1, 1] = 1
+    vel = np.zeros((4, 4, 4, 3), np.float32)
+    vel[1, 1, 1, 0] = 1.25
+    fl = _fluid_with((4, 4, 4), obs, velocity=vel)
+    fl.compute_divergence(0)
+    assert float(fl.divergence[0, 1, 1]) == pytest.approx(5.0, abs=1e-6)
+    assert float(fl.divergence[1, 1, 1]) == pytest.approx(-5.0, abs=1e-6)
+    assert float(fl.divergence[2, 1, 1]) == pytest.approx(0.0, abs=1e-6)
+
+
+# test_core_fluid.py:1057 the FV divergence is the pressure gradient's adjoint next to obstacles
+def test_divergence_of_the_gradient_is_the_fv_laplacian_next_to_obstacles():
+    nodes = (5, 4, 4)
+    obs = np.zeros(nodes, np.int32)
+    obs[3, 1:3, 1:3] = 1
+    i, j, k = np.meshgrid(*[np.arange(n) for n in nodes], indexing="ij")
+    p = (0.7 * i - 0.3 * j + 0.11 * k + 0.05 * i * j).astype(np.float32)
+    p[obs == 1] = 0.0
+    fl = _fluid_with(nodes, obs, pressure=p)
+    fl.subtract_pressure_gradient(0.25)
+    fl.compute_divergence(0)
+    w = [np.asarray(m["w"], np.float32).astype(np.float64) for m in fl.metrics[0]]
+    cd = [np.asarray(m["cd"], np.float32).astype(np.float64) for m in fl.metrics[0]]
+    expected = np.zeros(nodes)
+    for c in zip(*np.nonzero(obs == 0)):
+        applied, centre = 0.0, float(p[c])
+        for a in range(3):
+            for step in (-1, 1):
+                q = list(c)
+                q[a] += step
+                if not 0 <= q[a] < nodes[a] or obs[tuple(q)] != 0:
+                    continue
+                dist = cd[a][c[a]] if step < 0 else cd[a][c[a] + 1]
+                applied += (float(p[tuple(q)]) - centre) / (w[a][c[a]] * dist)
+        expected[c] = -0.25 * applied
+    active = obs == 0
+    np.testing.assert_allclose(np.asarray(fl.divergence)[active], expected[active], rtol=2e-5, atol=1e-5)
+
+
+# test_core_fluid.py:1124 divergence of the gradient is globally conservative with obstacles
+def test_divergence_of_the_gradient_is_globally_conservative():
+    nodes = (6, 5, 4)
+    obs = np.zeros(nodes, np.int32)
+    obs[3, 1:4, 1:3] = 1
+    i, j, k = np.meshgrid(*[np.arange(n) for n in nodes], indexing="ij")
+    p = (0.17 * i * i - 0.31 * j + 0.13 * k).astype(np.float32)
+    p[obs == 1] = 0.0
+    fl = _fluid_with(nodes, obs, pressure=p)
+    fl.subtract_pressure_gradient(0.4)
+    fl.compute_divergence(0)
+    cell_volume = 1.0 / (6 * 5 * 4)
+    net = float(np.sum(np.asarray(fl.divergence, np.float64)[obs == 0] * cell_volume))
+    assert net == pytest.approx(0.0, abs=1e-7)
