@@ -821,3 +821,48 @@ def test_divergence_of_the_gradient_is_globally_conservative():
     cell_volume = 1.0 / (6 * 5 * 4)
     net = float(np.sum(np.asarray(fl.divergence, np.float64)[obs == 0] * cell_volume))
     assert net == pytest.approx(0.0, abs=1e-7)
+
+
+# test_core_fluid.py:1353 the uniform FV Laplacian converges at second order
+def test_uniform_fv_laplacian_converges_at_second_order():
+    errors = []
+    for n in (16, 32, 64):
+        fl = _fluid(_uniform_box(n))
+        c = (np.arange(n, dtype=np.float64) + 0.5) / n
+        x, y, z = np.meshgrid(c, c, c, indexing="ij")
+        p = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
+        expected = -3.0 * np.pi * np.pi * p
+        discrete = -fl.fv_apply(p, 0)  # the operator is -laplacian
+        err = (discrete - expected)[1:-1, 1:-1, 1:-1]
+        errors.append(float(np.sqrt(np.mean(err * err))))
+    assert errors[1] < errors[0] * 0.30
+    assert errors[2] < errors[1] * 0.30
+
+
+# test_core_fluid.py:882 pressure inside an obstacle is Neumann for the projection
+def test_obstacle_pressure_does_not_drive_the_fluid():
+    obs = np.zeros((8, 8, 8), np.int32)
+    obs[4, 4, 4] = 1
+    p = np.zeros((8, 8, 8))
+    p[4, 4, 4] = 1000.0
+    fl = _fluid_with((8, 8, 8), obs, pressure=p)
+    fl.project(dt=1.0e-3, max_iters=1)
+    assert float(np.linalg.norm(np.asarray(fl.velocity, np.float64), axis=-1).max()) < 1.0e-8
+
+
+# test_core_fluid.py:927 the projection solves the consistent divergence-gradient system
+def test_projection_solves_the_consistent_system():
+    n = 24
+    fl = _fluid(_uniform_box(n))
+    c = _centres(n)
+    two_pi = np.float32(2.0 * math.pi)
+    fl.velocity[..., 0] = (np.float32(0.15) * np.sin(two_pi * c))[:, None, None]
+    fl.velocity[..., 1] = (np.float32(0.075) * np.sin(two_pi * c))[None, :, None]
+    fl.velocity[..., 2] = (np.float32(-0.0375) * np.sin(two_pi * c))[None, None, :]
+    fl.compute_divergence(0)
+    before = _divergence_stats(fl)
+    fl.project(dt=2.0e-3, max_iters=480, tol=1.0e-8)
+    after = _divergence_stats(fl)
+    assert before["l2"] > 0.1
+    assert after["l2"] < before["l2"] * 0.05
+    assert after["max_abs"] < before["max_abs"] * 0.08
