@@ -866,3 +866,49 @@ def test_projection_solves_the_consistent_system():
     assert before["l2"] > 0.1
     assert after["l2"] < before["l2"] * 0.05
     assert after["max_abs"] < before["max_abs"] * 0.08
+
+
+def _nonuniform_fluid(wx, wy, wz):
+    return _fluid(CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=wx, cell_widths_y_m=wy,
+                                cell_widths_z_m=wz))
+
+
+# test_core_fluid.py:504 the non-uniform divergence and gradient use the grid metrics
+def test_nonuniform_divergence_and_gradient_use_grid_metrics():
+    fl = _nonuniform_fluid((0.1, 0.2, 0.3, 0.4), (0.25,) * 4, (0.25,) * 4)
+    fl.velocity[...] = 0.0
+    fl.velocity[1, 1, 1, 0] = 1.0
+    fl.velocity[2, 1, 1, 0] = 1.6
+    fl.compute_divergence(0)
+    assert float(fl.divergence[1, 1, 1]) == pytest.approx(3.0, abs=1e-6)
+    fl.velocity[...] = 0.0
+    fl.pressure[...] = 0.0
+    fl.pressure[0, 1, 1] = 4.0
+    fl.pressure[1, 1, 1] = 10.0
+    fl.subtract_pressure_gradient(1.0)
+    assert float(fl.velocity[1, 1, 1, 0]) == pytest.approx(-40.0, abs=1e-5)
+
+
+# test_core_fluid.py:541 (body-force part) the impulse integrates over the cell volumes
+def test_nonuniform_body_force_impulse_uses_cell_volumes():
+    fl = _nonuniform_fluid((0.1, 0.2, 0.3, 0.4), (0.2, 0.2, 0.3, 0.3), (0.1, 0.2, 0.3, 0.4))
+    fl.velocity[...] = 0.0
+    fl.force = np.zeros((4, 4, 4, 3), np.float32)
+    fl.force[0, 0, 0, 0] = 200.0
+    fl.force[2, 1, 3, 0] = 300.0
+    vol = _cell_volumes(fl)
+    before = np.asarray(fl.velocity, np.float64).copy()
+    fl.apply_body_force(2.0e-3)
+    expected = (200.0 * vol[0, 0, 0] + 300.0 * vol[2, 1, 3]) * 2.0e-3
+    assert _momentum_change(fl, before)[0] == pytest.approx(expected, abs=1e-8)
+
+
+# test_core_fluid.py:593 non-uniform spreading uses the cell volumes
+def test_nonuniform_spreading_uses_cell_volumes():
+    fl = _nonuniform_fluid((0.1, 0.2, 0.3, 0.4), (0.2, 0.2, 0.3, 0.3), (0.1, 0.2, 0.3, 0.4))
+    rep = fl.spread_surface_forces([(0.0, 0.0, 0.0)], [(1.0, -2.0, 3.0)], center=(0.05, 0.1, 0.05), force_sign=-1.0)
+    assert np.count_nonzero(np.abs(fl.force).sum(axis=-1)) == 1
+    np.testing.assert_allclose(rep[3:], (-1.0, 2.0, -3.0), rtol=1e-6, atol=1e-6)
+    before = np.asarray(fl.velocity, np.float64).copy()
+    fl.apply_body_force(1.5e-3)
+    np.testing.assert_allclose(_momentum_change(fl, before), rep[3:] * 1.5e-3, rtol=1e-6, atol=1e-8)
