@@ -232,6 +232,14 @@ class OracleFluid:
                                            _p(owner), _p(nbr), _p(trans))
         return out
 
+    def apply_closed_boundary(self, outlet: int = 0) -> None:
+        """fluid.py:5529-5536: the normal velocity on the min faces is zeroed (z-min kept with the outlet)."""
+        self.lib.efo_apply_closed_boundary(byref(self.levels[0]), c_int(outlet), _p(self.velocity))
+
+    def apply_zmin_no_backflow(self) -> None:
+        """fluid.py:5762-5766: no inflow through the z-min outlet."""
+        self.lib.efo_apply_zmin_no_backflow(byref(self.levels[0]), _p(self.obstacle), _p(self.velocity))
+
     def subtract_pressure_gradient(self, dt_over_rho: float, outlet: int = 0) -> None:
         """fluid.py:5538-5582 _subtract_pressure_gradient_kernel on the current
         pressure (no Dirichlet rows)."""

@@ -912,3 +912,41 @@ def test_nonuniform_spreading_uses_cell_volumes():
     before = np.asarray(fl.velocity, np.float64).copy()
     fl.apply_body_force(1.5e-3)
     np.testing.assert_allclose(_momentum_change(fl, before), rep[3:] * 1.5e-3, rtol=1e-6, atol=1e-8)
+
+
+# test_core_fluid.py:835 the closed-boundary clamp keeps the shifted MAC max faces
+def test_closed_boundary_clamp_keeps_the_max_faces():
+    fl = _fluid(_uniform_box(4))
+    fl.velocity[...] = 0.0
+    fl.velocity[0, 1, 1, 0], fl.velocity[-1, 1, 1, 0] = -0.2, 0.3
+    fl.velocity[1, 0, 1, 1], fl.velocity[1, -1, 1, 1] = -0.4, 0.5
+    fl.velocity[1, 1, 0, 2], fl.velocity[1, 1, -1, 2] = -0.6, 0.7
+    fl.apply_closed_boundary(0)
+    assert float(fl.velocity[0, 1, 1, 0]) == 0.0 and float(fl.velocity[1, 0, 1, 1]) == 0.0
+    assert float(fl.velocity[1, 1, 0, 2]) == 0.0
+    assert float(fl.velocity[-1, 1, 1, 0]) == pytest.approx(0.3, abs=1e-7)
+    assert float(fl.velocity[1, -1, 1, 1]) == pytest.approx(0.5, abs=1e-7)
+    assert float(fl.velocity[1, 1, -1, 2]) == pytest.approx(0.7, abs=1e-7)
+
+
+# test_core_fluid.py:745 (kernel part) the z-min outlet clamps only backflow
+def test_zmin_outlet_clamps_only_backflow():
+    fl = _fluid(_uniform_box(8))
+    fl.velocity[...] = (0.0, 0.0, 0.05)
+    fl.apply_zmin_no_backflow()
+    assert float(np.asarray(fl.velocity)[:, :, 0, 2].max()) <= 1.0e-8
+    fl.velocity[...] = (0.0, 0.0, -0.05)
+    fl.apply_zmin_no_backflow()
+    assert float(np.asarray(fl.velocity)[:, :, 0, 2].min()) < -0.049
+
+
+# test_core_fluid.py:772 the predictor's backtrace ignores velocities inside obstacles
+def test_predict_backtrace_ignores_obstacle_velocity():
+    fl = orc.OracleFluid(_uniform_box(8), rho=1000.0, mu=0.0)
+    fl.obstacle[3, 4, 4] = 1
+    fl.velocity[...] = 0.0
+    fl.velocity[..., 0] = -4.0
+    fl.velocity[3, 4, 4, :] = 0.0
+    fl.predict(1.0 / 64.0)
+    assert float(fl.velocity[2, 4, 4, 0]) == pytest.approx(-4.0, abs=1e-5)
+    np.testing.assert_allclose(fl.velocity[3, 4, 4], (0.0, 0.0, 0.0), atol=1e-7)
