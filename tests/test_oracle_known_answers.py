@@ -950,3 +950,45 @@ def test_predict_backtrace_ignores_obstacle_velocity():
     fl.predict(1.0 / 64.0)
     assert float(fl.velocity[2, 4, 4, 0]) == pytest.approx(-4.0, abs=1e-5)
     np.testing.assert_allclose(fl.velocity[3, 4, 4], (0.0, 0.0, 0.0), atol=1e-7)
+
+
+# --------------------------------------------------------------------------
+# Marker tractions and forces (tests/test_hibm.py:109-410 of the reference)
+# --------------------------------------------------------------------------
+def _markers_at(positions, normals, areas, regions):
+    return orc.OracleMarkers(x=np.asarray(positions, np.float32), normal=np.asarray(normals, np.float32),
+                             area=np.asarray(areas, np.float32), region=np.asarray(regions, np.int32))
+
+
+# test_hibm.py:109 per-marker force from traction and area
+def test_marker_force_is_traction_times_area():
+    m = _markers_at([(0.0, 0.0, 0.0), (1.0, 0.0, 0.0)], [(0.0, 0.0, 1.0), (0.0, 1.0, 0.0)], [0.5, 0.25], [101, 202])
+    m.t[0], m.t[1] = (2.0, 0.0, -4.0), (0.0, 8.0, 0.0)
+    m.compute_forces()
+    assert tuple(m.F[0]) == (1.0, 0.0, -2.0)
+    assert tuple(m.F[1]) == (0.0, 2.0, 0.0)
+
+
+# test_hibm.py:336 a uniform pressure samples the full stress traction -p n
+def test_uniform_pressure_samples_minus_p_n():
+    fl = _fluid(_uniform_box(8))
+    fl.pressure[...] = 7.0
+    m = _markers_at([(0.625, 0.625, 0.5)], [(1.0, 0.0, 0.0)], [0.5], [101])
+    rep = m.sample_tractions(fl)
+    m.compute_forces()
+    assert rep.valid == 1 and rep.invalid == 0
+    assert tuple(m.t[0]) == (-7.0, 0.0, 0.0)
+    assert tuple(m.F[0]) == (-3.5, 0.0, 0.0)
+
+
+# test_hibm.py:374 a two-sided thin wall samples the pressure jump, not the centre average
+def test_two_sided_wall_samples_the_pressure_jump():
+    fl = _fluid(_uniform_box(8))
+    fl.pressure[:, :, :4] = 2.0
+    fl.pressure[:, :, 4:] = 10.0
+    m = _markers_at([(0.625, 0.625, 0.5)], [(0.0, 0.0, 1.0)], [1.0], [101])
+    rep = m.sample_tractions(fl, two_sided=1)
+    m.compute_forces()
+    assert rep.valid == 1 and rep.invalid == 0 and rep.two_sided == 1
+    assert tuple(m.t[0]) == (0.0, 0.0, -8.0)
+    assert tuple(m.F[0]) == (0.0, 0.0, -8.0)
