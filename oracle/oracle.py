@@ -513,6 +513,27 @@ def ib_build_boundary_conditions(search: dict, *, markers_v, markers_n, marker_g
     return out
 
 
+def outlet_reachability(obstacle, *, velocity_dirichlet_active=None, barrier=None, variant: str = "mirror") -> dict:
+    """z-min outlet pressure reachability and the unreached components
+    (fluid.py:1649-1876, 4764-4910): per-cell reachable flags, component
+    labels (-(rank + 1) for unreached cells, 1 << 30 elsewhere), the unreached
+    count, component count, sweep count and convergence flags."""
+    lib = load(variant)
+    obs = np.ascontiguousarray(obstacle, np.int32)
+    nx, ny, nz = obs.shape
+    vd = None if velocity_dirichlet_active is None else np.ascontiguousarray(velocity_dirichlet_active, np.int32)
+    br = None if barrier is None else np.ascontiguousarray(barrier, np.int32)
+    reach = np.zeros(obs.shape, np.int32)
+    label = np.zeros(obs.shape, np.int32)
+    info = np.zeros(5, np.int64)
+    lib.efo_outlet_reachability.restype = c_int64
+    unreached = lib.efo_outlet_reachability(c_int(nx), c_int(ny), c_int(nz), _p(obs), _p(vd), _p(br), _p(reach),
+                                            _p(label), _p(info))
+    return {"reachable": reach, "label": label, "unreached": int(unreached), "components": int(info[0]),
+            "sweeps": int(info[1]), "converged": bool(info[2]), "labels_converged": bool(info[3]),
+            "overflow": bool(info[4])}
+
+
 VD_REPORT_KEYS = (
     "active_velocity_dirichlet_rows", "inactive_obstacle_rows", "max_abs_velocity_mps",
     "invalid_reconstruction_row_count", "invalid_no_fluid_sample_row_count", "invalid_nonpositive_gap_row_count",

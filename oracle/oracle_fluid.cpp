@@ -1078,3 +1078,133 @@ EFO_API void efo_fv_interface_coupling(const efo_level* Lp, const int32_t* obs, 
         }
       }
 }
+
+// ---------------------------------------------------------------------------
+// z-min outlet pressure reachability and the unreached components
+// (CartesianFluidSolver.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells,
+// fluid.py:1649-1876, 4764-4910).  Restated as the reference's Jacobi sweeps:
+// seed the fluid z = 0 cells, expand until nothing changes (a cell joins from a
+// reached neighbour through a face whose upper cell has no Dirichlet row and
+// no barrier), then label the unreached fluid cells with the smallest linear
+// index of their component (same face rule, min-label sweeps in place) and
+// number the components by increasing raw label, stored as -(rank + 1).
+// Outputs: reachable (0/1) and label per cell; returns the unreached count,
+// and component count / sweeps / convergence through `info`
+// (info[0] components, [1] reachability sweeps, [2] converged, [3] labels
+// converged, [4] component overflow).
+// ---------------------------------------------------------------------------
+EFO_API int64_t efo_outlet_reachability(int nx, int ny, int nz, const int32_t* obs, const int32_t* vdir,
+                                        const int32_t* barrier, int32_t* reach, int32_t* label, int64_t* info) {
+  const int64_t n = (int64_t)nx * ny * nz;
+  auto at = [&](const int32_t* a, int i, int j, int k) { return a == nullptr ? 0 : a[efo_idx(i, j, k, ny, nz)]; };
+  // face (lower, upper) between cell c and its neighbour, passable iff the
+  // upper cell has no Dirichlet row and no barrier (fluid.py:1649-1698)
+  auto face_open = [&](int ui, int uj, int uk) { return at(vdir, ui, uj, uk) == 0 && at(barrier, ui, uj, uk) == 0; };
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k)
+        reach[efo_idx(i, j, k, ny, nz)] =
+            (at(obs, i, j, k) == 0 && at(barrier, i, j, k) == 0 && k == 0 && at(vdir, i, j, k) == 0) ? 1 : 0;
+  const int64_t max_sweeps = std::max<int64_t>(1, 32 * (int64_t)(nx + ny + nz));
+  std::vector<int32_t> next(reach, reach + n);
+  int64_t sweeps = 0;
+  bool converged = false;
+  for (int64_t s = 0; s < max_sweeps; ++s) {
+    int64_t changed = 0;
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k) {
+          const int64_t c = efo_idx(i, j, k, ny, nz);
+          int32_t r = reach[c];
+          if (at(obs, i, j, k) == 0 && at(barrier, i, j, k) == 0 && r == 0) {
+            const bool hit = (i > 0 && at(reach, i - 1, j, k) != 0 && face_open(i, j, k)) ||
+                             (i < nx - 1 && at(reach, i + 1, j, k) != 0 && face_open(i + 1, j, k)) ||
+                             (j > 0 && at(reach, i, j - 1, k) != 0 && face_open(i, j, k)) ||
+                             (j < ny - 1 && at(reach, i, j + 1, k) != 0 && face_open(i, j + 1, k)) ||
+                             (k > 0 && at(reach, i, j, k - 1) != 0 && face_open(i, j, k)) ||
+                             (k < nz - 1 && at(reach, i, j, k + 1) != 0 && face_open(i, j, k + 1));
+            if (hit) {
+              r = 1;
+              changed += 1;
+            }
+          }
+          next[c] = r;
+        }
+    std::copy(next.begin(), next.end(), reach);
+    sweeps += 1;
+    if (changed == 0) {
+      converged = true;
+      break;
+    }
+  }
+  int64_t unreached = 0;
+  auto open_cell = [&](int i, int j, int k) {
+    return at(obs, i, j, k) == 0 && at(barrier, i, j, k) == 0 && at(reach, i, j, k) == 0;
+  };
+  const int32_t none = 1 << 30;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const int64_t c = efo_idx(i, j, k, ny, nz);
+        label[c] = open_cell(i, j, k) ? (int32_t)c : none;
+        if (open_cell(i, j, k)) unreached += 1;
+      }
+  int64_t components = 0;
+  bool labels_converged = true, overflow = false;
+  if (unreached > 0) {
+    labels_converged = false;
+    // fluid.py:4776-4845: a neighbour contributes through a face whose upper
+    // cell has no barrier and no Dirichlet row, if it is fluid and unreached
+    auto nb_ok = [&](int ni, int nj, int nk, int ui, int uj, int uk) {
+      return at(obs, ni, nj, nk) == 0 && at(barrier, ui, uj, uk) == 0 && at(reach, ni, nj, nk) == 0 &&
+             at(vdir, ui, uj, uk) == 0;
+    };
+    for (int64_t s = 0; s < max_sweeps; ++s) {
+      int64_t changed = 0;
+      for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+          for (int k = 0; k < nz; ++k) {
+            if (!open_cell(i, j, k)) continue;
+            const int64_t c = efo_idx(i, j, k, ny, nz);
+            int32_t best = label[c];
+            if (i > 0 && nb_ok(i - 1, j, k, i, j, k)) best = std::min(best, label[efo_idx(i - 1, j, k, ny, nz)]);
+            if (i < nx - 1 && nb_ok(i + 1, j, k, i + 1, j, k))
+              best = std::min(best, label[efo_idx(i + 1, j, k, ny, nz)]);
+            if (j > 0 && nb_ok(i, j - 1, k, i, j, k)) best = std::min(best, label[efo_idx(i, j - 1, k, ny, nz)]);
+            if (j < ny - 1 && nb_ok(i, j + 1, k, i, j + 1, k))
+              best = std::min(best, label[efo_idx(i, j + 1, k, ny, nz)]);
+            if (k > 0 && nb_ok(i, j, k - 1, i, j, k)) best = std::min(best, label[efo_idx(i, j, k - 1, ny, nz)]);
+            if (k < nz - 1 && nb_ok(i, j, k + 1, i, j, k + 1))
+              best = std::min(best, label[efo_idx(i, j, k + 1, ny, nz)]);
+            if (best < label[c]) {
+              label[c] = best;
+              changed += 1;
+            }
+          }
+      if (changed == 0) {
+        labels_converged = true;
+        break;
+      }
+    }
+    // fluid.py:4885-4910: rank the raw labels; up to 256 components
+    std::vector<int32_t> raw;
+    for (int64_t c = 0; c < n; ++c)
+      if (label[c] >= 0 && label[c] < none) raw.push_back(label[c]);
+    std::sort(raw.begin(), raw.end());
+    raw.erase(std::unique(raw.begin(), raw.end()), raw.end());
+    const int64_t capacity = 256;  // HIBM_PRESSURE_COMPONENT_CAPACITY (fluid.py:17)
+    components = std::min<int64_t>((int64_t)raw.size(), capacity);
+    overflow = (int64_t)raw.size() > capacity;
+    for (int64_t c = 0; c < n; ++c) {
+      if (!(label[c] >= 0 && label[c] < none)) continue;
+      const auto it = std::lower_bound(raw.begin(), raw.begin() + components, label[c]);
+      if (it != raw.begin() + components && *it == label[c]) label[c] = -(int32_t)(it - raw.begin()) - 1;
+    }
+  }
+  info[0] = components;
+  info[1] = sweeps;
+  info[2] = converged ? 1 : 0;
+  info[3] = labels_converged ? 1 : 0;
+  info[4] = overflow ? 1 : 0;
+  return unreached;
+}

@@ -992,3 +992,59 @@ def test_two_sided_wall_samples_the_pressure_jump():
     assert rep.valid == 1 and rep.invalid == 0 and rep.two_sided == 1
     assert tuple(m.t[0]) == (0.0, 0.0, -8.0)
     assert tuple(m.F[0]) == (0.0, 0.0, -8.0)
+
+
+# --------------------------------------------------------------------------
+# z-min outlet reachability (fluid.py:1649-1876), tests/test_core_fluid.py:2243-2472
+# --------------------------------------------------------------------------
+# test_core_fluid.py:2243 a component cut off from the outlet is counted, not frozen
+def test_outlet_reachability_counts_the_cut_off_layers():
+    obs = np.zeros((5, 5, 5), np.int32)
+    obs[:, :, 2] = 1
+    vd = np.zeros((5, 5, 5), np.int32)
+    vd[2, 2, 4] = 1
+    r = orc.outlet_reachability(obs, velocity_dirichlet_active=vd)
+    assert r["unreached"] == 50 and r["converged"]
+    assert r["reachable"][:, :, :2].all() and not r["reachable"][:, :, 3:].any()
+    assert r["components"] == 1
+
+
+# test_core_fluid.py:2450 the fill reaches its fixed point along a long serpentine path
+def test_outlet_reachability_reaches_the_end_of_a_long_path():
+    obs = np.zeros((16, 4, 16), np.int32)
+    obs[:, :, 4] = 1
+    obs[15, :, 4] = 0
+    obs[:, :, 8] = 1
+    obs[0, :, 8] = 0
+    obs[:, :, 12] = 1
+    obs[15, :, 12] = 0
+    r = orc.outlet_reachability(obs)
+    assert r["unreached"] == 0 and r["converged"]
+    assert r["reachable"][8, 1, 15] == 1
+
+
+# test_core_fluid.py:2307 separate pockets become separate components
+def test_outlet_reachability_labels_separate_pockets():
+    obs = np.ones((9, 4, 9), np.int32)
+    obs[:, :, 0] = 0
+    obs[2, 2, 4] = 0
+    obs[2, 2, 5] = 0
+    obs[6, 2, 6] = 0
+    r = orc.outlet_reachability(obs)
+    assert r["unreached"] == 3 and r["components"] == 2 and not r["overflow"]
+    # components ranked by their smallest linear cell index
+    assert r["label"][2, 2, 4] == r["label"][2, 2, 5] == -1
+    assert r["label"][6, 2, 6] == -2
+
+
+def test_outlet_reachability_faces_follow_the_upper_cell():
+    """A Dirichlet row closes the faces on its lower sides only
+    (fluid.py:1649-1698): the row cell joins through its upper z face."""
+    obs = np.zeros((1, 1, 4), np.int32)
+    vd = np.zeros((1, 1, 4), np.int32)
+    vd[0, 0, 1] = 1
+    r = orc.outlet_reachability(obs, velocity_dirichlet_active=vd)
+    # k = 0 is seeded; the face (0, 1) is closed by the row at k = 1, so k = 1
+    # is reached only from k = 2, which has no way in: nothing above k = 0
+    assert r["reachable"][0, 0].tolist() == [1, 0, 0, 0]
+    assert r["unreached"] == 3
