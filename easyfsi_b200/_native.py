@@ -114,6 +114,10 @@ class IbVdFields(Structure):  # efsi_ib_vd_fields
                 ("anchor_cell", c_void_p), ("marker_region_id", c_void_p), ("report", c_void_p)]
 
 
+class ReachReport(Structure):  # efsi_reach_report
+    _fields_ = [("unreached_cells", ctypes.c_int64), ("components", c_int32), ("overflow", c_int32)]
+
+
 class MpmState(Structure):
     _fields_ = [
         ("particle_count", c_int32),
@@ -196,6 +200,9 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_ib_reset_anchor_cells": [P, ctypes.c_int64, P],
     "efsi_ib_build_boundary_conditions": [ctypes.c_int64, P, P, P, P, P, P, P, I, P, P, P, P, P, P],
     "efsi_ib_velocity_dirichlet_rows": [P, POINTER(IbVdParams), POINTER(IbVdFields), I, P],
+    "efsi_reach_plan_create": [POINTER(c_void_p)],
+    "efsi_reach_plan_destroy": [P],
+    "efsi_outlet_reachability": [P, I, I, I, P, P, P, P, I, I, P, P, POINTER(ReachReport), P],
 }
 
 _lib = None

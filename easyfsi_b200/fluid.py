@@ -281,6 +281,13 @@ class CartesianFluidSolver:
             except Exception:
                 pass
             self._plan = None
+        reach = getattr(self, "_reach_plan", None)
+        if reach is not None and reach.value:
+            try:
+                _native.load().efsi_reach_plan_destroy(reach)
+            except Exception:
+                pass
+            self._reach_plan = None
 
     # ------------------------------------------------------------------
     # helpers
@@ -331,6 +338,67 @@ class CartesianFluidSolver:
             _stream(),
         )
         self._structure_cache = key
+
+    def mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(
+        self, *, pressure_outlet_zmin: bool = False, node_kind_code=None, barrier_node_code: int = 0,
+        use_existing_reachability_barrier: bool = False,
+    ) -> int:
+        """fluid.py:1771-1876: z-min outlet pressure reachability of the fluid
+        cells, and the unreached cells' components (labels -(rank + 1) in
+        ``hibm_pressure_unreached_component_label``).  Unreached cells are
+        neither masked nor changed.  ``efsi_outlet_reachability`` computes both
+        with one union-find (``last_hibm_pressure_reachability_sweeps`` is 1);
+        the reference's opt-in checksum reuse is not provided."""
+        if getattr(self, "hibm_pressure_outlet_reachable", None) is None:
+            shape = self.obstacle.shape
+            self.hibm_pressure_outlet_reachable = Field(shape, i32, device=self.device)
+            self.hibm_pressure_unreached_component_label = Field(shape, i32, device=self.device)
+            self.hibm_pressure_reachability_barrier = Field(shape, i32, device=self.device)
+            handle = c_void_p()
+            _native.call("efsi_reach_plan_create", byref(handle))
+            self._reach_plan = handle
+        self.last_hibm_pressure_reachability_reused = False
+        self.last_hibm_pressure_component_labels_converged = True
+        self.last_hibm_unreached_cells_with_interface_diagonal = 0
+        self.last_hibm_unreached_cells_with_interface_coupling = 0
+        self.last_hibm_unreached_components_with_interface_hits = 0
+        self.last_hibm_pressure_unreached_component_overflow = False
+        if not pressure_outlet_zmin:
+            if not use_existing_reachability_barrier:
+                self.hibm_pressure_reachability_barrier.tensor.zero_()
+            self.last_hibm_pressure_unreached_cell_count = 0
+            self.last_hibm_pressure_reachability_converged = True
+            self.last_hibm_pressure_reachability_sweeps = 0
+            self._hibm_pressure_unreached_count = 0
+            self.last_hibm_pressure_unreached_component_count = 0
+            self._hibm_pressure_unreached_component_count = 0
+            return 0
+        kind_ptr = None
+        update = 0 if use_existing_reachability_barrier else 1
+        if update and node_kind_code is not None:
+            kind = node_kind_code.tensor if isinstance(node_kind_code, Field) else torch.as_tensor(node_kind_code)
+            if tuple(kind.shape) != tuple(self.obstacle.shape):
+                raise ValueError(
+                    f"node_kind_code shape {tuple(kind.shape)} does not match the fluid cell grid "
+                    f"{tuple(self.obstacle.shape)}"
+                )
+            kind = kind.to(device=self.device, dtype=torch.int32).contiguous()
+            kind_ptr = kind.data_ptr()
+        rep = _native.ReachReport()
+        _native.call(
+            "efsi_outlet_reachability", self._reach_plan, *self.obstacle.shape, self.obstacle.ptr(),
+            self.velocity_dirichlet_boundary_active.ptr(), self.hibm_pressure_reachability_barrier.ptr(), kind_ptr,
+            int(barrier_node_code), update, self.hibm_pressure_outlet_reachable.ptr(),
+            self.hibm_pressure_unreached_component_label.ptr(), byref(rep), current_stream_handle())
+        unreached = int(rep.unreached_cells)
+        self.last_hibm_pressure_unreached_cell_count = unreached
+        self.last_hibm_pressure_reachability_converged = True
+        self.last_hibm_pressure_reachability_sweeps = 1
+        self._hibm_pressure_unreached_count = unreached
+        self.last_hibm_pressure_unreached_component_count = int(rep.components)
+        self._hibm_pressure_unreached_component_count = int(rep.components)
+        self.last_hibm_pressure_unreached_component_overflow = bool(rep.overflow)
+        return unreached
 
     def _as_f64(self, field: Field) -> torch.Tensor:
         return field.tensor if field.dtype == f64 else field.tensor.to(torch.float64).contiguous()
@@ -928,6 +996,10 @@ class CartesianFluidSolver:
             )
         report = bool(read_report)
         outlet = bool(pressure_outlet_zmin)
+        if outlet and self._hibm_pressure_unreached_count > 0:
+            raise NotImplementedError(
+                "the set-restricted mean projection of outlet-unreached components is not built on the B200 path"
+            )
         self.last_divergence_report_host_reads = 0
         self._refresh_structure()
         iface_active = self._iface_active

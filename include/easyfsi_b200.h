@@ -35,6 +35,7 @@ typedef struct efsi_fv_plan efsi_fv_plan;
 typedef struct efsi_mpm_plan efsi_mpm_plan;
 typedef struct efsi_bin_plan efsi_bin_plan;
 typedef struct efsi_ib_search_plan efsi_ib_search_plan;
+typedef struct efsi_reach_plan efsi_reach_plan;
 
 /* Last error message of the calling thread (never NULL). */
 const char* efsi_last_error(void);
@@ -475,6 +476,29 @@ int efsi_ib_velocity_dirichlet_rows(efsi_ib_search_plan* plan, const efsi_ib_vd_
 /* hibm_mpm.py:5463-5475 _reset_node_anchor_cells_kernel: every node's
  * anchor cell (3 int32 each) to (-1, -1, -1). */
 int efsi_ib_reset_anchor_cells(int32_t* anchor_cells, int64_t node_count, void* stream);
+
+/* Report of efsi_outlet_reachability. */
+typedef struct efsi_reach_report {
+  int64_t unreached_cells;
+  int32_t components; /* ranked components, at most 256 */
+  int32_t overflow;   /* more than 256 components */
+} efsi_reach_report;
+
+int efsi_reach_plan_create(efsi_reach_plan** out);
+int efsi_reach_plan_destroy(efsi_reach_plan* plan);
+
+/* fluid.py:1614-1876 mark_hibm_pressure_outlet_disconnected_nonprojectable_cells
+ * (reachability part) with fluid.py:4764-4910 (unreached component labels):
+ * the z-min outlet reachability of every fluid, non-barrier cell, and the
+ * unreached components' labels (-(rank + 1) by smallest cell index, up to
+ * 256; 1 << 30 for reached and non-fluid cells).  With update_barrier the
+ * barrier field is first set from node_kind == barrier_code (node_kind NULL:
+ * cleared), fluid.py:1618-1647.  One union-find over the open faces instead
+ * of the reference's Jacobi sweeps; synchronises the stream twice. */
+int efsi_outlet_reachability(efsi_reach_plan* plan, int32_t nx, int32_t ny, int32_t nz, const int32_t* obstacle,
+                             const int32_t* velocity_dirichlet_active, int32_t* barrier, const int32_t* node_kind,
+                             int32_t barrier_code, int32_t update_barrier, int32_t* reachable, int32_t* label,
+                             efsi_reach_report* report, void* stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

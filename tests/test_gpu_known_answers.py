@@ -502,3 +502,64 @@ def test_vd_rows_fall_back_along_the_line_of_sight(node, bp, ip, value, weight):
     np.testing.assert_allclose(fluid.velocity_dirichlet_boundary_value_mps[node], (value, 0.0, 0.0), atol=1e-6)
     if weight is not None:
         assert fluid.velocity_dirichlet_boundary_projection_weight[node] == pytest.approx(weight, abs=1e-6)
+
+
+# --------------------------------------------------------------------------
+# z-min outlet reachability (fluid.py:1771-1876) through the drop-in solver;
+# the oracle side passes in tests/test_oracle_known_answers.py.
+# --------------------------------------------------------------------------
+_REACH_NOT_YET_ON_GPU = pytest.mark.skip(reason="reachability kernels not yet run on a B200")
+
+
+def _box_solver(nodes):
+    from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
+
+    return CartesianFluidSolver(FluidDomainSpec.unit_box(grid_nodes=nodes, dt_s=1.0e-3))
+
+
+# test_core_fluid.py:2243
+@_REACH_NOT_YET_ON_GPU
+def test_outlet_reachability_counts_the_cut_off_layers():
+    s = _box_solver((5, 5, 5))
+    obs = np.zeros((5, 5, 5), np.int32)
+    obs[:, :, 2] = 1
+    s.obstacle.from_numpy(obs)
+    s.velocity_dirichlet_boundary_active[2, 2, 4] = 1
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 50
+    assert s.last_hibm_pressure_unreached_cell_count == 50 and s.last_hibm_pressure_reachability_converged
+    assert (s.obstacle.to_numpy()[:, :, 3:] == 0).all()
+    with pytest.raises(NotImplementedError):
+        s.project(iterations=10, pressure_outlet_zmin=True, pressure_solver="fv_cg")
+
+
+# test_core_fluid.py:2450
+@_REACH_NOT_YET_ON_GPU
+def test_outlet_reachability_reaches_the_end_of_a_long_path():
+    s = _box_solver((16, 4, 16))
+    obs = np.zeros((16, 4, 16), np.int32)
+    obs[:, :, 4] = 1
+    obs[15, :, 4] = 0
+    obs[:, :, 8] = 1
+    obs[0, :, 8] = 0
+    obs[:, :, 12] = 1
+    obs[15, :, 12] = 0
+    s.obstacle.from_numpy(obs)
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 0
+    assert int(s.hibm_pressure_outlet_reachable[8, 1, 15]) == 1
+
+
+# test_core_fluid.py:2307 (reachability part)
+@_REACH_NOT_YET_ON_GPU
+def test_outlet_reachability_labels_separate_pockets():
+    s = _box_solver((9, 4, 9))
+    obs = np.ones((9, 4, 9), np.int32)
+    obs[:, :, 0] = 0
+    obs[2, 2, 4] = 0
+    obs[2, 2, 5] = 0
+    obs[6, 2, 6] = 0
+    s.obstacle.from_numpy(obs)
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 3
+    assert s.last_hibm_pressure_unreached_component_count == 2
+    assert not s.last_hibm_pressure_unreached_component_overflow
+    labels = s.hibm_pressure_unreached_component_label.to_numpy()
+    assert labels[2, 2, 4] == labels[2, 2, 5] == -1 and labels[6, 2, 6] == -2
