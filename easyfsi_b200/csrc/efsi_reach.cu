@@ -54,15 +54,23 @@ __device__ __forceinline__ bool face_open(const ReachArgs& A, int64_t u) {
   return at(A.vdir, u) == 0 && at(A.barrier, u) == 0;
 }
 
-// volatile: other threads relink roots while this one walks
-__device__ __forceinline__ int32_t find_root(const int32_t* parent_, int32_t x) {
-  const volatile int32_t* parent = parent_;
-  int32_t p = parent[x];
-  while (p != x) {
-    x = p;
-    p = parent[x];
+// The root of x, shortening the path as it walks (intermediate pointer
+// jumping, as in the ECL-CC connected-components algorithm): a parent always
+// has a smaller index than its child, so every pointer written still points
+// to an ancestor, and roots (changed only by the linking CAS) are never
+// written here.  volatile: other threads relink and shorten concurrently.
+__device__ __forceinline__ int32_t find_root(int32_t* parent_, int32_t x) {
+  volatile int32_t* parent = parent_;
+  int32_t cur = parent[x];
+  if (cur != x) {
+    int32_t prev = x, next;
+    while (cur > (next = parent[cur])) {
+      parent[prev] = next;
+      prev = cur;
+      cur = next;
+    }
   }
-  return x;
+  return cur;
 }
 
 // node_kind -> barrier (fluid.py:1618-1627), or clear it
