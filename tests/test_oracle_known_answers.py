@@ -1048,3 +1048,56 @@ def test_outlet_reachability_faces_follow_the_upper_cell():
     # is reached only from k = 2, which has no way in: nothing above k = 0
     assert r["reachable"][0, 0].tolist() == [1, 0, 0, 0]
     assert r["unreached"] == 3
+
+
+# --------------------------------------------------------------------------
+# Marker surface feedback from the MPM particles (tests/test_hibm.py:726-899)
+# --------------------------------------------------------------------------
+def _feedback_case(marker_normal, marker_area, px, pv, pn=None, pa=None, box=(1.0, 1.0, 1.0)):
+    m = _markers_at([(0.5, 0.5, 0.5)], [marker_normal], [marker_area], [202])
+    x, vol, mass = _box_particles((1, 1, 1), (0.0,) * 3, box, 1000.0)
+    s = orc.OracleSolid(capacity=1, grid_nodes=(4, 4, 4))
+    s.load(x=x, volume=vol, mass=mass, normal=None if pn is None else np.asarray([pn], np.float32),
+           area=None if pa is None else np.asarray([pa], np.float32))
+    if px is not None:
+        s.x[0] = px
+    s.v[0] = pv
+    return m, s
+
+
+# test_hibm.py:726 feedback moves the marker by the supporting particles' velocity
+def test_feedback_updates_marker_position_and_velocity():
+    m, s = _feedback_case((0.0, 0.0, 1.0), 1.0, (0.6, 0.45, 0.7), (1.0, -2.0, 3.0))
+    rep = m.feedback(s, 0.5, 0.1, geometry=False)
+    assert rep.updated == 1 and rep.invalid == 0
+    np.testing.assert_allclose(m.x[0], (0.6, 0.3, 0.8), atol=1e-6)
+    np.testing.assert_allclose(m.v[0], (1.0, -2.0, 3.0), atol=1e-6)
+
+
+# test_hibm.py:770 feedback takes the particles' surface normal and area
+def test_feedback_updates_marker_normal_and_area():
+    m, s = _feedback_case((0.0, 0.0, 1.0), 0.25, (0.6, 0.45, 0.7), (1.0, -2.0, 3.0), pn=(0.0, 2.0, 0.0), pa=0.75)
+    rep = m.feedback(s, 0.5, 0.1, geometry=True)
+    assert rep.updated == 1 and rep.invalid == 0 and rep.geometry_updated == 1
+    assert tuple(m.n[0]) == (0.0, 1.0, 0.0)
+    assert float(m.A[0]) == pytest.approx(0.75, abs=1e-6)
+    assert rep.max_area_change == pytest.approx(0.5, abs=1e-6)
+    assert rep.max_normal_change > 0.0
+
+
+# test_hibm.py:817 the marker advances by velocity, not to the particle centroid
+def test_feedback_advances_by_velocity_not_to_the_centroid():
+    m, s = _feedback_case((0.0, 0.0, 1.0), 0.25, (0.9, 0.5, 0.5), (0.1, 0.0, 0.0), pn=(0.0, 0.0, 1.0), pa=0.25)
+    rep = m.feedback(s, 0.5, 0.1, geometry=True)
+    assert rep.updated == 1 and rep.invalid == 0
+    np.testing.assert_allclose(m.x[0], (0.51, 0.5, 0.5), atol=1e-6)
+    np.testing.assert_allclose(m.v[0], (0.1, 0.0, 0.0), atol=1e-6)
+    assert rep.max_displacement == pytest.approx(0.01, abs=1e-6)
+
+
+# test_hibm.py:864 a marker without supporting particles is recorded invalid and kept
+def test_feedback_records_unsupported_marker_invalid():
+    m, s = _feedback_case((0.0, 1.0, 0.0), 1.0, None, (0.0, 0.0, 0.0), box=(0.2, 0.2, 0.2))
+    rep = m.feedback(s, 0.1, 0.1, geometry=False)
+    assert rep.updated == 0 and rep.invalid == 1
+    assert tuple(m.x[0]) == (0.5, 0.5, 0.5) and tuple(m.v[0]) == (0.0, 0.0, 0.0)
