@@ -14,6 +14,10 @@
 // first triangle that sees them outside, since that alone makes the node
 // "none" whatever the remaining triangles give.
 //
+// The same file holds the consumers of the search: the boundary-condition
+// targets of the external IB nodes and the velocity-Dirichlet row assemblies
+// (HibmMpmIbBoundaryConditions, hibm_mpm.py:6222-7800).
+//
 // Geometry runs in f32 with the reference's order of operations.  This file
 // is compiled with -fmad=false, so no product is fused into a sum and the
 // results round exactly as the expressions read.

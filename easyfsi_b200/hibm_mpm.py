@@ -10,8 +10,10 @@ signatures: ``load_markers`` (:553), ``set_marker_tractions_pa`` (:893),
 updates (:5055, :5182).  Every method accepts an extra ``read_report=False``
 keyword that skips the host read of its report (the report is then ``None``).
 
-Projection triangles (``set_projection_triangles`` :590) and the IB node
-search (class ``HibmMpmIbNodeSearch`` :5385) are provided too.  The viscous /
+Projection triangles (``set_projection_triangles`` :590), the IB node search
+(class ``HibmMpmIbNodeSearch`` :5385) and the boundary-condition targets and
+velocity-Dirichlet rows built from it (class ``HibmMpmIbBoundaryConditions``
+:6222, without its pressure-Neumann rows) are provided too.  The viscous /
 closure stress sampler of the reference is outside the hot path and not
 provided.
 """
