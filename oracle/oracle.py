@@ -232,6 +232,28 @@ class OracleFluid:
                                            _p(owner), _p(nbr), _p(trans))
         return out
 
+    def multigrid_solve(self, *, outlet: int, iterations: int, cycles: int) -> None:
+        """fluid.py fv_multigrid solve of the prepared rhs (efo_fv_multigrid_solve)."""
+        self.lib.efo_fv_multigrid_solve(c_int(len(self.levels)), self.levels, _p(self.obstacle), None, None, None,
+                                        _p(self.rhs0), _p(self.pressure), c_int(outlet), c_int(iterations),
+                                        c_int(cycles), c_int(1 if self.uniform else 0))
+
+    def project_outlet_multigrid(self, *, dt: float, iterations: int, cycles: int) -> None:
+        """project(pressure_outlet_zmin=True, reset_pressure=True,
+        pressure_solver="fv_multigrid") without Dirichlet rows (fluid.py:7190-7260):
+        boundary conditions, divergence, rhs with the volume source, the MG
+        solve, the gradient correction and the boundary conditions again."""
+        self.apply_closed_boundary(1)
+        self.apply_zmin_no_backflow()
+        self.compute_divergence(1)
+        self.pressure[...] = 0.0
+        self.prepare_rhs(self.rho / dt)
+        self.multigrid_solve(outlet=1, iterations=iterations, cycles=cycles)
+        self.subtract_pressure_gradient(dt / self.rho, 1)
+        self.apply_closed_boundary(1)
+        self.apply_zmin_no_backflow()
+        self.compute_divergence(1)
+
     def apply_closed_boundary(self, outlet: int = 0) -> None:
         """fluid.py:5529-5536: the normal velocity on the min faces is zeroed (z-min kept with the outlet)."""
         self.lib.efo_apply_closed_boundary(byref(self.levels[0]), c_int(outlet), _p(self.velocity))

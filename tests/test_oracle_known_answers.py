@@ -1101,3 +1101,20 @@ def test_feedback_records_unsupported_marker_invalid():
     rep = m.feedback(s, 0.1, 0.1, geometry=False)
     assert rep.updated == 0 and rep.invalid == 1
     assert tuple(m.x[0]) == (0.5, 0.5, 0.5) and tuple(m.v[0]) == (0.0, 0.0, 0.0)
+
+
+# test_core_fluid.py:1292 the pressure outlet balances an explicit volume source
+def test_pressure_outlet_balances_a_volume_source():
+    n = 16
+    fl = _fluid(_uniform_box(n))
+    cell_volume = 1.0 / n ** 3
+    total = 2.0e-6
+    fl.volume_source[7:9, 7:9, 10:12] = np.float32(total / (8.0 * cell_volume))
+    fl.velocity[...] = 0.0
+    fl.project_outlet_multigrid(dt=1.0e-3, iterations=8, cycles=8)
+    area = (1.0 / n) ** 2
+    outlet_flux = float(np.sum(-np.asarray(fl.velocity, np.float64)[:, :, 0, 2]) * area)
+    residual = float(np.sum((np.asarray(fl.divergence, np.float64) - np.asarray(fl.volume_source, np.float64))
+                            * cell_volume))
+    assert outlet_flux == pytest.approx(total, abs=total * 0.08)
+    assert residual == pytest.approx(0.0, abs=total * 0.02)
