@@ -243,12 +243,23 @@ class OracleFluid:
         pressure_solver="fv_multigrid") without Dirichlet rows (fluid.py:7190-7260):
         boundary conditions, divergence, rhs with the volume source, the MG
         solve, the gradient correction and the boundary conditions again."""
+        self._project_outlet(dt, lambda: self.multigrid_solve(outlet=1, iterations=iterations, cycles=cycles))
+
+    def project_outlet_cg(self, *, dt: float, max_iters: int, tol: float, precond: int = 1) -> CgStats:
+        """The same with pressure_solver="fv_cg" (flexible PCG, outlet rows,
+        no mean projection)."""
+        out = []
+        self._project_outlet(dt, lambda: out.append(
+            self.pcg_solve(outlet=1, max_iters=max_iters, tol=tol, precond=precond, remove_mean=False)))
+        return out[0]
+
+    def _project_outlet(self, dt: float, solve) -> None:
         self.apply_closed_boundary(1)
         self.apply_zmin_no_backflow()
         self.compute_divergence(1)
         self.pressure[...] = 0.0
         self.prepare_rhs(self.rho / dt)
-        self.multigrid_solve(outlet=1, iterations=iterations, cycles=cycles)
+        solve()
         self.subtract_pressure_gradient(dt / self.rho, 1)
         self.apply_closed_boundary(1)
         self.apply_zmin_no_backflow()

@@ -1118,3 +1118,21 @@ def test_pressure_outlet_balances_a_volume_source():
                             * cell_volume))
     assert outlet_flux == pytest.approx(total, abs=total * 0.08)
     assert residual == pytest.approx(0.0, abs=total * 0.02)
+
+
+# test_core_fluid.py:1591 (CG part) the non-uniform outlet CG converges and balances the source
+def test_nonuniform_outlet_cg_converges_and_balances_the_source():
+    widths = tuple(0.02 * (1.0 + 0.15 * ((i % 4) / 3.0)) for i in range(24))
+    fl = _nonuniform_fluid(widths, widths, widths)
+    assert len(fl.metrics) >= 4
+    vol = _cell_volumes(fl)
+    total = 2.0e-6
+    cells = np.s_[11:13, 11:13, 18:20]
+    fl.volume_source[cells] = np.float32(total / float(np.sum(vol[cells])))
+    fl.velocity[...] = 0.0
+    st = fl.project_outlet_cg(dt=1.0e-3, max_iters=160, tol=1.0e-6)
+    assert st.converged and st.iterations < 160
+    w = [np.asarray(m["w"], np.float32).astype(np.float64) for m in fl.metrics[0]]
+    area = np.outer(w[0], w[1])
+    outlet_flux = float(np.sum(-np.asarray(fl.velocity, np.float64)[:, :, 0, 2] * area))
+    assert abs(1.0 - outlet_flux / total) < 1.0e-3
