@@ -245,6 +245,16 @@ class OracleFluid:
         solve, the gradient correction and the boundary conditions again."""
         self._project_outlet(dt, lambda: self.multigrid_solve(outlet=1, iterations=iterations, cycles=cycles))
 
+    def project_outlet_jacobi(self, *, dt: float, iterations: int) -> None:
+        """The same with pressure_solver="fv_jacobi": damped Jacobi sweeps
+        (omega 0.8) of the level-0 system, the one-level case of
+        efo_fv_multigrid_solve (fluid.py:5862-5900)."""
+        def solve():
+            self.lib.efo_fv_multigrid_solve(c_int(1), self.levels, _p(self.obstacle), None, None, None,
+                                            _p(self.rhs0), _p(self.pressure), c_int(1), c_int(iterations), c_int(1),
+                                            c_int(1 if self.uniform else 0))
+        self._project_outlet(dt, solve)
+
     def project_outlet_cg(self, *, dt: float, max_iters: int, tol: float, precond: int = 1) -> CgStats:
         """The same with pressure_solver="fv_cg" (flexible PCG, outlet rows,
         no mean projection)."""

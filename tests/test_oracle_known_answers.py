@@ -1136,3 +1136,23 @@ def test_nonuniform_outlet_cg_converges_and_balances_the_source():
     area = np.outer(w[0], w[1])
     outlet_flux = float(np.sum(-np.asarray(fl.velocity, np.float64)[:, :, 0, 2] * area))
     assert abs(1.0 - outlet_flux / total) < 1.0e-3
+
+
+# test_core_fluid.py:1548 an obstacle-adjacent volume source is conserved by the fv_jacobi projection
+def test_fv_jacobi_obstacle_adjacent_source_is_conserved():
+    nodes = (14, 10, 10)
+    obs = np.zeros(nodes, np.int32)
+    obs[8, 4:6, 5:7] = 1
+    fl = _fluid_with(nodes, obs)
+    cell_volume = 1.0 / (14 * 10 * 10)
+    total = 1.0e-6
+    fl.volume_source[7:8, 4:6, 5:7] = np.float32(total / (4.0 * cell_volume))
+    fl.project_outlet_jacobi(dt=1.0e-3, iterations=2400)
+    area = (1.0 / 14) * (1.0 / 10)
+    outlet_flux = float(np.sum(-np.asarray(fl.velocity, np.float64)[:, :, 0, 2]) * area)
+    active = obs == 0
+    residual = float(np.sum((np.asarray(fl.divergence, np.float64)[active]
+                             - np.asarray(fl.volume_source, np.float64)[active]) * cell_volume))
+    assert outlet_flux > 0.0
+    assert outlet_flux / total == pytest.approx(1.0, abs=0.12)
+    assert residual == pytest.approx(0.0, abs=total * 0.01)
