@@ -4,6 +4,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import pytest
+
 from easyfsi_b200 import _native
 from easyfsi_b200.build import LIB_PATH, build
 
@@ -81,3 +83,35 @@ def test_ib_entry_points_reject_bad_arguments_without_gpu():
     assert lib.efsi_ib_velocity_dirichlet_rows(fake_plan, byref(vd), byref(fields), 1, None) == 1
     assert b">= 2" in lib.efsi_last_error()
     assert lib.efsi_ib_reset_anchor_cells(None, 4, None) == 1
+
+
+def test_header_compiles_as_c99_and_cxx_and_links(tmp_path):
+    """include/easyfsi_b200.h is a plain C header: a C99 and a C++17
+    translation unit that include it compile warning-free and link against
+    the library; the C program runs (no device work)."""
+    import shutil
+    import subprocess
+
+    build()
+    src_c = tmp_path / "use.c"
+    src_c.write_text(
+        '#include <stdio.h>\n#include <string.h>\n#include "easyfsi_b200.h"\n'
+        "int main(void) {\n"
+        '  if (strstr(efsi_version(), "sm_100a") == NULL) return 1;\n'
+        "  if (efsi_mpm_plan_create(0, 4, 4, 4, NULL) != EFSI_ERR_ARG) return 2;\n"
+        '  printf("%s\\n", efsi_last_error());\n'
+        "  return 0;\n}\n"
+    )
+    src_cpp = tmp_path / "use.cpp"
+    src_cpp.write_text('#include "easyfsi_b200.h"\nint probe() { return EFSI_OK; }\n')
+    gcc, gxx = shutil.which("gcc"), shutil.which("g++")
+    if gcc is None or gxx is None:
+        pytest.skip("no host C/C++ compiler")
+    inc = str(HEADER.parent)
+    exe = tmp_path / "use"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", inc, str(src_c), "-o", str(exe),
+                    str(LIB_PATH), f"-Wl,-rpath,{LIB_PATH.parent}"], check=True, capture_output=True)
+    subprocess.run([gxx, "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", inc, "-c", str(src_cpp), "-o",
+                    str(tmp_path / "use_cpp.o")], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True)
+    assert out.stdout.strip()
