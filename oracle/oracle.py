@@ -232,6 +232,19 @@ class OracleFluid:
                                            _p(owner), _p(nbr), _p(trans))
         return out
 
+    def bicgstab(self, rhs, *, outlet: int, max_iters: int, tol: float, b_norm: float,
+                 remove_mean: bool = False) -> dict:
+        """fluid.py:6264-6533: the BiCGSTAB fallback on the level-0 system
+        A p = rhs from the current pressure (efo_bicgstab)."""
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        stats = np.zeros(4, np.int64)
+        rel = c_double(0.0)
+        self.lib.efo_bicgstab(byref(self.levels[0]), _p(self.obstacle), _p(rhs), _p(self.pressure), c_int(outlet),
+                              c_int(max_iters), c_double(tol), c_double(b_norm), c_int(1 if remove_mean else 0),
+                              _p(stats), byref(rel))
+        return {"iterations": int(stats[0]), "converged": bool(stats[1]), "restarts": int(stats[2]),
+                "breakdown": int(stats[3]), "relative_residual": rel.value}
+
     def multigrid_solve(self, *, outlet: int, iterations: int, cycles: int) -> None:
         """fluid.py fv_multigrid solve of the prepared rhs (efo_fv_multigrid_solve)."""
         self.lib.efo_fv_multigrid_solve(c_int(len(self.levels)), self.levels, _p(self.obstacle), None, None, None,

@@ -1208,3 +1208,184 @@ EFO_API int64_t efo_outlet_reachability(int nx, int ny, int nz, const int32_t* o
   info[4] = overflow ? 1 : 0;
   return unreached;
 }
+
+// ---------------------------------------------------------------------------
+// fluid.py:6264-6533 _continue_pressure_poisson_fv_bicgstab: the BiCGSTAB
+// fallback (right Jacobi preconditioning, fluid.py:4614-4661 vector kernels),
+// on the level-0 system with rhs `rhs`, from the pressure in `p`.  Every
+// breakdown restarts from the true residual until the last iteration, as the
+// reference does; remove_mean applies the zero-mean projection where the
+// reference's project_field does (no unreached-set anchoring here).
+// stats: [0] iterations, [1] converged, [2] restarts, [3] breakdown code
+// (0 none, 1 shadow dot, 2 recurrence scalar, 3 beta, 4 alpha denominator,
+// 5 alpha, 6 omega denominator, 7 omega, 8 not converged);
+// rel_res: the final relative residual.
+// ---------------------------------------------------------------------------
+EFO_API void efo_bicgstab(const efo_level* Lp, const int32_t* obs, const double* rhs, double* p, int outlet,
+                          int max_iters, double tol, double b_norm, int remove_mean, int64_t* stats,
+                          double* rel_res) {
+  const efo_level& L = *Lp;
+  const int64_t n = ncells(L);
+  std::vector<double> r(n), r_old(n), d(n, 0.0), Ad(n, 0.0), z(n, 0.0), s(n, 0.0), t(n, 0.0), diag(n);
+  fv_diagonal(L, obs, nullptr, nullptr, nullptr, diag.data(), outlet);
+  auto project = [&](double* f) {
+    if (remove_mean) subtract_mean(L, obs, f);
+  };
+  auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+    return weighted_dot(L, obs, a.data(), b.data());
+  };
+  auto true_residual = [&]() {
+    fv_apply(L, obs, nullptr, nullptr, nullptr, p, Ad.data(), outlet);
+    for (int64_t c = 0; c < n; ++c) r[c] = 1.0 * rhs[c] + -1.0 * Ad[c];
+    project(r.data());
+  };
+  auto reset = [&]() {  // fluid.py:4614-4627
+    for (int64_t c = 0; c < n; ++c) {
+      r_old[c] = obs[c] == 1 ? 0.0 : r[c];
+      d[c] = Ad[c] = s[c] = t[c] = 0.0;
+    }
+  };
+  const int iters = std::max(1, max_iters);
+  const double tolerance = std::max(0.0, tol), floor = 1.0e-300;
+  int64_t it_done = 0, restarts = 0, code = 0;
+  bool converged = false;
+  double rr;
+  true_residual();
+  rr = std::sqrt(std::max(dot(r, r), 0.0)) / b_norm;
+  if (rr <= tolerance) converged = true;
+  double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+  if (!converged) reset();
+  for (int it = 1; it <= iters && !converged; ++it) {
+    const double rho = dot(r_old, r);
+    auto restart = [&](int why) -> bool {  // true: give up
+      if (it >= iters) {
+        code = why;
+        return true;
+      }
+      return false;
+    };
+    if (!std::isfinite(rho) || std::fabs(rho) <= floor) {
+      if (restart(1)) break;
+      true_residual();
+      rr = std::sqrt(std::max(dot(r, r), 0.0)) / b_norm;
+      it_done = it;
+      if (rr <= tolerance) {
+        converged = true;
+        break;
+      }
+      reset();
+      rho_prev = alpha = omega = 1.0;
+      restarts += 1;
+      continue;
+    }
+    double beta = 0.0;
+    if (it > 1) {
+      if (!std::isfinite(rho_prev) || std::fabs(rho_prev) <= floor || !std::isfinite(omega) ||
+          std::fabs(omega) <= floor) {
+        if (restart(2)) break;
+        true_residual();
+        reset();
+        rho_prev = alpha = omega = 1.0;
+        restarts += 1;
+        continue;
+      }
+      beta = (rho / rho_prev) * (alpha / omega);
+      if (!std::isfinite(beta)) {
+        if (restart(3)) break;
+        true_residual();
+        reset();
+        rho_prev = alpha = omega = 1.0;
+        restarts += 1;
+        continue;
+      }
+    }
+    for (int64_t c = 0; c < n; ++c) d[c] = obs[c] == 1 ? 0.0 : r[c] + beta * (d[c] - omega * Ad[c]);
+    jacobi_precond(n, obs, diag.data(), d.data(), z.data());
+    project(z.data());
+    fv_apply(L, obs, nullptr, nullptr, nullptr, z.data(), Ad.data(), outlet);
+    const double alpha_den = dot(r_old, Ad);
+    if (!std::isfinite(alpha_den) || std::fabs(alpha_den) <= floor) {
+      if (restart(4)) break;
+      true_residual();
+      reset();
+      rho_prev = alpha = omega = 1.0;
+      restarts += 1;
+      continue;
+    }
+    alpha = rho / alpha_den;
+    if (!std::isfinite(alpha)) {
+      if (restart(5)) break;
+      true_residual();
+      reset();
+      rho_prev = alpha = omega = 1.0;
+      restarts += 1;
+      continue;
+    }
+    for (int64_t c = 0; c < n; ++c) {
+      if (obs[c] == 1) {
+        p[c] = 0.0;
+        s[c] = 0.0;
+      } else {
+        p[c] += alpha * z[c];
+        s[c] = r[c] - alpha * Ad[c];
+      }
+    }
+    project(s.data());
+    rr = std::sqrt(std::max(dot(s, s), 0.0)) / b_norm;
+    it_done = it;
+    if (rr <= tolerance) {
+      r = s;
+      converged = true;
+      break;
+    }
+    jacobi_precond(n, obs, diag.data(), s.data(), z.data());
+    project(z.data());
+    fv_apply(L, obs, nullptr, nullptr, nullptr, z.data(), t.data(), outlet);
+    const double ts = dot(t, s), tt = dot(t, t);
+    if (!std::isfinite(tt) || std::fabs(tt) <= floor) {
+      if (restart(6)) break;
+      r = s;
+      project(r.data());
+      reset();
+      rho_prev = alpha = omega = 1.0;
+      restarts += 1;
+      continue;
+    }
+    omega = ts / tt;
+    if (!std::isfinite(omega) || std::fabs(omega) <= floor) {
+      if (restart(7)) break;
+      r = s;
+      project(r.data());
+      reset();
+      rho_prev = alpha = omega = 1.0;
+      restarts += 1;
+      continue;
+    }
+    for (int64_t c = 0; c < n; ++c) {
+      if (obs[c] == 1) {
+        p[c] = 0.0;
+        r[c] = 0.0;
+      } else {
+        p[c] += omega * z[c];
+        r[c] = s[c] - omega * t[c];
+      }
+    }
+    if (it % 16 == 0) {
+      project(p);
+      project(r.data());
+    }
+    rr = std::sqrt(std::max(dot(r, r), 0.0)) / b_norm;
+    it_done = it;
+    if (rr <= tolerance) {
+      converged = true;
+      break;
+    }
+    rho_prev = rho;
+  }
+  if (!converged && code == 0) code = 8;
+  stats[0] = it_done;
+  stats[1] = converged ? 1 : 0;
+  stats[2] = restarts;
+  stats[3] = code;
+  *rel_res = rr;
+}

@@ -1156,3 +1156,18 @@ def test_fv_jacobi_obstacle_adjacent_source_is_conserved():
     assert outlet_flux > 0.0
     assert outlet_flux / total == pytest.approx(1.0, abs=0.12)
     assert residual == pytest.approx(0.0, abs=total * 0.01)
+
+
+# test_core_fluid.py:3713 the BiCGSTAB fallback solves a generic FV rhs
+def test_bicgstab_fallback_solves_a_generic_rhs():
+    fl = _fluid(_uniform_box(4))
+    rhs = np.zeros((4, 4, 4))
+    rhs[2, 2, 2] = 1.0
+    fl.pressure[...] = 0.0
+    b_norm = math.sqrt(max(fl.weighted_dot(rhs, rhs), 0.0))
+    st = fl.bicgstab(rhs, outlet=1, max_iters=80, tol=1.0e-8, b_norm=b_norm)
+    assert st["converged"] and st["breakdown"] == 0
+    assert st["relative_residual"] <= 1.0e-8
+    # the recurrence agrees with the true residual of the returned pressure
+    res = rhs - fl.fv_apply(np.asarray(fl.pressure), 1)
+    assert math.sqrt(fl.weighted_dot(res, res)) / b_norm <= 1.0e-7
