@@ -200,6 +200,7 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_ib_reset_anchor_cells": [P, ctypes.c_int64, P],
     "efsi_ib_build_boundary_conditions": [ctypes.c_int64, P, P, P, P, P, P, P, I, P, P, P, P, P, P],
     "efsi_ib_velocity_dirichlet_rows": [P, POINTER(IbVdParams), POINTER(IbVdFields), I, P],
+    "efsi_fv_bicgstab": [P, P, P, I, I, D, D, I, POINTER(ctypes.c_int64), POINTER(c_double), P],
     "efsi_reach_plan_create": [POINTER(c_void_p)],
     "efsi_reach_plan_destroy": [P],
     "efsi_outlet_reachability": [P, I, I, I, P, P, P, P, I, I, P, P, POINTER(ReachReport), P],

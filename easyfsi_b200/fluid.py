@@ -18,6 +18,7 @@ fields exist where the plain path reads them; their kernels are not provided.
 
 from __future__ import annotations
 
+import ctypes
 import math
 from ctypes import byref, c_double, c_void_p
 from dataclasses import dataclass
@@ -338,6 +339,40 @@ class CartesianFluidSolver:
             _stream(),
         )
         self._structure_cache = key
+
+    _BICGSTAB_BREAKDOWN_TEXT = {
+        1: "BiCGSTAB shadow residual dot is not finite",
+        2: "BiCGSTAB recurrence scalar is not finite",
+        3: "BiCGSTAB beta is not finite",
+        4: "BiCGSTAB alpha denominator is not finite",
+        5: "BiCGSTAB alpha is not finite",
+        6: "BiCGSTAB omega denominator is not finite",
+        7: "BiCGSTAB omega is not finite",
+        8: "BiCGSTAB fallback did not converge",
+    }
+
+    def _continue_pressure_poisson_fv_bicgstab(self, *, start_iteration: int, max_iters: int, b_norm: float,
+                                               outlet: int, tolerance: float, anchor_unreached: bool,
+                                               remove_nullspace_mean: bool) -> None:
+        """fluid.py:6264-6533: the BiCGSTAB fallback on ``cg_rhs`` from the
+        current pressure (``efsi_fv_bicgstab``).  The unreached-set anchoring
+        of the reference is not built."""
+        if anchor_unreached:
+            raise NotImplementedError(
+                "the set-restricted mean projection of outlet-unreached components is not built on the B200 path"
+            )
+        self.last_cg_restart_policy = "periodic_exact_residual+bicgstab_fallback"
+        self.last_cg_breakdown = ""
+        stats = (ctypes.c_int64 * 4)()
+        rel = c_double(0.0)
+        _native.call("efsi_fv_bicgstab", self._plan, self.cg_rhs.ptr(), self.pressure.ptr(), 1 if outlet else 0,
+                     max(1, int(max_iters)), max(0.0, float(tolerance)), float(b_norm),
+                     1 if remove_nullspace_mean else 0, stats, byref(rel), current_stream_handle())
+        self.last_cg_iterations = int(start_iteration) + int(stats[0])
+        self.last_cg_converged = bool(stats[1])
+        self.last_cg_restart_count = int(getattr(self, "last_cg_restart_count", 0)) + int(stats[2])
+        self.last_cg_relative_residual = float(rel.value)
+        self.last_cg_breakdown = self._BICGSTAB_BREAKDOWN_TEXT.get(int(stats[3]), "")
 
     def mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(
         self, *, pressure_outlet_zmin: bool = False, node_kind_code=None, barrier_node_code: int = 0,

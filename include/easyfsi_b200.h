@@ -477,6 +477,19 @@ int efsi_ib_velocity_dirichlet_rows(efsi_ib_search_plan* plan, const efsi_ib_vd_
  * anchor cell (3 int32 each) to (-1, -1, -1). */
 int efsi_ib_reset_anchor_cells(int32_t* anchor_cells, int64_t node_count, void* stream);
 
+/* fluid.py:6264-6533 _continue_pressure_poisson_fv_bicgstab: the BiCGSTAB
+ * fallback (right Jacobi preconditioning) of the level-0 system A p = rhs
+ * from the pressure in `pressure`, relative to b_norm; remove_mean applies
+ * the zero-mean projection where the reference does (no unreached-set
+ * anchoring).  Host loop with one host read per inner product; allocates
+ * nine work vectors for the call.  stats: int64[4] = iterations, converged,
+ * restarts, breakdown code (0 none, 1 shadow dot, 2 recurrence scalar,
+ * 3 beta, 4 alpha denominator, 5 alpha, 6 omega denominator, 7 omega,
+ * 8 not converged). */
+int efsi_fv_bicgstab(efsi_fv_plan* plan, const double* rhs, double* pressure, int32_t outlet, int32_t max_iters,
+                     double tolerance, double b_norm, int32_t remove_mean, int64_t* stats, double* relative_residual,
+                     void* stream);
+
 /* Report of efsi_outlet_reachability. */
 typedef struct efsi_reach_report {
   int64_t unreached_cells;

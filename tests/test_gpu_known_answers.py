@@ -563,3 +563,18 @@ def test_outlet_reachability_labels_separate_pockets():
     assert not s.last_hibm_pressure_unreached_component_overflow
     labels = s.hibm_pressure_unreached_component_label.to_numpy()
     assert labels[2, 2, 4] == labels[2, 2, 5] == -1 and labels[6, 2, 6] == -2
+
+
+# test_core_fluid.py:3713 the BiCGSTAB fallback solves a generic FV rhs
+@pytest.mark.skip(reason="BiCGSTAB fallback not yet run on a B200")
+def test_bicgstab_fallback_solves_a_generic_rhs():
+    s = _box_solver((4, 4, 4))
+    rhs = np.zeros((4, 4, 4))
+    rhs[2, 2, 2] = 1.0
+    s.cg_rhs.from_numpy(rhs)
+    b_norm = float(np.sqrt(max(s._weighted_dot_kernel(s.cg_rhs, s.cg_rhs), 0.0)))
+    s._continue_pressure_poisson_fv_bicgstab(start_iteration=0, max_iters=80, b_norm=b_norm, outlet=1,
+                                             tolerance=1.0e-8, anchor_unreached=False, remove_nullspace_mean=False)
+    assert s.last_cg_converged, s.last_cg_breakdown
+    assert s.last_cg_relative_residual <= 1.0e-8
+    assert "bicgstab_fallback" in s.last_cg_restart_policy
