@@ -98,3 +98,26 @@ def test_domain_spec_validation():
         FluidDomainSpec((0, 0, 0), (1, 1, 1), (8, 8, 8), -1.0, 1e-3, 1e-3)
     spec = FluidDomainSpec.unit_box(grid_nodes=(8, 8, 8))
     assert spec.cell_volume_m3 == pytest.approx(1.0 / 512)
+
+
+def test_multigrid_default_cycles_cover_nonuniform_grids():
+    """test_core_fluid.py:704 (fluid.py:688-689, 731-734): graded grids get more
+    default V-cycles than uniform ones (host logic, through a stand-in)."""
+    from types import SimpleNamespace
+
+    from easyfsi_b200.fluid import CartesianFluidSolver
+    from easyfsi_b200.grid import CartesianGrid
+
+    uniform = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=(0.125,) * 8, cell_widths_y_m=(0.125,) * 8,
+                            cell_widths_z_m=(0.125,) * 8)
+    graded_w = (0.08, 0.09, 0.10, 0.13, 0.14, 0.15, 0.16, 0.15)
+    graded = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=graded_w, cell_widths_y_m=(0.125,) * 8,
+                           cell_widths_z_m=graded_w)
+    cycles = {}
+    for name, grid in (("uniform", uniform), ("graded", graded)):
+        stub = SimpleNamespace(grid=grid, DEFAULT_MULTIGRID_CYCLES=CartesianFluidSolver.DEFAULT_MULTIGRID_CYCLES,
+                               DEFAULT_NONUNIFORM_MULTIGRID_CYCLES=CartesianFluidSolver.DEFAULT_NONUNIFORM_MULTIGRID_CYCLES)
+        cycles[name] = CartesianFluidSolver.default_multigrid_cycles(stub)
+    assert cycles["uniform"] == CartesianFluidSolver.DEFAULT_MULTIGRID_CYCLES == 12
+    assert cycles["graded"] == CartesianFluidSolver.DEFAULT_NONUNIFORM_MULTIGRID_CYCLES == 24
+    assert cycles["graded"] > cycles["uniform"] >= 1
