@@ -8,8 +8,8 @@ reference test (tests/<file>:<line> in the reference tree) it restates.
 import math
 
 import numpy as np
-import torch
 import pytest
+import torch
 
 pytestmark = pytest.mark.gpu
 
