@@ -361,6 +361,7 @@ class CartesianFluidSolver:
             raise NotImplementedError(
                 "the set-restricted mean projection of outlet-unreached components is not built on the B200 path"
             )
+        self._refresh_structure()
         self.last_cg_restart_policy = "periodic_exact_residual+bicgstab_fallback"
         self.last_cg_breakdown = ""
         stats = (ctypes.c_int64 * 4)()
