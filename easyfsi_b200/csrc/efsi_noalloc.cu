@@ -9,13 +9,17 @@
 // it, or code holding no plan).  Limits:
 //   * at most kMaxBlocks partial sums, hence at most kMaxCells cells; larger
 //     grids are rejected with EFSI_ERR_ARG before anything is launched;
-//   * the ticket counter must start at zero: static device memory is zeroed
-//     at module load and the last block resets it after every call;
+//   * the ticket counter must start at zero: every call clears it on its
+//     stream (cudaMemsetAsync, which allocates nothing) before the launch, so
+//     a call never depends on what an earlier call left in the scratch;
 //   * the scratch is shared by all calls on a device, so calls must not
 //     overlap (issue them on one stream, or synchronise between streams);
 //   * the first call on each device resolves the scratch address with
 //     cudaGetSymbolAddress, with that device current, and may load the
-//     module; make that first call before any stream capture.
+//     module; make that first call before any stream capture;
+//   * the resolved address is kept for the life of the process, so the
+//     library must not be used across a cudaDeviceReset of a device it has
+//     already used (the reset unloads the module and the address goes stale).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -32,7 +36,7 @@ constexpr int64_t kMaxCells = (int64_t)kMaxBlocks * kNoAllocThreads * kNoAllocCe
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_dot_partials[kMaxBlocks];
-static __device__ __align__(256) unsigned g_dot_ticket;  // zero at module load; reset by the last block
+static __device__ __align__(256) unsigned g_dot_ticket;  // cleared by every call before its launch
 
 struct Scratch {
   double* partials = nullptr;
@@ -111,6 +115,7 @@ extern "C" int efsi_weighted_dot_noalloc(int32_t nx, int32_t ny, int32_t nz, con
   EFSI_TRY(scratch_for_current_device(sc));
   const int64_t per_block = (int64_t)kNoAllocThreads * kNoAllocCellsPerThread;
   const unsigned blocks = (unsigned)((n + per_block - 1) / per_block);
+  EFSI_CUDA_CHECK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned), as_stream(stream)));
   EFSI_COUNTED k_weighted_dot_noalloc<<<blocks, kNoAllocThreads, 0, as_stream(stream)>>>(
       nx, ny, nz, obstacle, wx, wy, wz, a, b, sc.partials, sc.ticket, result_device);
   EFSI_LAUNCH_CHECK();

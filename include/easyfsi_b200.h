@@ -117,9 +117,12 @@ int efsi_weighted_dot(efsi_fv_plan* plan, const double* a, const double* b, doub
  * obstacle == 0, V = wx[i] wy[j] wz[k]) with no plan and no allocation; its
  * reduction scratch is a static device array of the library, so at most
  * 268435456 cells (larger grids return EFSI_ERR_ARG) and calls on one device
- * must not overlap.  The first call on a device resolves that scratch (and
- * may load the module): make it before any stream capture.  Writes the total
- * to result_device without synchronising. */
+ * must not overlap.  Each call clears the scratch's ticket on its stream
+ * before the launch.  The first call on a device resolves that scratch (and
+ * may load the module): make it before any stream capture.  The resolved
+ * address is kept for the life of the process: do not use the library across
+ * a cudaDeviceReset of a device it has used.  Writes the total to
+ * result_device without synchronising. */
 int efsi_weighted_dot_noalloc(int32_t nx, int32_t ny, int32_t nz, const int32_t* obstacle, const float* wx,
                               const float* wy, const float* wz, const double* a, const double* b,
                               double* result_device, void* stream);
@@ -184,6 +187,29 @@ typedef struct efsi_cg_stats {
  * efsi_mg_prepare_level0.  pressure is the warm start and the solution. */
 int efsi_fv_pcg_solve(efsi_fv_plan* plan, const double* rhs0, double* pressure, const efsi_pcg_params* params,
                       efsi_cg_stats* stats, void* stream);
+
+/* The PCG's device scalars of a plan (the reference's 0-D cg_rz, cg_rz_new,
+ * cg_dAd, cg_beta_numerator, cg_alpha, cg_beta, cg_breakdown_dAd and
+ * cg_breakdown_code fields, fluid.py:1098-1112). */
+typedef struct efsi_cg_scalar_values {
+  double rz, rz_new, dAd, beta_numerator, alpha, beta, breakdown_dAd;
+  int32_t breakdown_code;
+} efsi_cg_scalar_values;
+
+/* Writes / reads the plan's device scalars (read synchronises the stream). */
+int efsi_cg_scalars_write(efsi_fv_plan* plan, const efsi_cg_scalar_values* values, void* stream);
+int efsi_cg_scalars_read(efsi_fv_plan* plan, efsi_cg_scalar_values* values, void* stream);
+
+/* fluid.py:4567-4574 _cg_compute_alpha_kernel on the plan's device scalars
+ * (the same device step the PCG's SpMV finishers run): alpha = rz / dAd, or
+ * breakdown code 1 when dAd <= 0. */
+int efsi_cg_compute_alpha(efsi_fv_plan* plan, void* stream);
+
+/* fluid.py:4590-4601 _cg_compute_beta_kernel on the plan's device scalars
+ * (the same device step the PCG's dots finishers run): Polak-Ribiere beta
+ * clamped at 0 when use_mg, else rz_new / rz; breakdown code 2 when rz <=
+ * 1e-300 or rz_new <= 0. */
+int efsi_cg_compute_beta(efsi_fv_plan* plan, int32_t use_mg, void* stream);
 
 /* Why CUDA-graph capture was abandoned for this plan ("" when it was not). */
 const char* efsi_fv_graph_error(efsi_fv_plan* plan);

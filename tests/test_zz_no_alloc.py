@@ -1,9 +1,13 @@
 """efsi_weighted_dot_noalloc: the plan-free, allocation-free weighted dot.
 
-Collected last so that it runs after every other test has used the library
-(its static scratch and ticket must be in their initial state for any
-caller).  Compares against the plan-based efsi_weighted_dot on two calls in a
-row (the second call checks that the ticket was reset by the first).
+Some callers cannot allocate device memory at the point where they need the
+dot: the owner of a caching allocator that must not re-enter it, or code that
+holds no solver plan.  This entry point serves them with a static scratch
+array.  The file is collected last, so that a run stopping at the first
+failure has already run every other test; the test also passes alone.  It
+compares the entry point with the plan-based efsi_weighted_dot on calls in a
+row, with a smaller grid in between: every call clears the scratch's ticket
+itself, so the partials and ticket left by an earlier call do not matter.
 """
 
 import numpy as np
@@ -49,6 +53,12 @@ def test_noalloc_dot_matches_plan_dot_on_consecutive_calls():
 
     out = torch.full((1,), float("nan"), dtype=torch.float64, device=fl.device)
     stream = torch.cuda.current_stream(fl.device).cuda_stream
+    # a smaller grid first (fewer blocks): the next calls must not depend on
+    # the partial sums or the ticket it leaves in the shared scratch
+    small = torch.full((1,), float("nan"), dtype=torch.float64, device=fl.device)
+    _native.call("efsi_weighted_dot_noalloc", 1, ny, nz, fl.obstacle.ptr(), fl.cell_width_x_m.ptr(),
+                 fl.cell_width_y_m.ptr(), fl.cell_width_z_m.ptr(), fl.pressure_tmp.ptr(), fl.cg_d.ptr(),
+                 small.data_ptr(), stream)
     for _ in range(2):
         out.fill_(float("nan"))
         _native.call(
