@@ -114,6 +114,11 @@ class IbVdFields(Structure):  # efsi_ib_vd_fields
                 ("anchor_cell", c_void_p), ("marker_region_id", c_void_p), ("report", c_void_p)]
 
 
+class CgScalarValues(Structure):  # efsi_cg_scalar_values
+    _fields_ = [(name, c_double) for name in (
+        "rz", "rz_new", "dAd", "beta_numerator", "alpha", "beta", "breakdown_dAd")] + [("breakdown_code", c_int32)]
+
+
 class ReachReport(Structure):  # efsi_reach_report
     _fields_ = [("unreached_cells", ctypes.c_int64), ("components", c_int32), ("overflow", c_int32)]
 
@@ -173,6 +178,10 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_mg_prolong": [P, I, P, P, D, P],
     "efsi_mg_vcycle": [P, P, P, I, I, I, I, P],
     "efsi_fv_pcg_solve": [P, P, P, POINTER(PcgParams), POINTER(CgStats), P],
+    "efsi_cg_scalars_write": [P, POINTER(CgScalarValues), P],
+    "efsi_cg_scalars_read": [P, POINTER(CgScalarValues), P],
+    "efsi_cg_compute_alpha": [P, P],
+    "efsi_cg_compute_beta": [P, I, P],
     "efsi_fv_multigrid_solve": [P, P, P, I, I, I, P],
     "efsi_fv_jacobi_solve": [P, P, P, I, I, P],
     "efsi_subtract_pressure_gradient": [P, P, P, P, P, F, I, P, P],
@@ -267,6 +276,11 @@ KERNEL_FAMILIES = {
     "cg_dots": 4,
     "p2g": 5,
     "predict": 6,
+    "grid_update": 7,
+    "g2p": 8,
+    "scatter": 9,
+    "feedback": 10,
+    "mpm_step": 11,
     # replay only
     "sweep0_l0": 16,
     "sweep_prolong_l0": 17,

@@ -103,9 +103,10 @@ int efsi_fv_bicgstab(efsi_fv_plan* P, const double* rhs, double* pressure, int32
   const int64_t n = P->lv[0].n;
   const uint8_t* mask = L.mask;
   const unsigned grid = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
-  // work vectors: r, r_old, d, Ad, z, s, t, diag, ones
-  double* w = nullptr;
-  EFSI_CUDA_CHECK(cudaMalloc(&w, 9 * (size_t)n * sizeof(double)));
+  // work vectors: r, r_old, d, Ad, z, s, t, diag, ones; the plan keeps them
+  // from the first fallback on (level 0 never changes size within a plan)
+  if (P->bicg_work == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&P->bicg_work, 9 * (size_t)n * sizeof(double)));
+  double* w = P->bicg_work;
   double *r = w, *r_old = w + n, *d = w + 2 * n, *Ad = w + 3 * n, *z = w + 4 * n, *sv = w + 5 * n, *t = w + 6 * n,
          *diag = w + 7 * n, *ones = w + 8 * n;
   int status = EFSI_OK;
@@ -257,8 +258,11 @@ int efsi_fv_bicgstab(efsi_fv_plan* P, const double* rhs, double* pressure, int32
     return EFSI_OK;
   };
   status = run();
-  cudaStreamSynchronize(s);
-  cudaFree(w);
+  const cudaError_t sync = cudaStreamSynchronize(s);
+  if (status == EFSI_OK && sync != cudaSuccess) {
+    set_error(std::string("efsi_fv_bicgstab: ") + cudaGetErrorString(sync));
+    return EFSI_ERR_CUDA;
+  }
   return status;
 }
 

@@ -512,15 +512,7 @@ __global__ void __launch_bounds__(256) kt_spmv_dir(LevelDev L, const double* __r
   double v[1] = {part}, t[1];
   if (grid_sum<1>(v, partials, &sc->ticket, t)) {
     if (flat_tid() == 0) {
-      const double dAd = t[0];
-      sc->dAd = dAd;
-      sc->alpha = 0.0;
-      if (dAd <= 0.0) {
-        if (sc->code == 0) sc->code_dAd = dAd;
-        sc->code = 1;
-      } else {
-        sc->alpha = sc->rz / dAd;
-      }
+      cg_alpha_step(sc, t[0]);
     }
   }
 }
@@ -637,20 +629,8 @@ __global__ void __launch_bounds__(256) kt_cg_dots(LevelDev L, const double* __re
       if (kRestart) {
         sc->rz = t[0];
       } else {
-        const double rz = sc->rz, rz_new = t[0];
-        sc->rz_new = rz_new;
-        sc->beta_num = t[1];
-        double beta = 0.0;
-        if (rz <= 1.0e-300 || rz_new <= 0.0) {
-          sc->code = 2;
-        } else if (kMG) {
-          beta = t[1] / rz;
-          if (beta < 0.0) beta = 0.0;
-        } else {
-          beta = rz_new / rz;
-        }
-        sc->beta = beta;
-        sc->rz = rz_new;
+        cg_beta_step(sc, t[0], t[1], kMG);
+        sc->rz = t[0];
       }
     }
   }
@@ -984,15 +964,7 @@ __global__ void __launch_bounds__(256) k_spmv_dir(LevelDev L, const double* __re
   double v[1] = {part}, t[1];
   if (grid_sum<1>(v, partials, &sc->ticket, t)) {
     if (flat_tid() == 0) {
-      double dAd = t[0];
-      sc->dAd = dAd;
-      sc->alpha = 0.0;
-      if (dAd <= 0.0) {
-        if (sc->code == 0) sc->code_dAd = dAd;
-        sc->code = 1;
-      } else {
-        sc->alpha = sc->rz / dAd;
-      }
+      cg_alpha_step(sc, t[0]);
     }
   }
 }
@@ -1100,20 +1072,8 @@ __global__ void __launch_bounds__(256) k_cg_dots(LevelDev L, const double* __res
       if (kRestart) {
         sc->rz = t[0];
       } else {
-        double rz = sc->rz, rz_new = t[0];
-        sc->rz_new = rz_new;
-        sc->beta_num = t[1];
-        double beta = 0.0;
-        if (rz <= 1.0e-300 || rz_new <= 0.0) {
-          sc->code = 2;
-        } else if (kMG) {
-          beta = t[1] / rz;
-          if (beta < 0.0) beta = 0.0;
-        } else {
-          beta = rz_new / rz;
-        }
-        sc->beta = beta;
-        sc->rz = rz_new;
+        cg_beta_step(sc, t[0], t[1], kMG);
+        sc->rz = t[0];
       }
     }
   }
@@ -1696,6 +1656,7 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   for (double* v : vecs) cudaFree(v);
   cudaFree(P->sc);
   cudaFree(P->aux);
+  cudaFree(P->bicg_work);
   if (P->host_sc) cudaFreeHost(P->host_sc);
   delete P;
   return EFSI_OK;
@@ -2855,6 +2816,67 @@ int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double*
   EFSI_LAUNCH_CHECK();
   *avg_ms = (double)ms / reps;
   *bytes_per_launch = bytes;
+  return EFSI_OK;
+}
+
+}  // extern "C"
+
+namespace efsi {
+namespace {
+__global__ void k_cg_alpha(CgScalars* sc) { cg_alpha_step(sc, sc->dAd); }
+__global__ void k_cg_beta(CgScalars* sc, int mg) { cg_beta_step(sc, sc->rz_new, sc->beta_num, mg != 0); }
+}  // namespace
+}  // namespace efsi
+
+extern "C" {
+
+int efsi_cg_scalars_write(efsi_fv_plan* P, const efsi_cg_scalar_values* v, void* stream) {
+  EFSI_ARG_CHECK(P != nullptr && v != nullptr, "null argument");
+  cudaStream_t s = as_stream(stream);
+  CgScalars* h = P->host_sc;
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(h, P->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  h->rz = v->rz;
+  h->rz_new = v->rz_new;
+  h->dAd = v->dAd;
+  h->beta_num = v->beta_numerator;
+  h->alpha = v->alpha;
+  h->beta = v->beta;
+  h->code_dAd = v->breakdown_dAd;
+  h->code = v->breakdown_code;
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(P->sc, h, sizeof(CgScalars), cudaMemcpyHostToDevice, s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  return EFSI_OK;
+}
+
+int efsi_cg_scalars_read(efsi_fv_plan* P, efsi_cg_scalar_values* v, void* stream) {
+  EFSI_ARG_CHECK(P != nullptr && v != nullptr, "null argument");
+  cudaStream_t s = as_stream(stream);
+  const CgScalars* h = P->host_sc;
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(P->host_sc, P->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  v->rz = h->rz;
+  v->rz_new = h->rz_new;
+  v->dAd = h->dAd;
+  v->beta_numerator = h->beta_num;
+  v->alpha = h->alpha;
+  v->beta = h->beta;
+  v->breakdown_dAd = h->code_dAd;
+  v->breakdown_code = h->code;
+  return EFSI_OK;
+}
+
+int efsi_cg_compute_alpha(efsi_fv_plan* P, void* stream) {
+  EFSI_ARG_CHECK(P != nullptr, "null plan");
+  EFSI_COUNTED k_cg_alpha<<<1, 1, 0, as_stream(stream)>>>(P->sc);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_cg_compute_beta(efsi_fv_plan* P, int32_t use_mg, void* stream) {
+  EFSI_ARG_CHECK(P != nullptr, "null plan");
+  EFSI_COUNTED k_cg_beta<<<1, 1, 0, as_stream(stream)>>>(P->sc, use_mg);
+  EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
 

@@ -55,6 +55,41 @@ struct CgScalars {
   int fault;  // a plane-marching kernel's stage copy did not complete in time
 };
 
+// fluid.py:4567-4574 _cg_compute_alpha_kernel on the device scalars: alpha =
+// rz / dAd, or breakdown code 1 (and the first offending dAd) when dAd <= 0.
+// Shared by every SpMV finisher and by efsi_cg_compute_alpha.
+__device__ __forceinline__ void cg_alpha_step(CgScalars* sc, double dAd) {
+  sc->dAd = dAd;
+  sc->alpha = 0.0;
+  if (dAd <= 0.0) {
+    if (sc->code == 0) sc->code_dAd = dAd;
+    sc->code = 1;
+  } else {
+    sc->alpha = sc->rz / dAd;
+  }
+}
+
+// fluid.py:4590-4601 _cg_compute_beta_kernel on the device scalars: the
+// flexible (Polak-Ribiere, clamped at 0) beta with the multigrid
+// preconditioner, Fletcher-Reeves otherwise; breakdown code 2 when rz <=
+// 1e-300 or rz_new <= 0.  Shared by every dots finisher and by
+// efsi_cg_compute_beta.
+__device__ __forceinline__ void cg_beta_step(CgScalars* sc, double rz_new, double beta_num, bool mg) {
+  const double rz = sc->rz;
+  sc->rz_new = rz_new;
+  sc->beta_num = beta_num;
+  double beta = 0.0;
+  if (rz <= 1.0e-300 || rz_new <= 0.0) {
+    sc->code = 2;
+  } else if (mg) {
+    beta = beta_num / rz;
+    if (beta < 0.0) beta = 0.0;
+  } else {
+    beta = rz_new / rz;
+  }
+  sc->beta = beta;
+}
+
 // Coarse iterate whose prolongation p += scale * p_coarse is fused into a sweep.
 struct ProlongSrc {
   const float* pc;  // coarse iterate, null when no prolongation is fused
@@ -209,6 +244,7 @@ struct efsi_fv_plan {
   double* partials = nullptr;
   size_t partials_len = 0;
   double* aux = nullptr;  // 16 doubles of statistics scratch
+  double* bicg_work = nullptr;  // BiCGSTAB fallback's nine level-0 work vectors, allocated at its first use
   efsi::CgScalars* sc = nullptr;
   efsi::CgScalars* host_sc = nullptr;  // pinned readback
   bool has_vdir = false;

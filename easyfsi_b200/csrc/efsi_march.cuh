@@ -520,17 +520,8 @@ __device__ __forceinline__ void sweep_epilogue(const Op& op, double* partials, C
         const double mz = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
         sc->mean_z = mz;
         sc->zproj = 1;
-        const double rz = sc->rz, rz_new = t[1] - mz * t[2], bnum = t[3] - mz * t[4];
-        sc->rz_new = rz_new;
-        sc->beta_num = bnum;
-        double beta = 0.0;
-        if (rz <= 1.0e-300 || rz_new <= 0.0) {
-          sc->code = 2;
-        } else {
-          beta = bnum / rz;
-          if (beta < 0.0) beta = 0.0;
-        }
-        sc->beta = beta;
+        const double rz_new = t[1] - mz * t[2];
+        cg_beta_step(sc, rz_new, t[3] - mz * t[4], true);
         sc->rz = rz_new;
       }
     }
@@ -799,15 +790,7 @@ __global__ void __launch_bounds__(kMK* kTY, 3)
   double v[1] = {op.part}, t[1];
   if (grid_sum<1>(v, partials, &sc->ticket, t)) {
     if (flat_tid() == 0) {
-      const double dAd = t[0];
-      sc->dAd = dAd;
-      sc->alpha = 0.0;
-      if (dAd <= 0.0) {
-        if (sc->code == 0) sc->code_dAd = dAd;
-        sc->code = 1;
-      } else {
-        sc->alpha = sc->rz / dAd;
-      }
+      cg_alpha_step(sc, t[0]);
     }
   }
 }

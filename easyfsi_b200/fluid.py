@@ -351,6 +351,34 @@ class CartesianFluidSolver:
         8: "BiCGSTAB fallback did not converge",
     }
 
+    _CG_SCALAR_FIELDS = (("rz", "cg_rz"), ("rz_new", "cg_rz_new"), ("dAd", "cg_dAd"),
+                         ("beta_numerator", "cg_beta_numerator"), ("alpha", "cg_alpha"), ("beta", "cg_beta"),
+                         ("breakdown_dAd", "cg_breakdown_dAd"), ("breakdown_code", "cg_breakdown_code"))
+
+    def _run_cg_scalar_step(self, name: str, *args) -> None:
+        """Runs one of the PCG's device scalar steps on the solver's 0-D
+        ``cg_*`` fields: they are written to the plan's device scalars, the
+        step runs there (the same device code as the PCG finishers) and the
+        results are written back to the fields."""
+        vals = _native.CgScalarValues()
+        for key, field in self._CG_SCALAR_FIELDS:
+            value = getattr(self, field)[None]
+            setattr(vals, key, int(value) if key == "breakdown_code" else float(value))
+        _native.call("efsi_cg_scalars_write", self._plan, byref(vals), _stream())
+        _native.call(name, self._plan, *args, _stream())
+        _native.call("efsi_cg_scalars_read", self._plan, byref(vals), _stream())
+        for key, field in self._CG_SCALAR_FIELDS:
+            getattr(self, field)[None] = getattr(vals, key)
+
+    def _cg_compute_alpha_kernel(self) -> None:
+        """fluid.py:4567-4574: alpha = rz / dAd, or breakdown code 1 when dAd <= 0."""
+        self._run_cg_scalar_step("efsi_cg_compute_alpha")
+
+    def _cg_compute_beta_kernel(self, use_mg_preconditioner: int) -> None:
+        """fluid.py:4590-4601: the flexible / Fletcher-Reeves beta, or
+        breakdown code 2 when rz <= 1e-300 or rz_new <= 0."""
+        self._run_cg_scalar_step("efsi_cg_compute_beta", 1 if use_mg_preconditioner else 0)
+
     def _continue_pressure_poisson_fv_bicgstab(self, *, start_iteration: int, max_iters: int, b_norm: float,
                                                outlet: int, tolerance: float, anchor_unreached: bool,
                                                remove_nullspace_mean: bool) -> None:

@@ -376,9 +376,6 @@ def test_ib_search_rejects_bad_arguments():
 # hibm_mpm.py:6222-7800) through the drop-in classes.  The oracle side of the
 # same cases passes in tests/test_oracle_known_answers.py.
 # --------------------------------------------------------------------------
-_NOT_YET_ON_GPU = pytest.mark.skip(reason="boundary-condition kernels not yet run on a B200")
-
-
 def _boundary(nodes, capacity):
     from easyfsi_b200.hibm_mpm import HibmMpmIbBoundaryConditions
 
@@ -411,7 +408,6 @@ def _one_node(node, bv, n, bp, ip, obstacle=None, velocity=None):
 
 
 # test_hibm.py:1301
-@_NOT_YET_ON_GPU
 def test_ib_boundary_targets_from_the_plane_search():
     mk = _markers(((0.5, 0.5, 0.5),), ((0.0, 0.0, 2.0),))
     mk.v_gamma_mps[0] = (1.25, -0.5, 0.75)
@@ -428,7 +424,6 @@ def test_ib_boundary_targets_from_the_plane_search():
 
 
 # test_hibm.py:3337
-@_NOT_YET_ON_GPU
 def test_vd_rows_reconstruct_along_the_surface_normal():
     mk = _markers(((0.625, 0.625, 0.5),), ((0.0, 0.0, 1.0),))
     mk.v_gamma_mps[0] = (0.0, 0.0, 0.1)
@@ -451,7 +446,6 @@ def test_vd_rows_reconstruct_along_the_surface_normal():
 
 
 # test_hibm.py:3478
-@_NOT_YET_ON_GPU
 def test_vd_rows_relocate_a_masked_node_to_the_first_fluid_cell():
     obs = np.zeros((4, 4, 4), np.int32)
     obs[2, 2, 2] = 1
@@ -466,7 +460,6 @@ def test_vd_rows_relocate_a_masked_node_to_the_first_fluid_cell():
 
 
 # test_hibm.py:3540
-@_NOT_YET_ON_GPU
 def test_vd_rows_relocate_to_the_opposite_side():
     obs = np.zeros((4, 4, 4), np.int32)
     obs[2:, :, :] = 1
@@ -479,7 +472,6 @@ def test_vd_rows_relocate_to_the_opposite_side():
 
 
 # test_hibm.py:3597
-@_NOT_YET_ON_GPU
 def test_vd_rows_wall_limited_gap_is_a_narrow_gap_row():
     obs = np.zeros((4, 4, 4), np.int32)
     obs[3, :, :] = 1
@@ -491,7 +483,6 @@ def test_vd_rows_wall_limited_gap_is_a_narrow_gap_row():
 
 
 # test_hibm.py:3658 and 3718
-@_NOT_YET_ON_GPU
 @pytest.mark.parametrize("node,bp,ip,value,weight", [
     ((2, 2, 2), (0.25, 0.625, 0.625), (0.375, 0.625, 0.625), 0.35, None),
     ((1, 2, 2), (0.5, 0.625, 0.625), (0.625, 0.625, 0.625), 0.3, 0.5),
@@ -508,9 +499,6 @@ def test_vd_rows_fall_back_along_the_line_of_sight(node, bp, ip, value, weight):
 # z-min outlet reachability (fluid.py:1771-1876) through the drop-in solver;
 # the oracle side passes in tests/test_oracle_known_answers.py.
 # --------------------------------------------------------------------------
-_REACH_NOT_YET_ON_GPU = pytest.mark.skip(reason="reachability kernels not yet run on a B200")
-
-
 def _box_solver(nodes):
     from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
 
@@ -518,7 +506,6 @@ def _box_solver(nodes):
 
 
 # test_core_fluid.py:2243
-@_REACH_NOT_YET_ON_GPU
 def test_outlet_reachability_counts_the_cut_off_layers():
     s = _box_solver((5, 5, 5))
     obs = np.zeros((5, 5, 5), np.int32)
@@ -533,7 +520,6 @@ def test_outlet_reachability_counts_the_cut_off_layers():
 
 
 # test_core_fluid.py:2450
-@_REACH_NOT_YET_ON_GPU
 def test_outlet_reachability_reaches_the_end_of_a_long_path():
     s = _box_solver((16, 4, 16))
     obs = np.zeros((16, 4, 16), np.int32)
@@ -549,7 +535,6 @@ def test_outlet_reachability_reaches_the_end_of_a_long_path():
 
 
 # test_core_fluid.py:2307 (reachability part)
-@_REACH_NOT_YET_ON_GPU
 def test_outlet_reachability_labels_separate_pockets():
     s = _box_solver((9, 4, 9))
     obs = np.ones((9, 4, 9), np.int32)
@@ -566,7 +551,6 @@ def test_outlet_reachability_labels_separate_pockets():
 
 
 # test_core_fluid.py:3713 the BiCGSTAB fallback solves a generic FV rhs
-@pytest.mark.skip(reason="BiCGSTAB fallback not yet run on a B200")
 def test_bicgstab_fallback_solves_a_generic_rhs():
     s = _box_solver((4, 4, 4))
     rhs = np.zeros((4, 4, 4))
@@ -578,3 +562,47 @@ def test_bicgstab_fallback_solves_a_generic_rhs():
     assert s.last_cg_converged, s.last_cg_breakdown
     assert s.last_cg_relative_residual <= 1.0e-8
     assert "bicgstab_fallback" in s.last_cg_restart_policy
+
+
+# test_core_fluid.py:3259 negative curvature sets the device breakdown code
+# (the same device alpha / beta steps the PCG's finishers run)
+def test_fv_cg_negative_curvature_sets_device_breakdown_code():
+    s = _unit_solver(4)
+    s.cg_rz[None] = 1.0
+    s.cg_rz_new[None] = 1.0
+    s.cg_dAd[None] = 0.0
+    s._cg_compute_alpha_kernel()
+    assert int(s.cg_breakdown_code[None]) == 1
+    assert float(s.cg_alpha[None]) == 0.0
+    assert float(s.cg_breakdown_dAd[None]) == 0.0
+    s._cg_compute_beta_kernel(0)
+    assert int(s.cg_breakdown_code[None]) == 1
+
+
+def test_fv_cg_alpha_and_flexible_beta_steps():
+    s = _unit_solver(4)
+    s.cg_breakdown_code[None] = 0
+    s.cg_rz[None] = 2.0
+    s.cg_dAd[None] = 8.0
+    s._cg_compute_alpha_kernel()
+    assert float(s.cg_alpha[None]) == 0.25 and int(s.cg_breakdown_code[None]) == 0
+    # flexible (Polak-Ribiere) beta is clamped at zero; Fletcher-Reeves is rz_new / rz
+    s.cg_rz_new[None] = 3.0
+    s.cg_beta_numerator[None] = -1.0
+    s._cg_compute_beta_kernel(1)
+    assert float(s.cg_beta[None]) == 0.0 and int(s.cg_breakdown_code[None]) == 0
+    s.cg_beta_numerator[None] = 1.0
+    s._cg_compute_beta_kernel(1)
+    assert float(s.cg_beta[None]) == 0.5
+    s._cg_compute_beta_kernel(0)
+    assert float(s.cg_beta[None]) == 1.5
+    # rz_new <= 0 is breakdown code 2; a negative dAd keeps the first offending value
+    s.cg_rz_new[None] = 0.0
+    s._cg_compute_beta_kernel(0)
+    assert int(s.cg_breakdown_code[None]) == 2 and float(s.cg_beta[None]) == 0.0
+    s.cg_breakdown_code[None] = 0
+    s.cg_dAd[None] = -3.0
+    s._cg_compute_alpha_kernel()
+    s.cg_dAd[None] = -5.0
+    s._cg_compute_alpha_kernel()
+    assert int(s.cg_breakdown_code[None]) == 1 and float(s.cg_breakdown_dAd[None]) == -3.0
