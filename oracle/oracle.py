@@ -370,10 +370,18 @@ class OracleFluid:
         self.last_stats = st
         return st
 
-    def predict(self, dt: float) -> None:
+    def predict(self, dt: float, rk2: bool = False) -> None:
+        """fluid.py:2447-2527: semi-Lagrangian predictor (Euler backtrace, or
+        the RK2 midpoint with ``rk2``) plus explicit viscosity."""
         self.velocity_prev[...] = self.velocity
         self.lib.efo_predict(byref(self.gridstruct), _p(self.obstacle), _p(self.velocity_prev), c_float(dt),
-                             c_float(self.mu / self.rho), c_int(0), _p(self.velocity))
+                             c_float(self.mu / self.rho), c_int(1 if rk2 else 0), _p(self.velocity))
+
+    def apply_velocity_dirichlet_rows(self, active, value) -> None:
+        """fluid.py:2549-2593: velocity = row value on active fluid cells."""
+        self.lib.efo_apply_velocity_dirichlet_rows(ctypes.c_int64(self.obstacle.size), _p(self.obstacle),
+                                                   _p(np.ascontiguousarray(active, np.int32)),
+                                                   _p(np.ascontiguousarray(value, self.rt)), _p(self.velocity))
 
     def project(self, *, dt: float, max_iters: int = 400, tol: float = 1.0e-8, precond: int = 1) -> CgStats:
         """Plain closed-box fv_cg projection (fluid.py:6889-7340 without Dirichlet rows)."""

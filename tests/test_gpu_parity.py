@@ -447,7 +447,6 @@ def test_ib_node_search_matches_oracle():
     assert (search.node_anchor_cell.to_numpy() == -1).all()
 
 
-@pytest.mark.skip(reason="boundary-condition kernels not yet run on a B200")
 def test_ib_boundary_rows_match_oracle():
     """Node search -> boundary targets -> reconstructed velocity-Dirichlet
     rows on a closed surface over a graded grid with masked cells and a
@@ -521,7 +520,6 @@ def test_ib_boundary_rows_match_oracle():
                                rtol=0.0, atol=1e-6)
 
 
-@pytest.mark.skip(reason="reachability kernels not yet run on a B200")
 def test_outlet_reachability_matches_oracle():
     """Union-find reachability and component labels against the oracle's
     Jacobi sweeps on random obstacles, Dirichlet rows and barriers (via
@@ -547,7 +545,6 @@ def test_outlet_reachability_matches_oracle():
     s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=False)
 
 
-@pytest.mark.skip(reason="BiCGSTAB fallback not yet run on a B200")
 @pytest.mark.parametrize("outlet,remove_mean", [(1, False), (0, True)])
 def test_bicgstab_matches_oracle(outlet, remove_mean):
     """The device BiCGSTAB fallback against the oracle's on a graded grid with
@@ -575,9 +572,11 @@ def test_bicgstab_matches_oracle(outlet, remove_mean):
                                               remove_nullspace_mean=remove_mean)
     ref = ofl.bicgstab(rhs, outlet=outlet, max_iters=400, tol=1e-8, b_norm=b_norm, remove_mean=remove_mean)
     assert fl.last_cg_converged and ref["converged"]
-    # reductions run in other orders on the device, so the Krylov iterates
-    # drift apart slowly: about the same count, the same system solved
-    assert abs(fl.last_cg_iterations - ref["iterations"]) <= 8
+    # reductions run in other orders on the device; BiCGSTAB's iterates are
+    # sensitive to that (measured on a B200: 112 against the oracle's 130
+    # iterations for the outlet case), so the counts agree only roughly and
+    # the solution is judged by its true residual and the pressure below
+    assert abs(fl.last_cg_iterations - ref["iterations"]) <= max(8, 0.25 * ref["iterations"])
     p = fl.pressure.to_numpy()
     res = rhs - ofl.fv_apply(p, outlet)
     res[obs == 1] = 0.0
@@ -587,3 +586,169 @@ def test_bicgstab_matches_oracle(outlet, remove_mean):
         res[obs == 1] = 0.0
     assert math.sqrt(ofl.weighted_dot(res, res)) / b_norm <= 5e-8
     assert rel_l2(p, ofl.pressure) <= 1e-4
+
+
+# --------------------------------------------------------------------------
+# Standalone solvers, boundary rows, spreading, RK2 predictor and two-sided
+# traction probes: each against the oracle on the same seeded inputs.
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("cycles", [2, None])
+def test_standalone_multigrid_solve_matches_oracle(case, cycles):
+    """fluid.py:5992-6083 fv_multigrid (3 / 36 / 3 sweeps per cycle, 0.7
+    graded prolongation, then the level-0 polish sweeps) against the oracle's
+    restatement.  Coarse levels are f32 in both; the pressure agrees to the
+    f32 coarse arithmetic."""
+    grid, fl, ofl, rng = case
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    fl.divergence.from_numpy(div)
+    ofl.divergence[...] = div
+    fl.pressure.tensor.zero_()
+    ofl.pressure[...] = 0.0
+    n_cycles = cycles if cycles is not None else fl.default_multigrid_cycles()
+    fl._solve_pressure_poisson_fv_multigrid(iterations=6, rhs_scale=1.0e6, pressure_outlet_zmin=False,
+                                            multigrid_cycles=cycles)
+    ofl.prepare_rhs(1.0e6)
+    ofl.multigrid_solve(outlet=0, iterations=6, cycles=n_cycles)
+    err = rel_l2(fl.pressure.to_numpy(), ofl.pressure)
+    print(f"fv_multigrid cycles={n_cycles}: pressure rel-L2 {err:.3e}")
+    assert err <= 1e-9
+
+
+@pytest.mark.parametrize("outlet", [0, 1])
+def test_standalone_fv_jacobi_solve_matches_oracle(case, outlet):
+    """fluid.py:5977-5990 fv_jacobi: damped Jacobi (omega 0.8) sweeps of the
+    level-0 system, f64 throughout."""
+    grid, fl, ofl, rng = case
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    fl.divergence.from_numpy(div)
+    ofl.divergence[...] = div
+    fl.pressure.tensor.zero_()
+    ofl.pressure[...] = 0.0
+    fl._solve_pressure_poisson_fv_jacobi(iterations=40, rhs_scale=1.0e6, pressure_outlet_zmin=bool(outlet))
+    ofl.compute_divergence(outlet)
+    ofl.divergence[...] = div
+    ofl.prepare_rhs(1.0e6)
+    ofl.lib.efo_fv_multigrid_solve(orc.c_int(1), ofl.levels, orc._p(ofl.obstacle), None, None, None,
+                                   orc._p(ofl.rhs0), orc._p(ofl.pressure), orc.c_int(outlet), orc.c_int(40),
+                                   orc.c_int(1), orc.c_int(0))
+    err = rel_l2(fl.pressure.to_numpy(), ofl.pressure)
+    print(f"fv_jacobi outlet={outlet}: pressure rel-L2 {err:.3e}")
+    assert err <= 1e-12
+
+
+def test_velocity_dirichlet_rows_and_zmin_no_backflow_match_oracle(case):
+    """fluid.py:2549-2593 (row values written on active fluid cells, with the
+    reference's report sums) and fluid.py:5762-5766 (no inflow through the
+    z-min outlet): identical velocities."""
+    grid, fl, ofl, rng = case
+    vel = (0.1 * rng.normal(size=grid.grid_nodes + (3,))).astype(np.float32)
+    active = (rng.random(grid.grid_nodes) < 0.1).astype(np.int32)
+    value = (0.2 * rng.normal(size=grid.grid_nodes + (3,))).astype(np.float32)
+    weight = rng.random(grid.grid_nodes).astype(np.float32)
+    fl.velocity.from_numpy(vel)
+    ofl.velocity[...] = vel
+    fl.velocity_dirichlet_boundary_active.from_numpy(active)
+    fl.velocity_dirichlet_boundary_value_mps.from_numpy(value)
+    fl.velocity_dirichlet_boundary_projection_weight.from_numpy(weight)
+    rep = fl.apply_velocity_dirichlet_boundary_rows(read_report=True)
+    ofl.apply_velocity_dirichlet_rows(active, value)
+    np.testing.assert_array_equal(fl.velocity.to_numpy(), ofl.velocity)
+    rows = (active != 0) & (ofl.obstacle == 0)
+    delta = value.astype(np.float64) - vel.astype(np.float64)
+    norms = np.linalg.norm(delta, axis=-1)[rows]
+    assert rep.active_cells == int(rows.sum())
+    assert rep.max_delta_mps == pytest.approx(float(norms.max()), rel=1e-6)
+    assert rep.mean_delta_mps == pytest.approx(float(norms.mean()), rel=1e-5)
+    vol = np.einsum("i,j,k->ijk", *[np.asarray(m["w"], np.float32).astype(np.float64) for m in ofl.metrics[0]])
+    mom = 1000.0 * (delta * vol[..., None])[rows].sum(axis=0)
+    np.testing.assert_allclose(rep.momentum_delta_n_s, mom, rtol=1e-4, atol=1e-12 * np.abs(mom).max())
+    # z-min outlet: upward (inflow) z velocities of the first layer cleared
+    fl.velocity_dirichlet_boundary_active.tensor.zero_()
+    vel = (0.1 * rng.normal(size=grid.grid_nodes + (3,))).astype(np.float32)
+    fl.velocity.from_numpy(vel)
+    ofl.velocity[...] = vel
+    fl._apply_zmin_no_backflow_kernel()
+    ofl.apply_zmin_no_backflow()
+    np.testing.assert_array_equal(fl.velocity.to_numpy(), ofl.velocity)
+    assert (fl.velocity.to_numpy()[:, :, 0, 2][ofl.obstacle[:, :, 0] == 0] <= 0.0).all()
+
+
+@pytest.mark.parametrize("sign", [-1.0, 1.0])
+def test_spread_surface_forces_and_body_force_match_oracle(case, sign):
+    """fluid.py:3196-3273 trilinear spreading of point forces to force
+    densities, renormalised over the fluid corners next to obstacles, and
+    fluid.py:3301-3328 u += f dt / rho: force density and velocity against the
+    oracle; the spread total equals force_sign times the surface total
+    (the reference's action-reaction check, tests/test_fluid.py:79-175)."""
+    grid, fl, ofl, rng = case
+    m = 300
+    pos = (0.15 + 0.7 * rng.random((m, 3))).astype(np.float32)
+    frc = rng.normal(size=(m, 3)).astype(np.float32)
+    vel = (0.1 * rng.normal(size=grid.grid_nodes + (3,))).astype(np.float32)
+    fl.velocity.from_numpy(vel)
+    ofl.velocity[...] = vel
+    rep = fl.spread_surface_forces(torch.as_tensor(pos), torch.as_tensor(frc), m, (0.0, 0.0, 0.0), force_sign=sign)
+    oref = ofl.spread_surface_forces(pos, frc, force_sign=sign)
+    assert rel_l2(fl.force.to_numpy(), ofl.force) <= 1e-6
+    np.testing.assert_allclose(rep.surface_force_n, oref[:3], rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(rep.grid_force_n, sign * np.asarray(oref[:3]), rtol=1e-4, atol=1e-4)
+    imp = fl.apply_body_force(1.0e-3, read_report=True)
+    ofl.apply_body_force(1.0e-3)
+    assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) <= 1e-6
+    assert imp.impulse_relative_error <= 1e-4
+
+
+def test_rk2_predictor_matches_oracle(case):
+    """fluid.py:2447-2527 with advection_scheme="rk2" (midpoint backtrace) and
+    the explicit viscous term, against the oracle (test_core_fluid.py:3738)."""
+    grid, fl, ofl, rng = case
+    vel = (0.2 * rng.normal(size=grid.grid_nodes + (3,))).astype(np.float32)
+    fl.velocity.from_numpy(vel)
+    ofl.velocity[...] = vel
+    fl.predict(2.0e-2, advection_scheme="rk2")
+    ofl.predict(2.0e-2, rk2=True)
+    err = rel_l2(fl.velocity.to_numpy(), ofl.velocity)
+    print(f"rk2 predictor: velocity rel-L2 {err:.3e}")
+    assert err <= 1e-6
+    euler = vel.copy()
+    ofl.velocity[...] = euler
+    ofl.predict(2.0e-2, rk2=False)
+    assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) > 10 * err  # the RK2 branch really ran
+
+
+@pytest.mark.parametrize("two_sided,one_sided_region", [(True, -1), (False, 101)])
+def test_two_sided_and_one_sided_pressure_probes_match_oracle(case, two_sided, one_sided_region):
+    """hibm_mpm.py:2253-2432: marker tractions from pressure probes at k h_n
+    (k = 1..3) on both sides of the surface (two-sided jump), or one side
+    against a reference pressure, against the oracle: tractions, validity and
+    report counts."""
+    from easyfsi_b200.hibm_mpm import HibmMpmSurfaceMarkers
+
+    grid, fl, ofl, rng = case
+    p = 1.0e3 * rng.normal(size=grid.grid_nodes)
+    fl.pressure.from_numpy(p)
+    ofl.pressure[...] = p
+    m = 400
+    d = rng.normal(size=(m, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    x = (np.array([0.5, 0.5, 0.5]) + 0.2 * d).astype(np.float32)
+    n = d.astype(np.float32)
+    region = np.where(rng.random(m) < 0.5, 101, 202).astype(np.int32)
+    mk = HibmMpmSurfaceMarkers(marker_capacity=m)
+    mk.load_markers(positions_m=x, velocities_mps=np.zeros_like(x), normals=n, areas_m2=np.full(m, 1.0e-3),
+                    region_ids=region)
+    rep = mk.sample_fluid_stress_to_marker_tractions(
+        fl.velocity, fl.pressure, fl.obstacle, fl.cell_face_x_m, fl.cell_face_y_m, fl.cell_face_z_m,
+        fl.cell_center_x_m, fl.cell_center_y_m, fl.cell_center_z_m, fl.cell_width_x_m, fl.cell_width_y_m,
+        fl.cell_width_z_m, grid.grid_nodes, viscosity_pa_s=0.0, two_sided_pressure=two_sided,
+        one_sided_pressure_region_id=one_sided_region, one_sided_reference_pressure_pa=250.0)
+    om = orc.OracleMarkers(x=x, normal=mk.n_gamma.to_numpy()[:m], area=np.full(m, 1.0e-3, np.float32), region=region)
+    orep = om.sample_tractions(ofl, two_sided=1 if two_sided else 0, one_sided_region=one_sided_region,
+                               one_sided_ref=250.0)
+    err = rel_l2(mk.t_gamma_pa.to_numpy()[:m], om.t)
+    print(f"probes two_sided={two_sided} one_sided={one_sided_region}: traction rel-L2 {err:.3e}")
+    assert err <= 1e-6
+    np.testing.assert_array_equal(mk._stress_pressure_valid.to_numpy()[:m], om.valid)
+    assert rep.valid_marker_count == int(orep.valid)
+    assert rep.two_sided_pressure_marker_count == int(orep.two_sided)
+    assert rep.one_sided_pressure_marker_count == int(orep.one_sided)
