@@ -201,6 +201,41 @@ def pressure_solve_stats(scene, reps: int, jacobi_max_iterations: int = 20000) -
     return out
 
 
+PARTICLE_FAMILIES = ("p2g", "grid_update", "g2p", "scatter", "feedback", "mpm_step")
+
+
+def family_timing(scene, steps: int, peak_gbs: float, world: int) -> dict:
+    """Per-launch CUDA-event times of the MPM and HIBM kernel families over
+    `steps` coupled steps (timing on, outside the headline's timed region),
+    with each family's algorithmic bytes per launch and its fraction of the
+    HBM peak."""
+    import torch
+    import torch.distributed as dist
+
+    from easyfsi_b200 import _native
+
+    for fam in PARTICLE_FAMILIES:
+        _native.kernel_timing_enable(fam, True)
+    try:
+        for _ in range(max(1, steps)):
+            scene.step()
+        torch.cuda.synchronize()
+        out = {}
+        for fam in PARTICLE_FAMILIES:
+            n, ms, nbytes = _native.kernel_timing_read(fam)
+            if n == 0:
+                continue
+            gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+            out[fam] = {"launches": n, "avg_launch_us": 1000.0 * ms / n, "bytes_per_launch": nbytes / n,
+                        "achieved_gbs": gbs, "frac": gbs / peak_gbs if gbs else None}
+    finally:
+        for fam in PARTICLE_FAMILIES:
+            _native.kernel_timing_enable(fam, False)
+    if world > 1:
+        dist.barrier()
+    return out
+
+
 def max_over_ranks(ms: float, world: int, device) -> float:
     """Largest per-rank time over all ranks (every rank calls this in the same
     order; a no-op for one rank)."""
@@ -281,7 +316,9 @@ def main() -> None:
     ap.add_argument("--no-mixed", action="store_true", help="skip the fv_multigrid_mixed measurement")
     ap.add_argument("--no-ib-search", action="store_true", help="skip the IB node search measurement")
     ap.add_argument("--no-pressure-solve", action="store_true", help="skip the per-preconditioner solve timing")
-    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="timed CPU-oracle steps of the GPU arm's cpu_baseline")
+    ap.add_argument("--cpu-warmup", type=int, default=1)
+    ap.add_argument("--no-family-timing", action="store_true", help="skip the MPM / HIBM kernel-family timing pass")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-reps", type=int, default=50)
     args = ap.parse_args()
@@ -464,6 +501,11 @@ def main() -> None:
         }
 
     peak, peak_kind = _hbm_peak()
+    # --- MPM and HIBM kernel families: CUDA events around each launch (on its
+    # own stream) over `steps` further coupled steps ---
+    particle_families = None
+    if not args.no_family_timing:
+        particle_families = family_timing(scene, args.steps, peak, world)
     dom = max(fam_stats, key=lambda f: fam_stats[f]["ms_per_step"])
     st = fam_stats[dom]
     traffic = None
@@ -491,11 +533,16 @@ def main() -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference(cfg, args.cpu_steps, 0, initial_velocity=scene.fluid.velocity.to_numpy())
+            cpu = cpu_reference(cfg, args.cpu_steps, args.cpu_warmup, initial_velocity=scene.fluid.velocity.to_numpy())
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {exc}"}
     if rank == 0:
+        solve_ms, solve_iters = None, None
+        if isinstance(psolve, dict) and "error" not in psolve:
+            names = [k for k, v in psolve.items() if isinstance(v, dict) and "ms" in v]
+            solve_ms = {k: round(psolve[k]["ms"], 4) for k in names}
+            solve_iters = {k: psolve[k]["iterations"] for k in names}
         line = {
             "metric": METRIC,
             "value": value,
@@ -520,20 +567,21 @@ def main() -> None:
                 "parallelism": f"replicas x{world}",
                 "l2": WORKING_SET_NOTE,
             },
-            "pressure_solve": {
-                "cg_iterations_mean": float(np.mean(iters)) if iters else None,
-                "cg_iterations": iters,
-            },
-            "kernel_families": fam_stats,
-            "preconditioner": vcycle_stats,
-            "mixed_precision": mixed,
-            "ib_node_search": ib_search,
-            "pressure_solve": psolve,
+            "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "solve_ms": solve_ms,
+            "solve_iterations": solve_iters,
+            "cg_iterations_mean": float(np.mean(iters)) if iters else None,
+            "mixed_precision": mixed,
+            "particle_families": particle_families,
+            "kernel_families": fam_stats,
+            "preconditioner": vcycle_stats,
+            "pressure_solve": psolve,
+            "ib_node_search": ib_search,
+            "cg_iterations": iters,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -65,7 +65,12 @@ enum KernelFamily : int {
   KF_CG_DOTS = 4,
   KF_P2G = 5,
   KF_PREDICT = 6,
-  KF_COUNT = 7
+  KF_GRID_UPDATE = 7,
+  KF_G2P = 8,
+  KF_SCATTER = 9,
+  KF_FEEDBACK = 10,
+  KF_MPM_STEP = 11,  // the whole substep: clears, binning, P2G, grid update, G2P
+  KF_COUNT = 12
 };
 bool timing_enabled(int family);
 void timing_begin(int family, cudaStream_t s);

@@ -624,8 +624,11 @@ int efsi_scatter_marker_forces(efsi_bin_plan* P, int32_t marker_count, const flo
   cudaStream_t s = as_stream(stream);
   EFSI_CUDA_CHECK(cudaMemsetAsync(report_device, 0, 9 * sizeof(double), s));
   if (marker_count <= 0) return EFSI_OK;
-  EFSI_COUNTED k_scatter<<<(marker_count + 7) / 8, 256, 0, s>>>(bin_view(P), marker_count, x_gamma, f_gamma,
-                                                                  particle_x, external_force, report_device);
+  // 36 bytes per marker (x, F) and 12 per binned particle position read
+  EFSI_TIMED(KF_SCATTER, 36.0 * marker_count + 12.0 * P->count_last, s,
+             EFSI_COUNTED k_scatter<<<(marker_count + 7) / 8, 256, 0, s>>>(bin_view(P), marker_count, x_gamma, f_gamma,
+                                                                             particle_x, external_force,
+                                                                             report_device));
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
@@ -639,9 +642,12 @@ int efsi_surface_feedback(efsi_bin_plan* P, int32_t marker_count, float* x_gamma
   cudaStream_t s = as_stream(stream);
   EFSI_CUDA_CHECK(cudaMemsetAsync(report_device, 0, 8 * sizeof(double), s));
   if (marker_count <= 0) return EFSI_OK;
-  EFSI_COUNTED k_feedback<<<(marker_count + 7) / 8, 256, 0, s>>>(bin_view(P), marker_count, x_gamma, v_gamma,
-                                                                   n_gamma, area_gamma, particle_x, particle_v,
-                                                                   particle_normal, particle_area, dt, report_device);
+  // 52 bytes per marker (read x; write x, v, n, A) and 40 per binned
+  // particle (x, v, normal, area)
+  EFSI_TIMED(KF_FEEDBACK, 52.0 * marker_count + 40.0 * P->count_last, s,
+             EFSI_COUNTED k_feedback<<<(marker_count + 7) / 8, 256, 0, s>>>(
+                 bin_view(P), marker_count, x_gamma, v_gamma, n_gamma, area_gamma, particle_x, particle_v,
+                 particle_normal, particle_area, dt, report_device));
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
