@@ -299,11 +299,39 @@ __device__ __forceinline__ void block_max(double* acc, int slot, double v) {
 // ---------------------------------------------------------------------------
 // P2G (neo_hookean_mpm.py:712-801): one CTA per tile (+ one for the
 // out-of-stencil bucket, which only clamps F and reports).
+//
+// The tile's particles are taken in chunks of kP2gChunk.  Each thread first
+// forms its particle's transfer terms (weights, fractional offsets, mass,
+// momentum, APIC/stress affine matrix, external force) and the particle is
+// placed, by a counting sort in shared memory, in the run of its base cell
+// (one of the tile's 4^3 cells).  Then the work is split by (base cell,
+// stencil offset): the thread of item (c, o) sums the contributions of all
+// particles of cell c to the node c + o in registers -- the threads of one
+// cell read the same particle record together (shared-memory broadcast) -- and
+// adds the sums to the 6^3 node block with one shared atomic per value.  The
+// block is flushed to the grid with one global atomic per non-zero value.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_p2g(efsi_mpm_state S, int tx, int ty, int tz, int ntiles,
-                                             const int32_t* __restrict__ sorted, const int32_t* __restrict__ offset,
-                                             float dt, float mu, float lam, double* acc) {
+constexpr int kP2gThreads = 256;
+constexpr int kP2gChunk = 256;  // particles per chunk (one per thread)
+constexpr int kTileCells = kTile * kTile * kTile;
+
+struct P2gRecords {
+  float w[9][kP2gChunk];   // w[3 a + o]: quadratic weight of offset o on axis a
+  float fx[3][kP2gChunk];  // fractional offset from the base node, per axis
+  float m[kP2gChunk];
+  float mom[3][kP2gChunk];
+  float aff[9][kP2gChunk];
+  float fe[3][kP2gChunk];
+};
+
+__global__ void __launch_bounds__(kP2gThreads) k_p2g(efsi_mpm_state S, int tx, int ty, int tz, int ntiles,
+                                                     const int32_t* __restrict__ sorted,
+                                                     const int32_t* __restrict__ offset, float dt, float mu,
+                                                     float lam, double* acc) {
   __shared__ float sacc[7][kHaloN];
+  __shared__ P2gRecords rec;
+  __shared__ int cell_count[kTileCells];
+  __shared__ int cell_start[kTileCells + 1];
   const int tile = blockIdx.x;
   const int beg = offset[tile], end = offset[tile + 1];
   if (beg == end) return;  // uniform per block
@@ -316,19 +344,23 @@ __global__ void __launch_bounds__(256) k_p2g(efsi_mpm_state S, int tx, int ty, i
   }
   const int nb0 = t0 * kTile, nb1 = t1 * kTile, nb2 = t2 * kTile;
   for (int q = threadIdx.x; q < 7 * kHaloN; q += blockDim.x) (&sacc[0][0])[q] = 0.0f;
-  __syncthreads();
   const float inv4[3] = {(float)(4.0 / ((double)S.dx[0] * S.dx[0])), (float)(4.0 / ((double)S.dx[1] * S.dx[1])),
                          (float)(4.0 / ((double)S.dx[2] * S.dx[2]))};
+  const float dxs[3] = {S.dx[0], S.dx[1], S.dx[2]};
   double rm = 0, rv = 0, rp0 = 0, rp1 = 0, rp2 = 0, rf0 = 0, rf1 = 0, rf2 = 0, rmom2 = 0, rmaxj = 0, roob = 0,
          rclamp = 0;
-  for (int q0 = beg; q0 < end; q0 += blockDim.x) {
-    const int q = q0 + threadIdx.x;
-    if (q < end) {
+  for (int c0 = beg; c0 < end; c0 += kP2gChunk) {
+    for (int q = threadIdx.x; q < kTileCells; q += blockDim.x) cell_count[q] = 0;
+    __syncthreads();
+    const int q = c0 + threadIdx.x;
+    const bool have = q < end;
+    int lc = -1, rank = 0;
+    float w[3][3], fx[3], mass = 0.0f, mom[3] = {0, 0, 0}, fe[3] = {0, 0, 0}, aff[9];
+    if (have) {
       const int p = sorted[q];
       float X[3];
       grid_coord(S, p, X);
       int base[3];
-      float fx[3], w[3][3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         base[a] = (int)floorf(X[a] - 0.5f);
@@ -358,9 +390,9 @@ __global__ void __launch_bounds__(256) k_p2g(efsi_mpm_state S, int tx, int ty, i
         float finvT = cof[a] / Jr;
         Pm[a] = mu * (Fp[a] - finvT) + lam * lnJ * finvT;
       }
-      const float mass = S.mass[p], vol = S.volume[p];
+      mass = S.mass[p];
+      const float vol = S.volume[p];
       const float sv = -dt * vol;
-      float aff[9];
 #pragma unroll
       for (int ii = 0; ii < 3; ++ii)
 #pragma unroll
@@ -368,7 +400,6 @@ __global__ void __launch_bounds__(256) k_p2g(efsi_mpm_state S, int tx, int ty, i
           float pf = Pm[3 * ii] * Fp[3 * jj] + Pm[3 * ii + 1] * Fp[3 * jj + 1] + Pm[3 * ii + 2] * Fp[3 * jj + 2];
           aff[3 * ii + jj] = sv * (pf * inv4[jj]) + mass * S.C[9 * p + 3 * ii + jj];
         }
-      float mom[3], fe[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         mom[a] = mass * S.v[3 * p + a];
@@ -393,27 +424,73 @@ __global__ void __launch_bounds__(256) k_p2g(efsi_mpm_state S, int tx, int ty, i
       if (!in_stencil_bucket) {
         roob += 1.0;
       } else {
-        const int l0 = base[0] - nb0, l1 = base[1] - nb1, l2 = base[2] - nb2;
-#pragma unroll
-        for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-          for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-            for (int oz = 0; oz < 3; ++oz) {
-              const float wt = w[0][ox] * w[1][oy] * w[2][oz];
-              const float d0 = ((float)ox - fx[0]) * S.dx[0], d1 = ((float)oy - fx[1]) * S.dx[1],
-                          d2 = ((float)oz - fx[2]) * S.dx[2];
-              const int ln = ((l0 + ox) * kHalo + (l1 + oy)) * kHalo + (l2 + oz);
-              atomicAdd(&sacc[0][ln], wt * mass);
-              atomicAdd(&sacc[1][ln], wt * (mom[0] + (aff[0] * d0 + aff[1] * d1 + aff[2] * d2)));
-              atomicAdd(&sacc[2][ln], wt * (mom[1] + (aff[3] * d0 + aff[4] * d1 + aff[5] * d2)));
-              atomicAdd(&sacc[3][ln], wt * (mom[2] + (aff[6] * d0 + aff[7] * d1 + aff[8] * d2)));
-              atomicAdd(&sacc[4][ln], wt * fe[0]);
-              atomicAdd(&sacc[5][ln], wt * fe[1]);
-              atomicAdd(&sacc[6][ln], wt * fe[2]);
-            }
+        // base - tile origin is in [0, kTile) on every axis (the bin key)
+        lc = ((base[0] - nb0) * kTile + (base[1] - nb1)) * kTile + (base[2] - nb2);
+        rank = atomicAdd(&cell_count[lc], 1);
       }
     }
+    if (!in_stencil_bucket) continue;  // uniform per block
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      // exclusive scan of the 64 cell counts by one warp, two per lane
+      const int l = threadIdx.x;
+      const int a = cell_count[2 * l], b = cell_count[2 * l + 1];
+      int v = a + b;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (l >= o) v += u;
+      }
+      cell_start[2 * l] = v - a - b;
+      cell_start[2 * l + 1] = v - b;
+      if (l == 31) cell_start[kTileCells] = v;
+    }
+    __syncthreads();
+    if (lc >= 0) {
+      const int slot = cell_start[lc] + rank;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int o = 0; o < 3; ++o) rec.w[3 * a + o][slot] = w[a][o];
+        rec.fx[a][slot] = fx[a];
+        rec.mom[a][slot] = mom[a];
+        rec.fe[a][slot] = fe[a];
+      }
+      rec.m[slot] = mass;
+#pragma unroll
+      for (int a = 0; a < 9; ++a) rec.aff[a][slot] = aff[a];
+    }
+    __syncthreads();
+    for (int item = threadIdx.x; item < kTileCells * 27; item += blockDim.x) {
+      const int c = item / 27, o = item - 27 * c;
+      const int pb = cell_start[c], pe = cell_start[c + 1];
+      if (pb == pe) continue;
+      const int o0 = o / 9, o1 = (o / 3) % 3, o2 = o % 3;
+      const float fo[3] = {(float)o0, (float)o1, (float)o2};
+      float sm = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f, s4 = 0.0f, s5 = 0.0f, s6 = 0.0f;
+      for (int r = pb; r < pe; ++r) {
+        const float wt = rec.w[o0][r] * rec.w[3 + o1][r] * rec.w[6 + o2][r];
+        const float d0 = (fo[0] - rec.fx[0][r]) * dxs[0], d1 = (fo[1] - rec.fx[1][r]) * dxs[1],
+                    d2 = (fo[2] - rec.fx[2][r]) * dxs[2];
+        sm += wt * rec.m[r];
+        s1 += wt * (rec.mom[0][r] + (rec.aff[0][r] * d0 + rec.aff[1][r] * d1 + rec.aff[2][r] * d2));
+        s2 += wt * (rec.mom[1][r] + (rec.aff[3][r] * d0 + rec.aff[4][r] * d1 + rec.aff[5][r] * d2));
+        s3 += wt * (rec.mom[2][r] + (rec.aff[6][r] * d0 + rec.aff[7][r] * d1 + rec.aff[8][r] * d2));
+        s4 += wt * rec.fe[0][r];
+        s5 += wt * rec.fe[1][r];
+        s6 += wt * rec.fe[2][r];
+      }
+      const int b0 = c / (kTile * kTile), b1 = (c / kTile) % kTile, b2 = c % kTile;
+      const int ln = ((b0 + o0) * kHalo + (b1 + o1)) * kHalo + (b2 + o2);
+      atomicAdd(&sacc[0][ln], sm);
+      atomicAdd(&sacc[1][ln], s1);
+      atomicAdd(&sacc[2][ln], s2);
+      atomicAdd(&sacc[3][ln], s3);
+      atomicAdd(&sacc[4][ln], s4);
+      atomicAdd(&sacc[5][ln], s5);
+      atomicAdd(&sacc[6][ln], s6);
+    }
+    __syncthreads();  // records and counts are reused by the next chunk
   }
   __syncthreads();
   if (in_stencil_bucket) {
@@ -743,6 +820,10 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
   const int64_t G = (int64_t)S.nx * S.ny * S.nz;
   const int Pn = S.particle_count;
   double* acc = report_device != nullptr ? P->acc : nullptr;
+  // algorithmic bytes of the substep: 216 per particle (read x, v, C, F, mass,
+  // volume, f_ext, fixed; write x, v, C, F) and 28 per node cleared
+  const bool time_step = timing_enabled(KF_MPM_STEP);
+  if (time_step) timing_begin(KF_MPM_STEP, s);
   EFSI_CUDA_CHECK(cudaMemsetAsync(S.grid_mass, 0, G * sizeof(float), s));
   EFSI_CUDA_CHECK(cudaMemsetAsync(S.grid_velocity, 0, 3 * G * sizeof(float), s));
   EFSI_CUDA_CHECK(cudaMemsetAsync(S.grid_force, 0, 3 * G * sizeof(float), s));
@@ -753,14 +834,20 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
   EFSI_COUNTED k_scan<<<1, 1024, 0, s>>>(P->count, P->ntiles + 1, P->offset, P->cursor);
   EFSI_COUNTED k_bin_scatter<<<pb, 256, 0, s>>>(Pn, P->key, P->offset, P->cursor, P->sorted);
   EFSI_TIMED(KF_P2G, 124.0 * Pn, s,
-             EFSI_COUNTED k_p2g<<<P->ntiles + 1, 256, 0, s>>>(S, P->tx, P->ty, P->tz, P->ntiles, P->sorted, P->offset, dt,
+             EFSI_COUNTED k_p2g<<<P->ntiles + 1, kP2gThreads, 0, s>>>(S, P->tx, P->ty, P->tz, P->ntiles, P->sorted, P->offset, dt,
                                                              mu, lambda_, acc));
-  EFSI_COUNTED k_grid_update<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(S, dt, velocity_damping, acc);
-  EFSI_COUNTED k_g2p<<<pb, 256, 0, s>>>(S, P->sorted, dt, primary_region, secondary_region, acc);
+  // grid update: the mass of every node is read; active nodes add 36 bytes
+  // that are not counted here (a lower bound)
+  EFSI_TIMED(KF_GRID_UPDATE, 4.0 * (double)G, s,
+             EFSI_COUNTED k_grid_update<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(S, dt, velocity_damping, acc));
+  // G2P: read x, F, fixed, region (56 bytes), write x, v, C, F (96 bytes)
+  EFSI_TIMED(KF_G2P, 152.0 * Pn, s,
+             EFSI_COUNTED k_g2p<<<pb, 256, 0, s>>>(S, P->sorted, dt, primary_region, secondary_region, acc));
   if (acc) {
     EFSI_COUNTED k_radial<<<pb, 256, 0, s>>>(S, acc);
     EFSI_COUNTED k_mpm_finalize<<<1, 32, 0, s>>>(acc, dt, report_device);
   }
+  if (time_step) timing_end(KF_MPM_STEP, s, 216.0 * Pn + 28.0 * (double)G);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
