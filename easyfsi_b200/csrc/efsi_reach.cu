@@ -9,10 +9,11 @@
 // (fluid.py:1649-1698 / 4776-4845 read the same rule in both directions).  A
 // cell is reached iff its connected component holds a seed (a fluid,
 // non-barrier, row-free cell at k = 0), and an unreached component's label is
-// its smallest linear cell index.  So here one lock-free union-find over the
-// open faces (every root is the smallest index of its component) gives both;
-// the components are then ranked by their root as the reference ranks its
-// labels (up to 256, the rest keep their raw label).
+// its smallest linear cell index.  So here one connected-components labelling
+// of the open faces (rounds of hooking and pointer jumping; every component
+// ends labelled by its smallest index) gives both; the components are then
+// ranked by their root as the reference ranks its labels (up to 256, the rest
+// keep their raw label).
 #include <algorithm>
 #include <vector>
 
@@ -21,7 +22,7 @@
 struct efsi_reach_plan {
   int32_t* roots = nullptr;  // unreached component roots, appended
   int64_t roots_cap = 0;
-  int32_t* counters = nullptr;  // [0] roots, [1] unreached cells, [2] union retry overflow
+  int32_t* counters = nullptr;  // [0] roots, [1] unreached cells, [2] a hook changed a label this round
   int32_t* table = nullptr;     // the ranked roots (256)
   int32_t* host_counters = nullptr;
 };
@@ -31,7 +32,7 @@ namespace {
 
 constexpr int32_t kNoLabel = 1 << 30;
 constexpr int kComponentCapacity = 256;  // HIBM_PRESSURE_COMPONENT_CAPACITY (fluid.py:17)
-constexpr int kMaxUnionTries = 1 << 20;
+constexpr int kMaxRounds = 4096;  // hook-and-jump rounds before giving up
 
 struct ReachArgs {
   int nx, ny, nz;
@@ -40,7 +41,7 @@ struct ReachArgs {
   const int32_t* vdir;     // may be null
   const int32_t* barrier;  // may be null
   int32_t* reach;
-  int32_t* label;  // parent pointers during the union-find
+  int32_t* label;  // component labels (smallest cell index) while labelling
 };
 
 __device__ __forceinline__ int32_t at(const int32_t* a, int64_t c) { return a == nullptr ? 0 : __ldg(a + c); }
@@ -52,25 +53,6 @@ __device__ __forceinline__ bool node(const ReachArgs& A, int64_t c) {
 // the face below the upper cell u is open
 __device__ __forceinline__ bool face_open(const ReachArgs& A, int64_t u) {
   return at(A.vdir, u) == 0 && at(A.barrier, u) == 0;
-}
-
-// The root of x, shortening the path as it walks (intermediate pointer
-// jumping, as in the ECL-CC connected-components algorithm): a parent always
-// has a smaller index than its child, so every pointer written still points
-// to an ancestor, and roots (changed only by the linking CAS) are never
-// written here.  volatile: other threads relink and shorten concurrently.
-__device__ __forceinline__ int32_t find_root(int32_t* parent_, int32_t x) {
-  volatile int32_t* parent = parent_;
-  int32_t cur = parent[x];
-  if (cur != x) {
-    int32_t prev = x, next;
-    while (cur > (next = parent[cur])) {
-      parent[prev] = next;
-      prev = cur;
-      cur = next;
-    }
-  }
-  return cur;
 }
 
 // node_kind -> barrier (fluid.py:1618-1627), or clear it
@@ -86,41 +68,46 @@ __global__ void k_reach_init(ReachArgs A) {
   A.reach[c] = 0;
 }
 
-// Join every node with its upper neighbours through open faces; the larger
-// root is linked under the smaller, so a root is its component's minimum.
-__global__ void k_reach_union(ReachArgs A, int32_t* overflow) {
+// Connected components by rounds of hooking and pointer jumping.  Every label
+// is a cell of the same component with an index no larger than its own.  A
+// round first hooks: for every open face whose two cells carry different
+// labels, the larger label's cell is pointed (atomicMin) at the smaller label.
+// Then it jumps: every cell follows its labels to the end of the chain, where
+// the label points to itself.  Labels only decrease, and a round whose hooks
+// change nothing leaves every face with equal labels at both ends (the jump of
+// the previous round made every label a chain end), so then each component is
+// labelled by its smallest cell index.  Nothing here depends on the order in
+// which the device's threads see each other's writes.
+__global__ void k_reach_hook(ReachArgs A, int32_t* changed) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= A.n || !node(A, c)) return;
   const int k = (int)(c % A.nz), j = (int)((c / A.nz) % A.ny), i = (int)(c / ((int64_t)A.ny * A.nz));
   const int64_t up[3] = {i < A.nx - 1 ? c + (int64_t)A.ny * A.nz : -1, j < A.ny - 1 ? c + A.nz : -1,
                          k < A.nz - 1 ? c + 1 : -1};
+  bool any = false;
   for (int d = 0; d < 3; ++d) {
     const int64_t u = up[d];
     if (u < 0 || !node(A, u) || !face_open(A, u)) continue;
-    int32_t a = (int32_t)c, b = (int32_t)u;
-    int tries = 0;
-    while (true) {
-      a = find_root(A.label, a);
-      b = find_root(A.label, b);
-      if (a == b) break;
-      if (a < b) {
-        const int32_t t = a;
-        a = b;
-        b = t;
-      }
-      if (atomicCAS(A.label + a, a, b) == a) break;
-      if (++tries >= kMaxUnionTries) {
-        atomicAdd(overflow, 1);
-        break;
-      }
-    }
+    const int32_t a = atomicAdd(A.label + c, 0), b = atomicAdd(A.label + u, 0);
+    if (a == b) continue;
+    const int32_t hi = a > b ? a : b, lo = a > b ? b : a;
+    if (atomicMin(A.label + hi, lo) > lo) any = true;
   }
+  if (any) atomicOr(changed, 1);
 }
 
-__global__ void k_reach_compress(ReachArgs A) {
+__global__ void k_reach_jump(ReachArgs A) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= A.n || A.label[c] == kNoLabel) return;
-  A.label[c] = find_root(A.label, (int32_t)c);
+  if (c >= A.n) return;
+  int32_t l = A.label[c];
+  if (l == kNoLabel) return;
+  // labels strictly decrease along a chain, so the walk ends
+  int32_t next = atomicAdd(A.label + l, 0);
+  while (next < l) {
+    l = next;
+    next = atomicAdd(A.label + l, 0);
+  }
+  atomicMin(A.label + c, l);
 }
 
 // seeds (fluid.py:1714-1725) mark their component's root
@@ -219,15 +206,24 @@ int efsi_outlet_reachability(efsi_reach_plan* P, int32_t nx, int32_t ny, int32_t
   EFSI_CUDA_CHECK(cudaMemsetAsync(P->counters, 0, 4 * sizeof(int32_t), s));
   ReachArgs A{nx, ny, nz, n, obstacle, velocity_dirichlet_active, barrier, reachable, label};
   EFSI_COUNTED k_reach_init<<<grid, 256, 0, s>>>(A);
-  EFSI_COUNTED k_reach_union<<<grid, 256, 0, s>>>(A, P->counters + 2);
-  EFSI_COUNTED k_reach_compress<<<grid, 256, 0, s>>>(A);
+  int rounds = 0;
+  for (;;) {
+    EFSI_CUDA_CHECK(cudaMemsetAsync(P->counters + 2, 0, sizeof(int32_t), s));
+    EFSI_COUNTED k_reach_hook<<<grid, 256, 0, s>>>(A, P->counters + 2);
+    EFSI_COUNTED k_reach_jump<<<grid, 256, 0, s>>>(A);
+    EFSI_LAUNCH_CHECK();
+    EFSI_CUDA_CHECK(cudaMemcpyAsync(P->host_counters + 2, P->counters + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+    ++rounds;
+    if (P->host_counters[2] == 0) break;
+    EFSI_ARG_CHECK(rounds < kMaxRounds, "the component labels did not settle");
+  }
   EFSI_COUNTED k_reach_seed<<<grid, 256, 0, s>>>(A);
   EFSI_COUNTED k_reach_spread<<<grid, 256, 0, s>>>(A, P->roots, P->counters);
   EFSI_LAUNCH_CHECK();
   EFSI_CUDA_CHECK(cudaMemcpyAsync(P->host_counters, P->counters, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
-  const int32_t nroots = P->host_counters[0], unreached = P->host_counters[1], overflow = P->host_counters[2];
-  EFSI_ARG_CHECK(overflow == 0, "the union-find did not settle");
+  const int32_t nroots = P->host_counters[0], unreached = P->host_counters[1];
   int count = 0;
   if (nroots > 0) {
     std::vector<int32_t> roots((size_t)nroots);
