@@ -1,8 +1,11 @@
 """CUDA path vs the CPU oracle on identical seeded inputs (mirror precision).
 
-Tolerances: f64 quantities (pressure, CG vectors, tractions) relative L2
-<= 1e-10 (the operator itself to 1e-13); f32 quantities (velocity,
-divergence, MPM state, marker geometry) relative L2 <= 1e-5.
+Tolerances (relative L2): the operator 1e-13, the V-cycle 1e-13 (the same
+per-row arithmetic and f32 / f64 mix as the oracle), f64 pressure of the PCG
+solves, projections and coupled steps 1e-10; f32 fields that the same
+arithmetic produces (fluid velocity, particle and marker displacement) 1e-6;
+f32 fields summed by atomics in another order (particle velocity, F - I,
+external forces) 1e-5.
 """
 
 import math
@@ -98,7 +101,8 @@ def test_vcycle_matches_oracle(case):
     fl._apply_fv_multigrid_preconditioner(fl.cg_r, pressure_outlet_zmin=False)
     z_gpu = fl.cg_z.to_numpy()
     z_ref = ofl.vcycle(r, 0)
-    assert rel_l2(z_gpu, z_ref) <= 1e-6
+    # same per-row arithmetic and f32 / f64 mix as the oracle: measured 1e-16
+    assert rel_l2(z_gpu, z_ref) <= 1e-13
 
 
 @pytest.mark.parametrize("precond", ["fv_multigrid", "jacobi", "fv_multigrid_light"])
@@ -117,7 +121,9 @@ def test_pcg_solve_matches_oracle(case, precond):
     st = ofl.pcg_solve(outlet=0, max_iters=300, tol=1e-8, precond=code, remove_mean=True)
     assert fl.last_cg_converged and st.converged
     assert fl.last_cg_iterations == st.iterations
-    tol = 1e-10 if precond == "jacobi" else 1e-7
+    # measured on a B200: 4.5e-16 (jacobi), 3.6e-13 (fv_multigrid), 8.5e-11
+    # (fv_multigrid_light, whose f32 coarse levels run more cycles)
+    tol = {"jacobi": 1e-12, "fv_multigrid": 1e-10, "fv_multigrid_light": 1e-9}[precond]
     assert rel_l2(fl.pressure.to_numpy(), ofl.pressure) <= tol
     # true residual of the GPU solution, measured by the oracle operator
     rhs = ofl.rhs0.copy()
@@ -142,14 +148,17 @@ def test_projection_gradient_and_predict(case):
     ofl.pressure[...] = 0.0
     fl.project(iterations=300, dt_s=1e-3, pressure_solver="fv_cg", cg_tolerance=1e-8, cg_preconditioner="fv_multigrid", read_report=False)
     ofl.project(dt=1e-3, max_iters=300, tol=1e-8)
-    assert rel_l2(fl.pressure.to_numpy(), ofl.pressure) <= 1e-7
-    assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) <= 1e-5
+    assert rel_l2(fl.pressure.to_numpy(), ofl.pressure) <= 1e-10
+    assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) <= 1e-6
     fl.predict(1e-3)
     ofl.predict(1e-3)
     assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) <= 1e-5
 
 
 def test_mpm_step_matches_oracle():
+    """20 MPM substeps of a moving block against the oracle: the displacement
+    x - x0, the velocity and F - I (the parts that change; x and F themselves
+    are dominated by x0 and I) to f32 parity, <= 1e-5 relative after 20 steps."""
     from easyfsi_b200.neo_hookean_mpm import NeoHookeanMpmState
 
     rng = np.random.default_rng(5)
@@ -167,29 +176,90 @@ def test_mpm_step_matches_oracle():
     for _ in range(20):
         rep = gpu.step(dt_s=1e-4, mu_pa=1.7e4, lambda_pa=1.6e5, primary_region_id=101, secondary_region_id=202)
         ref.step(dt=1e-4, mu=1.7e4, lam=1.6e5)
-    assert rel_l2(gpu.x.to_numpy()[:n], ref.x[:n]) <= 1e-5
-    assert rel_l2(gpu.v.to_numpy()[:n], ref.v[:n]) <= 1e-4
-    assert rel_l2(gpu.F.to_numpy()[:n], ref.F[:n]) <= 1e-5
+    x64 = x.astype(np.float64)
+    eye = np.eye(3).ravel()
+    err = {
+        "displacement": rel_l2(gpu.x.to_numpy()[:n] - x64, ref.x[:n] - x64),
+        "v": rel_l2(gpu.v.to_numpy()[:n], ref.v[:n]),
+        "F-I": rel_l2(gpu.F.to_numpy()[:n].reshape(n, 9) - eye, ref.F[:n].reshape(n, 9) - eye),
+    }
+    print("mpm 20 steps:", err)
+    assert err["displacement"] <= 1e-5 and err["v"] <= 1e-5 and err["F-I"] <= 1e-5
+    assert np.abs(ref.x[:n] - x64).max() > 5e-6  # the particles really moved
     assert rep.transfer_relative_error < 2e-5
 
 
 def test_coupled_scene_matches_oracle():
+    """The tiny graded coupled scene, every step against the oracle: the same
+    CG iteration counts; pressure (f64) <= 1e-10; velocity, particle
+    displacement and marker positions (f32) <= 1e-7; particle velocity,
+    F - I and the spread external forces (f32, atomic sums in another order)
+    <= 1e-5.  Measured on a B200: pressure <= 3e-12, velocity, displacement
+    and markers bit-identical, v 2e-7, F - I 5e-7, f_ext 2e-7."""
     from easyfsi_b200.scenarios import CoupledScene, tiny_config
 
     cfg = tiny_config()
     gpu = CoupledScene(cfg)
     u0 = gpu.fluid.velocity.to_numpy()
     ref = orc.OracleScene(cfg, variant="mirror", initial_velocity=u0, project_initial=False)
+    n = gpu.solid.particle_count
+    x0 = gpu.solid.x.to_numpy()[:n].astype(np.float64)
+    eye = np.eye(3).ravel()
     for _ in range(cfg.steps):
         gpu.step()
         ref.step()
         assert gpu.last_cg_iterations == ref.last_stats.iterations
-    assert rel_l2(gpu.fluid.pressure.to_numpy(), ref.fluid.pressure) <= 1e-6
-    assert rel_l2(gpu.fluid.velocity.to_numpy(), ref.fluid.velocity) <= 1e-5
+        assert rel_l2(gpu.fluid.pressure.to_numpy(), ref.fluid.pressure) <= 1e-10
+        assert rel_l2(gpu.fluid.velocity.to_numpy(), ref.fluid.velocity) <= 1e-7
+        assert rel_l2(gpu.solid.x.to_numpy()[:n] - x0, ref.solid.x[:n] - x0) <= 1e-7
+        assert rel_l2(gpu.solid.v.to_numpy()[:n], ref.solid.v[:n]) <= 1e-5
+        assert rel_l2(gpu.solid.F.to_numpy()[:n].reshape(n, 9) - eye, ref.solid.F[:n].reshape(n, 9) - eye) <= 1e-5
+        assert rel_l2(gpu.solid.external_force_n.to_numpy()[:n], ref.solid.fext[:n]) <= 1e-5
+        assert rel_l2(gpu.markers.x_gamma_m.to_numpy()[: ref.markers.count], ref.markers.x) <= 1e-7
+
+
+def test_c1_twenty_coupled_steps_match_oracle():
+    """The c1 workload (uniform 64^3, sphere of about 29.6k particles), 20
+    coupled steps on the GPU and on the FP64-oracle mirror from the same
+    state: the same CG iteration count every step; per field relative L2
+    after every step: pressure <= 1e-10 (f64); fluid velocity, particle
+    displacement and marker displacement <= 1e-6 (f32; measured bit-identical);
+    particle velocity, F - I and f_ext <= 1e-5 (f32 atomic sums in other
+    orders; measured <= 1e-6 after 20 steps)."""
+    from easyfsi_b200.scenarios import CONFIGS, CoupledScene
+
+    cfg = CONFIGS["c1"]
+    gpu = CoupledScene(cfg)
+    u0 = gpu.fluid.velocity.to_numpy()
+    ref = orc.OracleScene(cfg, variant="mirror", initial_velocity=u0, project_initial=False)
     n = gpu.solid.particle_count
-    assert rel_l2(gpu.solid.x.to_numpy()[:n], ref.solid.x[:n]) <= 1e-5
-    assert rel_l2(gpu.markers.x_gamma_m.to_numpy()[: ref.markers.count], ref.markers.x) <= 1e-5
-    assert rel_l2(gpu.solid.external_force_n.to_numpy()[:n], ref.solid.fext[:n]) <= 1e-5
+    m = ref.markers.count
+    x0 = gpu.solid.x.to_numpy()[:n].astype(np.float64)
+    m0 = gpu.markers.x_gamma_m.to_numpy()[:m].astype(np.float64)
+    eye = np.eye(3).ravel()
+    worst = {}
+    for step in range(cfg.steps):
+        gpu.step()
+        ref.step()
+        assert gpu.last_cg_iterations == ref.last_stats.iterations, step
+        err = {
+            "pressure": rel_l2(gpu.fluid.pressure.to_numpy(), ref.fluid.pressure),
+            "velocity": rel_l2(gpu.fluid.velocity.to_numpy(), ref.fluid.velocity),
+            "displacement": rel_l2(gpu.solid.x.to_numpy()[:n] - x0, ref.solid.x[:n] - x0),
+            "marker_displacement": rel_l2(gpu.markers.x_gamma_m.to_numpy()[:m] - m0, ref.markers.x - m0),
+            "v": rel_l2(gpu.solid.v.to_numpy()[:n], ref.solid.v[:n]),
+            "F-I": rel_l2(gpu.solid.F.to_numpy()[:n].reshape(n, 9) - eye, ref.solid.F[:n].reshape(n, 9) - eye),
+            "f_ext": rel_l2(gpu.solid.external_force_n.to_numpy()[:n], ref.solid.fext[:n]),
+        }
+        for k, v in err.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+    print("c1 worst per-field relative L2 over 20 steps:", worst)
+    assert worst["pressure"] <= 1e-10
+    for k in ("velocity", "displacement", "marker_displacement"):
+        assert worst[k] <= 1e-6, k
+    for k in ("v", "F-I", "f_ext"):
+        assert worst[k] <= 1e-5, k
+    assert np.abs(ref.solid.x[:n] - x0).max() > 0.0
 
 
 def test_graph_blocks_match_direct_launches(case):
@@ -535,13 +605,14 @@ def test_outlet_reachability_matches_oracle():
         kind = rng.integers(0, 3, nodes).astype(np.int32)
         s.obstacle.from_numpy(obs)
         s.velocity_dirichlet_boundary_active.from_numpy(vd)
-        got = s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(
-            pressure_outlet_zmin=True, node_kind_code=torch.as_tensor(kind, device="cuda"), barrier_node_code=2)
         ref = orc.outlet_reachability(obs, velocity_dirichlet_active=vd, barrier=(kind == 2).astype(np.int32))
-        assert got == ref["unreached"] and ref["unreached"] > 0
-        assert s.last_hibm_pressure_unreached_component_count == ref["components"]
-        np.testing.assert_array_equal(s.hibm_pressure_outlet_reachable.to_numpy(), ref["reachable"])
-        np.testing.assert_array_equal(s.hibm_pressure_unreached_component_label.to_numpy(), ref["label"])
+        for _ in range(3):  # the same answer on every call (no dependence on thread timing)
+            got = s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(
+                pressure_outlet_zmin=True, node_kind_code=torch.as_tensor(kind, device="cuda"), barrier_node_code=2)
+            assert got == ref["unreached"] and ref["unreached"] > 0
+            assert s.last_hibm_pressure_unreached_component_count == ref["components"]
+            np.testing.assert_array_equal(s.hibm_pressure_outlet_reachable.to_numpy(), ref["reachable"])
+            np.testing.assert_array_equal(s.hibm_pressure_unreached_component_label.to_numpy(), ref["label"])
     s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=False)
 
 
@@ -690,8 +761,10 @@ def test_spread_surface_forces_and_body_force_match_oracle(case, sign):
     rep = fl.spread_surface_forces(torch.as_tensor(pos), torch.as_tensor(frc), m, (0.0, 0.0, 0.0), force_sign=sign)
     oref = ofl.spread_surface_forces(pos, frc, force_sign=sign)
     assert rel_l2(fl.force.to_numpy(), ofl.force) <= 1e-6
+    # totals as the oracle reports them (forces whose eight corners are all
+    # solid are dropped, so the grid total differs from the surface total)
     np.testing.assert_allclose(rep.surface_force_n, oref[:3], rtol=1e-5, atol=1e-5)
-    np.testing.assert_allclose(rep.grid_force_n, sign * np.asarray(oref[:3]), rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(rep.grid_force_n, oref[3:6], rtol=1e-5, atol=1e-5)
     imp = fl.apply_body_force(1.0e-3, read_report=True)
     ofl.apply_body_force(1.0e-3)
     assert rel_l2(fl.velocity.to_numpy(), ofl.velocity) <= 1e-6
