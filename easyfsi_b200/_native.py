@@ -53,7 +53,7 @@ class CgStats(Structure):
         ("mean_projection_count", c_int32),
         ("used_mg", c_int32),
         ("used_graphs", c_int32),
-        ("reserved", c_int32),
+        ("learned_iterations", c_int32),
         ("initial_relative_residual", c_double),
         ("relative_residual", c_double),
         ("breakdown_dAd", c_double),
@@ -210,6 +210,21 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_ib_build_boundary_conditions": [ctypes.c_int64, P, P, P, P, P, P, P, I, P, P, P, P, P, P],
     "efsi_ib_velocity_dirichlet_rows": [P, POINTER(IbVdParams), POINTER(IbVdFields), I, P],
     "efsi_fv_bicgstab": [P, P, P, I, I, D, D, I, POINTER(ctypes.c_int64), POINTER(c_double), P],
+    "efsi_conv3d_bf16": [I, I, I, I, I, P, P, P, I, P, P, P, P],
+    "efsi_conv3d_wgrad": [I, I, I, I, I, P, P, P, P],
+    "efsi_unet_create": [I, POINTER(c_void_p)],
+    "efsi_unet_destroy": [P],
+    "efsi_unet_param_count": [P, POINTER(ctypes.c_int64)],
+    "efsi_unet_layer_offsets": [P, P, P, P],
+    "efsi_unet_get_params": [P, P, P],
+    "efsi_unet_set_params": [P, P],
+    "efsi_unet_forward": [P, I, I, I, P, P, P],
+    "efsi_unet_accumulate_gradient": [P, I, I, I, P, P, P, POINTER(c_double), P],
+    "efsi_unet_backward_from": [P, I, I, I, P, P, P],
+    "efsi_unet_zero_grad": [P, P],
+    "efsi_unet_adam_step": [P, F, F, F, F, P],
+    "efsi_fv_set_learned_preconditioner": [P, P, P],
+    "efsi_fv_learned_input": [P, P, P, P],
     "efsi_reach_plan_create": [POINTER(c_void_p)],
     "efsi_reach_plan_destroy": [P],
     "efsi_outlet_reachability": [P, I, I, I, P, P, P, P, I, I, P, P, POINTER(ReachReport), P],

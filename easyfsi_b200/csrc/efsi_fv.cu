@@ -39,6 +39,8 @@
 #include <vector>
 
 #include "efsi_fv_internal.cuh"
+#include "efsi_unet_internal.cuh"
+#include <cuda_bf16.h>
 #include "efsi_march.cuh"
 
 namespace efsi {
@@ -1109,6 +1111,79 @@ __global__ void __launch_bounds__(256) k_jacobi_precond(LevelDev L, const double
   }
 }
 
+// Learned preconditioner (code 4).  k_learned_sumsq reduces sum_fluid r^2 V
+// into sc->dot; k_learned_pack forms the network input (r over its
+// volume-weighted RMS, fluid mask, log2 cell widths over the finest width);
+// k_learned_unpack writes z = RMS * output channel 0 on the fluid cells and,
+// with the zero-mean projection, the z mean (as the Jacobi preconditioner).
+__global__ void __launch_bounds__(256) k_learned_sumsq(LevelDev L, const double* __restrict__ r, double* partials,
+                                                       CgScalars* sc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  double a = 0.0;
+  if (active && (__ldg(L.mask + c) & M_FLUID)) {
+    const double rv = __ldg(r + c);
+    a = rv * rv * vol64(L, i, j, k);
+  }
+  double v[1] = {a}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) sc->dot = t[0];
+  }
+}
+
+__device__ __forceinline__ double learned_rms(const CgScalars* sc) {
+  const double ms = sc->free_vol > 0.0 ? sc->dot / sc->free_vol : 0.0;
+  return ms > 0.0 ? sqrt(ms) : 1.0;
+}
+
+__global__ void __launch_bounds__(256) k_learned_pack(LevelDev L, const double* __restrict__ r,
+                                                      __nv_bfloat16* __restrict__ in, float wx0, float wy0, float wz0,
+                                                      const CgScalars* sc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const bool fluid = (__ldg(L.mask + c) & M_FLUID) != 0;
+  const float inv = (float)(1.0 / learned_rms(sc));
+  float ch[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) ch[q] = 0.0f;
+  ch[0] = fluid ? (float)__ldg(r + c) * inv : 0.0f;
+  ch[1] = fluid ? 1.0f : 0.0f;
+  ch[2] = log2f(__ldg(L.wx + i) / wx0);
+  ch[3] = log2f(__ldg(L.wy + j) / wy0);
+  ch[4] = log2f(__ldg(L.wz + k) / wz0);
+  __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) hb[q] = __float2bfloat16_rn(ch[q]);
+  uint4* dst = reinterpret_cast<uint4*>(in + c * 16);
+  dst[0] = reinterpret_cast<const uint4*>(hb)[0];
+  dst[1] = reinterpret_cast<const uint4*>(hb)[1];
+}
+
+__global__ void __launch_bounds__(256) k_learned_unpack(LevelDev L, const float* __restrict__ out,
+                                                        double* __restrict__ z, int want_mean, double* partials,
+                                                        CgScalars* sc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  double pz = 0.0;
+  if (active) {
+    const unsigned m = __ldg(L.mask + c);
+    double zv = 0.0;
+    if (m & M_FLUID) zv = (double)__ldg(out + c * 16) * learned_rms(sc);
+    z[c] = zv;
+    if (m & M_FLUID) pz = zv * vol64(L, i, j, k);
+  }
+  if (want_mean) {
+    double v[1] = {pz}, t[1];
+    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+      if (flat_tid() == 0) {
+        sc->mean_z = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+        sc->zproj = 1;
+      }
+    }
+  }
+}
+
 // fluid.py:4677-4693 with multiplier -1 on the level-0 rhs, plus the free
 // volume (computed in the same pass as the reference does).
 __global__ void __launch_bounds__(256) k_rhs_mean(LevelDev L, const double* __restrict__ rhs, double multiplier,
@@ -1657,6 +1732,7 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   cudaFree(P->sc);
   cudaFree(P->aux);
   cudaFree(P->bicg_work);
+  cudaFree(P->unet_in);
   if (P->host_sc) cudaFreeHost(P->host_sc);
   delete P;
   return EFSI_OK;
@@ -2245,6 +2321,7 @@ struct PcgRun {
   bool copy_next;  // next SpMV starts a fresh direction d = z'
   bool dots_fused;  // the last preconditioner sweep also finished the PCG dots
   bool mixed;       // FP32 level-0 V-cycle
+  bool learned;     // the attached network (code 4)
 };
 
 static int read_scalars(PcgRun& R) {
@@ -2261,7 +2338,17 @@ static int read_scalars(PcgRun& R) {
 static int precondition(PcgRun& R) {
   const bool want_mean = R.prm->remove_mean != 0;
   R.dots_fused = false;
-  if (R.use_mg) {
+  if (R.learned) {
+    efsi_fv_plan* P = R.P;
+    __nv_bfloat16* in = static_cast<__nv_bfloat16*>(P->unet_in);
+    EFSI_COUNTED launch_pdl(k_learned_sumsq, R.S.grid, R.S.block, 0, R.s, R.L, P->r, P->partials, P->sc);
+    EFSI_COUNTED launch_pdl(k_learned_pack, R.S.grid, R.S.block, 0, R.s, R.L, (const double*)P->r, in, P->unet_wmin[0],
+                            P->unet_wmin[1], P->unet_wmin[2], (const CgScalars*)P->sc);
+    const float* out = nullptr;
+    EFSI_TRY(unet_run(P->unet, in, &P->sc->fault, &out, R.s));
+    EFSI_COUNTED launch_pdl(k_learned_unpack, R.S.grid, R.S.block, 0, R.s, R.L, out, P->z, want_mean ? 1 : 0,
+                            P->partials, P->sc);
+  } else if (R.use_mg) {
     // with the zero-mean projection the V-cycle's last sweep finishes the dots
     // (EFSI_SEPARATE_DOTS keeps them in their own kernel)
     static const bool separate = std::getenv("EFSI_SEPARATE_DOTS") != nullptr;
@@ -2287,6 +2374,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   cudaStream_t s = as_stream(stream);
   PcgRun R;
   R.mixed = false;
+  R.learned = false;
   R.dots_fused = false;
   R.P = P;
   R.prm = prm;
@@ -2341,7 +2429,16 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     st->converged = 1;
     return EFSI_OK;
   }
-  R.use_mg = P->n_levels > 1 && !prm->iface_active && (prm->precond == 1 || prm->precond == 2 || prm->precond == 3);
+  // 4: the learned network; the flexible beta of the V-cycle path applies to
+  // it, and the 2/24/2 V-cycle (or Jacobi when no V-cycle applies) takes over
+  // when it stalls.
+  if (prm->precond == 4) {
+    EFSI_ARG_CHECK(P->unet != nullptr && P->unet_in != nullptr,
+                   "cg_preconditioner 'learned' needs a network (efsi_fv_set_learned_preconditioner)");
+  }
+  const bool mg_possible = P->n_levels > 1 && !prm->iface_active;
+  R.learned = prm->precond == 4;
+  R.use_mg = R.learned || (mg_possible && (prm->precond == 1 || prm->precond == 2 || prm->precond == 3));
   // 3: the FP32 level-0 V-cycle.  It needs the plane-marching kernels on
   // level 0 with TMA maps of all three fields (mask rows of 16-byte multiples:
   // nz % 16 == 0) and no interface diagonal; otherwise the f64 V-cycle runs.
@@ -2358,6 +2455,16 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   EFSI_LAUNCH_CHECK();
   EFSI_TRY(read_scalars(R));
   double rz = P->host_sc->rz;
+  if (R.learned && (!std::isfinite(rz) || rz <= 0.0)) {
+    // the network's first z is not a descent direction: the V-cycle takes over
+    R.learned = false;
+    R.use_mg = mg_possible;
+    EFSI_TRY(precondition(R));
+    EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
+    EFSI_LAUNCH_CHECK();
+    EFSI_TRY(read_scalars(R));
+    rz = P->host_sc->rz;
+  }
   if (!std::isfinite(rz) || std::fabs(rz) <= 1.0e-300) {
     // Downgrade to Jacobi; the reference does not re-project z here.
     R.use_mg = false;
@@ -2477,7 +2584,8 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   };
   auto run_block = [&](bool cont) -> int {
     if (!prm->use_graphs || P->graphs_disabled) return launch_block(cont);
-    const PcgGraphKey key{cont, R.use_mg, remove_mean, outlet, R.pre, R.coarse, R.post, pressure, R.mixed};
+    PcgGraphKey key{cont, R.use_mg, remove_mean, outlet, R.pre, R.coarse, R.post, pressure, R.mixed};
+    key.learned = R.learned;
     cudaGraphExec_t exec = nullptr;
     for (auto& g : P->graphs)
       if (g.key == key) exec = g.exec;
@@ -2520,6 +2628,10 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   bool pending = false;  // preconditioner + dots of the previous iteration not launched yet
   int n_precond = 0;     // preconditioner applications inside the loop
   int it = 1;
+  // the learned preconditioner must cut the residual by this factor over every
+  // 16-iteration block, or the V-cycle takes over
+  constexpr double kLearnedBlockReduction = 0.5;
+  double learned_prev = st->initial_relative_residual;
   while (it <= max_iters) {
     const bool block = ((it - 1) % 16 == 0) && (it + 15 <= max_iters) && (pending || R.copy_next);
     if (block) {
@@ -2559,6 +2671,41 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       break;
     }
     const int code = P->host_sc->code;
+    if (R.learned) st->learned_iterations = it;
+    if (R.learned && it < max_iters && (code != 0 || !(st->relative_residual <= kLearnedBlockReduction * learned_prev))) {
+      // fallback: restart from the exact residual with the V-cycle
+      R.learned = false;
+      R.use_mg = mg_possible;
+      EFSI_TRY(true_residual());
+      r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+      st->relative_residual = r_norm / b_norm;
+      if (st->relative_residual <= tol) {
+        st->converged = 1;
+        break;
+      }
+      EFSI_TRY(precondition(R));
+      if (remove_mean) st->mean_projection_count += 1;
+      EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
+      EFSI_LAUNCH_CHECK();
+      EFSI_TRY(read_scalars(R));
+      rz = P->host_sc->rz;
+      CgScalars* hs = P->host_sc;
+      hs->code = 0;
+      hs->code_dAd = 0.0;
+      EFSI_CUDA_CHECK(cudaMemcpyAsync(&P->sc->code, &hs->code, sizeof(int), cudaMemcpyHostToDevice, s));
+      EFSI_CUDA_CHECK(cudaMemcpyAsync(&P->sc->code_dAd, &hs->code_dAd, sizeof(double), cudaMemcpyHostToDevice, s));
+      EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (!std::isfinite(rz) || rz <= 0.0) {
+        st->breakdown_reason = 3;
+        break;
+      }
+      R.copy_next = true;
+      pending = false;
+      st->restart_count += 1;
+      ++it;
+      continue;
+    }
+    if (R.learned) learned_prev = st->relative_residual;
     if (code != 0) {
       st->breakdown_dAd = P->host_sc->code_dAd;
       if (it < max_iters) {
@@ -2876,6 +3023,52 @@ int efsi_cg_compute_alpha(efsi_fv_plan* P, void* stream) {
 int efsi_cg_compute_beta(efsi_fv_plan* P, int32_t use_mg, void* stream) {
   EFSI_ARG_CHECK(P != nullptr, "null plan");
   EFSI_COUNTED k_cg_beta<<<1, 1, 0, as_stream(stream)>>>(P->sc, use_mg);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int efsi_fv_set_learned_preconditioner(efsi_fv_plan* P, efsi_unet* net, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  cudaStream_t s = as_stream(stream);
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (net == nullptr) {
+    P->unet = nullptr;
+    return EFSI_OK;
+  }
+  const LevelBuf& B = P->lv[0];
+  EFSI_TRY(unet_prepare(net, B.nx, B.ny, B.nz));
+  if (P->unet_in == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&P->unet_in, (size_t)B.n * 16 * sizeof(__nv_bfloat16)));
+  // finest width per axis, for the input's width channels
+  const float* w[3] = {B.wx, B.wy, B.wz};
+  const int n[3] = {B.nx, B.ny, B.nz};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<float> h((size_t)n[a]);
+    EFSI_CUDA_CHECK(cudaMemcpy(h.data(), w[a], n[a] * sizeof(float), cudaMemcpyDeviceToHost));
+    P->unet_wmin[a] = *std::min_element(h.begin(), h.end());
+  }
+  P->unet = net;
+  // graphs captured with another network's buffers are not reused
+  for (PcgGraph& g : P->graphs) cudaGraphExecDestroy(g.exec);
+  P->graphs.clear();
+  return EFSI_OK;
+}
+
+int efsi_fv_learned_input(efsi_fv_plan* P, const double* r, void* input, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(r != nullptr && input != nullptr, "null argument");
+  EFSI_ARG_CHECK(P->unet != nullptr, "no learned preconditioner attached (its finest widths define the input)");
+  cudaStream_t s = as_stream(stream);
+  const LevelDev L = level_dev(P, 0);
+  const Shape3 S = P->lv[0].shape;
+  // the free volume and r's RMS as the solve computes them
+  EFSI_COUNTED k_rhs_mean<<<S.grid, S.block, 0, s>>>(L, r, 0.0, P->partials, P->sc);
+  EFSI_COUNTED k_learned_sumsq<<<S.grid, S.block, 0, s>>>(L, r, P->partials, P->sc);
+  EFSI_COUNTED k_learned_pack<<<S.grid, S.block, 0, s>>>(L, r, static_cast<__nv_bfloat16*>(input), P->unet_wmin[0],
+                                                         P->unet_wmin[1], P->unet_wmin[2], (const CgScalars*)P->sc);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }

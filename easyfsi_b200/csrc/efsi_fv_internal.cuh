@@ -208,13 +208,16 @@ struct LevelBuf {
 
 }  // namespace efsi
 
+struct efsi_unet;
+
 struct PcgGraphKey {
   bool cont, use_mg, remove_mean;
   int outlet, pre, coarse, post;
   const double* pressure;
   bool mixed;  // FP32 level-0 V-cycle
+  bool learned = false;  // the learned preconditioner
   bool operator==(const PcgGraphKey& o) const {
-    return cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
+    return learned == o.learned && cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
            pre == o.pre && coarse == o.coarse && post == o.post && pressure == o.pressure && mixed == o.mixed;
   }
 };
@@ -245,6 +248,9 @@ struct efsi_fv_plan {
   size_t partials_len = 0;
   double* aux = nullptr;  // 16 doubles of statistics scratch
   double* bicg_work = nullptr;  // BiCGSTAB fallback's nine level-0 work vectors, allocated at its first use
+  efsi_unet* unet = nullptr;    // learned preconditioner (code 4), not owned
+  void* unet_in = nullptr;      // its BF16 input [n0][16]
+  float unet_wmin[3] = {1.0f, 1.0f, 1.0f};  // finest level-0 width per axis
   efsi::CgScalars* sc = nullptr;
   efsi::CgScalars* host_sc = nullptr;  // pinned readback
   bool has_vdir = false;

@@ -56,8 +56,8 @@ __all__ = [
 # "fv_multigrid_mixed" (no reference counterpart): the fv_multigrid V-cycle
 # with FP32 storage and arithmetic on level 0, inside the same FP64 flexible CG
 # (true residual, inner products and scalars in FP64).
-CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light", "fv_multigrid_mixed")
-_PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2, "fv_multigrid_mixed": 3}
+CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light", "fv_multigrid_mixed", "learned")
+_PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2, "fv_multigrid_mixed": 3, "learned": 4}
 _BREAKDOWN_TEXT = {
     0: "",
     1: "initial residual/preconditioner dot is not positive finite",
@@ -350,6 +350,17 @@ class CartesianFluidSolver:
         7: "BiCGSTAB omega is not finite",
         8: "BiCGSTAB fallback did not converge",
     }
+
+    def set_learned_preconditioner(self, network) -> None:
+        """Attaches a trained ``easyfsi_b200.learned.UNetPreconditioner`` as
+        ``cg_preconditioner="learned"`` (no counterpart in the reference):
+        z = network(r) inside the flexible PCG, with the multigrid V-cycle
+        taking over when a 16-iteration block does not halve the residual.
+        ``None`` detaches it."""
+        self._refresh_structure()
+        handle = None if network is None else network.handle
+        _native.call("efsi_fv_set_learned_preconditioner", self._plan, handle, _stream())
+        self._learned_network = network
 
     _CG_SCALAR_FIELDS = (("rz", "cg_rz"), ("rz_new", "cg_rz_new"), ("dAd", "cg_dAd"),
                          ("beta_numerator", "cg_beta_numerator"), ("alpha", "cg_alpha"), ("beta", "cg_beta"),
@@ -904,6 +915,7 @@ class CartesianFluidSolver:
         self.last_cg_breakdown_dAd = float(stats.breakdown_dAd)
         self.last_cg_used_multigrid = bool(stats.used_mg)
         self.last_cg_used_graphs = bool(stats.used_graphs)
+        self.last_cg_learned_iterations = int(stats.learned_iterations)
         if use_graphs and not stats.used_graphs:
             self.last_cg_graph_error = _native.load().efsi_fv_graph_error(self._plan).decode(errors="replace")
         self._last_cg_breakdown_code = int(stats.breakdown_code)

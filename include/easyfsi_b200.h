@@ -157,7 +157,9 @@ typedef struct efsi_pcg_params {
   int32_t max_iters;
   int32_t precond;      /* 0 jacobi, 1 fv_multigrid (2/24/2), 2 fv_multigrid_light (1/12/1),
                            3 fv_multigrid_mixed: the 2/24/2 V-cycle with FP32 level-0 iterates and
-                           arithmetic (no reference counterpart; the CG stays FP64) */
+                           arithmetic (no reference counterpart; the CG stays FP64),
+                           4 learned: the network attached by efsi_fv_set_learned_preconditioner,
+                           falling back to the 2/24/2 V-cycle (no reference counterpart) */
   int32_t remove_mean;  /* closed-domain zero-mean projection */
   int32_t outlet;       /* pressure_outlet_zmin */
   int32_t iface_active; /* interface terms present: MG disabled, restart every 256 */
@@ -175,7 +177,8 @@ typedef struct efsi_cg_stats {
   int32_t mean_projection_count;
   int32_t used_mg;
   int32_t used_graphs; /* the 16-iteration blocks ran as CUDA graphs */
-  int32_t reserved;
+  int32_t learned_iterations; /* iterations preconditioned by the learned network (code 4) before any
+                                 fallback to the V-cycle */
   double initial_relative_residual;
   double relative_residual;
   double breakdown_dAd;
@@ -538,6 +541,69 @@ int efsi_outlet_reachability(efsi_reach_plan* plan, int32_t nx, int32_t ny, int3
                              const int32_t* velocity_dirichlet_active, int32_t* barrier, const int32_t* node_kind,
                              int32_t barrier_code, int32_t update_barrier, int32_t* reachable, int32_t* label,
                              efsi_reach_report* report, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned preconditioner (no counterpart in the reference: a new
+ * preconditioner for the reference's flexible PCG, fluid.py:6535-6811, whose
+ * multigrid V-cycle stays the fallback).  A 3-D convolutional U-Net (4
+ * levels, 16/32/48/64 channels, 15 convolutions of 3x3x3, about 0.69 M
+ * parameters) on channels-last BF16 volumes; convolutions on the tensor cores
+ * (tcgen05, FP32 accumulation), weight gradients and Adam in FP32.
+ * ------------------------------------------------------------------------ */
+typedef struct efsi_unet efsi_unet;
+
+/* One 3x3x3 convolution, zero padded, of x (BF16 [n][cin]) with w (BF16
+ * [cout][27][cin], tap t = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1)), plus the
+ * bias and an optional ReLU; writes BF16 y [n][cout] and/or FP32 yf.  cin and
+ * cout are multiples of 16.  A pipeline wait that gives up sets
+ * *error_device. */
+int efsi_conv3d_bf16(int32_t nx, int32_t ny, int32_t nz, int32_t cin, int32_t cout, const void* x, const void* w,
+                     const float* bias, int32_t relu, void* y, float* yf, int32_t* error_device, void* stream);
+
+/* Weight gradient of that convolution: dw[co][t][ci] += sum_v dy[v][co]
+ * x[v + off(t)][ci] (FP32 accumulation into dw). */
+int efsi_conv3d_wgrad(int32_t nx, int32_t ny, int32_t nz, int32_t cin, int32_t cout, const void* x,
+                      const void* dy, float* dw, void* stream);
+
+/* The network: He-normal weights from `seed`, zero biases. */
+int efsi_unet_create(int32_t seed, efsi_unet** out);
+int efsi_unet_destroy(efsi_unet* net);
+int efsi_unet_param_count(efsi_unet* net, int64_t* count);
+/* Per layer (15): weight and bias offsets in the packed parameter vector, and
+ * (level, cin, cout, relu). */
+int efsi_unet_layer_offsets(efsi_unet* net, int64_t* weight_offsets, int64_t* bias_offsets, int32_t* shapes);
+/* FP32 parameters and accumulated gradients to the host (either may be NULL). */
+int efsi_unet_get_params(efsi_unet* net, float* host_params, float* host_grads);
+/* Loads FP32 parameters from the host and resets the Adam state. */
+int efsi_unet_set_params(efsi_unet* net, const float* host_params);
+/* Forward pass of a volume: input BF16 [n][16]; output FP32 [n][16]
+ * (channel 0 is the network output) or NULL.  Synchronises the stream. */
+int efsi_unet_forward(efsi_unet* net, int32_t nx, int32_t ny, int32_t nz, const void* input, float* output,
+                      void* stream);
+/* Forward, masked mean-square loss of output channel 0 against target (FP32
+ * [n]; mask FP32 [n]) and backward; gradients are accumulated.  Writes the
+ * loss to *loss_host and synchronises the stream. */
+int efsi_unet_accumulate_gradient(efsi_unet* net, int32_t nx, int32_t ny, int32_t nz, const void* input,
+                                  const float* target, const float* mask, double* loss_host, void* stream);
+/* Forward and backward from a given output gradient dout (FP32 [n][16]);
+ * gradients are accumulated (gradient checks). */
+int efsi_unet_backward_from(efsi_unet* net, int32_t nx, int32_t ny, int32_t nz, const void* input,
+                            const float* dout, void* stream);
+int efsi_unet_zero_grad(efsi_unet* net, void* stream);
+/* One Adam step on the accumulated gradients (which it clears). */
+int efsi_unet_adam_step(efsi_unet* net, float lr, float beta1, float beta2, float eps, void* stream);
+
+/* Attaches a network to a solver plan as preconditioner code 4 of
+ * efsi_fv_pcg_solve (NULL detaches): z = net(r) inside the flexible PCG, with
+ * the multigrid V-cycle taking over when a 16-iteration block does not reduce
+ * the residual.  Allocates the network's workspace for level 0 (call before
+ * any stream capture); synchronises. */
+int efsi_fv_set_learned_preconditioner(efsi_fv_plan* plan, efsi_unet* net, void* stream);
+
+/* The network input of the plan's level 0 for residual r (f64): channel 0 r
+ * scaled to unit volume-weighted RMS over the fluid cells, 1 the fluid mask,
+ * 2-4 log2 of the cell widths over the finest width of each axis (BF16 [n][16]). */
+int efsi_fv_learned_input(efsi_fv_plan* plan, const double* r, void* input, void* stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop
