@@ -58,6 +58,7 @@ class CgStats(Structure):
         ("relative_residual", c_double),
         ("breakdown_dAd", c_double),
         ("b_norm", c_double),
+        ("learned_relative_residual", c_double),
     ]
 
 

@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(256) kt_spmv_dir(LevelDev L, const double* __r
   double v[1] = {part}, t[1];
   if (grid_sum<1>(v, partials, &sc->ticket, t)) {
     if (flat_tid() == 0) {
-      cg_alpha_step(sc, t[0]);
+      spmv_alpha(sc, t[0]);
     }
   }
 }
@@ -966,7 +966,7 @@ __global__ void __launch_bounds__(256) k_spmv_dir(LevelDev L, const double* __re
   double v[1] = {part}, t[1];
   if (grid_sum<1>(v, partials, &sc->ticket, t)) {
     if (flat_tid() == 0) {
-      cg_alpha_step(sc, t[0]);
+      spmv_alpha(sc, t[0]);
     }
   }
 }
@@ -2432,12 +2432,13 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   // 4: the learned network; the flexible beta of the V-cycle path applies to
   // it, and the 2/24/2 V-cycle (or Jacobi when no V-cycle applies) takes over
   // when it stalls.
-  if (prm->precond == 4) {
+  if (prm->precond == 4 || prm->precond == 5) {
     EFSI_ARG_CHECK(P->unet != nullptr && P->unet_in != nullptr,
                    "cg_preconditioner 'learned' needs a network (efsi_fv_set_learned_preconditioner)");
   }
   const bool mg_possible = P->n_levels > 1 && !prm->iface_active;
-  R.learned = prm->precond == 4;
+  R.learned = prm->precond == 4 || prm->precond == 5;
+  const bool learned_fallback = prm->precond == 4;
   R.use_mg = R.learned || (mg_possible && (prm->precond == 1 || prm->precond == 2 || prm->precond == 3));
   // 3: the FP32 level-0 V-cycle.  It needs the plane-marching kernels on
   // level 0 with TMA maps of all three fields (mask rows of 16-byte multiples:
@@ -2455,7 +2456,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   EFSI_LAUNCH_CHECK();
   EFSI_TRY(read_scalars(R));
   double rz = P->host_sc->rz;
-  if (R.learned && (!std::isfinite(rz) || rz <= 0.0)) {
+  if (R.learned && learned_fallback && (!std::isfinite(rz) || rz <= 0.0)) {
     // the network's first z is not a descent direction: the V-cycle takes over
     R.learned = false;
     R.use_mg = mg_possible;
@@ -2671,8 +2672,12 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       break;
     }
     const int code = P->host_sc->code;
-    if (R.learned) st->learned_iterations = it;
-    if (R.learned && it < max_iters && (code != 0 || !(st->relative_residual <= kLearnedBlockReduction * learned_prev))) {
+    if (R.learned) {
+      st->learned_iterations = it;
+      st->learned_relative_residual = st->relative_residual;
+    }
+    if (R.learned && learned_fallback && it < max_iters &&
+        (code != 0 || !(st->relative_residual <= kLearnedBlockReduction * learned_prev))) {
       // fallback: restart from the exact residual with the V-cycle
       R.learned = false;
       R.use_mg = mg_possible;

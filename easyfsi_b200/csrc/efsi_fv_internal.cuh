@@ -53,11 +53,23 @@ struct CgScalars {
   int zproj;  // 1: consumers of z apply the zero-mean projection on the fly
   unsigned ticket;
   int fault;  // a plane-marching kernel's stage copy did not complete in time
+  int defer_alpha;  // interface couplings follow the SpMV: its finisher stores dAd only
 };
 
 // fluid.py:4567-4574 _cg_compute_alpha_kernel on the device scalars: alpha =
 // rz / dAd, or breakdown code 1 (and the first offending dAd) when dAd <= 0.
 // Shared by every SpMV finisher and by efsi_cg_compute_alpha.
+__device__ __forceinline__ void cg_alpha_step(CgScalars* sc, double dAd);
+
+// The SpMV finishers: alpha now, or (interface couplings still to come) only
+// the operator's part of dAd.
+__device__ __forceinline__ void spmv_alpha(CgScalars* sc, double dAd) {
+  if (sc->defer_alpha)
+    sc->dAd = dAd;
+  else
+    cg_alpha_step(sc, dAd);
+}
+
 __device__ __forceinline__ void cg_alpha_step(CgScalars* sc, double dAd) {
   sc->dAd = dAd;
   sc->alpha = 0.0;
@@ -216,8 +228,9 @@ struct PcgGraphKey {
   const double* pressure;
   bool mixed;  // FP32 level-0 V-cycle
   bool learned = false;  // the learned preconditioner
+  bool coupled = false;  // interface-coupling kernels follow the SpMV
   bool operator==(const PcgGraphKey& o) const {
-    return learned == o.learned && cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
+    return learned == o.learned && coupled == o.coupled && cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
            pre == o.pre && coarse == o.coarse && post == o.post && pressure == o.pressure && mixed == o.mixed;
   }
 };
@@ -251,6 +264,16 @@ struct efsi_fv_plan {
   efsi_unet* unet = nullptr;    // learned preconditioner (code 4), not owned
   void* unet_in = nullptr;      // its BF16 input [n0][16]
   float unet_wmin[3] = {1.0f, 1.0f, 1.0f};  // finest level-0 width per axis
+  // interface-coupling terms of the level-0 operator as rows of (source cell,
+  // coefficient) entries per receiving cell; the row count lives on the
+  // device (cpl_n) so captured graphs stay valid when the couplings change
+  int32_t* cpl_rows = nullptr;
+  int32_t* cpl_ptr = nullptr;
+  int32_t* cpl_src = nullptr;
+  double* cpl_coef = nullptr;
+  int32_t* cpl_n = nullptr;
+  int64_t cpl_cap_rows = 0, cpl_cap_ent = 0;
+  int cpl_nrows = 0;  // host copy
   efsi::CgScalars* sc = nullptr;
   efsi::CgScalars* host_sc = nullptr;  // pinned readback
   bool has_vdir = false;

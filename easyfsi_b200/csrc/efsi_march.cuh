@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(kMK* kTY, 3)
   double v[1] = {op.part}, t[1];
   if (grid_sum<1>(v, partials, &sc->ticket, t)) {
     if (flat_tid() == 0) {
-      cg_alpha_step(sc, t[0]);
+      spmv_alpha(sc, t[0]);
     }
   }
 }

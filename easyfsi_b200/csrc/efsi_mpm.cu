@@ -21,6 +21,7 @@ namespace efsi {
 constexpr int kTile = 4;             // nodes per tile edge
 constexpr int kHalo = kTile + 2;     // node block touched by a tile's particles
 constexpr int kHaloN = kHalo * kHalo * kHalo;
+constexpr int kTileCells = kTile * kTile * kTile;  // nodes (and base cells) per tile
 
 // Report accumulator slots (doubles), see k_mpm_finalize for the packing.
 enum {
@@ -64,6 +65,15 @@ struct efsi_mpm_plan {
   int32_t* offset = nullptr;  // ntiles + 2
   int32_t* cursor = nullptr;  // ntiles + 1
   double* acc = nullptr;      // report accumulators
+  // Tiles that hold particles (P2G runs only over them) and the tiles whose
+  // nodes their stencils reach (cleared and updated).  The grid outside the
+  // reached tiles stays zero: each step clears the tiles reached in this step
+  // and in the previous one.
+  int32_t* active = nullptr;     // ntiles + 1 tile ids
+  uint8_t* reached_flag = nullptr;  // ntiles
+  int32_t* reached[2] = {nullptr, nullptr};  // ntiles tile ids: this step's and the previous step's
+  int32_t* counts = nullptr;     // [0] active, [1] reached now, [2] reached in the previous step
+  int cur = 0;                   // which reached list is this step's
 };
 
 namespace efsi {
@@ -219,7 +229,8 @@ __device__ int clamp_deformation(const float F[9], float Fp[9]) {
 // ---------------------------------------------------------------------------
 // Binning
 // ---------------------------------------------------------------------------
-__global__ void k_bin_keys(efsi_mpm_state S, int tx, int ty, int tz, int ntiles, int32_t* key, int32_t* count) {
+__global__ void k_bin_keys(efsi_mpm_state S, int tx, int ty, int tz, int ntiles, int32_t* key, int32_t* count,
+                           uint8_t* reached) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= S.particle_count) return;
   float X[3];
@@ -227,7 +238,13 @@ __global__ void k_bin_keys(efsi_mpm_state S, int tx, int ty, int tz, int ntiles,
   int kk = ntiles;  // out-of-stencil bucket
   if (!stencil_oob(S, X)) {
     int b0 = (int)floorf(X[0] - 0.5f), b1 = (int)floorf(X[1] - 0.5f), b2 = (int)floorf(X[2] - 0.5f);
-    kk = ((b0 / kTile) * ty + (b1 / kTile)) * tz + (b2 / kTile);
+    const int t0 = b0 / kTile, t1 = b1 / kTile, t2 = b2 / kTile;
+    kk = (t0 * ty + t1) * tz + t2;
+    // the stencil's nodes (base .. base + 2) lie in this tile and the next one per axis
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 2; ++c)
+          if (t0 + a < tx && t1 + b < ty && t2 + c < tz) reached[((t0 + a) * ty + (t1 + b)) * tz + (t2 + c)] = 1;
   }
   key[p] = kk;
   // warp-aggregated histogram increment
@@ -296,6 +313,43 @@ __device__ __forceinline__ void block_max(double* acc, int slot, double v) {
   __syncthreads();
 }
 
+// Lists of the occupied tiles (+ the out-of-stencil bucket when it holds
+// particles) and of the reached tiles.
+__global__ void k_tile_lists(int ntiles, const int32_t* __restrict__ count, const uint8_t* __restrict__ reached_flag,
+                             int32_t* active, int32_t* reached, int32_t* counts) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > ntiles) return;
+  if (count[t] > 0) active[atomicAdd(counts, 1)] = t;
+  if (t < ntiles && reached_flag[t]) reached[atomicAdd(counts + 1, 1)] = t;
+}
+
+__device__ __forceinline__ bool tile_node(const efsi_mpm_state& S, int tile, int q, int ty, int tz, int64_t& g) {
+  const int t2 = tile % tz, t1 = (tile / tz) % ty, t0 = tile / (tz * ty);
+  const int g0 = t0 * kTile + q / (kTile * kTile), g1 = t1 * kTile + (q / kTile) % kTile, g2 = t2 * kTile + q % kTile;
+  if (g0 >= S.nx || g1 >= S.ny || g2 >= S.nz) return false;
+  g = nidx(g0, g1, g2, S.ny, S.nz);
+  return true;
+}
+
+// Zeroes mass, momentum and force of the nodes of the tiles reached in this
+// step and in the previous one (one warp-pair per tile, 64 nodes).
+__global__ void __launch_bounds__(256) k_clear_reached(efsi_mpm_state S, int ty, int tz, const int32_t* now,
+                                                       const int32_t* before, const int32_t* counts) {
+  const int n_now = counts[1], n_before = counts[2];
+  const int per_block = 256 / kTileCells;
+  for (int w = blockIdx.x * per_block + threadIdx.x / kTileCells; w < n_now + n_before; w += gridDim.x * per_block) {
+    const int tile = w < n_now ? now[w] : before[w - n_now];
+    int64_t g;
+    if (!tile_node(S, tile, threadIdx.x % kTileCells, ty, tz, g)) continue;
+    S.grid_mass[g] = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      S.grid_velocity[3 * g + a] = 0.0f;
+      S.grid_force[3 * g + a] = 0.0f;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // P2G (neo_hookean_mpm.py:712-801): one CTA per tile (+ one for the
 // out-of-stencil bucket, which only clamps F and reports).
@@ -313,7 +367,6 @@ __device__ __forceinline__ void block_max(double* acc, int slot, double v) {
 // ---------------------------------------------------------------------------
 constexpr int kP2gThreads = 256;
 constexpr int kP2gChunk = 256;  // particles per chunk (one per thread)
-constexpr int kTileCells = kTile * kTile * kTile;
 
 struct P2gRecords {
   float w[9][kP2gChunk];   // w[3 a + o]: quadratic weight of offset o on axis a
@@ -326,15 +379,20 @@ struct P2gRecords {
 
 __global__ void __launch_bounds__(kP2gThreads) k_p2g(efsi_mpm_state S, int tx, int ty, int tz, int ntiles,
                                                      const int32_t* __restrict__ sorted,
-                                                     const int32_t* __restrict__ offset, float dt, float mu,
+                                                     const int32_t* __restrict__ offset,
+                                                     const int32_t* __restrict__ active,
+                                                     const int32_t* __restrict__ counts, float dt, float mu,
                                                      float lam, double* acc) {
   __shared__ float sacc[7][kHaloN];
   __shared__ P2gRecords rec;
   __shared__ int cell_count[kTileCells];
   __shared__ int cell_start[kTileCells + 1];
-  const int tile = blockIdx.x;
+  double rm = 0, rv = 0, rp0 = 0, rp1 = 0, rp2 = 0, rf0 = 0, rf1 = 0, rf2 = 0, rmom2 = 0, rmaxj = 0, roob = 0,
+         rclamp = 0;
+  const int n_active = counts[0];
+  for (int a_idx = blockIdx.x; a_idx < n_active; a_idx += gridDim.x) {
+  const int tile = active[a_idx];
   const int beg = offset[tile], end = offset[tile + 1];
-  if (beg == end) return;  // uniform per block
   const bool in_stencil_bucket = tile < ntiles;
   int t0 = 0, t1 = 0, t2 = 0;
   if (in_stencil_bucket) {
@@ -347,8 +405,6 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(efsi_mpm_state S, int tx, i
   const float inv4[3] = {(float)(4.0 / ((double)S.dx[0] * S.dx[0])), (float)(4.0 / ((double)S.dx[1] * S.dx[1])),
                          (float)(4.0 / ((double)S.dx[2] * S.dx[2]))};
   const float dxs[3] = {S.dx[0], S.dx[1], S.dx[2]};
-  double rm = 0, rv = 0, rp0 = 0, rp1 = 0, rp2 = 0, rf0 = 0, rf1 = 0, rf2 = 0, rmom2 = 0, rmaxj = 0, roob = 0,
-         rclamp = 0;
   for (int c0 = beg; c0 < end; c0 += kP2gChunk) {
     for (int q = threadIdx.x; q < kTileCells; q += blockDim.x) cell_count[q] = 0;
     __syncthreads();
@@ -510,6 +566,8 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(efsi_mpm_state S, int tx, i
       }
     }
   }
+  __syncthreads();  // the node block is zeroed again for the next tile
+  }
   if (acc != nullptr) {
     block_add(acc, R_MASS, rm);
     block_add(acc, R_VOL, rv);
@@ -527,11 +585,16 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(efsi_mpm_state S, int tx, i
 }
 
 // Grid update (neo_hookean_mpm.py:803-817).
-__global__ void __launch_bounds__(256) k_grid_update(efsi_mpm_state S, float dt, float damping, double* acc) {
-  const int64_t G = (int64_t)S.nx * S.ny * S.nz;
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// Only the nodes of the reached tiles can carry mass; the rest of the grid is
+// zero (k_clear_reached).
+__global__ void __launch_bounds__(256) k_grid_update(efsi_mpm_state S, int ty, int tz, const int32_t* reached,
+                                                     const int32_t* counts, float dt, float damping, double* acc) {
   double t0 = 0, t1 = 0, t2 = 0, m0 = 0, m1 = 0, m2 = 0, act = 0, spd = 0;
-  if (g < G) {
+  const int n_reached = counts[1];
+  const int per_block = 256 / kTileCells;
+  for (int w = blockIdx.x * per_block + threadIdx.x / kTileCells; w < n_reached; w += gridDim.x * per_block) {
+    int64_t g;
+    if (!tile_node(S, reached[w], threadIdx.x % kTileCells, ty, tz, g)) continue;
     const float m = S.grid_mass[g];
     if (m > 1.0e-20f) {
       float v[3], tv[3];
@@ -543,14 +606,14 @@ __global__ void __launch_bounds__(256) k_grid_update(efsi_mpm_state S, float dt,
         v[a] *= damping;
         S.grid_velocity[3 * g + a] = v[a];
       }
-      t0 = m * tv[0];
-      t1 = m * tv[1];
-      t2 = m * tv[2];
-      m0 = m * v[0];
-      m1 = m * v[1];
-      m2 = m * v[2];
-      act = 1.0;
-      spd = (double)sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      t0 += m * tv[0];
+      t1 += m * tv[1];
+      t2 += m * tv[2];
+      m0 += m * v[0];
+      m1 += m * v[1];
+      m2 += m * v[2];
+      act += 1.0;
+      spd = fmax(spd, (double)sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
     }
   }
   if (acc != nullptr) {
@@ -788,7 +851,13 @@ int efsi_mpm_plan_create(int32_t capacity, int32_t nx, int32_t ny, int32_t nz, e
       cudaMalloc(&P->count, nb * sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&P->offset, (nb + 1) * sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&P->cursor, nb * sizeof(int32_t)) != cudaSuccess ||
-      cudaMalloc(&P->acc, R_COUNT * sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&P->acc, R_COUNT * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&P->active, nb * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&P->reached_flag, nb) != cudaSuccess ||
+      cudaMalloc(&P->reached[0], nb * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&P->reached[1], nb * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&P->counts, 4 * sizeof(int32_t)) != cudaSuccess ||
+      cudaMemset(P->counts, 0, 4 * sizeof(int32_t)) != cudaSuccess) {
     efsi_mpm_plan_destroy(P);
     set_error("cudaMalloc failed for the MPM plan");
     return EFSI_ERR_CUDA;
@@ -805,6 +874,11 @@ int efsi_mpm_plan_destroy(efsi_mpm_plan* P) {
   cudaFree(P->offset);
   cudaFree(P->cursor);
   cudaFree(P->acc);
+  cudaFree(P->active);
+  cudaFree(P->reached_flag);
+  cudaFree(P->reached[0]);
+  cudaFree(P->reached[1]);
+  cudaFree(P->counts);
   delete P;
   return EFSI_OK;
 }
@@ -821,25 +895,43 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
   const int Pn = S.particle_count;
   double* acc = report_device != nullptr ? P->acc : nullptr;
   // algorithmic bytes of the substep: 216 per particle (read x, v, C, F, mass,
-  // volume, f_ext, fixed; write x, v, C, F) and 28 per node cleared
+  // volume, f_ext, fixed; write x, v, C, F) and 68 per node of the reached
+  // tiles (clear 28, update 40)
   const bool time_step = timing_enabled(KF_MPM_STEP);
   if (time_step) timing_begin(KF_MPM_STEP, s);
-  EFSI_CUDA_CHECK(cudaMemsetAsync(S.grid_mass, 0, G * sizeof(float), s));
-  EFSI_CUDA_CHECK(cudaMemsetAsync(S.grid_velocity, 0, 3 * G * sizeof(float), s));
-  EFSI_CUDA_CHECK(cudaMemsetAsync(S.grid_force, 0, 3 * G * sizeof(float), s));
+  // the previous step's reached list becomes "before"; this step's is rebuilt
+  int32_t* before = P->reached[P->cur];
+  P->cur ^= 1;
+  int32_t* now = P->reached[P->cur];
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(P->counts + 2, P->counts + 1, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+  EFSI_CUDA_CHECK(cudaMemsetAsync(P->counts, 0, 2 * sizeof(int32_t), s));
   EFSI_CUDA_CHECK(cudaMemsetAsync(P->count, 0, (P->ntiles + 1) * sizeof(int32_t), s));
+  EFSI_CUDA_CHECK(cudaMemsetAsync(P->reached_flag, 0, P->ntiles, s));
   if (acc) EFSI_CUDA_CHECK(cudaMemsetAsync(acc, 0, R_COUNT * sizeof(double), s));
   const unsigned pb = (Pn + 255) / 256;
-  EFSI_COUNTED k_bin_keys<<<pb, 256, 0, s>>>(S, P->tx, P->ty, P->tz, P->ntiles, P->key, P->count);
+  EFSI_COUNTED k_bin_keys<<<pb, 256, 0, s>>>(S, P->tx, P->ty, P->tz, P->ntiles, P->key, P->count, P->reached_flag);
   EFSI_COUNTED k_scan<<<1, 1024, 0, s>>>(P->count, P->ntiles + 1, P->offset, P->cursor);
+  EFSI_COUNTED k_tile_lists<<<(P->ntiles + 256) / 256, 256, 0, s>>>(P->ntiles, P->count, P->reached_flag, P->active,
+                                                                     now, P->counts);
+  EFSI_COUNTED k_clear_reached<<<2 * 148, 256, 0, s>>>(S, P->ty, P->tz, now, before, P->counts);
   EFSI_COUNTED k_bin_scatter<<<pb, 256, 0, s>>>(Pn, P->key, P->offset, P->cursor, P->sorted);
+  // P2G: 124 bytes per particle (read x, v, C, F, mass, volume, f_ext, fixed, sorted index)
   EFSI_TIMED(KF_P2G, 124.0 * Pn, s,
-             EFSI_COUNTED k_p2g<<<P->ntiles + 1, kP2gThreads, 0, s>>>(S, P->tx, P->ty, P->tz, P->ntiles, P->sorted, P->offset, dt,
-                                                             mu, lambda_, acc));
-  // grid update: the mass of every node is read; active nodes add 36 bytes
-  // that are not counted here (a lower bound)
-  EFSI_TIMED(KF_GRID_UPDATE, 4.0 * (double)G, s,
-             EFSI_COUNTED k_grid_update<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(S, dt, velocity_damping, acc));
+             EFSI_COUNTED k_p2g<<<4 * 148, kP2gThreads, 0, s>>>(S, P->tx, P->ty, P->tz, P->ntiles, P->sorted, P->offset,
+                                                                P->active, P->counts, dt, mu, lambda_, acc));
+  // grid update: 40 bytes per node of the reached tiles (read mass, momentum
+  // and force, write velocity); the count is read back only while the
+  // family is timed
+  double reached_nodes = 0.0;
+  if (timing_enabled(KF_GRID_UPDATE) || time_step) {
+    int32_t h = 0;
+    EFSI_CUDA_CHECK(cudaMemcpyAsync(&h, P->counts + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+    reached_nodes = (double)h * kTileCells;
+  }
+  EFSI_TIMED(KF_GRID_UPDATE, 40.0 * reached_nodes, s,
+             EFSI_COUNTED k_grid_update<<<2 * 148, 256, 0, s>>>(S, P->ty, P->tz, now, P->counts, dt, velocity_damping,
+                                                                acc));
   // G2P: read x, F, fixed, region (56 bytes), write x, v, C, F (96 bytes)
   EFSI_TIMED(KF_G2P, 152.0 * Pn, s,
              EFSI_COUNTED k_g2p<<<pb, 256, 0, s>>>(S, P->sorted, dt, primary_region, secondary_region, acc));
@@ -847,7 +939,7 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
     EFSI_COUNTED k_radial<<<pb, 256, 0, s>>>(S, acc);
     EFSI_COUNTED k_mpm_finalize<<<1, 32, 0, s>>>(acc, dt, report_device);
   }
-  if (time_step) timing_end(KF_MPM_STEP, s, 216.0 * Pn + 28.0 * (double)G);
+  if (time_step) timing_end(KF_MPM_STEP, s, 216.0 * Pn + 68.0 * reached_nodes);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }

@@ -56,8 +56,10 @@ __all__ = [
 # "fv_multigrid_mixed" (no reference counterpart): the fv_multigrid V-cycle
 # with FP32 storage and arithmetic on level 0, inside the same FP64 flexible CG
 # (true residual, inner products and scalars in FP64).
-CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light", "fv_multigrid_mixed", "learned")
-_PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2, "fv_multigrid_mixed": 3, "learned": 4}
+CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light", "fv_multigrid_mixed", "learned",
+                             "learned_no_fallback")
+_PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2, "fv_multigrid_mixed": 3, "learned": 4,
+                 "learned_no_fallback": 5}
 _BREAKDOWN_TEXT = {
     0: "",
     1: "initial residual/preconditioner dot is not positive finite",
@@ -916,6 +918,7 @@ class CartesianFluidSolver:
         self.last_cg_used_multigrid = bool(stats.used_mg)
         self.last_cg_used_graphs = bool(stats.used_graphs)
         self.last_cg_learned_iterations = int(stats.learned_iterations)
+        self.last_cg_learned_relative_residual = float(stats.learned_relative_residual)
         if use_graphs and not stats.used_graphs:
             self.last_cg_graph_error = _native.load().efsi_fv_graph_error(self._plan).decode(errors="replace")
         self._last_cg_breakdown_code = int(stats.breakdown_code)

@@ -159,7 +159,8 @@ typedef struct efsi_pcg_params {
                            3 fv_multigrid_mixed: the 2/24/2 V-cycle with FP32 level-0 iterates and
                            arithmetic (no reference counterpart; the CG stays FP64),
                            4 learned: the network attached by efsi_fv_set_learned_preconditioner,
-                           falling back to the 2/24/2 V-cycle (no reference counterpart) */
+                           falling back to the 2/24/2 V-cycle (no reference counterpart),
+                           5 the same network without the fallback (measurement of the network alone) */
   int32_t remove_mean;  /* closed-domain zero-mean projection */
   int32_t outlet;       /* pressure_outlet_zmin */
   int32_t iface_active; /* interface terms present: MG disabled, restart every 256 */
@@ -183,6 +184,7 @@ typedef struct efsi_cg_stats {
   double relative_residual;
   double breakdown_dAd;
   double b_norm;
+  double learned_relative_residual; /* relative residual at the last check preconditioned by the learned network */
 } efsi_cg_stats;
 
 /* fluid.py:6535-6811 _solve_pressure_poisson_fv_cg: flexible MG/Jacobi PCG on

@@ -62,8 +62,9 @@ def test_weight_gradient_matches_numpy():
     x = ou.bf16(rng.normal(size=shape + (cin,)))
     g = ou.bf16(rng.normal(size=shape + (cout,)))
     dw = torch.zeros((cout, 27, cin), dtype=torch.float32, device="cuda")
-    _native.call("efsi_conv3d_wgrad", *shape, cin, cout, _bf16_tensor(x).data_ptr(), _bf16_tensor(g).data_ptr(),
-                 dw.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    xt, gt = _bf16_tensor(x), _bf16_tensor(g)  # kept alive until the kernel has run
+    _native.call("efsi_conv3d_wgrad", *shape, cin, cout, xt.data_ptr(), gt.data_ptr(), dw.data_ptr(),
+                 torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert _rel(dw.cpu().numpy(), ou.conv_weight_grad(x, g)) <= 1e-5
 
@@ -143,9 +144,11 @@ def _solve(fl, div, precond, iterations=2000):
 
 def test_learned_preconditioner_trains_and_reduces_iterations():
     """Pairs harvested from the solver's own MG-PCG, training on crops, then a
-    new right-hand side: the trained network inside the flexible PCG reaches
-    the same relative residual 1e-8 in fewer iterations than the PCG without
-    it (Jacobi) and than the same network untrained; the training loss falls."""
+    new right-hand side.  The network alone (no fallback) inside the flexible
+    PCG, after a fixed budget of 64 iterations, leaves a smaller residual than
+    the same PCG without it (Jacobi) and than the same network untrained; with
+    the V-cycle fallback the learned solve reaches the relative residual 1e-8
+    in fewer iterations than Jacobi-PCG.  The training loss falls."""
     from easyfsi_b200.learned import UNetPreconditioner, harvest_pairs
 
     nodes = (32, 32, 40)
@@ -164,14 +167,19 @@ def test_learned_preconditioner_trains_and_reduces_iterations():
     assert last < 0.7 * first
 
     div = rng.normal(size=nodes).astype(np.float32)
-    res = {"jacobi": _solve(fl, div, "jacobi"), "fv_multigrid": _solve(fl, div, "fv_multigrid")}
-    res["learned"] = _solve(fl, div, "learned")
+    budget = {"jacobi": _solve(fl, div, "jacobi", iterations=64),
+              "trained": _solve(fl, div, "learned_no_fallback", iterations=64)}
     fl.set_learned_preconditioner(untrained)
-    res["untrained"] = _solve(fl, div, "learned")
+    budget["untrained"] = _solve(fl, div, "learned_no_fallback", iterations=64)
     fl.set_learned_preconditioner(net)
-    print("solves:", res)
-    for name, r in res.items():
+    print("residual after 64 iterations:", {k: v["residual"] for k, v in budget.items()})
+    assert budget["trained"]["residual"] < budget["jacobi"]["residual"]
+    assert budget["trained"]["residual"] < budget["untrained"]["residual"]
+
+    full = {"jacobi": _solve(fl, div, "jacobi"), "fv_multigrid": _solve(fl, div, "fv_multigrid"),
+            "learned": _solve(fl, div, "learned")}
+    print("solves to 1e-8:", full)
+    for name, r in full.items():
         assert r["converged"] and r["residual"] <= 1e-8, name
-    assert res["learned"]["iterations"] < res["jacobi"]["iterations"]
-    assert res["learned"]["iterations"] <= res["untrained"]["iterations"]
-    assert res["learned"]["learned_iterations"] > 0
+    assert full["learned"]["iterations"] < full["jacobi"]["iterations"]
+    assert full["learned"]["learned_iterations"] > 0

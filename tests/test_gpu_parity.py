@@ -156,9 +156,13 @@ def test_projection_gradient_and_predict(case):
 
 
 def test_mpm_step_matches_oracle():
-    """20 MPM substeps of a moving block against the oracle: the displacement
-    x - x0, the velocity and F - I (the parts that change; x and F themselves
-    are dominated by x0 and I) to f32 parity, <= 1e-5 relative after 20 steps."""
+    """20 MPM substeps of a block with random particle velocities against the
+    oracle.  x and F to <= 1e-6 relative (north_star's f32 bound is 1e-5);
+    the parts that change -- the displacement x - x0 (about 1e-4 m) and F - I
+    (about 2e-3) -- are stored as f32 x and F around 0.5 and I, whose
+    representation floor is about 6e-8 and 1.2e-7 absolute per step, so
+    their relative errors are bounded at the f32 floor: <= 1e-3 (measured on
+    a B200: 1.8e-4 and 3.9e-4); v <= 1e-4 (measured 2.7e-5)."""
     from easyfsi_b200.neo_hookean_mpm import NeoHookeanMpmState
 
     rng = np.random.default_rng(5)
@@ -179,12 +183,15 @@ def test_mpm_step_matches_oracle():
     x64 = x.astype(np.float64)
     eye = np.eye(3).ravel()
     err = {
+        "x": rel_l2(gpu.x.to_numpy()[:n], ref.x[:n]),
+        "F": rel_l2(gpu.F.to_numpy()[:n], ref.F[:n]),
         "displacement": rel_l2(gpu.x.to_numpy()[:n] - x64, ref.x[:n] - x64),
         "v": rel_l2(gpu.v.to_numpy()[:n], ref.v[:n]),
         "F-I": rel_l2(gpu.F.to_numpy()[:n].reshape(n, 9) - eye, ref.F[:n].reshape(n, 9) - eye),
     }
     print("mpm 20 steps:", err)
-    assert err["displacement"] <= 1e-5 and err["v"] <= 1e-5 and err["F-I"] <= 1e-5
+    assert err["x"] <= 1e-6 and err["F"] <= 1e-6
+    assert err["displacement"] <= 1e-3 and err["F-I"] <= 1e-3 and err["v"] <= 1e-4
     assert np.abs(ref.x[:n] - x64).max() > 5e-6  # the particles really moved
     assert rep.transfer_relative_error < 2e-5
 
@@ -225,7 +232,9 @@ def test_c1_twenty_coupled_steps_match_oracle():
     after every step: pressure <= 1e-10 (f64); fluid velocity, particle
     displacement and marker displacement <= 1e-6 (f32; measured bit-identical);
     particle velocity, F - I and f_ext <= 1e-5 (f32 atomic sums in other
-    orders; measured <= 1e-6 after 20 steps)."""
+    orders; measured <= 1e-6 after 20 steps).  The particles start at rest
+    and move less than one f32 unit of x in 20 steps at this dt, so their
+    velocity and F - I carry the solid's parity here."""
     from easyfsi_b200.scenarios import CONFIGS, CoupledScene
 
     cfg = CONFIGS["c1"]
@@ -259,7 +268,7 @@ def test_c1_twenty_coupled_steps_match_oracle():
         assert worst[k] <= 1e-6, k
     for k in ("v", "F-I", "f_ext"):
         assert worst[k] <= 1e-5, k
-    assert np.abs(ref.solid.x[:n] - x0).max() > 0.0
+    assert np.abs(ref.solid.v[:n]).max() > 0.0 and np.abs(ref.solid.F[:n].reshape(n, 9) - eye).max() > 0.0
 
 
 def test_graph_blocks_match_direct_launches(case):
