@@ -225,6 +225,8 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_unet_zero_grad": [P, P],
     "efsi_unet_adam_step": [P, F, F, F, F, P],
     "efsi_fv_set_learned_preconditioner": [P, P, P],
+    "efsi_fv_set_interface_coupling": [P, I, P, P, P, P, P],
+    "efsi_fv_copy_rhs": [P, P, P],
     "efsi_fv_learned_input": [P, P, P, P],
     "efsi_reach_plan_create": [POINTER(c_void_p)],
     "efsi_reach_plan_destroy": [P],

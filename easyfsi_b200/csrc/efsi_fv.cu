@@ -1111,6 +1111,68 @@ __global__ void __launch_bounds__(256) k_jacobi_precond(LevelDev L, const double
   }
 }
 
+// fluid.py:4345-4456: the interface-coupling terms of the level-0 operator,
+// held as rows of (source cell, coefficient = T / V_receiver) entries per
+// receiving cell in the order the reference's coupling list visits them:
+// out[c] += -(coef * p[src]) entry by entry (with `residual`, the terms are
+// subtracted from a residual b - A p instead).  Rows are distinct cells, so
+// the result does not depend on thread order.  The row count is read from the
+// device, which keeps captured graphs valid when the couplings change.
+__global__ void __launch_bounds__(256) k_couple(const int32_t* __restrict__ rows, const int32_t* __restrict__ ptr,
+                                                const int32_t* __restrict__ src, const double* __restrict__ coef,
+                                                const int32_t* __restrict__ nrows, const double* __restrict__ p,
+                                                double* __restrict__ out, int residual) {
+  pdl_wait();
+  const int n = *nrows;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int c = rows[r];
+    double acc = out[c];
+    for (int e = ptr[r]; e < ptr[r + 1]; ++e) {
+      const double term = -(coef[e] * __ldg(p + src[e]));
+      acc = residual ? acc - term : acc + term;
+    }
+    out[c] = acc;
+  }
+}
+
+// <d, Ad>_V after the coupling terms, and alpha (fluid.py:4567-4574).
+__global__ void __launch_bounds__(256) k_dot_alpha(LevelDev L, const double* __restrict__ d,
+                                                   const double* __restrict__ Ad, double* partials, CgScalars* sc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  double a = 0.0;
+  if (active && (__ldg(L.mask + c) & M_FLUID)) a = __ldg(d + c) * __ldg(Ad + c) * vol64(L, i, j, k);
+  double v[1] = {a}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) cg_alpha_step(sc, t[0]);
+  }
+}
+
+// The residual's V-weighted mean (mean) or <r, r>_V, after the couplings.
+__global__ void __launch_bounds__(256) k_residual_reduce(LevelDev L, const double* __restrict__ r, int mean,
+                                                         double* partials, CgScalars* sc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  double a = 0.0;
+  if (active && (__ldg(L.mask + c) & M_FLUID)) {
+    const double rv = __ldg(r + c), V = vol64(L, i, j, k);
+    a = mean ? rv * V : rv * rv * V;
+  }
+  double v[1] = {a}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) {
+      if (mean)
+        sc->mean_r = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
+      else
+        sc->rr = t[0];
+    }
+  }
+}
+
+__global__ void k_set_defer(CgScalars* sc, int v) {
+  if (threadIdx.x == 0) sc->defer_alpha = v;
+}
+
 // Learned preconditioner (code 4).  k_learned_sumsq reduces sum_fluid r^2 V
 // into sc->dot; k_learned_pack forms the network input (r over its
 // volume-weighted RMS, fluid mask, log2 cell widths over the finest width);
@@ -1688,7 +1750,8 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
   P->partials_len = 4 * max_blocks;
   if (cudaMalloc(&P->partials, P->partials_len * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&P->sc, sizeof(CgScalars)) != cudaSuccess || cudaMalloc(&P->aux, 16 * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&P->host_sc, sizeof(CgScalars)) != cudaSuccess) {
+      cudaMallocHost(&P->host_sc, sizeof(CgScalars)) != cudaSuccess ||
+      cudaMemset(P->sc, 0, sizeof(CgScalars)) != cudaSuccess) {
     set_error("cudaMalloc failed for reduction scratch");
     return fail(EFSI_ERR_CUDA);
   }
@@ -1733,6 +1796,11 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   cudaFree(P->aux);
   cudaFree(P->bicg_work);
   cudaFree(P->unet_in);
+  cudaFree(P->cpl_rows);
+  cudaFree(P->cpl_ptr);
+  cudaFree(P->cpl_src);
+  cudaFree(P->cpl_coef);
+  cudaFree(P->cpl_n);
   if (P->host_sc) cudaFreeHost(P->host_sc);
   delete P;
   return EFSI_OK;
@@ -1794,6 +1862,9 @@ int efsi_fv_apply(efsi_fv_plan* P, const double* p, double* out, int32_t outlet,
   LevelDev L = level_dev(P, 0);
   const Shape3& S = P->lv[0].shape;
   EFSI_COUNTED k_fv_apply<<<S.grid, S.block, 0, as_stream(stream)>>>(L, p, out, outlet);
+  if (P->cpl_nrows > 0)
+    EFSI_COUNTED k_couple<<<148, 256, 0, as_stream(stream)>>>(P->cpl_rows, P->cpl_ptr, P->cpl_src, P->cpl_coef, P->cpl_n,
+                                                            p, out, 0);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
@@ -2389,6 +2460,8 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   const int outlet = prm->outlet;
   const bool remove_mean = prm->remove_mean != 0;
   EFSI_COUNTED k_reset_scalars<<<1, 32, 0, s>>>(P->sc);
+  const bool coupled = P->cpl_nrows > 0;
+  if (coupled) EFSI_COUNTED k_set_defer<<<1, 32, 0, s>>>(P->sc, 1);
   // fluid.py:6581 diagonal (Jacobi path and fallback).
   EFSI_COUNTED k_fv_diag<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->diag, outlet);
   // b = -rhs - V-mean(-rhs)  (fluid.py:6589-6601); the free volume is reduced
@@ -2412,6 +2485,12 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   auto true_residual = [&]() -> int {
     EFSI_COUNTED k_true_residual<<<R.S.grid, R.S.block, 0, s>>>(R.L, pressure, P->b, P->r, outlet, remove_mean ? 1 : 0,
                                                    P->partials, P->sc);
+    if (coupled) {
+      // r -= C p, then the mean or <r, r>_V of the corrected residual
+      EFSI_COUNTED k_couple<<<148, 256, 0, s>>>(P->cpl_rows, P->cpl_ptr, P->cpl_src, P->cpl_coef, P->cpl_n, pressure,
+                                              P->r, 1);
+      EFSI_COUNTED k_residual_reduce<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, remove_mean ? 1 : 0, P->partials, P->sc);
+    }
     if (remove_mean) {
       EFSI_COUNTED k_sub_mean_r<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, P->partials, P->sc);
       st->mean_projection_count += 1;
@@ -2489,7 +2568,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   const unsigned tg0 = P->lv[0].tgrid;
   const dim3 tblk(kTK, kTJ);
   const bool march0 = P->lv[0].march;
-  auto launch_spmv = [&](bool copy, double* d_old, double* d_new) {
+  auto launch_spmv_operator = [&](bool copy, double* d_old, double* d_new) {
     if (march0) {
       bool done = false;
       EFSI_TIMED(KF_SPMV_DIR, (copy ? 25.0 : 33.0) * n0d, s,
@@ -2515,6 +2594,17 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       EFSI_TIMED(KF_SPMV_DIR, 33.0 * n0d, s,
                  EFSI_COUNTED launch_pdl(k_spmv_dir<false>, R.S.grid, R.S.block, 0, s, R.L, P->z, d_old, d_new, P->Ad, outlet,
                                                                                P->partials, P->sc));
+  };
+  auto launch_spmv = [&](bool copy, double* d_old, double* d_new) {
+    launch_spmv_operator(copy, d_old, d_new);
+    if (coupled) {
+      // Ad += C d, then <d, Ad>_V and alpha (the SpMV's finisher deferred them)
+      EFSI_COUNTED launch_pdl(k_couple, 148, 256, 0, s, (const int32_t*)P->cpl_rows, (const int32_t*)P->cpl_ptr,
+                              (const int32_t*)P->cpl_src, (const double*)P->cpl_coef, (const int32_t*)P->cpl_n,
+                              (const double*)d_new, P->Ad, 0);
+      EFSI_COUNTED launch_pdl(k_dot_alpha, R.S.grid, R.S.block, 0, s, R.L, (const double*)d_new, (const double*)P->Ad,
+                              P->partials, P->sc);
+    }
   };
   auto launch_update = [&](double* d, bool mean_now, bool want_rr) {
     if (tiled0) {
@@ -2587,6 +2677,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     if (!prm->use_graphs || P->graphs_disabled) return launch_block(cont);
     PcgGraphKey key{cont, R.use_mg, remove_mean, outlet, R.pre, R.coarse, R.post, pressure, R.mixed};
     key.learned = R.learned;
+    key.coupled = coupled;
     cudaGraphExec_t exec = nullptr;
     for (auto& g : P->graphs)
       if (g.key == key) exec = g.exec;
@@ -3059,6 +3150,76 @@ int efsi_fv_set_learned_preconditioner(efsi_fv_plan* P, efsi_unet* net, void* st
   // graphs captured with another network's buffers are not reused
   for (PcgGraph& g : P->graphs) cudaGraphExecDestroy(g.exec);
   P->graphs.clear();
+  return EFSI_OK;
+}
+
+int efsi_fv_set_interface_coupling(efsi_fv_plan* P, int32_t nrows, const int32_t* rows, const int32_t* row_ptr,
+                                   const int32_t* src, const double* coef, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(nrows >= 0, "nrows must be non-negative");
+  cudaStream_t s = as_stream(stream);
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (P->cpl_n == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&P->cpl_n, sizeof(int32_t)));
+  if (nrows == 0) {
+    const int32_t zero = 0;
+    EFSI_CUDA_CHECK(cudaMemcpy(P->cpl_n, &zero, sizeof(int32_t), cudaMemcpyHostToDevice));
+    P->cpl_nrows = 0;
+    return EFSI_OK;
+  }
+  EFSI_ARG_CHECK(rows != nullptr && row_ptr != nullptr && src != nullptr && coef != nullptr, "null coupling array");
+  // the rows are validated on the host before they reach a kernel
+  std::vector<int32_t> h_rows((size_t)nrows), h_ptr((size_t)nrows + 1);
+  EFSI_CUDA_CHECK(cudaMemcpy(h_rows.data(), rows, nrows * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  EFSI_CUDA_CHECK(cudaMemcpy(h_ptr.data(), row_ptr, (nrows + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  const int64_t n0 = P->lv[0].n;
+  EFSI_ARG_CHECK(h_ptr[0] == 0, "row_ptr must start at 0");
+  for (int32_t r = 0; r < nrows; ++r) {
+    EFSI_ARG_CHECK(h_rows[r] >= 0 && h_rows[r] < n0, "coupling row cell out of range");
+    EFSI_ARG_CHECK(h_ptr[r + 1] >= h_ptr[r], "row_ptr must not decrease");
+    if (r > 0) EFSI_ARG_CHECK(h_rows[r] > h_rows[r - 1], "coupling rows must be distinct, in increasing order");
+  }
+  const int32_t nent = h_ptr[nrows];
+  std::vector<int32_t> h_src((size_t)std::max(nent, 1));
+  std::vector<double> h_coef((size_t)std::max(nent, 1));
+  if (nent > 0) {
+    EFSI_CUDA_CHECK(cudaMemcpy(h_src.data(), src, nent * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    EFSI_CUDA_CHECK(cudaMemcpy(h_coef.data(), coef, nent * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  for (int32_t e = 0; e < nent; ++e) EFSI_ARG_CHECK(h_src[e] >= 0 && h_src[e] < n0, "coupling source cell out of range");
+  if (P->cpl_cap_rows < nrows || P->cpl_cap_ent < nent) {
+    // new buffers: graphs that captured the old pointers are dropped
+    for (PcgGraph& g : P->graphs) cudaGraphExecDestroy(g.exec);
+    P->graphs.clear();
+    cudaFree(P->cpl_rows);
+    cudaFree(P->cpl_ptr);
+    cudaFree(P->cpl_src);
+    cudaFree(P->cpl_coef);
+    P->cpl_rows = P->cpl_ptr = P->cpl_src = nullptr;
+    P->cpl_coef = nullptr;
+    P->cpl_cap_rows = P->cpl_cap_ent = 0;
+    const int64_t cr = std::max<int64_t>(nrows, 2 * P->cpl_cap_rows), ce = std::max<int64_t>(std::max(nent, 1), 1);
+    EFSI_CUDA_CHECK(cudaMalloc(&P->cpl_rows, cr * sizeof(int32_t)));
+    EFSI_CUDA_CHECK(cudaMalloc(&P->cpl_ptr, (cr + 1) * sizeof(int32_t)));
+    EFSI_CUDA_CHECK(cudaMalloc(&P->cpl_src, ce * sizeof(int32_t)));
+    EFSI_CUDA_CHECK(cudaMalloc(&P->cpl_coef, ce * sizeof(double)));
+    P->cpl_cap_rows = cr;
+    P->cpl_cap_ent = ce;
+  }
+  EFSI_CUDA_CHECK(cudaMemcpy(P->cpl_rows, h_rows.data(), nrows * sizeof(int32_t), cudaMemcpyHostToDevice));
+  EFSI_CUDA_CHECK(cudaMemcpy(P->cpl_ptr, h_ptr.data(), (nrows + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (nent > 0) {
+    EFSI_CUDA_CHECK(cudaMemcpy(P->cpl_src, h_src.data(), nent * sizeof(int32_t), cudaMemcpyHostToDevice));
+    EFSI_CUDA_CHECK(cudaMemcpy(P->cpl_coef, h_coef.data(), nent * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  EFSI_CUDA_CHECK(cudaMemcpy(P->cpl_n, &nrows, sizeof(int32_t), cudaMemcpyHostToDevice));
+  P->cpl_nrows = nrows;
+  return EFSI_OK;
+}
+
+int efsi_fv_copy_rhs(efsi_fv_plan* P, double* out, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(out != nullptr, "null output");
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(out, P->b, P->lv[0].n * sizeof(double), cudaMemcpyDeviceToDevice, as_stream(stream)));
   return EFSI_OK;
 }
 

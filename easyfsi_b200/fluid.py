@@ -56,6 +56,7 @@ __all__ = [
 # "fv_multigrid_mixed" (no reference counterpart): the fv_multigrid V-cycle
 # with FP32 storage and arithmetic on level 0, inside the same FP64 flexible CG
 # (true residual, inner products and scalars in FP64).
+PRESSURE_INTERFACE_COUPLING_SLOT_COUNT = 16  # pressure_interface.py:10: one slot plus 15 extra per owner cell
 CG_PRECONDITIONER_CHOICES = ("auto", "jacobi", "fv_multigrid", "fv_multigrid_light", "fv_multigrid_mixed", "learned",
                              "learned_no_fallback")
 _PRECOND_CODE = {"jacobi": 0, "fv_multigrid": 1, "fv_multigrid_light": 2, "fv_multigrid_mixed": 3, "learned": 4,
@@ -156,6 +157,14 @@ class CartesianFluidSolver:
         self.volume_source_s = scalar(f32)
         self.pressure_interface_matrix_diagonal = scalar(f64)
         self.pressure_interface_matrix_rhs = scalar(f64)
+        # interface couplings (fluid.py:772-811): per-cell slots and an
+        # explicit row list; the 15 extra slots per cell and the row arrays
+        # (capacity nx * ny * nz) are created on first access
+        self.pressure_interface_coupling_active = scalar(i32)
+        self.pressure_interface_coupling_neighbor = vector(i32)
+        self.pressure_interface_coupling_coefficient = scalar(f64)
+        self.pressure_interface_row_capacity = int(np.prod(shape))
+        self.pressure_interface_row_count = Field((), i32, device=dev)
         self.obstacle = scalar(i32)
         self.force = vector(f32)
         self.velocity_dirichlet_boundary_active = scalar(i32)
@@ -307,14 +316,108 @@ class CartesianFluidSolver:
             * self.cell_width_z_m.tensor[None, None, :]
         )
 
+    _LAZY_COUPLING_FIELDS = ("pressure_interface_coupling_extra_neighbor",
+                             "pressure_interface_coupling_extra_coefficient", "pressure_interface_row_owner",
+                             "pressure_interface_row_neighbor", "pressure_interface_row_transmissibility")
+
+    def __getattr__(self, name):
+        # the large coupling arrays of the reference (fluid.py:783-811) exist
+        # from their first access on
+        if name in CartesianFluidSolver._LAZY_COUPLING_FIELDS:
+            dev = self.__dict__["device"]
+            shape = tuple(self.grid.grid_nodes)
+            cap = self.pressure_interface_row_capacity
+            extra = shape + (PRESSURE_INTERFACE_COUPLING_SLOT_COUNT - 1,)
+            made = {
+                "pressure_interface_coupling_extra_neighbor": lambda: Field(extra, i32, n=3, device=dev),
+                "pressure_interface_coupling_extra_coefficient": lambda: Field(extra, f64, device=dev),
+                "pressure_interface_row_owner": lambda: Field((cap,), i32, n=3, device=dev),
+                "pressure_interface_row_neighbor": lambda: Field((cap,), i32, n=3, device=dev),
+                "pressure_interface_row_transmissibility": lambda: Field((cap,), f64, device=dev),
+            }[name]()
+            self.__dict__[name] = made
+            return made
+        raise AttributeError(f"{type(self).__name__!s} has no attribute {name!r}")
+
     def _structure_key(self):
-        fields = (
+        fields = [
             self.obstacle,
             self.velocity_dirichlet_boundary_active,
             self.velocity_dirichlet_boundary_projection_weight,
             self.pressure_interface_matrix_diagonal,
-        )
+            self.pressure_interface_coupling_active,
+            self.pressure_interface_coupling_neighbor,
+            self.pressure_interface_coupling_coefficient,
+            self.pressure_interface_row_count,
+        ]
+        fields += [self.__dict__[n] for n in CartesianFluidSolver._LAZY_COUPLING_FIELDS if n in self.__dict__]
+        fields += [self.cell_width_x_m, self.cell_width_y_m, self.cell_width_z_m]
         return tuple((f.tensor.data_ptr(), f.tensor._version) for f in fields)
+
+    def _interface_coupling_rows(self):
+        """fluid.py:4345-4456: the couplings as (owner, neighbour, T) pairs in
+        the reference's visiting order -- the row list when its count is
+        positive, else the per-cell slots in cell order -- kept where both
+        cells are fluid and T > 0; returned as CSR rows per receiving cell
+        (entries in visiting order, coef = T / V_receiver with V the f32
+        product of the widths).  None when there are none."""
+        nx, ny, nz = self.grid.grid_nodes
+        obs = self.obstacle.tensor.reshape(-1)
+        row_count = int(self.pressure_interface_row_count[None])
+        if row_count > 0:
+            limit = min(row_count, self.pressure_interface_row_capacity)
+            own = self.pressure_interface_row_owner.tensor[:limit].to(torch.int64)
+            nbr = self.pressure_interface_row_neighbor.tensor[:limit].to(torch.int64)
+            trans = self.pressure_interface_row_transmissibility.tensor[:limit]
+            inside = ((own >= 0) & (own < torch.tensor([nx, ny, nz], device=own.device))).all(dim=1)
+            inside &= ((nbr >= 0) & (nbr < torch.tensor([nx, ny, nz], device=own.device))).all(dim=1)
+        else:
+            act = self.pressure_interface_coupling_active.tensor.reshape(-1)
+            if not bool((act > 0).any()):
+                return None
+            have_extra = "pressure_interface_coupling_extra_neighbor" in self.__dict__
+            n_slots = PRESSURE_INTERFACE_COUPLING_SLOT_COUNT if have_extra else 1
+            cells = torch.nonzero((act > 0) & (obs == 0)).reshape(-1)
+            slots = torch.clamp(act[cells], max=n_slots).to(torch.int64)
+            nb0 = self.pressure_interface_coupling_neighbor.tensor.reshape(-1, 3)[cells].to(torch.int64)
+            tr0 = self.pressure_interface_coupling_coefficient.tensor.reshape(-1)[cells]
+            if have_extra:
+                xnb = self.pressure_interface_coupling_extra_neighbor.tensor.reshape(-1, n_slots - 1, 3)[cells]
+                xtr = self.pressure_interface_coupling_extra_coefficient.tensor.reshape(-1, n_slots - 1)[cells]
+                nbr = torch.cat([nb0[:, None, :], xnb.to(torch.int64)], dim=1).reshape(-1, 3)
+                trans = torch.cat([tr0[:, None], xtr], dim=1).reshape(-1)
+            else:
+                nbr, trans = nb0, tr0
+            valid_slot = (torch.arange(n_slots, device=cells.device)[None, :] < slots[:, None]).reshape(-1)
+            own_lin = cells.repeat_interleave(n_slots)
+            own = torch.stack([own_lin // (ny * nz), (own_lin // nz) % ny, own_lin % nz], dim=1)
+            inside = valid_slot & ((nbr >= 0) & (nbr < torch.tensor([nx, ny, nz], device=nbr.device))).all(dim=1)
+        own_c = torch.where(inside[:, None], own, torch.zeros_like(own))
+        nbr_c = torch.where(inside[:, None], nbr, torch.zeros_like(nbr))
+        o_lin = (own_c[:, 0] * ny + own_c[:, 1]) * nz + own_c[:, 2]
+        n_lin = (nbr_c[:, 0] * ny + nbr_c[:, 1]) * nz + nbr_c[:, 2]
+        keep = inside & (obs[o_lin] == 0) & (obs[n_lin] == 0) & (trans > 0.0)
+        o_lin, n_lin, trans = o_lin[keep], n_lin[keep], trans[keep]
+        own_c, nbr_c = own_c[keep], nbr_c[keep]
+        if o_lin.numel() == 0:
+            return None
+        w = [getattr(self, f"cell_width_{a}_m").tensor for a in "xyz"]
+
+        def volume(ijk):
+            v = (w[0][ijk[:, 0]] * w[1][ijk[:, 1]]) * w[2][ijk[:, 2]]  # f32 product, as the reference
+            return torch.clamp(v, min=1.0e-30).to(torch.float64)
+
+        # two entries per coupling, owner's first, in visiting order
+        recv = torch.stack([o_lin, n_lin], dim=1).reshape(-1)
+        src = torch.stack([n_lin, o_lin], dim=1).reshape(-1)
+        coef = torch.stack([trans / volume(own_c), trans / volume(nbr_c)], dim=1).reshape(-1)
+        order = torch.sort(recv, stable=True).indices
+        recv, src, coef = recv[order], src[order], coef[order]
+        rows, counts = torch.unique_consecutive(recv, return_counts=True)
+        ptr = torch.zeros(rows.numel() + 1, dtype=torch.int64, device=rows.device)
+        ptr[1:] = torch.cumsum(counts, dim=0)
+        return (rows.to(torch.int32).contiguous(), ptr.to(torch.int32).contiguous(), src.to(torch.int32).contiguous(),
+                coef.to(torch.float64).contiguous())
 
     def _refresh_structure(self) -> None:
         """Rebuild every level's stencil masks from obstacle / Dirichlet rows /
@@ -340,6 +443,16 @@ class CartesianFluidSolver:
             self.pressure_interface_matrix_diagonal.ptr() if self._iface_active else None,
             _stream(),
         )
+        csr = self._interface_coupling_rows()
+        if csr is None:
+            if getattr(self, "_coupling_rows_installed", 0):
+                _native.call("efsi_fv_set_interface_coupling", self._plan, 0, None, None, None, None, _stream())
+            self._coupling_rows_installed = 0
+        else:
+            rows, ptr, src, coef = csr
+            _native.call("efsi_fv_set_interface_coupling", self._plan, int(rows.numel()), rows.data_ptr(),
+                         ptr.data_ptr(), src.data_ptr(), coef.data_ptr(), _stream())
+            self._coupling_rows_installed = int(rows.numel())
         self._structure_cache = key
 
     _BICGSTAB_BREAKDOWN_TEXT = {
@@ -922,6 +1035,15 @@ class CartesianFluidSolver:
         if use_graphs and not stats.used_graphs:
             self.last_cg_graph_error = _native.load().efsi_fv_graph_error(self._plan).decode(errors="replace")
         self._last_cg_breakdown_code = int(stats.breakdown_code)
+        if (pressure_interface_matrix_active and not stats.converged and int(stats.breakdown_reason) == 0
+                and int(self.pressure_interface_row_count[None]) > 0):
+            # fluid.py:6799-6811: with row-list couplings, an exhausted CG loop
+            # continues as BiCGSTAB on the same system from its pressure
+            _native.call("efsi_fv_copy_rhs", self._plan, self.cg_rhs.ptr(), _stream())
+            self._continue_pressure_poisson_fv_bicgstab(
+                start_iteration=max(1, int(iterations)), max_iters=max(1, int(iterations)), b_norm=float(stats.b_norm),
+                outlet=1 if pressure_outlet_zmin else 0, tolerance=max(0.0, float(tolerance)), anchor_unreached=False,
+                remove_nullspace_mean=bool(remove_nullspace_mean))
         if stats.b_norm <= 1.0e-30:
             self.pressure_tmp.tensor.zero_()
             self.pressure_accum.tensor.zero_()

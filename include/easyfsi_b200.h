@@ -544,6 +544,20 @@ int efsi_outlet_reachability(efsi_reach_plan* plan, int32_t nx, int32_t ny, int3
                              int32_t barrier_code, int32_t update_barrier, int32_t* reachable, int32_t* label,
                              efsi_reach_report* report, void* stream);
 
+/* fluid.py:4345-4456, the interface-coupling terms of _fv_laplacian_apply_kernel
+ * (row list, or per-cell slots when the row count is 0): installs them in the
+ * plan's level-0 operator (efsi_fv_apply, the PCG and the BiCGSTAB fallback).
+ * They arrive as rows: for receiving cell rows[r] (distinct, increasing
+ * linear indices), entries row_ptr[r] .. row_ptr[r + 1] of (src, coef) add
+ * -(coef * p[src]) in entry order, coef = T / V_receiver.  Device arrays,
+ * validated on the host (synchronises); nrows = 0 removes them. */
+int efsi_fv_set_interface_coupling(efsi_fv_plan* plan, int32_t nrows, const int32_t* rows, const int32_t* row_ptr,
+                                   const int32_t* src, const double* coef, void* stream);
+
+/* The positive right-hand side b of the last efsi_fv_pcg_solve (the reference's
+ * cg_rhs, fluid.py:6589-6603), copied to out (f64, level 0). */
+int efsi_fv_copy_rhs(efsi_fv_plan* plan, double* out, void* stream);
+
 /* ------------------------------------------------------------------------
  * Learned preconditioner (no counterpart in the reference: a new
  * preconditioner for the reference's flexible PCG, fluid.py:6535-6811, whose

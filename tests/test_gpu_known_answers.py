@@ -606,3 +606,88 @@ def test_fv_cg_alpha_and_flexible_beta_steps():
     s.cg_dAd[None] = -5.0
     s._cg_compute_alpha_kernel()
     assert int(s.cg_breakdown_code[None]) == 1 and float(s.cg_breakdown_dAd[None]) == -3.0
+
+
+# --------------------------------------------------------------------------
+# Interface-coupling terms of the FV operator (fluid.py:4345-4456) through the
+# drop-in solver; the oracle side passes in tests/test_oracle_known_answers.py.
+# --------------------------------------------------------------------------
+# test_core_fluid.py:1756
+def test_fv_cg_interface_coupling_enters_operator_symmetrically():
+    s = _unit_solver(5)
+    pressure = np.ones((5, 5, 5), np.float32)
+    pressure[2, 2, 2] = 3.0
+    pressure[2, 2, 3] = 1.0
+    s.pressure_tmp.from_numpy(pressure)
+    s._fv_laplacian_apply_kernel(s.pressure_tmp, s.cg_r, 0)
+    base = s.cg_r.to_numpy()
+    diagonal = np.zeros((5, 5, 5), np.float32)
+    diagonal[2, 2, 2] = 4.0
+    diagonal[2, 2, 3] = 4.0
+    s.pressure_interface_matrix_diagonal.from_numpy(diagonal)
+    s.pressure_interface_coupling_active[2, 2, 2] = 1
+    s.pressure_interface_coupling_neighbor[2, 2, 2] = (2, 2, 3)
+    s.pressure_interface_coupling_coefficient[2, 2, 2] = 4.0 * 0.2 * 0.2 * 0.2
+    s._fv_laplacian_apply_kernel(s.pressure_tmp, s.cg_Ad, 0)
+    coupled = s.cg_Ad.to_numpy()
+    assert coupled[2, 2, 2] - base[2, 2, 2] == pytest.approx(8.0, abs=1e-5)
+    assert coupled[2, 2, 3] - base[2, 2, 3] == pytest.approx(-8.0, abs=1e-5)
+
+
+# test_core_fluid.py:1793
+def test_fv_cg_interface_coupling_uses_transmissibility_on_nonuniform_cells():
+    from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
+    from easyfsi_b200.grid import CartesianGrid
+
+    grid = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0), cell_widths_x_m=(0.1, 0.2, 0.35, 0.35),
+                         cell_widths_y_m=(0.25,) * 4, cell_widths_z_m=(0.25,) * 4)
+    s = CartesianFluidSolver(FluidDomainSpec(grid.bounds_min_m, grid.bounds_max_m, None, 1000.0, 1.0e-3, 1.0e-3,
+                                             cartesian_grid=grid))
+    rng = np.random.default_rng(41)
+    x = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    y = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    t, left, right = 0.375, (1, 2, 2), (2, 2, 2)
+    diagonal = np.zeros(grid.grid_nodes, np.float32)
+    diagonal[left] = t / (0.2 * 0.25 * 0.25)
+    diagonal[right] = t / (0.35 * 0.25 * 0.25)
+    s.pressure_interface_matrix_diagonal.from_numpy(diagonal)
+    s.pressure_interface_coupling_active[left] = 1
+    s.pressure_interface_coupling_neighbor[left] = right
+    s.pressure_interface_coupling_coefficient[left] = t
+    s.pressure_tmp.from_numpy(x)
+    s.cg_d.from_numpy(y)
+    s._fv_laplacian_apply_kernel(s.pressure_tmp, s.cg_r, 0)
+    s._fv_laplacian_apply_kernel(s.cg_d, s.cg_Ad, 0)
+    lhs = float(s._weighted_dot_kernel(s.cg_r, s.cg_d))
+    rhs = float(s._weighted_dot_kernel(s.pressure_tmp, s.cg_Ad))
+    assert abs(lhs - rhs) / max(abs(lhs), abs(rhs), 1e-30) < 1e-5
+
+
+# test_core_fluid.py:1836
+def test_fv_cg_interface_coupling_applies_multiple_owner_slots():
+    s = _unit_solver(5)
+    pressure = np.ones((5, 5, 5), np.float32)
+    owner, n0, n1 = (2, 2, 2), (2, 2, 3), (2, 3, 2)
+    pressure[owner] = 3.0
+    pressure[n0] = 1.0
+    pressure[n1] = 2.0
+    s.pressure_tmp.from_numpy(pressure)
+    s._fv_laplacian_apply_kernel(s.pressure_tmp, s.cg_r, 0)
+    base = s.cg_r.to_numpy()
+    v = 0.2**3
+    c0, c1 = 4.0 * v, 7.0 * v
+    diagonal = np.zeros((5, 5, 5), np.float32)
+    diagonal[owner] = (c0 + c1) / v
+    diagonal[n0] = c0 / v
+    diagonal[n1] = c1 / v
+    s.pressure_interface_matrix_diagonal.from_numpy(diagonal)
+    s.pressure_interface_coupling_active[owner] = 2
+    s.pressure_interface_coupling_neighbor[owner] = n0
+    s.pressure_interface_coupling_coefficient[owner] = c0
+    s.pressure_interface_coupling_extra_neighbor[owner[0], owner[1], owner[2], 0] = n1
+    s.pressure_interface_coupling_extra_coefficient[owner[0], owner[1], owner[2], 0] = c1
+    s._fv_laplacian_apply_kernel(s.pressure_tmp, s.cg_Ad, 0)
+    op = s.cg_Ad.to_numpy()
+    assert op[owner] - base[owner] == pytest.approx(15.0, abs=5e-5)
+    assert op[n0] - base[n0] == pytest.approx(-8.0, abs=5e-5)
+    assert op[n1] - base[n1] == pytest.approx(-7.0, abs=5e-5)
