@@ -236,6 +236,99 @@ def family_timing(scene, steps: int, peak_gbs: float, world: int) -> dict:
     return out
 
 
+def learned_arm(scene, steps: int, warmup: int, world: int, plain_value: float, train_steps: int) -> dict:
+    """The learned preconditioner on the same scene: a U-Net trained on
+    (residual, error) pairs harvested from the scene's own MG-PCG solves
+    (systems of two predicted velocities; truncated solves of 1..32
+    iterations), on 32^3 crops; then one pressure solve and `steps` coupled
+    steps with cg_preconditioner="learned" (flexible PCG, z = network(r), the
+    2/24/2 V-cycle taking over a 16-iteration block that does not halve the
+    residual), next to the plain FP64 MG-PCG step.  The training is timed
+    apart and is not part of a step."""
+    import torch
+    import torch.distributed as dist
+
+    from easyfsi_b200.learned import UNetPreconditioner, harvest_pairs
+
+    fl, cfg = scene.fluid, scene.cfg
+    stream = torch.cuda.current_stream()
+    net = UNetPreconditioner(seed=7)
+    fl.set_learned_preconditioner(net)
+    saved = (fl.velocity.tensor.clone(), fl.pressure.tensor.clone())
+    t0 = time.perf_counter()
+    pairs = []
+    for _ in range(2):
+        fl.predict(cfg.dt_s)
+        fl.compute_divergence()
+        pairs += harvest_pairs(fl, rhs_scale=cfg.density_kgm3 / cfg.dt_s)
+    torch.cuda.synchronize()
+    harvest_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    hist = net.train(pairs, steps=train_steps, batch=4, crop=32, lr=1e-3, seed=3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del pairs
+    # one pressure solve of the last predicted velocity's system
+    solve = {}
+    for name, iters in (("fv_multigrid", cfg.cg_max_iterations), ("learned", cfg.cg_max_iterations),
+                        ("learned_no_fallback", 48)):
+        times = []
+        for r in range(3):
+            fl.pressure.tensor.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fl._solve_pressure_poisson_fv_cg(iterations=iters, rhs_scale=cfg.density_kgm3 / cfg.dt_s,
+                                             pressure_outlet_zmin=False, tolerance=cfg.cg_tolerance,
+                                             preconditioner=name)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if r > 0:
+                times.append(e0.elapsed_time(e1))
+        solve[name] = {"ms": float(np.median(times)), "iterations": int(fl.last_cg_iterations),
+                       "converged": bool(fl.last_cg_converged),
+                       "relative_residual": float(fl.last_cg_relative_residual),
+                       "learned_iterations": int(fl.last_cg_learned_iterations),
+                       "learned_relative_residual": float(fl.last_cg_learned_relative_residual)}
+    fl.velocity.tensor.copy_(saved[0])
+    fl.pressure.tensor.copy_(saved[1])
+    # coupled steps with the learned preconditioner
+    scene.preconditioner = "learned"
+    for _ in range(max(1, warmup)):
+        scene.step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    its, lits, res = [], [], []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        scene.step()
+        its.append(scene.last_cg_iterations)
+        lits.append(fl.last_cg_learned_iterations)
+        res.append(fl.last_cg_relative_residual)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    scene.preconditioner = "fv_multigrid"
+    value = replica_steps_per_s(world, steps, max_over_ranks(e0.elapsed_time(e1), world, "cuda"))
+    fl.set_learned_preconditioner(None)
+    return {
+        "value": value,
+        "unit": "steps/s",
+        "ratio_to_fv_multigrid": value / plain_value,
+        "preconditioner": "U-Net (4 levels, 16/32/48/64 ch, BF16, FP32 accumulation on tcgen05) in the FP64 "
+                          "flexible PCG; 2/24/2 V-cycle fallback",
+        "cg_iterations_mean": float(np.mean(its)),
+        "learned_iterations_mean": float(np.mean(lits)),
+        "max_relative_residual": float(max(res)),
+        "solve": solve,
+        "parameters": net.param_count,
+        "training": {"steps": train_steps, "batch": 4, "crop": 32, "harvest_s": harvest_s, "train_s": train_s,
+                     "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-10:]))},
+    }
+
+
 def max_over_ranks(ms: float, world: int, device) -> float:
     """Largest per-rank time over all ranks (every rank calls this in the same
     order; a no-op for one rank)."""
@@ -319,6 +412,8 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=3, help="timed CPU-oracle steps of the GPU arm's cpu_baseline")
     ap.add_argument("--cpu-warmup", type=int, default=1)
     ap.add_argument("--no-family-timing", action="store_true", help="skip the MPM / HIBM kernel-family timing pass")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
+    ap.add_argument("--learned-train-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-reps", type=int, default=50)
     args = ap.parse_args()
@@ -445,6 +540,14 @@ def main() -> None:
             psolve = pressure_solve_stats(scene, reps=2)
         except Exception as exc:  # reported, never fatal to the step's line
             psolve = {"error": f"{type(exc).__name__}: {exc}"}
+
+    # --- the learned preconditioner (trained here, then timed like the step) ---
+    learned = None
+    if not args.no_learned:
+        try:
+            learned = learned_arm(scene, args.steps, args.warmup, world, value, args.learned_train_steps)
+        except Exception as exc:  # reported, never fatal to the step's line
+            learned = {"error": f"{type(exc).__name__}: {exc}"}
 
     # --- e2e through the public API with host-resident state ---
     e2e = None
@@ -576,6 +679,7 @@ def main() -> None:
             "solve_iterations": solve_iters,
             "cg_iterations_mean": float(np.mean(iters)) if iters else None,
             "mixed_precision": mixed,
+            "learned": learned,
             "particle_families": particle_families,
             "kernel_families": fam_stats,
             "preconditioner": vcycle_stats,

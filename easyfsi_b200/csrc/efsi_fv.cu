@@ -2416,7 +2416,7 @@ static int precondition(PcgRun& R) {
     EFSI_COUNTED launch_pdl(k_learned_pack, R.S.grid, R.S.block, 0, R.s, R.L, (const double*)P->r, in, P->unet_wmin[0],
                             P->unet_wmin[1], P->unet_wmin[2], (const CgScalars*)P->sc);
     const float* out = nullptr;
-    EFSI_TRY(unet_run(P->unet, in, &P->sc->fault, &out, R.s));
+    EFSI_TRY(unet_run(P->unet, P->lv[0].nx, P->lv[0].ny, P->lv[0].nz, in, &P->sc->fault, &out, R.s));
     EFSI_COUNTED launch_pdl(k_learned_unpack, R.S.grid, R.S.block, 0, R.s, R.L, out, P->z, want_mean ? 1 : 0,
                             P->partials, P->sc);
   } else if (R.use_mg) {

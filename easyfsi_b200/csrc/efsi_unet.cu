@@ -307,6 +307,23 @@ using namespace efsi;
 // ---------------------------------------------------------------------------
 // The network object
 // ---------------------------------------------------------------------------
+namespace efsi {
+// Buffers of one volume size: layer outputs, decoder inputs, pooled inputs,
+// the FP32 output and the backward pass's gradients.
+struct UnetWorkspace {
+  Dims dims[kLevels] = {};
+  bf16* act[kLayers] = {};     // layer outputs
+  bf16* cat[3] = {};           // decoder inputs [up, skip] at levels 2, 1, 0
+  bf16* pooled[3] = {};        // encoder inputs at levels 1, 2, 3
+  float* outf = nullptr;       // FP32 output of the last layer
+  float* gbuf[2] = {};         // gradient ping-pong (FP32), sized for the largest layer input
+  float* gskip[kLevels] = {};  // accumulated gradients of e_0 .. e_3
+  float* gcoarse = nullptr;
+  bf16* dpre = nullptr;
+  float* dout = nullptr;
+};
+}  // namespace efsi
+
 struct efsi_unet {
   // parameters (FP32 master, gradients, Adam moments) packed per layer:
   // weights [cout][27][cin] then bias [cout]
@@ -319,78 +336,76 @@ struct efsi_unet {
   bf16* wb[kLayers] = {};
   bf16* wt[kLayers] = {};
   int adam_step = 0;
-  // workspace for one volume size
-  Dims dims[kLevels] = {};
-  int64_t cap[kLevels] = {0, 0, 0, 0};
-  bf16* act[kLayers] = {};   // layer outputs
-  bf16* cat[3] = {};         // decoder inputs [up, skip] at levels 2, 1, 0
-  bf16* pooled[3] = {};      // encoder inputs at levels 1, 2, 3
-  float* outf = nullptr;     // FP32 output of the last layer
-  float* gbuf[2] = {};       // gradient ping-pong (FP32), sized for the largest layer input
-  float* gskip[kLevels] = {};  // accumulated gradients of e_0 .. e_3
-  float* gcoarse = nullptr;
-  bf16* dpre = nullptr;
+  // one workspace per volume size, kept until the network is destroyed (a
+  // solver plan may have captured a workspace's buffers in its CUDA graphs);
+  // `w` is the one of the current pass
+  std::vector<efsi::UnetWorkspace*> spaces;
+  efsi::UnetWorkspace* w = nullptr;
   double* loss = nullptr;
   int* error = nullptr;      // the network's own error word
   int* run_error = nullptr;  // where the convolutions of a run report (the PCG's fault word inside a solve)
-  float* target = nullptr;
-  float* mask = nullptr;
-  float* dout = nullptr;
-  int64_t in_cap = 0;
 };
 
 namespace efsi {
 namespace {
 
-void free_workspace(efsi_unet* U) {
-  for (auto& a : U->act) cudaFree(a), a = nullptr;
-  for (auto& a : U->cat) cudaFree(a), a = nullptr;
-  for (auto& a : U->pooled) cudaFree(a), a = nullptr;
-  for (auto& a : U->gbuf) cudaFree(a), a = nullptr;
-  for (auto& a : U->gskip) cudaFree(a), a = nullptr;
-  cudaFree(U->outf);
-  cudaFree(U->gcoarse);
-  cudaFree(U->dpre);
-  cudaFree(U->target);
-  cudaFree(U->mask);
-  cudaFree(U->dout);
-  U->outf = U->gcoarse = U->target = U->mask = U->dout = nullptr;
-  U->dpre = nullptr;
-  for (int l = 0; l < kLevels; ++l) U->cap[l] = 0;
-  U->dims[0] = Dims{0, 0, 0};
+constexpr int kMaxWorkspaces = 8;
+
+void free_workspace(UnetWorkspace* W) {
+  for (auto& a : W->act) cudaFree(a), a = nullptr;
+  for (auto& a : W->cat) cudaFree(a), a = nullptr;
+  for (auto& a : W->pooled) cudaFree(a), a = nullptr;
+  for (auto& a : W->gbuf) cudaFree(a), a = nullptr;
+  for (auto& a : W->gskip) cudaFree(a), a = nullptr;
+  cudaFree(W->outf);
+  cudaFree(W->gcoarse);
+  cudaFree(W->dpre);
+  cudaFree(W->dout);
+  W->outf = W->gcoarse = W->dout = nullptr;
+  W->dpre = nullptr;
 }
 
-// (Re)allocates the workspace for a level-0 volume of the given extents.
+// Selects (allocating on first use) the workspace of a level-0 volume.
 int ensure_workspace(efsi_unet* U, int nx, int ny, int nz) {
+  for (UnetWorkspace* W : U->spaces)
+    if (W->dims[0].nx == nx && W->dims[0].ny == ny && W->dims[0].nz == nz) {
+      U->w = W;
+      return EFSI_OK;
+    }
+  if ((int)U->spaces.size() >= kMaxWorkspaces) {
+    set_error("the U-Net already holds workspaces for 8 volume sizes");
+    return EFSI_ERR_ARG;
+  }
+  UnetWorkspace* W = new UnetWorkspace();
   const Dims d0{nx, ny, nz};
-  if (U->dims[0].nx == nx && U->dims[0].ny == ny && U->dims[0].nz == nz) return EFSI_OK;
-  free_workspace(U);
-  U->dims[0] = d0;
-  for (int l = 1; l < kLevels; ++l) U->dims[l] = coarse_of(U->dims[l - 1]);
+  W->dims[0] = d0;
+  for (int l = 1; l < kLevels; ++l) W->dims[l] = coarse_of(W->dims[l - 1]);
   auto alloc_bf = [](bf16** p, int64_t n) { return cudaMalloc(p, (size_t)std::max<int64_t>(n, 1) * sizeof(bf16)); };
   auto alloc_f = [](float** p, int64_t n) { return cudaMalloc(p, (size_t)std::max<int64_t>(n, 1) * sizeof(float)); };
   int64_t gmax = 0;
   for (int l = 0; l < kLayers; ++l) {
-    const int64_t n = U->dims[kSpec[l].level].n();
-    if (alloc_bf(&U->act[l], n * kSpec[l].cout) != cudaSuccess) goto fail;
+    const int64_t n = W->dims[kSpec[l].level].n();
+    if (alloc_bf(&W->act[l], n * kSpec[l].cout) != cudaSuccess) goto fail;
     gmax = std::max(gmax, n * std::max(kSpec[l].cin, kSpec[l].cout));
   }
   for (int q = 0; q < 3; ++q) {
     const int l = 2 - q;  // decoder levels 2, 1, 0
-    const int64_t n = U->dims[l].n();
-    if (alloc_bf(&U->cat[q], n * (kCh[l + 1] + kCh[l])) != cudaSuccess) goto fail;
-    if (alloc_bf(&U->pooled[q], U->dims[q + 1].n() * kCh[q]) != cudaSuccess) goto fail;
+    const int64_t n = W->dims[l].n();
+    if (alloc_bf(&W->cat[q], n * (kCh[l + 1] + kCh[l])) != cudaSuccess) goto fail;
+    if (alloc_bf(&W->pooled[q], W->dims[q + 1].n() * kCh[q]) != cudaSuccess) goto fail;
   }
   for (int l = 0; l < kLevels; ++l)
-    if (alloc_f(&U->gskip[l], U->dims[l].n() * kCh[l]) != cudaSuccess) goto fail;
-  if (alloc_f(&U->gbuf[0], gmax) != cudaSuccess || alloc_f(&U->gbuf[1], gmax) != cudaSuccess ||
-      alloc_f(&U->gcoarse, gmax) != cudaSuccess || alloc_bf(&U->dpre, gmax) != cudaSuccess ||
-      alloc_f(&U->outf, d0.n() * kOutCh) != cudaSuccess || alloc_f(&U->target, d0.n()) != cudaSuccess ||
-      alloc_f(&U->mask, d0.n()) != cudaSuccess || alloc_f(&U->dout, d0.n() * kOutCh) != cudaSuccess)
+    if (alloc_f(&W->gskip[l], W->dims[l].n() * kCh[l]) != cudaSuccess) goto fail;
+  if (alloc_f(&W->gbuf[0], gmax) != cudaSuccess || alloc_f(&W->gbuf[1], gmax) != cudaSuccess ||
+      alloc_f(&W->gcoarse, gmax) != cudaSuccess || alloc_bf(&W->dpre, gmax) != cudaSuccess ||
+      alloc_f(&W->outf, d0.n() * kOutCh) != cudaSuccess || alloc_f(&W->dout, d0.n() * kOutCh) != cudaSuccess)
     goto fail;
+  U->spaces.push_back(W);
+  U->w = W;
   return EFSI_OK;
 fail:
-  free_workspace(U);
+  free_workspace(W);
+  delete W;
   set_error("cudaMalloc failed for the U-Net workspace");
   return EFSI_ERR_CUDA;
 }
@@ -442,35 +457,35 @@ int forward(efsi_unet* U, const bf16* input, cudaStream_t s) {
   int* err = U->run_error != nullptr ? U->run_error : U->error;
   // encoder
   for (int l = 0; l < kLevels; ++l) {
-    const Dims& d = U->dims[l];
+    const Dims& d = U->w->dims[l];
     if (l > 0) {
-      EFSI_COUNTED k_pool<<<grid_for(d.n() * kCh[l - 1]), 256, 0, s>>>(U->dims[l - 1], d, kCh[l - 1], U->act[2 * l - 1],
-                                                                    U->pooled[l - 1]);
-      x = U->pooled[l - 1];
+      EFSI_COUNTED k_pool<<<grid_for(d.n() * kCh[l - 1]), 256, 0, s>>>(U->w->dims[l - 1], d, kCh[l - 1], U->w->act[2 * l - 1],
+                                                                    U->w->pooled[l - 1]);
+      x = U->w->pooled[l - 1];
     }
     const int a = 2 * l, b = 2 * l + 1;
-    EFSI_TRY(conv_launch(d, kSpec[a].cin, kSpec[a].cout, x, U->wb[a], U->p + U->boff[a], 1, U->act[a], nullptr,
+    EFSI_TRY(conv_launch(d, kSpec[a].cin, kSpec[a].cout, x, U->wb[a], U->p + U->boff[a], 1, U->w->act[a], nullptr,
                          err, s));
-    EFSI_TRY(conv_launch(d, kSpec[b].cin, kSpec[b].cout, U->act[a], U->wb[b], U->p + U->boff[b], 1, U->act[b],
+    EFSI_TRY(conv_launch(d, kSpec[b].cin, kSpec[b].cout, U->w->act[a], U->wb[b], U->p + U->boff[b], 1, U->w->act[b],
                          nullptr, err, s));
   }
   // decoder
-  const bf16* coarse = U->act[7];
+  const bf16* coarse = U->w->act[7];
   for (int q = 0; q < 3; ++q) {
     const int l = 2 - q;
-    const Dims& d = U->dims[l];
+    const Dims& d = U->w->dims[l];
     const int ca = kCh[l + 1];
-    EFSI_COUNTED k_up_concat<<<grid_for(d.n() * (ca + kCh[l])), 256, 0, s>>>(d, U->dims[l + 1], ca, kCh[l], coarse,
-                                                                          U->act[2 * l + 1], U->cat[q]);
+    EFSI_COUNTED k_up_concat<<<grid_for(d.n() * (ca + kCh[l])), 256, 0, s>>>(d, U->w->dims[l + 1], ca, kCh[l], coarse,
+                                                                          U->w->act[2 * l + 1], U->w->cat[q]);
     const int a = 8 + 2 * q, b = 9 + 2 * q;
-    EFSI_TRY(conv_launch(d, kSpec[a].cin, kSpec[a].cout, U->cat[q], U->wb[a], U->p + U->boff[a], 1, U->act[a],
+    EFSI_TRY(conv_launch(d, kSpec[a].cin, kSpec[a].cout, U->w->cat[q], U->wb[a], U->p + U->boff[a], 1, U->w->act[a],
                          nullptr, err, s));
-    EFSI_TRY(conv_launch(d, kSpec[b].cin, kSpec[b].cout, U->act[a], U->wb[b], U->p + U->boff[b], 1, U->act[b],
+    EFSI_TRY(conv_launch(d, kSpec[b].cin, kSpec[b].cout, U->w->act[a], U->wb[b], U->p + U->boff[b], 1, U->w->act[b],
                          nullptr, err, s));
-    coarse = U->act[b];
+    coarse = U->w->act[b];
   }
-  EFSI_TRY(conv_launch(U->dims[0], kSpec[14].cin, kSpec[14].cout, U->act[13], U->wb[14], U->p + U->boff[14], 0,
-                       U->act[14], U->outf, err, s));
+  EFSI_TRY(conv_launch(U->w->dims[0], kSpec[14].cin, kSpec[14].cout, U->w->act[13], U->wb[14], U->p + U->boff[14], 0,
+                       U->w->act[14], U->w->outf, err, s));
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
@@ -478,32 +493,32 @@ int forward(efsi_unet* U, const bf16* input, cudaStream_t s) {
 // Input of layer l during the forward pass.
 const bf16* layer_input(efsi_unet* U, const bf16* input, int l) {
   if (l == 0) return input;
-  if (l < 8) return (l % 2 == 1) ? U->act[l - 1] : U->pooled[l / 2 - 1];
-  if (l < 14) return (l % 2 == 0) ? U->cat[(l - 8) / 2] : U->act[l - 1];
-  return U->act[13];
+  if (l < 8) return (l % 2 == 1) ? U->w->act[l - 1] : U->w->pooled[l / 2 - 1];
+  if (l < 14) return (l % 2 == 0) ? U->w->cat[(l - 8) / 2] : U->w->act[l - 1];
+  return U->w->act[13];
 }
 
 // Backward of one layer: gy (FP32 [n][cout]) -> parameter gradients, and the
 // input gradient into gx (FP32 [n][cin]) when gx is given.
 int layer_backward(efsi_unet* U, const bf16* input, int l, const float* gy, float* gx, cudaStream_t s) {
   const LayerSpec& L = kSpec[l];
-  const Dims& d = U->dims[L.level];
+  const Dims& d = U->w->dims[L.level];
   const int64_t n = d.n();
-  EFSI_COUNTED k_relu_back<<<grid_for(n * L.cout), 256, 0, s>>>(n, L.cout, L.relu, gy, U->act[l], U->dpre,
+  EFSI_COUNTED k_relu_back<<<grid_for(n * L.cout), 256, 0, s>>>(n, L.cout, L.relu, gy, U->w->act[l], U->w->dpre,
                                                              U->g + U->boff[l]);
-  EFSI_TRY(wgrad_launch(d, L.cin, L.cout, layer_input(U, input, l), U->dpre, U->g + U->woff[l], s));
+  EFSI_TRY(wgrad_launch(d, L.cin, L.cout, layer_input(U, input, l), U->w->dpre, U->g + U->woff[l], s));
   if (gx != nullptr)
-    EFSI_TRY(conv_launch(d, L.cout, L.cin, U->dpre, U->wt[l], nullptr, 0, nullptr, gx, U->error, s));
+    EFSI_TRY(conv_launch(d, L.cout, L.cin, U->w->dpre, U->wt[l], nullptr, 0, nullptr, gx, U->error, s));
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
 
 // Backward pass from dout (FP32 [n0][16]); accumulates into U->g.
 int backward(efsi_unet* U, const bf16* input, const float* dout, cudaStream_t s) {
-  float* ga = U->gbuf[0];
-  float* gb = U->gbuf[1];
+  float* ga = U->w->gbuf[0];
+  float* gb = U->w->gbuf[1];
   for (int l = 0; l < kLevels; ++l)
-    EFSI_CUDA_CHECK(cudaMemsetAsync(U->gskip[l], 0, (size_t)U->dims[l].n() * kCh[l] * sizeof(float), s));
+    EFSI_CUDA_CHECK(cudaMemsetAsync(U->w->gskip[l], 0, (size_t)U->w->dims[l].n() * kCh[l] * sizeof(float), s));
   // output layer and the decoder, level 0 up to level 2
   EFSI_TRY(layer_backward(U, input, 14, dout, ga, s));  // -> g(d0)
   const float* gcur = ga;
@@ -515,25 +530,25 @@ int backward(efsi_unet* U, const bf16* input, const float* dout, cudaStream_t s)
     float* t2 = (t1 == ga) ? gb : ga;
     EFSI_TRY(layer_backward(U, input, a, t1, t2, s));  // -> g([up, skip])
     const int ca = kCh[l + 1], cb = kCh[l];
-    EFSI_COUNTED k_up_concat_back_skip<<<grid_for(U->dims[l].n() * cb), 256, 0, s>>>(U->dims[l], ca, cb, t2,
-                                                                                   U->gskip[l]);
-    EFSI_COUNTED k_up_concat_back_coarse<<<grid_for(U->dims[l + 1].n() * ca), 256, 0, s>>>(
-        U->dims[l], U->dims[l + 1], ca, cb, t2, U->gcoarse);
+    EFSI_COUNTED k_up_concat_back_skip<<<grid_for(U->w->dims[l].n() * cb), 256, 0, s>>>(U->w->dims[l], ca, cb, t2,
+                                                                                   U->w->gskip[l]);
+    EFSI_COUNTED k_up_concat_back_coarse<<<grid_for(U->w->dims[l + 1].n() * ca), 256, 0, s>>>(
+        U->w->dims[l], U->w->dims[l + 1], ca, cb, t2, U->w->gcoarse);
     // the coarse gradient is that of d_{l+1} (or e_3 for the deepest block)
     float* nxt = (t2 == ga) ? gb : ga;
-    EFSI_CUDA_CHECK(cudaMemcpyAsync(nxt, U->gcoarse, (size_t)U->dims[l + 1].n() * ca * sizeof(float),
+    EFSI_CUDA_CHECK(cudaMemcpyAsync(nxt, U->w->gcoarse, (size_t)U->w->dims[l + 1].n() * ca * sizeof(float),
                                     cudaMemcpyDeviceToDevice, s));
     gcur = nxt;
   }
   // gcur is g(e_3) from the decoder; the encoder from level 3 down to 0
   for (int l = kLevels - 1; l >= 0; --l) {
-    const Dims& d = U->dims[l];
+    const Dims& d = U->w->dims[l];
     float* gin;
     if (l == kLevels - 1) {
       gin = const_cast<float*>(gcur);
     } else {
       // e_l receives its skip gradient plus the pooled path's
-      gin = U->gskip[l];
+      gin = U->w->gskip[l];
     }
     const int a = 2 * l, b = 2 * l + 1;
     float* t1 = (gin == ga) ? gb : ga;
@@ -544,8 +559,8 @@ int backward(efsi_unet* U, const bf16* input, const float* dout, cudaStream_t s)
     }
     float* t2 = (t1 == ga) ? gb : ga;
     EFSI_TRY(layer_backward(U, input, a, t1, t2, s));  // -> g(pooled e_{l-1})
-    EFSI_COUNTED k_pool_back<<<grid_for(U->dims[l - 1].n() * kCh[l - 1]), 256, 0, s>>>(U->dims[l - 1], d, kCh[l - 1],
-                                                                                     t2, U->gskip[l - 1]);
+    EFSI_COUNTED k_pool_back<<<grid_for(U->w->dims[l - 1].n() * kCh[l - 1]), 256, 0, s>>>(U->w->dims[l - 1], d, kCh[l - 1],
+                                                                                     t2, U->w->gskip[l - 1]);
   }
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
@@ -566,11 +581,14 @@ int check_error(efsi_unet* U, cudaStream_t s) {
 
 int unet_prepare(efsi_unet* U, int nx, int ny, int nz) { return ensure_workspace(U, nx, ny, nz); }
 
-int unet_run(efsi_unet* U, const void* input, int* error_word, const float** out, cudaStream_t s) {
+int unet_run(efsi_unet* U, int nx, int ny, int nz, const void* input, int* error_word, const float** out,
+             cudaStream_t s) {
+  // the volume's workspace exists (unet_prepare), so this only selects it
+  EFSI_TRY(ensure_workspace(U, nx, ny, nz));
   U->run_error = error_word;
   const int rc = forward(U, static_cast<const bf16*>(input), s);
   U->run_error = nullptr;
-  *out = U->outf;
+  *out = U->w->outf;
   return rc;
 }
 
@@ -649,7 +667,11 @@ int efsi_unet_create(int32_t seed, efsi_unet** out) {
 
 int efsi_unet_destroy(efsi_unet* U) {
   if (U == nullptr) return EFSI_OK;
-  free_workspace(U);
+  for (UnetWorkspace* W : U->spaces) {
+    free_workspace(W);
+    delete W;
+  }
+  U->spaces.clear();
   cudaFree(U->p);
   cudaFree(U->g);
   cudaFree(U->m);
@@ -710,7 +732,7 @@ int efsi_unet_forward(efsi_unet* U, int32_t nx, int32_t ny, int32_t nz, const vo
   EFSI_TRY(ensure_workspace(U, nx, ny, nz));
   EFSI_TRY(forward(U, static_cast<const bf16*>(input), s));
   if (output != nullptr)
-    EFSI_CUDA_CHECK(cudaMemcpyAsync(output, U->outf, (size_t)U->dims[0].n() * kOutCh * sizeof(float),
+    EFSI_CUDA_CHECK(cudaMemcpyAsync(output, U->w->outf, (size_t)U->w->dims[0].n() * kOutCh * sizeof(float),
                                     cudaMemcpyDeviceToDevice, s));
   return check_error(U, s);
 }
@@ -724,10 +746,10 @@ int efsi_unet_accumulate_gradient(efsi_unet* U, int32_t nx, int32_t ny, int32_t 
   EFSI_TRY(ensure_workspace(U, nx, ny, nz));
   const bf16* in = static_cast<const bf16*>(input);
   EFSI_TRY(forward(U, in, s));
-  const int64_t n = U->dims[0].n();
+  const int64_t n = U->w->dims[0].n();
   EFSI_CUDA_CHECK(cudaMemsetAsync(U->loss, 0, sizeof(double), s));
-  EFSI_COUNTED k_loss<<<grid_for(n), 256, 0, s>>>(n, U->outf, target, mask, 1.0f / (float)n, U->dout, U->loss);
-  EFSI_TRY(backward(U, in, U->dout, s));
+  EFSI_COUNTED k_loss<<<grid_for(n), 256, 0, s>>>(n, U->w->outf, target, mask, 1.0f / (float)n, U->w->dout, U->loss);
+  EFSI_TRY(backward(U, in, U->w->dout, s));
   EFSI_CUDA_CHECK(cudaMemcpyAsync(loss_host, U->loss, sizeof(double), cudaMemcpyDeviceToHost, s));
   return check_error(U, s);
 }

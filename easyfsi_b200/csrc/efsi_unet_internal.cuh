@@ -11,10 +11,11 @@ namespace efsi {
 // stream capture of unet_run).
 int unet_prepare(efsi_unet* U, int nx, int ny, int nz);
 
-// One forward pass over the prepared volume: input [n][16] BF16; *out is set
+// One forward pass over a prepared volume: input [n][16] BF16; *out is set
 // to the network's FP32 output [n][16] (channel 0 is the preconditioned
 // residual).  Convolutions that give up on a wait set *error_word.  Launches
 // only (no allocation, no synchronisation), so it can be captured.
-int unet_run(efsi_unet* U, const void* input, int* error_word, const float** out, cudaStream_t s);
+int unet_run(efsi_unet* U, int nx, int ny, int nz, const void* input, int* error_word, const float** out,
+             cudaStream_t s);
 
 }  // namespace efsi
