@@ -227,6 +227,7 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_fv_set_learned_preconditioner": [P, P, P],
     "efsi_fv_set_interface_coupling": [P, I, P, P, P, P, P],
     "efsi_fv_copy_rhs": [P, P, P],
+    "efsi_zero_buffers": [I, P, P, P],
     "efsi_fv_learned_input": [P, P, P, P],
     "efsi_reach_plan_create": [POINTER(c_void_p)],
     "efsi_reach_plan_destroy": [P],

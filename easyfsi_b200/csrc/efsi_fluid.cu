@@ -1,3 +1,4 @@
+#include <algorithm>
 // Fluid kernels around the pressure solve, B200 path: divergence, the level-0
 // right-hand side, the pressure-gradient correction and wall conditions, the
 // semi-Lagrangian predictor, divergence statistics and the point-force
@@ -398,6 +399,20 @@ __global__ void k_body_force(LevelDev L, const float* __restrict__ force, float 
 
 }  // namespace efsi
 
+namespace efsi {
+constexpr int kZeroListMax = 64;
+struct ZeroList {
+  int n;
+  uint32_t* p[kZeroListMax];
+  int64_t words[kZeroListMax];
+};
+__global__ void k_zero_list(ZeroList Z) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int b = 0; b < Z.n; ++b)
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < Z.words[b]; q += stride) Z.p[b][q] = 0u;
+}
+}  // namespace efsi
+
 using namespace efsi;
 
 extern "C" {
@@ -539,6 +554,29 @@ int efsi_apply_body_force(efsi_fv_plan* P, const float* grid_force_density, floa
   cudaStream_t s = as_stream(stream);
   if (report_device) EFSI_CUDA_CHECK(cudaMemsetAsync(report_device, 0, 7 * sizeof(double), s));
   EFSI_COUNTED k_body_force<<<S.grid, S.block, 0, s>>>(L, grid_force_density, dt, density, velocity, report_device);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+
+// Zeroes up to 64 buffers (4-byte multiples) in one launch: the per-solve
+// clears of the reference's multigrid work fields (fluid.py:5228-5260
+// _prepare_fv_multigrid_rhs) as one kernel instead of one fill per field.
+int efsi_zero_buffers(int32_t count, void* const* ptrs, const int64_t* bytes, void* stream) {
+  EFSI_ARG_CHECK(count >= 0 && count <= efsi::kZeroListMax, "at most 64 buffers per call");
+  if (count == 0) return EFSI_OK;
+  EFSI_ARG_CHECK(ptrs != nullptr && bytes != nullptr, "null argument");
+  efsi::ZeroList Z{};
+  Z.n = count;
+  int64_t total = 0;
+  for (int q = 0; q < count; ++q) {
+    EFSI_ARG_CHECK(ptrs[q] != nullptr && bytes[q] >= 0 && bytes[q] % 4 == 0, "buffers must be 4-byte multiples");
+    Z.p[q] = static_cast<uint32_t*>(ptrs[q]);
+    Z.words[q] = bytes[q] / 4;
+    total += Z.words[q];
+  }
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 8));
+  EFSI_COUNTED efsi::k_zero_list<<<grid, 256, 0, as_stream(stream)>>>(Z);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }

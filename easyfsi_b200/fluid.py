@@ -769,10 +769,20 @@ class CartesianFluidSolver:
             self._mg_rhs[0].ptr(),
             _stream(),
         )
-        self._mg_residual[0].tensor.zero_()
-        for level in range(1, len(self._mg_shapes)):
-            for lst in (self._mg_pressure, self._mg_tmp, self._mg_rhs, self._mg_residual, self._mg_pressure_interface_matrix_diagonal):
-                lst[level].tensor.zero_()
+        # the multigrid work fields start from zero (fluid.py:5228-5260): one
+        # library launch clears them all
+        if getattr(self, "_mg_zero_list", None) is None:
+            fields = [self._mg_residual[0]]
+            for level in range(1, len(self._mg_shapes)):
+                for lst in (self._mg_pressure, self._mg_tmp, self._mg_rhs, self._mg_residual,
+                            self._mg_pressure_interface_matrix_diagonal):
+                    fields.append(lst[level])
+            fields = fields[:64]
+            ptrs = (c_void_p * len(fields))(*[f.ptr() for f in fields])
+            sizes = (ctypes.c_int64 * len(fields))(*[f.tensor.numel() * f.tensor.element_size() for f in fields])
+            self._mg_zero_list = (len(fields), ptrs, sizes)
+        n, ptrs, sizes = self._mg_zero_list
+        _native.call("efsi_zero_buffers", n, ptrs, sizes, _stream())
 
     def _smooth_fv_pressure_level(self, level: int, *, iterations: int, pressure_outlet_zmin: bool, omega: float) -> None:
         self._refresh_structure()
@@ -1284,7 +1294,9 @@ class CartesianFluidSolver:
                 self._apply_closed_boundary_no_normal_flow_kernel(1)
 
         nan_stats = {"max_abs": math.nan, "l2": math.nan}
-        self.pressure_interface_projection_divergence_s.tensor.zero_()
+        f = self.pressure_interface_projection_divergence_s
+        _native.call("efsi_zero_buffers", 1, (c_void_p * 1)(f.ptr()),
+                     (ctypes.c_int64 * 1)(f.tensor.numel() * f.tensor.element_size()), _stream())
         apply_bc()
         self._compute_divergence_kernel(1 if outlet else 0)
         pre_raw = self.divergence_stats() if report else nan_stats

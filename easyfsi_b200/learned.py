@@ -13,8 +13,8 @@ as the plain method.
 
 Pairs (``harvest_pairs``): for a prepared right-hand side b, the multigrid
 PCG is run to convergence (x*) and, from zero, truncated after k iterations
-(x_k); r_k = b - A x_k and e_k = x* - x_k (both with the closed-domain mean
-removed) satisfy A e_k = r_k.  The network input is the solver's own encoding
+(x_k; k = 0 gives r = b, e = x*); r_k = b - A x_k and e_k = x* - x_k (both
+with the closed-domain mean removed) satisfy A e_k = r_k.  The network input is the solver's own encoding
 of r_k (``efsi_fv_learned_input``: r over its volume-weighted RMS, the fluid
 mask, log2 cell widths); the target is e_k over its RMS, since the flexible
 PCG is invariant to the scale of z.  Training takes random crops of the pairs.
@@ -155,7 +155,7 @@ class UNetPreconditioner:
         return history
 
 
-def harvest_pairs(solver, *, rhs_scale: float, truncations=(1, 2, 4, 8, 16, 32), tolerance: float = 1.0e-10,
+def harvest_pairs(solver, *, rhs_scale: float, truncations=(0, 1, 2, 4, 8, 16, 32), tolerance: float = 1.0e-10,
                   max_iterations: int = 400) -> list[TrainingPair]:
     """(residual, error) pairs from the solver's own MG-PCG on the system of
     its current divergence (closed domain, zero-mean pressure).  The network
@@ -180,8 +180,9 @@ def harvest_pairs(solver, *, rhs_scale: float, truncations=(1, 2, 4, 8, 16, 32),
         pairs = []
         for k in truncations:
             fl.pressure.tensor.zero_()
-            fl._solve_pressure_poisson_fv_cg(iterations=int(k), rhs_scale=rhs_scale, pressure_outlet_zmin=False,
-                                             tolerance=0.0, preconditioner="fv_multigrid")
+            if int(k) > 0:  # k = 0: x_0 = 0, r = b, e = x*
+                fl._solve_pressure_poisson_fv_cg(iterations=int(k), rhs_scale=rhs_scale, pressure_outlet_zmin=False,
+                                                 tolerance=0.0, preconditioner="fv_multigrid")
             x_k = fl.pressure.tensor.clone()
             fl._fv_laplacian_apply_kernel(fl.pressure, fl.cg_Ad, 0)
             r = zero_mean(b - fl.cg_Ad.tensor)
@@ -198,3 +199,64 @@ def harvest_pairs(solver, *, rhs_scale: float, truncations=(1, 2, 4, 8, 16, 32),
         return pairs
     finally:
         fl.pressure.tensor.copy_(saved)
+
+
+def _demo(argv=None) -> None:
+    """Train a network on one graded grid and compare solves:
+
+        python -m easyfsi_b200.learned [--nodes 96 96 96] [--steps 200]
+
+    prints one JSON line with the training loss, and ms / iterations of the
+    MG-PCG, the learned PCG (with fallback) and the network alone over a
+    fixed budget of 48 iterations."""
+    import argparse
+    import json
+    import time
+
+    from .fluid import CartesianFluidSolver, FluidDomainSpec
+    from .grid import CartesianGrid
+    from .scenarios import graded_axis_widths
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nodes", type=int, nargs=3, default=(96, 96, 96))
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    nodes = tuple(args.nodes)
+    grid = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0),
+                         cell_widths_x_m=graded_axis_widths(nodes[0], 0.0, 1.0, 0.3, 0.7),
+                         cell_widths_y_m=graded_axis_widths(nodes[1], 0.0, 1.0, 0.3, 0.7),
+                         cell_widths_z_m=graded_axis_widths(nodes[2], 0.0, 1.0, 0.2, 0.8))
+    fl = CartesianFluidSolver(FluidDomainSpec((0, 0, 0), grid.bounds_max_m, None, 1000.0, 1.0e-3, 1.0e-3,
+                                              cartesian_grid=grid))
+    rng = np.random.default_rng(args.seed)
+    net = UNetPreconditioner(seed=args.seed)
+    fl.set_learned_preconditioner(net)
+    pairs = []
+    for _ in range(2):
+        fl.divergence.from_numpy(rng.normal(size=nodes).astype(np.float32))
+        pairs += harvest_pairs(fl, rhs_scale=1.0e6)
+    t0 = time.perf_counter()
+    hist = net.train(pairs, steps=args.steps, batch=4, crop=32, lr=1.0e-3, seed=args.seed)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    fl.divergence.from_numpy(rng.normal(size=nodes).astype(np.float32))
+    out = {"nodes": list(nodes), "parameters": net.param_count, "train_s": train_s,
+           "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-10:]))}
+    for name, iters in (("fv_multigrid", 400), ("learned", 400), ("learned_no_fallback", 48)):
+        for rep in range(2):
+            fl.pressure.tensor.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fl._solve_pressure_poisson_fv_cg(iterations=iters, rhs_scale=1.0e6, pressure_outlet_zmin=False,
+                                             tolerance=1.0e-8, preconditioner=name)
+            torch.cuda.synchronize()
+            ms = 1e3 * (time.perf_counter() - t0)
+        out[name] = {"ms": ms, "iterations": fl.last_cg_iterations, "converged": fl.last_cg_converged,
+                     "relative_residual": fl.last_cg_relative_residual,
+                     "learned_iterations": fl.last_cg_learned_iterations}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    _demo()
