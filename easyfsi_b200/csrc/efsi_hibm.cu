@@ -326,28 +326,21 @@ __device__ __forceinline__ float tent(const float* xm, const float* xp, float R)
   return w;
 }
 
-// Visits the particles of the 3 x 3 x 3 bins around xm; lane `lane` of the
-// calling warp takes every 32nd particle of each bin (in bin order).
+// Visits the particles of the 3 x 3 x 3 bins around xm with one bin per lane
+// (lanes 0..26; lane (d0 + 1) * 9 + (d1 + 1) * 3 + (d2 + 1)), each lane
+// walking its bin in bin order: the 27 bins' offsets and particles are
+// fetched in parallel rather than one bin after another.
 template <class Fn>
-__device__ __forceinline__ void for_near(const BinView& B, const float* xm, int lane, Fn fn) {
-  int c[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) c[a] = bin_axis(xm[a], B.bmin[a], B.invR, B.nb[a]);
-  for (int d0 = -1; d0 <= 1; ++d0) {
-    int b0 = c[0] + d0;
-    if (b0 < 0 || b0 >= B.nb[0]) continue;
-    for (int d1 = -1; d1 <= 1; ++d1) {
-      int b1 = c[1] + d1;
-      if (b1 < 0 || b1 >= B.nb[1]) continue;
-      for (int d2 = -1; d2 <= 1; ++d2) {
-        int b2 = c[2] + d2;
-        if (b2 < 0 || b2 >= B.nb[2]) continue;
-        const int bin = (b0 * B.nb[1] + b1) * B.nb[2] + b2;
-        const int lo = __ldg(B.offset + bin), hi = __ldg(B.offset + bin + 1);
-        for (int q = lo + lane; q < hi; q += 32) fn(__ldg(B.sorted + q));
-      }
-    }
-  }
+__device__ __forceinline__ void for_near_lanes(const BinView& B, const float* xm, int lane, Fn fn) {
+  if (lane >= 27) return;
+  const int d0 = lane / 9 - 1, d1 = (lane / 3) % 3 - 1, d2 = lane % 3 - 1;
+  const int b0 = bin_axis(xm[0], B.bmin[0], B.invR, B.nb[0]) + d0;
+  const int b1 = bin_axis(xm[1], B.bmin[1], B.invR, B.nb[1]) + d1;
+  const int b2 = bin_axis(xm[2], B.bmin[2], B.invR, B.nb[2]) + d2;
+  if (b0 < 0 || b0 >= B.nb[0] || b1 < 0 || b1 >= B.nb[1] || b2 < 0 || b2 >= B.nb[2]) return;
+  const int bin = (b0 * B.nb[1] + b1) * B.nb[2] + b2;
+  const int lo = __ldg(B.offset + bin), hi = __ldg(B.offset + bin + 1);
+  for (int q = lo; q < hi; ++q) fn(__ldg(B.sorted + q));
 }
 
 // Butterfly sums over the warp: every lane gets the same total, summed in a
@@ -364,8 +357,9 @@ __device__ __forceinline__ double warp_allsum(double v) {
 }
 
 // hibm_mpm.py:4899-4959 _scatter_marker_forces_to_mpm_particles_kernel: one
-// warp per marker; the tent-weight sum over the marker's neighbourhood is a
-// warp reduction, then every lane spreads F * w / wsum to its particles.
+// warp per marker, one neighbour bin per lane; the tent-weight sum over the
+// marker's neighbourhood is a warp reduction, then every lane spreads
+// F * w / wsum to its bin's particles.
 __global__ void k_scatter(BinView B, int M, const float* xg, const double* Fg, const float* xp, float* fext,
                           double* rep) {
   const int m = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
@@ -375,11 +369,11 @@ __global__ void k_scatter(BinView B, int M, const float* xg, const double* Fg, c
   const bool valid = finite3(xm) && isfinite(Fm[0]) && isfinite(Fm[1]) && isfinite(Fm[2]);
   const float R = B.R;
   float wl = 0.0f;
-  if (valid) for_near(B, xm, lane, [&](int p) { wl += tent(xm, xp + 3 * p, R); });
+  if (valid) for_near_lanes(B, xm, lane, [&](int p) { wl += tent(xm, xp + 3 * p, R); });
   const float wsum = warp_allsum(wl);
   if (valid && wsum > 1.0e-12f) {
     double e0 = 0, e1 = 0, e2 = 0, contrib = 0;
-    for_near(B, xm, lane, [&](int p) {
+    for_near_lanes(B, xm, lane, [&](int p) {
       float w = tent(xm, xp + 3 * p, R);
       if (w > 0.0f) {
         const double ratio = (double)(w / wsum);
@@ -425,7 +419,7 @@ __global__ void k_feedback(BinView B, int M, float* xg, float* vg, float* ng, fl
   const float ao = Ag[m];
   float vs[3] = {0, 0, 0}, ns[3] = {0, 0, 0}, as = 0.0f, ws = 0.0f, gs = 0.0f;
   const float R = B.R;
-  for_near(B, xo, lane, [&](int p) {
+  for_near_lanes(B, xo, lane, [&](int p) {
     float w = tent(xo, xp + 3 * p, R);
     if (w > 0.0f) {
       vs[0] += w * __ldg(vp + 3 * p);
