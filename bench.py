@@ -240,11 +240,14 @@ def learned_arm(scene, steps: int, warmup: int, world: int, plain_value: float, 
     """The learned preconditioner on the same scene: a U-Net trained on
     (residual, error) pairs harvested from the scene's own MG-PCG solves
     (systems of two predicted velocities; truncated solves of 1..32
-    iterations), on 32^3 crops; then one pressure solve and `steps` coupled
-    steps with cg_preconditioner="learned" (flexible PCG, z = network(r), the
-    2/24/2 V-cycle taking over a 16-iteration block that does not halve the
-    residual), next to the plain FP64 MG-PCG step.  The training is timed
-    apart and is not part of a step."""
+    iterations, minus the pre-smoothing), on 32^3 crops; then one pressure
+    solve per preconditioner and `steps` coupled steps with
+    cg_preconditioner="learned" (flexible PCG; two-level preconditioner: two
+    damped-Jacobi sweeps, the network's correction at its energy-minimising
+    scale, two sweeps; the 2/24/2 V-cycle taking over a 16-iteration block
+    that does not halve the residual), next to the plain FP64 MG-PCG step.
+    "learned_no_fallback" runs the two-level preconditioner alone for at most
+    256 iterations.  The training is timed apart and is not part of a step."""
     import torch
     import torch.distributed as dist
 
@@ -271,7 +274,7 @@ def learned_arm(scene, steps: int, warmup: int, world: int, plain_value: float, 
     # one pressure solve of the last predicted velocity's system
     solve = {}
     for name, iters in (("fv_multigrid", cfg.cg_max_iterations), ("learned", cfg.cg_max_iterations),
-                        ("learned_no_fallback", 48)):
+                        ("learned_no_fallback", 256)):
         times = []
         for r in range(3):
             fl.pressure.tensor.zero_()
@@ -317,7 +320,8 @@ def learned_arm(scene, steps: int, warmup: int, world: int, plain_value: float, 
         "value": value,
         "unit": "steps/s",
         "ratio_to_fv_multigrid": value / plain_value,
-        "preconditioner": "U-Net (4 levels, 16/32/48/64 ch, BF16, FP32 accumulation on tcgen05) in the FP64 "
+        "preconditioner": "two-level: 2 damped-Jacobi sweeps, U-Net correction (4 levels, 16/32/48/64 ch, BF16, "
+                          "FP32 accumulation on tcgen05) at its energy-minimising scale, 2 sweeps; in the FP64 "
                           "flexible PCG; 2/24/2 V-cycle fallback",
         "cg_iterations_mean": float(np.mean(its)),
         "learned_iterations_mean": float(np.mean(lits)),

@@ -6,13 +6,14 @@
 // M = 128 consecutive voxels per CTA, N = Cout (16..256, a multiple of 16) and
 // K = 27 taps x Cin (Cin a multiple of 16).  Per tap the 128 x Cin slice of
 // the im2col matrix (zero outside the volume) and the Cout x Cin slice of the
-// weights are staged by the CTA's threads into shared memory in the canonical
-// no-swizzle K-major layout (8-row x 16-byte core matrices: SBO = 128 bytes
-// between 8-row groups, LBO = rows x 16 bytes between 8-element K chunks),
-// double-buffered; one elected thread issues tcgen05.mma.kind::f16 (BF16
-// operands, FP32 accumulator in tensor memory) per 16-channel K step and
-// commits to the stage's mbarrier, so the next tap's gather overlaps the
-// MMAs.  The epilogue reads the accumulator with tcgen05.ld (warp w owns
+// weights are copied by the CTA's threads (cp.async, 16 bytes each, zero
+// filled outside the volume) into shared memory in the canonical no-swizzle
+// K-major layout (8-row x 16-byte core matrices: SBO = 128 bytes between
+// 8-row groups, LBO = rows x 16 bytes between 8-element K chunks), through a
+// ring of kStages stages, so the copies of the next kStages - 1 taps are in
+// flight while one elected thread issues tcgen05.mma.kind::f16 (BF16
+// operands, FP32 accumulator in tensor memory) per 16-channel K step of the
+// current tap and commits to the stage's mbarrier.  The epilogue reads the accumulator with tcgen05.ld (warp w owns
 // lanes 32w..32w+31 = voxels), adds the bias, applies ReLU if asked and
 // stores BF16 (and optionally FP32).
 //
@@ -31,6 +32,7 @@ namespace conv {
 
 constexpr int kTileM = 128;          // voxels per CTA (MMA M)
 constexpr int kThreads = 128;        // 4 warps: one TMEM lane quadrant each
+constexpr int kStages = 4;           // taps in the shared-memory ring
 constexpr long long kWaitLimit = 4000000000LL;  // ~2 s of clock64
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -72,6 +74,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
   while (!mbar_test(bar, parity))
     if (clock64() - t0 > kWaitLimit) return false;
   return true;
+}
+
+// 16-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -116,10 +129,10 @@ struct ConvArgs {
   int* error;                    // set to 1 when a wait gives up
 };
 
-// Bytes of dynamic shared memory for one launch (two stages of A and B).
+// Bytes of dynamic shared memory for one launch (kStages stages of A and B).
 __host__ __device__ inline int conv_smem_bytes(int cin, int cout) {
   const int a = kTileM * cin * 2, b = cout * cin * 2;
-  return 2 * (a + b) + 128;
+  return kStages * (a + b) + 128;
 }
 
 __host__ __device__ inline uint32_t tmem_columns(int cout) {
@@ -130,21 +143,19 @@ __host__ __device__ inline uint32_t tmem_columns(int cout) {
 
 __global__ void __launch_bounds__(kThreads) k_conv3d_tc(ConvArgs A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t bars[kStages];
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cin = A.cin, cout = A.cout;
   const int a_bytes = kTileM * cin * 2, b_bytes = cout * cin * 2;
-  unsigned char* stage_a[2] = {smem_raw, smem_raw + a_bytes + b_bytes};
-  unsigned char* stage_b[2] = {smem_raw + a_bytes, smem_raw + 2 * a_bytes + b_bytes};
+  const int stage_bytes = a_bytes + b_bytes;
   const uint32_t lbo_a = (kTileM / 8) * 128, lbo_b = (uint32_t)(cout / 8) * 128;
   const uint32_t ncols = tmem_columns(cout);
   const int64_t n = (int64_t)A.nx * A.ny * A.nz;
   const int64_t v0 = (int64_t)blockIdx.x * kTileM;
 
   if (tid == 0) {
-    mbar_init(&bars[0]);
-    mbar_init(&bars[1]);
+    for (int q = 0; q < kStages; ++q) mbar_init(&bars[q]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -168,51 +179,60 @@ __global__ void __launch_bounds__(kThreads) k_conv3d_tc(ConvArgs A) {
     vi = (int)(ij / A.ny);
   }
   const int kchunks = cin / 8;
+  // copies of tap t into its stage: the thread's A row and a share of B
+  auto issue = [&](int t) {
+    unsigned char* sa = smem_raw + (t % kStages) * stage_bytes;
+    unsigned char* sb = sa + a_bytes;
+    const int di = t / 9 - 1, dj = (t / 3) % 3 - 1, dk = t % 3 - 1;
+    const int ii = vi + di, jj = vj + dj, kk = vk + dk;
+    const bool in = v < n && ii >= 0 && ii < A.nx && jj >= 0 && jj < A.ny && kk >= 0 && kk < A.nz;
+    const __nv_bfloat16* src = in ? A.x + (((int64_t)ii * A.ny + jj) * A.nz + kk) * cin : A.x;
+    unsigned char* dst = sa + (tid >> 3) * 128 + (tid & 7) * 16;
+    for (int c = 0; c < kchunks; ++c) cp_async16(dst + c * lbo_a, src + (in ? c * 8 : 0), in ? 16 : 0);
+    for (int q = tid; q < cout * kchunks; q += kThreads) {
+      const int co = q / kchunks, c = q - co * kchunks;
+      cp_async16(sb + c * lbo_b + (co >> 3) * 128 + (co & 7) * 16, A.w + ((int64_t)co * 27 + t) * cin + c * 8, 16);
+    }
+  };
   const uint32_t idesc = idesc_bf16(kTileM, cout);
-  bool ok = true;
+  // prologue: taps 0 .. kStages - 2 in flight (one commit group per tap)
+  for (int t = 0; t < kStages - 1; ++t) {
+    issue(t);
+    cp_async_commit();
+  }
+  bool ok = true, good = true;
   for (int t = 0; t < 27; ++t) {
-    const int s = t & 1;
-    // the stage is free once the MMAs of tap t - 2 completed; the decision to
-    // give up is taken by the whole block, so no thread leaves the loop alone
-    const bool good = t < 2 || mbar_wait_bounded(&bars[s], (unsigned)(((t - 2) >> 1) & 1));
+    // this thread's copies of tap t have landed once at most kStages - 2
+    // newer groups are pending; the block decides together whether to go on
+    cp_async_wait<kStages - 2>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (!__syncthreads_and(good)) {
       ok = false;
       break;
     }
-    // A: row tid <- X[v + off(t)][0..cin)
-    {
-      const int di = t / 9 - 1, dj = (t / 3) % 3 - 1, dk = t % 3 - 1;
-      const int ii = vi + di, jj = vj + dj, kk = vk + dk;
-      const bool in = v < n && ii >= 0 && ii < A.nx && jj >= 0 && jj < A.ny && kk >= 0 && kk < A.nz;
-      const uint4* src = in ? reinterpret_cast<const uint4*>(A.x + (((int64_t)ii * A.ny + jj) * A.nz + kk) * cin)
-                            : nullptr;
-      unsigned char* dst = stage_a[s] + (tid >> 3) * 128 + (tid & 7) * 16;
-      for (int c = 0; c < kchunks; ++c) {
-        const uint4 val = in ? __ldg(src + c) : make_uint4(0u, 0u, 0u, 0u);
-        *reinterpret_cast<uint4*>(dst + c * lbo_a) = val;
-      }
-    }
-    // B: W[co][t][0..cin) for every co
-    for (int q = tid; q < cout * kchunks; q += kThreads) {
-      const int co = q / kchunks, c = q - co * kchunks;
-      const uint4 val = __ldg(reinterpret_cast<const uint4*>(A.w + ((int64_t)co * 27 + t) * cin) + c);
-      *reinterpret_cast<uint4*>(stage_b[s] + c * lbo_b + (co >> 3) * 128 + (co & 7) * 16) = val;
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t a0 = smem_u32(stage_a[s]), b0 = smem_u32(stage_b[s]);
+      const uint32_t a0 = smem_u32(smem_raw + (t % kStages) * stage_bytes);
+      const uint32_t b0 = a0 + a_bytes;
       for (int ks = 0; ks < cin / 16; ++ks) {
         const uint64_t ad = umma_desc(a0 + ks * 2 * lbo_a, lbo_a, 128);
         const uint64_t bd = umma_desc(b0 + ks * 2 * lbo_b, lbo_b, 128);
         tc_mma(tmem, ad, bd, idesc, (t > 0 || ks > 0) ? 1 : 0);
       }
-      tc_commit(&bars[s]);
+      tc_commit(&bars[t % kStages]);
     }
+    // refill the stage of tap t - 1 with tap t + kStages - 1 once the MMAs of
+    // tap t - 1 have read it
+    const int tn = t + kStages - 1;
+    if (tn < 27) {
+      if (t >= 1) good = mbar_wait_bounded(&bars[(t - 1) % kStages], (unsigned)(((t - 1) / kStages) & 1));
+      if (good) issue(tn);
+    }
+    cp_async_commit();  // one group per iteration, possibly empty
   }
+  cp_async_wait<0>();
   // the last commit covers every MMA issued before it
-  ok = __syncthreads_and(ok && mbar_wait_bounded(&bars[26 & 1], (unsigned)((26 >> 1) & 1)));
+  ok = __syncthreads_and(ok && mbar_wait_bounded(&bars[26 % kStages], (unsigned)((26 / kStages) & 1)));
   tc_fence_after();
   if (ok) {
     const int64_t vr = v0 + warp * 32 + lane;
@@ -243,8 +263,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3d_tc(ConvArgs A) {
   } else {
     if (tid == 0) atomicExch(A.error, 1);
     // drain: give the MMAs in flight a bounded chance to finish
-    mbar_wait_bounded(&bars[0], 0);
-    mbar_wait_bounded(&bars[1], 0);
+    for (int q = 0; q < kStages; ++q) mbar_wait_bounded(&bars[q], 0);
   }
   tc_fence_before();
   __syncthreads();

@@ -1173,18 +1173,22 @@ __global__ void k_set_defer(CgScalars* sc, int v) {
   if (threadIdx.x == 0) sc->defer_alpha = v;
 }
 
-// Learned preconditioner (code 4).  k_learned_sumsq reduces sum_fluid r^2 V
-// into sc->dot; k_learned_pack forms the network input (r over its
+// Learned preconditioner (codes 4 and 5): a two-level preconditioner whose
+// coarse correction is the network.  With r' = r - A z_pre after the
+// pre-smoothing sweeps, k_learned_sumsq reduces sum_fluid r'^2 V into
+// sc->dot; k_learned_pack forms the network input (r' over its
 // volume-weighted RMS, fluid mask, log2 cell widths over the finest width);
-// k_learned_unpack writes z = RMS * output channel 0 on the fluid cells and,
-// with the zero-mean projection, the z mean (as the Jacobi preconditioner).
-__global__ void __launch_bounds__(256) k_learned_sumsq(LevelDev L, const double* __restrict__ r, double* partials,
-                                                       CgScalars* sc) {
+// k_learned_unpack writes n = RMS * output channel 0 on the fluid cells and
+// reduces <r', n>_V; k_learned_combine adds s n to z_pre with the energy-
+// minimising scale s = <r', n>_V / <n, A n>_V (sc->dot holds the denominator).
+// az == nullptr means A z_pre = 0 (the network input of r itself).
+__global__ void __launch_bounds__(256) k_learned_sumsq(LevelDev L, const double* __restrict__ r,
+                                                       const double* __restrict__ az, double* partials, CgScalars* sc) {
   pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   double a = 0.0;
   if (active && (__ldg(L.mask + c) & M_FLUID)) {
-    const double rv = __ldg(r + c);
+    const double rv = __ldg(r + c) - (az != nullptr ? __ldg(az + c) : 0.0);
     a = rv * rv * vol64(L, i, j, k);
   }
   double v[1] = {a}, t[1];
@@ -1199,17 +1203,18 @@ __device__ __forceinline__ double learned_rms(const CgScalars* sc) {
 }
 
 __global__ void __launch_bounds__(256) k_learned_pack(LevelDev L, const double* __restrict__ r,
-                                                      __nv_bfloat16* __restrict__ in, float wx0, float wy0, float wz0,
-                                                      const CgScalars* sc) {
+                                                      const double* __restrict__ az, __nv_bfloat16* __restrict__ in,
+                                                      float wx0, float wy0, float wz0, const CgScalars* sc) {
   pdl_wait();
   EFSI_CELL_PROLOGUE(L)
   if (!active) return;
   const bool fluid = (__ldg(L.mask + c) & M_FLUID) != 0;
   const float inv = (float)(1.0 / learned_rms(sc));
+  const double rv = fluid ? __ldg(r + c) - (az != nullptr ? __ldg(az + c) : 0.0) : 0.0;
   float ch[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) ch[q] = 0.0f;
-  ch[0] = fluid ? (float)__ldg(r + c) * inv : 0.0f;
+  ch[0] = (float)rv * inv;
   ch[1] = fluid ? 1.0f : 0.0f;
   ch[2] = log2f(__ldg(L.wx + i) / wx0);
   ch[3] = log2f(__ldg(L.wy + j) / wy0);
@@ -1223,27 +1228,34 @@ __global__ void __launch_bounds__(256) k_learned_pack(LevelDev L, const double* 
 }
 
 __global__ void __launch_bounds__(256) k_learned_unpack(LevelDev L, const float* __restrict__ out,
-                                                        double* __restrict__ z, int want_mean, double* partials,
-                                                        CgScalars* sc) {
+                                                        const double* __restrict__ r, const double* __restrict__ az,
+                                                        double* __restrict__ n_out, double* partials, CgScalars* sc) {
   pdl_wait();
   EFSI_CELL_PROLOGUE(L)
-  double pz = 0.0;
+  double pn = 0.0;
   if (active) {
     const unsigned m = __ldg(L.mask + c);
-    double zv = 0.0;
-    if (m & M_FLUID) zv = (double)__ldg(out + c * 16) * learned_rms(sc);
-    z[c] = zv;
-    if (m & M_FLUID) pz = zv * vol64(L, i, j, k);
-  }
-  if (want_mean) {
-    double v[1] = {pz}, t[1];
-    if (grid_sum<1>(v, partials, &sc->ticket, t)) {
-      if (flat_tid() == 0) {
-        sc->mean_z = sc->free_vol > 0.0 ? 1.0 * t[0] / sc->free_vol : 0.0;
-        sc->zproj = 1;
-      }
+    double nv = 0.0;
+    if (m & M_FLUID) {
+      nv = (double)__ldg(out + c * 16) * learned_rms(sc);
+      pn = (__ldg(r + c) - __ldg(az + c)) * nv * vol64(L, i, j, k);
     }
+    n_out[c] = nv;
   }
+  double v[1] = {pn}, t[1];
+  if (grid_sum<1>(v, partials, &sc->ticket, t)) {
+    if (flat_tid() == 0) sc->learned_num = t[0];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_learned_combine(LevelDev L, const double* __restrict__ zpre,
+                                                         double* __restrict__ n_io, const CgScalars* sc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const double den = sc->dot, num = sc->learned_num;
+  const double s = (den > 0.0 && isfinite(den) && isfinite(num)) ? num / den : 0.0;
+  n_io[c] = __ldg(zpre + c) + s * n_io[c];
 }
 
 // fluid.py:4677-4693 with multiplier -1 on the level-0 rhs, plus the free
@@ -2410,15 +2422,35 @@ static int precondition(PcgRun& R) {
   const bool want_mean = R.prm->remove_mean != 0;
   R.dots_fused = false;
   if (R.learned) {
+    // two-level: two damped-Jacobi sweeps (the V-cycle's level-0 smoother)
+    // from zero, the network's correction of the remaining residual at its
+    // energy-minimising scale, two more sweeps
     efsi_fv_plan* P = R.P;
+    const int outlet = R.prm->outlet;
+    const double om = (double)0.8f;
+    const ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+    double* za = static_cast<double*>(P->lv[0].pa);
+    double* zb = static_cast<double*>(P->lv[0].pb);
     __nv_bfloat16* in = static_cast<__nv_bfloat16*>(P->unet_in);
-    EFSI_COUNTED launch_pdl(k_learned_sumsq, R.S.grid, R.S.block, 0, R.s, R.L, P->r, P->partials, P->sc);
-    EFSI_COUNTED launch_pdl(k_learned_pack, R.S.grid, R.S.block, 0, R.s, R.L, (const double*)P->r, in, P->unet_wmin[0],
-                            P->unet_wmin[1], P->unet_wmin[2], (const CgScalars*)P->sc);
+    launch_sweep<double, true, true>(P, 0, nullptr, P->r, za, outlet, om, none, nullptr, R.s);
+    launch_sweep<double, true, false>(P, 0, za, P->r, zb, outlet, om, none, nullptr, R.s);
+    EFSI_COUNTED k_fv_apply<<<R.S.grid, R.S.block, 0, R.s>>>(R.L, zb, P->Ad, outlet);
+    EFSI_COUNTED launch_pdl(k_learned_sumsq, R.S.grid, R.S.block, 0, R.s, R.L, (const double*)P->r,
+                            (const double*)P->Ad, P->partials, P->sc);
+    EFSI_COUNTED launch_pdl(k_learned_pack, R.S.grid, R.S.block, 0, R.s, R.L, (const double*)P->r,
+                            (const double*)P->Ad, in, P->unet_wmin[0], P->unet_wmin[1], P->unet_wmin[2],
+                            (const CgScalars*)P->sc);
     const float* out = nullptr;
     EFSI_TRY(unet_run(P->unet, P->lv[0].nx, P->lv[0].ny, P->lv[0].nz, in, &P->sc->fault, &out, R.s));
-    EFSI_COUNTED launch_pdl(k_learned_unpack, R.S.grid, R.S.block, 0, R.s, R.L, out, P->z, want_mean ? 1 : 0,
-                            P->partials, P->sc);
+    EFSI_COUNTED launch_pdl(k_learned_unpack, R.S.grid, R.S.block, 0, R.s, R.L, out, (const double*)P->r,
+                            (const double*)P->Ad, za, P->partials, P->sc);
+    EFSI_COUNTED k_fv_apply<<<R.S.grid, R.S.block, 0, R.s>>>(R.L, za, P->Ad, outlet);
+    EFSI_COUNTED k_weighted_dot<<<R.S.grid, R.S.block, 0, R.s>>>(R.L, za, P->Ad, P->partials, P->sc);
+    EFSI_COUNTED launch_pdl(k_learned_combine, R.S.grid, R.S.block, 0, R.s, R.L, (const double*)zb, za,
+                            (const CgScalars*)P->sc);
+    launch_sweep<double, true, false>(P, 0, za, P->r, zb, outlet, om, none, nullptr, R.s);
+    launch_sweep<double, true, false>(P, 0, zb, P->r, P->z, outlet, om, none, want_mean ? P->partials : nullptr,
+                                      R.s);
   } else if (R.use_mg) {
     // with the zero-mean projection the V-cycle's last sweep finishes the dots
     // (EFSI_SEPARATE_DOTS keeps them in their own kernel)
@@ -2758,15 +2790,15 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     st->host_residual_checks += 1;
     r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
     st->relative_residual = r_norm / b_norm;
+    if (R.learned) {
+      st->learned_iterations = it;
+      st->learned_relative_residual = st->relative_residual;
+    }
     if (st->relative_residual <= tol) {
       st->converged = 1;
       break;
     }
     const int code = P->host_sc->code;
-    if (R.learned) {
-      st->learned_iterations = it;
-      st->learned_relative_residual = st->relative_residual;
-    }
     if (R.learned && learned_fallback && it < max_iters &&
         (code != 0 || !(st->relative_residual <= kLearnedBlockReduction * learned_prev))) {
       // fallback: restart from the exact residual with the V-cycle
@@ -3232,9 +3264,23 @@ int efsi_fv_learned_input(efsi_fv_plan* P, const double* r, void* input, void* s
   const Shape3 S = P->lv[0].shape;
   // the free volume and r's RMS as the solve computes them
   EFSI_COUNTED k_rhs_mean<<<S.grid, S.block, 0, s>>>(L, r, 0.0, P->partials, P->sc);
-  EFSI_COUNTED k_learned_sumsq<<<S.grid, S.block, 0, s>>>(L, r, P->partials, P->sc);
-  EFSI_COUNTED k_learned_pack<<<S.grid, S.block, 0, s>>>(L, r, static_cast<__nv_bfloat16*>(input), P->unet_wmin[0],
-                                                         P->unet_wmin[1], P->unet_wmin[2], (const CgScalars*)P->sc);
+  EFSI_COUNTED k_learned_sumsq<<<S.grid, S.block, 0, s>>>(L, r, nullptr, P->partials, P->sc);
+  EFSI_COUNTED k_learned_pack<<<S.grid, S.block, 0, s>>>(L, r, nullptr, static_cast<__nv_bfloat16*>(input),
+                                                         P->unet_wmin[0], P->unet_wmin[1], P->unet_wmin[2],
+                                                         (const CgScalars*)P->sc);
+  EFSI_LAUNCH_CHECK();
+  return EFSI_OK;
+}
+
+int efsi_fv_learned_presmooth(efsi_fv_plan* P, const double* r, double* z, int32_t outlet, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(r != nullptr && z != nullptr, "null argument");
+  cudaStream_t s = as_stream(stream);
+  const ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+  const double om = (double)0.8f;
+  double* za = static_cast<double*>(P->lv[0].pa);
+  launch_sweep<double, true, true>(P, 0, nullptr, r, za, outlet, om, none, nullptr, s);
+  launch_sweep<double, true, false>(P, 0, za, r, z, outlet, om, none, nullptr, s);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }

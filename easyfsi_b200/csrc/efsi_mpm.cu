@@ -254,13 +254,21 @@ __global__ void k_bin_keys(efsi_mpm_state S, int tx, int ty, int tz, int ntiles,
 }
 
 // Exclusive scan of count[0..n) into offset[0..n] by one 1024-thread block.
+// Each thread owns a run of `per` (a multiple of 4) consecutive counts, read
+// and written as int4 (the runs start on 16-byte boundaries; count, offset
+// and cursor are cudaMalloc'd), so the block issues all its loads at once.
 __global__ void k_scan(const int32_t* count, int n, int32_t* offset, int32_t* cursor) {
   __shared__ int32_t part[1024];
   const int t = threadIdx.x;
-  const int per = (n + 1023) / 1024;
-  const int lo = t * per, hi = min(n, lo + per);
+  const int per = (((n + 1023) / 1024) + 3) & ~3;
+  const int lo = min(n, t * per), hi = min(n, lo + per);
   int32_t s = 0;
-  for (int q = lo; q < hi; ++q) s += count[q];
+  int q = lo;
+  for (; q + 4 <= hi; q += 4) {
+    const int4 c4 = *reinterpret_cast<const int4*>(count + q);
+    s += c4.x + c4.y + c4.z + c4.w;
+  }
+  for (; q < hi; ++q) s += count[q];
   part[t] = s;
   __syncthreads();
   for (int o = 1; o < 1024; o <<= 1) {
@@ -270,7 +278,19 @@ __global__ void k_scan(const int32_t* count, int n, int32_t* offset, int32_t* cu
     __syncthreads();
   }
   int32_t run = part[t] - s;
-  for (int q = lo; q < hi; ++q) {
+  q = lo;
+  for (; q + 4 <= hi; q += 4) {
+    const int4 c4 = *reinterpret_cast<const int4*>(count + q);
+    int4 o4;
+    o4.x = run;
+    o4.y = run + c4.x;
+    o4.z = o4.y + c4.y;
+    o4.w = o4.z + c4.z;
+    run = o4.w + c4.w;
+    *reinterpret_cast<int4*>(offset + q) = o4;
+    *reinterpret_cast<int4*>(cursor + q) = make_int4(0, 0, 0, 0);
+  }
+  for (; q < hi; ++q) {
     offset[q] = run;
     cursor[q] = 0;
     run += count[q];
@@ -891,7 +911,6 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
   EFSI_ARG_CHECK(S.nx == P->nx && S.ny == P->ny && S.nz == P->nz, "MPM state grid does not match the plan");
   EFSI_ARG_CHECK(S.particle_count > 0 && S.particle_count <= P->capacity, "particle_count out of range");
   cudaStream_t s = as_stream(stream);
-  const int64_t G = (int64_t)S.nx * S.ny * S.nz;
   const int Pn = S.particle_count;
   double* acc = report_device != nullptr ? P->acc : nullptr;
   // algorithmic bytes of the substep: 216 per particle (read x, v, C, F, mass,

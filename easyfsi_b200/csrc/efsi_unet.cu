@@ -291,10 +291,6 @@ __global__ void k_loss(int64_t n, const float* __restrict__ out, const float* __
   if (threadIdx.x == 0) atomicAdd(loss, a[0] * (double)inv_count);
 }
 
-__global__ void k_f32_to_bf16(int64_t n, const float* __restrict__ a, bf16* __restrict__ b) {
-  UNET_STRIDE(q, n) b[q] = __float2bfloat16_rn(a[q]);
-}
-
 #undef UNET_STRIDE
 
 unsigned grid_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
@@ -424,9 +420,10 @@ int set_kernel_attributes() {
 int conv_launch(const Dims& d, int cin, int cout, const bf16* x, const bf16* w, const float* bias, int relu, bf16* y,
                 float* yf, int* error, cudaStream_t s) {
   conv::ConvArgs A{d.nx, d.ny, d.nz, cin, cout, x, w, bias, relu, y, yf, error};
-  // at least ~57 KB of shared memory per CTA, so that at most three CTAs
-  // (3 x 128 tensor-memory columns) share an SM
-  const int smem = std::max(conv::conv_smem_bytes(cin, cout), 58 * 1024);
+  // enough shared memory per CTA that the CTAs resident on an SM never ask for
+  // more than its 512 tensor-memory columns
+  const int per_sm = 512 / (int)conv::tmem_columns(cout);
+  const int smem = std::max(conv::conv_smem_bytes(cin, cout), 228 * 1024 / per_sm + 1024);
   EFSI_TRY(set_kernel_attributes());
   const unsigned blocks = (unsigned)((d.n() + conv::kTileM - 1) / conv::kTileM);
   EFSI_COUNTED conv::k_conv3d_tc<<<blocks, conv::kThreads, smem, s>>>(A);

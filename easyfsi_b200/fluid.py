@@ -469,9 +469,12 @@ class CartesianFluidSolver:
     def set_learned_preconditioner(self, network) -> None:
         """Attaches a trained ``easyfsi_b200.learned.UNetPreconditioner`` as
         ``cg_preconditioner="learned"`` (no counterpart in the reference):
-        z = network(r) inside the flexible PCG, with the multigrid V-cycle
-        taking over when a 16-iteration block does not halve the residual.
-        ``None`` detaches it."""
+        inside the flexible PCG the network is the coarse correction of a
+        two-level preconditioner (two damped-Jacobi sweeps, the network's
+        correction at its energy-minimising scale, two sweeps), with the
+        multigrid V-cycle taking over when a 16-iteration block does not halve
+        the residual (``"learned_no_fallback"`` runs it alone).  ``None``
+        detaches it."""
         self._refresh_structure()
         handle = None if network is None else network.handle
         _native.call("efsi_fv_set_learned_preconditioner", self._plan, handle, _stream())

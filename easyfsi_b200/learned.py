@@ -6,18 +6,27 @@ parameters, BF16 activations and weights with FP32 accumulation on the tensor
 cores, FP32 master weights and Adam).  It is trained on (residual, error)
 pairs that the solver's own multigrid-preconditioned CG produces, and is then
 attached to a ``CartesianFluidSolver`` as ``cg_preconditioner="learned"``.
-The flexible PCG of the reference (fluid.py:6535-6811) runs with z =
-network(r); the 2/24/2 V-cycle takes over whenever a 16-iteration block does
-not halve the residual, and every solve ends on the same true-residual test
-as the plain method.
+
+Inside the flexible PCG of the reference (fluid.py:6535-6811) the network is
+the coarse correction of a two-level preconditioner: two damped-Jacobi sweeps
+of the V-cycle's level-0 smoother from zero (z_pre), the network's estimate n
+of the error that remains, added at the scale that minimises the energy norm
+of the error (s = <r', n>_V / <n, A n>_V with r' = r - A z_pre), and two more
+sweeps.  The sweeps remove the rough error the network leaves; the network
+removes the smooth error the sweeps cannot.  The 2/24/2 V-cycle takes over
+whenever a 16-iteration block does not halve the residual, and every solve
+ends on the same true-residual test as the plain method.
 
 Pairs (``harvest_pairs``): for a prepared right-hand side b, the multigrid
 PCG is run to convergence (x*) and, from zero, truncated after k iterations
 (x_k; k = 0 gives r = b, e = x*); r_k = b - A x_k and e_k = x* - x_k (both
-with the closed-domain mean removed) satisfy A e_k = r_k.  The network input is the solver's own encoding
-of r_k (``efsi_fv_learned_input``: r over its volume-weighted RMS, the fluid
-mask, log2 cell widths); the target is e_k over its RMS, since the flexible
-PCG is invariant to the scale of z.  Training takes random crops of the pairs.
+with the closed-domain mean removed) satisfy A e_k = r_k.  The pre-smoothing
+z_pre of r_k is subtracted as inside the PCG: the pair is (r_k - A z_pre,
+e_k - z_pre).  The network input is the solver's own encoding of that
+residual (``efsi_fv_learned_input``: r over its volume-weighted RMS, the
+fluid mask, log2 cell widths); the target is the error over its RMS (the
+energy-minimising scale makes the correction independent of the output's
+scale).  Training takes random crops of the pairs.
 """
 
 from __future__ import annotations
@@ -158,8 +167,12 @@ class UNetPreconditioner:
 def harvest_pairs(solver, *, rhs_scale: float, truncations=(0, 1, 2, 4, 8, 16, 32), tolerance: float = 1.0e-10,
                   max_iterations: int = 400) -> list[TrainingPair]:
     """(residual, error) pairs from the solver's own MG-PCG on the system of
-    its current divergence (closed domain, zero-mean pressure).  The network
-    must already be attached (its input encoding uses the finest widths)."""
+    its current divergence (closed domain, zero-mean pressure): for every
+    truncated iterate x_k, the residual r_k = b - A x_k and error x* - x_k
+    minus the learned preconditioner's pre-smoothing z_pre of r_k, i.e. the
+    residual r_k - A z_pre and error x* - x_k - z_pre that its network
+    corrects.  The network must already be attached (its input encoding uses
+    the finest widths)."""
     fl = solver
     saved = fl.pressure.tensor.clone()
     try:
@@ -185,8 +198,16 @@ def harvest_pairs(solver, *, rhs_scale: float, truncations=(0, 1, 2, 4, 8, 16, 3
                                                  tolerance=0.0, preconditioner="fv_multigrid")
             x_k = fl.pressure.tensor.clone()
             fl._fv_laplacian_apply_kernel(fl.pressure, fl.cg_Ad, 0)
-            r = zero_mean(b - fl.cg_Ad.tensor)
-            e = zero_mean(x_star - x_k)
+            r_k = zero_mean(b - fl.cg_Ad.tensor).contiguous()
+            # what the network sees inside the PCG: the residual and error left
+            # after the pre-smoothing sweeps
+            z_pre = torch.zeros_like(r_k)
+            _native.call("efsi_fv_learned_presmooth", fl._plan, c_void_p(r_k.data_ptr()), c_void_p(z_pre.data_ptr()),
+                         0, _stream())
+            az = torch.zeros_like(r_k)
+            _native.call("efsi_fv_apply", fl._plan, c_void_p(z_pre.data_ptr()), c_void_p(az.data_ptr()), 0, _stream())
+            r = zero_mean(r_k - az)
+            e = zero_mean(x_star - x_k - z_pre)
             rms_e = float(torch.sqrt((e * e * vol * fluid).sum() / max(fvol, 1e-300)))
             if not np.isfinite(rms_e) or rms_e <= 0.0:
                 continue
@@ -206,9 +227,9 @@ def _demo(argv=None) -> None:
 
         python -m easyfsi_b200.learned [--nodes 96 96 96] [--steps 200]
 
-    prints one JSON line with the training loss, and ms / iterations of the
-    MG-PCG, the learned PCG (with fallback) and the network alone over a
-    fixed budget of 48 iterations."""
+    prints one JSON line with the training loss, and ms / iterations to the
+    relative residual 1e-8 of the MG-PCG, the Jacobi-PCG, the learned PCG
+    with the V-cycle fallback and without it."""
     import argparse
     import json
     import time
@@ -243,7 +264,7 @@ def _demo(argv=None) -> None:
     fl.divergence.from_numpy(rng.normal(size=nodes).astype(np.float32))
     out = {"nodes": list(nodes), "parameters": net.param_count, "train_s": train_s,
            "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-10:]))}
-    for name, iters in (("fv_multigrid", 400), ("learned", 400), ("learned_no_fallback", 48)):
+    for name, iters in (("fv_multigrid", 400), ("jacobi", 4000), ("learned", 400), ("learned_no_fallback", 4000)):
         for rep in range(2):
             fl.pressure.tensor.zero_()
             torch.cuda.synchronize()

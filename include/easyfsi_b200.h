@@ -158,9 +158,11 @@ typedef struct efsi_pcg_params {
   int32_t precond;      /* 0 jacobi, 1 fv_multigrid (2/24/2), 2 fv_multigrid_light (1/12/1),
                            3 fv_multigrid_mixed: the 2/24/2 V-cycle with FP32 level-0 iterates and
                            arithmetic (no reference counterpart; the CG stays FP64),
-                           4 learned: the network attached by efsi_fv_set_learned_preconditioner,
-                           falling back to the 2/24/2 V-cycle (no reference counterpart),
-                           5 the same network without the fallback (measurement of the network alone) */
+                           4 learned: two-level, with the network attached by
+                           efsi_fv_set_learned_preconditioner as the coarse correction between two
+                           damped-Jacobi sweeps on each side, falling back to the 2/24/2 V-cycle
+                           (no reference counterpart),
+                           5 the same without the fallback (measurement of the learned preconditioner alone) */
   int32_t remove_mean;  /* closed-domain zero-mean projection */
   int32_t outlet;       /* pressure_outlet_zmin */
   int32_t iface_active; /* interface terms present: MG disabled, restart every 256 */
@@ -544,6 +546,12 @@ int efsi_outlet_reachability(efsi_reach_plan* plan, int32_t nx, int32_t ny, int3
                              int32_t barrier_code, int32_t update_barrier, int32_t* reachable, int32_t* label,
                              efsi_reach_report* report, void* stream);
 
+/* Zeroes `count` (<= 64) device buffers of bytes[q] bytes (multiples of 4)
+ * in one launch: the per-solve clears of the multigrid work fields of
+ * fluid.py:5228-5260 _prepare_fv_multigrid_rhs.  ptrs and bytes are host
+ * arrays. */
+int efsi_zero_buffers(int32_t count, void* const* ptrs, const int64_t* bytes, void* stream);
+
 /* fluid.py:4345-4456, the interface-coupling terms of _fv_laplacian_apply_kernel
  * (row list, or per-cell slots when the row count is 0): installs them in the
  * plan's level-0 operator (efsi_fv_apply, the PCG and the BiCGSTAB fallback).
@@ -609,17 +617,27 @@ int efsi_unet_zero_grad(efsi_unet* net, void* stream);
 /* One Adam step on the accumulated gradients (which it clears). */
 int efsi_unet_adam_step(efsi_unet* net, float lr, float beta1, float beta2, float eps, void* stream);
 
-/* Attaches a network to a solver plan as preconditioner code 4 of
- * efsi_fv_pcg_solve (NULL detaches): z = net(r) inside the flexible PCG, with
- * the multigrid V-cycle taking over when a 16-iteration block does not reduce
- * the residual.  Allocates the network's workspace for level 0 (call before
- * any stream capture); synchronises. */
+/* Attaches a network to a solver plan as preconditioner codes 4 and 5 of
+ * efsi_fv_pcg_solve (NULL detaches).  Inside the flexible PCG, z is: z_pre =
+ * two damped-Jacobi sweeps (the V-cycle's level-0 smoother) on A z = r from
+ * zero; r' = r - A z_pre; n = RMS(r') net(r')[0]; z_c = z_pre + s n with
+ * s = <r', n>_V / <n, A n>_V (the energy-minimising scale; 0 when <n, A n>_V
+ * is not positive); z = two more sweeps from z_c.  With code 4 the multigrid
+ * V-cycle takes over when a 16-iteration block does not halve the residual.
+ * Allocates the network's workspace for level 0 (call before any stream
+ * capture); synchronises. */
 int efsi_fv_set_learned_preconditioner(efsi_fv_plan* plan, efsi_unet* net, void* stream);
 
 /* The network input of the plan's level 0 for residual r (f64): channel 0 r
  * scaled to unit volume-weighted RMS over the fluid cells, 1 the fluid mask,
  * 2-4 log2 of the cell widths over the finest width of each axis (BF16 [n][16]). */
 int efsi_fv_learned_input(efsi_fv_plan* plan, const double* r, void* input, void* stream);
+
+/* z = the learned preconditioner's pre-smoothing of r: two damped-Jacobi
+ * sweeps of the plan's level 0 on A z = r from zero (training pairs are
+ * formed from the residual and error that remain after it).  No reference
+ * counterpart. */
+int efsi_fv_learned_presmooth(efsi_fv_plan* plan, const double* r, double* z, int32_t outlet, void* stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -144,11 +144,11 @@ def _solve(fl, div, precond, iterations=2000):
 
 def test_learned_preconditioner_trains_and_reduces_iterations():
     """Pairs harvested from the solver's own MG-PCG, training on crops, then a
-    new right-hand side.  The network alone (no fallback) inside the flexible
-    PCG, after a fixed budget of 64 iterations, leaves a smaller residual than
-    the same PCG without it (Jacobi) and than the same network untrained; with
-    the V-cycle fallback the learned solve reaches the relative residual 1e-8
-    in fewer iterations than Jacobi-PCG.  The training loss falls."""
+    new right-hand side, solved to the relative residual 1e-8.  The trained
+    two-level preconditioner alone (no fallback) takes fewer iterations than
+    the same preconditioner with an untrained network (the sweeps alone, in
+    effect) and than Jacobi-PCG, the method without it; with the V-cycle
+    fallback it also converges.  The training loss falls."""
     from easyfsi_b200.learned import UNetPreconditioner, harvest_pairs
 
     nodes = (32, 32, 40)
@@ -167,19 +167,15 @@ def test_learned_preconditioner_trains_and_reduces_iterations():
     assert last < 0.7 * first
 
     div = rng.normal(size=nodes).astype(np.float32)
-    budget = {"jacobi": _solve(fl, div, "jacobi", iterations=64),
-              "trained": _solve(fl, div, "learned_no_fallback", iterations=64)}
+    res = {"jacobi": _solve(fl, div, "jacobi"), "fv_multigrid": _solve(fl, div, "fv_multigrid"),
+           "trained": _solve(fl, div, "learned_no_fallback"), "learned": _solve(fl, div, "learned")}
     fl.set_learned_preconditioner(untrained)
-    budget["untrained"] = _solve(fl, div, "learned_no_fallback", iterations=64)
+    res["untrained"] = _solve(fl, div, "learned_no_fallback")
     fl.set_learned_preconditioner(net)
-    print("residual after 64 iterations:", {k: v["residual"] for k, v in budget.items()})
-    assert budget["trained"]["residual"] < budget["jacobi"]["residual"]
-    assert budget["trained"]["residual"] < budget["untrained"]["residual"]
-
-    full = {"jacobi": _solve(fl, div, "jacobi"), "fv_multigrid": _solve(fl, div, "fv_multigrid"),
-            "learned": _solve(fl, div, "learned")}
-    print("solves to 1e-8:", full)
-    for name, r in full.items():
+    print("solves to 1e-8:", res)
+    for name, r in res.items():
         assert r["converged"] and r["residual"] <= 1e-8, name
-    assert full["learned"]["iterations"] < full["jacobi"]["iterations"]
-    assert full["learned"]["learned_iterations"] > 0
+    assert res["trained"]["iterations"] < res["untrained"]["iterations"]
+    assert res["trained"]["iterations"] < res["jacobi"]["iterations"]
+    assert res["trained"]["learned_iterations"] == res["trained"]["iterations"]
+    assert res["learned"]["learned_iterations"] > 0
