@@ -844,9 +844,8 @@ __device__ void tail_restrict(const TailDesc& T, int l, const TailTables& tb, co
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
-  pdl_wait();
-  extern __shared__ __align__(16) unsigned char tail_smem[];
+// The whole tail V-cycle by one CTA (all threads of the block take part).
+__device__ void tail_body(const TailDesc& T, unsigned char* tail_smem) {
   float* fpool = reinterpret_cast<float*>(tail_smem);
   // row tables and masks of every tail level, the rhs of level lt
   for (int l = T.lt; l < T.nl; ++l) tail_build_tables(T, l, tail_smem, tail_smem + T.moff[l]);
@@ -907,6 +906,229 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
     for (int t = threadIdx.x; t < n; t += blockDim.x) T.p_out[t] = res[t];
   }
 }
+
+__global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
+  pdl_wait();
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  tail_body(T, tail_smem);
+}
+
+// ---------------------------------------------------------------------------
+// Coarse levels 1 .. lt-1 and the tail in one cooperative launch.  The blocks
+// of the grid share the cells of each phase (grid-stride); a grid barrier
+// separates the phases.  Per V-cycle this replaces the per-level launches
+// (3 + 2 per level: the pre-sweeps, the restriction and the post-sweeps) and
+// the tail launch by one launch and its barriers.  The arithmetic is that of
+// k_sweep / k_restrict / k_prolong (and so of the plane-marching kernels):
+// the same `stencil` rows in the same order.  Fields written inside the
+// launch are read with plain (coherent) loads, never through the read-only
+// path.  Phases:
+//   level 1: the zero-guess sweep, the other pre-sweeps;
+//   level l: the restriction into l+1 fused with the zero-guess sweep of
+//            l+1 (it only needs the cell's own rhs), the other pre-sweeps;
+//   the tail (block 0);
+//   level l = lt-1 .. 1: the prolongation-fused first post-sweep, the others.
+// Every barrier wait is bounded; a block that gives up sets the fault flag,
+// and every block returns at the next barrier that sees the flag.
+// ---------------------------------------------------------------------------
+struct CoarseDesc {
+  TailDesc T;  // T.L[l] for every level l >= 1; the tail of levels lt..nl-1
+  float* pa[kTailMaxLevels];
+  float* pb[kTailMaxLevels];
+  float* rhs[kTailMaxLevels];
+  unsigned* bar;  // [0] arrivals, [1] generation
+  int* fault;
+};
+
+constexpr long long kCoarseWaitLimit = 4000000000LL;  // ~2 s of clock64
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ bool coarse_barrier(const CoarseDesc& D) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    unsigned* count = D.bar;
+    unsigned* gen = D.bar + 1;
+    const unsigned g = ld_acquire_u32(gen);
+    __threadfence();
+    if (atomicAdd(count, 1u) == gridDim.x - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (ld_acquire_u32(gen) == g) {
+        if (clock64() - t0 > kCoarseWaitLimit) {
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    if (!ok) atomicExch(D.fault, 1);
+    if (*reinterpret_cast<volatile int*>(D.fault) != 0) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// fused_iterate<float> with plain loads
+__device__ __forceinline__ double pk_iterate(const float* p, const ProlongSrc& pr, int64_t cell, int ii, int jj, int kk,
+                                             bool fluid) {
+  float v = p[cell];
+  if (pr.pc != nullptr && fluid) {
+    const int ci = min(ii / 2, pr.cnx - 1), cj = min(jj / 2, pr.cny - 1), ck = min(kk / 2, pr.cnz - 1);
+    v = __fadd_rn(v, __fmul_rn(pr.scale, pr.pc[cidx(ci, cj, ck, pr.cny, pr.cnz)]));
+  }
+  return (double)v;
+}
+
+// One cell of the damped-Jacobi sweep of k_sweep<float, false, kZero>.
+template <bool kZero>
+__device__ __forceinline__ float pk_sweep_cell(const LevelDev& L, const float* p, double rhs_v, int outlet,
+                                               double omega, const ProlongSrc& pr, int i, int j, int k, int64_t c,
+                                               unsigned m) {
+  if (m & M_SOLID) return 0.0f;
+  double ns, den;
+  if (kZero) {
+    auto zero = [](int64_t, int, int, int) { return 0.0; };
+    stencil(L, zero, i, j, k, c, m, outlet, ns, den);
+  } else {
+    auto val = [&](int64_t cell, int ii, int jj, int kk) { return pk_iterate(p, pr, cell, ii, jj, kk, true); };
+    stencil(L, val, i, j, k, c, m, outlet, ns, den);
+  }
+  den += iface_at<float>(L, c);
+  if (den <= 0.0) return 0.0f;
+  const double jv = (ns - rhs_v) / den;
+  const double pc = kZero ? 0.0 : pk_iterate(p, pr, c, i, j, k, (m & M_FLUID) != 0);
+  return (float)(pc + omega * (jv - pc));
+}
+
+// row_residual<float, false> with plain loads
+__device__ __forceinline__ float pk_residual(const LevelDev& L, const float* p, const float* rhs, int i, int j, int k,
+                                             int64_t c, unsigned m, int outlet) {
+  if (m & M_SOLID) return 0.0f;
+  double ns, den;
+  auto val = [&](int64_t cell, int, int, int) { return (double)p[cell]; };
+  stencil(L, val, i, j, k, c, m, outlet, ns, den);
+  den += iface_at<float>(L, c);
+  const double applied = ns - den * (double)p[c];
+  return (float)((double)rhs[c] - applied);
+}
+
+// k_restrict<float, false, true> of coarse cell (i, j, k)
+__device__ __forceinline__ float pk_restrict_cell(const LevelDev& F, const float* p, const float* rhs, int outlet,
+                                                  int i, int j, int k) {
+  float wres = 0.0f, free_vol = 0.0f;
+  int ocount = 0;
+#pragma unroll
+  for (int oi = 0; oi < 2; ++oi)
+#pragma unroll
+    for (int oj = 0; oj < 2; ++oj)
+#pragma unroll
+      for (int ok = 0; ok < 2; ++ok) {
+        const int fi = 2 * i + oi, fj = 2 * j + oj, fk = 2 * k + ok;
+        if (fi < F.nx && fj < F.ny && fk < F.nz) {
+          const int64_t f = cidx(fi, fj, fk, F.ny, F.nz);
+          const unsigned m = __ldg(F.mask + f);
+          if (m & M_SOLID) {
+            ocount += 1;
+          } else {
+            const float vol = __fmul_rn(__fmul_rn(__ldg(F.wx + fi), __ldg(F.wy + fj)), __ldg(F.wz + fk));
+            const float r = pk_residual(F, p, rhs, fi, fj, fk, f, m, outlet);
+            wres = __fadd_rn(wres, __fmul_rn(r, vol));
+            free_vol = __fadd_rn(free_vol, vol);
+          }
+        }
+      }
+  return ocount > 0 ? 0.0f : __fdiv_rn(wres, fmaxf(free_vol, 1.0e-30f));
+}
+
+__device__ __forceinline__ void pk_ijk(const LevelDev& L, int64_t t, int& i, int& j, int& k) {
+  k = (int)(t % L.nz);
+  const int64_t ij = t / L.nz;
+  j = (int)(ij % L.ny);
+  i = (int)(ij / L.ny);
+}
+
+#define PK_CELLS(L, t)                                                                    \
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x,                        \
+               t##_n = (int64_t)(L).nx * (L).ny * (L).nz;                                 \
+       t < t##_n; t += (int64_t)gridDim.x * blockDim.x)
+
+// One sweep of level l from `src` (null: zero guess) into `dst`.
+__device__ void pk_sweep(const LevelDev& L, const float* src, const float* rhs, float* dst, int outlet, double omega,
+                         const ProlongSrc& pr) {
+  PK_CELLS(L, t) {
+    int i, j, k;
+    pk_ijk(L, t, i, j, k);
+    const unsigned m = __ldg(L.mask + t);
+    dst[t] = src == nullptr ? pk_sweep_cell<true>(L, nullptr, (double)rhs[t], outlet, omega, pr, i, j, k, t, m)
+                            : pk_sweep_cell<false>(L, src, (double)rhs[t], outlet, omega, pr, i, j, k, t, m);
+  }
+}
+
+__global__ void __launch_bounds__(kTailThreads) k_mg_coarse(const __grid_constant__ CoarseDesc D) {
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  const TailDesc& T = D.T;
+  const int lt = T.lt;
+  const ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+  int cur[kTailMaxLevels];
+  // down
+  for (int l = 1; l < lt; ++l) {
+    const LevelDev& L = T.L[l];
+    float* buf[2] = {D.pa[l], D.pb[l]};
+    if (l == 1) pk_sweep(L, nullptr, D.rhs[1], buf[0], T.outlet, T.omega, none);
+    int c = 0;
+    for (int it = 1; it < T.pre; ++it) {
+      if (!coarse_barrier(D)) return;
+      pk_sweep(L, buf[c], D.rhs[l], buf[1 - c], T.outlet, T.omega, none);
+      c = 1 - c;
+    }
+    cur[l] = c;
+    if (!coarse_barrier(D)) return;
+    const LevelDev& C = T.L[l + 1];
+    const bool fuse0 = l + 1 < lt;
+    PK_CELLS(C, t) {
+      int i, j, k;
+      pk_ijk(C, t, i, j, k);
+      const float v = pk_restrict_cell(L, buf[c], D.rhs[l], T.outlet, i, j, k);
+      D.rhs[l + 1][t] = v;
+      if (fuse0)
+        D.pa[l + 1][t] = pk_sweep_cell<true>(C, nullptr, (double)v, T.outlet, T.omega, none, i, j, k, t,
+                                             __ldg(C.mask + t));
+    }
+  }
+  if (!coarse_barrier(D)) return;
+  if (blockIdx.x == 0) tail_body(T, tail_smem);
+  if (!coarse_barrier(D)) return;
+  // up
+  const float* fin = T.p_out;  // final iterate of level l + 1
+  for (int l = lt - 1; l >= 1; --l) {
+    const LevelDev& L = T.L[l];
+    const LevelDev& C = T.L[l + 1];
+    const ProlongSrc pr{fin, C.nx, C.ny, C.nz, T.scale};
+    float* buf[2] = {D.pa[l], D.pb[l]};
+    const int c = cur[l];
+    float* seq[2] = {buf[1 - c], buf[c]};
+    const float* src = buf[c];
+    for (int it = 0; it < T.post; ++it) {
+      if (it > 0 && !coarse_barrier(D)) return;
+      pk_sweep(L, src, D.rhs[l], seq[it & 1], T.outlet, T.omega, it == 0 ? pr : none);
+      src = seq[it & 1];
+    }
+    fin = src;
+    if (l > 1 && !coarse_barrier(D)) return;
+  }
+}
+#undef PK_CELLS
 
 // ---------------------------------------------------------------------------
 // Level-0 CG kernels (f64)
@@ -1634,6 +1856,41 @@ static void configure_tail(efsi_fv_plan* P) {
     return;
   }
 }
+
+// The cooperative coarse-level kernel runs levels 1 .. lt-1 and the tail when
+// the tail exists and starts at level 2 or deeper, cooperative launches are
+// supported, and EFSI_NO_COARSE_KERNEL is unset: as many blocks as fit on the
+// GPU at once (at most two per SM), each with the tail's shared memory.
+static void configure_coarse(efsi_fv_plan* P) {
+  P->coarse_blocks = 0;
+  const bool off = std::getenv("EFSI_NO_COARSE_KERNEL") != nullptr;
+  if (off || P->tail_level < 2 || P->tail_level >= P->n_levels) return;
+  int dev = 0, coop = 0, sms = 0, smem_optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (!coop || sms <= 0) return;
+  if (cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_coarse, kTailThreads, P->tail_smem_bytes) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return;
+  }
+  if (cudaMalloc(&P->coarse_bar, 2 * sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(P->coarse_bar, 0, 2 * sizeof(unsigned)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(P->coarse_bar);
+    P->coarse_bar = nullptr;
+    return;
+  }
+  P->coarse_blocks = std::min(per_sm, 2) * sms;
+}
 }  // namespace efsi
 
 using namespace efsi;
@@ -1769,6 +2026,7 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
   }
   preload_kernels();
   configure_tail(P);
+  configure_coarse(P);
   if (cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
     set_error("cannot create the capture stream");
     return fail(EFSI_ERR_CUDA);
@@ -1808,6 +2066,7 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   cudaFree(P->aux);
   cudaFree(P->bicg_work);
   cudaFree(P->unet_in);
+  cudaFree(P->coarse_bar);
   cudaFree(P->cpl_rows);
   cudaFree(P->cpl_ptr);
   cudaFree(P->cpl_src);
@@ -2249,8 +2508,10 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
   // Down: the iterate after pre-smoothing of level l lives in cur[l].  Levels
   // from P->tail_level on run inside k_mg_tail.
   const int lt = P->tail_level;
+  // levels 1 .. lt-1 and the tail in one cooperative launch (k_mg_coarse)
+  const bool coarse_kernel = P->coarse_blocks > 0 && lt >= 2 && lt < nl;
   std::vector<const void*> cur(nl, nullptr);
-  const int down_end = (lt < nl) ? lt : nl - 1;
+  const int down_end = coarse_kernel ? 1 : (lt < nl) ? lt : nl - 1;
   for (int l = 0; l < down_end; ++l) {
     LevelDev L = level_dev(P, l);
     LevelBuf& B = P->lv[l];
@@ -2296,7 +2557,8 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       launch_restrict<float, false>(P, l, (const float*)c, B.rhs, outlet, s);
   }
   if (lt < nl) {
-    TailDesc T;
+    CoarseDesc D;
+    TailDesc& T = D.T;
     T.lt = lt;
     T.nl = nl;
     T.outlet = outlet;
@@ -2314,8 +2576,36 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     }
     T.rhs_in = P->lv[lt].rhs;
     T.p_out = (float*)P->lv[lt].pa;
-    EFSI_COUNTED launch_pdl(k_mg_tail, 1, kTailThreads, P->tail_smem_bytes, s, T);
-    cur[lt] = P->lv[lt].pa;
+    if (coarse_kernel) {
+      for (int l = 1; l < nl; ++l) {
+        T.L[l] = level_dev(P, l);
+        D.pa[l] = (float*)P->lv[l].pa;
+        D.pb[l] = (float*)P->lv[l].pb;
+        D.rhs[l] = P->lv[l].rhs;
+      }
+      D.bar = P->coarse_bar;
+      D.fault = &P->sc->fault;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)P->coarse_blocks);
+      cfg.blockDim = dim3(kTailThreads);
+      cfg.dynamicSmemBytes = P->tail_smem_bytes;
+      cfg.stream = s;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      EFSI_COUNTED cudaLaunchKernelEx(&cfg, k_mg_coarse, D);
+      // the kernel's final level-1 iterate: the pre-sweeps end in buffer
+      // (pre - 1) & 1, the post-sweeps alternate from the other one
+      const int c = (pre - 1) & 1;
+      void* bufs1[2] = {P->lv[1].pa, P->lv[1].pb};
+      void* seq1[2] = {bufs1[1 - c], bufs1[c]};
+      cur[1] = seq1[(post - 1) & 1];
+    } else {
+      EFSI_COUNTED launch_pdl(k_mg_tail, 1, kTailThreads, P->tail_smem_bytes, s, T);
+      cur[lt] = P->lv[lt].pa;
+    }
   } else {
     // Coarsest level: `coarse` sweeps from zero.
     const int l = nl - 1;
@@ -2333,7 +2623,7 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     cur[l] = c;
   }
   // Up: prolongation fused into the first post sweep.
-  const int up_start = (lt < nl) ? lt - 1 : nl - 2;
+  const int up_start = coarse_kernel ? 0 : (lt < nl) ? lt - 1 : nl - 2;
   for (int l = up_start; l >= 0; --l) {
     LevelBuf& B = P->lv[l];
     const LevelBuf& C = P->lv[l + 1];

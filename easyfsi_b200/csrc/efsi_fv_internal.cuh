@@ -290,6 +290,8 @@ struct efsi_fv_plan {
   int tail_moff[12] = {0};
   int tail_coff[12] = {0};
   int tail_noff[12] = {0};
+  int coarse_blocks = 0;               // grid of the cooperative coarse-level kernel (0: per-level launches)
+  unsigned* coarse_bar = nullptr;      // its grid barrier: arrivals, generation
   std::string graph_error;
   std::deque<PlaneMap> maps;  // deque: descriptors stay in place as the cache grows
 };

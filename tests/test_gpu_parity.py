@@ -291,12 +291,14 @@ def test_graph_blocks_match_direct_launches(case):
     assert np.array_equal(out[1][1], out[2][1])
 
 
-def _paired_solvers(n, aux=False):
+def _paired_solvers(n, aux=False, alt_env=None):
     """The same graded grid and obstacle built twice: plane-marching kernels
-    (default) and the per-cell kernels (selected at plan creation).  With
-    `aux`, Dirichlet velocity rows and an interface diagonal are live too."""
+    (default) and the per-cell kernels (selected at plan creation), or the
+    variant that `alt_env` selects.  With `aux`, Dirichlet velocity rows and
+    an interface diagonal are live too."""
     import os
 
+    alt_env = alt_env or {"EFSI_NO_MARCH": "1", "EFSI_NO_TILED": "1"}
     grid = _graded_grid(n)
     obs = _obstacle(grid, seed=7)
     rng = np.random.default_rng(23)
@@ -304,8 +306,8 @@ def _paired_solvers(n, aux=False):
     vw = rng.random(grid.grid_nodes).astype(np.float32)
     iface = np.where(rng.random(grid.grid_nodes) < 0.05, rng.random(grid.grid_nodes), 0.0)
     out = []
-    for env in ({}, {"EFSI_NO_MARCH": "1", "EFSI_NO_TILED": "1"}):
-        saved = {k: os.environ.get(k) for k in ("EFSI_NO_MARCH", "EFSI_NO_TILED")}
+    for env in ({}, alt_env):
+        saved = {k: os.environ.get(k) for k in alt_env}
         os.environ.update(env)
         try:
             fl = _solver(grid)
@@ -364,6 +366,44 @@ def test_march_kernels_match_per_cell_kernels(n, aux):
             iterations=4, rhs_scale=1.0e6, pressure_outlet_zmin=True, multigrid_cycles=2
         )
     assert rel_l2(fm.pressure.to_numpy(), fc.pressure.to_numpy()) <= 1e-12
+
+
+@pytest.mark.parametrize("n,aux", [((40, 24, 48), False), ((64, 48, 96), False), ((64, 48, 96), True)])
+def test_coarse_kernel_matches_per_level_launches(n, aux):
+    """The cooperative coarse-level kernel (levels 1 .. lt-1 and the tail in
+    one launch) reproduces the per-level launches: the same rows in the same
+    order, so the V-cycle agrees bit for bit and the PCG takes the same path;
+    it replaces the coarse launches of every V-cycle."""
+    from easyfsi_b200 import _native
+
+    grid, (fk, fl_) = _paired_solvers(n, aux, alt_env={"EFSI_NO_COARSE_KERNEL": "1"})
+    rng = np.random.default_rng(29)
+    r = rng.normal(size=grid.grid_nodes)
+    r[fk.obstacle.to_numpy() == 1] = 0.0
+    zs, launches = [], []
+    lib = _native.load()
+    for fl in (fk, fl_):
+        fl.cg_r.from_numpy(r)
+        fl._apply_fv_multigrid_preconditioner(fl.cg_r, pressure_outlet_zmin=False)  # warm-up
+        torch.cuda.synchronize()
+        n0 = lib.efsi_kernel_launch_count()
+        fl._apply_fv_multigrid_preconditioner(fl.cg_r, pressure_outlet_zmin=False)
+        torch.cuda.synchronize()
+        launches.append(lib.efsi_kernel_launch_count() - n0)
+        zs.append(fl.cg_z.to_numpy())
+    assert np.array_equal(zs[0], zs[1])
+    assert launches[0] < launches[1], launches
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    res = []
+    for fl in (fk, fl_):
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(iterations=300, rhs_scale=1.0e6, pressure_outlet_zmin=False, tolerance=1e-10,
+                                         preconditioner="fv_multigrid")
+        assert fl.last_cg_used_graphs, getattr(fl, "last_cg_graph_error", "")
+        res.append((fl.last_cg_iterations, fl.pressure.to_numpy()))
+    assert res[0][0] == res[1][0]
+    assert rel_l2(res[0][1], res[1][1]) <= 1e-13
 
 
 # (level 0 streams its mask rows by TMA only when nz % 16 == 0; below that
