@@ -230,6 +230,7 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_zero_buffers": [I, P, P, P],
     "efsi_fv_learned_input": [P, P, P, P],
     "efsi_fv_learned_presmooth": [P, P, P, I, P],
+    "efsi_fv_coarse_kernel_blocks": [P, POINTER(c_int32)],
     "efsi_reach_plan_create": [POINTER(c_void_p)],
     "efsi_reach_plan_destroy": [P],
     "efsi_outlet_reachability": [P, I, I, I, P, P, P, P, I, I, P, P, POINTER(ReachReport), P],

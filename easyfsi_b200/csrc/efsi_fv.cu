@@ -1864,22 +1864,35 @@ static void configure_tail(efsi_fv_plan* P) {
 static void configure_coarse(efsi_fv_plan* P) {
   P->coarse_blocks = 0;
   const bool off = std::getenv("EFSI_NO_COARSE_KERNEL") != nullptr;
-  if (off || P->tail_level < 2 || P->tail_level >= P->n_levels) return;
+  if (off) {
+    P->coarse_note = "EFSI_NO_COARSE_KERNEL is set";
+    return;
+  }
+  if (P->tail_level < 2 || P->tail_level >= P->n_levels) {
+    P->coarse_note = "no tail below level 1 (tail level " + std::to_string(P->tail_level) + " of " +
+                     std::to_string(P->n_levels) + " levels)";
+    return;
+  }
   int dev = 0, coop = 0, sms = 0, smem_optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (!coop || sms <= 0) return;
-  if (cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin) != cudaSuccess) {
+  if (!coop || sms <= 0) {
+    P->coarse_note = "cooperative launches are not supported on this device";
+    return;
+  }
+  cudaError_t e = cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin);
+  if (e != cudaSuccess) {
     cudaGetLastError();
+    P->coarse_note = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_coarse, kTailThreads, P->tail_smem_bytes) !=
-          cudaSuccess ||
-      per_sm < 1) {
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_coarse, kTailThreads, P->tail_smem_bytes);
+  if (e != cudaSuccess || per_sm < 1) {
     cudaGetLastError();
+    P->coarse_note = std::string("occupancy: ") + cudaGetErrorString(e) + ", blocks per SM " + std::to_string(per_sm);
     return;
   }
   if (cudaMalloc(&P->coarse_bar, 2 * sizeof(unsigned)) != cudaSuccess ||
@@ -1887,9 +1900,11 @@ static void configure_coarse(efsi_fv_plan* P) {
     cudaGetLastError();
     cudaFree(P->coarse_bar);
     P->coarse_bar = nullptr;
+    P->coarse_note = "cannot allocate the grid barrier";
     return;
   }
   P->coarse_blocks = std::min(per_sm, 2) * sms;
+  P->coarse_note = "";
 }
 }  // namespace efsi
 
@@ -3578,3 +3593,10 @@ int efsi_fv_learned_presmooth(efsi_fv_plan* P, const double* r, double* z, int32
 }  // extern "C"
 
 extern "C" const char* efsi_fv_graph_error(efsi_fv_plan* P) { return P ? P->graph_error.c_str() : ""; }
+
+extern "C" int efsi_fv_coarse_kernel_blocks(efsi_fv_plan* P, int32_t* blocks) {
+  EFSI_ARG_CHECK(P != nullptr && blocks != nullptr, "null argument");
+  *blocks = P->coarse_blocks;
+  if (P->coarse_blocks == 0) set_error(P->coarse_note);
+  return EFSI_OK;
+}

@@ -292,6 +292,7 @@ struct efsi_fv_plan {
   int tail_noff[12] = {0};
   int coarse_blocks = 0;               // grid of the cooperative coarse-level kernel (0: per-level launches)
   unsigned* coarse_bar = nullptr;      // its grid barrier: arrivals, generation
+  std::string coarse_note;             // why the per-level launches run instead
   std::string graph_error;
   std::deque<PlaneMap> maps;  // deque: descriptors stay in place as the cache grows
 };

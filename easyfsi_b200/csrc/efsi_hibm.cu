@@ -326,21 +326,47 @@ __device__ __forceinline__ float tent(const float* xm, const float* xp, float R)
   return w;
 }
 
-// Visits the particles of the 3 x 3 x 3 bins around xm with one bin per lane
-// (lanes 0..26; lane (d0 + 1) * 9 + (d1 + 1) * 3 + (d2 + 1)), each lane
-// walking its bin in bin order: the 27 bins' offsets and particles are
-// fetched in parallel rather than one bin after another.
+// Visits the particles of the 3 x 3 x 3 bins around xm with the whole warp
+// (every lane must call it): lane b < 27 fetches the offsets of neighbour bin
+// b = (d0 + 1) * 9 + (d1 + 1) * 3 + (d2 + 1), a warp scan of the bin sizes
+// numbers the visits 0 .. total-1 in bin order, and the lanes take visits
+// lane, lane + 32, ..., each finding its bin by a binary search over the
+// scan.  The 27 bins are fetched in parallel and every lane has work.
 template <class Fn>
-__device__ __forceinline__ void for_near_lanes(const BinView& B, const float* xm, int lane, Fn fn) {
-  if (lane >= 27) return;
-  const int d0 = lane / 9 - 1, d1 = (lane / 3) % 3 - 1, d2 = lane % 3 - 1;
-  const int b0 = bin_axis(xm[0], B.bmin[0], B.invR, B.nb[0]) + d0;
-  const int b1 = bin_axis(xm[1], B.bmin[1], B.invR, B.nb[1]) + d1;
-  const int b2 = bin_axis(xm[2], B.bmin[2], B.invR, B.nb[2]) + d2;
-  if (b0 < 0 || b0 >= B.nb[0] || b1 < 0 || b1 >= B.nb[1] || b2 < 0 || b2 >= B.nb[2]) return;
-  const int bin = (b0 * B.nb[1] + b1) * B.nb[2] + b2;
-  const int lo = __ldg(B.offset + bin), hi = __ldg(B.offset + bin + 1);
-  for (int q = lo; q < hi; ++q) fn(__ldg(B.sorted + q));
+__device__ __forceinline__ void for_near(const BinView& B, const float* xm, int lane, Fn fn) {
+  int lo = 0, cnt = 0;
+  if (lane < 27) {
+    const int d0 = lane / 9 - 1, d1 = (lane / 3) % 3 - 1, d2 = lane % 3 - 1;
+    const int b0 = bin_axis(xm[0], B.bmin[0], B.invR, B.nb[0]) + d0;
+    const int b1 = bin_axis(xm[1], B.bmin[1], B.invR, B.nb[1]) + d1;
+    const int b2 = bin_axis(xm[2], B.bmin[2], B.invR, B.nb[2]) + d2;
+    if (b0 >= 0 && b0 < B.nb[0] && b1 >= 0 && b1 < B.nb[1] && b2 >= 0 && b2 < B.nb[2]) {
+      const int bin = (b0 * B.nb[1] + b1) * B.nb[2] + b2;
+      lo = __ldg(B.offset + bin);
+      cnt = __ldg(B.offset + bin + 1) - lo;
+    }
+  }
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int excl = incl - cnt;
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  for (int base = 0; base < total; base += 32) {
+    const int idx = base + lane;
+    // the last lane j with excl_j <= idx owns visit idx (excl is non-decreasing)
+    int j = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int e = __shfl_sync(0xffffffffu, excl, j + step);
+      if (e <= idx) j += step;
+    }
+    const int lo_j = __shfl_sync(0xffffffffu, lo, j);
+    const int ex_j = __shfl_sync(0xffffffffu, excl, j);
+    if (idx < total) fn(__ldg(B.sorted + lo_j + (idx - ex_j)));
+  }
 }
 
 // Butterfly sums over the warp: every lane gets the same total, summed in a
@@ -357,9 +383,8 @@ __device__ __forceinline__ double warp_allsum(double v) {
 }
 
 // hibm_mpm.py:4899-4959 _scatter_marker_forces_to_mpm_particles_kernel: one
-// warp per marker, one neighbour bin per lane; the tent-weight sum over the
-// marker's neighbourhood is a warp reduction, then every lane spreads
-// F * w / wsum to its bin's particles.
+// warp per marker; the tent-weight sum over the marker's neighbourhood is a
+// warp reduction, then the lanes spread F * w / wsum to the particles.
 __global__ void k_scatter(BinView B, int M, const float* xg, const double* Fg, const float* xp, float* fext,
                           double* rep) {
   const int m = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
@@ -369,11 +394,11 @@ __global__ void k_scatter(BinView B, int M, const float* xg, const double* Fg, c
   const bool valid = finite3(xm) && isfinite(Fm[0]) && isfinite(Fm[1]) && isfinite(Fm[2]);
   const float R = B.R;
   float wl = 0.0f;
-  if (valid) for_near_lanes(B, xm, lane, [&](int p) { wl += tent(xm, xp + 3 * p, R); });
+  if (valid) for_near(B, xm, lane, [&](int p) { wl += tent(xm, xp + 3 * p, R); });
   const float wsum = warp_allsum(wl);
   if (valid && wsum > 1.0e-12f) {
     double e0 = 0, e1 = 0, e2 = 0, contrib = 0;
-    for_near_lanes(B, xm, lane, [&](int p) {
+    for_near(B, xm, lane, [&](int p) {
       float w = tent(xm, xp + 3 * p, R);
       if (w > 0.0f) {
         const double ratio = (double)(w / wsum);
@@ -419,7 +444,7 @@ __global__ void k_feedback(BinView B, int M, float* xg, float* vg, float* ng, fl
   const float ao = Ag[m];
   float vs[3] = {0, 0, 0}, ns[3] = {0, 0, 0}, as = 0.0f, ws = 0.0f, gs = 0.0f;
   const float R = B.R;
-  for_near_lanes(B, xo, lane, [&](int p) {
+  for_near(B, xo, lane, [&](int p) {
     float w = tent(xo, xp + 3 * p, R);
     if (w > 0.0f) {
       vs[0] += w * __ldg(vp + 3 * p);

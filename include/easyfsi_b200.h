@@ -221,6 +221,12 @@ int efsi_cg_compute_beta(efsi_fv_plan* plan, int32_t use_mg, void* stream);
 /* Why CUDA-graph capture was abandoned for this plan ("" when it was not). */
 const char* efsi_fv_graph_error(efsi_fv_plan* plan);
 
+/* Grid size of the cooperative kernel that runs the V-cycle's levels 1 ..
+ * lt-1 and its tail in one launch (0: per-level launches; efsi_last_error()
+ * then says why).  No reference counterpart: the reference launches every
+ * level's kernels (fluid.py:6085-6262). */
+int efsi_fv_coarse_kernel_blocks(efsi_fv_plan* plan, int32_t* blocks);
+
 /* fluid.py:5992-6083 _solve_pressure_poisson_fv_multigrid (standalone cycles). */
 int efsi_fv_multigrid_solve(efsi_fv_plan* plan, const double* rhs0, double* pressure, int32_t outlet,
                             int32_t iterations, int32_t cycles, void* stream);

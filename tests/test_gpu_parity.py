@@ -8,6 +8,7 @@ f32 fields summed by atomics in another order (particle velocity, F - I,
 external forces) 1e-5.
 """
 
+import ctypes
 import math
 
 import numpy as np
@@ -377,6 +378,12 @@ def test_coarse_kernel_matches_per_level_launches(n, aux):
     from easyfsi_b200 import _native
 
     grid, (fk, fl_) = _paired_solvers(n, aux, alt_env={"EFSI_NO_COARSE_KERNEL": "1"})
+    blocks = []
+    for fl in (fk, fl_):
+        b = ctypes.c_int32(0)
+        _native.call("efsi_fv_coarse_kernel_blocks", fl._plan, ctypes.byref(b))
+        blocks.append(b.value)
+    assert blocks[0] > 0 and blocks[1] == 0, (blocks, _native.load().efsi_last_error().decode())
     rng = np.random.default_rng(29)
     r = rng.normal(size=grid.grid_nodes)
     r[fk.obstacle.to_numpy() == 1] = 0.0
