@@ -59,6 +59,7 @@ class CgStats(Structure):
         ("breakdown_dAd", c_double),
         ("b_norm", c_double),
         ("learned_relative_residual", c_double),
+        ("unreached_set_mean_projection_count", c_int32),
     ]
 
 
@@ -231,6 +232,9 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_fv_learned_input": [P, P, P, P],
     "efsi_fv_learned_presmooth": [P, P, P, I, P],
     "efsi_fv_coarse_kernel_blocks": [P, POINTER(c_int32)],
+    "efsi_fv_set_unreached_components": [P, P, I, P],
+    "efsi_divergence_final_report": [P, P, P, P, P, P, I, P, P],
+    "efsi_fv_subtract_unreached_means": [P, P, P, P, P],
     "efsi_reach_plan_create": [POINTER(c_void_p)],
     "efsi_reach_plan_destroy": [P],
     "efsi_outlet_reachability": [P, I, I, I, P, P, P, P, I, I, P, P, POINTER(ReachReport), P],

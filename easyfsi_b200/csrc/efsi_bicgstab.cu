@@ -118,7 +118,11 @@ int efsi_fv_bicgstab(efsi_fv_plan* P, const double* rhs, double* pressure, int32
       EFSI_TRY(efsi_weighted_dot(P, ones, ones, &free_vol, stream));
     }
     auto dot = [&](const double* a, const double* b, double& out) { return efsi_weighted_dot(P, a, b, &out, stream); };
+    // with an outlet and unreached components: their means first
+    // (fluid.py:6282-6296 project_field / project_pressure_and_residual)
+    const bool anchor = outlet != 0 && P->ucomp_n > 0;
     auto project = [&](double* f) -> int {
+      if (anchor) EFSI_TRY(efsi_fv_subtract_unreached_means(P, f, nullptr, nullptr, stream));
       if (!remove_mean) return EFSI_OK;
       double sum = 0.0;
       EFSI_TRY(dot(f, ones, sum));

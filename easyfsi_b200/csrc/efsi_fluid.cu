@@ -338,6 +338,81 @@ __global__ void k_div_stats(LevelDev L, const float* __restrict__ div, const dou
   }
 }
 
+// fluid.py:3574-3663 _divergence_final_report_kernel with the stencil tests
+// of fluid.py:3665-3768: per fluid cell the raw |div| and residual
+// |div - source| into 18 slots (max, sum of squares, count each):
+//   0/1 all, 2/3 interior, 4/5 near a velocity-Dirichlet row, 6/7 far from
+//   one, 8/9 with a pressure-correctable face, 10/11 without (12-15 the
+//   interior ones of those two), 16/17 outlet-unreached cells (reach given),
+//   which are kept out of all other slots.
+// Block sums in shared memory, then one global atomic per slot (the
+// reference's own reductions are atomic).
+__global__ void __launch_bounds__(256) k_div_final_report(LevelDev L, const float* __restrict__ div,
+                                                          const double* __restrict__ idiv,
+                                                          const float* __restrict__ src,
+                                                          const int32_t* __restrict__ vda,
+                                                          const int32_t* __restrict__ reach, int outlet,
+                                                          double* out) {
+  __shared__ double s_sum[18], s_cnt[18];
+  __shared__ unsigned long long s_max[18];
+  const unsigned tid = flat_tid();
+  if (tid < 18) {
+    s_sum[tid] = 0.0;
+    s_cnt[tid] = 0.0;
+    s_max[tid] = 0ull;
+  }
+  __syncthreads();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i < L.nx && j < L.ny && k < L.nz) {
+    const int64_t c = cix(i, j, k, L.ny, L.nz);
+    const unsigned m = L.mask[c];
+    if (m & M_FLUID) {
+      const int64_t sx = (int64_t)L.ny * L.nz, sy = L.nz;
+      const double total = (double)div[c] + (idiv ? idiv[c] : 0.0);
+      const double raw = fabs(total), res = fabs(total - (double)src[c]);
+      auto put = [&](int slot, double v) {
+        atomicAdd(&s_sum[slot], v * v);
+        atomicAdd(&s_cnt[slot], 1.0);
+        atomicMax(&s_max[slot], (unsigned long long)__double_as_longlong(v));
+      };
+      if (reach != nullptr && reach[c] == 0) {
+        put(16, raw);
+        put(17, res);
+      } else {
+        const bool interior = i > 0 && i < L.nx - 1 && j > 0 && j < L.ny - 1 && k > 0 && k < L.nz - 1;
+        auto va = [&](int64_t q) { return vda != nullptr && vda[q] != 0; };
+        const bool near = va(c) || (i < L.nx - 1 && va(c + sx)) || (j < L.ny - 1 && va(c + sy)) ||
+                          (k < L.nz - 1 && va(c + 1));
+        const bool corr = ((m & M_XM) && !va(c)) || ((m & M_XP) && !va(c + sx)) || ((m & M_YM) && !va(c)) ||
+                          ((m & M_YP) && !va(c + sy)) || ((m & M_ZM) && !va(c)) || ((m & M_ZP) && !va(c + 1)) ||
+                          (outlet && k == 0 && !va(c));
+        put(0, raw);
+        put(1, res);
+        if (interior) {
+          put(2, raw);
+          put(3, res);
+        }
+        put(near ? 4 : 6, raw);
+        put(near ? 5 : 7, res);
+        put(corr ? 8 : 10, raw);
+        put(corr ? 9 : 11, res);
+        if (interior) {
+          put(corr ? 12 : 14, raw);
+          put(corr ? 13 : 15, res);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid < 18 && s_cnt[tid] > 0.0) {
+    atomicAdd(out + 3 * tid + 1, s_sum[tid]);
+    atomicAdd(out + 3 * tid + 2, s_cnt[tid]);
+    atomic_max_nonneg(out + 3 * tid, __longlong_as_double((long long)s_max[tid]));
+  }
+}
+
 // fluid.py:3196-3273 _spread_surface_forces_kernel (force density, per vertex).
 __global__ void k_spread(LevelDev L, efsi_grid_axes A, const float* __restrict__ pos, const float* __restrict__ fs,
                          int nv, float cx, float cy, float cz, float sign, float* __restrict__ force, double* rep) {
@@ -527,6 +602,25 @@ int efsi_divergence_stats(efsi_fv_plan* P, const float* divergence, const double
                                          &P->sc->ticket, tmp);
   EFSI_LAUNCH_CHECK();
   EFSI_CUDA_CHECK(cudaMemcpyAsync(out_host, tmp, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  return EFSI_OK;
+}
+
+int efsi_divergence_final_report(efsi_fv_plan* P, const float* divergence, const double* iface_div,
+                                 const float* volume_source, const int32_t* velocity_dirichlet_active,
+                                 const int32_t* outlet_reachable, int32_t outlet, double* out_host, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(divergence != nullptr && volume_source != nullptr && out_host != nullptr, "null argument");
+  LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  cudaStream_t s = as_stream(stream);
+  if (P->report_buf == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&P->report_buf, 54 * sizeof(double)));
+  EFSI_CUDA_CHECK(cudaMemsetAsync(P->report_buf, 0, 54 * sizeof(double), s));
+  EFSI_COUNTED k_div_final_report<<<S.grid, S.block, 0, s>>>(L, divergence, iface_div, volume_source,
+                                                             velocity_dirichlet_active, outlet_reachable,
+                                                             outlet ? 1 : 0, P->report_buf);
+  EFSI_LAUNCH_CHECK();
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(out_host, P->report_buf, 54 * sizeof(double), cudaMemcpyDeviceToHost, s));
   EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
   return EFSI_OK;
 }

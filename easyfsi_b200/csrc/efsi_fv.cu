@@ -1480,6 +1480,60 @@ __global__ void __launch_bounds__(256) k_learned_combine(LevelDev L, const doubl
   n_io[c] = __ldg(zpre + c) + s * n_io[c];
 }
 
+// Unreached-component anchoring of outlet solves (fluid.py:4905-4981):
+// per component c, the volume-weighted sum and volume of a field over its
+// cells (shared-memory sums per block, then one global atomic per block and
+// component, as the reference's atomic sums), then field -= sum / volume on
+// the component's cells.
+constexpr int kMaxUnreachedComponents = 256;
+
+__global__ void k_comp_zero(double* acc) {
+  pdl_wait();
+  for (int q = threadIdx.x; q < 2 * kMaxUnreachedComponents; q += blockDim.x) acc[q] = 0.0;
+}
+
+__global__ void __launch_bounds__(256) k_comp_accumulate(LevelDev L, const double* __restrict__ f,
+                                                         const int32_t* __restrict__ comp, int ncomp, double* acc) {
+  pdl_wait();
+  __shared__ double s_sum[kMaxUnreachedComponents], s_vol[kMaxUnreachedComponents];
+  __shared__ int s_any;
+  const int tid = flat_tid(), nthr = blockDim.x * blockDim.y * blockDim.z;
+  for (int q = tid; q < ncomp; q += nthr) {
+    s_sum[q] = 0.0;
+    s_vol[q] = 0.0;
+  }
+  if (tid == 0) s_any = 0;
+  __syncthreads();
+  EFSI_CELL_PROLOGUE(L)
+  if (active) {
+    const int cc = __ldg(comp + c);
+    if (cc >= 0 && cc < ncomp) {
+      const double vol = vol64(L, i, j, k);
+      atomicAdd(&s_sum[cc], __ldg(f + c) * vol);
+      atomicAdd(&s_vol[cc], vol);
+      s_any = 1;
+    }
+  }
+  __syncthreads();
+  if (!s_any) return;
+  for (int q = tid; q < ncomp; q += nthr)
+    if (s_vol[q] != 0.0) {
+      atomicAdd(acc + q, s_sum[q]);
+      atomicAdd(acc + kMaxUnreachedComponents + q, s_vol[q]);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_comp_subtract(LevelDev L, double* __restrict__ f,
+                                                       const int32_t* __restrict__ comp, const double* acc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const int cc = __ldg(comp + c);
+  if (cc < 0) return;
+  const double vol = acc[kMaxUnreachedComponents + cc];
+  if (vol > 0.0) f[c] -= acc[cc] / vol;
+}
+
 // fluid.py:4677-4693 with multiplier -1 on the level-0 rhs, plus the free
 // volume (computed in the same pass as the reference does).
 __global__ void __launch_bounds__(256) k_rhs_mean(LevelDev L, const double* __restrict__ rhs, double multiplier,
@@ -1873,16 +1927,26 @@ static void configure_coarse(efsi_fv_plan* P) {
                      std::to_string(P->n_levels) + " levels)";
     return;
   }
-  int dev = 0, coop = 0, sms = 0, smem_optin = 0;
+  int dev = 0, coop = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (!coop || sms <= 0) {
     P->coarse_note = "cooperative launches are not supported on this device";
     return;
   }
-  cudaError_t e = cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin);
+  // the largest tail of any plan so far (the kernel's own static shared
+  // memory comes on top, so the opt-in maximum itself would be refused)
+  static std::mutex attr_mutex;
+  static int attr_bytes = 0;
+  cudaError_t e = cudaSuccess;
+  {
+    std::lock_guard<std::mutex> lock(attr_mutex);
+    if ((int)P->tail_smem_bytes > attr_bytes) {
+      e = cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->tail_smem_bytes);
+      if (e == cudaSuccess) attr_bytes = (int)P->tail_smem_bytes;
+    }
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     P->coarse_note = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
@@ -2082,6 +2146,9 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   cudaFree(P->bicg_work);
   cudaFree(P->unet_in);
   cudaFree(P->coarse_bar);
+  cudaFree(P->ucomp);
+  cudaFree(P->ucomp_acc);
+  cudaFree(P->report_buf);
   cudaFree(P->cpl_rows);
   cudaFree(P->cpl_ptr);
   cudaFree(P->cpl_src);
@@ -2710,7 +2777,20 @@ struct PcgRun {
   bool dots_fused;  // the last preconditioner sweep also finished the PCG dots
   bool mixed;       // FP32 level-0 V-cycle
   bool learned;     // the attached network (code 4)
+  bool anchor;      // outlet solve with unreached components: their means are subtracted
 };
+
+// fluid.py:4965-4981 on a level-0 field: the unreached components' means
+// subtracted (three launches, capturable).
+static void subtract_unreached_means(efsi_fv_plan* P, double* f, cudaStream_t s) {
+  const LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  EFSI_COUNTED launch_pdl(k_comp_zero, 1, 256, 0, s, P->ucomp_acc);
+  EFSI_COUNTED launch_pdl(k_comp_accumulate, S.grid, S.block, 0, s, L, (const double*)f, (const int32_t*)P->ucomp,
+                          P->ucomp_n, P->ucomp_acc);
+  EFSI_COUNTED launch_pdl(k_comp_subtract, S.grid, S.block, 0, s, L, f, (const int32_t*)P->ucomp,
+                          (const double*)P->ucomp_acc);
+}
 
 static int read_scalars(PcgRun& R) {
   EFSI_CUDA_CHECK(cudaMemcpyAsync(R.P->host_sc, R.P->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, R.s));
@@ -2766,6 +2846,7 @@ static int precondition(PcgRun& R) {
     EFSI_COUNTED launch_pdl(k_jacobi_precond, R.S.grid, R.S.block, 0, R.s, R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
                                                       R.P->partials, R.P->sc);
   }
+  if (R.anchor) subtract_unreached_means(R.P, R.P->z, R.s);
   if (!want_mean) EFSI_COUNTED launch_pdl(k_set_zproj, 1, 32, 0, R.s, R.P->sc, 0);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
@@ -2784,6 +2865,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   R.mixed = false;
   R.learned = false;
   R.dots_fused = false;
+  R.anchor = prm->outlet != 0 && P->ucomp_n > 0;
   R.P = P;
   R.prm = prm;
   R.s = s;
@@ -2805,6 +2887,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   // in the same pass whether or not the mean is used.
   EFSI_COUNTED k_rhs_mean<<<R.S.grid, R.S.block, 0, s>>>(R.L, rhs0, -1.0, P->partials, P->sc);
   if (remove_mean) st->mean_projection_count += 1;
+  if (R.anchor) st->unreached_set_mean_projection_count += 1;
   EFSI_COUNTED k_build_b<<<R.S.grid, R.S.block, 0, s>>>(R.L, rhs0, remove_mean ? 1 : 0, P->b, P->partials, P->sc);
   EFSI_LAUNCH_CHECK();
   EFSI_TRY(read_scalars(R));
@@ -2826,6 +2909,12 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       // r -= C p, then the mean or <r, r>_V of the corrected residual
       EFSI_COUNTED k_couple<<<148, 256, 0, s>>>(P->cpl_rows, P->cpl_ptr, P->cpl_src, P->cpl_coef, P->cpl_n, pressure,
                                               P->r, 1);
+      EFSI_COUNTED k_residual_reduce<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, remove_mean ? 1 : 0, P->partials, P->sc);
+    }
+    if (R.anchor) {
+      // r's unreached-component means, then <r, r>_V of the anchored residual
+      subtract_unreached_means(P, P->r, s);
+      st->unreached_set_mean_projection_count += 1;
       EFSI_COUNTED k_residual_reduce<<<R.S.grid, R.S.block, 0, s>>>(R.L, P->r, remove_mean ? 1 : 0, P->partials, P->sc);
     }
     if (remove_mean) {
@@ -2868,6 +2957,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   // Initial preconditioning and rz (fluid.py:6644-6673).
   EFSI_TRY(precondition(R));
   if (remove_mean) st->mean_projection_count += 1;
+  if (R.anchor) st->unreached_set_mean_projection_count += 1;
   EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
   EFSI_LAUNCH_CHECK();
   EFSI_TRY(read_scalars(R));
@@ -2971,6 +3061,15 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     if (mean_now)
       EFSI_COUNTED launch_pdl(k_sub_mean_xr, R.S.grid, R.S.block, 0, s, R.L, pressure, P->r, P->partials, P->sc);
   };
+  // every 16th iteration of an anchored solve (fluid.py:6682-6684): the
+  // pressure's and the residual's unreached-component means, then <r, r>_V
+  auto anchor_pressure_residual = [&](bool want_rr) {
+    subtract_unreached_means(P, pressure, s);
+    subtract_unreached_means(P, P->r, s);
+    if (want_rr)
+      EFSI_COUNTED launch_pdl(k_residual_reduce, R.S.grid, R.S.block, 0, s, R.L, (const double*)P->r, 0, P->partials,
+                              P->sc);
+  };
   auto launch_precond_dots = [&]() -> int {
     EFSI_TRY(precondition(R));
     if (R.dots_fused) return EFSI_OK;
@@ -3004,7 +3103,8 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     for (int j = 0; j < 16; ++j) {
       launch_spmv(!cont && j == 0, d[j & 1], d[(j + 1) & 1]);
       const bool last = (j == 15);
-      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean);
+      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean && !R.anchor);
+      if (last && R.anchor) anchor_pressure_residual(true);
       if (!last) EFSI_TRY(launch_precond_dots());
     }
     EFSI_LAUNCH_CHECK();
@@ -3015,6 +3115,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     PcgGraphKey key{cont, R.use_mg, remove_mean, outlet, R.pre, R.coarse, R.post, pressure, R.mixed};
     key.learned = R.learned;
     key.coupled = coupled;
+    key.anchor = R.anchor;
     cudaGraphExec_t exec = nullptr;
     for (auto& g : P->graphs)
       if (g.key == key) exec = g.exec;
@@ -3078,11 +3179,14 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       launch_spmv(R.copy_next, d_old, d_new);
       R.copy_next = false;
       const bool mean_now = remove_mean && (it % 16 == 0);
+      const bool anchor_now = R.anchor && (it % 16 == 0);
       const bool check_now = (it % 16 == 0) || it == max_iters;
-      launch_update(d_new, mean_now, check_now && !mean_now);
+      launch_update(d_new, mean_now, check_now && !mean_now && !anchor_now);
+      if (anchor_now) anchor_pressure_residual(check_now && !mean_now);
       EFSI_LAUNCH_CHECK();
     }
     if (remove_mean && it % 16 == 0) st->mean_projection_count += 2;
+    if (R.anchor && it % 16 == 0) st->unreached_set_mean_projection_count += 2;
     st->iterations = it;
     const bool check = (it % 16 == 0) || it == max_iters;
     if (!check) {
@@ -3118,6 +3222,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       }
       EFSI_TRY(precondition(R));
       if (remove_mean) st->mean_projection_count += 1;
+      if (R.anchor) st->unreached_set_mean_projection_count += 1;
       EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
       EFSI_LAUNCH_CHECK();
       EFSI_TRY(read_scalars(R));
@@ -3151,6 +3256,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
         }
         EFSI_TRY(precondition(R));
         if (remove_mean) st->mean_projection_count += 1;
+        if (R.anchor) st->unreached_set_mean_projection_count += 1;
         EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
         EFSI_LAUNCH_CHECK();
         EFSI_TRY(read_scalars(R));
@@ -3183,6 +3289,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       }
       EFSI_TRY(precondition(R));
       if (remove_mean) st->mean_projection_count += 1;
+      if (R.anchor) st->unreached_set_mean_projection_count += 1;
       EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
       EFSI_LAUNCH_CHECK();
       EFSI_TRY(read_scalars(R));
@@ -3203,6 +3310,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   }
   // mean projections of z: one per preconditioner application
   if (remove_mean) st->mean_projection_count += n_precond;
+  if (R.anchor) st->unreached_set_mean_projection_count += n_precond;
   EFSI_TRY(read_scalars(R));
   st->used_graphs = (prm->use_graphs && !P->graphs_disabled) ? 1 : 0;
   st->breakdown_code = P->host_sc->code;
@@ -3487,6 +3595,43 @@ int efsi_fv_set_learned_preconditioner(efsi_fv_plan* P, efsi_unet* net, void* st
   // graphs captured with another network's buffers are not reused
   for (PcgGraph& g : P->graphs) cudaGraphExecDestroy(g.exec);
   P->graphs.clear();
+  return EFSI_OK;
+}
+
+int efsi_fv_set_unreached_components(efsi_fv_plan* P, const int32_t* comp, int32_t ncomp, void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(ncomp >= 0 && ncomp <= kMaxUnreachedComponents, "ncomp must lie in [0, 256]");
+  EFSI_ARG_CHECK(ncomp == 0 || comp != nullptr, "null component array");
+  cudaStream_t s = as_stream(stream);
+  if (ncomp > 0) {
+    const size_t n = (size_t)P->lv[0].n;
+    if (P->ucomp == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&P->ucomp, n * sizeof(int32_t)));
+    if (P->ucomp_acc == nullptr)
+      EFSI_CUDA_CHECK(cudaMalloc(&P->ucomp_acc, 2 * kMaxUnreachedComponents * sizeof(double)));
+    EFSI_CUDA_CHECK(cudaMemcpyAsync(P->ucomp, comp, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
+  P->ucomp_n = ncomp;
+  return EFSI_OK;
+}
+
+int efsi_fv_subtract_unreached_means(efsi_fv_plan* P, double* field, double* sums_host, double* volumes_host,
+                                     void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(field != nullptr, "null field");
+  if (P->ucomp_n <= 0) return EFSI_OK;
+  cudaStream_t s = as_stream(stream);
+  subtract_unreached_means(P, field, s);
+  EFSI_LAUNCH_CHECK();
+  if (sums_host != nullptr || volumes_host != nullptr) {
+    const int nc = P->ucomp_n;
+    if (sums_host != nullptr)
+      EFSI_CUDA_CHECK(cudaMemcpyAsync(sums_host, P->ucomp_acc, nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (volumes_host != nullptr)
+      EFSI_CUDA_CHECK(cudaMemcpyAsync(volumes_host, P->ucomp_acc + kMaxUnreachedComponents, nc * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s));
+    EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
   return EFSI_OK;
 }
 

@@ -230,8 +230,9 @@ struct PcgGraphKey {
   bool mixed;  // FP32 level-0 V-cycle
   bool learned = false;  // the learned preconditioner
   bool coupled = false;  // interface-coupling kernels follow the SpMV
+  bool anchor = false;   // unreached-component means are subtracted
   bool operator==(const PcgGraphKey& o) const {
-    return learned == o.learned && coupled == o.coupled && cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
+    return learned == o.learned && coupled == o.coupled && anchor == o.anchor && cont == o.cont && use_mg == o.use_mg && remove_mean == o.remove_mean && outlet == o.outlet &&
            pre == o.pre && coarse == o.coarse && post == o.post && pressure == o.pressure && mixed == o.mixed;
   }
 };
@@ -262,6 +263,10 @@ struct efsi_fv_plan {
   size_t partials_len = 0;
   double* aux = nullptr;  // 16 doubles of statistics scratch
   double* bicg_work = nullptr;  // BiCGSTAB fallback's nine level-0 work vectors, allocated at its first use
+  double* report_buf = nullptr;  // 54 doubles of the final divergence report
+  int32_t* ucomp = nullptr;      // unreached component of every level-0 cell (-1: none)
+  int ucomp_n = 0;               // components anchored by an outlet solve (0: none)
+  double* ucomp_acc = nullptr;   // per component: volume-weighted sums [256], volumes [256]
   efsi_unet* unet = nullptr;    // learned preconditioner (code 4), not owned
   void* unet_in = nullptr;      // its BF16 input [n0][16]
   float unet_wmin[3] = {1.0f, 1.0f, 1.0f};  // finest level-0 width per axis

@@ -281,6 +281,15 @@ class CartesianFluidSolver:
         self.last_cg_breakdown_dAd = 0.0
         self.last_cg_used_multigrid = False
         self._hibm_pressure_unreached_count = 0
+        self._hibm_pressure_unreached_component_count = 0
+        self.last_hibm_unreached_incompatible_component_count = 0
+        self.last_hibm_unreached_component_rhs_mean_max_abs = 0.0
+        self.last_hibm_unreached_component_rhs_integral_max_abs = 0.0
+        self.last_hibm_unreached_cells_with_interface_diagonal = 0
+        self.last_hibm_unreached_cells_with_interface_coupling = 0
+        self.last_hibm_unreached_components_with_interface_hits = 0
+        self.last_unreached_divergence_raw_stats = {"max_abs": 0.0, "l2": 0.0, "count": 0}
+        self.last_unreached_divergence_stats = {"max_abs": 0.0, "l2": 0.0, "count": 0}
         self.last_divergence_report_host_reads = 0
         self._reset_project_cg_stats()
         self.clear()
@@ -512,12 +521,11 @@ class CartesianFluidSolver:
                                                outlet: int, tolerance: float, anchor_unreached: bool,
                                                remove_nullspace_mean: bool) -> None:
         """fluid.py:6264-6533: the BiCGSTAB fallback on ``cg_rhs`` from the
-        current pressure (``efsi_fv_bicgstab``).  The unreached-set anchoring
-        of the reference is not built."""
-        if anchor_unreached:
-            raise NotImplementedError(
-                "the set-restricted mean projection of outlet-unreached components is not built on the B200 path"
-            )
+        current pressure (``efsi_fv_bicgstab``).  With ``anchor_unreached`` the
+        library subtracts the unreached components' means where the reference
+        does (the components installed by the reachability marking)."""
+        if anchor_unreached and not outlet:
+            raise ValueError("the unreached-component anchoring applies to outlet solves only")
         self._refresh_structure()
         self.last_cg_restart_policy = "periodic_exact_residual+bicgstab_fallback"
         self.last_cg_breakdown = ""
@@ -540,8 +548,10 @@ class CartesianFluidSolver:
         cells, and the unreached cells' components (labels -(rank + 1) in
         ``hibm_pressure_unreached_component_label``).  Unreached cells are
         neither masked nor changed.  ``efsi_outlet_reachability`` computes both
-        with one union-find (``last_hibm_pressure_reachability_sweeps`` is 1);
-        the reference's opt-in checksum reuse is not provided."""
+        from the connected components of the open faces (hook and pointer-jump
+        rounds; ``last_hibm_pressure_reachability_sweeps`` is 1); the
+        reference's opt-in checksum reuse is not provided.  The components
+        are handed to the library, which anchors them in outlet solves."""
         if getattr(self, "hibm_pressure_outlet_reachable", None) is None:
             shape = self.obstacle.shape
             self.hibm_pressure_outlet_reachable = Field(shape, i32, device=self.device)
@@ -565,6 +575,7 @@ class CartesianFluidSolver:
             self._hibm_pressure_unreached_count = 0
             self.last_hibm_pressure_unreached_component_count = 0
             self._hibm_pressure_unreached_component_count = 0
+            self._install_unreached_components(0)
             return 0
         kind_ptr = None
         update = 0 if use_existing_reachability_barrier else 1
@@ -591,7 +602,82 @@ class CartesianFluidSolver:
         self.last_hibm_pressure_unreached_component_count = int(rep.components)
         self._hibm_pressure_unreached_component_count = int(rep.components)
         self.last_hibm_pressure_unreached_component_overflow = bool(rep.overflow)
+        self._install_unreached_components(unreached)
         return unreached
+
+    def _unreached_mask(self) -> torch.Tensor:
+        """fluid.py:4733-4737: fluid, no reachability barrier, not reached."""
+        return ((self.obstacle.tensor == 0) & (self.hibm_pressure_reachability_barrier.tensor == 0)
+                & (self.hibm_pressure_outlet_reachable.tensor == 0))
+
+    def _install_unreached_components(self, unreached: int) -> None:
+        """Hands the anchored components of outlet solves to the library
+        (``efsi_fv_set_unreached_components``): the ranked components
+        -(rank + 1) of ``hibm_pressure_unreached_component_label`` when there
+        are any, else the whole unreached set as one (fluid.py:4965-4981)."""
+        if getattr(self, "_plan", None) is None:
+            return
+        if int(unreached) <= 0 or getattr(self, "hibm_pressure_outlet_reachable", None) is None:
+            _native.call("efsi_fv_set_unreached_components", self._plan, None, 0, _stream())
+            return
+        mask = self._unreached_mask()
+        count = int(self._hibm_pressure_unreached_component_count)
+        if count > 0:
+            label = self.hibm_pressure_unreached_component_label.tensor
+            comp = -label - 1
+            comp = torch.where(mask & (label < 0) & (comp < count), comp, torch.full_like(comp, -1))
+            ncomp = count
+        else:
+            comp = torch.where(mask, torch.zeros_like(self.obstacle.tensor), torch.full_like(self.obstacle.tensor, -1))
+            ncomp = 1
+        comp = comp.to(torch.int32).contiguous()
+        _native.call("efsi_fv_set_unreached_components", self._plan, c_void_p(comp.data_ptr()), ncomp, _stream())
+
+    def _record_unreached_interface_hit_diagnostics(self) -> None:
+        """fluid.py:5037-5222: unreached cells whose row the interface terms
+        touch -- a positive interface diagonal, or a valid coupling (row list,
+        else the per-cell slots) of which the cell is owner or neighbour --
+        and the ranked components that hold such cells."""
+        unreached = self._unreached_mask().reshape(-1)
+        label = self.hibm_pressure_unreached_component_label.tensor.reshape(-1)
+        count = int(self._hibm_pressure_unreached_component_count)
+        diag = unreached & (self.pressure_interface_matrix_diagonal.tensor.reshape(-1) > 0.0)
+        cell_hit = torch.zeros_like(unreached)
+        csr = self._interface_coupling_rows()
+        if csr is not None:
+            rows = csr[0].to(torch.int64)
+            cell_hit[rows] = unreached[rows]
+        flagged = label[diag | cell_hit].to(torch.int64)
+        comp = -flagged - 1
+        comp = comp[(flagged < 0) & (comp < count)]
+        self.last_hibm_unreached_cells_with_interface_diagonal = int(diag.sum())
+        self.last_hibm_unreached_cells_with_interface_coupling = int(cell_hit.sum())
+        self.last_hibm_unreached_components_with_interface_hits = int(torch.unique(comp).numel())
+
+    def _measure_and_subtract_unreached_rhs_means(self, field: Field, *, mean_abs_tolerance: float = 1.0e-12) -> int:
+        """fluid.py:4985-5020 and 4965-4981 on the level-0 rhs: each ranked
+        component's volume-weighted integral and mean (the incompatibility
+        measure: components whose |mean| exceeds the tolerance), then the
+        components' means subtracted.  Returns the incompatible count."""
+        sums = (c_double * 256)()
+        vols = (c_double * 256)()
+        _native.call("efsi_fv_subtract_unreached_means", self._plan, field.ptr(), sums, vols, _stream())
+        count = int(self._hibm_pressure_unreached_component_count)
+        incompatible, max_mean, max_integral = 0, 0.0, 0.0
+        tol = max(0.0, float(mean_abs_tolerance))
+        for c in range(count):
+            volume, integral = float(vols[c]), float(sums[c])
+            max_integral = max(max_integral, abs(integral))
+            if volume <= 0.0:
+                continue
+            mean = abs(integral / volume)
+            max_mean = max(max_mean, mean)
+            if mean > tol:
+                incompatible += 1
+        self.last_hibm_unreached_incompatible_component_count = incompatible
+        self.last_hibm_unreached_component_rhs_mean_max_abs = max_mean
+        self.last_hibm_unreached_component_rhs_integral_max_abs = max_integral
+        return incompatible
 
     def _as_f64(self, field: Field) -> torch.Tensor:
         return field.tensor if field.dtype == f64 else field.tensor.to(torch.float64).contiguous()
@@ -630,6 +716,7 @@ class CartesianFluidSolver:
         ):
             fld.tensor.zero_()
         self._hibm_pressure_unreached_count = 0
+        self._install_unreached_components(0)
 
     def clear_force(self) -> None:
         self.force.tensor.zero_()
@@ -723,7 +810,49 @@ class CartesianFluidSolver:
         return self._div_stats(0, interior_only)
 
     def divergence_residual_stats(self, *, interior_only: bool = False) -> dict[str, float]:
+        """fluid.py:3837-3848: outlet-unreached cells are left out while any exist."""
+        if int(self._hibm_pressure_unreached_count) > 0:
+            slots = self._final_report_slots(pressure_outlet_zmin=False)
+            return {k: slots[3 if interior_only else 1][k] for k in ("max_abs", "l2")}
         return self._div_stats(1, interior_only)
+
+    def _final_report_slots(self, *, pressure_outlet_zmin: bool) -> list[dict]:
+        """The 18 slots of ``efsi_divergence_final_report`` decoded as the
+        reference's _decode_divergence_report_snapshot (fluid.py:3850-3858)."""
+        self._refresh_structure()
+        out = (c_double * 54)()
+        reach = None
+        if int(self._hibm_pressure_unreached_count) > 0 and getattr(self, "hibm_pressure_outlet_reachable", None) is not None:
+            reach = self.hibm_pressure_outlet_reachable.ptr()
+        _native.call("efsi_divergence_final_report", self._plan, self.divergence.ptr(),
+                     self.pressure_interface_projection_divergence_s.ptr(), self.volume_source_s.ptr(),
+                     self.velocity_dirichlet_boundary_active.ptr(), reach, 1 if pressure_outlet_zmin else 0, out,
+                     _stream())
+        self.last_divergence_report_host_reads += 1
+        slots = []
+        for q in range(18):
+            count = int(out[3 * q + 2])
+            slots.append({"max_abs": float(out[3 * q]), "l2": math.sqrt(float(out[3 * q + 1]) / max(1, count)),
+                          "count": count})
+        return slots
+
+    def final_divergence_report_stats(self, *, pressure_outlet_zmin: bool = False):
+        """fluid.py:3870-3896: (raw, residual, interior raw, interior residual)
+        over the reached fluid cells; the unreached cells' stats land in
+        ``last_unreached_divergence_raw_stats`` / ``last_unreached_divergence_stats``."""
+        slots = self._final_report_slots(pressure_outlet_zmin=pressure_outlet_zmin)
+        self.last_unreached_divergence_raw_stats = slots[16]
+        self.last_unreached_divergence_stats = slots[17]
+        return slots[0], slots[1], slots[2], slots[3]
+
+    def final_and_dirichlet_partition_report_stats(self, *, pressure_outlet_zmin: bool = False):
+        """fluid.py:3898-3990: the final stats followed by the velocity-Dirichlet
+        near / far and pressure-correctable / fixed partitions (raw, residual
+        each, then the interior correctable / fixed ones)."""
+        slots = self._final_report_slots(pressure_outlet_zmin=pressure_outlet_zmin)
+        self.last_unreached_divergence_raw_stats = slots[16]
+        self.last_unreached_divergence_stats = slots[17]
+        return tuple(slots[:16])
 
     # ------------------------------------------------------------------
     # FV operator and pressure-solver kernels (fluid.py:4080-4726, 5228-6262)
@@ -1014,7 +1143,21 @@ class CartesianFluidSolver:
             raise ValueError(f"unsupported cg_preconditioner: {preconditioner!r}")
         if name == "auto":
             name = "jacobi" if self.grid.is_uniform else "fv_multigrid"
+        # fluid.py:6567-6588: an outlet solve with flood-unreached cells anchors
+        # each unreached component by subtracting its volume-weighted mean
+        anchor_unreached = bool(pressure_outlet_zmin) and int(self._hibm_pressure_unreached_count) > 0
+        self.last_hibm_unreached_cells_with_interface_diagonal = 0
+        self.last_hibm_unreached_cells_with_interface_coupling = 0
+        self.last_hibm_unreached_components_with_interface_hits = 0
+        if anchor_unreached:
+            self._record_unreached_interface_hit_diagnostics()
         self._prepare_fv_multigrid_rhs(rhs_scale)
+        if anchor_unreached:
+            self._measure_and_subtract_unreached_rhs_means(self._mg_rhs[0])
+        else:
+            self.last_hibm_unreached_incompatible_component_count = 0
+            self.last_hibm_unreached_component_rhs_mean_max_abs = 0.0
+            self.last_hibm_unreached_component_rhs_integral_max_abs = 0.0
         params = _native.PcgParams(
             max(1, int(iterations)),
             _PRECOND_CODE[name],
@@ -1036,7 +1179,7 @@ class CartesianFluidSolver:
         self.last_cg_host_residual_checks = int(stats.host_residual_checks)
         self.last_cg_mean_host_reads = 0
         self.last_cg_mean_projection_count = int(stats.mean_projection_count)
-        self.last_cg_unreached_set_mean_projection_count = 0
+        self.last_cg_unreached_set_mean_projection_count = int(stats.unreached_set_mean_projection_count)
         self.last_cg_restart_count = int(stats.restart_count)
         self.last_cg_restart_count_measured = True
         self.last_cg_restart_policy = "periodic_exact_residual"
@@ -1055,8 +1198,8 @@ class CartesianFluidSolver:
             _native.call("efsi_fv_copy_rhs", self._plan, self.cg_rhs.ptr(), _stream())
             self._continue_pressure_poisson_fv_bicgstab(
                 start_iteration=max(1, int(iterations)), max_iters=max(1, int(iterations)), b_norm=float(stats.b_norm),
-                outlet=1 if pressure_outlet_zmin else 0, tolerance=max(0.0, float(tolerance)), anchor_unreached=False,
-                remove_nullspace_mean=bool(remove_nullspace_mean))
+                outlet=1 if pressure_outlet_zmin else 0, tolerance=max(0.0, float(tolerance)),
+                anchor_unreached=anchor_unreached, remove_nullspace_mean=bool(remove_nullspace_mean))
         if stats.b_norm <= 1.0e-30:
             self.pressure_tmp.tensor.zero_()
             self.pressure_accum.tensor.zero_()
@@ -1133,16 +1276,79 @@ class CartesianFluidSolver:
         self.last_project_cg_breakdown = ""
 
     def pressure_interface_matrix_terms_report(self) -> dict[str, float]:
+        """fluid.py:2864-3118 _pressure_interface_matrix_terms_report_kernel:
+        integrals of the interface diagonal and rhs over the cells, the row
+        list (or, without one, the per-cell slots) checked as couplings --
+        both cells inside and fluid, T > 0, not a self coupling -- with the
+        diagonal density they imply, and its mismatch against the diagonal."""
+        nx, ny, nz = self.grid.grid_nodes
         diag = self.pressure_interface_matrix_diagonal.tensor
         rhs = self.pressure_interface_matrix_rhs.tensor
-        vol = self._cell_volume_f32().to(torch.float64)
-        fluid = self.obstacle.tensor == 0
+        vol32 = self._cell_volume_f32()
+        obs = self.obstacle.tensor.reshape(-1)
+        density = torch.zeros(nx * ny * nz, dtype=diag.dtype, device=diag.device)
+        row_count = int(self.pressure_interface_row_count[None])
+        capacity = int(self.pressure_interface_row_capacity)
+        active_rows, invalid_rows, row_integral, max_t = 0, 0, 0.0, 0.0
+        dims = torch.tensor([nx, ny, nz], device=diag.device)
+        pairs = None
+        if row_count > 0:
+            limit = min(row_count, capacity)
+            own = self.pressure_interface_row_owner.tensor[:limit].to(torch.int64)
+            nbr = self.pressure_interface_row_neighbor.tensor[:limit].to(torch.int64)
+            trans = self.pressure_interface_row_transmissibility.tensor[:limit]
+            pairs = (own, nbr, trans, torch.ones(limit, dtype=torch.bool, device=diag.device))
+        else:
+            act = self.pressure_interface_coupling_active.tensor.reshape(-1)
+            cells = torch.nonzero((act > 0) & (obs == 0)).reshape(-1)
+            if cells.numel() > 0:
+                have_extra = "pressure_interface_coupling_extra_neighbor" in self.__dict__
+                n_slots = PRESSURE_INTERFACE_COUPLING_SLOT_COUNT if have_extra else 1
+                slots = torch.clamp(act[cells], max=PRESSURE_INTERFACE_COUPLING_SLOT_COUNT).to(torch.int64)
+                nb0 = self.pressure_interface_coupling_neighbor.tensor.reshape(-1, 3)[cells].to(torch.int64)
+                tr0 = self.pressure_interface_coupling_coefficient.tensor.reshape(-1)[cells]
+                if have_extra:
+                    xnb = self.pressure_interface_coupling_extra_neighbor.tensor.reshape(-1, n_slots - 1, 3)[cells]
+                    xtr = self.pressure_interface_coupling_extra_coefficient.tensor.reshape(-1, n_slots - 1)[cells]
+                    nbr = torch.cat([nb0[:, None, :], xnb.to(torch.int64)], dim=1).reshape(-1, 3)
+                    trans = torch.cat([tr0[:, None], xtr], dim=1).reshape(-1)
+                else:
+                    nbr, trans = nb0, tr0
+                in_use = (torch.arange(n_slots, device=cells.device)[None, :] < slots[:, None]).reshape(-1)
+                own_lin = cells.repeat_interleave(n_slots)
+                own = torch.stack([own_lin // (ny * nz), (own_lin // nz) % ny, own_lin % nz], dim=1)
+                pairs = (own, nbr, trans, in_use)
+                if not have_extra:
+                    # never-written extra slots hold T = 0: invalid couplings
+                    invalid_rows += int((slots - 1).sum())
+        if pairs is not None:
+            own, nbr, trans, in_use = pairs
+            inside = ((own >= 0) & (own < dims)).all(dim=1) & ((nbr >= 0) & (nbr < dims)).all(dim=1)
+            oc = torch.where(inside[:, None], own, torch.zeros_like(own))
+            nc = torch.where(inside[:, None], nbr, torch.zeros_like(nbr))
+            o_lin = (oc[:, 0] * ny + oc[:, 1]) * nz + oc[:, 2]
+            n_lin = (nc[:, 0] * ny + nc[:, 1]) * nz + nc[:, 2]
+            valid = inside & (obs[o_lin] == 0) & (obs[n_lin] == 0) & (trans > 0.0) & (o_lin != n_lin)
+            v_flat = vol32.reshape(-1)
+            t_ok = trans[valid & in_use]
+            density.index_add_(0, o_lin[valid & in_use],
+                               (t_ok / torch.clamp(v_flat[o_lin[valid & in_use]], min=1.0e-30)).to(density.dtype))
+            density.index_add_(0, n_lin[valid & in_use],
+                               (t_ok / torch.clamp(v_flat[n_lin[valid & in_use]], min=1.0e-30)).to(density.dtype))
+            active_rows = int((valid & in_use).sum())
+            invalid_rows += int((~valid & in_use).sum())
+            row_integral = float((2.0 * t_ok.to(torch.float64)).sum()) if t_ok.numel() else 0.0
+            max_t = float(t_ok.max()) if t_ok.numel() else 0.0
+        vol64 = vol32.to(torch.float64)
+        mismatch = (diag - density.reshape(diag.shape)).to(torch.float64)
         vals = torch.stack(
             [
-                torch.where(fluid, diag * vol, 0.0).sum(),
-                torch.where(fluid, rhs * vol, 0.0).sum(),
-                diag.abs().max(),
-                ((diag != 0) & fluid).sum().to(torch.float64),
+                (diag.to(torch.float64) * vol64).sum(),
+                (rhs.to(torch.float64) * vol64).sum(),
+                diag.abs().max().to(torch.float64),
+                ((diag.abs() > 0) | (rhs.abs() > 0)).sum().to(torch.float64),
+                (mismatch.abs() * vol64).sum(),
+                mismatch.abs().max(),
             ]
         ).cpu().tolist()
         return {
@@ -1150,8 +1356,14 @@ class CartesianFluidSolver:
             "rhs_integral": vals[1],
             "max_abs_diagonal": vals[2],
             "active_cells": int(vals[3]),
-            "row_count": 0,
-            "row_active_count": 0,
+            "row_count": row_count,
+            "row_active_count": active_rows,
+            "row_invalid_count": invalid_rows,
+            "row_overflow_count": max(row_count - capacity, 0),
+            "row_diagonal_integral": row_integral,
+            "row_diagonal_integral_abs_mismatch": vals[4],
+            "row_diagonal_max_abs_density_mismatch": vals[5],
+            "row_max_transmissibility": max_t,
         }
 
     def project(
@@ -1210,10 +1422,6 @@ class CartesianFluidSolver:
             )
         report = bool(read_report)
         outlet = bool(pressure_outlet_zmin)
-        if outlet and self._hibm_pressure_unreached_count > 0:
-            raise NotImplementedError(
-                "the set-restricted mean projection of outlet-unreached components is not built on the B200 path"
-            )
         self.last_divergence_report_host_reads = 0
         self._refresh_structure()
         iface_active = self._iface_active
@@ -1244,6 +1452,8 @@ class CartesianFluidSolver:
             self.last_project_cg_iterations_max = max(self.last_project_cg_iterations_max, int(self.last_cg_iterations))
             self.last_project_cg_host_residual_checks += int(self.last_cg_host_residual_checks)
             self.last_project_cg_mean_projection_count += int(self.last_cg_mean_projection_count)
+            self.last_project_cg_unreached_set_mean_projection_count += int(
+                self.last_cg_unreached_set_mean_projection_count)
             self.last_project_cg_restart_count += int(self.last_cg_restart_count)
             self.last_project_cg_restart_policy = str(self.last_cg_restart_policy)
             if math.isfinite(self.last_cg_initial_relative_residual):
@@ -1263,6 +1473,34 @@ class CartesianFluidSolver:
                     self.last_project_cg_breakdown_dAd = self.last_cg_breakdown_dAd
                 if self.last_cg_breakdown:
                     self.last_project_cg_breakdown = self.last_cg_breakdown
+
+        physical = {"failed": False, "reason": "", "action": "none", "incompatible": 0, "mean": 0.0, "integral": 0.0}
+
+        def record_physical_stats() -> None:
+            # fluid.py:7069-7112: an anchored component whose rhs has a
+            # non-zero mean cannot be made divergence free
+            physical["incompatible"] = max(physical["incompatible"],
+                                           int(self.last_hibm_unreached_incompatible_component_count))
+            physical["mean"] = max(physical["mean"], float(self.last_hibm_unreached_component_rhs_mean_max_abs))
+            physical["integral"] = max(physical["integral"],
+                                       float(self.last_hibm_unreached_component_rhs_integral_max_abs))
+            if int(self.last_hibm_unreached_incompatible_component_count) > 0:
+                physical["failed"] = True
+                physical["reason"] = "unreached_component_rhs_incompatible"
+
+        def handle_physical_failure() -> None:
+            # fluid.py:7114-7131
+            if not physical["failed"]:
+                return
+            if policy != "raise":
+                physical["action"] = "reported"
+                return
+            physical["action"] = "raised"
+            raise RuntimeError(
+                "FV-CG pressure projection physical gate failed: unreached component RHS is incompatible with a "
+                f"sealed incompressible component (components={physical['incompatible']}, "
+                f"max_abs_rhs_mean={physical['mean']:.6g})"
+            )
 
         def handle_failure() -> None:
             if solver != "fv_cg" or self.last_cg_converged:
@@ -1323,7 +1561,9 @@ class CartesianFluidSolver:
         )
         self._solve_pressure_poisson_with_solver(**solve_kwargs)
         record_cg_stats()
+        record_physical_stats()
         handle_failure()
+        handle_physical_failure()
         self._subtract_pressure_gradient_kernel(step_dt_s / self.rho, 1 if outlet else 0)
         apply_bc()
         self._compute_divergence_kernel(1 if outlet else 0)
@@ -1349,7 +1589,9 @@ class CartesianFluidSolver:
                 self.pressure_interface_matrix_rhs.tensor.zero_()
                 self._solve_pressure_poisson_with_solver(**{**solve_kwargs, "iterations": cleanup_iterations})
                 record_cg_stats()
+                record_physical_stats()
                 handle_failure()
+                handle_physical_failure()
                 self._subtract_pressure_gradient_kernel(step_dt_s / self.rho, 1)
                 corrected = self.pressure_accum.tensor + self.pressure.tensor
                 self.pressure_accum.tensor.copy_(corrected)
@@ -1365,10 +1607,9 @@ class CartesianFluidSolver:
         if not report:
             return {}
         self._compute_divergence_kernel(1 if outlet else 0)
-        final_raw = self.divergence_stats()
-        final = self.divergence_residual_stats()
-        final_int_raw = self.divergence_stats(interior_only=True)
-        final_int = self.divergence_residual_stats(interior_only=True)
+        (final_raw, final, final_int_raw, final_int, near_raw, near, far_raw, far, corr_raw, corr, fixed_raw, fixed,
+         int_corr_raw, int_corr, int_fixed_raw, int_fixed) = self.final_and_dirichlet_partition_report_stats(
+            pressure_outlet_zmin=outlet)
         iface = self.pressure_interface_matrix_terms_report()
         n_vdir = vdir_calls["cells"]
         return {
@@ -1396,23 +1637,58 @@ class CartesianFluidSolver:
             "post_boundary_max_abs": post["max_abs"],
             "post_boundary_raw_l2": post_raw["l2"],
             "post_boundary_raw_max_abs": post_raw["max_abs"],
-            "post_constraint_l2": post["l2"],
-            "post_constraint_max_abs": post["max_abs"],
-            "post_constraint_raw_l2": post_raw["l2"],
-            "post_constraint_raw_max_abs": post_raw["max_abs"],
+            "post_constraint_l2": final["l2"],
+            "post_constraint_max_abs": final["max_abs"],
+            "post_constraint_raw_l2": final_raw["l2"],
+            "post_constraint_raw_max_abs": final_raw["max_abs"],
+            "velocity_dirichlet_near_l2": near["l2"],
+            "velocity_dirichlet_near_max_abs": near["max_abs"],
+            "velocity_dirichlet_near_raw_l2": near_raw["l2"],
+            "velocity_dirichlet_near_raw_max_abs": near_raw["max_abs"],
+            "velocity_dirichlet_far_l2": far["l2"],
+            "velocity_dirichlet_far_max_abs": far["max_abs"],
+            "velocity_dirichlet_far_raw_l2": far_raw["l2"],
+            "velocity_dirichlet_far_raw_max_abs": far_raw["max_abs"],
             "velocity_dirichlet_boundary_apply_calls": vdir_calls["n"],
             "velocity_dirichlet_boundary_active_cells_total": n_vdir,
             "velocity_dirichlet_boundary_active_cells_max": vdir_calls["cells_max"],
             "velocity_dirichlet_boundary_max_delta_mps": vdir_calls["dmax"],
             "velocity_dirichlet_boundary_mean_delta_mps": vdir_calls["dsum"] / n_vdir if n_vdir > 0 else 0.0,
             "velocity_dirichlet_boundary_momentum_delta_n_s": tuple(vdir_calls["mom"]),
+            "pressure_correctable_l2": corr["l2"],
+            "pressure_correctable_max_abs": corr["max_abs"],
+            "pressure_correctable_cell_count": corr["count"],
+            "pressure_correctable_raw_l2": corr_raw["l2"],
+            "pressure_correctable_raw_max_abs": corr_raw["max_abs"],
+            "pressure_fixed_l2": fixed["l2"],
+            "pressure_fixed_max_abs": fixed["max_abs"],
+            "pressure_fixed_cell_count": fixed["count"],
+            "pressure_fixed_raw_l2": fixed_raw["l2"],
+            "pressure_fixed_raw_max_abs": fixed_raw["max_abs"],
+            "interior_pressure_correctable_l2": int_corr["l2"],
+            "interior_pressure_correctable_max_abs": int_corr["max_abs"],
+            "interior_pressure_correctable_cell_count": int_corr["count"],
+            "interior_pressure_correctable_raw_l2": int_corr_raw["l2"],
+            "interior_pressure_correctable_raw_max_abs": int_corr_raw["max_abs"],
+            "interior_pressure_fixed_l2": int_fixed["l2"],
+            "interior_pressure_fixed_max_abs": int_fixed["max_abs"],
+            "interior_pressure_fixed_cell_count": int_fixed["count"],
+            "interior_pressure_fixed_raw_l2": int_fixed_raw["l2"],
+            "interior_pressure_fixed_raw_max_abs": int_fixed_raw["max_abs"],
             "pressure_interface_matrix_diagonal_integral": iface["diagonal_integral"],
             "pressure_interface_matrix_rhs_integral": iface["rhs_integral"],
             "pressure_interface_matrix_max_abs_diagonal": iface["max_abs_diagonal"],
             "pressure_interface_matrix_active_cells": iface["active_cells"],
             "pressure_interface_matrix_active": iface_active,
-            "pressure_interface_matrix_row_count": 0,
-            "pressure_interface_matrix_row_active_count": 0,
+            "pressure_interface_matrix_row_count": iface["row_count"],
+            "pressure_interface_matrix_row_active_count": iface["row_active_count"],
+            "pressure_interface_matrix_row_invalid_count": iface["row_invalid_count"],
+            "pressure_interface_matrix_row_overflow_count": iface["row_overflow_count"],
+            "pressure_interface_matrix_row_diagonal_integral": iface["row_diagonal_integral"],
+            "pressure_interface_matrix_row_diagonal_integral_abs_mismatch": iface["row_diagonal_integral_abs_mismatch"],
+            "pressure_interface_matrix_row_diagonal_max_abs_density_mismatch": iface[
+                "row_diagonal_max_abs_density_mismatch"],
+            "pressure_interface_matrix_row_max_transmissibility": iface["row_max_transmissibility"],
             "pressure_nullspace_policy": nullspace_policy,
             "pressure_nullspace_compatibility_measured": compat,
             "pressure_nullspace_zero_mean_projection_applied": remove_mean,
@@ -1420,16 +1696,37 @@ class CartesianFluidSolver:
             "pressure_solve_failure_policy": policy,
             "pressure_solve_failed": state["failed"],
             "pressure_solve_failure_action": state["action"],
-            "pressure_projection_physical_failure": False,
-            "pressure_projection_physical_failure_reason": "",
-            "pressure_projection_physical_failure_action": "none",
+            "pressure_projection_physical_failure": physical["failed"],
+            "pressure_projection_physical_failure_reason": physical["reason"],
+            "pressure_projection_physical_failure_action": physical["action"],
+            "hibm_unreached_incompatible_component_count": physical["incompatible"],
+            "hibm_unreached_component_rhs_mean_max_abs": physical["mean"],
+            "hibm_unreached_component_rhs_integral_max_abs": physical["integral"],
             "cg_project_calls": self.last_project_cg_project_calls,
             "cg_iterations_total": self.last_project_cg_iterations_total,
             "cg_iterations_max": self.last_project_cg_iterations_max,
             "cg_host_residual_checks": self.last_project_cg_host_residual_checks,
             "cg_mean_host_reads": 0,
             "cg_mean_projection_count": self.last_project_cg_mean_projection_count,
-            "cg_unreached_set_mean_projection_count": 0,
+            "cg_unreached_set_mean_projection_count": self.last_project_cg_unreached_set_mean_projection_count,
+            "hibm_pressure_unreached_cell_count": int(getattr(self, "last_hibm_pressure_unreached_cell_count", 0)),
+            "hibm_pressure_reachability_converged": bool(
+                getattr(self, "last_hibm_pressure_reachability_converged", True)),
+            "cg_unreached_component_count": int(getattr(self, "last_hibm_pressure_unreached_component_count", 0)),
+            "cg_unreached_component_overflow": bool(
+                getattr(self, "last_hibm_pressure_unreached_component_overflow", False)),
+            "unreached_cells_with_interface_diagonal": int(self.last_hibm_unreached_cells_with_interface_diagonal),
+            "unreached_cells_with_interface_coupling": int(self.last_hibm_unreached_cells_with_interface_coupling),
+            "unreached_components_with_interface_hits": int(self.last_hibm_unreached_components_with_interface_hits),
+            "hibm_pressure_component_labels_converged": bool(
+                getattr(self, "last_hibm_pressure_component_labels_converged", True)),
+            # the solid-band and pressure-fill sweeps (fluid.py:1300-1610,
+            # 2100-2170) are not part of this path: their counters keep the
+            # reference's "not run" value
+            "hibm_solid_band_last_marked_increment": int(getattr(self, "last_hibm_solid_band_marked_increment", 0)),
+            "hibm_solid_band_interior_cells": int(getattr(self, "last_hibm_solid_band_interior_cells", -1)),
+            "hibm_solid_band_enclosed_water_cells": int(getattr(self, "last_hibm_solid_band_enclosed_water_cells", -1)),
+            "hibm_pressure_filled_cell_count": int(getattr(self, "last_hibm_pressure_filled_cell_count", -1)),
             "cg_restart_count": self.last_project_cg_restart_count,
             "cg_restart_count_measured": self.last_project_cg_restart_count_measured,
             "cg_restart_policy": self.last_project_cg_restart_policy,
@@ -1438,6 +1735,7 @@ class CartesianFluidSolver:
             "cg_converged_all": self.last_project_cg_converged_all,
             "cg_breakdown_count": self.last_project_cg_breakdown_count,
             "cg_breakdown_code": self.last_project_cg_breakdown_code,
+            "cg_breakdown_dAd": float(self.last_project_cg_breakdown_dAd),
             "cg_breakdown": self.last_project_cg_breakdown,
         }
 

@@ -187,6 +187,7 @@ typedef struct efsi_cg_stats {
   double breakdown_dAd;
   double b_norm;
   double learned_relative_residual; /* relative residual at the last check preconditioned by the learned network */
+  int32_t unreached_set_mean_projection_count; /* fluid.py:4965 _subtract_unreached_set_mean_device calls */
 } efsi_cg_stats;
 
 /* fluid.py:6535-6811 _solve_pressure_poisson_fv_cg: flexible MG/Jacobi PCG on
@@ -270,6 +271,17 @@ typedef struct efsi_grid_axes {
 /* fluid.py:2447-2527 _predict_kernel (velocity_prev is read, velocity written). */
 int efsi_predict(efsi_fv_plan* plan, const efsi_grid_axes* axes, const float* velocity_prev, float dt, float nu,
                  int32_t rk2, float* velocity, void* stream);
+
+/* fluid.py:3574-3663 _divergence_final_report_kernel: out_host[54] = 18 slots
+ * of (max_abs, sum_sq, count) over the fluid cells, raw |div + iface_div|
+ * then residual |... - source| per pair: all, interior, near / far from a
+ * velocity-Dirichlet row (fluid.py:3665-3690), with / without a pressure-
+ * correctable face (fluid.py:3717-3768), interior with / without, and the
+ * outlet-unreached cells (outlet_reachable == 0; NULL: none), which are kept
+ * out of every other slot.  velocity_dirichlet_active may be NULL. */
+int efsi_divergence_final_report(efsi_fv_plan* plan, const float* divergence, const double* iface_div,
+                                 const float* volume_source, const int32_t* velocity_dirichlet_active,
+                                 const int32_t* outlet_reachable, int32_t outlet, double* out_host, void* stream);
 
 /* fluid.py:3494-3565 _divergence_stats_kernel / _divergence_residual_stats_kernel.
  * mode 0 raw, 1 residual (minus volume source).  out_host: max_abs, sum_sq, count. */
@@ -519,8 +531,8 @@ int efsi_ib_reset_anchor_cells(int32_t* anchor_cells, int64_t node_count, void* 
 /* fluid.py:6264-6533 _continue_pressure_poisson_fv_bicgstab: the BiCGSTAB
  * fallback (right Jacobi preconditioning) of the level-0 system A p = rhs
  * from the pressure in `pressure`, relative to b_norm; remove_mean applies
- * the zero-mean projection where the reference does (no unreached-set
- * anchoring).  Host loop with one host read per inner product; allocates
+ * the zero-mean projection where the reference does, and with an outlet the
+ * unreached-component anchoring of efsi_fv_set_unreached_components.  Host loop with one host read per inner product; allocates
  * nine work vectors for the call.  stats: int64[4] = iterations, converged,
  * restarts, breakdown code (0 none, 1 shadow dot, 2 recurrence scalar,
  * 3 beta, 4 alpha denominator, 5 alpha, 6 omega denominator, 7 omega,
@@ -528,6 +540,24 @@ int efsi_ib_reset_anchor_cells(int32_t* anchor_cells, int64_t node_count, void* 
 int efsi_fv_bicgstab(efsi_fv_plan* plan, const double* rhs, double* pressure, int32_t outlet, int32_t max_iters,
                      double tolerance, double b_norm, int32_t remove_mean, int64_t* stats, double* relative_residual,
                      void* stream);
+
+/* The unreached components of an outlet solve (fluid.py:4729-4981): comp[c]
+ * (device int32 per level-0 cell) is the component of an outlet-unreached
+ * fluid cell that the PCG anchors, -1 elsewhere; at most 256 components
+ * (ncomp 0 clears them).  With an outlet, efsi_fv_pcg_solve and
+ * efsi_fv_bicgstab then subtract each component's volume-weighted mean from
+ * the residual, the preconditioned residual and the pressure where the
+ * reference calls _subtract_unreached_set_mean_device.  Copies comp into the
+ * plan; synchronises. */
+int efsi_fv_set_unreached_components(efsi_fv_plan* plan, const int32_t* comp, int32_t ncomp, void* stream);
+
+/* fluid.py:4965-4981 _subtract_unreached_set_mean_device on a level-0 f64
+ * field with the components set by efsi_fv_set_unreached_components; with
+ * sums_host / volumes_host (double[ncomp], either may be NULL) also returns
+ * each component's volume-weighted integral and volume before the subtraction
+ * (fluid.py:4985-5020 measures the rhs incompatibility from them). */
+int efsi_fv_subtract_unreached_means(efsi_fv_plan* plan, double* field, double* sums_host, double* volumes_host,
+                                     void* stream);
 
 /* Report of efsi_outlet_reachability. */
 typedef struct efsi_reach_report {

@@ -68,6 +68,7 @@ class CgStats(Structure):
         ("relative_residual", c_double),
         ("breakdown_dAd", c_double),
         ("b_norm", c_double),
+        ("unreached_set_mean_projection_count", c_int32),
     ]
 
 
@@ -362,11 +363,18 @@ class OracleFluid:
                                c_int(post), c_int(1 if self.uniform else 0))
         return z
 
-    def pcg_solve(self, *, outlet: int, max_iters: int, tol: float, precond: int, remove_mean: bool) -> CgStats:
+    def pcg_solve(self, *, outlet: int, max_iters: int, tol: float, precond: int, remove_mean: bool,
+                  components=None, component_count: int = 0) -> CgStats:
+        """The flexible PCG; with an outlet, `components` (int32 per cell, -1
+        outside the anchored set) and `component_count` anchor the unreached
+        components as fluid.py:6582-6789 does."""
         st = CgStats()
-        self.lib.efo_fv_pcg_solve(c_int(len(self.metrics)), self.levels, _p(self.obstacle), None, None, None, _p(self.rhs0),
-                                  _p(self.pressure), c_int(outlet), c_int(max_iters), c_double(tol), c_int(precond),
-                                  c_int(1 if remove_mean else 0), c_int(1 if self.uniform else 0), c_int(0), byref(st))
+        comp = None if components is None else np.ascontiguousarray(components, dtype=np.int32)
+        self.lib.efo_fv_pcg_solve_anchored(c_int(len(self.metrics)), self.levels, _p(self.obstacle), None, None, None,
+                                           _p(self.rhs0), _p(self.pressure), c_int(outlet), c_int(max_iters),
+                                           c_double(tol), c_int(precond), c_int(1 if remove_mean else 0),
+                                           c_int(1 if self.uniform else 0), c_int(0), None if comp is None else _p(comp),
+                                           c_int(int(component_count) if comp is not None else 0), byref(st))
         self.last_stats = st
         return st
 

@@ -521,19 +521,49 @@ typedef struct efo_cg_stats {
   double relative_residual;
   double breakdown_dAd;
   double b_norm;
+  int32_t unreached_set_mean_projection_count;
 } efo_cg_stats;
 
-// fluid.py:6535-6811 _solve_pressure_poisson_fv_cg (no interface row list, no
-// unreached-set anchoring: both are inactive on the plain path).
+// fluid.py:4905-4981 _accumulate_unreached_component_means_kernel and
+// _subtract_unreached_component_means_kernel: comp[c] is the component of an
+// anchored (outlet-unreached) cell, -1 elsewhere; each component's
+// volume-weighted mean (f64 volumes of the f32 widths) is subtracted from the
+// field on its cells.
+static void subtract_components(const efo_level& L, const int32_t* comp, int ncomp, double* f) {
+  if (comp == nullptr || ncomp <= 0) return;
+  std::vector<double> sum(ncomp, 0.0), vol(ncomp, 0.0);
+  for (int i = 0; i < L.nx; ++i)
+    for (int j = 0; j < L.ny; ++j)
+      for (int k = 0; k < L.nz; ++k) {
+        const int64_t c = ((int64_t)i * L.ny + j) * L.nz + k;
+        const int q = comp[c];
+        if (q < 0 || q >= ncomp) continue;
+        const double v = (double)L.wx[i] * (double)L.wy[j] * (double)L.wz[k];
+        sum[q] += f[c] * v;
+        vol[q] += v;
+      }
+  for (int64_t c = 0; c < ncells(L); ++c) {
+    const int q = comp[c];
+    if (q < 0 || q >= ncomp || !(vol[q] > 0.0)) continue;
+    f[c] -= sum[q] / vol[q];
+  }
+}
+
+// fluid.py:6535-6811 _solve_pressure_poisson_fv_cg (no interface row list).
 //   rhs_in     : the f64 level-0 rhs _mg_rhs[0] built by efo_mg_prepare_level0
 //   pressure   : warm start in, solution out (f64)
 //   precond    : 0 jacobi, 1 fv_multigrid (2/24/2), 2 fv_multigrid_light (1/12/1)
-EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32_t* obs, const int32_t* va,
-                              const r32* vw, const double* iface, const double* rhs_in, double* pressure,
-                              int outlet, int max_iters_in, double tolerance, int precond, int remove_mean,
-                              int uniform_grid, int iface_active, efo_cg_stats* st) {
+//   comp/ncomp : with an outlet, the unreached components anchored where the
+//                reference calls _subtract_unreached_set_mean_device
+//                (fluid.py:6582-6789); null / 0 for none
+EFO_API void efo_fv_pcg_solve_anchored(int n_levels, const efo_level* levels, const int32_t* obs, const int32_t* va,
+                                       const r32* vw, const double* iface, const double* rhs_in, double* pressure,
+                                       int outlet, int max_iters_in, double tolerance, int precond, int remove_mean,
+                                       int uniform_grid, int iface_active, const int32_t* comp, int ncomp,
+                                       efo_cg_stats* st) {
   const efo_level& L = levels[0];
   const int64_t n = ncells(L);
+  const bool anchor = outlet != 0 && comp != nullptr && ncomp > 0;
   const int max_iters = std::max(1, max_iters_in);
   const double tol = std::max(0.0, tolerance);
   std::memset(st, 0, sizeof(*st));
@@ -546,6 +576,12 @@ EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32
   Levels lv(n_levels, levels);
   Fine fine{obs, va, vw, iface};
   fv_diagonal(L, obs, va, vw, iface, diag.data(), outlet);
+  auto anchor_field = [&](double* f) {
+    if (!anchor) return;
+    subtract_components(L, comp, ncomp, f);
+    st->unreached_set_mean_projection_count += 1;
+  };
+  anchor_field(rhs0.data());
   if (remove_mean) {
     double mean = weighted_mean(L, obs, rhs0.data(), -1.0);
     st->mean_projection_count += 1;
@@ -566,6 +602,7 @@ EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32
   auto exact_residual = [&]() {
     fv_apply(L, obs, va, vw, iface, pressure, Ad.data(), outlet);
     for (int64_t c = 0; c < n; ++c) r[c] = (obs[c] == 1) ? 0.0 : 1.0 * rhs_cg[c] + -1.0 * Ad[c];
+    anchor_field(r.data());
     if (remove_mean) {
       subtract_mean(L, obs, r.data());
       st->mean_projection_count += 1;
@@ -577,6 +614,7 @@ EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32
   // Initial residual r = b - A p  (fluid.py:6613-6622).
   fv_apply(L, obs, va, vw, iface, pressure, Ad.data(), outlet);
   for (int64_t c = 0; c < n; ++c) r[c] = (obs[c] == 1) ? 0.0 : 1.0 * z[c] + -1.0 * Ad[c];
+  anchor_field(r.data());
   if (remove_mean) {
     subtract_mean(L, obs, r.data());
     st->mean_projection_count += 1;
@@ -602,6 +640,7 @@ EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32
       jacobi_precond(n, obs, diag.data(), r.data(), z.data());
   };
   auto project_z = [&]() {
+    anchor_field(z.data());
     if (remove_mean) {
       subtract_mean(L, obs, z.data());
       st->mean_projection_count += 1;
@@ -645,6 +684,10 @@ EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32
         pressure[c] += alpha * d[c];
         r[c] -= alpha * Ad[c];
       }
+    }
+    if (anchor && it % 16 == 0) {
+      anchor_field(pressure);
+      anchor_field(r.data());
     }
     if (remove_mean && it % 16 == 0) {
       subtract_mean(L, obs, pressure);
@@ -728,6 +771,14 @@ EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32
   }
   st->breakdown_code = code;
   if (st->breakdown_dAd == 0.0) st->breakdown_dAd = code_dAd;
+}
+
+EFO_API void efo_fv_pcg_solve(int n_levels, const efo_level* levels, const int32_t* obs, const int32_t* va,
+                              const r32* vw, const double* iface, const double* rhs_in, double* pressure,
+                              int outlet, int max_iters_in, double tolerance, int precond, int remove_mean,
+                              int uniform_grid, int iface_active, efo_cg_stats* st) {
+  efo_fv_pcg_solve_anchored(n_levels, levels, obs, va, vw, iface, rhs_in, pressure, outlet, max_iters_in, tolerance,
+                            precond, remove_mean, uniform_grid, iface_active, nullptr, 0, st);
 }
 
 // fluid.py:5992-6083 _solve_pressure_poisson_fv_multigrid (standalone cycles);

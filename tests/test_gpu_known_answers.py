@@ -691,3 +691,89 @@ def test_fv_cg_interface_coupling_applies_multiple_owner_slots():
     assert op[owner] - base[owner] == pytest.approx(15.0, abs=5e-5)
     assert op[n0] - base[n0] == pytest.approx(-8.0, abs=5e-5)
     assert op[n1] - base[n1] == pytest.approx(-7.0, abs=5e-5)
+
+
+def _sealed_cells_solver(cells, sources=None):
+    """(9, 4, 9) unit box, solid except the z-min layer (the outlet) and the
+    given sealed cells; optional volume sources on them."""
+    from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
+
+    s = CartesianFluidSolver(FluidDomainSpec.unit_box(grid_nodes=(9, 4, 9), dt_s=1.0e-3))
+    obs = np.ones((9, 4, 9), np.int32)
+    obs[:, :, 0] = 0
+    for c in cells:
+        obs[c] = 0
+    s.obstacle.from_numpy(obs)
+    if sources:
+        src = np.zeros((9, 4, 9), np.float32)
+        for c, v in sources.items():
+            src[c] = v
+        s.volume_source_s.from_numpy(src)
+    return s
+
+
+# test_core_fluid.py:2277
+def test_fv_cg_anchors_pressure_mean_over_outlet_unreached_set():
+    from easyfsi_b200.fluid import CartesianFluidSolver, FluidDomainSpec
+
+    s = CartesianFluidSolver(FluidDomainSpec.unit_box(grid_nodes=(5, 5, 5), dt_s=1.0e-3))
+    obs = np.zeros((5, 5, 5), np.int32)
+    obs[:, :, 2] = 1
+    s.obstacle.from_numpy(obs)
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 50
+    vel = np.zeros((5, 5, 5, 3), np.float32)
+    vel[2, 2, 4, 0] = 0.4
+    s.velocity.from_numpy(vel)
+    report = s.project(iterations=200, pressure_outlet_zmin=True, pressure_solver="fv_cg", cg_tolerance=1.0e-6)
+    assert report["cg_converged_all"]
+    assert int(report["cg_unreached_set_mean_projection_count"]) >= 1
+
+
+# test_core_fluid.py:2306
+def test_fv_cg_anchors_multiple_disconnected_components_independently():
+    s = _sealed_cells_solver([(2, 2, 4), (2, 2, 5), (6, 2, 6)],
+                             {(2, 2, 4): 1.0, (2, 2, 5): 3.0, (6, 2, 6): -2.0})
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 3
+    assert s.last_hibm_pressure_unreached_component_count == 2
+    assert not s.last_hibm_pressure_unreached_component_overflow
+    report = s.project(iterations=200, pressure_outlet_zmin=True, pressure_solver="fv_cg", cg_tolerance=1.0e-6)
+    assert report["cg_converged_all"]
+    assert int(report["cg_unreached_component_count"]) == 2
+    assert int(report["cg_unreached_set_mean_projection_count"]) >= 1
+
+
+# test_core_fluid.py:2344
+def test_fv_cg_reports_unreached_component_rhs_incompatibility():
+    s = _sealed_cells_solver([(2, 2, 4), (2, 2, 5), (6, 2, 6)],
+                             {(2, 2, 4): 1.0, (2, 2, 5): 3.0, (6, 2, 6): -2.0})
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 3
+    report = s.project(iterations=200, pressure_outlet_zmin=True, pressure_solver="fv_cg", cg_tolerance=1.0e-6)
+    assert report["cg_converged_all"]
+    assert not report["pressure_solve_failed"]
+    assert report["pressure_projection_physical_failure"]
+    assert report["pressure_projection_physical_failure_reason"] == "unreached_component_rhs_incompatible"
+    assert int(report["hibm_unreached_incompatible_component_count"]) == 2
+    assert float(report["hibm_unreached_component_rhs_mean_max_abs"]) > 0.0
+
+
+# test_core_fluid.py:2386
+def test_fv_cg_raises_on_unreached_component_rhs_incompatibility():
+    s = _sealed_cells_solver([(2, 2, 4), (2, 2, 5)], {(2, 2, 4): 1.0, (2, 2, 5): 3.0})
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 2
+    with pytest.raises(RuntimeError, match="unreached component RHS is incompatible"):
+        s.project(iterations=200, pressure_outlet_zmin=True, pressure_solver="fv_cg", cg_tolerance=1.0e-6,
+                  pressure_solve_failure_policy="raise")
+
+
+# test_core_fluid.py:2415
+def test_final_divergence_report_excludes_anchored_unreached_cells():
+    s = _sealed_cells_solver([(2, 2, 4), (2, 2, 5), (6, 2, 6)],
+                             {(2, 2, 4): 1.0, (2, 2, 5): 3.0, (6, 2, 6): -2.0})
+    assert s.mark_hibm_pressure_outlet_disconnected_nonprojectable_cells(pressure_outlet_zmin=True) == 3
+    residual = s.divergence_residual_stats(interior_only=True)
+    _raw, final, _int_raw, final_int = s.final_divergence_report_stats(pressure_outlet_zmin=True)
+    assert residual["l2"] == pytest.approx(0.0, abs=1e-12)
+    assert final["l2"] == pytest.approx(0.0, abs=1e-12)
+    assert final_int["l2"] == pytest.approx(0.0, abs=1e-12)
+    assert int(s.last_unreached_divergence_stats["count"]) == 3
+    assert float(s.last_unreached_divergence_stats["l2"]) > 1.0

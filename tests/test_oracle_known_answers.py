@@ -1171,3 +1171,43 @@ def test_bicgstab_fallback_solves_a_generic_rhs():
     # the recurrence agrees with the true residual of the returned pressure
     res = rhs - fl.fv_apply(np.asarray(fl.pressure), 1)
     assert math.sqrt(fl.weighted_dot(res, res)) / b_norm <= 1.0e-7
+
+
+# test_core_fluid.py:2277-2342 (the anchoring the reference's outlet solves
+# apply to flood-unreached components): two sealed pockets make the outlet
+# system singular; with each pocket's mean subtracted where fluid.py:6567-6789
+# does it, the PCG converges and leaves each pocket's pressure with zero mean,
+# while the same PCG without the anchoring does not converge.
+@pytest.mark.parametrize("precond", [0, 1])
+def test_anchored_outlet_pcg_converges_on_sealed_pockets(precond):
+    n = (12, 10, 16)
+    grid = CartesianGrid(bounds_min_m=(0.0, 0.0, 0.0),
+                         cell_widths_x_m=graded_axis_widths(n[0], 0.0, 1.0, 0.3, 0.7),
+                         cell_widths_y_m=graded_axis_widths(n[1], 0.0, 1.0, 0.3, 0.7),
+                         cell_widths_z_m=graded_axis_widths(n[2], 0.0, 1.0, 0.2, 0.8))
+    obs = np.zeros(grid.grid_nodes, np.int32)
+    for (i0, j0, k0, m) in ((1, 1, 4, 4), (6, 5, 9, 5)):
+        obs[i0:i0 + m, j0:j0 + m, k0:k0 + m] = 1
+        obs[i0 + 1:i0 + m - 1, j0 + 1:j0 + m - 1, k0 + 1:k0 + m - 1] = 0
+    reach = orc.outlet_reachability(obs)
+    assert reach["unreached"] == 2 ** 3 + 3 ** 3 and reach["components"] == 2
+    label = reach["label"]
+    comp = np.where((obs == 0) & (reach["reachable"] == 0) & (label < 0), -label - 1, -1).astype(np.int32)
+    div = np.random.default_rng(5).normal(size=grid.grid_nodes).astype(np.float32)
+    runs = {}
+    for anchored in (True, False):
+        ofl = orc.OracleFluid(grid, rho=1000.0, mu=1.0e-3, variant="mirror")
+        ofl.obstacle[...] = obs
+        ofl.divergence[...] = div
+        ofl.pressure[...] = 0.0
+        ofl.prepare_rhs(1.0e6)
+        st = ofl.pcg_solve(outlet=1, max_iters=300, tol=1e-10, precond=precond, remove_mean=False,
+                           components=comp if anchored else None, component_count=2)
+        runs[anchored] = (st, ofl.pressure.copy(), ofl)
+    st, p, ofl = runs[True]
+    assert st.converged and st.unreached_set_mean_projection_count > 0
+    assert not runs[False][0].converged
+    vol = np.einsum("i,j,k->ijk", *[np.asarray(m["w"], np.float32).astype(np.float64) for m in ofl.metrics[0]])
+    for c in range(2):
+        on = comp == c
+        assert abs((p * vol)[on].sum() / vol[on].sum()) <= 1e-10 * np.abs(p).max()
