@@ -39,6 +39,7 @@ class PcgParams(Structure):
         ("iface_active", c_int32),
         ("use_graphs", c_int32),
         ("tolerance", c_double),
+        ("device_loop", c_int32),
     ]
 
 

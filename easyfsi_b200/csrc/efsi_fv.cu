@@ -938,6 +938,7 @@ struct CoarseDesc {
   float* rhs[kTailMaxLevels];
   unsigned* bar;  // [0] arrivals, [1] generation
   int* fault;
+  unsigned spin_ns;  // back-off between polls of the generation (0: none)
 };
 
 constexpr long long kCoarseWaitLimit = 4000000000LL;  // ~2 s of clock64
@@ -964,6 +965,7 @@ __device__ bool coarse_barrier(const CoarseDesc& D) {
     } else {
       const long long t0 = clock64();
       while (ld_acquire_u32(gen) == g) {
+        if (D.spin_ns > 0) __nanosleep(D.spin_ns);
         if (clock64() - t0 > kCoarseWaitLimit) {
           ok = 0;
           break;
@@ -1917,9 +1919,11 @@ static void configure_tail(efsi_fv_plan* P) {
 // GPU at once (at most two per SM), each with the tail's shared memory.
 static void configure_coarse(efsi_fv_plan* P) {
   P->coarse_blocks = 0;
-  const bool off = std::getenv("EFSI_NO_COARSE_KERNEL") != nullptr;
-  if (off) {
-    P->coarse_note = "EFSI_NO_COARSE_KERNEL is set";
+  // opt-in (EFSI_COARSE_KERNEL=1): on a B200 the per-level launches measured
+  // faster (c2: 94 us against 143 us per V-cycle for levels 1-6)
+  const char* on = std::getenv("EFSI_COARSE_KERNEL");
+  if (on == nullptr || std::atoi(on) == 0 || std::getenv("EFSI_NO_COARSE_KERNEL") != nullptr) {
+    P->coarse_note = "the cooperative coarse-level kernel is off (EFSI_COARSE_KERNEL=1 selects it)";
     return;
   }
   if (P->tail_level < 2 || P->tail_level >= P->n_levels) {
@@ -1967,7 +1971,9 @@ static void configure_coarse(efsi_fv_plan* P) {
     P->coarse_note = "cannot allocate the grid barrier";
     return;
   }
-  P->coarse_blocks = std::min(per_sm, 2) * sms;
+  int want = 2;
+  if (const char* env = std::getenv("EFSI_COARSE_BLOCKS_PER_SM")) want = std::max(1, std::atoi(env));
+  P->coarse_blocks = std::min(per_sm, want) * sms;
   P->coarse_note = "";
 }
 }  // namespace efsi
@@ -2667,6 +2673,8 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       }
       D.bar = P->coarse_bar;
       D.fault = &P->sc->fault;
+      static const unsigned spin_ns = std::getenv("EFSI_COARSE_SPIN_NS") ? (unsigned)std::atoi(std::getenv("EFSI_COARSE_SPIN_NS")) : 0u;
+      D.spin_ns = spin_ns;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeCooperative;
       attr[0].val.cooperative = 1;

@@ -50,6 +50,10 @@ struct CgScalars {
   double rz, rz_new, dAd, rr, beta_num, alpha, beta;
   double mean_z, mean_x, mean_r, mean_b, free_vol, bnorm2, code_dAd, dot;
   double learned_num;  // <r', n>_V of the learned coarse correction (its 1-D Galerkin scale)
+  // device-side loop (efsi_pcg_params::device_loop): iterations done, the
+  // relative residuals, b_norm, converged flag
+  double dl_bnorm, dl_rel0, dl_rel;
+  int dl_iter, dl_converged;
   int code;
   int zproj;  // 1: consumers of z apply the zero-mean projection on the fly
   unsigned ticket;

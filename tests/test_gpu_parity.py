@@ -372,12 +372,23 @@ def test_march_kernels_match_per_cell_kernels(n, aux):
 @pytest.mark.parametrize("n,aux", [((40, 24, 48), False), ((64, 48, 96), False), ((64, 48, 96), True)])
 def test_coarse_kernel_matches_per_level_launches(n, aux):
     """The cooperative coarse-level kernel (levels 1 .. lt-1 and the tail in
-    one launch) reproduces the per-level launches: the same rows in the same
-    order, so the V-cycle agrees bit for bit and the PCG takes the same path;
-    it replaces the coarse launches of every V-cycle."""
+    one launch; opt-in, EFSI_COARSE_KERNEL=1) reproduces the per-level
+    launches: the same rows in the same order, so the V-cycle agrees bit for
+    bit and the PCG takes the same path; it replaces the coarse launches of
+    every V-cycle."""
     from easyfsi_b200 import _native
 
-    grid, (fk, fl_) = _paired_solvers(n, aux, alt_env={"EFSI_NO_COARSE_KERNEL": "1"})
+    import os
+
+    saved = os.environ.get("EFSI_COARSE_KERNEL")
+    os.environ["EFSI_COARSE_KERNEL"] = "1"
+    try:
+        grid, (fk, fl_) = _paired_solvers(n, aux, alt_env={"EFSI_NO_COARSE_KERNEL": "1"})
+    finally:
+        if saved is None:
+            os.environ.pop("EFSI_COARSE_KERNEL", None)
+        else:
+            os.environ["EFSI_COARSE_KERNEL"] = saved
     blocks, notes = [], []
     for fl in (fk, fl_):
         b = ctypes.c_int32(0)
