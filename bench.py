@@ -333,6 +333,55 @@ def learned_arm(scene, steps: int, warmup: int, world: int, plain_value: float, 
     }
 
 
+def graph_step_arm(scene, steps: int, warmup: int, world: int, plain_value: float) -> dict:
+    """The coupled step captured as one CUDA graph (efsi_step_graph_*): the
+    pressure solve runs its device-side loop (a WHILE node of 16-iteration
+    bodies that stops on the residual test), so the step makes no host reads;
+    each timed step is one graph launch.  The statistics of the last step's
+    solve are read after the timed region."""
+    import torch
+    import torch.distributed as dist
+
+    from easyfsi_b200.runtime import StepGraph
+
+    stream = torch.cuda.current_stream()
+    fl = scene.fluid
+    fl.device_loop_solves = True
+    graph = StepGraph()
+    try:
+        scene.step()  # eager, with the device-side loop
+        torch.cuda.synchronize()
+        graph.capture(scene.step)
+        torch.cuda.synchronize()
+        for _ in range(max(1, warmup)):
+            graph.launch()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            graph.launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        fl.read_device_pcg_stats()
+        value = replica_steps_per_s(world, steps, max_over_ranks(e0.elapsed_time(e1), world, "cuda"))
+        return {
+            "value": value,
+            "unit": "steps/s",
+            "ratio_to_fv_multigrid": value / plain_value,
+            "graph": "whole coupled step as one CUDA graph; PCG as a device-side WHILE loop of 16-iteration bodies",
+            "last_cg_iterations": int(fl.last_cg_iterations),
+            "last_cg_converged": bool(fl.last_cg_converged),
+            "last_relative_residual": float(fl.last_cg_relative_residual),
+        }
+    finally:
+        graph.close()
+        fl.device_loop_solves = False
+
+
 def max_over_ranks(ms: float, world: int, device) -> float:
     """Largest per-rank time over all ranks (every rank calls this in the same
     order; a no-op for one rank)."""
@@ -417,6 +466,7 @@ def main() -> None:
     ap.add_argument("--cpu-warmup", type=int, default=1)
     ap.add_argument("--no-family-timing", action="store_true", help="skip the MPM / HIBM kernel-family timing pass")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
+    ap.add_argument("--no-graph-step", action="store_true", help="skip the whole-step CUDA graph arm")
     ap.add_argument("--learned-train-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-reps", type=int, default=50)
@@ -528,6 +578,15 @@ def main() -> None:
             "ratio_to_fv_multigrid": m_value / value,
         }
         scene.preconditioner = "fv_multigrid"
+
+    # --- the same coupled step captured whole as one CUDA graph (device-side
+    # PCG loop, no host reads), replayed once per step ---
+    graph_step = None
+    if not args.no_graph_step:
+        try:
+            graph_step = graph_step_arm(scene, args.steps, args.warmup, world, value)
+        except Exception as exc:  # reported, never fatal to the step's line
+            graph_step = {"error": f"{type(exc).__name__}: {exc}"}
 
     # --- the IB node search on the same grid and markers (not part of the step) ---
     ib_search = None
@@ -683,6 +742,7 @@ def main() -> None:
             "solve_iterations": solve_iters,
             "cg_iterations_mean": float(np.mean(iters)) if iters else None,
             "mixed_precision": mixed,
+            "graph_step": graph_step,
             "learned": learned,
             "particle_families": particle_families,
             "kernel_families": fam_stats,

@@ -233,6 +233,11 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_fv_learned_input": [P, P, P, P],
     "efsi_fv_learned_presmooth": [P, P, P, I, P],
     "efsi_fv_coarse_kernel_blocks": [P, POINTER(c_int32)],
+    "efsi_fv_pcg_device_stats": [P, POINTER(CgStats), P],
+    "efsi_step_graph_begin": [P],
+    "efsi_step_graph_end": [P, POINTER(c_void_p)],
+    "efsi_step_graph_launch": [P, P],
+    "efsi_step_graph_destroy": [P],
     "efsi_fv_set_unreached_components": [P, P, I, P],
     "efsi_divergence_final_report": [P, P, P, P, P, P, I, P, P],
     "efsi_fv_subtract_unreached_means": [P, P, P, P, P],

@@ -1536,6 +1536,61 @@ __global__ void __launch_bounds__(256) k_comp_subtract(LevelDev L, double* __res
   if (vol > 0.0) f[c] -= acc[cc] / vol;
 }
 
+// Device-side PCG loop (efsi_pcg_params::device_loop).  k_dl_init runs
+// after the initial residual and preconditioner: b_norm, the initial
+// relative residual, beta = 0 (the first direction is z), and whether the
+// loop body runs at all; k_dl_check ends every 16-iteration body: the
+// relative residual of the last update, and whether to go on (not
+// converged, no breakdown or fault, and another 16 iterations within
+// max_iters).
+__global__ void k_dl_init(CgScalars* sc, double tol, cudaGraphConditionalHandle h) {
+  pdl_wait();
+  if (threadIdx.x != 0) return;
+  const double bn = sqrt(fmax(sc->bnorm2, 0.0));
+  sc->dl_bnorm = bn;
+  sc->dl_iter = 0;
+  sc->dl_converged = 0;
+  unsigned go = 0;
+  if (bn <= 1.0e-30) {
+    sc->dl_converged = 1;
+    sc->dl_rel0 = sc->dl_rel = 0.0;
+  } else {
+    const double rel = sqrt(fmax(sc->rr, 0.0)) / bn;
+    sc->dl_rel0 = sc->dl_rel = rel;
+    if (rel <= tol)
+      sc->dl_converged = 1;
+    else if (!(isfinite(sc->rz) && sc->rz > 0.0))
+      sc->code = 2;
+    else
+      go = 1;
+  }
+  sc->beta = 0.0;
+  cudaGraphSetConditional(h, go);
+}
+
+__global__ void k_dl_zero_if_tiny(LevelDev L, double* __restrict__ pressure, const CgScalars* sc) {
+  pdl_wait();
+  EFSI_CELL_PROLOGUE(L)
+  if (active && !(sqrt(fmax(sc->bnorm2, 0.0)) > 1.0e-30)) pressure[c] = 0.0;
+}
+
+__global__ void k_dl_check(CgScalars* sc, double tol, int max_iters, cudaGraphConditionalHandle h) {
+  pdl_wait();
+  if (threadIdx.x != 0) return;
+  const int it = sc->dl_iter + 16;
+  sc->dl_iter = it;
+  const double rel = sqrt(fmax(sc->rr, 0.0)) / sc->dl_bnorm;
+  sc->dl_rel = rel;
+  unsigned go = 1;
+  if (rel <= tol) {
+    sc->dl_converged = 1;
+    go = 0;
+  } else if (sc->code != 0 || sc->fault != 0 || !isfinite(rel) || it + 16 > max_iters) {
+    go = 0;
+  }
+  cudaGraphSetConditional(h, go);
+}
+
 // fluid.py:4677-4693 with multiplier -1 on the level-0 rhs, plus the free
 // volume (computed in the same pass as the reference does).
 __global__ void __launch_bounds__(256) k_rhs_mean(LevelDev L, const double* __restrict__ rhs, double multiplier,
@@ -1715,9 +1770,13 @@ unsigned long long take_capture_count() {
   g_capture_count = 0;
   return v;
 }
+namespace {
+thread_local bool g_pdl_suppressed = false;
+}
+void set_pdl_suppressed(bool on) { g_pdl_suppressed = on; }
 bool pdl_enabled() {
   static const bool on = std::getenv("EFSI_NO_PDL") == nullptr;
-  return on;
+  return on && !g_pdl_suppressed;
 }
 
 namespace {
@@ -2131,6 +2190,7 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   for (PcgGraph& g : P->graphs) cudaGraphExecDestroy(g.exec);
   P->graphs.clear();
   if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
+  if (P->body_stream) cudaStreamDestroy(P->body_stream);
   for (LevelBuf& B : P->lv) {
     cudaFree(B.coef);
     cudaFree(B.mask);
@@ -2862,6 +2922,129 @@ static int precondition(PcgRun& R) {
 
 }  // namespace efsi
 
+namespace efsi {
+
+// Appends to the capture in progress on `cs`: the pressure reset of a zero
+// right-hand side, k_dl_init, and a WHILE node whose body (captured on the
+// plan's body stream) is one 16-iteration block plus k_dl_check.  Inside the
+// body the launches go without PDL and the V-cycle uses its per-level
+// launches.
+template <class Body>
+static int build_device_loop(efsi_fv_plan* P, cudaStream_t cs, double* pressure, double tol, int max_iters, Body body) {
+  cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+  unsigned long long id = 0;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  EFSI_CUDA_CHECK(cudaStreamGetCaptureInfo(cs, &status, &id, &g, &deps, &nd));
+  EFSI_ARG_CHECK(status == cudaStreamCaptureStatusActive && g != nullptr, "the device-side loop needs a capturing stream");
+  cudaGraphConditionalHandle h;
+  EFSI_CUDA_CHECK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  const LevelDev L0 = level_dev(P, 0);
+  const Shape3& S0 = P->lv[0].shape;
+  EFSI_COUNTED k_dl_zero_if_tiny<<<S0.grid, S0.block, 0, cs>>>(L0, pressure, (const CgScalars*)P->sc);
+  EFSI_COUNTED k_dl_init<<<1, 32, 0, cs>>>(P->sc, tol, h);
+  EFSI_CUDA_CHECK(cudaGetLastError());
+  EFSI_CUDA_CHECK(cudaStreamGetCaptureInfo(cs, &status, &id, &g, &deps, &nd));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  EFSI_CUDA_CHECK(cudaGraphAddNode(&node, g, deps, nd, &cp));
+  cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+  EFSI_CUDA_CHECK(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+  if (P->body_stream == nullptr) EFSI_CUDA_CHECK(cudaStreamCreateWithFlags(&P->body_stream, cudaStreamNonBlocking));
+  EFSI_CUDA_CHECK(cudaStreamBeginCaptureToGraph(P->body_stream, bodyg, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal));
+  const int keep_blocks = P->coarse_blocks;
+  P->coarse_blocks = 0;
+  set_pdl_suppressed(true);
+  int rc = body(P->body_stream);
+  EFSI_COUNTED k_dl_check<<<1, 32, 0, P->body_stream>>>(P->sc, tol, max_iters, h);
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(P->body_stream, &out);
+  set_pdl_suppressed(false);
+  P->coarse_blocks = keep_blocks;
+  if (rc != EFSI_OK) return rc;
+  if (e != cudaSuccess) {
+    set_error(std::string("capturing the device-side PCG loop body: ") + cudaGetErrorString(e));
+    return EFSI_ERR_CUDA;
+  }
+  return EFSI_OK;
+}
+
+static void fill_device_stats(efsi_fv_plan* P, efsi_cg_stats* st) {
+  const CgScalars* h = P->host_sc;
+  st->iterations = h->dl_iter;
+  st->converged = h->dl_converged;
+  st->breakdown_code = h->code;
+  st->breakdown_dAd = h->code_dAd;
+  st->initial_relative_residual = h->dl_rel0;
+  st->relative_residual = h->dl_rel;
+  st->b_norm = h->dl_bnorm;
+  st->used_mg = P->dl_used_mg;
+  st->used_graphs = 1;
+}
+
+// The device-side loop after the preamble: inside the caller's stream
+// capture, or as a graph of its own that is launched and waited for.
+template <class Body>
+static int pcg_device_loop(efsi_fv_plan* P, PcgRun& R, efsi_cg_stats* st, cudaStream_t s, double* pressure,
+                           double tol, int max_iters, int64_t n0, Body body) {
+  EFSI_CUDA_CHECK(cudaMemsetAsync(P->d0, 0, n0 * sizeof(double), s));
+  EFSI_CUDA_CHECK(cudaMemsetAsync(P->d1, 0, n0 * sizeof(double), s));
+  P->dl_used_mg = R.use_mg ? 1 : 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  EFSI_CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
+  if (cs == cudaStreamCaptureStatusActive) {
+    EFSI_TRY(build_device_loop(P, s, pressure, tol, max_iters, body));
+    st->converged = -1;  // read later with efsi_fv_pcg_device_stats
+    st->used_mg = P->dl_used_mg;
+    st->used_graphs = 1;
+    return EFSI_OK;
+  }
+  // a graph of its own, ordered after the preamble by its launch on s
+  EFSI_CUDA_CHECK(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal));
+  set_capturing(true);
+  take_capture_count();
+  int rc = build_device_loop(P, P->cap_stream, pressure, tol, max_iters, body);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(P->cap_stream, &g);
+  set_capturing(false);
+  const unsigned long long nodes = take_capture_count();
+  cudaGraphExec_t ex = nullptr;
+  if (rc == EFSI_OK && e == cudaSuccess) {
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    if (ei != cudaSuccess) {
+      set_error(std::string("instantiating the device-side PCG loop: ") + cudaGetErrorString(ei));
+      rc = EFSI_ERR_CUDA;
+    }
+  } else if (rc == EFSI_OK) {
+    set_error(std::string("capturing the device-side PCG loop: ") + cudaGetErrorString(e));
+    rc = EFSI_ERR_CUDA;
+  }
+  if (g != nullptr) cudaGraphDestroy(g);
+  if (rc != EFSI_OK) {
+    cudaGetLastError();
+    return rc;
+  }
+  EFSI_CUDA_CHECK(cudaGraphLaunch(ex, s));
+  count_graph_launch(nodes);
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(P->host_sc, P->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  cudaGraphExecDestroy(ex);
+  if (P->host_sc->fault) {
+    set_error("a plane-marching kernel's TMA stage did not complete in time");
+    return EFSI_ERR_CUDA;
+  }
+  fill_device_stats(P, st);
+  return EFSI_OK;
+}
+
+}  // namespace efsi
+
 extern "C" {
 
 int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, const efsi_pcg_params* prm,
@@ -2886,6 +3069,10 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   st->relative_residual = INFINITY;
   const int outlet = prm->outlet;
   const bool remove_mean = prm->remove_mean != 0;
+  // device_loop: no host reads; the loop runs on the device (WHILE node)
+  const bool device = prm->device_loop != 0;
+  EFSI_ARG_CHECK(!device || (prm->precond != 4 && prm->precond != 5),
+                 "the device-side loop does not take the learned preconditioner (its fallback is a host decision)");
   EFSI_COUNTED k_reset_scalars<<<1, 32, 0, s>>>(P->sc);
   const bool coupled = P->cpl_nrows > 0;
   if (coupled) EFSI_COUNTED k_set_defer<<<1, 32, 0, s>>>(P->sc, 1);
@@ -2898,11 +3085,11 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   if (R.anchor) st->unreached_set_mean_projection_count += 1;
   EFSI_COUNTED k_build_b<<<R.S.grid, R.S.block, 0, s>>>(R.L, rhs0, remove_mean ? 1 : 0, P->b, P->partials, P->sc);
   EFSI_LAUNCH_CHECK();
-  EFSI_TRY(read_scalars(R));
-  const double b_norm = std::sqrt(std::max(P->host_sc->bnorm2, 0.0));
+  if (!device) EFSI_TRY(read_scalars(R));
+  const double b_norm = device ? 1.0 : std::sqrt(std::max(P->host_sc->bnorm2, 0.0));
   st->b_norm = b_norm;
   const int64_t n0 = P->lv[0].n;
-  if (b_norm <= 1.0e-30) {
+  if (!device && b_norm <= 1.0e-30) {
     EFSI_CUDA_CHECK(cudaMemsetAsync(pressure, 0, n0 * sizeof(double), s));
     st->initial_relative_residual = 0.0;
     st->relative_residual = 0.0;
@@ -2930,15 +3117,16 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       st->mean_projection_count += 1;
     }
     EFSI_LAUNCH_CHECK();
+    if (device) return EFSI_OK;
     EFSI_TRY(read_scalars(R));
     st->host_residual_checks += 1;
     return EFSI_OK;
   };
   EFSI_TRY(true_residual());
-  double r_norm = std::sqrt(std::max(P->host_sc->rr, 0.0));
+  double r_norm = device ? 1.0 : std::sqrt(std::max(P->host_sc->rr, 0.0));
   st->initial_relative_residual = r_norm / b_norm;
   st->relative_residual = st->initial_relative_residual;
-  if (r_norm <= tol * b_norm) {
+  if (!device && r_norm <= tol * b_norm) {
     st->converged = 1;
     return EFSI_OK;
   }
@@ -2968,8 +3156,8 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   if (R.anchor) st->unreached_set_mean_projection_count += 1;
   EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
   EFSI_LAUNCH_CHECK();
-  EFSI_TRY(read_scalars(R));
-  double rz = P->host_sc->rz;
+  if (!device) EFSI_TRY(read_scalars(R));
+  double rz = device ? 1.0 : P->host_sc->rz;
   if (R.learned && learned_fallback && (!std::isfinite(rz) || rz <= 0.0)) {
     // the network's first z is not a descent direction: the V-cycle takes over
     R.learned = false;
@@ -3163,6 +3351,26 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     count_graph_launch(nodes_now);
     return EFSI_OK;
   };
+  if (device) return pcg_device_loop(P, R, st, s, pressure, tol, max_iters, n0, [&](cudaStream_t bs) -> int {
+    // one iteration block of the loop body: 16 x (direction + SpMV + alpha,
+    // update, preconditioner + dots for the next one), as launch_block does
+    // after its first iteration
+    const cudaStream_t keep = s;
+    s = bs;
+    R.s = bs;
+    double* d[2] = {P->d0, P->d1};
+    int rc = EFSI_OK;
+    for (int j = 0; j < 16 && rc == EFSI_OK; ++j) {
+      launch_spmv(false, d[j & 1], d[(j + 1) & 1]);
+      const bool last = (j == 15);
+      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean && !R.anchor);
+      if (last && R.anchor) anchor_pressure_residual(true);
+      rc = launch_precond_dots();
+    }
+    s = keep;
+    R.s = keep;
+    return rc;
+  });
   bool pending = false;  // preconditioner + dots of the previous iteration not launched yet
   int n_precond = 0;     // preconditioner applications inside the loop
   int it = 1;
@@ -3746,6 +3954,81 @@ int efsi_fv_learned_presmooth(efsi_fv_plan* P, const double* r, double* z, int32
 }  // extern "C"
 
 extern "C" const char* efsi_fv_graph_error(efsi_fv_plan* P) { return P ? P->graph_error.c_str() : ""; }
+
+extern "C" int efsi_fv_pcg_device_stats(efsi_fv_plan* P, efsi_cg_stats* st, void* stream) {
+  EFSI_ARG_CHECK(P != nullptr && st != nullptr, "null argument");
+  cudaStream_t s = as_stream(stream);
+  EFSI_CUDA_CHECK(cudaMemcpyAsync(P->host_sc, P->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  EFSI_CUDA_CHECK(cudaStreamSynchronize(s));
+  std::memset(st, 0, sizeof(*st));
+  if (P->host_sc->fault) {
+    set_error("a plane-marching kernel's TMA stage did not complete in time");
+    return EFSI_ERR_CUDA;
+  }
+  fill_device_stats(P, st);
+  return EFSI_OK;
+}
+
+// Whole-step graphs: everything the library launches on `stream` between
+// begin and end is captured (the caller's stream must not be the legacy
+// default stream); launch replays it.
+struct efsi_step_graph {
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long nodes = 0;
+};
+
+extern "C" int efsi_step_graph_begin(void* stream) {
+  cudaStream_t s = as_stream(stream);
+  EFSI_ARG_CHECK(s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread,
+                 "a step graph is captured on a created stream, not the default stream");
+  EFSI_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  set_capturing(true);
+  take_capture_count();
+  return EFSI_OK;
+}
+
+extern "C" int efsi_step_graph_end(void* stream, efsi_step_graph** out) {
+  EFSI_ARG_CHECK(out != nullptr, "null output");
+  *out = nullptr;
+  cudaStream_t s = as_stream(stream);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  set_capturing(false);
+  const unsigned long long nodes = take_capture_count();
+  if (e != cudaSuccess) {
+    if (g != nullptr) cudaGraphDestroy(g);
+    cudaGetLastError();
+    set_error(std::string("step graph capture: ") + cudaGetErrorString(e));
+    return EFSI_ERR_CUDA;
+  }
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("step graph instantiation: ") + cudaGetErrorString(ei));
+    return EFSI_ERR_CUDA;
+  }
+  efsi_step_graph* G = new efsi_step_graph();
+  G->exec = ex;
+  G->nodes = nodes;
+  *out = G;
+  return EFSI_OK;
+}
+
+extern "C" int efsi_step_graph_launch(efsi_step_graph* G, void* stream) {
+  EFSI_ARG_CHECK(G != nullptr && G->exec != nullptr, "null step graph");
+  EFSI_CUDA_CHECK(cudaGraphLaunch(G->exec, as_stream(stream)));
+  count_graph_launch(G->nodes);
+  return EFSI_OK;
+}
+
+extern "C" int efsi_step_graph_destroy(efsi_step_graph* G) {
+  if (G == nullptr) return EFSI_OK;
+  if (G->exec != nullptr) cudaGraphExecDestroy(G->exec);
+  delete G;
+  return EFSI_OK;
+}
 
 extern "C" int efsi_fv_coarse_kernel_blocks(efsi_fv_plan* P, int32_t* blocks) {
   EFSI_ARG_CHECK(P != nullptr && blocks != nullptr, "null argument");

@@ -292,6 +292,8 @@ struct efsi_fv_plan {
   const int32_t* obstacle0 = nullptr;  // caller's level-0 obstacle (legacy Jacobi)
   std::vector<PcgGraph> graphs;        // instantiated 16-iteration PCG blocks
   cudaStream_t cap_stream = nullptr;   // private stream used for graph capture
+  cudaStream_t body_stream = nullptr;  // captures the body of the device-side PCG loop
+  int dl_used_mg = 0;                  // preconditioner kind of the last device-side loop
   bool graphs_disabled = false;        // a capture failed; blocks run as direct launches
   int tail_level = 1 << 30;            // first level run by the single-CTA V-cycle tail
   size_t tail_smem_bytes = 0;

@@ -72,8 +72,8 @@ struct efsi_mpm_plan {
   int32_t* active = nullptr;     // ntiles + 1 tile ids
   uint8_t* reached_flag = nullptr;  // ntiles
   int32_t* reached[2] = {nullptr, nullptr};  // ntiles tile ids: this step's and the previous step's
-  int32_t* counts = nullptr;     // [0] active, [1] reached now, [2] reached in the previous step
-  int cur = 0;                   // which reached list is this step's
+  int32_t* counts = nullptr;     // [0] active, [1] reached now, [2] reached in the previous step,
+                                 // [3] which reached list is this step's (flipped on the device)
 };
 
 namespace efsi {
@@ -335,10 +335,33 @@ __device__ __forceinline__ void block_max(double* acc, int slot, double v) {
 
 // Lists of the occupied tiles (+ the out-of-stencil bucket when it holds
 // particles) and of the reached tiles.
+// The two reached-tile lists alternate between steps by a device-side parity
+// (counts[3]), so a captured step replays with the same arguments:
+// counts[0] occupied tiles, [1] this step's reached tiles, [2] the previous
+// step's, [3] which of reached0 / reached1 is this step's list.
+__device__ __forceinline__ int32_t* reached_now(int32_t* r0, int32_t* r1, const int32_t* counts) {
+  return counts[3] ? r1 : r0;
+}
+__device__ __forceinline__ int32_t* reached_before(int32_t* r0, int32_t* r1, const int32_t* counts) {
+  return counts[3] ? r0 : r1;
+}
+
+// Start of a step: the previous step's count moves to counts[2], the parity
+// flips, the new counts start at zero.
+__global__ void k_reached_flip(int32_t* counts) {
+  if (threadIdx.x == 0) {
+    counts[2] = counts[1];
+    counts[3] ^= 1;
+    counts[0] = 0;
+    counts[1] = 0;
+  }
+}
+
 __global__ void k_tile_lists(int ntiles, const int32_t* __restrict__ count, const uint8_t* __restrict__ reached_flag,
-                             int32_t* active, int32_t* reached, int32_t* counts) {
+                             int32_t* active, int32_t* reached0, int32_t* reached1, int32_t* counts) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t > ntiles) return;
+  int32_t* reached = reached_now(reached0, reached1, counts);
   if (count[t] > 0) active[atomicAdd(counts, 1)] = t;
   if (t < ntiles && reached_flag[t]) reached[atomicAdd(counts + 1, 1)] = t;
 }
@@ -353,9 +376,11 @@ __device__ __forceinline__ bool tile_node(const efsi_mpm_state& S, int tile, int
 
 // Zeroes mass, momentum and force of the nodes of the tiles reached in this
 // step and in the previous one (one warp-pair per tile, 64 nodes).
-__global__ void __launch_bounds__(256) k_clear_reached(efsi_mpm_state S, int ty, int tz, const int32_t* now,
-                                                       const int32_t* before, const int32_t* counts) {
+__global__ void __launch_bounds__(256) k_clear_reached(efsi_mpm_state S, int ty, int tz, int32_t* reached0,
+                                                       int32_t* reached1, const int32_t* counts) {
   const int n_now = counts[1], n_before = counts[2];
+  const int32_t* now = reached_now(reached0, reached1, counts);
+  const int32_t* before = reached_before(reached0, reached1, counts);
   const int per_block = 256 / kTileCells;
   for (int w = blockIdx.x * per_block + threadIdx.x / kTileCells; w < n_now + n_before; w += gridDim.x * per_block) {
     const int tile = w < n_now ? now[w] : before[w - n_now];
@@ -607,10 +632,12 @@ __global__ void __launch_bounds__(kP2gThreads) k_p2g(efsi_mpm_state S, int tx, i
 // Grid update (neo_hookean_mpm.py:803-817).
 // Only the nodes of the reached tiles can carry mass; the rest of the grid is
 // zero (k_clear_reached).
-__global__ void __launch_bounds__(256) k_grid_update(efsi_mpm_state S, int ty, int tz, const int32_t* reached,
-                                                     const int32_t* counts, float dt, float damping, double* acc) {
+__global__ void __launch_bounds__(256) k_grid_update(efsi_mpm_state S, int ty, int tz, int32_t* reached0,
+                                                     int32_t* reached1, const int32_t* counts, float dt,
+                                                     float damping, double* acc) {
   double t0 = 0, t1 = 0, t2 = 0, m0 = 0, m1 = 0, m2 = 0, act = 0, spd = 0;
   const int n_reached = counts[1];
+  const int32_t* reached = reached_now(reached0, reached1, counts);
   const int per_block = 256 / kTileCells;
   for (int w = blockIdx.x * per_block + threadIdx.x / kTileCells; w < n_reached; w += gridDim.x * per_block) {
     int64_t g;
@@ -919,11 +946,7 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
   const bool time_step = timing_enabled(KF_MPM_STEP);
   if (time_step) timing_begin(KF_MPM_STEP, s);
   // the previous step's reached list becomes "before"; this step's is rebuilt
-  int32_t* before = P->reached[P->cur];
-  P->cur ^= 1;
-  int32_t* now = P->reached[P->cur];
-  EFSI_CUDA_CHECK(cudaMemcpyAsync(P->counts + 2, P->counts + 1, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
-  EFSI_CUDA_CHECK(cudaMemsetAsync(P->counts, 0, 2 * sizeof(int32_t), s));
+  EFSI_COUNTED k_reached_flip<<<1, 32, 0, s>>>(P->counts);
   EFSI_CUDA_CHECK(cudaMemsetAsync(P->count, 0, (P->ntiles + 1) * sizeof(int32_t), s));
   EFSI_CUDA_CHECK(cudaMemsetAsync(P->reached_flag, 0, P->ntiles, s));
   if (acc) EFSI_CUDA_CHECK(cudaMemsetAsync(acc, 0, R_COUNT * sizeof(double), s));
@@ -931,8 +954,8 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
   EFSI_COUNTED k_bin_keys<<<pb, 256, 0, s>>>(S, P->tx, P->ty, P->tz, P->ntiles, P->key, P->count, P->reached_flag);
   EFSI_COUNTED k_scan<<<1, 1024, 0, s>>>(P->count, P->ntiles + 1, P->offset, P->cursor);
   EFSI_COUNTED k_tile_lists<<<(P->ntiles + 256) / 256, 256, 0, s>>>(P->ntiles, P->count, P->reached_flag, P->active,
-                                                                     now, P->counts);
-  EFSI_COUNTED k_clear_reached<<<2 * 148, 256, 0, s>>>(S, P->ty, P->tz, now, before, P->counts);
+                                                                     P->reached[0], P->reached[1], P->counts);
+  EFSI_COUNTED k_clear_reached<<<2 * 148, 256, 0, s>>>(S, P->ty, P->tz, P->reached[0], P->reached[1], P->counts);
   EFSI_COUNTED k_bin_scatter<<<pb, 256, 0, s>>>(Pn, P->key, P->offset, P->cursor, P->sorted);
   // P2G: 124 bytes per particle (read x, v, C, F, mass, volume, f_ext, fixed, sorted index)
   EFSI_TIMED(KF_P2G, 124.0 * Pn, s,
@@ -949,7 +972,8 @@ int efsi_mpm_step(efsi_mpm_plan* P, const efsi_mpm_state* Sp, float dt, float mu
     reached_nodes = (double)h * kTileCells;
   }
   EFSI_TIMED(KF_GRID_UPDATE, 40.0 * reached_nodes, s,
-             EFSI_COUNTED k_grid_update<<<2 * 148, 256, 0, s>>>(S, P->ty, P->tz, now, P->counts, dt, velocity_damping,
+             EFSI_COUNTED k_grid_update<<<2 * 148, 256, 0, s>>>(S, P->ty, P->tz, P->reached[0], P->reached[1],
+                                                                P->counts, dt, velocity_damping,
                                                                 acc));
   // G2P: read x, F, fixed, region (56 bytes), write x, v, C, F (96 bytes)
   EFSI_TIMED(KF_G2P, 152.0 * Pn, s,

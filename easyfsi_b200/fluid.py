@@ -489,6 +489,21 @@ class CartesianFluidSolver:
         _native.call("efsi_fv_set_learned_preconditioner", self._plan, handle, _stream())
         self._learned_network = network
 
+    def read_device_pcg_stats(self) -> None:
+        """After a captured step ran: the statistics of its device-side PCG loop
+        (``efsi_fv_pcg_device_stats``) into ``last_cg_*``."""
+        stats = _native.CgStats()
+        _native.call("efsi_fv_pcg_device_stats", self._plan, byref(stats), _stream())
+        self.last_cg_iterations = int(stats.iterations)
+        self.last_cg_initial_relative_residual = float(stats.initial_relative_residual)
+        self.last_cg_relative_residual = float(stats.relative_residual)
+        self.last_cg_converged = bool(stats.converged)
+        self.last_cg_breakdown_dAd = float(stats.breakdown_dAd)
+        self.last_cg_used_multigrid = bool(stats.used_mg)
+        self.last_cg_used_graphs = True
+        self._last_cg_breakdown_code = int(stats.breakdown_code)
+        self._device_stats_pending = False
+
     _CG_SCALAR_FIELDS = (("rz", "cg_rz"), ("rz_new", "cg_rz_new"), ("dAd", "cg_dAd"),
                          ("beta_numerator", "cg_beta_numerator"), ("alpha", "cg_alpha"), ("beta", "cg_beta"),
                          ("breakdown_dAd", "cg_breakdown_dAd"), ("breakdown_code", "cg_breakdown_code"))
@@ -1158,6 +1173,9 @@ class CartesianFluidSolver:
             self.last_hibm_unreached_incompatible_component_count = 0
             self.last_hibm_unreached_component_rhs_mean_max_abs = 0.0
             self.last_hibm_unreached_component_rhs_integral_max_abs = 0.0
+        # device-side loop (no host reads) when the solver is set up for
+        # captured steps; the learned preconditioner's fallback is a host decision
+        device = bool(getattr(self, "device_loop_solves", False)) and name not in ("learned", "learned_no_fallback")
         params = _native.PcgParams(
             max(1, int(iterations)),
             _PRECOND_CODE[name],
@@ -1166,11 +1184,17 @@ class CartesianFluidSolver:
             1 if pressure_interface_matrix_active else 0,
             1 if use_graphs else 0,
             max(0.0, float(tolerance)),
+            1 if device else 0,
         )
         stats = _native.CgStats()
         _native.call(
             "efsi_fv_pcg_solve", self._plan, self._mg_rhs[0].ptr(), self.pressure.ptr(), byref(params), byref(stats), _stream()
         )
+        self._device_stats_pending = int(stats.converged) == -1
+        if self._device_stats_pending:
+            # inside a step-graph capture: the statistics exist once the graph ran
+            # (read_device_pcg_stats)
+            return
         self.last_cg_iterations = int(stats.iterations)
         self.last_cg_initial_relative_residual = float(stats.initial_relative_residual)
         self.last_cg_relative_residual = float(stats.relative_residual)
@@ -1445,7 +1469,7 @@ class CartesianFluidSolver:
         state = {"failed": False, "action": "none"}
 
         def record_cg_stats() -> None:
-            if solver != "fv_cg":
+            if solver != "fv_cg" or getattr(self, "_device_stats_pending", False):
                 return
             self.last_project_cg_project_calls += 1
             self.last_project_cg_iterations_total += int(self.last_cg_iterations)
@@ -1503,7 +1527,7 @@ class CartesianFluidSolver:
             )
 
         def handle_failure() -> None:
-            if solver != "fv_cg" or self.last_cg_converged:
+            if solver != "fv_cg" or self.last_cg_converged or getattr(self, "_device_stats_pending", False):
                 return
             if policy != "raise":
                 state["action"] = "reported_cleared_pressure_correction"

@@ -68,3 +68,49 @@ init_taichi = init_runtime
 
 def current_stream_handle() -> int:
     return torch.cuda.current_stream().cuda_stream
+
+
+class StepGraph:
+    """A whole coupled step as one CUDA graph (``efsi_step_graph_*``; no
+    reference counterpart).  ``capture(step)`` runs ``step`` once under a
+    stream capture on a stream of its own -- every library launch of the step
+    is recorded, PCG solves run their device-side loop -- and ``launch()``
+    replays it on the current stream.  The step must make no host reads and
+    allocate nothing: run it once eagerly first, and keep its reports off."""
+
+    def __init__(self) -> None:
+        self._handle = None
+        self._stream = None
+
+    def capture(self, step) -> None:
+        from ctypes import byref, c_void_p
+
+        self.close()
+        self._stream = torch.cuda.Stream()
+        self._stream.wait_stream(torch.cuda.current_stream())
+        handle = c_void_p()
+        with torch.cuda.stream(self._stream):
+            _native.call("efsi_step_graph_begin", c_void_p(self._stream.cuda_stream))
+            try:
+                step()
+            finally:
+                _native.call("efsi_step_graph_end", c_void_p(self._stream.cuda_stream), byref(handle))
+        self._handle = handle
+
+    def launch(self) -> None:
+        from ctypes import c_void_p
+
+        if self._handle is None:
+            raise RuntimeError("no step graph has been captured")
+        _native.call("efsi_step_graph_launch", self._handle, c_void_p(torch.cuda.current_stream().cuda_stream))
+
+    def close(self) -> None:
+        if self._handle is not None and self._handle.value:
+            _native.call("efsi_step_graph_destroy", self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -168,6 +168,12 @@ typedef struct efsi_pcg_params {
   int32_t iface_active; /* interface terms present: MG disabled, restart every 256 */
   int32_t use_graphs;   /* capture the 16-iteration blocks into CUDA graphs */
   double tolerance;
+  int32_t device_loop;  /* no host reads: the iterations run as a device-side loop (a CUDA-graph WHILE
+                           node) that stops on convergence, a breakdown code or max_iters; the stream
+                           must be under stream capture (efsi_step_graph_begin) or the solve builds and
+                           launches a graph of its own; stats come from efsi_fv_pcg_device_stats.
+                           No reference counterpart (the reference reads the residual every 16
+                           iterations on the host). */
 } efsi_pcg_params;
 
 typedef struct efsi_cg_stats {
@@ -221,6 +227,24 @@ int efsi_cg_compute_beta(efsi_fv_plan* plan, int32_t use_mg, void* stream);
 
 /* Why CUDA-graph capture was abandoned for this plan ("" when it was not). */
 const char* efsi_fv_graph_error(efsi_fv_plan* plan);
+
+/* Statistics of the last efsi_fv_pcg_solve with device_loop under an outer
+ * stream capture, read after the captured graph ran (synchronises the
+ * stream): iterations, converged, relative residuals, b_norm, breakdown code.
+ * No reference counterpart. */
+int efsi_fv_pcg_device_stats(efsi_fv_plan* plan, efsi_cg_stats* stats, void* stream);
+
+/* Whole-step CUDA graphs (no reference counterpart: the reference launches
+ * every kernel of a step from Python, hibm_mpm.py:10533-10616).  begin starts
+ * a stream capture on a created stream (not the legacy default stream); the
+ * library calls of one step follow, with device-side PCG loops
+ * (efsi_pcg_params::device_loop) and no host reads; end instantiates the
+ * graph; launch replays the whole step with one call. */
+typedef struct efsi_step_graph efsi_step_graph;
+int efsi_step_graph_begin(void* stream);
+int efsi_step_graph_end(void* stream, efsi_step_graph** out);
+int efsi_step_graph_launch(efsi_step_graph* graph, void* stream);
+int efsi_step_graph_destroy(efsi_step_graph* graph);
 
 /* Grid size of the cooperative kernel that runs the V-cycle's levels 1 ..
  * lt-1 and its tail in one launch (0: per-level launches; efsi_last_error()

@@ -1114,3 +1114,70 @@ def test_project_report_has_the_reference_keys_and_consistent_partitions(outlet)
         assert rep["velocity_dirichlet_near_max_abs"] == pytest.approx(res[fluid & near].max(), rel=1e-12)
     assert rep["velocity_dirichlet_far_max_abs"] == pytest.approx(res[fluid & ~near].max(), rel=1e-12)
     assert rep["cg_converged_all"]
+
+
+@pytest.mark.parametrize("precond", ["jacobi", "fv_multigrid"])
+def test_device_loop_pcg_matches_the_host_loop(case, precond):
+    """The device-side PCG loop (a CUDA-graph WHILE node of 16-iteration
+    bodies that tests the residual on the device) stops at the same 16-
+    iteration check as the host loop and leaves the same pressure, bit for
+    bit; its statistics come back through efsi_fv_pcg_device_stats."""
+    grid, fl, ofl, rng = case
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    out = []
+    for device in (False, True):
+        fl.device_loop_solves = device
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(iterations=400, rhs_scale=1.0e6, pressure_outlet_zmin=False, tolerance=1e-9,
+                                         preconditioner=precond)
+        out.append((fl.last_cg_iterations, fl.last_cg_converged, fl.last_cg_relative_residual,
+                    fl.pressure.to_numpy()))
+    fl.device_loop_solves = False
+    (it_h, conv_h, res_h, p_h), (it_d, conv_d, res_d, p_d) = out
+    assert conv_h and conv_d
+    assert it_d == ((it_h + 15) // 16) * 16
+    if it_h % 16 == 0:
+        np.testing.assert_array_equal(p_d, p_h)
+        assert res_d == pytest.approx(res_h, rel=1e-12)
+    assert rel_l2(p_d, p_h) <= 1e-8
+
+
+def test_whole_step_graph_replays_the_eager_steps():
+    """A coupled step captured whole (efsi_step_graph_*; device-side PCG loop)
+    and replayed three times gives the same fluid, particle and marker state
+    as three eager steps from the same start (to the order of the f32 atomic
+    sums, 1e-6) and the same CG iteration count."""
+    from easyfsi_b200.runtime import StepGraph
+    from easyfsi_b200.scenarios import CoupledScene, tiny_config
+
+    cfg = tiny_config(16)
+    start = CoupledScene(cfg)
+    u0 = start.fluid.velocity.to_numpy()
+    a = CoupledScene(cfg, initial_velocity=u0, project_initial=False)
+    b = CoupledScene(cfg, initial_velocity=u0, project_initial=False)
+    b.fluid.device_loop_solves = True
+    a.step()
+    b.step()  # eager, with the device-side loop in a graph of its own
+    graph = StepGraph()
+    graph.capture(b.step)
+    for _ in range(3):
+        a.step()
+        graph.launch()
+    torch.cuda.synchronize()
+    b.fluid.read_device_pcg_stats()
+    assert b.fluid.last_cg_converged
+    assert b.fluid.last_cg_iterations == ((a.fluid.last_cg_iterations + 15) // 16) * 16
+    n = a.solid.particle_count
+    fields = [
+        (a.fluid.pressure, b.fluid.pressure), (a.fluid.velocity, b.fluid.velocity), (a.solid.x, b.solid.x),
+        (a.solid.v, b.solid.v), (a.solid.F, b.solid.F), (a.markers.x_gamma_m, b.markers.x_gamma_m),
+    ]
+    for fa, fb in fields:
+        xa, xb = fa.to_numpy(), fb.to_numpy()
+        if xa.shape[0] != xb.shape[0] or xa.ndim == 0:
+            continue
+        if fa is a.solid.x or fa is a.solid.v or fa is a.solid.F:
+            xa, xb = xa[:n], xb[:n]
+        assert rel_l2(xb, xa) <= 1e-6
+    graph.close()
