@@ -1591,6 +1591,26 @@ __global__ void k_dl_check(CgScalars* sc, double tol, int max_iters, cudaGraphCo
   cudaGraphSetConditional(h, go);
 }
 
+// Reciprocal of the level-0 row denominator (fluid.py:4080-4221: the open
+// faces' coefficients in the order x-, x+, y-, y+, z-, z+, the outlet term,
+// the interface diagonal), 0 where the denominator is not positive or the
+// cell is solid.  The plane-marching sweeps multiply by it instead of
+// forming the denominator and dividing.
+__global__ void __launch_bounds__(256) k_rden(LevelDev L, int outlet, double* __restrict__ rden) {
+  EFSI_CELL_PROLOGUE(L)
+  if (!active) return;
+  const unsigned m = __ldg(L.mask + c);
+  double rd = 0.0;
+  if (!(m & M_SOLID)) {
+    double ns, den;
+    stencil_sel<true>(L, row_coef(L, j, k), __ldg(L.cxm + i), __ldg(L.cxp + i), i, j, k, c, m, outlet, 0.0, 0.0,
+                      0.0, 0.0, 0.0, 0.0, ns, den);
+    den += iface_at<double>(L, c);
+    if (den > 0.0) rd = 1.0 / den;
+  }
+  rden[c] = rd;
+}
+
 // fluid.py:4677-4693 with multiplier -1 on the level-0 rhs, plus the free
 // volume (computed in the same pass as the reference does).
 __global__ void __launch_bounds__(256) k_rhs_mean(LevelDev L, const double* __restrict__ rhs, double multiplier,
@@ -1885,7 +1905,10 @@ static void preload_kernels() {
       (const void*)km_sweep0<double, false, A>, (const void*)km_sweep0<float, false, A>,                   \
       (const void*)km_restrict<double, true, A>, (const void*)km_restrict<double, false, A>,               \
       (const void*)km_restrict<float, false, A>, (const void*)km_spmv_dir<true, A>,                        \
-      (const void*)km_spmv_dir<false, A>
+      (const void*)km_spmv_dir<false, A>, (const void*)km_sweep<double, true, false, A, false, true>,      \
+      (const void*)km_sweep<double, true, true, A, false, true>,                                           \
+      (const void*)km_sweep<double, true, false, A, true, true>,                                           \
+      (const void*)km_sweep<double, true, true, A, true, true>
       EFSI_MARCH_FNS(false), EFSI_MARCH_FNS(true),
 #undef EFSI_MARCH_FNS
 #define EFSI_MIXED_FNS(A)                                                                                       \
@@ -1909,7 +1932,11 @@ static void preload_kernels() {
       {(const void*)km_restrict<double, false, A>, march_smem<double, 1, double, true>()},                        \
       {(const void*)km_restrict<float, false, A>, march_smem<float, 1, float, true>()},                           \
       {(const void*)km_spmv_dir<true, A>, march_smem<double, 1, double, false>()},                                \
-      {(const void*)km_spmv_dir<false, A>, march_smem<double, 2, double, false>()}
+      {(const void*)km_spmv_dir<false, A>, march_smem<double, 2, double, false>()},                               \
+      {(const void*)km_sweep<double, true, false, A, false, true>, march_smem<double, 1, double, true>()},        \
+      {(const void*)km_sweep<double, true, true, A, false, true>, march_smem<double, 1, double, true>()},         \
+      {(const void*)km_sweep<double, true, false, A, true, true>, march_smem<double, 1, double, true>()},         \
+      {(const void*)km_sweep<double, true, true, A, true, true>, march_smem<double, 1, double, true>()}
 #define EFSI_MIXED_SMEM(A)                                                                                        \
   {(const void*)km_sweep32<false, A, false>, march_smem<float, 1, double, true>()},                              \
       {(const void*)km_sweep32<false, A, true>, march_smem<float, 1, double, true>()},                           \
@@ -2215,6 +2242,8 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   cudaFree(P->ucomp);
   cudaFree(P->ucomp_acc);
   cudaFree(P->report_buf);
+  cudaFree(P->rden[0]);
+  cudaFree(P->rden[1]);
   cudaFree(P->cpl_rows);
   cudaFree(P->cpl_ptr);
   cudaFree(P->cpl_src);
@@ -2230,6 +2259,7 @@ int efsi_fv_set_masks(efsi_fv_plan* P, const int32_t* obstacle, const int32_t* v
   EFSI_ARG_CHECK(P != nullptr && obstacle != nullptr, "null plan or obstacle");
   EFSI_ARG_CHECK((vdir_active == nullptr) == (vdir_weight == nullptr), "vdir_active and vdir_weight go together");
   cudaStream_t s = as_stream(stream);
+  P->rden_ok[0] = P->rden_ok[1] = false;
   P->has_vdir = vdir_active != nullptr;
   P->has_iface = iface_diag != nullptr;
   P->iface0 = iface_diag;
@@ -2502,9 +2532,14 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   using TR = typename std::conditional<kNegR, double, TP>::type;
   const LevelBuf& B = P->lv[l];
   const dim3 blk(kMK, kTY);
+  // level 0 of the PCG's V-cycle: the precomputed reciprocal denominators
+  // when they are current for this outlet mode
+  const double* rden = (l == 0 && kNegR && std::is_same<TP, double>::value && P->rden_ok[outlet ? 1 : 0])
+                           ? P->rden[outlet ? 1 : 0]
+                           : nullptr;
   if (kZero) {
     EFSI_COUNTED launch_pdl(km_sweep0<TP, kNegR, kAux>, sweep0_grid(B.nx, B.ny, B.nz), blk, 0, s, L, rhs, out, outlet, om,
-                                                                                           partials, P->sc);
+                                                                                           partials, P->sc, rden);
     return true;
   }
   const CUtensorMap* mp = plane_map(P, l, p, MAP_VALUE);
@@ -2513,22 +2548,39 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   if (!mp || !mr || !mm) return false;
   const int sm = march_smem<TP, 1, TR, true>();
   if constexpr (std::is_same<TP, double>::value && kNegR && !kZero) {
-    if (dots_delta != nullptr) {
-      if (pr.pc != nullptr)
+    const double* dd = dots_delta;
+    const bool pro = pr.pc != nullptr;
+    if (rden != nullptr) {
+      if (dd != nullptr && pro)
+        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, true, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp, *mr,
+                                *mm, out, outlet, om, pr, partials, P->sc, dd, rden);
+      else if (dd != nullptr)
+        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, true, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp,
+                                *mr, *mm, out, outlet, om, pr, partials, P->sc, dd, rden);
+      else if (pro)
+        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, false, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp,
+                                *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr, rden);
+      else
+        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, false, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp,
+                                *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr, rden);
+      return true;
+    }
+    if (dd != nullptr) {
+      if (pro)
         EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, true>, B.mgrid, blk, sm, s, 
-            L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dots_delta);
+            L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dd, (const double*)nullptr);
       else
         EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, true>, B.mgrid, blk, sm, s, 
-            L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dots_delta);
+            L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, dd, (const double*)nullptr);
       return true;
     }
   }
   if (pr.pc != nullptr)
     EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, false>, B.mgrid, blk, sm, s, 
-        L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr);
+        L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, (const double*)nullptr, (const double*)nullptr);
   else
     EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, false>, B.mgrid, blk, sm, s, 
-        L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr);
+        L, B.mchunk, *mp, *mr, *mm, out, outlet, om, pr, partials, P->sc, (const double*)nullptr, (const double*)nullptr);
   return true;
 }
 
@@ -2615,6 +2667,21 @@ static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs
   }
   EFSI_COUNTED launch_pdl(k_restrict<TP, kNegR, true>, C.shape.grid, C.shape.block, 0, s, L, p, rhs, outlet, C.nx, C.ny,
                                                                                  C.nz, C.rhs);
+}
+
+// The level-0 reciprocal denominators for this outlet mode (recomputed after
+// every efsi_fv_set_masks).  EFSI_NO_RDEN keeps the sweeps dividing.
+static int ensure_rden(efsi_fv_plan* P, int outlet, cudaStream_t s) {
+  static const bool off = std::getenv("EFSI_NO_RDEN") != nullptr;
+  const int o = outlet ? 1 : 0;
+  if (off || P->rden_ok[o] || !P->lv[0].march) return EFSI_OK;
+  if (P->rden[o] == nullptr) EFSI_CUDA_CHECK(cudaMalloc(&P->rden[o], P->lv[0].n * sizeof(double)));
+  const LevelDev L = level_dev(P, 0);
+  const Shape3& S = P->lv[0].shape;
+  EFSI_COUNTED k_rden<<<S.grid, S.block, 0, s>>>(L, o, P->rden[o]);
+  EFSI_LAUNCH_CHECK();
+  P->rden_ok[o] = true;
+  return EFSI_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -2815,6 +2882,7 @@ extern "C" {
 int efsi_mg_vcycle(efsi_fv_plan* P, const double* r, double* z, int32_t outlet, int32_t pre, int32_t coarse,
                    int32_t post, void* stream) {
   EFSI_TRY(level_zero_check(P));
+  EFSI_TRY(ensure_rden(P, outlet, as_stream(stream)));
   return vcycle(P, r, z, outlet, pre, coarse, post, false, as_stream(stream));
 }
 
@@ -3074,6 +3142,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   EFSI_ARG_CHECK(!device || (prm->precond != 4 && prm->precond != 5),
                  "the device-side loop does not take the learned preconditioner (its fallback is a host decision)");
   EFSI_COUNTED k_reset_scalars<<<1, 32, 0, s>>>(P->sc);
+  EFSI_TRY(ensure_rden(P, outlet, s));
   const bool coupled = P->cpl_nrows > 0;
   if (coupled) EFSI_COUNTED k_set_defer<<<1, 32, 0, s>>>(P->sc, 1);
   // fluid.py:6581 diagonal (Jacobi path and fallback).

@@ -268,6 +268,8 @@ struct efsi_fv_plan {
   double* aux = nullptr;  // 16 doubles of statistics scratch
   double* bicg_work = nullptr;  // BiCGSTAB fallback's nine level-0 work vectors, allocated at its first use
   double* report_buf = nullptr;  // 54 doubles of the final divergence report
+  double* rden[2] = {nullptr, nullptr};  // level-0 reciprocal row denominators (outlet off / on)
+  bool rden_ok[2] = {false, false};      // current for the masks and weights set last
   int32_t* ucomp = nullptr;      // unreached component of every level-0 cell (-1: none)
   int ucomp_n = 0;               // components anchored by an outlet solve (0: none)
   double* ucomp_acc = nullptr;   // per component: volume-weighted sums [256], volumes [256]

@@ -391,7 +391,7 @@ __device__ __forceinline__ void report_fault(CgScalars* sc) {
 // prolongation p += s * p_coarse of fluid cells fused in when kProlong
 // (fluid.py:5391-5406) and, when `partials`, the fluid sum of out * V.
 // ---------------------------------------------------------------------------
-template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots>
+template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots, bool kRd = false>
 struct SweepOp {
   const LevelDev& L;
   TP* __restrict__ out;
@@ -406,6 +406,10 @@ struct SweepOp {
   const double* __restrict__ delta;
   double srz, sr, sdz, sd;
   double dl[2 * kRows];  // kDots: delta of the iteration's cells, prefetched
+  // kRd: the rows' reciprocal denominators 1 / den (0 where den <= 0),
+  // precomputed per plan, prefetched like delta
+  const double* __restrict__ rden;
+  double rdv[2 * kRows];
 
   // kProlong: every thread prolongs up to kPCells cells of each landed value
   // tile (the (kMJ + 2) x (kMK + 2) cells with halo, strided by the block);
@@ -451,6 +455,13 @@ struct SweepOp {
         for (int r = 0; r < kRows; ++r)
           dl[d * kRows + r] = __ldg(delta + min(pbase + d * sx, (int64_t)(L.nx - 1) * sx) + g.off[r]);
     }
+    if (kRd) {
+#pragma unroll
+      for (int d = 0; d < 2; ++d)
+#pragma unroll
+        for (int r = 0; r < kRows; ++r)
+          rdv[d * kRows + r] = __ldg(rden + min(pbase + d * sx, (int64_t)(L.nx - 1) * sx) + g.off[r]);
+    }
   }
 
   // The prolongation p + s * p_coarse (in the level's storage precision) is
@@ -483,11 +494,20 @@ struct SweepOp {
       const double ym = val(0, 0, -1, 0), yp = val(0, 0, 1, 0), zm = val(0, 0, 0, -1), zp = val(0, 0, 0, 1);
       double ns, den;
       stencil_sel<kAux>(L, rc, kxm, kxp, i, j, k, c, m, outlet, xm, xp, ym, yp, zm, zp, ns, den);
-      if (kAux) den += iface_at<TP>(L, c);
-      if (den > 0.0) {
-        const double rv = kNegR ? -e : e;
-        const double jv = (ns - rv) / den;
-        res = (TP)(x0 + omega * (jv - x0));
+      if (kRd) {
+        const double rd = rdv[slot];
+        if (rd > 0.0) {
+          const double rv = kNegR ? -e : e;
+          const double jv = (ns - rv) * rd;
+          res = (TP)(x0 + omega * (jv - x0));
+        }
+      } else {
+        if (kAux) den += iface_at<TP>(L, c);
+        if (den > 0.0) {
+          const double rv = kNegR ? -e : e;
+          const double jv = (ns - rv) / den;
+          res = (TP)(x0 + omega * (jv - x0));
+        }
       }
       if ((want_sum || kDots) && (m & M_FLUID)) {
         const double vol = vol64(L, i, j, k);
@@ -539,18 +559,18 @@ __device__ __forceinline__ void sweep_epilogue(const Op& op, double* partials, C
 }
 
 // Three blocks per SM (the shared-memory ring allows three).
-template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots>
+template <typename TP, bool kNegR, bool kProlong, bool kAux, bool kDots, bool kRd = false>
 __global__ void __launch_bounds__(kMK* kTY, 3)
     km_sweep(LevelDev L, int chunk, const __grid_constant__ CUtensorMap map_p,
              const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m,
              TP* __restrict__ out, int outlet, double omega, ProlongSrc pr, double* partials, CgScalars* sc,
-             const double* __restrict__ delta) {
+             const double* __restrict__ delta, const double* __restrict__ rden) {
   pdl_wait();
   using TR = typename std::conditional<kNegR, double, TP>::type;
   MarchGeom g;
   const bool any = march_geom(L, chunk, g);
-  SweepOp<TP, kNegR, kProlong, kAux, kDots> op{L, out, outlet, omega, pr, partials != nullptr, 0.0,
-                                               delta, 0.0, 0.0, 0.0, 0.0};
+  SweepOp<TP, kNegR, kProlong, kAux, kDots, kRd> op{L, out, outlet, omega, pr, partials != nullptr, 0.0,
+                                                    delta, 0.0, 0.0, 0.0, 0.0, {}, rden};
   const CUtensorMap* const mv[1] = {&map_p};
   if (any && !march<TP, 1, TR, true>(L, g, mv, &map_r, &map_m, op)) report_fault(sc);
   sweep_epilogue<kDots>(op, partials, sc);
@@ -663,10 +683,11 @@ inline dim3 sweep0_grid(int nx, int ny, int nz) {
               (unsigned)((nx + kSweep0Planes - 1) / kSweep0Planes));
 }
 
+// rden (level 0, may be null): the rows' precomputed reciprocal denominators.
 template <typename TP, bool kNegR, bool kAux>
 __global__ void __launch_bounds__(kMK* kTY)
     km_sweep0(LevelDev L, const void* rhs, TP* __restrict__ out, int outlet, double omega, double* partials,
-              CgScalars* sc) {
+              CgScalars* sc, const double* __restrict__ rden) {
   pdl_wait();
   const int k = (int)(blockIdx.x * kMK + threadIdx.x), j = (int)(blockIdx.y * kTY + threadIdx.y);
   const int i0 = (int)blockIdx.z * kSweep0Planes;
@@ -677,13 +698,14 @@ __global__ void __launch_bounds__(kMK* kTY)
     const RowCoef rc = row_coef(L, j, k);
     const int n = min(kSweep0Planes, L.nx - i0);
     unsigned m[kSweep0Planes];
-    double e[kSweep0Planes];
+    double e[kSweep0Planes], rd[kSweep0Planes];
 #pragma unroll
     for (int q = 0; q < kSweep0Planes; ++q) {
       if (q >= n) break;
       m[q] = __ldg(L.mask + c0 + q * sx);
       e[q] = kNegR ? __ldg(reinterpret_cast<const double*>(rhs) + c0 + q * sx)
                    : (double)__ldg(reinterpret_cast<const TP*>(rhs) + c0 + q * sx);
+      rd[q] = rden != nullptr ? __ldg(rden + c0 + q * sx) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < kSweep0Planes; ++q) {
@@ -692,14 +714,21 @@ __global__ void __launch_bounds__(kMK* kTY)
       const int64_t c = c0 + q * sx;
       TP res = (TP)0;
       if (!(m[q] & M_SOLID)) {
-        double ns, den;
-        stencil_sel<kAux>(L, rc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, j, k, c, m[q], outlet, 0.0, 0.0, 0.0, 0.0,
-                          0.0, 0.0, ns, den);
-        if (kAux) den += iface_at<TP>(L, c);
-        if (den > 0.0) {
-          const double rv = kNegR ? -e[q] : e[q];
-          const double jv = (ns - rv) / den;
-          res = (TP)(0.0 + omega * (jv - 0.0));
+        if (rden != nullptr) {
+          if (rd[q] > 0.0) {
+            const double rv = kNegR ? -e[q] : e[q];
+            res = (TP)(0.0 + omega * ((0.0 - rv) * rd[q] - 0.0));
+          }
+        } else {
+          double ns, den;
+          stencil_sel<kAux>(L, rc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, j, k, c, m[q], outlet, 0.0, 0.0, 0.0,
+                            0.0, 0.0, 0.0, ns, den);
+          if (kAux) den += iface_at<TP>(L, c);
+          if (den > 0.0) {
+            const double rv = kNegR ? -e[q] : e[q];
+            const double jv = (ns - rv) / den;
+            res = (TP)(0.0 + omega * (jv - 0.0));
+          }
         }
         if (partials != nullptr && (m[q] & M_FLUID)) zsum += (double)res * vol64(L, i, j, k);
       }
