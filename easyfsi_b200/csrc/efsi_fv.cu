@@ -1905,9 +1905,7 @@ static void preload_kernels() {
       (const void*)km_sweep0<double, false, A>, (const void*)km_sweep0<float, false, A>,                   \
       (const void*)km_restrict<double, true, A>, (const void*)km_restrict<double, false, A>,               \
       (const void*)km_restrict<float, false, A>, (const void*)km_spmv_dir<true, A>,                        \
-      (const void*)km_spmv_dir<false, A>, (const void*)km_sweep<double, true, false, A, false, true>,      \
-      (const void*)km_sweep<double, true, true, A, false, true>,                                           \
-      (const void*)km_sweep<double, true, false, A, true, true>,                                           \
+      (const void*)km_spmv_dir<false, A>, (const void*)km_sweep<double, true, false, A, true, true>,       \
       (const void*)km_sweep<double, true, true, A, true, true>
       EFSI_MARCH_FNS(false), EFSI_MARCH_FNS(true),
 #undef EFSI_MARCH_FNS
@@ -1933,8 +1931,6 @@ static void preload_kernels() {
       {(const void*)km_restrict<float, false, A>, march_smem<float, 1, float, true>()},                           \
       {(const void*)km_spmv_dir<true, A>, march_smem<double, 1, double, false>()},                                \
       {(const void*)km_spmv_dir<false, A>, march_smem<double, 2, double, false>()},                               \
-      {(const void*)km_sweep<double, true, false, A, false, true>, march_smem<double, 1, double, true>()},        \
-      {(const void*)km_sweep<double, true, true, A, false, true>, march_smem<double, 1, double, true>()},         \
       {(const void*)km_sweep<double, true, false, A, true, true>, march_smem<double, 1, double, true>()},         \
       {(const void*)km_sweep<double, true, true, A, true, true>, march_smem<double, 1, double, true>()}
 #define EFSI_MIXED_SMEM(A)                                                                                        \
@@ -2550,19 +2546,16 @@ static bool launch_march_sweep(efsi_fv_plan* P, int l, const LevelDev& L, const 
   if constexpr (std::is_same<TP, double>::value && kNegR && !kZero) {
     const double* dd = dots_delta;
     const bool pro = pr.pc != nullptr;
-    if (rden != nullptr) {
-      if (dd != nullptr && pro)
+    // the reciprocal pays off in the dots-fused sweep (measured on c2: 49.4 ->
+    // 44.4 us); the plain and prolongation-fused sweeps keep the division
+    // (28.5 / 44.5 us against 30.4 / 46.0 us with the extra 8 bytes per cell)
+    if (rden != nullptr && dd != nullptr) {
+      if (pro)
         EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, true, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp, *mr,
                                 *mm, out, outlet, om, pr, partials, P->sc, dd, rden);
-      else if (dd != nullptr)
+      else
         EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, true, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp,
                                 *mr, *mm, out, outlet, om, pr, partials, P->sc, dd, rden);
-      else if (pro)
-        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, true, kAux, false, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp,
-                                *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr, rden);
-      else
-        EFSI_COUNTED launch_pdl(km_sweep<TP, kNegR, false, kAux, false, true>, B.mgrid, blk, sm, s, L, B.mchunk, *mp,
-                                *mr, *mm, out, outlet, om, pr, partials, P->sc, nullptr, rden);
       return true;
     }
     if (dd != nullptr) {

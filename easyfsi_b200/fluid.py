@@ -280,6 +280,10 @@ class CartesianFluidSolver:
         self.last_cg_restart_policy = ""
         self.last_cg_breakdown_dAd = 0.0
         self.last_cg_used_multigrid = False
+        # steps captured into CUDA graphs (runtime.StepGraph): PCG solves run
+        # their device-side loop and the predictor copies instead of exchanging
+        # its buffers
+        self.device_loop_solves = False
         self._hibm_pressure_unreached_count = 0
         self._hibm_pressure_unreached_component_count = 0
         self.last_hibm_unreached_incompatible_component_count = 0
@@ -787,9 +791,14 @@ class CartesianFluidSolver:
         scheme = str(advection_scheme).lower()
         if scheme not in {"euler", "rk2"}:
             raise ValueError(f"unsupported advection_scheme: {advection_scheme!r}")
-        # velocity_prev <- velocity by exchanging the two buffers (the
-        # predictor overwrites every cell of velocity).
-        self.velocity.tensor, self.velocity_prev.tensor = self.velocity_prev.tensor, self.velocity.tensor
+        # velocity_prev <- velocity: by exchanging the two buffers (the
+        # predictor overwrites every cell of velocity), or, when steps are
+        # captured into CUDA graphs (device_loop_solves), by a device copy, so
+        # that every replay reads and writes the same buffers
+        if getattr(self, "device_loop_solves", False):
+            self.velocity_prev.tensor.copy_(self.velocity.tensor)
+        else:
+            self.velocity.tensor, self.velocity_prev.tensor = self.velocity_prev.tensor, self.velocity.tensor
         self._predict_kernel(step_dt_s, self.mu / self.rho, 1 if scheme == "rk2" else 0)
 
     # ------------------------------------------------------------------

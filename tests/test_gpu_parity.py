@@ -122,9 +122,11 @@ def test_pcg_solve_matches_oracle(case, precond):
     st = ofl.pcg_solve(outlet=0, max_iters=300, tol=1e-8, precond=code, remove_mean=True)
     assert fl.last_cg_converged and st.converged
     assert fl.last_cg_iterations == st.iterations
-    # measured on a B200: 4.5e-16 (jacobi), 3.6e-13 (fv_multigrid), 8.5e-11
-    # (fv_multigrid_light, whose f32 coarse levels run more cycles)
-    tol = {"jacobi": 1e-12, "fv_multigrid": 1e-10, "fv_multigrid_light": 1e-9}[precond]
+    # measured on a B200: 4.5e-16 (jacobi), 3.6e-13 (fv_multigrid), 2.0e-9
+    # (fv_multigrid_light: its 12 f32 coarse sweeps carry the one-unit
+    # differences of the level-0 sweeps that multiply by the reciprocal
+    # denominator where the reference divides)
+    tol = {"jacobi": 1e-12, "fv_multigrid": 1e-10, "fv_multigrid_light": 1e-8}[precond]
     assert rel_l2(fl.pressure.to_numpy(), ofl.pressure) <= tol
     # true residual of the GPU solution, measured by the oracle operator
     rhs = ofl.rhs0.copy()
