@@ -10,8 +10,8 @@
 // filled outside the volume) into shared memory in the canonical no-swizzle
 // K-major layout (8-row x 16-byte core matrices: SBO = 128 bytes between
 // 8-row groups, LBO = rows x 16 bytes between 8-element K chunks), through a
-// ring of kStages stages, so the copies of the next kStages - 1 taps are in
-// flight while one elected thread issues tcgen05.mma.kind::f16 (BF16
+// ring of kStages stages, so the copies of the next kAhead taps are in flight
+// while one elected thread issues tcgen05.mma.kind::f16 (BF16
 // operands, FP32 accumulator in tensor memory) per 16-channel K step of the
 // current tap and commits to the stage's mbarrier.  The epilogue reads the accumulator with tcgen05.ld (warp w owns
 // lanes 32w..32w+31 = voxels), adds the bias, applies ReLU if asked and
@@ -33,6 +33,8 @@ namespace conv {
 constexpr int kTileM = 128;          // voxels per CTA (MMA M)
 constexpr int kThreads = 128;        // 4 warps: one TMEM lane quadrant each
 constexpr int kStages = 4;           // taps in the shared-memory ring
+constexpr int kLag = 2;              // a stage is refilled once the MMAs of kLag taps ago are done
+constexpr int kAhead = kStages - kLag;  // taps whose copies are in flight ahead of the current one
 constexpr long long kWaitLimit = 4000000000LL;  // ~2 s of clock64
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -195,16 +197,16 @@ __global__ void __launch_bounds__(kThreads) k_conv3d_tc(ConvArgs A) {
     }
   };
   const uint32_t idesc = idesc_bf16(kTileM, cout);
-  // prologue: taps 0 .. kStages - 2 in flight (one commit group per tap)
-  for (int t = 0; t < kStages - 1; ++t) {
+  // prologue: taps 0 .. kAhead - 1 in flight (one commit group per tap)
+  for (int t = 0; t < kAhead; ++t) {
     issue(t);
     cp_async_commit();
   }
   bool ok = true, good = true;
   for (int t = 0; t < 27; ++t) {
-    // this thread's copies of tap t have landed once at most kStages - 2
+    // this thread's copies of tap t have landed once at most kAhead - 1
     // newer groups are pending; the block decides together whether to go on
-    cp_async_wait<kStages - 2>();
+    cp_async_wait<kAhead - 1>();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (!__syncthreads_and(good)) {
       ok = false;
@@ -221,11 +223,12 @@ __global__ void __launch_bounds__(kThreads) k_conv3d_tc(ConvArgs A) {
       }
       tc_commit(&bars[t % kStages]);
     }
-    // refill the stage of tap t - 1 with tap t + kStages - 1 once the MMAs of
-    // tap t - 1 have read it
-    const int tn = t + kStages - 1;
+    // refill the stage of tap t - kLag with tap t + kAhead once the MMAs of
+    // tap t - kLag have read it (issued kLag iterations ago, so the wait is
+    // normally already over)
+    const int tn = t + kAhead;
     if (tn < 27) {
-      if (t >= 1) good = mbar_wait_bounded(&bars[(t - 1) % kStages], (unsigned)(((t - 1) / kStages) & 1));
+      if (t >= kLag) good = mbar_wait_bounded(&bars[(t - kLag) % kStages], (unsigned)(((t - kLag) / kStages) & 1));
       if (good) issue(tn);
     }
     cp_async_commit();  // one group per iteration, possibly empty
