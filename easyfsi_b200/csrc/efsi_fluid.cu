@@ -181,9 +181,13 @@ __global__ void k_vdir_rows(LevelDev L, const int32_t* __restrict__ va, const fl
   }
 }
 
-// fluid.py:2407-2433 _axis_grid_coordinate_device (f32).
+// fluid.py:2407-2433 _axis_grid_coordinate_device (f32).  The bracketing
+// centre interval is the one the reference's bisection finds (the largest lo
+// with centers[lo] <= v); with a hint (the index of a cell near v, -1: none)
+// it is found by walking from the hint, which takes a step or two for a
+// semi-Lagrangian departure point instead of log2(count) dependent loads.
 __device__ __forceinline__ float axis_coord(float v, const float* __restrict__ faces,
-                                            const float* __restrict__ centers, int count) {
+                                            const float* __restrict__ centers, int count, int hint = -1) {
   float coord;
   const float c0 = __ldg(centers), cl = __ldg(centers + count - 1);
   if (v <= c0) {
@@ -194,12 +198,19 @@ __device__ __forceinline__ float axis_coord(float v, const float* __restrict__ f
     coord = __fadd_rn((float)(count - 1), __fdiv_rn(__fmul_rn(0.5f, __fsub_rn(v, cl)), hw));
   } else {
     int lo = 0, hi = count - 1;
-    while (hi - lo > 1) {
-      int mid = (lo + hi) / 2;
-      if (v >= __ldg(centers + mid))
-        lo = mid;
-      else
-        hi = mid;
+    if (hint >= 0) {
+      // c0 < v < cl: the bracket lo in [0, count - 2] exists and is unique
+      lo = min(max(hint, 0), count - 2);
+      while (lo < count - 2 && v >= __ldg(centers + lo + 1)) ++lo;
+      while (lo > 0 && v < __ldg(centers + lo)) --lo;
+    } else {
+      while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (v >= __ldg(centers + mid))
+          lo = mid;
+        else
+          hi = mid;
+      }
     }
     hi = min(lo + 1, count - 1);
     const float clo = __ldg(centers + lo);
@@ -266,15 +277,15 @@ __global__ void __launch_bounds__(256) k_predict(LevelDev L, efsi_grid_axes A, c
     float mx = __fsub_rn(x, __fmul_rn(hd, cen[0]));
     float my = __fsub_rn(y, __fmul_rn(hd, cen[1]));
     float mz = __fsub_rn(z, __fmul_rn(hd, cen[2]));
-    sample_prev(L, vp, axis_coord(mx, A.fx, A.cx, L.nx), axis_coord(my, A.fy, A.cy, L.ny),
-                axis_coord(mz, A.fz, A.cz, L.nz), cen, tr);
+    sample_prev(L, vp, axis_coord(mx, A.fx, A.cx, L.nx, i), axis_coord(my, A.fy, A.cy, L.ny, j),
+                axis_coord(mz, A.fz, A.cz, L.nz, k), cen, tr);
   }
   float bx = __fsub_rn(x, __fmul_rn(dt, tr[0]));
   float by = __fsub_rn(y, __fmul_rn(dt, tr[1]));
   float bz = __fsub_rn(z, __fmul_rn(dt, tr[2]));
   float adv[3];
-  sample_prev(L, vp, axis_coord(bx, A.fx, A.cx, L.nx), axis_coord(by, A.fy, A.cy, L.ny),
-              axis_coord(bz, A.fz, A.cz, L.nz), cen, adv);
+  sample_prev(L, vp, axis_coord(bx, A.fx, A.cx, L.nx, i), axis_coord(by, A.fy, A.cy, L.ny, j),
+              axis_coord(bz, A.fz, A.cz, L.nz, k), cen, adv);
   const float dtnu = __fmul_rn(dt, nu);
   const float icx = __ldg(L.cdx_f + i), icy = __ldg(L.cdy_f + j), icz = __ldg(L.cdz_f + k);
   const float icxp = (i < L.nx - 1) ? __ldg(L.cdx_f + i + 1) : 1.0f;

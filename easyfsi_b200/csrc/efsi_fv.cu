@@ -1766,6 +1766,18 @@ __global__ void k_reset_scalars(CgScalars* sc) {
   }
 }
 
+// Clears the breakdown code after the initial direction: a V-cycle whose last
+// sweep finished the dots ran the beta test against rz = 0 (no previous
+// direction yet) and flagged a breakdown that the first direction does not
+// have (fluid.py:6662-6673 computes only rz there).
+__global__ void k_clear_code(CgScalars* sc) {
+  pdl_wait();
+  if (threadIdx.x == 0) {
+    sc->code = 0;
+    sc->code_dAd = 0.0;
+  }
+}
+
 }  // namespace efsi
 
 namespace efsi {
@@ -1891,6 +1903,7 @@ static void preload_kernels() {
       (const void*)k_true_residual,               (const void*)k_sub_mean_r,
       (const void*)k_rhs_mean,                    (const void*)k_build_b,
       (const void*)k_fv_diag,                     (const void*)k_reset_scalars,
+      (const void*)k_clear_code,
       (const void*)kt_sweep<double, true, true>,  (const void*)kt_sweep<double, true, false>,
       (const void*)kt_sweep<float, false, true>,  (const void*)kt_sweep<float, false, false>,
       (const void*)kt_spmv_dir<true>,             (const void*)kt_spmv_dir<false>,
@@ -3217,6 +3230,7 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   if (remove_mean) st->mean_projection_count += 1;
   if (R.anchor) st->unreached_set_mean_projection_count += 1;
   EFSI_COUNTED launch_pdl(k_cg_dots<false, true>, R.S.grid, R.S.block, 0, s, R.L, P->r, P->z, nullptr, P->partials, P->sc);
+  if (R.dots_fused) EFSI_COUNTED launch_pdl(k_clear_code, 1, 32, 0, s, P->sc);
   EFSI_LAUNCH_CHECK();
   if (!device) EFSI_TRY(read_scalars(R));
   double rz = device ? 1.0 : P->host_sc->rz;

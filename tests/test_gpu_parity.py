@@ -1145,6 +1145,33 @@ def test_device_loop_pcg_matches_the_host_loop(case, precond):
     assert rel_l2(p_d, p_h) <= 1e-8
 
 
+def test_device_loop_runs_past_the_first_block():
+    """On a grid whose V-cycle finishes the PCG dots in its last level-0
+    sweep, a tight tolerance takes several 16-iteration blocks: the first
+    direction carries no breakdown code, so neither loop restarts and the
+    device loop does not stop after its first body."""
+    grid = _graded_grid((40, 24, 48))
+    fl = _solver(grid)
+    fl.obstacle.from_numpy(_obstacle(grid, seed=7))
+    fl._refresh_structure()
+    div = np.random.default_rng(29).normal(size=grid.grid_nodes).astype(np.float32)
+    out = []
+    for device in (False, True):
+        fl.device_loop_solves = device
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(iterations=400, rhs_scale=1.0e6, pressure_outlet_zmin=False, tolerance=1e-12,
+                                         preconditioner="fv_multigrid")
+        out.append((fl.last_cg_iterations, fl.last_cg_converged, fl.last_cg_restart_count, fl.pressure.to_numpy()))
+    fl.device_loop_solves = False
+    (it_h, conv_h, rs_h, p_h), (it_d, conv_d, _, p_d) = out
+    assert conv_h and conv_d
+    assert rs_h == 0
+    assert it_h > 16
+    assert it_d == ((it_h + 15) // 16) * 16
+    assert rel_l2(p_d, p_h) <= 1e-10
+
+
 def test_whole_step_graph_replays_the_eager_steps():
     """A coupled step captured whole (efsi_step_graph_*; device-side PCG loop)
     and replayed three times gives the same fluid, particle and marker state
