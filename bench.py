@@ -382,6 +382,93 @@ def graph_step_arm(scene, steps: int, warmup: int, world: int, plain_value: floa
         fl.device_loop_solves = False
 
 
+def batched_arm(steps: int, warmup: int, world: int, count: int) -> dict:
+    """The c5 batch: `count` independent coupled instances of uneven size
+    (uniform 48^3 .. 128^3 grids, 2k-340k particles each).  Eager: every
+    instance's step in turn on one stream (host reads at the PCG's 16-iteration
+    checks).  Graph: all instances' steps captured as ONE CUDA graph with one
+    branch per instance (runtime.BatchStepGraph; device-side PCG loops), one
+    launch per batch step.  The unit is instance-steps/s (each instance
+    advanced by one coupled step counts once)."""
+    import torch
+    import torch.distributed as dist
+
+    from easyfsi_b200.runtime import BatchStepGraph
+    from easyfsi_b200.scenarios import CoupledScene, batched_configs
+
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    cfgs = batched_configs(count)
+    scenes = [CoupledScene(c) for c in cfgs]
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    cells = int(sum(int(np.prod(c.grid_nodes)) for c in cfgs))
+    parts = int(sum(sc.solid.particle_count for sc in scenes))
+
+    def timed(run, k):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return max_over_ranks(e0.elapsed_time(e1), world, "cuda")
+
+    def eager():
+        for sc in scenes:
+            sc.step()
+
+    for _ in range(max(1, warmup)):
+        eager()
+    eager_ms = timed(eager, steps)
+    eager_iters = [int(sc.last_cg_iterations) for sc in scenes]
+    graph = BatchStepGraph()
+    try:
+        for sc in scenes:
+            sc.fluid.device_loop_solves = True
+        eager()  # every instance once with its device-side loop
+        torch.cuda.synchronize()
+        graph.capture([sc.step for sc in scenes])
+        for _ in range(max(1, warmup)):
+            graph.launch()
+        graph_ms = timed(graph.launch, steps)
+        conv, g_iters = [], []
+        for sc in scenes:
+            sc.fluid.read_device_pcg_stats()
+            conv.append(bool(sc.fluid.last_cg_converged))
+            g_iters.append(int(sc.fluid.last_cg_iterations))
+    finally:
+        graph.close()
+        for sc in scenes:
+            sc.fluid.device_loop_solves = False
+    n_inst = world * count
+    eager_v = n_inst * steps / (eager_ms / 1000.0)
+    graph_v = n_inst * steps / (graph_ms / 1000.0)
+    out = {
+        "workload": f"c5: {count} uniform instances of 48^3..128^3 cells (seed 5000+i), one sphere each",
+        "instances": count,
+        "cells": cells,
+        "particles": parts,
+        "unit": "instance-steps/s",
+        "eager": {"value": eager_v, "ms_per_batch_step": eager_ms / steps},
+        "graph": {"value": graph_v, "ms_per_batch_step": graph_ms / steps,
+                  "launch": "one CUDA graph launch per batch step, one branch per instance"},
+        "ratio_graph_to_eager": graph_v / eager_v,
+        "all_converged": all(conv),
+        "cg_iterations_eager": eager_iters,
+        "cg_iterations_graph": g_iters,
+        "setup_s": setup_s,
+    }
+    del scenes
+    torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(ms: float, world: int, device) -> float:
     """Largest per-rank time over all ranks (every rank calls this in the same
     order; a no-op for one rank)."""
@@ -467,6 +554,8 @@ def main() -> None:
     ap.add_argument("--no-family-timing", action="store_true", help="skip the MPM / HIBM kernel-family timing pass")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
     ap.add_argument("--no-graph-step", action="store_true", help="skip the whole-step CUDA graph arm")
+    ap.add_argument("--no-batched", action="store_true", help="skip the c5 batched-instances arm")
+    ap.add_argument("--batch-count", type=int, default=32, help="instances of the c5 batched arm")
     ap.add_argument("--learned-train-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replay-reps", type=int, default=50)
@@ -672,6 +761,13 @@ def main() -> None:
     particle_families = None
     if not args.no_family_timing:
         particle_families = family_timing(scene, args.steps, peak, world)
+    # --- the c5 batch of uneven independent instances, eager and as one graph ---
+    batched = None
+    if not args.no_batched:
+        try:
+            batched = batched_arm(args.steps, args.warmup, world, args.batch_count)
+        except Exception as exc:  # reported, never fatal to the step's line
+            batched = {"error": f"{type(exc).__name__}: {exc}"}
     dom = max(fam_stats, key=lambda f: fam_stats[f]["ms_per_step"])
     st = fam_stats[dom]
     traffic = None
@@ -743,6 +839,7 @@ def main() -> None:
             "cg_iterations_mean": float(np.mean(iters)) if iters else None,
             "mixed_precision": mixed,
             "graph_step": graph_step,
+            "batched": batched,
             "learned": learned,
             "particle_families": particle_families,
             "kernel_families": fam_stats,

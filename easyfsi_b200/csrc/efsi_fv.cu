@@ -914,31 +914,41 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(TailDesc T) {
 }
 
 // ---------------------------------------------------------------------------
-// Coarse levels 1 .. lt-1 and the tail in one cooperative launch.  The blocks
-// of the grid share the cells of each phase (grid-stride); a grid barrier
-// separates the phases.  Per V-cycle this replaces the per-level launches
-// (3 + 2 per level: the pre-sweeps, the restriction and the post-sweeps) and
-// the tail launch by one launch and its barriers.  The arithmetic is that of
-// k_sweep / k_restrict / k_prolong (and so of the plane-marching kernels):
-// the same `stencil` rows in the same order.  Fields written inside the
-// launch are read with plain (coherent) loads, never through the read-only
-// path.  Phases:
-//   level 1: the zero-guess sweep, the other pre-sweeps;
+// Coarse levels first .. lt-1 and the tail in one launch.  The blocks of the
+// grid share the cells of each phase (grid-stride); a barrier separates the
+// phases.  Per V-cycle this replaces the per-level launches (3 + 2 per level:
+// the pre-sweeps, the restriction and the post-sweeps) and the tail launch by
+// one launch and its barriers.  The arithmetic is that of k_sweep /
+// k_restrict / k_prolong (and so of the plane-marching kernels): the same
+// `stencil` rows in the same order.  Fields written inside the launch are
+// read with plain (coherent) loads, never through the read-only path.
+// Two forms:
+//   - cooperative (first = 1): as many blocks as fit on the GPU, a software
+//     grid barrier; every barrier wait is bounded, a block that gives up
+//     sets the fault flag, and every block returns at the next barrier that
+//     sees the flag;
+//   - one thread-block cluster (first = 2, level 1 stays on the
+//     plane-marching kernels): the cluster's hardware barrier
+//     (barrier.cluster arrive.release / wait.acquire), which every thread of
+//     every CTA reaches at the same phase boundaries.
+// Phases:
+//   level first: the zero-guess sweep, the other pre-sweeps;
 //   level l: the restriction into l+1 fused with the zero-guess sweep of
 //            l+1 (it only needs the cell's own rhs), the other pre-sweeps;
 //   the tail (block 0);
-//   level l = lt-1 .. 1: the prolongation-fused first post-sweep, the others.
-// Every barrier wait is bounded; a block that gives up sets the fault flag,
-// and every block returns at the next barrier that sees the flag.
+//   level l = lt-1 .. first: the prolongation-fused first post-sweep, the
+//            others.
 // ---------------------------------------------------------------------------
 struct CoarseDesc {
-  TailDesc T;  // T.L[l] for every level l >= 1; the tail of levels lt..nl-1
+  TailDesc T;  // T.L[l] for every level l >= first; the tail of levels lt..nl-1
   float* pa[kTailMaxLevels];
   float* pb[kTailMaxLevels];
   float* rhs[kTailMaxLevels];
   unsigned* bar;  // [0] arrivals, [1] generation
   int* fault;
   unsigned spin_ns;  // back-off between polls of the generation (0: none)
+  int first;         // first level run here (its rhs is already restricted)
+  int cluster;       // 1: the grid is one thread-block cluster (hardware barrier)
 };
 
 constexpr long long kCoarseWaitLimit = 4000000000LL;  // ~2 s of clock64
@@ -950,6 +960,12 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 }
 
 __device__ bool coarse_barrier(const CoarseDesc& D) {
+  if (D.cluster) {
+    // every thread of every CTA of the cluster arrives (release) and waits
+    // (acquire): the phase's global writes are visible to the whole cluster
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    return true;
+  }
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1053,11 +1069,13 @@ __device__ __forceinline__ float pk_restrict_cell(const LevelDev& F, const float
   return ocount > 0 ? 0.0f : __fdiv_rn(wres, fmaxf(free_vol, 1.0e-30f));
 }
 
+// (coarse levels hold fewer than 2^31 cells: 32-bit division)
 __device__ __forceinline__ void pk_ijk(const LevelDev& L, int64_t t, int& i, int& j, int& k) {
-  k = (int)(t % L.nz);
-  const int64_t ij = t / L.nz;
-  j = (int)(ij % L.ny);
-  i = (int)(ij / L.ny);
+  const unsigned u = (unsigned)t, nz = (unsigned)L.nz, ny = (unsigned)L.ny;
+  const unsigned ij = u / nz;
+  k = (int)(u - ij * nz);
+  i = (int)(ij / ny);
+  j = (int)(ij - (unsigned)i * ny);
 }
 
 #define PK_CELLS(L, t)                                                                    \
@@ -1084,10 +1102,10 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_coarse(const __grid_constan
   const ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
   int cur[kTailMaxLevels];
   // down
-  for (int l = 1; l < lt; ++l) {
+  for (int l = D.first; l < lt; ++l) {
     const LevelDev& L = T.L[l];
     float* buf[2] = {D.pa[l], D.pb[l]};
-    if (l == 1) pk_sweep(L, nullptr, D.rhs[1], buf[0], T.outlet, T.omega, none);
+    if (l == D.first) pk_sweep(L, nullptr, D.rhs[l], buf[0], T.outlet, T.omega, none);
     int c = 0;
     for (int it = 1; it < T.pre; ++it) {
       if (!coarse_barrier(D)) return;
@@ -1113,7 +1131,7 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_coarse(const __grid_constan
   if (!coarse_barrier(D)) return;
   // up
   const float* fin = T.p_out;  // final iterate of level l + 1
-  for (int l = lt - 1; l >= 1; --l) {
+  for (int l = lt - 1; l >= D.first; --l) {
     const LevelDev& L = T.L[l];
     const LevelDev& C = T.L[l + 1];
     const ProlongSrc pr{fin, C.nx, C.ny, C.nz, T.scale};
@@ -1127,7 +1145,7 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_coarse(const __grid_constan
       src = seq[it & 1];
     }
     fin = src;
-    if (l > 1 && !coarse_barrier(D)) return;
+    if (l > D.first && !coarse_barrier(D)) return;
   }
 }
 #undef PK_CELLS
@@ -2012,12 +2030,83 @@ static void configure_tail(efsi_fv_plan* P) {
 // the tail exists and starts at level 2 or deeper, cooperative launches are
 // supported, and EFSI_NO_COARSE_KERNEL is unset: as many blocks as fit on the
 // GPU at once (at most two per SM), each with the tail's shared memory.
+// Sets up the cluster form of the coarse-level kernel: levels 2 .. lt-1 and
+// the tail on one cluster of `ctas` CTAs (one per SM).  Returns false with a
+// note when the device cannot run it.
+static bool configure_coarse_cluster(efsi_fv_plan* P, int ctas) {
+  if (P->tail_level < 3 || P->tail_level >= P->n_levels) {
+    P->coarse_note = "no level between 1 and the tail (tail level " + std::to_string(P->tail_level) + " of " +
+                     std::to_string(P->n_levels) + " levels)";
+    return false;
+  }
+  if (ctas < 2 || ctas > 16) {
+    P->coarse_note = "EFSI_COARSE_CLUSTER must be 2 .. 16";
+    return false;
+  }
+  static std::mutex attr_mutex;
+  static int attr_bytes = 0;
+  static bool nonportable = false;
+  cudaError_t e = cudaSuccess;
+  {
+    std::lock_guard<std::mutex> lock(attr_mutex);
+    if ((int)P->tail_smem_bytes > attr_bytes) {
+      e = cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->tail_smem_bytes);
+      if (e == cudaSuccess) attr_bytes = (int)P->tail_smem_bytes;
+    }
+    if (e == cudaSuccess && ctas > 8 && !nonportable) {
+      e = cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e == cudaSuccess) nonportable = true;
+    }
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    P->coarse_note = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+    return false;
+  }
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)ctas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ctas);
+  cfg.blockDim = dim3(kTailThreads);
+  cfg.dynamicSmemBytes = P->tail_smem_bytes;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  e = cudaOccupancyMaxActiveClusters(&clusters, k_mg_coarse, &cfg);
+  if (e != cudaSuccess || clusters < 1) {
+    cudaGetLastError();
+    P->coarse_note = std::string("cluster occupancy: ") + cudaGetErrorString(e) + ", clusters " +
+                     std::to_string(clusters);
+    return false;
+  }
+  P->coarse_blocks = ctas;
+  P->coarse_first = 2;
+  P->coarse_cluster = 1;
+  P->coarse_note = "";
+  return true;
+}
+
 static void configure_coarse(efsi_fv_plan* P) {
   P->coarse_blocks = 0;
+  P->coarse_first = 1;
+  P->coarse_cluster = 0;
+  if (std::getenv("EFSI_NO_COARSE_KERNEL") != nullptr) {
+    P->coarse_note = "the coarse-level kernel is off (EFSI_NO_COARSE_KERNEL)";
+    return;
+  }
+  if (const char* cl = std::getenv("EFSI_COARSE_CLUSTER")) {
+    if (std::atoi(cl) > 0) {
+      configure_coarse_cluster(P, std::atoi(cl));
+      return;
+    }
+  }
   // opt-in (EFSI_COARSE_KERNEL=1): on a B200 the per-level launches measured
   // faster (c2: 94 us against 143 us per V-cycle for levels 1-6)
   const char* on = std::getenv("EFSI_COARSE_KERNEL");
-  if (on == nullptr || std::atoi(on) == 0 || std::getenv("EFSI_NO_COARSE_KERNEL") != nullptr) {
+  if (on == nullptr || std::atoi(on) == 0) {
     P->coarse_note = "the cooperative coarse-level kernel is off (EFSI_COARSE_KERNEL=1 selects it)";
     return;
   }
@@ -2730,9 +2819,10 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
   // from P->tail_level on run inside k_mg_tail.
   const int lt = P->tail_level;
   // levels 1 .. lt-1 and the tail in one cooperative launch (k_mg_coarse)
-  const bool coarse_kernel = P->coarse_blocks > 0 && lt >= 2 && lt < nl;
+  const int cfirst = P->coarse_first;
+  const bool coarse_kernel = P->coarse_blocks > 0 && lt >= cfirst + 1 && lt < nl;
   std::vector<const void*> cur(nl, nullptr);
-  const int down_end = coarse_kernel ? 1 : (lt < nl) ? lt : nl - 1;
+  const int down_end = coarse_kernel ? cfirst : (lt < nl) ? lt : nl - 1;
   for (int l = 0; l < down_end; ++l) {
     LevelDev L = level_dev(P, l);
     LevelBuf& B = P->lv[l];
@@ -2798,7 +2888,7 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     T.rhs_in = P->lv[lt].rhs;
     T.p_out = (float*)P->lv[lt].pa;
     if (coarse_kernel) {
-      for (int l = 1; l < nl; ++l) {
+      for (int l = cfirst; l < nl; ++l) {
         T.L[l] = level_dev(P, l);
         D.pa[l] = (float*)P->lv[l].pa;
         D.pb[l] = (float*)P->lv[l].pb;
@@ -2808,9 +2898,18 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       D.fault = &P->sc->fault;
       static const unsigned spin_ns = std::getenv("EFSI_COARSE_SPIN_NS") ? (unsigned)std::atoi(std::getenv("EFSI_COARSE_SPIN_NS")) : 0u;
       D.spin_ns = spin_ns;
+      D.first = cfirst;
+      D.cluster = P->coarse_cluster;
       cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeCooperative;
-      attr[0].val.cooperative = 1;
+      if (P->coarse_cluster) {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)P->coarse_blocks;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+      } else {
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+      }
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3((unsigned)P->coarse_blocks);
       cfg.blockDim = dim3(kTailThreads);
@@ -2819,12 +2918,12 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       EFSI_COUNTED cudaLaunchKernelEx(&cfg, k_mg_coarse, D);
-      // the kernel's final level-1 iterate: the pre-sweeps end in buffer
-      // (pre - 1) & 1, the post-sweeps alternate from the other one
+      // the kernel's final iterate of level cfirst: the pre-sweeps end in
+      // buffer (pre - 1) & 1, the post-sweeps alternate from the other one
       const int c = (pre - 1) & 1;
-      void* bufs1[2] = {P->lv[1].pa, P->lv[1].pb};
+      void* bufs1[2] = {P->lv[cfirst].pa, P->lv[cfirst].pb};
       void* seq1[2] = {bufs1[1 - c], bufs1[c]};
-      cur[1] = seq1[(post - 1) & 1];
+      cur[cfirst] = seq1[(post - 1) & 1];
     } else {
       EFSI_COUNTED launch_pdl(k_mg_tail, 1, kTailThreads, P->tail_smem_bytes, s, T);
       cur[lt] = P->lv[lt].pa;
@@ -2846,7 +2945,7 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     cur[l] = c;
   }
   // Up: prolongation fused into the first post sweep.
-  const int up_start = coarse_kernel ? 0 : (lt < nl) ? lt - 1 : nl - 2;
+  const int up_start = coarse_kernel ? cfirst - 1 : (lt < nl) ? lt - 1 : nl - 2;
   for (int l = up_start; l >= 0; --l) {
     LevelBuf& B = P->lv[l];
     const LevelBuf& C = P->lv[l + 1];

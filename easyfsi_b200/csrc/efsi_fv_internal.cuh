@@ -304,6 +304,8 @@ struct efsi_fv_plan {
   int tail_coff[12] = {0};
   int tail_noff[12] = {0};
   int coarse_blocks = 0;               // grid of the cooperative coarse-level kernel (0: per-level launches)
+  int coarse_first = 1;                // first level the coarse-level kernel runs
+  int coarse_cluster = 0;              // 1: one thread-block cluster of coarse_blocks CTAs, hardware barriers
   unsigned* coarse_bar = nullptr;      // its grid barrier: arrivals, generation
   std::string coarse_note;             // why the per-level launches run instead
   std::string graph_error;

@@ -114,3 +114,64 @@ class StepGraph:
             self.close()
         except Exception:
             pass
+
+
+class BatchStepGraph:
+    """Independent coupled steps (one per instance) as ONE CUDA graph: the
+    capture forks a stream per instance from its origin stream and joins them
+    all back, so the graph holds one independent branch per instance and a
+    single launch advances every instance; branches of uneven size run
+    concurrently on the GPU.  Each instance's pressure solve must run its
+    device-side loop (``device_loop_solves``), and each step must make no
+    host reads and allocate nothing (run every step once eagerly first and
+    keep the reports off).  No reference counterpart."""
+
+    def __init__(self) -> None:
+        self._handle = None
+        self._streams = []
+
+    def capture(self, steps) -> None:
+        from ctypes import byref, c_void_p
+
+        self.close()
+        origin = torch.cuda.Stream()
+        origin.wait_stream(torch.cuda.current_stream())
+        streams = [torch.cuda.Stream() for _ in steps]
+        handle = c_void_p()
+        with torch.cuda.stream(origin):
+            _native.call("efsi_step_graph_begin", c_void_p(origin.cuda_stream))
+            try:
+                fork = torch.cuda.Event()
+                fork.record(origin)
+                joins = []
+                for st, step in zip(streams, steps):
+                    st.wait_event(fork)
+                    with torch.cuda.stream(st):
+                        step()
+                    ev = torch.cuda.Event()
+                    ev.record(st)
+                    joins.append(ev)
+                for ev in joins:
+                    origin.wait_event(ev)
+            finally:
+                _native.call("efsi_step_graph_end", c_void_p(origin.cuda_stream), byref(handle))
+        self._handle = handle
+        self._streams = [origin] + streams
+
+    def launch(self) -> None:
+        from ctypes import c_void_p
+
+        if self._handle is None:
+            raise RuntimeError("no batch step graph has been captured")
+        _native.call("efsi_step_graph_launch", self._handle, c_void_p(torch.cuda.current_stream().cuda_stream))
+
+    def close(self) -> None:
+        if self._handle is not None and self._handle.value:
+            _native.call("efsi_step_graph_destroy", self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

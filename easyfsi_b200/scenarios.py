@@ -11,7 +11,11 @@ particles (8 per MPM cell, jittered) and wrapped by surface markers.
   [0.3, 0.7]^2 x [0.2, 0.8] and growing by 1.05 per cell outward, ellipsoid with
   semi-axes (0.12, 0.08, 0.2), E = 5e4 Pa, dt = 5e-5 (about 200k particles);
 * ``c3``: 256^3 with the same grading law, two spheres r = 0.1 with
-  E = 2e4 / 2e5 Pa, dt = 2e-5 (about 500k particles).
+  E = 2e4 / 2e5 Pa, dt = 2e-5 (about 500k particles);
+* ``c5`` (``batched_configs``): 32 independent instances, uniform grids of
+  48^3, 64^3, 96^3 or 128^3 cells (seeded per instance), each with one sphere
+  of seeded radius in [0.08, 0.18] and Young's modulus log-uniform in
+  [1e4, 1e6] Pa, 8 particles per cell, dt = 1e-4.
 
 One coupled step (``CoupledScene.step``) is: predict -> project (flexible
 MG-PCG to relative residual 1e-8) -> marker pressure tractions -> marker forces
@@ -114,6 +118,39 @@ CONFIGS = {
         marker_resolution=(48, 96),
     ),
 }
+
+
+BATCH_GRID_SIZES = (48, 64, 96, 128)
+
+
+def batched_configs(count: int = 32, seed: int = 5000, sizes: tuple[int, ...] = BATCH_GRID_SIZES) -> list[ScenarioConfig]:
+    """The uneven batch of independent instances: instance i draws, from
+    seed + i, its uniform grid size (one of `sizes`, the same along every
+    axis and for the MPM grid), a sphere radius in [0.08, 0.18] and a Young's
+    modulus log-uniform in [1e4, 1e6] Pa; the sphere sits at
+    (0.5, 0.5, 0.4), dt = 1e-4."""
+    out = []
+    for i in range(count):
+        rng = np.random.default_rng(seed + i)
+        n = int(rng.choice(np.asarray(sizes)))
+        radius = float(rng.uniform(0.08, 0.18))
+        youngs = float(10.0 ** rng.uniform(4.0, 6.0))
+        out.append(
+            ScenarioConfig(
+                name=f"c5_{i:02d}_uniform{n}_r{radius:.3f}",
+                grid_nodes=(n, n, n),
+                graded=False,
+                refine_box=None,
+                mpm_nodes=(n, n, n),
+                bodies=(Body((0.5, 0.5, 0.4), (radius, radius, radius), youngs, PRIMARY_REGION_ID),),
+                dt_s=1.0e-4,
+                steps=50,
+                velocity_seed=seed + 100 + i,
+                particle_seed=seed + 200 + i,
+                marker_resolution=(24, 48),
+            )
+        )
+    return out
 
 
 def tiny_config(n: int = 12, mpm: int = 12, seed: int = 7) -> ScenarioConfig:

@@ -378,26 +378,38 @@ def test_march_kernels_match_per_cell_kernels(n, aux):
     assert rel_l2(fm.pressure.to_numpy(), fc.pressure.to_numpy()) <= 1e-12
 
 
-@pytest.mark.parametrize("n,aux", [((40, 24, 48), False), ((64, 48, 96), False), ((64, 48, 96), True)])
-def test_coarse_kernel_matches_per_level_launches(n, aux):
-    """The cooperative coarse-level kernel (levels 1 .. lt-1 and the tail in
-    one launch; opt-in, EFSI_COARSE_KERNEL=1) reproduces the per-level
-    launches: the same rows in the same order, so the V-cycle agrees bit for
-    bit and the PCG takes the same path; it replaces the coarse launches of
-    every V-cycle."""
+@pytest.mark.parametrize(
+    "n,aux,env",
+    [
+        ((40, 24, 48), False, ("EFSI_COARSE_KERNEL", "1")),
+        ((64, 48, 96), False, ("EFSI_COARSE_KERNEL", "1")),
+        ((64, 48, 96), True, ("EFSI_COARSE_KERNEL", "1")),
+        ((64, 48, 96), False, ("EFSI_COARSE_CLUSTER", "8")),
+        ((64, 48, 96), True, ("EFSI_COARSE_CLUSTER", "16")),
+        ((128, 64, 128), False, ("EFSI_COARSE_CLUSTER", "16")),
+    ],
+)
+def test_coarse_kernel_matches_per_level_launches(n, aux, env):
+    """The coarse-level kernel reproduces the per-level launches: the same
+    rows in the same order, so the V-cycle agrees bit for bit and the PCG
+    takes the same path; it replaces the coarse launches of every V-cycle.
+    Two forms: cooperative over the whole GPU for levels 1 .. lt-1 and the
+    tail (EFSI_COARSE_KERNEL=1), and one thread-block cluster for levels
+    2 .. lt-1 and the tail (EFSI_COARSE_CLUSTER=<CTAs>)."""
     from easyfsi_b200 import _native
 
     import os
 
-    saved = os.environ.get("EFSI_COARSE_KERNEL")
-    os.environ["EFSI_COARSE_KERNEL"] = "1"
+    key, value = env
+    saved = os.environ.get(key)
+    os.environ[key] = value
     try:
         grid, (fk, fl_) = _paired_solvers(n, aux, alt_env={"EFSI_NO_COARSE_KERNEL": "1"})
     finally:
         if saved is None:
-            os.environ.pop("EFSI_COARSE_KERNEL", None)
+            os.environ.pop(key, None)
         else:
-            os.environ["EFSI_COARSE_KERNEL"] = saved
+            os.environ[key] = saved
     blocks, notes = [], []
     for fl in (fk, fl_):
         b = ctypes.c_int32(0)
@@ -1177,6 +1189,46 @@ def test_device_loop_runs_past_the_first_block():
     assert it_h > 16
     assert it_d == ((it_h + 15) // 16) * 16
     assert rel_l2(p_d, p_h) <= 1e-10
+
+
+def test_batch_step_graph_replays_the_eager_steps():
+    """Three instances of different sizes captured as ONE graph
+    (runtime.BatchStepGraph: a branch per instance, device-side PCG loops)
+    and replayed twice leave every instance in the state of two eager steps
+    from the same start (to the order of the f32 atomic sums, 1e-6), with
+    the eager CG iteration count rounded up to the 16-iteration check."""
+    from easyfsi_b200.runtime import BatchStepGraph
+    from easyfsi_b200.scenarios import CoupledScene, batched_configs, tiny_config
+
+    cfgs = [tiny_config(12), tiny_config(16, mpm=16, seed=9), batched_configs(1, sizes=(32,))[0]]
+    pairs = []
+    for cfg in cfgs:
+        u0 = CoupledScene(cfg).fluid.velocity.to_numpy()
+        a = CoupledScene(cfg, initial_velocity=u0, project_initial=False)
+        b = CoupledScene(cfg, initial_velocity=u0, project_initial=False)
+        b.fluid.device_loop_solves = True
+        a.step()
+        b.step()
+        pairs.append((a, b))
+    graph = BatchStepGraph()
+    graph.capture([b.step for _, b in pairs])
+    for _ in range(2):
+        for a, _ in pairs:
+            a.step()
+        graph.launch()
+    torch.cuda.synchronize()
+    for a, b in pairs:
+        b.fluid.read_device_pcg_stats()
+        assert b.fluid.last_cg_converged
+        assert b.fluid.last_cg_iterations == ((a.fluid.last_cg_iterations + 15) // 16) * 16
+        n = a.solid.particle_count
+        for fa, fb in ((a.fluid.pressure, b.fluid.pressure), (a.fluid.velocity, b.fluid.velocity),
+                       (a.solid.x, b.solid.x), (a.solid.v, b.solid.v), (a.markers.x_gamma_m, b.markers.x_gamma_m)):
+            xa, xb = fa.to_numpy(), fb.to_numpy()
+            if fa is a.solid.x or fa is a.solid.v:
+                xa, xb = xa[:n], xb[:n]
+            assert rel_l2(xb, xa) <= 1e-6
+    graph.close()
 
 
 def test_whole_step_graph_replays_the_eager_steps():
