@@ -382,7 +382,7 @@ def graph_step_arm(scene, steps: int, warmup: int, world: int, plain_value: floa
         fl.device_loop_solves = False
 
 
-def batched_arm(steps: int, warmup: int, world: int, count: int) -> dict:
+def batched_arm(steps: int, warmup: int, world: int, count: int, autotune: bool = True) -> dict:
     """The c5 batch: `count` independent coupled instances of uneven size
     (uniform 48^3 .. 128^3 grids, 2k-340k particles each).  Eager: every
     instance's step in turn on one stream (host reads at the PCG's 16-iteration
@@ -400,6 +400,7 @@ def batched_arm(steps: int, warmup: int, world: int, count: int) -> dict:
     t0 = time.perf_counter()
     cfgs = batched_configs(count)
     scenes = [CoupledScene(c) for c in cfgs]
+    picks = [sc.fluid.autotune() for sc in scenes] if autotune else None
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     cells = int(sum(int(np.prod(c.grid_nodes)) for c in cfgs))
@@ -463,6 +464,7 @@ def batched_arm(steps: int, warmup: int, world: int, count: int) -> dict:
         "cg_iterations_eager": eager_iters,
         "cg_iterations_graph": g_iters,
         "setup_s": setup_s,
+        "autotune_blocks_per_sm": [[p["blocks_per_sm"] for p in pk] for pk in picks] if picks else None,
     }
     del scenes
     torch.cuda.empty_cache()
@@ -555,6 +557,7 @@ def main() -> None:
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
     ap.add_argument("--no-graph-step", action="store_true", help="skip the whole-step CUDA graph arm")
     ap.add_argument("--no-batched", action="store_true", help="skip the c5 batched-instances arm")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default V-cycle launch shapes")
     ap.add_argument("--batch-count", type=int, default=32, help="instances of the c5 batched arm")
     ap.add_argument("--learned-train-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -583,6 +586,8 @@ def main() -> None:
 
     scene = CoupledScene(cfg)
     stream = torch.cuda.current_stream()
+    # the V-cycle's launch shapes come from the project's autotuner
+    autotune = None if args.no_autotune else scene.fluid.autotune()
 
     def barrier():
         if world > 1:
@@ -765,7 +770,7 @@ def main() -> None:
     batched = None
     if not args.no_batched:
         try:
-            batched = batched_arm(args.steps, args.warmup, world, args.batch_count)
+            batched = batched_arm(args.steps, args.warmup, world, args.batch_count, not args.no_autotune)
         except Exception as exc:  # reported, never fatal to the step's line
             batched = {"error": f"{type(exc).__name__}: {exc}"}
     dom = max(fam_stats, key=lambda f: fam_stats[f]["ms_per_step"])
@@ -843,6 +848,7 @@ def main() -> None:
             "learned": learned,
             "particle_families": particle_families,
             "kernel_families": fam_stats,
+            "autotune": autotune,
             "preconditioner": vcycle_stats,
             "pressure_solve": psolve,
             "ib_node_search": ib_search,

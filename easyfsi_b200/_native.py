@@ -164,6 +164,7 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_kernel_timing_enable": [I, I],
     "efsi_kernel_timing_read": [I, POINTER(ctypes.c_int64), POINTER(c_double), POINTER(c_double)],
     "efsi_fv_kernel_replay": [P, I, I, POINTER(c_double), POINTER(c_double), P],
+    "efsi_fv_autotune": [P, I, POINTER(I), POINTER(c_double), I, P],
     "efsi_fv_plan_create": [POINTER(LevelDesc), I, I, POINTER(c_void_p)],
     "efsi_fv_plan_destroy": [P],
     "efsi_fv_set_masks": [P, P, P, P, P, P],

@@ -2244,6 +2244,7 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
       int64_t march_min = 0;
       if (const char* env = std::getenv("EFSI_MARCH_MIN_CELLS")) march_min = std::atoll(env);
       B.march = B.nz >= 16 && B.ny >= 8 && B.n >= march_min && std::getenv("EFSI_NO_MARCH") == nullptr;
+      B.march_ok = B.march;
       B.mchunk = mc.chunk;
       B.mgrid = mc.grid;
     }
@@ -3788,6 +3789,102 @@ extern "C" {
 // Benchmark helper (no counterpart in the reference): launch one level-0
 // kernel family `reps` times back to back on the plan's own work buffers and
 // report the mean CUDA-event duration per launch and its algorithmic bytes.
+// Tile autotuner of the V-cycle's per-level launches.  For every level that
+// launches its own kernels (those above the single-CTA tail), each candidate
+// launch shape is timed with CUDA events over `reps` back-to-back pairs of
+// the level's plain sweep and its restriction (the sweep alone on a coarsest
+// level without a tail), after two untimed pairs: the plane-marching kernels
+// with 3 (the default), 1, 2, 4 or 6 blocks' worth of planes per SM and, on
+// levels >= 1, the tiled / per-cell kernels.  A candidate replaces the best so
+// far only when it is more than 3% faster.  Level 0 keeps the plane march
+// whenever it can run (the PCG's dots are fused into its last sweep).  Every
+// candidate computes the same rows; only the block partition of the z-mean /
+// dot partial sums of level 0 follows the chosen shape.  Captured PCG graphs
+// are dropped, so the next solve records the tuned launches.
+int efsi_fv_autotune(efsi_fv_plan* P, int32_t reps, int32_t* choice, double* best_us, int32_t max_levels,
+                     void* stream) {
+  EFSI_TRY(level_zero_check(P));
+  EFSI_ARG_CHECK(reps > 0 && max_levels >= 0 && (max_levels == 0 || (choice != nullptr && best_us != nullptr)),
+                 "invalid autotune arguments");
+  cudaStream_t s = as_stream(stream);
+  int dev = 0, nsm = 0;
+  EFSI_CUDA_CHECK(cudaGetDevice(&dev));
+  EFSI_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  for (int l = 0; l < max_levels; ++l) {
+    choice[l] = -1;
+    best_us[l] = 0.0;
+  }
+  const int nl = P->n_levels;
+  const int last = P->tail_level < nl ? P->tail_level : nl;
+  const ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
+  const double om = (double)0.8f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  EFSI_CUDA_CHECK(cudaEventCreate(&e0));
+  EFSI_CUDA_CHECK(cudaEventCreate(&e1));
+  int rc = EFSI_OK;
+  for (int l = 0; l < last && rc == EFSI_OK; ++l) {
+    LevelBuf& B = P->lv[l];
+    std::vector<int> cands;
+    if (B.march_ok) {
+      cands = {3, 1, 2, 4, 6};
+      if (l > 0) cands.push_back(0);
+    } else {
+      cands = {0};
+    }
+    auto apply = [&](int m) {
+      if (m == 0) {
+        B.march = false;
+      } else {
+        const MarchCfg mc = march_cfg(B.nx, B.ny, B.nz, nsm * m);
+        B.march = true;
+        B.mchunk = mc.chunk;
+        B.mgrid = mc.grid;
+      }
+    };
+    auto pair = [&]() {
+      if (l == 0) {
+        launch_sweep<double, true, false>(P, 0, (const double*)B.pa, P->r, (double*)B.pb, 0, om, none, nullptr, s);
+        if (nl > 1) launch_restrict<double, true>(P, 0, (const double*)B.pa, P->r, 0, s);
+      } else {
+        launch_sweep<float, false, false>(P, l, (const float*)B.pa, B.rhs, (float*)B.pb, 0, om, none, nullptr, s);
+        if (l + 1 < nl) launch_restrict<float, false>(P, l, (const float*)B.pa, B.rhs, 0, s);
+      }
+    };
+    int best = cands[0];
+    float best_ms = 0.0f;
+    for (size_t q = 0; q < cands.size(); ++q) {
+      apply(cands[q]);
+      for (int w = 0; w < 2; ++w) pair();
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < reps; ++r) pair();
+      cudaEventRecord(e1, s);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess) e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        set_error(std::string("autotune: ") + cudaGetErrorString(e));
+        rc = EFSI_ERR_CUDA;
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (q == 0 || ms < 0.97f * best_ms) {
+        best = cands[q];
+        best_ms = ms;
+      }
+    }
+    apply(best);
+    if (l < max_levels) {
+      choice[l] = best;
+      best_us[l] = 1000.0 * (double)best_ms / reps;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (PcgGraph& g : P->graphs) cudaGraphExecDestroy(g.exec);
+  P->graphs.clear();
+  return rc;
+}
+
 int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double* avg_ms, double* bytes_per_launch,
                           void* stream) {
   EFSI_TRY(level_zero_check(P));

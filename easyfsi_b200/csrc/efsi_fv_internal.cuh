@@ -219,6 +219,7 @@ struct LevelBuf {
   bool tiled = false;  // the tiled 32 x 8 x 4 kernels run on this level
   unsigned tgrid = 1;  // their grid-stride grid size
   bool march = false;  // the plane-marching stencil kernels run on this level
+  bool march_ok = false;  // they can (set at plan creation; the autotuner may switch them off)
   int mchunk = 2;      // their planes per block
   unsigned mgrid = 1;  // and grid size
 };

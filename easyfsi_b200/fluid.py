@@ -493,6 +493,19 @@ class CartesianFluidSolver:
         _native.call("efsi_fv_set_learned_preconditioner", self._plan, handle, _stream())
         self._learned_network = network
 
+    def autotune(self, reps: int = 10) -> list[dict]:
+        """Tile autotuner of the V-cycle (``efsi_fv_autotune``; no reference
+        counterpart): times each level's sweep + restriction under every
+        candidate launch shape and keeps the fastest.  Returns, per tuned
+        level, the blocks-per-SM multiple picked (0: tiled / per-cell kernels)
+        and its time per sweep + restriction in microseconds."""
+        self._refresh_structure()
+        n = 16
+        choice = (ctypes.c_int32 * n)()
+        best = (ctypes.c_double * n)()
+        _native.call("efsi_fv_autotune", self._plan, int(reps), choice, best, n, _stream())
+        return [{"level": l, "blocks_per_sm": int(choice[l]), "us": float(best[l])} for l in range(n) if choice[l] >= 0]
+
     def read_device_pcg_stats(self) -> None:
         """After a captured step ran: the statistics of its device-side PCG loop
         (``efsi_fv_pcg_device_stats``) into ``last_cg_*``."""

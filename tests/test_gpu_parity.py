@@ -1269,3 +1269,38 @@ def test_whole_step_graph_replays_the_eager_steps():
             xa, xb = xa[:n], xb[:n]
         assert rel_l2(xb, xa) <= 1e-6
     graph.close()
+
+
+def test_autotuned_plan_matches_the_default_launches():
+    """The tile autotuner (efsi_fv_autotune) changes only launch shapes: after
+    it, the V-cycle gives the default plan's z to rounding of the z-mean's
+    block partition, and the PCG takes the same iterations to the same
+    pressure and residual."""
+    grid, (fa, fb) = _paired_solvers((64, 48, 96), False, alt_env={"EFSI_NO_COARSE_KERNEL": "1"})
+    picks = fa.autotune(reps=3)
+    assert picks and picks[0]["level"] == 0 and picks[0]["blocks_per_sm"] > 0
+    assert all(p["us"] > 0.0 for p in picks)
+    rng = np.random.default_rng(29)
+    r = rng.normal(size=grid.grid_nodes)
+    r[fa.obstacle.to_numpy() == 1] = 0.0
+    zs = []
+    for fl in (fa, fb):
+        fl.cg_r.from_numpy(r)
+        fl._apply_fv_multigrid_preconditioner(fl.cg_r, pressure_outlet_zmin=False)
+        zs.append(fl.cg_z.to_numpy())
+    assert rel_l2(zs[0], zs[1]) <= 1e-13
+    div = rng.normal(size=grid.grid_nodes).astype(np.float32)
+    res = []
+    for fl in (fa, fb):
+        fl.divergence.from_numpy(div)
+        fl.pressure.tensor.zero_()
+        fl._solve_pressure_poisson_fv_cg(iterations=300, rhs_scale=1.0e6, pressure_outlet_zmin=False, tolerance=1e-10,
+                                         preconditioner="fv_multigrid")
+        res.append((fl.last_cg_iterations, fl.pressure.to_numpy(), fl.last_cg_converged, fl.last_cg_relative_residual,
+                    fl.last_cg_breakdown, fl.last_cg_restart_count))
+    # (this random right-hand side is not compatible with the obstacle
+    # pockets' null spaces: both solves stop at the same residual floor)
+    info = [(it, conv, rr, why, rs) for it, _, conv, rr, why, rs in res]
+    assert res[0][0] == res[1][0], (info, picks)
+    assert res[0][3] == pytest.approx(res[1][3], rel=1e-6), (info, picks)
+    assert rel_l2(res[0][1], res[1][1]) <= 1e-10
