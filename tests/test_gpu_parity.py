@@ -1298,8 +1298,10 @@ def test_autotuned_plan_matches_the_default_launches():
                                          preconditioner="fv_multigrid")
         res.append((fl.last_cg_iterations, fl.pressure.to_numpy(), fl.last_cg_converged, fl.last_cg_relative_residual,
                     fl.last_cg_breakdown, fl.last_cg_restart_count))
-    # (this random right-hand side is not compatible with the obstacle
-    # pockets' null spaces: both solves stop at the same residual floor)
+    # (a random right-hand side on a graded grid is not compatible with the
+    # operator's constant null space: the V-weighted mean removal of the
+    # reference leaves an unweighted sum of 8e-4 of its 1-norm, so both
+    # solves, like the oracle's, stop at the same residual floor near 6e-7)
     info = [(it, conv, rr, why, rs) for it, _, conv, rr, why, rs in res]
     assert res[0][0] == res[1][0], (info, picks)
     assert res[0][3] == pytest.approx(res[1][3], rel=1e-6), (info, picks)
