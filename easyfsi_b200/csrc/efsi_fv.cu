@@ -3791,9 +3791,10 @@ extern "C" {
 // report the mean CUDA-event duration per launch and its algorithmic bytes.
 // Tile autotuner of the V-cycle's per-level launches.  For every level that
 // launches its own kernels (those above the single-CTA tail), each candidate
-// launch shape is timed with CUDA events over `reps` back-to-back pairs of
-// the level's plain sweep and its restriction (the sweep alone on a coarsest
-// level without a tail), after two untimed pairs: the plane-marching kernels
+// launch shape is timed with CUDA events over `reps` back-to-back units after
+// two untimed ones -- on level 0 the PCG's direction SpMV and a whole V-cycle
+// with the dots fused in, on a coarse level its plain sweep and restriction
+// (the sweep alone on a coarsest level without a tail): the plane-marching kernels
 // with 3 (the default), 1, 2, 4 or 6 blocks' worth of planes per SM and, on
 // levels >= 1, the tiled / per-cell kernels.  A candidate replaces the best so
 // far only when it is more than 3% faster.  Level 0 keeps the plane march
@@ -3818,6 +3819,7 @@ int efsi_fv_autotune(efsi_fv_plan* P, int32_t reps, int32_t* choice, double* bes
   const int last = P->tail_level < nl ? P->tail_level : nl;
   const ProlongSrc none{nullptr, 0, 0, 0, 0.0f};
   const double om = (double)0.8f;
+  EFSI_TRY(ensure_rden(P, 0, s));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   EFSI_CUDA_CHECK(cudaEventCreate(&e0));
   EFSI_CUDA_CHECK(cudaEventCreate(&e1));
@@ -3843,8 +3845,13 @@ int efsi_fv_autotune(efsi_fv_plan* P, int32_t reps, int32_t* choice, double* bes
     };
     auto pair = [&]() {
       if (l == 0) {
-        launch_sweep<double, true, false>(P, 0, (const double*)B.pa, P->r, (double*)B.pb, 0, om, none, nullptr, s);
-        if (nl > 1) launch_restrict<double, true>(P, 0, (const double*)B.pa, P->r, 0, s);
+        // level 0: the direction SpMV and a whole V-cycle with the PCG dots
+        // fused in (every level-0 plane march of a PCG iteration)
+        const LevelDev L0 = level_dev(P, 0);
+        if (!launch_march_spmv(P, L0, false, P->z, P->d0, P->d1, P->Ad, 0, P->partials, P->sc, s))
+          launch_sweep<double, true, false>(P, 0, (const double*)B.pa, P->r, (double*)B.pb, 0, om, none, nullptr, s);
+        bool fused = false;
+        if (vcycle(P, P->r, P->z, 0, 2, 24, 2, true, s, P->delta, &fused) != EFSI_OK) rc = EFSI_ERR_CUDA;
       } else {
         launch_sweep<float, false, false>(P, l, (const float*)B.pa, B.rhs, (float*)B.pb, 0, om, none, nullptr, s);
         if (l + 1 < nl) launch_restrict<float, false>(P, l, (const float*)B.pa, B.rhs, 0, s);

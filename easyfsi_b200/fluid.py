@@ -495,10 +495,12 @@ class CartesianFluidSolver:
 
     def autotune(self, reps: int = 10) -> list[dict]:
         """Tile autotuner of the V-cycle (``efsi_fv_autotune``; no reference
-        counterpart): times each level's sweep + restriction under every
-        candidate launch shape and keeps the fastest.  Returns, per tuned
-        level, the blocks-per-SM multiple picked (0: tiled / per-cell kernels)
-        and its time per sweep + restriction in microseconds."""
+        counterpart): times a unit of each level's work (level 0: the PCG's
+        direction SpMV and a whole V-cycle; a coarse level: its sweep and
+        restriction) under every candidate launch shape and keeps the
+        fastest.  Returns, per tuned level, the blocks-per-SM multiple picked
+        (0: tiled / per-cell kernels) and the time of its unit in
+        microseconds."""
         self._refresh_structure()
         n = 16
         choice = (ctypes.c_int32 * n)()

@@ -60,13 +60,14 @@ int efsi_fv_kernel_replay(efsi_fv_plan* plan, int32_t family, int32_t reps, doub
                           double* bytes_per_launch, void* stream);
 
 /* Tile autotuner of the V-cycle (no counterpart in the reference): for every
- * level that launches its own kernels, times the level's sweep + restriction
- * under each candidate launch shape (plane-marching kernels with 3, 1, 2, 4
- * or 6 blocks' worth of planes per SM; on levels >= 1 also the tiled /
- * per-cell kernels) and keeps the fastest on the plan.  choice[l] is the
- * blocks-per-SM multiple picked (0: tiled / per-cell kernels, -1: level not
- * tuned) and best_us[l] its time per sweep + restriction, for
- * l < max_levels.  Needs the masks; drops the plan's captured PCG graphs
+ * level that launches its own kernels, times a unit of its work -- level 0:
+ * the PCG's direction SpMV plus a whole V-cycle with the dots fused in; a
+ * coarse level: its sweep + restriction -- under each candidate launch shape
+ * (plane-marching kernels with 3, 1, 2, 4 or 6 blocks' worth of planes per
+ * SM; on levels >= 1 also the tiled / per-cell kernels) and keeps the
+ * fastest on the plan.  choice[l] is the blocks-per-SM multiple picked (0:
+ * tiled / per-cell kernels, -1: level not tuned) and best_us[l] the time of
+ * its unit, for l < max_levels.  Needs the masks; drops the plan's captured PCG graphs
  * (the next solve records the tuned launches; a step graph captured before
  * must be captured again). */
 int efsi_fv_autotune(efsi_fv_plan* plan, int32_t reps, int32_t* choice, double* best_us, int32_t max_levels,
