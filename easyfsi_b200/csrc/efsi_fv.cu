@@ -2739,9 +2739,13 @@ static void launch_sweep(efsi_fv_plan* P, int l, const TP* p, const void* rhs, T
                                                                                    partials, P->sc);
 }
 
-// Residual of level l's iterate p restricted into level l+1's rhs.
+// Residual of level l's iterate p restricted into level l+1's rhs.  With
+// `czero` (level l+1's first iterate buffer) the plane-marching restriction
+// also writes level l+1's zero-guess sweep there (damping omega); returns
+// whether it did, so that the caller skips that sweep's own launch.
 template <typename TP, bool kNegR>
-static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs, int outlet, cudaStream_t s) {
+static bool launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs, int outlet, cudaStream_t s,
+                            float* czero = nullptr, double omega = 0.0) {
   LevelDev L = level_dev(P, l);
   const LevelBuf& B = P->lv[l];
   const LevelBuf& C = P->lv[l + 1];
@@ -2752,17 +2756,19 @@ static void launch_restrict(efsi_fv_plan* P, int l, const TP* p, const void* rhs
     const CUtensorMap* mm = plane_map(P, l, B.mask, MAP_MASK);
     if (mp && mr && mm) {
       const int sm = march_smem<TP, 1, TR, true>();
+      const LevelDev LC = level_dev(P, l + 1);
       if (L.fw != nullptr || L.iface != nullptr)
-        EFSI_COUNTED launch_pdl(km_restrict<TP, kNegR, true>, B.mgrid, dim3(kMK, kTY), sm, s, 
-            L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
+        EFSI_COUNTED launch_pdl(km_restrict<TP, kNegR, true>, B.mgrid, dim3(kMK, kTY), sm, s, L, B.mchunk, *mp, *mr,
+                                *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc, LC, czero, omega);
       else
-        EFSI_COUNTED launch_pdl(km_restrict<TP, kNegR, false>, B.mgrid, dim3(kMK, kTY), sm, s, 
-            L, B.mchunk, *mp, *mr, *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc);
-      return;
+        EFSI_COUNTED launch_pdl(km_restrict<TP, kNegR, false>, B.mgrid, dim3(kMK, kTY), sm, s, L, B.mchunk, *mp, *mr,
+                                *mm, outlet, C.nx, C.ny, C.nz, C.rhs, P->sc, LC, czero, omega);
+      return czero != nullptr;
     }
   }
   EFSI_COUNTED launch_pdl(k_restrict<TP, kNegR, true>, C.shape.grid, C.shape.block, 0, s, L, p, rhs, outlet, C.nx, C.ny,
                                                                                  C.nz, C.rhs);
+  return false;
 }
 
 // The level-0 reciprocal denominators for this outlet mode (recomputed after
@@ -2787,6 +2793,19 @@ static int ensure_rden(efsi_fv_plan* P, int outlet, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // mixed: level 0 runs in FP32 (fv_multigrid_mixed; the caller checks that
 // level 0 has the plane-marching kernels and more than one level exists).
+// Whether the V-cycle forms coarse level c's zero-guess sweep inside the
+// restriction into it: c runs its own pre-sweeps (it lies above the tail and
+// below the coarse-level kernel's first level), or it is the coarsest level
+// of a hierarchy without a tail.  EFSI_NO_RESTRICT_SWEEP0 keeps the separate
+// launch.
+static bool vcycle_fuses_zero(const efsi_fv_plan* P, int c) {
+  static const bool off = std::getenv("EFSI_NO_RESTRICT_SWEEP0") != nullptr;
+  const int nl = P->n_levels, lt = P->tail_level;
+  const bool coarse_kernel = P->coarse_blocks > 0 && lt >= P->coarse_first + 1 && lt < nl;
+  const int down_end = coarse_kernel ? P->coarse_first : (lt < nl) ? lt : nl - 1;
+  return !off && c >= 1 && (c < down_end || (!coarse_kernel && lt >= nl && c == nl - 1));
+}
+
 static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int pre, int coarse, int post,
                   bool want_mean, cudaStream_t s, const double* dots_delta = nullptr, bool* dots_done = nullptr,
                   bool mixed = false) {
@@ -2824,6 +2843,10 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
   const bool coarse_kernel = P->coarse_blocks > 0 && lt >= cfirst + 1 && lt < nl;
   std::vector<const void*> cur(nl, nullptr);
   const int down_end = coarse_kernel ? cfirst : (lt < nl) ? lt : nl - 1;
+  // zero_done[l]: level l's zero-guess sweep was formed by the restriction
+  // into it (into lv[l].pa), so its own launch is skipped
+  std::vector<char> zero_done(nl, 0);
+  auto fuse_zero = [&](int c) { return vcycle_fuses_zero(P, c); };
   for (int l = 0; l < down_end; ++l) {
     LevelDev L = level_dev(P, l);
     LevelBuf& B = P->lv[l];
@@ -2851,22 +2874,27 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
                      (launch_sweep<double, true, false>(P, 0, (const double*)c, r, (double*)dst, outlet, om, none,
                                                         nullptr, s)));
       } else {
-        if (it == 0)
-          launch_sweep<float, false, true>(P, l, nullptr, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
-        else
+        if (it == 0) {
+          if (!zero_done[l])
+            launch_sweep<float, false, true>(P, l, nullptr, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
+        } else {
           launch_sweep<float, false, false>(P, l, (const float*)c, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
+        }
       }
       c = dst;
     }
     cur[l] = c;
     const LevelBuf& C = P->lv[l + 1];
+    float* cz = fuse_zero(l + 1) ? (float*)C.pa : nullptr;
+    bool fz = false;
     if (l == 0 && mixed)
-      launch_restrict<float, true>(P, 0, (const float*)c, r, outlet, s);
+      fz = launch_restrict<float, true>(P, 0, (const float*)c, r, outlet, s, cz, om);
     else if (l == 0)
-      EFSI_TIMED(KF_RESTRICT_L0, 17.0 * B.n + 4.0 * C.n, s,
-                 (launch_restrict<double, true>(P, 0, (const double*)c, r, outlet, s)));
+      EFSI_TIMED(KF_RESTRICT_L0, 17.0 * B.n + (cz ? 9.0 : 4.0) * C.n, s,
+                 (fz = launch_restrict<double, true>(P, 0, (const double*)c, r, outlet, s, cz, om)));
     else
-      launch_restrict<float, false>(P, l, (const float*)c, B.rhs, outlet, s);
+      fz = launch_restrict<float, false>(P, l, (const float*)c, B.rhs, outlet, s, cz, om);
+    zero_done[l + 1] = fz ? 1 : 0;
   }
   if (lt < nl) {
     CoarseDesc D;
@@ -2937,9 +2965,10 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     const void* c = nullptr;
     for (int it = 0; it < coarse; ++it) {
       void* dst = bufs[it & 1];
-      if (it == 0)
-        launch_sweep<float, false, true>(P, l, nullptr, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
-      else
+      if (it == 0) {
+        if (!zero_done[l])
+          launch_sweep<float, false, true>(P, l, nullptr, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
+      } else
         launch_sweep<float, false, false>(P, l, (const float*)c, B.rhs, (float*)dst, outlet, om, none, nullptr, s);
       c = dst;
     }
@@ -3937,8 +3966,10 @@ int efsi_fv_kernel_replay(efsi_fv_plan* P, int32_t family, int32_t reps, double*
           return EFSI_ERR_ARG;
         }
         const LevelBuf& C = P->lv[1];
-        bytes = 17.0 * n0 + 4.0 * (double)C.n;
-        launch_restrict<double, true>(P, 0, (const double*)P->lv[0].pa, P->r, 0, s);
+        // as in the V-cycle: with level 1's zero-guess sweep when it is fused
+        float* cz = vcycle_fuses_zero(P, 1) ? (float*)C.pa : nullptr;
+        bytes = 17.0 * n0 + (cz ? 9.0 : 4.0) * (double)C.n;
+        launch_restrict<double, true>(P, 0, (const double*)P->lv[0].pa, P->r, 0, s, cz, (double)0.8f);
         break;
       }
       case KF_CG_DOTS:

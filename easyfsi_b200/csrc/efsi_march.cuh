@@ -831,6 +831,27 @@ __global__ void __launch_bounds__(kMK* kTY, 3)
 // 2 x 2 x 2 children in the reference's order (i-pair outer, then j, then k)
 // with the f32 volume weights.
 // ---------------------------------------------------------------------------
+// The zero-guess damped-Jacobi sweep of one coarse row (km_sweep0<float,
+// kNegR = false> / k_sweep<float, false, true>: the neighbours are zero, so
+// ns = 0 and only the row's own denominator and rhs enter), evaluated by the
+// restriction that produced the row's rhs value v.
+__device__ __forceinline__ float coarse_zero_sweep(const LevelDev& C, int ci, int cj, int ck, int64_t cc, float v,
+                                                   int outlet, double omega) {
+  const unsigned m = __ldg(C.mask + cc);
+  float res = 0.0f;
+  if (!(m & M_SOLID)) {
+    double ns, den;
+    stencil_sel<true>(C, row_coef(C, cj, ck), __ldg(C.cxm + ci), __ldg(C.cxp + ci), ci, cj, ck, cc, m, outlet, 0.0,
+                      0.0, 0.0, 0.0, 0.0, 0.0, ns, den);
+    den += iface_at<float>(C, cc);
+    if (den > 0.0) {
+      const double jv = (ns - (double)v) / den;
+      res = (float)(0.0 + omega * (jv - 0.0));
+    }
+  }
+  return res;
+}
+
 template <typename TP, bool kNegR, bool kAux>
 struct RestrictOp {
   static constexpr bool kPrepare = false;
@@ -846,6 +867,12 @@ struct RestrictOp {
   unsigned char (*rsolid)[kMJ * kMK];
   float wres, free_vol;
   int ocount;
+  // with cpa: the coarse level's first pre-sweep from a zero iterate, which
+  // reads only its own row's rhs, is formed too (in finish, over the
+  // block's coarse cells once the march is done)
+  const LevelDev& C;
+  float* __restrict__ cpa;
+  double omega;
 
   template <class V>
   __device__ __forceinline__ void cell(int i, int j, int k, int64_t c, int t, int, bool, unsigned m, double e,
@@ -916,21 +943,40 @@ struct RestrictOp {
     accumulate(g, i);
     if (np == 2) accumulate(g, i + 1);
   }
-  __device__ __forceinline__ void finish(const MarchGeom&) {}
+  // The block's coarse cells (8 x 16 per coarse plane of its chunk, each
+  // written by exactly one owner of this block) get their zero-guess sweep,
+  // all threads sharing them: off the march's per-plane path.
+  __device__ __forceinline__ void finish(const MarchGeom& g) {
+    if (cpa == nullptr) return;
+    __syncthreads();  // the owners' crhs stores are visible to the block
+    constexpr int kCJ = kMJ / 2, kCK = kMK / 2;
+    const int ci0 = g.ib >> 1, nci = ((g.ie + 1) >> 1) - ci0;
+    const int cj0 = g.j0 >> 1, ck0 = g.k0 >> 1;
+    for (int e = flat_tid(); e < nci * kCJ * kCK; e += kMK * kTY) {
+      const int ci = ci0 + e / (kCJ * kCK), rem = e % (kCJ * kCK);
+      const int cj = cj0 + rem / kCK, ck = ck0 + rem % kCK;
+      if (ci < cnx && cj < cny && ck < cnz) {
+        const int64_t cc = cidx(ci, cj, ck, cny, cnz);
+        cpa[cc] = coarse_zero_sweep(C, ci, cj, ck, cc, crhs[cc], outlet, omega);
+      }
+    }
+  }
 };
 
 template <typename TP, bool kNegR, bool kAux>
 __global__ void __launch_bounds__(kMK* kTY, 3)
     km_restrict(LevelDev F, int chunk, const __grid_constant__ CUtensorMap map_p,
                 const __grid_constant__ CUtensorMap map_r, const __grid_constant__ CUtensorMap map_m, int outlet,
-                int cnx, int cny, int cnz, float* __restrict__ crhs, CgScalars* sc) {
+                int cnx, int cny, int cnz, float* __restrict__ crhs, CgScalars* sc, LevelDev C,
+                float* __restrict__ cpa, double omega) {
   pdl_wait();
   using TR = typename std::conditional<kNegR, double, TP>::type;
   __shared__ double rs[2][kMJ * kMK];
   __shared__ unsigned char rsolid[2][kMJ * kMK];
   MarchGeom g;
   const bool any = march_geom(F, chunk, g);
-  RestrictOp<TP, kNegR, kAux> op{F, outlet, cnx, cny, cnz, crhs, rs, rsolid, 0.0f, 0.0f, 0, {0.0f, 0.0f}, {0.0f, 0.0f}};
+  RestrictOp<TP, kNegR, kAux> op{F,   outlet, cnx, cny, cnz, crhs,        rs,          rsolid, 0.0f, 0.0f,
+                                 0,   C,      cpa, omega, {0.0f, 0.0f}, {0.0f, 0.0f}};
   op.load_widths(g);
   const CUtensorMap* const mv[1] = {&map_p};
   if (any && !march<TP, 1, TR, true>(F, g, mv, &map_r, &map_m, op)) report_fault(sc);
