@@ -519,13 +519,17 @@ __global__ void __launch_bounds__(256) kt_spmv_dir(LevelDev L, const double* __r
   }
 }
 
-// Tiled CG update (see k_cg_update).
-template <bool kDelta>
+// Tiled CG update (see k_cg_update).  kPart 0 updates x and r (and delta);
+// 1 only x, 2 only r (and delta): the two halves of one update, which the
+// PCG runs on two streams when no sums are wanted (x is needed by nothing
+// but the next update, so its half overlaps the preconditioner).
+template <bool kDelta, int kPart = 0>
 __global__ void __launch_bounds__(256) kt_cg_update(LevelDev L, double* __restrict__ x, const double* __restrict__ d,
                                                     double* __restrict__ r, const double* __restrict__ Ad,
                                                     double* __restrict__ delta, int want_means, int want_rr,
                                                     double* partials, CgScalars* sc) {
   pdl_wait();
+  constexpr bool kX = kPart != 2, kR = kPart != 1;
   const int nt = tiles_of(L.nx, L.ny, L.nz);
   const int64_t sx = (int64_t)L.ny * L.nz;
   const double alpha = sc->alpha;
@@ -542,10 +546,14 @@ __global__ void __launch_bounds__(256) kt_cg_update(LevelDev L, double* __restri
       if (q >= qn) break;
       const int64_t c = (int64_t)(i0 + q) * sx + base;
       msk[q] = __ldg(L.mask + c);
-      xv[q] = x[c];
-      dv[q] = __ldg(d + c);
-      rv[q] = r[c];
-      av[q] = __ldg(Ad + c);
+      if (kX) {
+        xv[q] = x[c];
+        dv[q] = __ldg(d + c);
+      }
+      if (kR) {
+        rv[q] = r[c];
+        av[q] = __ldg(Ad + c);
+      }
     }
 #pragma unroll
     for (int q = 0; q < kCI; ++q) {
@@ -553,9 +561,15 @@ __global__ void __launch_bounds__(256) kt_cg_update(LevelDev L, double* __restri
       const int i = i0 + q;
       const int64_t c = (int64_t)i * sx + base;
       if (msk[q] & M_SOLID) {
-        x[c] = 0.0;
-        r[c] = 0.0;
-        if (kDelta) delta[c] = 0.0;
+        if (kX) x[c] = 0.0;
+        if (kR) r[c] = 0.0;
+        if (kR && kDelta) delta[c] = 0.0;
+      } else if (kPart == 1) {
+        x[c] = xv[q] + alpha * dv[q];
+      } else if (kPart == 2) {
+        const double rn = rv[q] - alpha * av[q];
+        r[c] = rn;
+        if (kDelta) delta[c] = 1.0 * rn + -1.0 * rv[q];
       } else {
         const double xn = xv[q] + alpha * dv[q];
         const double rn = rv[q] - alpha * av[q];
@@ -1926,6 +1940,7 @@ static void preload_kernels() {
       (const void*)kt_sweep<float, false, true>,  (const void*)kt_sweep<float, false, false>,
       (const void*)kt_spmv_dir<true>,             (const void*)kt_spmv_dir<false>,
       (const void*)kt_cg_update<true>,            (const void*)kt_cg_update<false>,
+      (const void*)kt_cg_update<true, 1>,         (const void*)kt_cg_update<true, 2>,
       (const void*)kt_cg_dots<true, false>,       (const void*)kt_cg_dots<false, false>,
       (const void*)kt_sub_mean_xr,                (const void*)k_mg_tail,
 #define EFSI_MARCH_FNS(A)                                                                              \
@@ -2317,6 +2332,9 @@ int efsi_fv_plan_destroy(efsi_fv_plan* P) {
   P->graphs.clear();
   if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
   if (P->body_stream) cudaStreamDestroy(P->body_stream);
+  if (P->side_stream) cudaStreamDestroy(P->side_stream);
+  if (P->ev_fork) cudaEventDestroy(P->ev_fork);
+  if (P->ev_join) cudaEventDestroy(P->ev_join);
   for (LevelBuf& B : P->lv) {
     cudaFree(B.coef);
     cudaFree(B.mask);
@@ -3434,7 +3452,35 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
                               P->partials, P->sc);
     }
   };
-  auto launch_update = [&](double* d, bool mean_now, bool want_rr) {
+  // The halves of an update on two streams: r and delta (which the
+  // preconditioner reads) on `s`, x on the plan's side stream, joined back
+  // by join_update() before the next SpMV.  Only the tiled multigrid path of
+  // a host-loop solve splits, and only where the update forms no sums.
+  static const bool no_split = std::getenv("EFSI_NO_SPLIT_UPDATE") != nullptr;
+  const bool split_ok = !no_split && tiled0 && R.use_mg && !device;
+  if (split_ok && P->side_stream == nullptr) {
+    EFSI_CUDA_CHECK(cudaStreamCreateWithFlags(&P->side_stream, cudaStreamNonBlocking));
+    EFSI_CUDA_CHECK(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
+    EFSI_CUDA_CHECK(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
+  }
+  bool joined = true;
+  auto join_update = [&]() {
+    if (!joined) cudaStreamWaitEvent(s, P->ev_join, 0);
+    joined = true;
+  };
+  auto launch_update = [&](double* d, bool mean_now, bool want_rr, bool may_split = false) {
+    if (may_split && split_ok && !mean_now && !want_rr) {
+      cudaEventRecord(P->ev_fork, s);
+      cudaStreamWaitEvent(P->side_stream, P->ev_fork, 0);
+      EFSI_COUNTED kt_cg_update<true, 1><<<tg0, tblk, 0, P->side_stream>>>(R.L, pressure, d, P->r, P->Ad, P->delta, 0,
+                                                                          0, P->partials, P->sc);
+      cudaEventRecord(P->ev_join, P->side_stream);
+      joined = false;
+      EFSI_COUNTED launch_pdl(kt_cg_update<true, 2>, tg0, tblk, 0, s, R.L, pressure, d, P->r, P->Ad, P->delta, 0, 0,
+                              P->partials, P->sc);
+      return;
+    }
+    join_update();
     if (tiled0) {
       if (R.use_mg)
         EFSI_TIMED(KF_CG_UPDATE, 56.0 * n0d, s,
@@ -3502,12 +3548,15 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     if (cont) EFSI_TRY(launch_precond_dots());
     double* d[2] = {P->d0, P->d1};
     for (int j = 0; j < 16; ++j) {
+      join_update();  // the previous x half reads the direction this SpMV rewrites two iterations on
       launch_spmv(!cont && j == 0, d[j & 1], d[(j + 1) & 1]);
       const bool last = (j == 15);
-      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean && !R.anchor);
+      // (the last update of the block is whole: the check reads x)
+      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean && !R.anchor, !last);
       if (last && R.anchor) anchor_pressure_residual(true);
       if (!last) EFSI_TRY(launch_precond_dots());
     }
+    join_update();
     EFSI_LAUNCH_CHECK();
     return EFSI_OK;
   };

@@ -296,6 +296,8 @@ struct efsi_fv_plan {
   std::vector<PcgGraph> graphs;        // instantiated 16-iteration PCG blocks
   cudaStream_t cap_stream = nullptr;   // private stream used for graph capture
   cudaStream_t body_stream = nullptr;  // captures the body of the device-side PCG loop
+  cudaStream_t side_stream = nullptr;  // the x half of a split CG update
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int dl_used_mg = 0;                  // preconditioner kind of the last device-side loop
   bool graphs_disabled = false;        // a capture failed; blocks run as direct launches
   int tail_level = 1 << 30;            // first level run by the single-CTA V-cycle tail
