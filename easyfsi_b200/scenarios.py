@@ -428,6 +428,12 @@ class CoupledScene:
         self.last_cg_iterations = 0
         # "fv_multigrid" (the reference's) or "fv_multigrid_mixed" (FP32 level-0 V-cycle)
         self.preconditioner = "fv_multigrid"
+        # overlap_solid: the marker forces, scatter, MPM substep and feedback of
+        # a step run on a side stream beside the next step's fluid work
+        # (finish() joins them); off, the step runs in order on one stream
+        self.overlap_solid = False
+        self._side = None
+        self._solid_pending = False
 
     def step(self) -> None:
         cfg, fluid, solid, mk = self.cfg, self.fluid, self.solid, self.markers
@@ -437,6 +443,7 @@ class CoupledScene:
             cg_preconditioner=self.preconditioner, read_report=False,
         )
         self.last_cg_iterations = fluid.last_cg_iterations
+        self.finish()  # the previous step's solid part has moved the markers
         mk.sample_fluid_stress_to_marker_tractions(
             fluid.velocity, fluid.pressure, fluid.obstacle,
             fluid.cell_face_x_m, fluid.cell_face_y_m, fluid.cell_face_z_m,
@@ -444,6 +451,32 @@ class CoupledScene:
             fluid.cell_width_x_m, fluid.cell_width_y_m, fluid.cell_width_z_m,
             fluid.grid.grid_nodes, viscosity_pa_s=0.0, two_sided_pressure=False, read_report=False,
         )
+        if not self.overlap_solid:
+            self._solid_part()
+            return
+        # The rest of the step reads and writes only markers and particles, and
+        # the next step's predict and projection only the fluid: it runs on a
+        # side stream beside them and is joined before the next tractions.
+        import torch
+
+        if self._side is None:
+            self._side = torch.cuda.Stream()
+        self._side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(self._side):
+            self._solid_part()
+        self._solid_pending = True
+
+    def finish(self) -> None:
+        """Joins the solid part of the last step (``overlap_solid``) into the
+        current stream; the particle and marker state is final after it."""
+        if self._solid_pending:
+            import torch
+
+            torch.cuda.current_stream().wait_stream(self._side)
+            self._solid_pending = False
+
+    def _solid_part(self) -> None:
+        cfg, solid, mk = self.cfg, self.solid, self.markers
         mk.compute_marker_forces()
         mk.clear_mpm_external_forces(solid.external_force_n, particle_count=solid.particle_count, read_report=False)
         mk.scatter_marker_forces_to_mpm_particles(

@@ -1306,3 +1306,31 @@ def test_autotuned_plan_matches_the_default_launches():
     assert res[0][0] == res[1][0], (info, picks)
     assert res[0][3] == pytest.approx(res[1][3], rel=1e-6), (info, picks)
     assert rel_l2(res[0][1], res[1][1]) <= 1e-10
+
+
+def test_overlapped_solid_part_gives_the_in_order_steps():
+    """CoupledScene.overlap_solid runs each step's marker forces, scatter,
+    MPM substep and feedback on a side stream beside the next step's fluid
+    work; after finish() the state matches the same steps in order (the fluid
+    bit for bit, the particle sums to their f32 atomic order, 1e-6)."""
+    from easyfsi_b200.scenarios import CoupledScene, tiny_config
+
+    cfg = tiny_config(16)
+    u0 = CoupledScene(cfg).fluid.velocity.to_numpy()
+    a = CoupledScene(cfg, initial_velocity=u0, project_initial=False)
+    b = CoupledScene(cfg, initial_velocity=u0, project_initial=False)
+    b.overlap_solid = True
+    for _ in range(4):
+        a.step()
+        b.step()
+    b.finish()
+    torch.cuda.synchronize()
+    assert a.last_cg_iterations == b.last_cg_iterations
+    n = a.solid.particle_count
+    np.testing.assert_array_equal(b.fluid.pressure.to_numpy(), a.fluid.pressure.to_numpy())
+    for fa, fb in ((a.fluid.velocity, b.fluid.velocity), (a.solid.x, b.solid.x), (a.solid.v, b.solid.v),
+                   (a.markers.x_gamma_m, b.markers.x_gamma_m)):
+        xa, xb = fa.to_numpy(), fb.to_numpy()
+        if fa is a.solid.x or fa is a.solid.v:
+            xa, xb = xa[:n], xb[:n]
+        assert rel_l2(xb, xa) <= 1e-6
