@@ -902,6 +902,17 @@ def main() -> None:
             names = [k for k, v in psolve.items() if isinstance(v, dict) and "ms" in v]
             solve_ms = {k: round(psolve[k]["ms"], 4) for k in names}
             solve_iters = {k: psolve[k]["iterations"] for k in names}
+        # the whole MG-PCG iteration against HBM: 267 algorithmic bytes per
+        # cell (89 for the SpMV, update and direction, 178 for the V-cycle),
+        # over the c2 solve's time per iteration (its once-per-solve setup
+        # included)
+        pcg_iteration = None
+        if solve_ms and solve_iters and solve_iters.get("fv_multigrid"):
+            cells = scene.fluid.nx * scene.fluid.ny * scene.fluid.nz
+            us = 1000.0 * solve_ms["fv_multigrid"] / solve_iters["fv_multigrid"]
+            gbs = 267.0 * cells / (us * 1e-6) / 1e9
+            pcg_iteration = {"bytes_per_cell": 267, "cells": int(cells), "us": us, "achieved_gbs": gbs,
+                             "frac": gbs / peak, "timing": "fv_multigrid solve ms / iterations"}
         line = {
             "metric": METRIC,
             "value": value,
@@ -934,6 +945,7 @@ def main() -> None:
             "gpu_launches": int(launches),
             "clocks": clocks,
             "solve_ms": solve_ms,
+            "pcg_iteration_roofline": pcg_iteration,
             "solve_iterations": solve_iters,
             "cg_iterations_mean": float(np.mean(iters)) if iters else None,
             "mixed_precision": mixed,
