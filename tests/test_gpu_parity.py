@@ -167,7 +167,7 @@ def test_projection_gradient_and_predict(case):
 
 def test_mpm_step_matches_oracle():
     """20 MPM substeps of a block with random particle velocities against the
-    oracle.  x and F to <= 1e-6 relative (north_star's f32 bound is 1e-5);
+    oracle.  x and F to <= 1e-6 relative (the f32 bound after 20 steps is 1e-5);
     the parts that change -- the displacement x - x0 (about 1e-4 m) and F - I
     (about 2e-3) -- are stored as f32 x and F around 0.5 and I, whose
     representation floor is about 6e-8 and 1.2e-7 absolute per step, so
@@ -784,7 +784,7 @@ def test_bicgstab_matches_oracle(outlet, remove_mean):
     # reductions run in other orders on the device; BiCGSTAB's iterates are
     # sensitive to that (measured on a B200: 112 against the oracle's 130
     # iterations for the outlet case), so the counts agree only roughly and
-    # the solution is judged by its true residual and the pressure below
+    # the solution is checked by its true residual and the pressure below
     assert abs(fl.last_cg_iterations - ref["iterations"]) <= max(8, 0.25 * ref["iterations"])
     p = fl.pressure.to_numpy()
     res = rhs - ofl.fv_apply(p, outlet)
