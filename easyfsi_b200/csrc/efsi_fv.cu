@@ -2262,6 +2262,9 @@ int efsi_fv_plan_create(const efsi_level_desc* levels, int32_t n_levels, int32_t
       B.march_ok = B.march;
       B.mchunk = mc.chunk;
       B.mgrid = mc.grid;
+      const MarchCfg ms = march_cfg(B.nx, B.ny, B.nz, nsm * 2);
+      B.spchunk = ms.chunk;
+      B.spgrid = ms.grid;
     }
     size_t ncoef = 2 * (size_t)(B.nx + B.ny + B.nz);
     if (cudaMalloc(&B.coef, ncoef * sizeof(double)) != cudaSuccess || cudaMalloc(&B.mask, B.n) != cudaSuccess) {
@@ -2626,16 +2629,16 @@ static bool launch_march_spmv(efsi_fv_plan* P, const LevelDev& L, bool copy, con
   const bool aux = L.fw != nullptr || L.iface != nullptr;
   const int sm1 = march_smem<double, 1, double, false>(), sm2 = march_smem<double, 2, double, false>();
   if (copy && aux)
-    EFSI_COUNTED launch_pdl(km_spmv_dir<true, true>, B.mgrid, blk, sm1, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<true, true>, B.spgrid, blk, sm1, s, L, B.spchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                     partials, sc);
   else if (copy)
-    EFSI_COUNTED launch_pdl(km_spmv_dir<true, false>, B.mgrid, blk, sm1, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<true, false>, B.spgrid, blk, sm1, s, L, B.spchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                      partials, sc);
   else if (aux)
-    EFSI_COUNTED launch_pdl(km_spmv_dir<false, true>, B.mgrid, blk, sm2, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<false, true>, B.spgrid, blk, sm2, s, L, B.spchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                      partials, sc);
   else
-    EFSI_COUNTED launch_pdl(km_spmv_dir<false, false>, B.mgrid, blk, sm2, s, L, B.mchunk, *mz, *md, *mm, d_new, Ad, outlet,
+    EFSI_COUNTED launch_pdl(km_spmv_dir<false, false>, B.spgrid, blk, sm2, s, L, B.spchunk, *mz, *md, *mm, d_new, Ad, outlet,
                                                                       partials, sc);
   return true;
 }

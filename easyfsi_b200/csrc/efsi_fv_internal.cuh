@@ -222,6 +222,8 @@ struct LevelBuf {
   bool march_ok = false;  // they can (set at plan creation; the autotuner may switch them off)
   int mchunk = 2;      // their planes per block
   unsigned mgrid = 1;  // and grid size
+  int spchunk = 2;      // the direction SpMV's (two blocks per SM)
+  unsigned spgrid = 1;
 };
 
 }  // namespace efsi
