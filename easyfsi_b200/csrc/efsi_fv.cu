@@ -3457,10 +3457,10 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   };
   // The halves of an update on two streams: r and delta (which the
   // preconditioner reads) on `s`, x on the plan's side stream, joined back
-  // by join_update() before the next SpMV.  Only the tiled multigrid path of
-  // a host-loop solve splits, and only where the update forms no sums.
+  // by join_update() before the next SpMV.  Only the tiled multigrid path
+  // splits, and only where the update forms no sums.
   static const bool no_split = std::getenv("EFSI_NO_SPLIT_UPDATE") != nullptr;
-  const bool split_ok = !no_split && tiled0 && R.use_mg && !device;
+  const bool split_ok = !no_split && tiled0 && R.use_mg;
   if (split_ok && P->side_stream == nullptr) {
     EFSI_CUDA_CHECK(cudaStreamCreateWithFlags(&P->side_stream, cudaStreamNonBlocking));
     EFSI_CUDA_CHECK(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
@@ -3618,12 +3618,14 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
     double* d[2] = {P->d0, P->d1};
     int rc = EFSI_OK;
     for (int j = 0; j < 16 && rc == EFSI_OK; ++j) {
+      join_update();
       launch_spmv(false, d[j & 1], d[(j + 1) & 1]);
       const bool last = (j == 15);
-      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean && !R.anchor);
+      launch_update(d[(j + 1) & 1], last && remove_mean, last && !remove_mean && !R.anchor, !last);
       if (last && R.anchor) anchor_pressure_residual(true);
       rc = launch_precond_dots();
     }
+    join_update();
     s = keep;
     R.s = keep;
     return rc;
