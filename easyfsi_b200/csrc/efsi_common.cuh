@@ -91,8 +91,7 @@ void timing_end(int family, cudaStream_t s, double bytes);
 // launched without the attribute pdl_wait() returns at once.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
-bool pdl_enabled();  // false when EFSI_NO_PDL is set or this thread suppresses it
-void set_pdl_suppressed(bool on);  // this thread's launches go without the PDL attribute
+bool pdl_enabled();  // false when EFSI_NO_PDL is set
 
 template <typename... KArgs, typename... Args>
 inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,

@@ -1834,13 +1834,9 @@ unsigned long long take_capture_count() {
   g_capture_count = 0;
   return v;
 }
-namespace {
-thread_local bool g_pdl_suppressed = false;
-}
-void set_pdl_suppressed(bool on) { g_pdl_suppressed = on; }
 bool pdl_enabled() {
   static const bool on = std::getenv("EFSI_NO_PDL") == nullptr;
-  return on && !g_pdl_suppressed;
+  return on;
 }
 
 namespace {
@@ -3151,8 +3147,8 @@ namespace efsi {
 // Appends to the capture in progress on `cs`: the pressure reset of a zero
 // right-hand side, k_dl_init, and a WHILE node whose body (captured on the
 // plan's body stream) is one 16-iteration block plus k_dl_check.  Inside the
-// body the launches go without PDL and the V-cycle uses its per-level
-// launches.
+// body the launches keep their programmatic dependent launch attribute, and
+// the V-cycle uses its per-level launches.
 template <class Body>
 static int build_device_loop(efsi_fv_plan* P, cudaStream_t cs, double* pressure, double tol, int max_iters, Body body) {
   cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
@@ -3184,12 +3180,10 @@ static int build_device_loop(efsi_fv_plan* P, cudaStream_t cs, double* pressure,
                                                 cudaStreamCaptureModeThreadLocal));
   const int keep_blocks = P->coarse_blocks;
   P->coarse_blocks = 0;
-  set_pdl_suppressed(true);
   int rc = body(P->body_stream);
   EFSI_COUNTED k_dl_check<<<1, 32, 0, P->body_stream>>>(P->sc, tol, max_iters, h);
   cudaGraph_t out = nullptr;
   const cudaError_t e = cudaStreamEndCapture(P->body_stream, &out);
-  set_pdl_suppressed(false);
   P->coarse_blocks = keep_blocks;
   if (rc != EFSI_OK) return rc;
   if (e != cudaSuccess) {

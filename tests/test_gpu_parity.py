@@ -241,10 +241,15 @@ def test_c1_twenty_coupled_steps_match_oracle():
     state: the same CG iteration count every step; per field relative L2
     after every step: pressure <= 1e-10 (f64); fluid velocity, particle
     displacement and marker displacement <= 1e-6 (f32; measured bit-identical);
-    particle velocity, F - I and f_ext <= 1e-5 (f32 atomic sums in other
-    orders; measured <= 1e-6 after 20 steps).  The particles start at rest
-    and move less than one f32 unit of x in 20 steps at this dt, so their
-    velocity and F - I carry the solid's parity here."""
+    f_ext <= 1e-5 (measured 1.5e-7).  The particles start at rest and move
+    less than one f32 unit of x in 20 steps at this dt, so their velocity and
+    F carry the solid's parity here.  F is f32 around I while |F - I| is
+    about 4e-5, so one unit in the last place of F (1.2e-7) is about 3e-3 of
+    |F - I|: the oracle's own OpenMP atomic sums flip such units from run to
+    run (two oracle runs from the same state differ by one unit), and the
+    GPU-vs-oracle error of F - I is 9e-7 or 2.8e-3 depending on the oracle's
+    run (v: 5e-7 or 7e-5).  So F is held to four units in the last place
+    (|dF| <= 4.8e-7 everywhere), F - I to 1e-2 and v to 1e-4 relative."""
     from easyfsi_b200.scenarios import CONFIGS, CoupledScene
 
     cfg = CONFIGS["c1"]
@@ -269,15 +274,18 @@ def test_c1_twenty_coupled_steps_match_oracle():
             "v": rel_l2(gpu.solid.v.to_numpy()[:n], ref.solid.v[:n]),
             "F-I": rel_l2(gpu.solid.F.to_numpy()[:n].reshape(n, 9) - eye, ref.solid.F[:n].reshape(n, 9) - eye),
             "f_ext": rel_l2(gpu.solid.external_force_n.to_numpy()[:n], ref.solid.fext[:n]),
+            "F_abs": float(np.abs(gpu.solid.F.to_numpy()[:n].astype(np.float64) - ref.solid.F[:n]).max()),
         }
         for k, v in err.items():
             worst[k] = max(worst.get(k, 0.0), v)
-    print("c1 worst per-field relative L2 over 20 steps:", worst)
+    print("c1 worst per-field errors over 20 steps:", worst)
     assert worst["pressure"] <= 1e-10
     for k in ("velocity", "displacement", "marker_displacement"):
         assert worst[k] <= 1e-6, k
-    for k in ("v", "F-I", "f_ext"):
-        assert worst[k] <= 1e-5, k
+    assert worst["f_ext"] <= 1e-5
+    assert worst["F_abs"] <= 4.8e-7
+    assert worst["F-I"] <= 1e-2
+    assert worst["v"] <= 1e-4
     assert np.abs(ref.solid.v[:n]).max() > 0.0 and np.abs(ref.solid.F[:n].reshape(n, 9) - eye).max() > 0.0
 
 
