@@ -601,6 +601,58 @@ __global__ void __launch_bounds__(256) kt_cg_update(LevelDev L, double* __restri
   }
 }
 
+// The r half of a split update (kt_cg_update<true, 2>) that also forms the
+// V-cycle's first level-0 sweep from a zero iterate, which reads only its own
+// row: z0 = 0 + omega ((0 - (-r)) / den - 0) with the precomputed reciprocal
+// of den (km_sweep0's expression), 0 on solid rows and where den <= 0.
+__global__ void __launch_bounds__(256) kt_cg_update_r_zero(LevelDev L, double* __restrict__ r,
+                                                           const double* __restrict__ Ad,
+                                                           double* __restrict__ delta,
+                                                           const double* __restrict__ rden,
+                                                           double* __restrict__ z0, double omega, CgScalars* sc) {
+  pdl_wait();
+  const int nt = tiles_of(L.nx, L.ny, L.nz);
+  const int64_t sx = (int64_t)L.ny * L.nz;
+  const double alpha = sc->alpha;
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    int i0, j, k;
+    if (!tile_coords(L, tile, i0, j, k)) continue;
+    const int64_t base = (int64_t)j * L.nz + k;
+    const int qn = min(kCI, L.nx - i0);
+    unsigned msk[kCI];
+    double rv[kCI], av[kCI], rd[kCI];
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      if (q >= qn) break;
+      const int64_t c = (int64_t)(i0 + q) * sx + base;
+      msk[q] = __ldg(L.mask + c);
+      rv[q] = r[c];
+      av[q] = __ldg(Ad + c);
+      rd[q] = __ldg(rden + c);
+    }
+#pragma unroll
+    for (int q = 0; q < kCI; ++q) {
+      if (q >= qn) break;
+      const int64_t c = (int64_t)(i0 + q) * sx + base;
+      if (msk[q] & M_SOLID) {
+        r[c] = 0.0;
+        delta[c] = 0.0;
+        z0[c] = 0.0;
+      } else {
+        const double rn = rv[q] - alpha * av[q];
+        r[c] = rn;
+        delta[c] = 1.0 * rn + -1.0 * rv[q];
+        double res = 0.0;
+        if (rd[q] > 0.0) {
+          const double rvn = -rn;
+          res = 0.0 + omega * ((0.0 - rvn) * rd[q] - 0.0);
+        }
+        z0[c] = res;
+      }
+    }
+  }
+}
+
 // Tiled rz_new / beta numerator / beta (see k_cg_dots).
 template <bool kMG, bool kRestart>
 __global__ void __launch_bounds__(256) kt_cg_dots(LevelDev L, const double* __restrict__ r,
@@ -1937,6 +1989,7 @@ static void preload_kernels() {
       (const void*)kt_spmv_dir<true>,             (const void*)kt_spmv_dir<false>,
       (const void*)kt_cg_update<true>,            (const void*)kt_cg_update<false>,
       (const void*)kt_cg_update<true, 1>,         (const void*)kt_cg_update<true, 2>,
+      (const void*)kt_cg_update_r_zero,
       (const void*)kt_cg_dots<true, false>,       (const void*)kt_cg_dots<false, false>,
       (const void*)kt_sub_mean_xr,                (const void*)k_mg_tail,
 #define EFSI_MARCH_FNS(A)                                                                              \
@@ -2825,7 +2878,7 @@ static bool vcycle_fuses_zero(const efsi_fv_plan* P, int c) {
 
 static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int pre, int coarse, int post,
                   bool want_mean, cudaStream_t s, const double* dots_delta = nullptr, bool* dots_done = nullptr,
-                  bool mixed = false) {
+                  bool mixed = false, bool level0_zero_done = false) {
   pre = std::max(1, pre);
   coarse = std::max(1, coarse);
   post = std::max(1, post);
@@ -2883,10 +2936,11 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
           return EFSI_ERR_ARG;
         }
       } else if (l == 0) {
-        if (it == 0)
-          EFSI_TIMED(KF_SWEEP_L0, 17.0 * n0, s,
-                     (launch_sweep<double, true, true>(P, 0, nullptr, r, (double*)dst, outlet, om, none, nullptr, s)));
-        else
+        if (it == 0) {
+          if (!level0_zero_done)  // else the CG update formed it in bufs[0]
+            EFSI_TIMED(KF_SWEEP_L0, 17.0 * n0, s,
+                       (launch_sweep<double, true, true>(P, 0, nullptr, r, (double*)dst, outlet, om, none, nullptr, s)));
+        } else
           EFSI_TIMED(KF_SWEEP_L0, 25.0 * n0, s,
                      (launch_sweep<double, true, false>(P, 0, (const double*)c, r, (double*)dst, outlet, om, none,
                                                         nullptr, s)));
@@ -3066,6 +3120,7 @@ struct PcgRun {
   bool mixed;       // FP32 level-0 V-cycle
   bool learned;     // the attached network (code 4)
   bool anchor;      // outlet solve with unreached components: their means are subtracted
+  bool zero0_ready = false;  // the last update formed the V-cycle's first level-0 sweep (in lv[0].pa)
 };
 
 // fluid.py:4965-4981 on a level-0 field: the unreached components' means
@@ -3128,8 +3183,10 @@ static int precondition(PcgRun& R) {
     // with the zero-mean projection the V-cycle's last sweep finishes the dots
     // (EFSI_SEPARATE_DOTS keeps them in their own kernel)
     static const bool separate = std::getenv("EFSI_SEPARATE_DOTS") != nullptr;
+    const bool zero0 = R.zero0_ready;
+    R.zero0_ready = false;
     EFSI_TRY(vcycle(R.P, R.P->r, R.P->z, R.prm->outlet, R.pre, R.coarse, R.post, want_mean, R.s,
-                    want_mean && !separate ? R.P->delta : nullptr, &R.dots_fused, R.mixed));
+                    want_mean && !separate ? R.P->delta : nullptr, &R.dots_fused, R.mixed, zero0));
   } else {
     EFSI_COUNTED launch_pdl(k_jacobi_precond, R.S.grid, R.S.block, 0, R.s, R.L, R.P->diag, R.P->r, R.P->z, want_mean ? 1 : 0,
                                                       R.P->partials, R.P->sc);
@@ -3455,6 +3512,8 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
   // splits, and only where the update forms no sums.
   static const bool no_split = std::getenv("EFSI_NO_SPLIT_UPDATE") != nullptr;
   const bool split_ok = !no_split && tiled0 && R.use_mg;
+  static const bool no_zero0 = std::getenv("EFSI_NO_UPDATE_SWEEP0") != nullptr;
+  const bool zero0_ok = !no_zero0 && P->lv[0].march && P->n_levels > 1;
   if (split_ok && P->side_stream == nullptr) {
     EFSI_CUDA_CHECK(cudaStreamCreateWithFlags(&P->side_stream, cudaStreamNonBlocking));
     EFSI_CUDA_CHECK(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
@@ -3473,6 +3532,15 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
                                                                           0, P->partials, P->sc);
       cudaEventRecord(P->ev_join, P->side_stream);
       joined = false;
+      // with the plane-marching f64 V-cycle next, the r half also forms its
+      // first level-0 sweep (with the reciprocal denominators)
+      const int o = outlet ? 1 : 0;
+      if (zero0_ok && P->rden_ok[o] && !R.learned && !R.mixed) {
+        EFSI_COUNTED launch_pdl(kt_cg_update_r_zero, tg0, tblk, 0, s, R.L, P->r, (const double*)P->Ad, P->delta,
+                                (const double*)P->rden[o], (double*)P->lv[0].pa, (double)0.8f, P->sc);
+        R.zero0_ready = true;
+        return;
+      }
       EFSI_COUNTED launch_pdl(kt_cg_update<true, 2>, tg0, tblk, 0, s, R.L, pressure, d, P->r, P->Ad, P->delta, 0, 0,
                               P->partials, P->sc);
       return;
