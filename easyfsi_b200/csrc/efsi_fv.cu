@@ -603,13 +603,17 @@ __global__ void __launch_bounds__(256) kt_cg_update(LevelDev L, double* __restri
 
 // The r half of a split update (kt_cg_update<true, 2>) that also forms the
 // V-cycle's first level-0 sweep from a zero iterate, which reads only its own
-// row: z0 = 0 + omega ((0 - (-r)) / den - 0) with the precomputed reciprocal
-// of den (km_sweep0's expression), 0 on solid rows and where den <= 0.
+// row: z0 = 0 + omega ((0 - (-r)) / den - 0), 0 on solid rows and where
+// den <= 0, as km_sweep0 forms it: f64 z0 with the precomputed reciprocal of
+// den; f32 z0 (the FP32 V-cycle, which runs without an interface diagonal)
+// dividing by den formed from the row's open faces.
+template <typename TZ>
 __global__ void __launch_bounds__(256) kt_cg_update_r_zero(LevelDev L, double* __restrict__ r,
                                                            const double* __restrict__ Ad,
                                                            double* __restrict__ delta,
                                                            const double* __restrict__ rden,
-                                                           double* __restrict__ z0, double omega, CgScalars* sc) {
+                                                           TZ* __restrict__ z0, double omega, int outlet,
+                                                           CgScalars* sc) {
   pdl_wait();
   const int nt = tiles_of(L.nx, L.ny, L.nz);
   const int64_t sx = (int64_t)L.ny * L.nz;
@@ -628,24 +632,34 @@ __global__ void __launch_bounds__(256) kt_cg_update_r_zero(LevelDev L, double* _
       msk[q] = __ldg(L.mask + c);
       rv[q] = r[c];
       av[q] = __ldg(Ad + c);
-      rd[q] = __ldg(rden + c);
+      if (sizeof(TZ) == 8) rd[q] = __ldg(rden + c);
     }
+    const RowCoef rc = row_coef(L, j, k);
 #pragma unroll
     for (int q = 0; q < kCI; ++q) {
       if (q >= qn) break;
-      const int64_t c = (int64_t)(i0 + q) * sx + base;
+      const int i = i0 + q;
+      const int64_t c = (int64_t)i * sx + base;
       if (msk[q] & M_SOLID) {
         r[c] = 0.0;
         delta[c] = 0.0;
-        z0[c] = 0.0;
+        z0[c] = (TZ)0;
       } else {
         const double rn = rv[q] - alpha * av[q];
         r[c] = rn;
         delta[c] = 1.0 * rn + -1.0 * rv[q];
-        double res = 0.0;
-        if (rd[q] > 0.0) {
-          const double rvn = -rn;
-          res = 0.0 + omega * ((0.0 - rvn) * rd[q] - 0.0);
+        const double rvn = -rn;
+        TZ res = (TZ)0;
+        if (sizeof(TZ) == 8) {
+          if (rd[q] > 0.0) res = (TZ)(0.0 + omega * ((0.0 - rvn) * rd[q] - 0.0));
+        } else {
+          double ns, den;
+          stencil_sel<true>(L, rc, __ldg(L.cxm + i), __ldg(L.cxp + i), i, j, k, c, msk[q], outlet, 0.0, 0.0, 0.0, 0.0,
+                            0.0, 0.0, ns, den);
+          if (den > 0.0) {
+            const double jv = (ns - rvn) / den;
+            res = (TZ)(0.0 + omega * (jv - 0.0));
+          }
         }
         z0[c] = res;
       }
@@ -1989,7 +2003,7 @@ static void preload_kernels() {
       (const void*)kt_spmv_dir<true>,             (const void*)kt_spmv_dir<false>,
       (const void*)kt_cg_update<true>,            (const void*)kt_cg_update<false>,
       (const void*)kt_cg_update<true, 1>,         (const void*)kt_cg_update<true, 2>,
-      (const void*)kt_cg_update_r_zero,
+      (const void*)kt_cg_update_r_zero<double>,   (const void*)kt_cg_update_r_zero<float>,
       (const void*)kt_cg_dots<true, false>,       (const void*)kt_cg_dots<false, false>,
       (const void*)kt_sub_mean_xr,                (const void*)k_mg_tail,
 #define EFSI_MARCH_FNS(A)                                                                              \
@@ -2929,9 +2943,10 @@ static int vcycle(efsi_fv_plan* P, const double* r, double* z, int outlet, int p
     for (int it = 0; it < pre; ++it) {
       void* dst = bufs[it & 1];
       if (l == 0 && mixed) {
-        if (it == 0)
-          launch_sweep<float, true, true>(P, 0, nullptr, r, (float*)dst, outlet, om, none, nullptr, s);
-        else if (!launch_sweep32(P, (const float*)c, r, (float*)dst, nullptr, outlet, om, none, nullptr, nullptr, s)) {
+        if (it == 0) {
+          if (!level0_zero_done)  // else the CG update formed it in bufs[0]
+            launch_sweep<float, true, true>(P, 0, nullptr, r, (float*)dst, outlet, om, none, nullptr, s);
+        } else if (!launch_sweep32(P, (const float*)c, r, (float*)dst, nullptr, outlet, om, none, nullptr, nullptr, s)) {
           set_error("the mixed-precision V-cycle needs the plane-marching kernels on level 0");
           return EFSI_ERR_ARG;
         }
@@ -3535,9 +3550,16 @@ int efsi_fv_pcg_solve(efsi_fv_plan* P, const double* rhs0, double* pressure, con
       // with the plane-marching f64 V-cycle next, the r half also forms its
       // first level-0 sweep (with the reciprocal denominators)
       const int o = outlet ? 1 : 0;
+      if (zero0_ok && !R.learned && R.mixed) {
+        EFSI_COUNTED launch_pdl(kt_cg_update_r_zero<float>, tg0, tblk, 0, s, R.L, P->r, (const double*)P->Ad, P->delta,
+                                (const double*)nullptr, (float*)P->lv[0].pa32, (double)0.8f, outlet, P->sc);
+        R.zero0_ready = true;
+        return;
+      }
       if (zero0_ok && P->rden_ok[o] && !R.learned && !R.mixed) {
-        EFSI_COUNTED launch_pdl(kt_cg_update_r_zero, tg0, tblk, 0, s, R.L, P->r, (const double*)P->Ad, P->delta,
-                                (const double*)P->rden[o], (double*)P->lv[0].pa, (double)0.8f, P->sc);
+        EFSI_COUNTED launch_pdl(kt_cg_update_r_zero<double>, tg0, tblk, 0, s, R.L, P->r, (const double*)P->Ad,
+                                P->delta, (const double*)P->rden[o], (double*)P->lv[0].pa, (double)0.8f, outlet,
+                                P->sc);
         R.zero0_ready = true;
         return;
       }
