@@ -155,6 +155,51 @@ def ib_node_search_stats(scene, reps: int) -> dict:
     }
 
 
+def shell_step_stats(steps: int = 50, warmup: int = 3) -> dict:
+    """The triangle Mooney membrane step (TriMooneyShellMpmState.step) on the
+    c4 membrane: the 0.4 m x 0.3 m plate of 20,000 triangles (10,201
+    vertices), t = 2 mm, C10 = 1e5 Pa, clamped root, its own 36^3 node grid,
+    50 Pa pressure and gravity.  CUDA events around `steps` steps without the
+    report read (the reference's read_report=False path); one more step reads
+    the report."""
+    import torch
+
+    from easyfsi_b200 import _native
+    from easyfsi_b200.geometry import make_plate_mesh
+    from easyfsi_b200.mooney_shell_mpm import TriMooneyShellMpmState
+
+    mesh, region = make_plate_mesh(100, 100)
+    st = TriMooneyShellMpmState(mesh, thickness_m=2.0e-3, density_kgm3=1000.0, c1_pa=1.0e5, c2_pa=0.0,
+                                face_region_id=region, primary_region_id=1, secondary_region_id=2,
+                                fixed_region_id=3)
+    kw = dict(dt_s=5.0e-5, pressure_pa=50.0, body_acceleration_mps2=(0.0, 0.0, -9.81), read_report=False)
+    for _ in range(warmup):
+        st.step(**kw)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    n0 = _native.kernel_launches()
+    e0.record(stream)
+    for _ in range(steps):
+        st.step(**kw)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    launches = (_native.kernel_launches() - n0) / steps
+    rep = st.step(**dict(kw, read_report=True))
+    return {
+        "workload": "c4_membrane_plate_20000_triangles",
+        "faces": st.face_count,
+        "vertices": st.particle_count,
+        "grid_nodes": list(st.grid_nodes),
+        "ms_per_step": ms,
+        "steps_per_s": 1e3 / ms,
+        "launches_per_step": launches,
+        "mean_radial_stretch": rep.mean_radial_stretch,
+        "transfer_relative_error": rep.transfer_relative_error,
+    }
+
+
 def pressure_solve_stats(scene, reps: int, jacobi_max_iterations: int = 20000) -> dict:
     """One c2 pressure solve to the scene's relative-residual tolerance (the
     Poisson system of a predicted, not yet projected velocity), timed with
@@ -641,6 +686,7 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the fv_multigrid_mixed measurement")
     ap.add_argument("--no-ib-search", action="store_true", help="skip the IB node search measurement")
+    ap.add_argument("--no-shell", action="store_true", help="skip the Mooney membrane step measurement")
     ap.add_argument("--no-pressure-solve", action="store_true", help="skip the per-preconditioner solve timing")
     ap.add_argument("--cpu-steps", type=int, default=3, help="timed CPU-oracle steps of the GPU arm's cpu_baseline")
     ap.add_argument("--cpu-warmup", type=int, default=1)
@@ -792,6 +838,14 @@ def main() -> None:
             ib_search = ib_node_search_stats(scene, reps=5)
         except Exception as exc:  # reported, never fatal to the step's line
             ib_search = {"error": f"{type(exc).__name__}: {exc}"}
+
+    # --- the Mooney membrane step on the c4 plate (its own solid; not part of the step) ---
+    shell = None
+    if not args.no_shell:
+        try:
+            shell = shell_step_stats()
+        except Exception as exc:  # reported, never fatal to the step's line
+            shell = {"error": f"{type(exc).__name__}: {exc}"}
 
     # --- one pressure solve per preconditioner (not part of the step) ---
     psolve = None
@@ -960,6 +1014,7 @@ def main() -> None:
             "preconditioner": vcycle_stats,
             "pressure_solve": psolve,
             "ib_node_search": ib_search,
+            "shell_step": shell,
             "cg_iterations": iters,
         }
         print(json.dumps(line), flush=True)

@@ -154,6 +154,34 @@ class MpmState(Structure):
     ]
 
 
+class ShellState(Structure):  # efsi_shell_state
+    _fields_ = [
+        ("particle_count", c_int32), ("face_count", c_int32), ("edge_count", c_int32),
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
+        ("bmin", c_float * 3), ("dx", c_float * 3),
+        ("x", c_void_p), ("u", c_void_p), ("v", c_void_p), ("rest_x", c_void_p), ("mass", c_void_p),
+        ("area", c_void_p), ("normal", c_void_p), ("internal_force", c_void_p), ("external_force", c_void_p),
+        ("vertex_region", c_void_p), ("fixed", c_void_p), ("faces", c_void_p), ("face_region", c_void_p),
+        ("edges", c_void_p), ("grid_mass", c_void_p), ("grid_velocity", c_void_p),
+        ("grid_velocity_before", c_void_p), ("grid_force", c_void_p),
+    ]
+
+
+class ShellParams(Structure):  # efsi_shell_params
+    _fields_ = [
+        ("dt", c_float), ("pressure", c_float), ("velocity_damping", c_float), ("flip_blend", c_float),
+        ("body_acceleration", c_float * 3),
+        ("c1", c_float), ("c2", c_float), ("membrane_force_scale", c_float),
+        ("thickness", c_float), ("primary_thickness", c_float), ("secondary_thickness", c_float),
+        ("region_loads", c_int32), ("preserve_external_force", c_int32),
+        ("primary_region", c_int32), ("secondary_region", c_int32), ("area_load_region", c_int32),
+        ("primary_area_load", c_float * 3), ("primary_reaction", c_float * 3), ("secondary_reaction", c_float * 3),
+        ("primary_area", c_float), ("secondary_area", c_float),
+    ]
+
+
+SHELL_SCRATCH_DOUBLES = 48
+
 P = c_void_p
 I = c_int32
 F = c_float
@@ -199,6 +227,10 @@ _PROTOTYPES: dict[str, list] = {
     "efsi_mpm_plan_create": [I, I, I, I, POINTER(c_void_p)],
     "efsi_mpm_plan_destroy": [P],
     "efsi_mpm_step": [P, POINTER(MpmState), F, F, F, F, I, I, P, P],
+    "efsi_shell_init": [POINTER(ShellState), P, P, P, F, F, F, F, I, I, I, P, P],
+    "efsi_shell_update_normals": [POINTER(ShellState), P],
+    "efsi_shell_add_region_area_load": [POINTER(ShellState), I, POINTER(c_float), P],
+    "efsi_shell_step": [POINTER(ShellState), POINTER(ShellParams), P, P, P],
     "efsi_sample_pressure_tractions": [I, I, I, POINTER(GridAxes), P, P, P, P, P, I, P, P, P, I, I, F, P, P, P, P],
     "efsi_compute_marker_forces": [I, P, P, P, P],
     "efsi_clear_external_forces": [I, P, P, P],

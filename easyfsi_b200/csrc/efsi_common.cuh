@@ -70,7 +70,8 @@ enum KernelFamily : int {
   KF_SCATTER = 9,
   KF_FEEDBACK = 10,
   KF_MPM_STEP = 11,  // the whole substep: clears, binning, P2G, grid update, G2P
-  KF_COUNT = 12
+  KF_SHELL_STEP = 12,  // the whole Mooney membrane step
+  KF_COUNT = 13
 };
 bool timing_enabled(int family);
 void timing_begin(int family, cudaStream_t s);

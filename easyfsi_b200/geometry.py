@@ -20,6 +20,10 @@ class SurfaceMesh:
     faces: np.ndarray
 
     @property
+    def vertex_count(self) -> int:
+        return int(np.asarray(self.vertices).shape[0])
+
+    @property
     def face_count(self) -> int:
         return int(self.faces.shape[0])
 
@@ -56,3 +60,23 @@ def make_uv_sphere(resolution: UvSphereResolution, radius_m: float) -> SurfaceMe
     flip = np.einsum("ij,ij->i", normals, (a + b + c) / 3.0 - centroid) < 0.0
     f[flip] = f[flip][:, [0, 2, 1]]
     return SurfaceMesh(v, f)
+
+
+def make_plate_mesh(nu: int, nv: int, size_m: tuple[float, float] = (0.4, 0.3), seed: int = 4001):
+    """Flat rectangular membrane of 2 nu nv triangles in the xy plane with a
+    seeded 1 mm out-of-plane jitter, and its face regions: 1 for the half at
+    x > size/2, 2 for the other half, 3 for the first column of quads (the
+    root, to be clamped).  The c4 membrane is the 0.4 m x 0.3 m plate with
+    nu = nv = 100 (20,000 triangles)."""
+    xs = np.linspace(0.0, size_m[0], nu + 1)
+    ys = np.linspace(0.0, size_m[1], nv + 1)
+    gx, gy = np.meshgrid(xs, ys, indexing="ij")
+    gz = 1.0e-3 * np.random.default_rng(seed).standard_normal(gx.shape)
+    verts = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
+    idx = np.arange((nu + 1) * (nv + 1)).reshape(nu + 1, nv + 1)
+    a, b, c, d = idx[:-1, :-1].ravel(), idx[1:, :-1].ravel(), idx[1:, 1:].ravel(), idx[:-1, 1:].ravel()
+    faces = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)]).astype(np.int32)
+    cx = verts[faces, 0].mean(axis=1)
+    region = np.where(cx > 0.5 * size_m[0], 1, 2).astype(np.int32)
+    region[cx < size_m[0] / nu] = 3
+    return SurfaceMesh(vertices=verts, faces=faces), region

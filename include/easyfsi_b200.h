@@ -379,6 +379,85 @@ int efsi_mpm_step(efsi_mpm_plan* plan, const efsi_mpm_state* state, float dt, fl
                   double* report_device, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Triangle Mooney-Rivlin membrane MPM                                       */
+/* ------------------------------------------------------------------------ */
+
+/* Doubles of caller-provided scratch that efsi_shell_step accumulates its
+ * report sums in (cleared by the step itself). */
+#define EFSI_SHELL_SCRATCH_DOUBLES 48
+
+/* Device buffers of one membrane (float3 arrays are [n][3]; the node grid is
+ * x-major [nx][ny][nz]).  Mirrors the fields of TriMooneyShellMpmState
+ * (mooney_shell_mpm.py:179-222). */
+typedef struct efsi_shell_state {
+  int32_t particle_count, face_count, edge_count;
+  int32_t nx, ny, nz;
+  float bmin[3];
+  float dx[3];
+  float* x;
+  float* u;
+  float* v;
+  const float* rest_x;
+  const float* mass;
+  float* area;
+  float* normal;
+  float* internal_force;
+  float* external_force;
+  const int32_t* vertex_region;
+  const int32_t* fixed;
+  const int32_t* faces;       /* [face_count][3] */
+  const int32_t* face_region; /* [face_count] */
+  const int32_t* edges;       /* [edge_count][2], unique undirected */
+  float* grid_mass;
+  float* grid_velocity;
+  float* grid_velocity_before;
+  float* grid_force;
+} efsi_shell_state;
+
+/* Arguments of one step.  region_loads = 0 is step() (uniform pressure on
+ * every face, mooney_shell_mpm.py:860-1003, 1179-1202); region_loads = 1 is
+ * advance_region_loads() / advance_with_external_forces() (:1005-1292), with
+ * the region thicknesses, the area load on area_load_region and the two
+ * interface reactions spread by rest area over primary_area / secondary_area. */
+typedef struct efsi_shell_params {
+  float dt, pressure, velocity_damping, flip_blend;
+  float body_acceleration[3];
+  float c1, c2, membrane_force_scale;
+  float thickness, primary_thickness, secondary_thickness;
+  int32_t region_loads;
+  int32_t preserve_external_force;
+  int32_t primary_region, secondary_region, area_load_region;
+  float primary_area_load[3];
+  float primary_reaction[3];
+  float secondary_reaction[3];
+  float primary_area, secondary_area;
+} efsi_shell_params;
+
+/* mooney_shell_mpm.py:480-540 _init_mass_kernel: zero the particle state,
+ * rest-area mass and area shares, vertex regions (minimum of the faces'),
+ * fixed vertices; region_totals (float[4] or NULL) = primary area, primary
+ * mass, secondary area, secondary mass; then the current-shape normals. */
+int efsi_shell_init(const efsi_shell_state* state, float* mass, int32_t* vertex_region, int32_t* fixed,
+                    float density, float thickness, float primary_thickness, float secondary_thickness,
+                    int32_t primary_region, int32_t secondary_region, int32_t fixed_region, float* region_totals,
+                    void* stream);
+
+/* mooney_shell_mpm.py:449-461 _update_particle_surface_normals (used after
+ * restore_state, :1301-1309). */
+int efsi_shell_update_normals(const efsi_shell_state* state, void* stream);
+
+/* mooney_shell_mpm.py:710-728 _add_region_area_load_kernel. */
+int efsi_shell_add_region_area_load(const efsi_shell_state* state, int32_t region_id, const float* area_load_npm2,
+                                    void* stream);
+
+/* mooney_shell_mpm.py:860-1003 _step_kernel and :1005-1177
+ * _step_region_kernel.  scratch: EFSI_SHELL_SCRATCH_DOUBLES doubles of device
+ * memory; report_device: double[37] in the layout of report_host_snapshot
+ * (:337-391), or NULL. */
+int efsi_shell_step(const efsi_shell_state* state, const efsi_shell_params* params, double* scratch,
+                    double* report_device, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* HIBM surface markers                                                      */
 /* ------------------------------------------------------------------------ */
 
