@@ -6,7 +6,7 @@
 // One Taichi kernel becomes eight launches on one stream, each a flat pass
 // over the faces, the particles or the node grid:
 //   clear      grid arrays, per-particle forces, the step's accumulators
-//   faces      Mooney face law (f32, as the reference) + pressure or region
+//   faces      Mooney face law (f64; the reference's is f32) + pressure or region
 //              loads, scattered to the three vertices with f32 atomics; the
 //              edge-strain maximum in the same launch
 //   p2g        body force, out-of-bounds test, trilinear 8-node scatter
@@ -69,7 +69,6 @@ __device__ __forceinline__ bool safe3(float3 v) { return finite_small(v.x) && fi
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
-__device__ __forceinline__ float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
 __device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
 __device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
@@ -160,13 +159,26 @@ __device__ __forceinline__ float face_thickness(const efsi_shell_params& p, int 
   return p.thickness;
 }
 
-// :552-560 _limit_vector_norm
-__device__ __forceinline__ float3 limit_norm(float3 v, float cap) {
-  const float n = norm3(v);
-  if (n != n || n > 1.0e30f) return f3(0.f, 0.f, 0.f);
-  if (cap > 0.0f && n > cap) return v * (cap / n);
-  return v;
+__device__ __forceinline__ double3 d3(double x, double y, double z) { return make_double3(x, y, z); }
+__device__ __forceinline__ double3 operator+(double3 a, double3 b) { return d3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ double3 operator-(double3 a, double3 b) { return d3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double3 operator-(double3 a) { return d3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ double3 operator*(double3 a, double s) { return d3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ double dot3(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double3 cross3(double3 a, double3 b) {
+  return d3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
+__device__ __forceinline__ double norm3(double3 a) { return sqrt(dot3(a, a)); }
+__device__ __forceinline__ double3 ld3d(const float* p, int i) { return d3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+// :552-560 _limit_vector_norm, in f64, rounded to f32 for the atomics
+__device__ __forceinline__ float3 limit_norm(double3 v, double cap) {
+  const double n = norm3(v);
+  if (n != n || n > 1.0e30) return make_float3(0.f, 0.f, 0.f);
+  const double k = (cap > 0.0 && n > cap) ? cap / n : 1.0;
+  return make_float3((float)(v.x * k), (float)(v.y * k), (float)(v.z * k));
+}
+
 
 // ---------------------------------------------------------------------------
 // clear: grid (4 arrays, 10 floats per node), per-particle forces, scratch
@@ -209,50 +221,55 @@ __global__ void __launch_bounds__(kThreads) k_shell_faces(efsi_shell_state s, ef
   const int ia = s.faces[3 * i], ib = s.faces[3 * i + 1], ic = s.faces[3 * i + 2];
   const int region = s.face_region[i];
   const float thickness = face_thickness(p, region);
-  const float3 ra = ld3(s.rest_x, ia), rb = ld3(s.rest_x, ib), rc = ld3(s.rest_x, ic);
-  const float3 a = ld3(s.x, ia), b = ld3(s.x, ib), c = ld3(s.x, ic);
-  const float3 rav = cross3(rb - ra, rc - ra);
-  const float3 av = cross3(b - a, c - a);
-  const float ravn = norm3(rav);
-  const float rarea = 0.5f * ravn;
-  const float avn = norm3(av);
-  const float area = 0.5f * avn;
-  if (rarea > 1.0e-12f && ravn > 1.0e-12f) {
-    const float3 rn = rav * (1.0f / ravn);
-    const float3 e0 = rb - ra;
-    const float e0l = norm3(e0);
-    if (e0l > 1.0e-12f) {
-      const float3 t0 = e0 * (1.0f / e0l);
-      const float3 t1 = cross3(rn, t0);
-      const float3 rac = rc - ra;
-      const float xc = dot3(rac, t0), yc = dot3(rac, t1);
-      if (fabsf(yc) > 1.0e-12f) {
+  // The face law runs in f64: near rest its stress terms are differences of
+  // O(1) values (1 - i00 idet) for strains of 1e-6 and below, which f32 (the
+  // reference's precision) resolves to about two digits.  Storage and the
+  // vertex atomics stay f32.
+  const double3 ra = ld3d(s.rest_x, ia), rb = ld3d(s.rest_x, ib), rc = ld3d(s.rest_x, ic);
+  const double3 a = ld3d(s.x, ia), b = ld3d(s.x, ib), c = ld3d(s.x, ic);
+  const double3 rav = cross3(rb - ra, rc - ra);
+  const double3 av = cross3(b - a, c - a);
+  const double ravn = norm3(rav);
+  const double rarea = 0.5 * ravn;
+  const double avn = norm3(av);
+  const double area = 0.5 * avn;
+  if (rarea > 1.0e-12 && ravn > 1.0e-12) {
+    const double3 rn = rav * (1.0 / ravn);
+    const double3 e0 = rb - ra;
+    const double e0l = norm3(e0);
+    if (e0l > 1.0e-12) {
+      const double3 t0 = e0 * (1.0 / e0l);
+      const double3 t1 = cross3(rn, t0);
+      const double3 rac = rc - ra;
+      const double xc = dot3(rac, t0), yc = dot3(rac, t1);
+      if (fabs(yc) > 1.0e-12) {
         // inverse of the rest edge matrix in the triangle's own frame
-        const float inv00 = 1.0f / e0l;
-        const float inv01 = -xc / (e0l * yc);
-        const float inv11 = 1.0f / yc;
-        const float3 g0 = b - a, g1 = c - a;
-        const float3 F0 = g0 * inv00;
-        const float3 F1 = g0 * inv01 + g1 * inv11;
-        const float cap_c = 1.0e6f;
-        const float c00 = fminf(dot3(F0, F0), cap_c);
-        const float c01 = fminf(fmaxf(dot3(F0, F1), -cap_c), cap_c);
-        const float c11 = fminf(dot3(F1, F1), cap_c);
-        const float det = fmaxf(c00 * c11 - c01 * c01, 1.0e-6f);
-        const float idet = 1.0f / det;
-        const float i00 = c11 * idet, i01 = -c01 * idet, i11 = c00 * idet;
-        const float tr = c00 + c11;
+        const double inv00 = 1.0 / e0l;
+        const double inv01 = -xc / (e0l * yc);
+        const double inv11 = 1.0 / yc;
+        const double3 g0 = b - a, g1 = c - a;
+        const double3 F0 = g0 * inv00;
+        const double3 F1 = g0 * inv01 + g1 * inv11;
+        const double cap_c = 1.0e6;
+        const double c00 = fmin(dot3(F0, F0), cap_c);
+        const double c01 = fmin(fmax(dot3(F0, F1), -cap_c), cap_c);
+        const double c11 = fmin(dot3(F1, F1), cap_c);
+        const double det = fmax(c00 * c11 - c01 * c01, 1.0e-6);
+        const double idet = 1.0 / det;
+        const double i00 = c11 * idet, i01 = -c01 * idet, i11 = c00 * idet;
+        const double tr = c00 + c11;
+        const double c1 = p.c1, c2 = p.c2;
         // second Piola-Kirchhoff stress of the incompressible Mooney membrane
-        const float s00 = p.c1 * (1.0f - i00 * idet) + p.c2 * (det * i00 + idet - tr * idet * i00);
-        const float s01 = p.c1 * (-i01 * idet) + p.c2 * (det * i01 - tr * idet * i01);
-        const float s11 = p.c1 * (1.0f - i11 * idet) + p.c2 * (det * i11 + idet - tr * idet * i11);
-        const float k2 = p.membrane_force_scale * 2.0f;
-        const float3 P0 = (F0 * s00 + F1 * s01) * k2;
-        const float3 P1 = (F0 * s01 + F1 * s11) * k2;
-        const float vol = thickness * rarea;
-        const float3 ge0 = (P0 * inv00 + P1 * inv01) * vol;
-        const float3 ge1 = (P1 * inv11) * vol;
-        const float cap = p.membrane_force_scale * (p.c1 + p.c2) * thickness * sqrtf(rarea) * 100.0f;
+        const double s00 = c1 * (1.0 - i00 * idet) + c2 * (det * i00 + idet - tr * idet * i00);
+        const double s01 = c1 * (-i01 * idet) + c2 * (det * i01 - tr * idet * i01);
+        const double s11 = c1 * (1.0 - i11 * idet) + c2 * (det * i11 + idet - tr * idet * i11);
+        const double k2 = (double)p.membrane_force_scale * 2.0;
+        const double3 P0 = (F0 * s00 + F1 * s01) * k2;
+        const double3 P1 = (F0 * s01 + F1 * s11) * k2;
+        const double vol = (double)thickness * rarea;
+        const double3 ge0 = (P0 * inv00 + P1 * inv01) * vol;
+        const double3 ge1 = (P1 * inv11) * vol;
+        const double cap = (double)p.membrane_force_scale * (c1 + c2) * thickness * sqrt(rarea) * 100.0;
         const float3 fa = limit_norm(ge0 + ge1, cap), fb = limit_norm(-ge0, cap), fc = limit_norm(-ge1, cap);
         if (safe3(fa)) atomic_add3(s.internal_force, ia, fa);
         if (safe3(fb)) atomic_add3(s.internal_force, ib, fb);
@@ -260,8 +277,9 @@ __global__ void __launch_bounds__(kThreads) k_shell_faces(efsi_shell_state s, ef
       }
     }
     if (!p.region_loads && p.pressure != 0.0f) {
-      const float3 normal = avn > 1.0e-12f ? av * (1.0f / avn) : rn;
-      const float3 pf = normal * (p.pressure * area / 3.0f);
+      const double3 normal = avn > 1.0e-12 ? av * (1.0 / avn) : rn;
+      const double3 pfd = normal * ((double)p.pressure * area / 3.0);
+      const float3 pf = f3((float)pfd.x, (float)pfd.y, (float)pfd.z);
       if (safe3(pf)) {
         atomic_add3(s.external_force, ia, pf);
         atomic_add3(s.external_force, ib, pf);
@@ -272,13 +290,13 @@ __global__ void __launch_bounds__(kThreads) k_shell_faces(efsi_shell_state s, ef
   if (p.region_loads) {
     float3 load = f3(0.f, 0.f, 0.f);
     if (region == p.area_load_region)
-      load = load + f3(p.primary_area_load[0], p.primary_area_load[1], p.primary_area_load[2]) * rarea;
+      load = load + f3(p.primary_area_load[0], p.primary_area_load[1], p.primary_area_load[2]) * (float)rarea;
     if (region == p.primary_region) {
       load = load + f3(p.primary_reaction[0], p.primary_reaction[1], p.primary_reaction[2]) *
-                        (rarea / fmaxf(p.primary_area, 1.0e-12f));
+                        ((float)rarea / fmaxf(p.primary_area, 1.0e-12f));
     } else if (region == p.secondary_region) {
       load = load + f3(p.secondary_reaction[0], p.secondary_reaction[1], p.secondary_reaction[2]) *
-                        (rarea / fmaxf(p.secondary_area, 1.0e-12f));
+                        ((float)rarea / fmaxf(p.secondary_area, 1.0e-12f));
     }
     if (norm3(load) > 0.0f) {
       const float3 share = load * (1.0f / 3.0f);

@@ -122,7 +122,10 @@ class OracleTriShell:
     def __init__(self, vertices, faces, *, thickness_m, density_kgm3, c1_pa, c2_pa,
                  membrane_force_scale=1.0, grid_nodes=(36, 36, 36), bounds_padding_fraction=0.5,
                  face_region_id=None, primary_region_id, secondary_region_id, fixed_region_id=-1,
-                 primary_thickness_m=None, secondary_thickness_m=None):
+                 primary_thickness_m=None, secondary_thickness_m=None, f32_state=True):
+        # f32_state mirrors the reference's f32 fields (mooney_shell_mpm.py:179-196):
+        # x, u, v and the vertex forces are rounded to f32 where the reference stores them.
+        self.f32_state = bool(f32_state)
         v32 = np.asarray(vertices, dtype=np.float32)
         self.faces = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
         self.edges = unique_undirected_edges(self.faces).astype(np.int64)
@@ -221,6 +224,11 @@ class OracleTriShell:
                     out.append((idx, w))
         return out
 
+    def _store(self, *names):
+        if self.f32_state:
+            for n in names:
+                setattr(self, n, getattr(self, n).astype(np.float32).astype(np.float64))
+
     def _faces_forces(self, thickness, pressure):
         force, ok, pok, normal, area = mooney_face_forces(
             self.rest_x, self.x, self.faces, self.c1, self.c2, self.scale, thickness)
@@ -283,6 +291,7 @@ class OracleTriShell:
         gm = np.zeros(nn)
         gp = np.zeros((nn, 3))
         gf = np.zeros((nn, 3))
+        self._store("fint", "fext")
         # edge strain statistic (:542-550)
         e = self.edges
         rl = _norm(self.rest_x[e[:, 1]] - self.rest_x[e[:, 0]])
@@ -291,6 +300,7 @@ class OracleTriShell:
         max_edge = float(np.max(np.abs(np.maximum(cl[ok] / rl[ok], 1e-6) - 1.0))) if np.any(ok) else 0.0
         # particle pass (:930-959)
         self.fext += self.mass[:, None] * np.asarray(body, np.float64)[None, :]
+        self._store("fext")
         c = self._coord(self.x)
         oob = self._oob(c)
         total = self.fint + self.fext
@@ -344,6 +354,7 @@ class OracleTriShell:
         self.u[mo] += dt * self.v[mo]
         if len(mo):
             max_speed = max(max_speed, float(np.max(_norm(self.v[mo]))))
+        self._store("x", "u", "v")
         ib2 = ~self._oob(self._coord(self.x))
         cnt = int(np.sum(ib2))
         cc = self.x[ib2].sum(axis=0) / max(cnt, 1)

@@ -2,12 +2,18 @@
 drop-in TriMooneyShellMpmState) against the reference's known answers and the
 FP64 oracle (oracle/oracle_shell.py).
 
-Bounds: the kernels compute in f32 like the reference, the oracle in f64.
-After 20 steps of a pressurised, gravity-loaded 2,400-triangle plate the
-displacement u, velocity v and membrane forces agree with the oracle to a
-relative L2 error of 1e-4 (f32 rounding of about 6e-8 per operation, summed
-through 20 transfers with f32 atomics in a run-to-run order); normals and
-area weights, which depend on the positions only, to 1e-5."""
+Bounds: the kernels store f32 like the reference and evaluate the face law
+in f64; the oracle computes in f64 and rounds the state to f32 where the
+reference stores it.  The plate starts from a 5% equal-biaxial pre-stretch:
+near rest the membrane strains of a pressurised plate (about 1e-6) sit below
+the f32 resolution of its positions (about 1e-7 of 0.4 m), and the force of
+the reference itself is then rounding noise.  After 20 steps the
+displacement u agrees with the oracle to a relative L2 error of 1e-5, the
+velocity v to 2e-5 and the membrane force to 5e-4 (one f32 unit of a vertex
+position moves a face force by about 6e-5 of its value; the f32 atomics sum
+in a run-to-run order); normals and area weights to 1e-5.  Measured on a
+B200: u 1.1e-6, v 2.2e-6, membrane force 4.6e-5, external force 5.5e-7,
+normals 1.4e-7, area weights 3.4e-7."""
 
 import numpy as np
 import pytest
@@ -45,16 +51,24 @@ def test_shell_step_matches_oracle_over_20_steps():
     gpu = _make(mesh, face_region_id=region, **PLATE_LAW)
     ref = sc.OracleShellAdapter(mesh, face_region_id=region, **PLATE_LAW)
     np.testing.assert_allclose(gpu.mass_kg.to_numpy(), ref.o.mass, rtol=1e-5)
+    # 5% equal-biaxial pre-stretch: strains well above the f32 resolution of the positions
+    pre = (mesh.vertices * np.array([1.05, 1.05, 1.0])).astype(np.float32)
+    gpu.x.from_numpy(pre)
+    ref.x.from_numpy(pre)
     assert gpu.fixed_particle.to_numpy().tolist() == ref.o.fixed.tolist()
     assert gpu.vertex_region_id.to_numpy().tolist() == ref.o.vregion.tolist()
     for _ in range(20):
         rg = gpu.step(dt_s=1.0e-4, pressure_pa=50.0, body_acceleration_mps2=(0.0, 0.0, -9.81))
         rr = ref.step(dt_s=1.0e-4, pressure_pa=50.0, body_acceleration_mps2=(0.0, 0.0, -9.81))
     assert np.linalg.norm(ref.o.u) > 1e-6
-    assert _rel(gpu.u.to_numpy(), ref.o.u) <= 1e-4
-    assert _rel(gpu.v.to_numpy(), ref.o.v) <= 1e-4
-    assert _rel(gpu.internal_force_n.to_numpy(), ref.o.fint) <= 1e-4
-    assert _rel(gpu.external_force_n.to_numpy(), ref.o.fext) <= 1e-5
+    errors = {name: _rel(getattr(gpu, name).to_numpy(), getattr(ref.o, attr)) for name, attr in (
+        ("u", "u"), ("v", "v"), ("internal_force_n", "fint"), ("external_force_n", "fext"),
+        ("surface_normal", "normal"), ("area_weight_m2", "area_w"))}
+    print("membrane step vs oracle after 20 steps (relative L2):", errors)
+    assert _rel(gpu.u.to_numpy(), ref.o.u) <= 1e-5
+    assert _rel(gpu.v.to_numpy(), ref.o.v) <= 2e-5
+    assert _rel(gpu.internal_force_n.to_numpy(), ref.o.fint) <= 5e-4
+    assert _rel(gpu.external_force_n.to_numpy(), ref.o.fext) <= 5e-6
     assert _rel(gpu.surface_normal.to_numpy(), ref.o.normal) <= 1e-5
     assert _rel(gpu.area_weight_m2.to_numpy(), ref.o.area_w) <= 1e-5
     fixed = ref.o.fixed != 0
@@ -78,6 +92,9 @@ def test_shell_region_loads_match_oracle():
     mesh, region = sc.plate_mesh(24, 18)
     gpu = _make(mesh, face_region_id=region, primary_thickness_m=3.0e-3, **PLATE_LAW)
     ref = sc.OracleShellAdapter(mesh, face_region_id=region, primary_thickness_m=3.0e-3, **PLATE_LAW)
+    pre = (mesh.vertices * np.array([1.05, 1.05, 1.0])).astype(np.float32)
+    gpu.x.from_numpy(pre)
+    ref.x.from_numpy(pre)
     args = dict(dt_s=1.0e-4, primary_region_id=1, secondary_region_id=2, primary_area_load_npm2=(0.0, 0.0, 100.0),
                 primary_interface_reaction_n=(1.0, 0.0, 2.0), secondary_interface_reaction_n=(0.0, -1.0, 0.5))
     for _ in range(10):
@@ -88,9 +105,12 @@ def test_shell_region_loads_match_oracle():
     for _ in range(10):
         rg = gpu.advance_with_external_forces(dt_s=1.0e-4, primary_region_id=1, secondary_region_id=2)
         rr = ref.advance_with_external_forces(dt_s=1.0e-4, primary_region_id=1, secondary_region_id=2)
-    assert _rel(gpu.u.to_numpy(), ref.o.u) <= 1e-4
-    assert _rel(gpu.v.to_numpy(), ref.o.v) <= 1e-4
-    assert _rel(gpu.external_force_n.to_numpy(), ref.o.fext) <= 1e-5
+    print("membrane region loads vs oracle (relative L2):", {
+        "u": _rel(gpu.u.to_numpy(), ref.o.u), "v": _rel(gpu.v.to_numpy(), ref.o.v),
+        "external_force_n": _rel(gpu.external_force_n.to_numpy(), ref.o.fext)})
+    assert _rel(gpu.u.to_numpy(), ref.o.u) <= 1e-5
+    assert _rel(gpu.v.to_numpy(), ref.o.v) <= 2e-5
+    assert _rel(gpu.external_force_n.to_numpy(), ref.o.fext) <= 1e-6
     assert _rel(rg.primary_mean_velocity_mps, rr.primary_mean_velocity_mps) <= 1e-4
     assert _rel(rg.total_force_n, rr.total_force_n) <= 1e-5
 

@@ -36,5 +36,6 @@ def test_oracle_region_load_moves_region_and_conserves_momentum():
     v32 = mesh.vertices.astype(np.float32).astype(np.float64)  # the membrane stores f32 positions
     area = sum(0.5 * np.linalg.norm(np.cross(v32[f[1]] - v32[f[0]], v32[f[2]] - v32[f[0]]))
                for f, r in zip(mesh.faces, region) if r == 1)
-    assert rep["total_force_n"][2] == pytest.approx(100.0 * area, rel=1e-9)
+    # vertex forces are stored in f32 as the reference stores them
+    assert rep["total_force_n"][2] == pytest.approx(100.0 * area, rel=1e-7)
     assert rep["transfer_relative_error"] < 1e-9
