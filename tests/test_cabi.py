@@ -47,6 +47,24 @@ def test_argument_validation_without_gpu():
     assert lib.efsi_mpm_plan_create(0, 4, 4, 4, None) == 1
 
 
+def test_membrane_entry_points_reject_bad_arguments_without_gpu():
+    # efsi_shell_*: the state checks run before any launch
+    from ctypes import byref, c_float
+
+    lib = _native.load()
+    assert lib.efsi_shell_step(None, None, None, None, None) == 1
+    assert b"shell state is NULL" in lib.efsi_last_error()
+    st = _native.ShellState()
+    st.particle_count, st.face_count, st.nx, st.ny, st.nz = 3, 1, 3, 8, 8
+    assert lib.efsi_shell_update_normals(byref(st), None) == 1
+    assert b"grid_nodes must be at least 4" in lib.efsi_last_error()
+    st.nx = 8
+    for a in range(3):
+        st.dx[a] = 0.1
+    assert lib.efsi_shell_add_region_area_load(byref(st), 1, (c_float * 3)(0, 0, 1), None) == 1
+    assert b"buffer is NULL" in lib.efsi_last_error()
+
+
 def test_ib_entry_points_reject_bad_arguments_without_gpu():
     """The IB node search, boundary-condition and row entry points check
     their arguments before any device work (hibm_mpm.py:6069-6094, 7673-7678)."""
