@@ -146,3 +146,53 @@ def test_shell_argument_errors():
     st.x.from_numpy(np.full((3, 3), 1.0e3, np.float32))
     with pytest.raises(RuntimeError, match="outside the background grid"):
         st.step(dt_s=0.0, pressure_pa=0.0)
+
+
+def test_marker_forces_drive_the_membrane_as_the_coupled_runner_does():
+    """The sharp coupling of the membrane solid (cases/squid_soft_robot.py:8113-8135):
+    marker forces F = t A cleared and scattered onto the vertices
+    (hibm_mpm.py:4861-5010), then advance_with_external_forces, five times, on
+    the GPU and on the oracles.  Bounds as for the plain step."""
+    from types import SimpleNamespace
+
+    from easyfsi_b200.hibm_mpm import HibmMpmSurfaceMarkers
+    from oracle.oracle import OracleMarkers
+
+    mesh, region = sc.plate_mesh(24, 18)
+    gpu = _make(mesh, face_region_id=region, **PLATE_LAW)
+    ref = sc.OracleShellAdapter(mesh, face_region_id=region, **PLATE_LAW)
+    pre = (mesh.vertices * np.array([1.05, 1.05, 1.0])).astype(np.float32)
+    gpu.x.from_numpy(pre)
+    ref.x.from_numpy(pre)
+    # one marker per face at the rest centroid, normal +z, seeded pressure tractions
+    v = mesh.vertices.astype(np.float32)
+    tri = v[mesh.faces]
+    mx = tri.mean(axis=1).astype(np.float32)
+    area = (0.5 * np.linalg.norm(np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]), axis=1)).astype(np.float32)
+    normal = np.tile(np.array([0.0, 0.0, 1.0], np.float32), (len(mx), 1))
+    p = 40.0 + 10.0 * np.random.default_rng(4002).standard_normal(len(mx))
+    traction = -p[:, None] * normal.astype(np.float64)
+    radius = 0.03
+    markers = HibmMpmSurfaceMarkers(marker_capacity=len(mx))
+    markers.load_markers(positions_m=mx, velocities_mps=np.zeros_like(mx), normals=normal, areas_m2=area,
+                         region_ids=np.full(len(mx), 7, np.int32))
+    markers.set_marker_tractions_pa(traction)
+    markers.compute_marker_forces()
+    om = OracleMarkers(x=mx, normal=normal, area=area, region=np.full(len(mx), 7, np.int32))
+    om.t[:] = traction
+    om.compute_forces()
+    for _ in range(5):
+        markers.clear_mpm_external_forces(gpu.external_force_n, particle_count=gpu.particle_count, read_report=False)
+        markers.scatter_marker_forces_to_mpm_particles(gpu.external_force_n, gpu.x, particle_count=gpu.particle_count,
+                                                       support_radius_m=radius, read_report=False)
+        gpu.advance_with_external_forces(dt_s=1.0e-4, primary_region_id=1, secondary_region_id=2, read_report=False)
+        solid = SimpleNamespace(count=ref.o.np_, x=ref.o.x.astype(np.float32),
+                                fext=np.zeros((ref.o.np_, 3), np.float32))
+        om.scatter(solid, radius)
+        ref.o.fext = solid.fext.astype(np.float64)
+        ref.advance_with_external_forces(dt_s=1.0e-4, primary_region_id=1, secondary_region_id=2)
+    errors = {"u": _rel(gpu.u.to_numpy(), ref.o.u), "v": _rel(gpu.v.to_numpy(), ref.o.v),
+              "external_force_n": _rel(gpu.external_force_n.to_numpy(), ref.o.fext)}
+    print("membrane driven by marker forces vs oracles (relative L2):", errors)
+    assert np.linalg.norm(ref.o.fext) > 0.0
+    assert errors["u"] <= 1e-5 and errors["v"] <= 2e-5 and errors["external_force_n"] <= 1e-5
