@@ -60,6 +60,11 @@ enum { U_ACTIVE = 0, U_OOB, U_STRETCH_N, U_PCOUNT, U_SCOUNT, U_CCOUNT, U_MAX_STR
 static_assert(S_ND + (U_N + 1) / 2 <= EFSI_SHELL_SCRATCH_DOUBLES, "shell scratch too small");
 
 constexpr int kThreads = 256;
+// Vertex and face passes launch 64-thread CTAs: a c4 membrane has about 10k
+// vertices, which 256-thread CTAs put on 40 of the 148 SMs, each then bound
+// by its own L1 atomic and load latency; 64-thread CTAs spread the same warps
+// over every SM.
+constexpr int kSmall = 64;
 
 __device__ __forceinline__ unsigned* uslots(double* scratch) { return reinterpret_cast<unsigned*>(scratch + S_ND); }
 
@@ -682,6 +687,7 @@ __global__ void __launch_bounds__(kThreads) k_shell_region_load(efsi_shell_state
 }
 
 inline unsigned nblk(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + kThreads - 1) / kThreads); }
+inline unsigned nblk_small(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + kSmall - 1) / kSmall); }
 
 int check_state(const efsi_shell_state* s) {
   EFSI_ARG_CHECK(s != nullptr, "shell state is NULL");
@@ -697,9 +703,9 @@ int check_state(const efsi_shell_state* s) {
 }
 
 int launch_normals(const efsi_shell_state& s, cudaStream_t st) {
-  EFSI_COUNTED k_shell_clear_normals<<<nblk(s.particle_count), kThreads, 0, st>>>(s);
-  EFSI_COUNTED k_shell_face_normals<<<nblk(s.face_count), kThreads, 0, st>>>(s);
-  EFSI_COUNTED k_shell_finish<<<nblk(s.particle_count), kThreads, 0, st>>>(s, efsi_shell_params{}, nullptr, nullptr);
+  EFSI_COUNTED k_shell_clear_normals<<<nblk_small(s.particle_count), kSmall, 0, st>>>(s);
+  EFSI_COUNTED k_shell_face_normals<<<nblk_small(s.face_count), kSmall, 0, st>>>(s);
+  EFSI_COUNTED k_shell_finish<<<nblk_small(s.particle_count), kSmall, 0, st>>>(s, efsi_shell_params{}, nullptr, nullptr);
   EFSI_LAUNCH_CHECK();
   return EFSI_OK;
 }
@@ -760,13 +766,13 @@ extern "C" int efsi_shell_step(const efsi_shell_state* state, const efsi_shell_p
   const int64_t clear_work = std::max<int64_t>(3 * nn, 3 * (int64_t)s.particle_count);
   EFSI_COUNTED k_shell_clear<<<std::min<unsigned>(nblk(clear_work), 148u * 8u), kThreads, 0, st>>>(
       s, p.region_loads ? p.preserve_external_force : 0, scratch);
-  EFSI_COUNTED k_shell_faces<<<nblk(std::max(s.face_count, s.edge_count)), kThreads, 0, st>>>(s, p, scratch);
-  EFSI_COUNTED k_shell_p2g<<<nblk(s.particle_count), kThreads, 0, st>>>(s, p, scratch);
+  EFSI_COUNTED k_shell_faces<<<nblk_small(std::max(s.face_count, s.edge_count)), kSmall, 0, st>>>(s, p, scratch);
+  EFSI_COUNTED k_shell_p2g<<<nblk_small(s.particle_count), kSmall, 0, st>>>(s, p, scratch);
   EFSI_COUNTED k_shell_grid<<<nblk(nn), kThreads, 0, st>>>(s, p, scratch);
-  EFSI_COUNTED k_shell_g2p<<<nblk(s.particle_count), kThreads, 0, st>>>(s, p, scratch);
-  EFSI_COUNTED k_shell_radial<<<nblk(s.particle_count), kThreads, 0, st>>>(s, scratch);
-  EFSI_COUNTED k_shell_face_normals<<<nblk(s.face_count), kThreads, 0, st>>>(s);
-  EFSI_COUNTED k_shell_finish<<<nblk(s.particle_count), kThreads, 0, st>>>(s, p, scratch, report_device);
+  EFSI_COUNTED k_shell_g2p<<<nblk_small(s.particle_count), kSmall, 0, st>>>(s, p, scratch);
+  EFSI_COUNTED k_shell_radial<<<nblk_small(s.particle_count), kSmall, 0, st>>>(s, scratch);
+  EFSI_COUNTED k_shell_face_normals<<<nblk_small(s.face_count), kSmall, 0, st>>>(s);
+  EFSI_COUNTED k_shell_finish<<<nblk_small(s.particle_count), kSmall, 0, st>>>(s, p, scratch, report_device);
   EFSI_LAUNCH_CHECK();
   // algorithmic bytes: particles 120 B (x, u, v, rest_x, forces, normal read/written once, mass, area, flags),
   // faces 48 B (indices, region, three vertex reads), nodes 40 B cleared + 40 B touched by the update
